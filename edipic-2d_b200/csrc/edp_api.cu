@@ -1,0 +1,1106 @@
+// C ABI of the EDIPIC-2D B200 particle cycle: context lifecycle, particle I/O, step orchestration.
+// The call order of one step follows MainProg (pic2d_MainProgram.f90:151-309).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "edp_internal.cuh"
+
+int edp_fail(edp_ctx* c, int code, const std::string& msg)
+{
+    if (c) c->last_error = msg;
+    return code;
+}
+
+int edp_cuda_check(edp_ctx* c, cudaError_t e, const char* what)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s", (int)e, cudaGetErrorString(e), what);
+    return edp_fail(c, EDP_ERR_CUDA, buf);
+}
+
+edp_mcc_dev edp_make_mcc_dev(const edp_ctx* c)
+{
+    edp_mcc_dev m;
+    memset(&m, 0, sizeof(m));
+    const edp_tables& t = c->tab;
+    m.prob = c->mcc_prob;
+    m.energy = c->mcc_energy;
+    m.maxwell_v = c->maxwell_v;
+    m.n_act = t.n_act;
+    m.n_seg = t.n_seg;
+    m.n_values = t.n_values;
+    m.rmax = t.maxwell_rmax;
+    for (int i = 0; i <= t.n_seg; ++i) {
+        m.seg_value[i] = t.seg_value[i];
+        m.seg_index[i] = t.seg_index[i];
+    }
+    for (int i = 0; i < t.n_seg; ++i) m.seg_step[i] = t.seg_step[i];
+    m.pmax = t.max_colliding_fraction;
+    for (int p = 0; p < EDP_MAX_COLPROC; ++p) {
+        m.type[p] = t.colproc_type[p];
+        m.thr[p] = t.threshold_eV[p];
+        m.ion_species[p] = t.ion_species_produced[p] - 1;
+        m.ion_vfactor[p] = t.ion_velocity_factor[p];
+    }
+    m.mass_amu = t.neutral_mass_amu;
+    m.energy_factor = t.energy_factor_eV;
+    m.on = t.en_on;
+    return m;
+}
+
+edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s)
+{
+    edp_rcx_dev r;
+    memset(&r, 0, sizeof(r));
+    const edp_tables& t = c->tab;
+    r.maxwell_v = c->maxwell_v;
+    r.rmax = t.maxwell_rmax;
+    r.on = t.rcx_on[s];
+    r.prob_factor = t.rcx_prob_factor;
+    r.v_scale = c->p.v_scale_ms;
+    r.factor_eV = c->p.ion_mass_me[s] * t.energy_factor_eV;
+    r.sigma_1eV = t.rcx_sigma_1eV;
+    r.alpha = t.rcx_alpha;
+    r.pth2 = t.rcx_probab_thermal[s] * t.rcx_probab_thermal[s];
+    r.vfactor = t.rcx_vfactor[s];
+    return r;
+}
+
+namespace {
+
+template <class T>
+int dalloc(edp_ctx* c, T** p, size_t n)
+{
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return edp_cuda_check(c, e, "cudaMalloc");
+    return EDP_OK;
+}
+
+#define TRY(x)                        \
+    do {                              \
+        int _r = (x);                 \
+        if (_r != EDP_OK) return _r;  \
+    } while (0)
+
+// Boris rotation matrix K11..K33 (pic2d_ElectronDynamics.f90:91-113) for uniform B
+void rotation(double ax, double ay, double az, double* K)
+{
+    double ax2 = ax * ax, ay2 = ay * ay, az2 = az * az, th = ax2 + ay2 + az2, inv = 1.0 / (1.0 + th);
+    K[0] = (1.0 - th + 2.0 * ax2) * inv;
+    K[1] = 2.0 * (ax * ay + az) * inv;
+    K[2] = 2.0 * (ax * az - ay) * inv;
+    K[3] = 2.0 * (ax * ay - az) * inv;
+    K[4] = (1.0 - th + 2.0 * ay2) * inv;
+    K[5] = 2.0 * (ay * az + ax) * inv;
+    K[6] = 2.0 * (ax * az + ay) * inv;
+    K[7] = 2.0 * (ay * az - ax) * inv;
+    K[8] = (1.0 - th + 2.0 * az2) * inv;
+}
+
+int alloc_species(edp_ctx* c, int sp, int64_t n)
+{
+    if (c->cap[sp] > 0) {
+        if (n <= c->cap[sp]) return EDP_OK;
+        return edp_fail(c, EDP_ERR_CAPACITY, "particle count exceeds the capacity allocated for this species");
+    }
+    int64_t cap = c->p.capacity[sp] > 0 ? c->p.capacity[sp] : (n + n / 4 + 65536);
+    cap = (cap + 3) & ~(int64_t)3;
+    if (n > cap) return edp_fail(c, EDP_ERR_CAPACITY, "particle count exceeds params.capacity");
+    c->cap[sp] = cap;
+    if (c->p.precision == EDP_PREC_MIXED) {
+        for (int b = 0; b < 2; ++b) {
+            edp_species_mixed& m = b ? c->pm_alt[sp] : c->pm[sp];
+            if (b && c->p.sort_every <= 0) break;
+            TRY(dalloc(c, &m.cell, cap));
+            TRY(dalloc(c, &m.ox, cap));
+            TRY(dalloc(c, &m.oy, cap));
+            TRY(dalloc(c, &m.vx, cap));
+            TRY(dalloc(c, &m.vy, cap));
+            TRY(dalloc(c, &m.vz, cap));
+            TRY(dalloc(c, &m.id, cap));
+            TRY(dalloc(c, &m.tag, cap));
+        }
+    } else {
+        edp_species_fp64& d = c->pd[sp];
+        TRY(dalloc(c, &d.x, cap));
+        TRY(dalloc(c, &d.y, cap));
+        TRY(dalloc(c, &d.vx, cap));
+        TRY(dalloc(c, &d.vy, cap));
+        TRY(dalloc(c, &d.vz, cap));
+        TRY(dalloc(c, &d.id, cap));
+        TRY(dalloc(c, &d.tag, cap));
+    }
+    if (sp == 0) {
+        // add lists for ionisation products: a small fraction of the electron capacity
+        int64_t bc = std::max<int64_t>(65536, cap / 64);
+        c->born_cap = bc;
+        for (int b = 0; b < 2; ++b) {
+            edp_born& e = c->pend_e[b];
+            e.cap = bc;
+            TRY(dalloc(c, &e.x, bc));
+            TRY(dalloc(c, &e.y, bc));
+            TRY(dalloc(c, &e.vx, bc));
+            TRY(dalloc(c, &e.vy, bc));
+            TRY(dalloc(c, &e.vz, bc));
+        }
+        for (int s = 0; s < c->p.n_ion_species; ++s) {
+            edp_born& e = c->born_i[s];
+            e.cap = bc;
+            TRY(dalloc(c, &e.x, bc));
+            TRY(dalloc(c, &e.y, bc));
+            TRY(dalloc(c, &e.vx, bc));
+            TRY(dalloc(c, &e.vy, bc));
+            TRY(dalloc(c, &e.vz, bc));
+        }
+    }
+    return EDP_OK;
+}
+
+int finish_sync(edp_ctx* c)
+{
+    if (!c->sync) return EDP_OK;
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
+// -------------------------------------------------------------------------------- utility kernels
+__global__ void upload_kernel(edp_kparams kp, int precision, int64_t n, int64_t base, const double* x, const double* y,
+                              const double* vx, const double* vy, const double* vz, const int32_t* tag,
+                              const uint32_t* id, edp_species_mixed m, edp_species_fp64 d, unsigned int* eflag)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double X = x[k], Y = y[k];
+        bool bad = !(Y >= 0.0 && Y <= (double)kp.ncy);
+        if (kp.periodic) {
+            if (X >= (double)kp.ncx) X -= (double)kp.ncx;   // overlap cell of the reference layout
+            bad = bad || !(X >= 0.0 && X < (double)kp.ncx);
+        } else {
+            bad = bad || !(X >= 0.0 && X <= (double)kp.ncx);
+        }
+        if (bad) atomicOr(eflag, EDP_EFLAG_BOUNDS);
+        int64_t slot = base + k;
+        uint32_t pid = id ? id[k] : (uint32_t)(base + k);
+        int32_t t = tag ? tag[k] : 0;
+        if (precision == EDP_PREC_MIXED) {
+            int i = (int)X, j = (int)Y;
+            float ox, oy;
+            if (!kp.periodic && i == kp.ncx) {
+                i = kp.ncx - 1;
+                ox = 1.0f;
+            } else {
+                ox = (float)(X - (double)i);
+                if (ox >= 1.0f) {
+                    ox -= 1.0f;
+                    ++i;
+                    if (kp.periodic && i == kp.ncx) i = 0;
+                }
+            }
+            if (j == kp.ncy) {
+                j = kp.ncy - 1;
+                oy = 1.0f;
+            } else {
+                oy = (float)(Y - (double)j);
+                if (oy >= 1.0f) {
+                    if (j + 1 < kp.ncy) {
+                        oy -= 1.0f;
+                        ++j;
+                    } else {
+                        oy = 1.0f;
+                    }
+                }
+            }
+            m.cell[slot] = bad ? -1 : ((j << 16) | i);
+            m.ox[slot] = ox;
+            m.oy[slot] = oy;
+            m.vx[slot] = (float)vx[k];
+            m.vy[slot] = (float)vy[k];
+            m.vz[slot] = (float)vz[k];
+            m.id[slot] = pid;
+            m.tag[slot] = t;
+        } else {
+            d.x[slot] = bad ? -1.0e30 : X;
+            d.y[slot] = Y;
+            d.vx[slot] = vx[k];
+            d.vy[slot] = vy[k];
+            d.vz[slot] = vz[k];
+            d.id[slot] = pid;
+            d.tag[slot] = t;
+        }
+    }
+}
+
+__global__ void deposit_mixed_kernel(edp_kparams kp, edp_species_mixed m, const unsigned long long* n_slots,
+                                     unsigned long long* rho)
+{
+    const int64_t n = (int64_t)*n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int c = m.cell[k];
+        if (c < 0) continue;
+        int i = c & 0xFFFF, j = c >> 16;
+        double dx = (double)m.ox[k], dy = (double)m.oy[k];
+        double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
+        long long q00 = __double2ll_rn(vij * EDP_FIX_ONE), q10 = __double2ll_rn(vip1j * EDP_FIX_ONE);
+        long long q01 = __double2ll_rn(vijp1 * EDP_FIX_ONE), q11 = 4294967296LL - q00 - q10 - q01;
+        int i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+        atomicAdd(&rho[r0 + i], (unsigned long long)q00);
+        atomicAdd(&rho[r0 + i1], (unsigned long long)q10);
+        atomicAdd(&rho[r1 + i], (unsigned long long)q01);
+        atomicAdd(&rho[r1 + i1], (unsigned long long)q11);
+    }
+}
+
+__global__ void deposit_fp64_kernel(edp_kparams kp, edp_species_fp64 d, const unsigned long long* n_slots, double* rho)
+{
+    const int64_t n = (int64_t)*n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double X = d.x[k];
+        if (X < -1.0e29) continue;
+        double Y = d.y[k];
+        int i = (int)X, j = (int)Y;
+        if (!kp.periodic && X == (double)kp.ncx) i = kp.ncx - 1;
+        if (Y == (double)kp.ncy) j = kp.ncy - 1;
+        int i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        double dx = X - (double)i, dy = Y - (double)j;
+        double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
+        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+        atomicAdd(&rho[r0 + i], vij);
+        atomicAdd(&rho[r0 + i1], vip1j);
+        atomicAdd(&rho[r1 + i], vijp1);
+        atomicAdd(&rho[r1 + i1], 1.0 - vij - vip1j - vijp1);
+    }
+}
+
+// DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325): per_cell particles in each cell, uniform offsets,
+// Maxwellian components from the inverse-CDF table, Philox stream EDP_STREAM_INIT keyed by the particle id.
+__global__ void distribute_kernel(edp_kparams kp, int precision, int sp, int per_cell, double fconv, int zero_vz,
+                                  int copy_pos, const double* maxwell_v, int rmax, int64_t base_id,
+                                  edp_species_mixed m, edp_species_fp64 d, edp_species_mixed me, edp_species_fp64 de,
+                                  int64_t n)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t id = (uint32_t)(base_id + k);
+        uint32_t b0[4], b1[4];
+        edp_philox(0u, EDP_STREAM_INIT(sp), 0u, kp.seed_hi, id, kp.seed_lo, b0);
+        edp_philox(0u, EDP_STREAM_INIT(sp), 1u, kp.seed_hi, id, kp.seed_lo, b1);
+        int64_t cellno = k / per_cell;
+        int i = (int)(cellno % kp.ncx), j = (int)(cellno / kp.ncx);
+        double X, Y;
+        if (copy_pos) {
+            if (precision == EDP_PREC_MIXED) {
+                int c = me.cell[k];
+                X = (double)(c & 0xFFFF) + (double)me.ox[k];
+                Y = (double)(c >> 16) + (double)me.oy[k];
+                if (c < 0) X = -1.0e30;
+            } else {
+                X = de.x[k];
+                Y = de.y[k];
+            }
+        } else {
+            float fx = (float)edp_u01(b0[0]), fy = (float)edp_u01(b0[1]);
+            if (fx >= 1.0f) fx = 0.99999994f;
+            if (fy >= 1.0f) fy = 0.99999994f;
+            X = (double)i + (double)fx;
+            Y = (double)j + (double)fy;
+        }
+        double vx = edp_maxwell(maxwell_v, rmax, edp_u01(b0[2])) * fconv;
+        double vy = edp_maxwell(maxwell_v, rmax, edp_u01(b0[3])) * fconv;
+        double vz = zero_vz ? 0.0 : edp_maxwell(maxwell_v, rmax, edp_u01(b1[0])) * fconv;
+        bool dead = X < -1.0e29;
+        for (int q = 0; q < kp.n_inner && !dead; ++q)
+            if (X > (double)kp.ileft[q] && X < (double)kp.iright[q] && Y > (double)kp.jbottom[q] && Y < (double)kp.jtop[q])
+                dead = true;
+        if (precision == EDP_PREC_MIXED) {
+            int ii = (int)X, jj = (int)Y;
+            m.cell[k] = dead ? -1 : ((jj << 16) | ii);
+            m.ox[k] = dead ? 0.f : (float)(X - ii);
+            m.oy[k] = dead ? 0.f : (float)(Y - jj);
+            m.vx[k] = (float)vx;
+            m.vy[k] = (float)vy;
+            m.vz[k] = (float)vz;
+            m.id[k] = id;
+            m.tag[k] = 0;
+        } else {
+            d.x[k] = dead ? -1.0e30 : X;
+            d.y[k] = Y;
+            d.vx[k] = vx;
+            d.vy[k] = vy;
+            d.vz[k] = vz;
+            d.id[k] = id;
+            d.tag[k] = 0;
+        }
+    }
+}
+
+__global__ void count_live_kernel(edp_kparams kp, int precision, edp_species_mixed m, edp_species_fp64 d, int64_t n,
+                                  unsigned long long* live)
+{
+    unsigned long long acc = 0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        acc += (precision == EDP_PREC_MIXED) ? (m.cell[k] >= 0) : (d.x[k] > -1.0e29);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(live, acc);
+}
+
+__global__ void moments_kernel(int precision, edp_species_mixed m, edp_species_fp64 d, const unsigned long long* n_slots,
+                               double* out)
+{
+    const int64_t n = (int64_t)*n_slots;
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double vx, vy, vz;
+        if (precision == EDP_PREC_MIXED) {
+            if (m.cell[k] < 0) continue;
+            vx = m.vx[k];
+            vy = m.vy[k];
+            vz = m.vz[k];
+        } else {
+            if (d.x[k] < -1.0e29) continue;
+            vx = d.vx[k];
+            vy = d.vy[k];
+            vz = d.vz[k];
+        }
+        a[0] += 1.0;
+        a[1] += vx;
+        a[2] += vy;
+        a[3] += vz;
+        a[4] += vx * vx;
+        a[5] += vy * vy;
+        a[6] += vz * vz;
+    }
+    for (int q = 0; q < 7; ++q) {
+        double v = a[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&out[q], v);
+    }
+}
+
+__global__ void mcc_choose_kernel(edp_mcc_dev m, int64_t n, const double* E, const double* r, int32_t* out)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        out[k] = edp_mcc_choose_dev(m, E[k], r[k]);
+}
+
+__global__ void rotate_pending_kernel(edp_dev_counters* dc, int n_ion)
+{
+    dc->pend_e_count[1] = dc->pend_e_count[0];
+    dc->pend_e_count[0] = 0ull;
+}
+
+__global__ void reset_born_ions_kernel(edp_dev_counters* dc)
+{
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) dc->born_i_count[s] = 0ull;
+}
+
+__global__ void reset_step_counters_kernel(edp_dev_counters* dc)
+{
+    for (int p = 0; p < EDP_MAX_COLPROC; ++p) dc->en_coll_step[p] = 0ull;
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) dc->rcx_step[s] = 0ull;
+}
+
+// node array: device canonical layout -> reference layout on the host side buffer (periodic: 2 overlap columns)
+__global__ void expand_kernel(edp_kparams kp, int mode, const double* src, const float2* src2, int comp, double* dst,
+                              int wout)
+{
+    int64_t n = (int64_t)wout * kp.nyg;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % wout), j = (int)(q / wout);
+        int ic = kp.periodic ? (i % kp.ncx) : i;
+        int64_t s = (int64_t)j * kp.nxg + ic;
+        dst[q] = (mode == 0) ? src[s] : (comp == 0 ? (double)src2[s].x : (double)src2[s].y);
+    }
+}
+
+__global__ void contract_kernel(edp_kparams kp, int mode, const double* src, int wout, double* dst, float2* dst2, int comp)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
+        double v = src[(int64_t)j * wout + i];
+        if (mode == 0) dst[q] = v;
+        else if (comp == 0) dst2[q].x = (float)v;
+        else dst2[q].y = (float)v;
+    }
+}
+
+// one species' density with the wall factors, FP64 on the canonical grid
+__global__ void species_density_kernel(edp_kparams kp, int precision, const unsigned long long* fix, const double* dd,
+                                       double w, double* out)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
+        double r = (precision == EDP_PREC_MIXED) ? (double)(long long)fix[q] * EDP_FIX_INV : dd[q];
+        double f = 1.0;
+        if (kp.periodic) {
+            if (j == 0 || j == kp.ncy) f = 2.0;
+        } else {
+            bool ex = (i == 0 || i == kp.ncx), ey = (j == 0 || j == kp.ncy);
+            f = (ex && ey) ? 4.0 : ((ex || ey) ? 2.0 : 1.0);
+        }
+        out[q] = w * r * f;
+    }
+}
+
+unsigned grid_of(int64_t n, int64_t cap_blocks = 148 * 16)
+{
+    int64_t g = (n + 255) / 256;
+    g = std::min(g, cap_blocks);
+    return (unsigned)std::max<int64_t>(g, 1);
+}
+
+int ref_width(const edp_ctx* c) { return c->kp.periodic ? c->p.ncx + 2 : c->p.ncx + 1; }
+
+int zero_density(edp_ctx* c, int sp)
+{
+    const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    if (c->p.precision == EDP_PREC_MIXED)
+        EDP_CUDA(c, cudaMemsetAsync(c->rho_fix[sp], 0, nn * sizeof(unsigned long long), c->stream));
+    else
+        EDP_CUDA(c, cudaMemsetAsync(c->rho_d[sp], 0, nn * sizeof(double), c->stream));
+    return EDP_OK;
+}
+
+int after_particles_changed(edp_ctx* c, int sp)
+{
+    // live count, then the initial sort and the deposit the first field solve needs
+    c->hc->n_live[sp] = 0;
+    EDP_CUDA(c, cudaMemsetAsync(&c->dc->n_live[sp], 0, sizeof(unsigned long long), c->stream));
+    count_live_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->kp, c->p.precision, c->pm[sp], c->pd[sp],
+                                                                          c->host_slots[sp], &c->dc->n_live[sp]);
+    EDP_CUDA(c, cudaGetLastError());
+    c->sorted_end[sp] = 0;
+    c->n_chunks[sp] = 0;
+    if (c->p.precision == EDP_PREC_MIXED && c->p.sort_every > 0) TRY(edp_launch_sort(c, sp));
+    TRY(zero_density(c, sp));
+    TRY(edp_launch_deposit(c, sp));
+    c->uploaded[sp] = 1;
+    return EDP_OK;
+}
+
+}  // namespace
+
+int edp_launch_deposit(edp_ctx* c, int sp)
+{
+    if (c->p.precision == EDP_PREC_MIXED)
+        deposit_mixed_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->kp, c->pm[sp], &c->dc->n_slots[sp],
+                                                                                 c->rho_fix[sp]);
+    else
+        deposit_fp64_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->kp, c->pd[sp], &c->dc->n_slots[sp],
+                                                                                c->rho_d[sp]);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+// ======================================================================================= public ABI
+extern "C" {
+
+int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
+{
+    if (!p || !t || !out) return EDP_ERR_ARG;
+    *out = nullptr;
+    if (p->abi_version != EDP_ABI_VERSION) return EDP_ERR_ARG;
+    if (p->ncx < 2 || p->ncy < 2 || p->ncx > 32768 || p->ncy > 32767) return EDP_ERR_ARG;
+    if (p->n_ion_species < 1 || p->n_ion_species > EDP_MAX_ION_SPECIES) return EDP_ERR_ARG;
+    if (p->n_subcycles < 1 || (p->n_subcycles % 2) == 0) return EDP_ERR_ARG;
+    if (p->n_of_particles_cell < 1 || p->n_inner < 0 || p->n_inner > EDP_MAX_INNER) return EDP_ERR_ARG;
+    if (p->solver == EDP_SOLVER_FFTX) {
+        if (!p->periodic_x || (p->ncx & (p->ncx - 1)) != 0 || p->ncx > 4096) return EDP_ERR_ARG;
+    } else if (p->solver == EDP_SOLVER_CG) {
+        if (p->periodic_x) return EDP_ERR_ARG;
+    } else {
+        return EDP_ERR_ARG;
+    }
+    if (p->precision != EDP_PREC_MIXED && p->precision != EDP_PREC_FP64) return EDP_ERR_ARG;
+    if (t->en_on && (t->n_act < 1 || t->n_act > EDP_MAX_COLPROC || t->n_seg < 1 || t->n_seg > EDP_MAX_SEGMENTS ||
+                     !t->prob || !t->energy_eV))
+        return EDP_ERR_ARG;
+    if (!t->maxwell_v || t->maxwell_rmax < 1) return EDP_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return EDP_ERR_CUDA;
+
+    edp_ctx* c = new edp_ctx();
+    c->p = *p;
+    c->tab = *t;
+    cudaGetDevice(&c->device);
+    c->nspec = 1 + p->n_ion_species;
+    edp_kparams& kp = c->kp;
+    memset(&kp, 0, sizeof(kp));
+    kp.ncx = p->ncx;
+    kp.ncy = p->ncy;
+    kp.periodic = p->periodic_x;
+    kp.nxg = p->periodic_x ? p->ncx : p->ncx + 1;
+    kp.nyg = p->ncy + 1;
+    kp.n_inner = p->n_inner;
+    for (int n = 0; n < p->n_inner; ++n) {
+        kp.ileft[n] = p->inner_ileft[n];
+        kp.jbottom[n] = p->inner_jbottom[n];
+        kp.iright[n] = p->inner_iright[n];
+        kp.jtop[n] = p->inner_jtop[n];
+    }
+    kp.nsub = p->n_subcycles;
+    kp.seed_lo = (uint32_t)p->seed;
+    kp.seed_hi = (uint32_t)(p->seed >> 32);
+    rotation(-0.5 * p->bx, -0.5 * p->by, -0.5 * p->bz, c->K[0]);
+    for (int s = 0; s < p->n_ion_species; ++s) {
+        double qn = p->n_subcycles * 0.5 * p->ion_charge[s] / p->ion_mass_me[s];
+        rotation(qn * p->bx, qn * p->by, qn * p->bz, c->K[1 + s]);
+    }
+    int r = EDP_OK;
+    auto fail = [&](int code) {
+        edp_destroy(c);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(EDP_ERR_CUDA);
+    if (cudaMalloc(&c->dc, sizeof(edp_dev_counters)) != cudaSuccess) return fail(EDP_ERR_CUDA);
+    if (cudaMallocHost(&c->hc, sizeof(edp_dev_counters)) != cudaSuccess) return fail(EDP_ERR_CUDA);
+    memset(c->hc, 0, sizeof(edp_dev_counters));
+    cudaMemset(c->dc, 0, sizeof(edp_dev_counters));
+    if (cudaMalloc(&c->dev_small, 4096) != cudaSuccess) return fail(EDP_ERR_CUDA);
+    const int64_t nn = (int64_t)kp.nxg * kp.nyg;
+    if (p->precision == EDP_PREC_MIXED) {
+        if ((r = dalloc(c, &c->E2, nn)) || (r = dalloc(c, &c->acc2, nn))) return fail(r);
+        for (int s = 0; s < c->nspec; ++s)
+            if ((r = dalloc(c, &c->rho_fix[s], nn))) return fail(r);
+        cudaMemset(c->E2, 0, nn * sizeof(float2));
+        cudaMemset(c->acc2, 0, nn * sizeof(float2));
+    } else {
+        if ((r = dalloc(c, &c->Ex, nn)) || (r = dalloc(c, &c->Ey, nn)) || (r = dalloc(c, &c->accx, nn)) ||
+            (r = dalloc(c, &c->accy, nn)))
+            return fail(r);
+        for (int s = 0; s < c->nspec; ++s)
+            if ((r = dalloc(c, &c->rho_d[s], nn))) return fail(r);
+        cudaMemset(c->Ex, 0, nn * sizeof(double));
+        cudaMemset(c->Ey, 0, nn * sizeof(double));
+        cudaMemset(c->accx, 0, nn * sizeof(double));
+        cudaMemset(c->accy, 0, nn * sizeof(double));
+    }
+    if ((r = dalloc(c, &c->rho_total, nn)) || (r = dalloc(c, &c->phi, nn)) || (r = dalloc(c, &c->phi_prev, nn)))
+        return fail(r);
+    cudaMemset(c->phi, 0, nn * sizeof(double));
+    cudaMemset(c->rho_total, 0, nn * sizeof(double));
+    if (p->solver == EDP_SOLVER_CG) {
+        if ((r = dalloc(c, &c->cg_b, nn)) || (r = dalloc(c, &c->cg_r, nn)) || (r = dalloc(c, &c->cg_p, nn)) ||
+            (r = dalloc(c, &c->cg_Ap, nn)) || (r = dalloc(c, &c->cg_z, nn)) || (r = dalloc(c, &c->cg_kind, nn)))
+            return fail(r);
+    }
+    // sort workspace
+    c->ntx = (p->ncx + EDP_TILE - 1) / EDP_TILE;
+    c->nty = (p->ncy + EDP_TILE - 1) / EDP_TILE;
+    if (p->precision == EDP_PREC_MIXED) {
+        int64_t ntiles = (int64_t)c->ntx * c->nty, nkeys = ntiles * 256, nb = (nkeys + 2047) / 2048;
+        if ((r = dalloc(c, &c->sort_count, nkeys + 1)) || (r = dalloc(c, &c->sort_offset, nkeys + 1)) ||
+            (r = dalloc(c, &c->scan_tmp, nb + 1 + nkeys + ntiles + 2)))
+            return fail(r);
+    }
+    // tables
+    if (t->en_on) {
+        int64_t np = (int64_t)(t->n_values + 1) * t->n_act;
+        if ((r = dalloc(c, &c->mcc_prob, np)) || (r = dalloc(c, &c->mcc_energy, t->n_values + 1))) return fail(r);
+        cudaMemcpy(c->mcc_prob, t->prob, np * sizeof(double), cudaMemcpyHostToDevice);
+        cudaMemcpy(c->mcc_energy, t->energy_eV, (t->n_values + 1) * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    if ((r = dalloc(c, &c->maxwell_v, t->maxwell_rmax + 1))) return fail(r);
+    cudaMemcpy(c->maxwell_v, t->maxwell_v, (t->maxwell_rmax + 1) * sizeof(double), cudaMemcpyHostToDevice);
+    c->tab.prob = nullptr;
+    c->tab.energy_eV = nullptr;
+    c->tab.maxwell_v = nullptr;
+    if ((r = edp_fields_prepare(c))) return fail(r);
+    for (int s = 0; s < 4; ++s) c->phi_wall[s] = p->wall_phi_const[s] + p->wall_phi_var[s] * std::sin(p->wall_phase[s]);
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDP_ERR_CUDA);
+    *out = c;
+    return EDP_OK;
+}
+
+int edp_destroy(edp_ctx* c)
+{
+    if (!c) return EDP_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    auto F = [](void* q) {
+        if (q) cudaFree(q);
+    };
+    for (int s = 0; s < EDP_MAX_SPECIES; ++s) {
+        for (edp_species_mixed* m : {&c->pm[s], &c->pm_alt[s]}) {
+            F(m->cell); F(m->ox); F(m->oy); F(m->vx); F(m->vy); F(m->vz); F(m->id); F(m->tag);
+        }
+        edp_species_fp64& d = c->pd[s];
+        F(d.x); F(d.y); F(d.vx); F(d.vy); F(d.vz); F(d.id); F(d.tag);
+        F(c->chunks[s]);
+        F(c->rho_fix[s]);
+        F(c->rho_d[s]);
+    }
+    for (int b = 0; b < 2; ++b) {
+        edp_born& e = c->pend_e[b];
+        F(e.x); F(e.y); F(e.vx); F(e.vy); F(e.vz);
+    }
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) {
+        edp_born& e = c->born_i[s];
+        F(e.x); F(e.y); F(e.vx); F(e.vy); F(e.vz);
+    }
+    F(c->sort_count); F(c->sort_offset); F(c->scan_tmp);
+    F(c->E2); F(c->acc2); F(c->Ex); F(c->Ey); F(c->accx); F(c->accy);
+    F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
+    F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
+    F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v);
+    F(c->dc); F(c->dev_small);
+    if (c->hc) cudaFreeHost(c->hc);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return EDP_OK;
+}
+
+int edp_last_error(const edp_ctx* c, char* buf, size_t len)
+{
+    if (!c || !buf || len == 0) return EDP_ERR_ARG;
+    snprintf(buf, len, "%s", c->last_error.c_str());
+    return EDP_OK;
+}
+
+int edp_set_sync(edp_ctx* c, int sync)
+{
+    if (!c) return EDP_ERR_ARG;
+    c->sync = sync;
+    return EDP_OK;
+}
+
+int edp_synchronize(edp_ctx* c)
+{
+    if (!c) return EDP_ERR_ARG;
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
+int edp_upload_particles(edp_ctx* c, int sp, int64_t n, const double* x, const double* y, const double* vx,
+                         const double* vy, const double* vz, const int32_t* tag, const uint32_t* id)
+{
+    if (!c || sp < 0 || sp >= c->nspec || n < 0 || (n > 0 && (!x || !y || !vx || !vy || !vz)))
+        return edp_fail(c, EDP_ERR_ARG, "edp_upload_particles: bad arguments");
+    TRY(alloc_species(c, sp, n));
+    // staging copies of the host columns
+    double* dbuf = nullptr;
+    int32_t* tbuf = nullptr;
+    uint32_t* ibuf = nullptr;
+    const int64_t nn = std::max<int64_t>(n, 1);
+    EDP_CUDA(c, cudaMalloc(&dbuf, nn * 5 * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&tbuf, nn * sizeof(int32_t)));
+    EDP_CUDA(c, cudaMalloc(&ibuf, nn * sizeof(uint32_t)));
+    const double* cols[5] = {x, y, vx, vy, vz};
+    for (int q = 0; q < 5; ++q)
+        if (n) EDP_CUDA(c, cudaMemcpyAsync(dbuf + q * nn, cols[q], n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (tag && n) EDP_CUDA(c, cudaMemcpyAsync(tbuf, tag, n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    if (id && n) EDP_CUDA(c, cudaMemcpyAsync(ibuf, id, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    if (n)
+        upload_kernel<<<grid_of(n), 256, 0, c->stream>>>(c->kp, c->p.precision, n, 0, dbuf, dbuf + nn, dbuf + 2 * nn,
+                                                         dbuf + 3 * nn, dbuf + 4 * nn, tag ? tbuf : nullptr,
+                                                         id ? ibuf : nullptr, c->pm[sp], c->pd[sp], &c->dc->error_flags);
+    EDP_CUDA(c, cudaGetLastError());
+    unsigned long long ns = (unsigned long long)n, nid = (unsigned long long)n;
+    if (id && n) {
+        std::vector<uint32_t> h(id, id + n);
+        nid = (unsigned long long)*std::max_element(h.begin(), h.end()) + 1ull;
+    }
+    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->n_slots[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->next_id[sp], &nid, sizeof(nid), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(dbuf);
+    cudaFree(tbuf);
+    cudaFree(ibuf);
+    c->host_slots[sp] = n;
+    TRY(after_particles_changed(c, sp));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    unsigned int flags = 0;
+    EDP_CUDA(c, cudaMemcpy(&flags, &c->dc->error_flags, sizeof(flags), cudaMemcpyDeviceToHost));
+    if (flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "edp_upload_particles: particle outside the domain");
+    return EDP_OK;
+}
+
+int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv, int32_t zero_vz, int32_t copy_pos)
+{
+    if (!c || sp < 0 || sp >= c->nspec || per_cell < 1) return edp_fail(c, EDP_ERR_ARG, "edp_distribute_particles");
+    if (copy_pos && (sp == 0 || !c->uploaded[0])) return edp_fail(c, EDP_ERR_STATE, "electrons must be distributed first");
+    const int64_t n = (int64_t)per_cell * c->p.ncx * c->p.ncy;
+    if (copy_pos && (n != c->host_slots[0] || c->sorted_end[0] != 0))
+        return edp_fail(c, EDP_ERR_STATE, "ions copy electron positions: same per_cell, before the electron sort");
+    TRY(alloc_species(c, sp, n));
+    const int64_t base_id = 0;
+    distribute_kernel<<<grid_of(n, 148 * 64), 256, 0, c->stream>>>(
+        c->kp, c->p.precision, sp, per_cell, fconv, zero_vz, copy_pos, c->maxwell_v, c->tab.maxwell_rmax, base_id,
+        c->pm[sp], c->pd[sp], c->pm[0], c->pd[0], n);
+    EDP_CUDA(c, cudaGetLastError());
+    unsigned long long ns = (unsigned long long)n;
+    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->n_slots[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->next_id[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
+    c->host_slots[sp] = n;
+    // the electron array is sorted only after the ions copied its positions
+    if (sp == 0 && copy_pos == 0) {
+        c->hc->n_live[sp] = 0;
+        EDP_CUDA(c, cudaMemsetAsync(&c->dc->n_live[sp], 0, sizeof(unsigned long long), c->stream));
+        count_live_kernel<<<grid_of(n), 256, 0, c->stream>>>(c->kp, c->p.precision, c->pm[sp], c->pd[sp], n,
+                                                             &c->dc->n_live[sp]);
+        TRY(zero_density(c, sp));
+        TRY(edp_launch_deposit(c, sp));
+        c->uploaded[sp] = 1;
+        c->sorted_end[sp] = 0;
+        c->n_chunks[sp] = 0;
+        EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+        return EDP_OK;
+    }
+    TRY(after_particles_changed(c, sp));
+    if (copy_pos && c->p.precision == EDP_PREC_MIXED && c->p.sort_every > 0 && c->sorted_end[0] == 0)
+        TRY(edp_launch_sort(c, 0));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
+int edp_download_particles(edp_ctx* c, int sp, int64_t cap, int64_t* n_out, double* x, double* y, double* vx,
+                           double* vy, double* vz, int32_t* tag, uint32_t* id)
+{
+    if (!c || sp < 0 || sp >= c->nspec || !n_out) return edp_fail(c, EDP_ERR_ARG, "edp_download_particles");
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    unsigned long long ns = 0;
+    EDP_CUDA(c, cudaMemcpy(&ns, &c->dc->n_slots[sp], sizeof(ns), cudaMemcpyDeviceToHost));
+    const int64_t n = (int64_t)ns;
+    int64_t w = 0;
+    if (c->p.precision == EDP_PREC_MIXED) {
+        std::vector<int32_t> cell(n), tg(n);
+        std::vector<float> ox(n), oy(n), fvx(n), fvy(n), fvz(n);
+        std::vector<uint32_t> ids(n);
+        const edp_species_mixed& m = c->pm[sp];
+        if (n) {
+            EDP_CUDA(c, cudaMemcpy(cell.data(), m.cell, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(ox.data(), m.ox, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(oy.data(), m.oy, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(fvx.data(), m.vx, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(fvy.data(), m.vy, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(fvz.data(), m.vz, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(ids.data(), m.id, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(tg.data(), m.tag, n * 4, cudaMemcpyDeviceToHost));
+        }
+        for (int64_t k = 0; k < n; ++k) {
+            if (cell[k] < 0) continue;
+            if (w < cap) {
+                if (x) x[w] = (double)(cell[k] & 0xFFFF) + (double)ox[k];
+                if (y) y[w] = (double)(cell[k] >> 16) + (double)oy[k];
+                if (vx) vx[w] = fvx[k];
+                if (vy) vy[w] = fvy[k];
+                if (vz) vz[w] = fvz[k];
+                if (tag) tag[w] = tg[k];
+                if (id) id[w] = ids[k];
+            }
+            ++w;
+        }
+    } else {
+        std::vector<double> hx(n), hy(n), hvx(n), hvy(n), hvz(n);
+        std::vector<int32_t> tg(n);
+        std::vector<uint32_t> ids(n);
+        const edp_species_fp64& d = c->pd[sp];
+        if (n) {
+            EDP_CUDA(c, cudaMemcpy(hx.data(), d.x, n * 8, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(hy.data(), d.y, n * 8, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(hvx.data(), d.vx, n * 8, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(hvy.data(), d.vy, n * 8, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(hvz.data(), d.vz, n * 8, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(ids.data(), d.id, n * 4, cudaMemcpyDeviceToHost));
+            EDP_CUDA(c, cudaMemcpy(tg.data(), d.tag, n * 4, cudaMemcpyDeviceToHost));
+        }
+        for (int64_t k = 0; k < n; ++k) {
+            if (hx[k] < -1.0e29) continue;
+            if (w < cap) {
+                if (x) x[w] = hx[k];
+                if (y) y[w] = hy[k];
+                if (vx) vx[w] = hvx[k];
+                if (vy) vy[w] = hvy[k];
+                if (vz) vz[w] = hvz[k];
+                if (tag) tag[w] = tg[k];
+                if (id) id[w] = ids[k];
+            }
+            ++w;
+        }
+    }
+    *n_out = w;
+    if (w > cap) return edp_fail(c, EDP_ERR_CAPACITY, "edp_download_particles: host buffer too small");
+    return EDP_OK;
+}
+
+int edp_gather_charge_density(edp_ctx* c, int sp, double* rho_out)
+{
+    if (!c || sp < 0 || sp >= c->nspec) return edp_fail(c, EDP_ERR_ARG, "edp_gather_charge_density");
+    if (!rho_out) return EDP_OK;
+    const int w = ref_width(c);
+    const int64_t nref = (int64_t)w * c->kp.nyg;
+    double *tmp = nullptr, *ref = nullptr;
+    EDP_CUDA(c, cudaMalloc(&tmp, (int64_t)c->kp.nxg * c->kp.nyg * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&ref, nref * sizeof(double)));
+    double wgt = sp == 0 ? 1.0 : (double)c->p.ion_charge[sp - 1];
+    species_density_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, c->p.precision, c->rho_fix[sp], c->rho_d[sp],
+                                                                  wgt, tmp);
+    expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, tmp, nullptr, 0, ref, w);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemcpyAsync(rho_out, ref, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(tmp);
+    cudaFree(ref);
+    return EDP_OK;
+}
+
+int edp_update_wall_potentials(edp_ctx* c, int64_t t)
+{
+    if (!c) return EDP_ERR_ARG;
+    for (int s = 0; s < 4; ++s)
+        c->phi_wall[s] = c->p.wall_phi_const[s] + c->p.wall_phi_var[s] * std::sin(c->p.wall_omega[s] * (double)t + c->p.wall_phase[s]);
+    return EDP_OK;
+}
+
+int edp_field_fftx(edp_ctx* c, double* phi_out)
+{
+    if (!c) return EDP_ERR_ARG;
+    if (c->p.solver != EDP_SOLVER_FFTX) return edp_fail(c, EDP_ERR_STATE, "context was not set up for FFT_X");
+    TRY(edp_launch_density(c));
+    TRY(edp_launch_fftx(c));
+    TRY(edp_launch_efield(c));
+    if (phi_out) TRY(edp_get_field(c, EDP_FIELD_PHI, phi_out));
+    return finish_sync(c);
+}
+
+int edp_field_cg(edp_ctx* c, double rtol, int32_t max_it, int32_t warm, int32_t* iters_out)
+{
+    if (!c || max_it < 1 || !(rtol > 0.0)) return edp_fail(c, EDP_ERR_ARG, "edp_field_cg");
+    if (c->p.solver != EDP_SOLVER_CG) return edp_fail(c, EDP_ERR_STATE, "context was not set up for CG");
+    TRY(edp_launch_density(c));
+    int it = 0;
+    int r = edp_launch_cg(c, rtol, max_it, warm, &it);
+    if (iters_out) *iters_out = it;
+    TRY(edp_launch_efield(c));
+    if (r != EDP_OK) return r;
+    return finish_sync(c);
+}
+
+int edp_advance_electrons(edp_ctx* c)
+{
+    if (!c) return EDP_ERR_ARG;
+    if (!c->uploaded[0]) return edp_fail(c, EDP_ERR_STATE, "electrons not uploaded");
+    const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
+    const bool fuse = c->p.fuse_collisions != 0;
+    reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
+    TRY(zero_density(c, 0));
+    TRY(edp_launch_push(c, 0, ion_step, fuse));
+    TRY(edp_launch_append_pending(c, ion_step && fuse));
+    return finish_sync(c);
+}
+
+int edp_advance_ions(edp_ctx* c)
+{
+    if (!c) return EDP_ERR_ARG;
+    const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
+    if (!ion_step) return EDP_OK;
+    const bool fuse = c->p.fuse_collisions != 0;
+    for (int s = 0; s < c->p.n_ion_species; ++s) {
+        if (!c->uploaded[1 + s]) continue;
+        TRY(zero_density(c, 1 + s));
+        TRY(edp_launch_push(c, 1 + s, true, fuse));
+    }
+    return finish_sync(c);
+}
+
+int edp_collide_en(edp_ctx* c, int64_t* counters_out)
+{
+    if (!c) return EDP_ERR_ARG;
+    const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
+    if (ion_step && !c->p.fuse_collisions) TRY(edp_launch_collide_en(c));
+    if (counters_out) {
+        EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+        unsigned long long h[EDP_MAX_COLPROC];
+        EDP_CUDA(c, cudaMemcpy(h, c->dc->en_coll_step, sizeof(h), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < EDP_MAX_COLPROC; ++p) counters_out[p] = (int64_t)h[p];
+    }
+    return finish_sync(c);
+}
+
+int edp_collide_rcx(edp_ctx* c, int64_t* count_out)
+{
+    if (!c) return EDP_ERR_ARG;
+    const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
+    if (ion_step && !c->p.fuse_collisions) TRY(edp_launch_collide_rcx(c));
+    if (count_out) {
+        EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+        unsigned long long h[EDP_MAX_ION_SPECIES];
+        EDP_CUDA(c, cudaMemcpy(h, c->dc->rcx_step, sizeof(h), cudaMemcpyDeviceToHost));
+        int64_t s = 0;
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) s += (int64_t)h[q];
+        *count_out = s;
+    }
+    return finish_sync(c);
+}
+
+int edp_end_ion_cycle(edp_ctx* c)
+{
+    if (!c) return EDP_ERR_ARG;
+    const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
+    const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    if (ion_step) {
+        TRY(edp_launch_append_born_ions(c));
+        reset_born_ions_kernel<<<1, 1, 0, c->stream>>>(c->dc);
+        if (c->p.precision == EDP_PREC_MIXED) {
+            EDP_CUDA(c, cudaMemsetAsync(c->acc2, 0, nn * sizeof(float2), c->stream));
+        } else {
+            EDP_CUDA(c, cudaMemsetAsync(c->accx, 0, nn * sizeof(double), c->stream));
+            EDP_CUDA(c, cudaMemsetAsync(c->accy, 0, nn * sizeof(double), c->stream));
+        }
+        c->n_sub_phase = 0;
+    } else {
+        c->n_sub_phase++;
+    }
+    rotate_pending_kernel<<<1, 1, 0, c->stream>>>(c->dc, c->p.n_ion_species);
+    EDP_CUDA(c, cudaGetLastError());
+    c->pend_cur ^= 1;
+    c->t_cntr++;
+    c->steps_since_sort++;
+    if (c->p.precision == EDP_PREC_MIXED && c->p.sort_every > 0 && c->steps_since_sort >= c->p.sort_every &&
+        c->n_sub_phase == 0) {
+        for (int s = 0; s < c->nspec; ++s)
+            if (c->uploaded[s]) TRY(edp_launch_sort(c, s));
+        c->steps_since_sort = 0;
+    }
+    return finish_sync(c);
+}
+
+int edp_step(edp_ctx* c, int32_t nsteps)
+{
+    if (!c || nsteps < 0) return EDP_ERR_ARG;
+    for (int32_t k = 0; k < nsteps; ++k) {
+        TRY(edp_update_wall_potentials(c, c->t_cntr));
+        if (c->p.solver == EDP_SOLVER_FFTX) {
+            TRY(edp_launch_density(c));
+            TRY(edp_launch_fftx(c));
+            TRY(edp_launch_efield(c));
+        } else {
+            TRY(edp_launch_density(c));
+            int it = 0;
+            TRY(edp_launch_cg(c, 1e-8, 100000, EDP_WARM_PREVIOUS, &it));
+            TRY(edp_launch_efield(c));
+        }
+        TRY(edp_advance_electrons(c));
+        TRY(edp_advance_ions(c));
+        TRY(edp_collide_en(c, nullptr));
+        TRY(edp_collide_rcx(c, nullptr));
+        TRY(edp_end_ion_cycle(c));
+    }
+    return EDP_OK;
+}
+
+int edp_query_counters(edp_ctx* c, edp_counters* out)
+{
+    if (!c || !out) return EDP_ERR_ARG;
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    EDP_CUDA(c, cudaMemcpy(c->hc, c->dc, sizeof(edp_dev_counters), cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof(*out));
+    for (int s = 0; s < c->nspec; ++s) out->n_particles[s] = (int64_t)c->hc->n_live[s];
+    for (int k = 0; k < EDP_N_HIT_COUNTERS; ++k) {
+        out->electron_hits[k] = (int64_t)c->hc->e_hits[k];
+        out->ion_hits[k] = (int64_t)c->hc->i_hits[k];
+    }
+    for (int p = 0; p < EDP_MAX_COLPROC; ++p) out->en_collisions[p] = (int64_t)c->hc->en_coll[p];
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) out->rcx_collisions[s] = (int64_t)c->hc->rcx[s];
+    out->step = c->t_cntr;
+    out->cg_iterations = c->last_cg_iters;
+    out->cg_relres = c->last_cg_relres;
+    out->error_flags = (int32_t)c->hc->error_flags;
+    for (int s = 0; s < c->nspec; ++s) c->host_slots[s] = std::max<int64_t>((int64_t)c->hc->n_slots[s], 0);
+    if (c->hc->error_flags & EDP_EFLAG_CAPACITY) return edp_fail(c, EDP_ERR_CAPACITY, "particle capacity exceeded");
+    if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
+    if (c->hc->error_flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "particle outside the domain");
+    return EDP_OK;
+}
+
+int edp_get_field(edp_ctx* c, int which, double* out)
+{
+    if (!c || !out) return EDP_ERR_ARG;
+    const int w = ref_width(c);
+    const int64_t nref = (int64_t)w * c->kp.nyg;
+    double* ref = nullptr;
+    EDP_CUDA(c, cudaMalloc(&ref, nref * sizeof(double)));
+    const bool mixed = c->p.precision == EDP_PREC_MIXED;
+    switch (which) {
+    case EDP_FIELD_EX: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->Ex, c->E2, 0, ref, w); break;
+    case EDP_FIELD_EY: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->Ey, c->E2, 1, ref, w); break;
+    case EDP_FIELD_ACC_EX: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->accx, c->acc2, 0, ref, w); break;
+    case EDP_FIELD_ACC_EY: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->accy, c->acc2, 1, ref, w); break;
+    case EDP_FIELD_PHI: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, c->phi, nullptr, 0, ref, w); break;
+    case EDP_FIELD_RHO_TOTAL: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, c->rho_total, nullptr, 0, ref, w); break;
+    default: cudaFree(ref); return edp_fail(c, EDP_ERR_ARG, "edp_get_field: unknown field");
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemcpyAsync(out, ref, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(ref);
+    return EDP_OK;
+}
+
+int edp_set_field(edp_ctx* c, int which, const double* in)
+{
+    if (!c || !in) return EDP_ERR_ARG;
+    const int w = ref_width(c);
+    const int64_t nref = (int64_t)w * c->kp.nyg;
+    double* ref = nullptr;
+    EDP_CUDA(c, cudaMalloc(&ref, nref * sizeof(double)));
+    EDP_CUDA(c, cudaMemcpyAsync(ref, in, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const bool mixed = c->p.precision == EDP_PREC_MIXED;
+    const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    switch (which) {
+    case EDP_FIELD_EX: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->Ex, c->E2, 0); break;
+    case EDP_FIELD_EY: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->Ey, c->E2, 1); break;
+    case EDP_FIELD_ACC_EX: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->accx, c->acc2, 0); break;
+    case EDP_FIELD_ACC_EY: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->accy, c->acc2, 1); break;
+    case EDP_FIELD_PHI: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, 0, ref, w, c->phi, nullptr, 0); break;
+    case EDP_FIELD_RHO_TOTAL: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, 0, ref, w, c->rho_total, nullptr, 0); break;
+    default: cudaFree(ref); return edp_fail(c, EDP_ERR_ARG, "edp_set_field: unknown field");
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(ref);
+    return EDP_OK;
+}
+
+int edp_moments(edp_ctx* c, int sp, double out[7])
+{
+    if (!c || !out || sp < 0 || sp >= c->nspec) return EDP_ERR_ARG;
+    double* d = nullptr;
+    EDP_CUDA(c, cudaMalloc(&d, 7 * sizeof(double)));
+    EDP_CUDA(c, cudaMemsetAsync(d, 0, 7 * sizeof(double), c->stream));
+    moments_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->p.precision, c->pm[sp], c->pd[sp],
+                                                                       &c->dc->n_slots[sp], d);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemcpyAsync(out, d, 7 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(d);
+    return EDP_OK;
+}
+
+int edp_mcc_choose(edp_ctx* c, int64_t n, const double* E, const double* r, int32_t* out)
+{
+    if (!c || n < 0 || (n && (!E || !r || !out))) return EDP_ERR_ARG;
+    if (!c->tab.en_on) return edp_fail(c, EDP_ERR_STATE, "no electron-neutral collisions configured");
+    if (n == 0) return EDP_OK;
+    double *dE = nullptr, *dr = nullptr;
+    int32_t* dout = nullptr;
+    EDP_CUDA(c, cudaMalloc(&dE, n * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&dr, n * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&dout, n * sizeof(int32_t)));
+    EDP_CUDA(c, cudaMemcpyAsync(dE, E, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaMemcpyAsync(dr, r, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    mcc_choose_kernel<<<grid_of(n), 256, 0, c->stream>>>(edp_make_mcc_dev(c), n, dE, dr, dout);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemcpyAsync(out, dout, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(dE);
+    cudaFree(dr);
+    cudaFree(dout);
+    return EDP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,413 @@
+// Internal definitions of the EDIPIC-2D B200 particle cycle: device context, random streams and the
+// collision arithmetic shared by the fused and the separate collision passes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/edipic_gpu.h"
+
+#define EDP_MAX_SPECIES (1 + EDP_MAX_ION_SPECIES)
+
+// tile geometry of the mixed-precision push: particles are cell-sorted tile by tile; a CTA stages the
+// field and accumulates the density of its tile plus a halo of HALO cells in shared memory.
+#define EDP_TILE 16
+#define EDP_HALO 2
+#define EDP_WIN_CELLS (EDP_TILE + 2 * EDP_HALO)
+#define EDP_WIN_NODES (EDP_WIN_CELLS + 1)
+#define EDP_CHUNK 8192          // particles per CTA work item inside one tile
+#define EDP_PUSH_THREADS 256
+#define EDP_ITEMS 4             // particles per thread per iteration (128-bit loads)
+
+// fixed-point density scale: one macroparticle = 2^32 units
+#define EDP_FIX_ONE 4294967296.0
+#define EDP_FIX_INV 2.3283064365386962890625e-10
+
+// device error word bits
+#define EDP_EFLAG_CAPACITY 1
+#define EDP_EFLAG_BOUNDS 2
+#define EDP_EFLAG_PENDING 4
+
+struct edp_chunk {      // one CTA work item of the sorted push
+    int64_t start, end; // slot range
+    int32_t wx0, wy0;   // window origin (cells), tile origin minus halo
+};
+
+// device-resident per-step scalars and counters (one allocation, read back by edp_query_counters)
+struct edp_dev_counters {
+    unsigned long long n_slots[EDP_MAX_SPECIES];   // high-water slot count (append cursor)
+    unsigned long long n_live[EDP_MAX_SPECIES];
+    unsigned long long e_hits[EDP_N_HIT_COUNTERS];
+    unsigned long long i_hits[EDP_N_HIT_COUNTERS];
+    unsigned long long en_coll[EDP_MAX_COLPROC];
+    unsigned long long en_coll_step[EDP_MAX_COLPROC];
+    unsigned long long rcx[EDP_MAX_ION_SPECIES];
+    unsigned long long rcx_step[EDP_MAX_ION_SPECIES];
+    unsigned long long pend_e_count[2];            // electrons born by ionisation (double buffer)
+    unsigned long long born_i_count[EDP_MAX_ION_SPECIES];
+    unsigned long long next_id[EDP_MAX_SPECIES];
+    unsigned int error_flags;
+    unsigned int pad;
+    double cg_scalars[8];                           // rr, pAp, rr_new, bnorm2, ...
+};
+
+struct edp_species_mixed {
+    int32_t* cell = nullptr;   // linear cell j*ncx + i, -1 dead
+    float *ox = nullptr, *oy = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    uint32_t* id = nullptr;
+    int32_t* tag = nullptr;
+};
+
+struct edp_species_fp64 {
+    double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;  // x < -1e29: dead
+    uint32_t* id = nullptr;
+    int32_t* tag = nullptr;
+};
+
+// born particles waiting to join a main array (FP64 in both precisions; small)
+struct edp_born {
+    double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    int64_t cap = 0;
+};
+
+// constant parameters handed to kernels by value
+struct edp_kparams {
+    int32_t ncx, ncy, periodic, nxg, nyg;     // nxg = node columns stored (ncx periodic, ncx+1 walled)
+    int32_t n_inner;
+    int32_t ileft[EDP_MAX_INNER], jbottom[EDP_MAX_INNER], iright[EDP_MAX_INNER], jtop[EDP_MAX_INNER];
+    int32_t nsub;
+    uint32_t seed_lo, seed_hi;
+};
+
+struct edp_ctx {
+    edp_params p;
+    edp_kparams kp;
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int sync = 0;
+    int64_t t_cntr = 0;           // T_cntr
+    int32_t n_sub_phase = 0;      // n_sub of MainProg
+    int32_t nspec = 1;            // electrons + ion species
+    int64_t cap[EDP_MAX_SPECIES] = {0};
+    int64_t host_slots[EDP_MAX_SPECIES] = {0};   // host-side upper bound of n_slots
+    int64_t sorted_end[EDP_MAX_SPECIES] = {0};   // slots [0, sorted_end) are tile-sorted
+    int64_t steps_since_sort = 0;
+    int uploaded[EDP_MAX_SPECIES] = {0};
+
+    // particles
+    edp_species_mixed pm[EDP_MAX_SPECIES], pm_alt[EDP_MAX_SPECIES];
+    edp_species_fp64 pd[EDP_MAX_SPECIES];
+    edp_born pend_e[2];           // [cur] appended this step, [cur^1] filled this step
+    int pend_cur = 0;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+    int64_t born_cap = 0;
+
+    // sort
+    edp_chunk* chunks[EDP_MAX_SPECIES] = {nullptr};
+    int64_t n_chunks[EDP_MAX_SPECIES] = {0};
+    int64_t chunk_cap[EDP_MAX_SPECIES] = {0};
+    uint32_t* sort_count = nullptr;   // per-cell counters (ncells + 1)
+    unsigned long long* sort_offset = nullptr;
+    unsigned long long* scan_tmp = nullptr;
+    int32_t ntx = 0, nty = 0;         // tiles
+
+    // grids
+    float2* E2 = nullptr;             // mixed: (EX, EY) per node, FP32
+    float2* acc2 = nullptr;           // mixed: accumulated field for ions
+    double *Ex = nullptr, *Ey = nullptr, *accx = nullptr, *accy = nullptr;   // FP64 field
+    unsigned long long* rho_fix[EDP_MAX_SPECIES] = {nullptr};   // mixed: fixed-point density per species
+    double* rho_d[EDP_MAX_SPECIES] = {nullptr};                  // FP64 path density per species
+    double* rho_total = nullptr;      // factor_rho*(rho_i - rho_e) with wall factors
+    double* phi = nullptr;
+    double* phi_prev = nullptr;
+    double2* spec = nullptr;          // FFT_X spectrum [nyg][nm]
+    double* aeq = nullptr;            // a_eq [nm][nyg]
+    double2* twiddle = nullptr;       // exp(+2 pi i k / N), k < N/2
+    int32_t nm = 0;
+    // CG workspace
+    double *cg_b = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_z = nullptr;
+    int8_t* cg_kind = nullptr;        // 0 unknown, 1 Dirichlet
+    int32_t last_cg_iters = 0;
+    double last_cg_relres = 0.0;
+
+    // tables
+    double* mcc_prob = nullptr;
+    double* mcc_energy = nullptr;
+    double* maxwell_v = nullptr;
+    edp_tables tab;                   // scalar part (pointers are host pointers; device copies above)
+    int32_t host_n_act = 0;
+
+    edp_dev_counters* dc = nullptr;   // device counters
+    edp_dev_counters* hc = nullptr;   // pinned host mirror
+
+    // constant Boris rotation matrices (uniform B): [0] electrons, [1+s] ion species
+    double K[EDP_MAX_SPECIES][9];
+    void* dev_small = nullptr;        // 4 KB device block for kernel pointer tables
+    double phi_wall[4];               // current wall potentials (normalised)
+};
+
+// ------------------------------------------------------------------------------------------ Philox
+__host__ __device__ inline void edp_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                           uint32_t k1, uint32_t out[4])
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+// uniform in (0,1), exactly representable: (x + 1/2) 2^-32
+__host__ __device__ inline double edp_u01(uint32_t x) { return ((double)x + 0.5) * 2.3283064365386962890625e-10; }
+
+// random streams (counter word 1)
+#define EDP_STREAM_MCC 0u
+#define EDP_STREAM_RCX(s) (1u + ((uint32_t)(s) << 8))
+#define EDP_STREAM_INIT(sp) (2u + ((uint32_t)(sp) << 8))
+
+// --------------------------------------------------------------------------- collision tables (device)
+struct edp_mcc_dev {
+    const double* prob;       // [(n_values+1) * n_act]
+    const double* energy;     // [n_values+1]
+    const double* maxwell_v;  // [rmax+1]
+    int32_t n_act, n_seg, n_values, rmax;
+    double seg_value[EDP_MAX_SEGMENTS + 1];
+    double seg_step[EDP_MAX_SEGMENTS];
+    int32_t seg_index[EDP_MAX_SEGMENTS + 1];
+    double pmax;
+    int32_t type[EDP_MAX_COLPROC];
+    double thr[EDP_MAX_COLPROC];
+    int32_t ion_species[EDP_MAX_COLPROC];   // 0-based, -1 none
+    double ion_vfactor[EDP_MAX_COLPROC];
+    double mass_amu, energy_factor;
+    int32_t on;
+};
+
+struct edp_rcx_dev {
+    const double* maxwell_v;
+    int32_t on, rmax;
+    double prob_factor, v_scale, factor_eV, sigma_1eV, alpha, pth2, vfactor;
+};
+
+// GetMaxwellVelocity (pic2d_ElectronWallCollisions.f90:961-985)
+__device__ inline double edp_maxwell(const double* v, int rmax, double u)
+{
+    double R = rmax * u;
+    int indx = (int)R;
+    if (indx < rmax) return __ldg(&v[indx]) + (R - indx) * (__ldg(&v[indx + 1]) - __ldg(&v[indx]));
+    return __ldg(&v[rmax]);
+}
+
+// kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (pic2d_enCollisionsGeneralProc.f90:451-485) with the
+// arithmetic spelled out in round-to-nearest intrinsics, so it matches the oracle bit for bit.
+__device__ inline int edp_mcc_choose_dev(const edp_mcc_dev& m, double E, double r)
+{
+    int indx;
+    double a0, a1;
+    if (E >= m.seg_value[m.n_seg]) {
+        indx = m.n_values - 1;
+        a1 = 1.0;
+        a0 = 0.0;
+    } else if (E < m.seg_value[0]) {
+        indx = 0;
+        a1 = 0.0;
+        a0 = 1.0;
+    } else {
+        int seg = 1;
+        for (int i = m.n_seg - 1; i >= 0; --i)
+            if (E >= m.seg_value[i]) {
+                seg = i + 1;
+                break;
+            }
+        double step = m.seg_step[seg - 1];
+        double fi = __dadd_rn((double)m.seg_index[seg - 1], __ddiv_rn(__dsub_rn(E, m.seg_value[seg - 1]), step));
+        indx = (int)fi;
+        indx = max(0, min(indx, m.n_values - 1));
+        a1 = __ddiv_rn(__dsub_rn(E, __ldg(&m.energy[indx])), step);
+        a0 = __dsub_rn(1.0, a1);
+    }
+    const int na = m.n_act;
+    int k;
+    for (k = na; k >= 1; --k) {
+        double thr = __fma_rn(a1, __ldg(&m.prob[(int64_t)(indx + 1) * na + k - 1]),
+                              __dmul_rn(a0, __ldg(&m.prob[(int64_t)indx * na + k - 1])));
+        if (r > thr) break;
+    }
+    return k + 1;
+}
+
+__device__ inline void edp_rotate(double cosk, double sink, double cosf, double sinf, double Vx, double Vy,
+                                  double Vz, double& ox, double& oy, double& oz)
+{
+    double V = sqrt(Vx * Vx + Vy * Vy + Vz * Vz);
+    double Vxy = sqrt(Vx * Vx + Vy * Vy);
+    if (Vxy > 1.0e-20) {
+        double a = Vx / Vxy, b = Vy / Vxy;
+        ox = Vx * cosk + (sinf * V * b + cosf * Vz * a) * sink;
+        oy = Vy * cosk - (sinf * V * a - cosf * Vz * b) * sink;
+        oz = Vz * cosk - Vxy * cosf * sink;
+    } else {
+        ox = fabs(Vz) * sink * cosf;
+        oy = fabs(Vz) * sink * sinf;
+        oz = Vz * cosk;
+    }
+}
+
+__device__ inline double edp_okh(double e, double R)
+{
+    double c = 1.0 - 2.0 * R / (1.0 + 8.0 * (e / 27.21) * (1.0 - R));
+    return fmax(fmin(0.999999999999, c), -0.999999999999);
+}
+
+// result of one electron's MCC test
+struct edp_mcc_out {
+    int kind_index;   // 0 none, else 1..n_act (counted)
+    int born;         // ionisation produced an electron + ion
+    double ne[3], ni[3];
+    int ion_species;
+};
+
+// PERFORM_ELECTRON_NEUTRAL_COLLISIONS + en_Collision_* (pic2d_enCollisionsSpecificProc.f90:61-639) for one
+// electron with Philox stream 0 (block 0 = select, kind, density; blocks 1-2 = scattering variates).
+__device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id, uint32_t step, uint32_t seed_lo,
+                                               uint32_t seed_hi, double& vx, double& vy, double& vz)
+{
+    edp_mcc_out o;
+    o.kind_index = 0;
+    o.born = 0;
+    uint32_t b0[4];
+    edp_philox(step, EDP_STREAM_MCC, 0u, seed_hi, id, seed_lo, b0);
+    if (!(edp_u01(b0[0]) < m.pmax)) return o;
+    double r = edp_u01(b0[1]);
+    double v2 = __fma_rn(vz, vz, __fma_rn(vy, vy, __dmul_rn(vx, vx)));
+    double E = __dmul_rn(v2, m.energy_factor);
+    int ki = edp_mcc_choose_dev(m, E, r);
+    if (ki > m.n_act) return o;
+    int kind = m.type[ki - 1];
+    double thr = m.thr[ki - 1];
+    if ((kind == 20 || kind == 30) && E <= thr) return o;
+    uint32_t b1[4], b2[4];
+    edp_philox(step, EDP_STREAM_MCC, 1u, seed_hi, id, seed_lo, b1);
+    double u0 = edp_u01(b1[0]), u1 = edp_u01(b1[1]), u2 = edp_u01(b1[2]), u3 = edp_u01(b1[3]);
+    double ox, oy, oz;
+    o.kind_index = ki;
+    if (kind == 10 || kind == 11) {
+        double c = (kind == 10) ? edp_okh(E, u0) : fmax(fmin(0.999999999999, 1.0 - 2.0 * u0), -0.999999999999);
+        double ks = acos(c), s = sin(ks), fi = u1 * 6.28318530718;
+        edp_rotate(c, s, cos(fi), sin(fi), vx, vy, vz, ox, oy, oz);
+        double alpha = sqrt(1.0 - (0.001097161 / m.mass_amu) * (1.0 - c));
+        vx = ox * alpha;
+        vy = oy * alpha;
+        vz = oz * alpha;
+        return o;
+    }
+    if (kind == 20) {
+        double esc = fmax(0.0, E - thr);
+        double c = edp_okh(esc, u0);
+        double ks = acos(c), s = sin(ks), fi = u1 * 6.28318530718;
+        edp_rotate(c, s, cos(fi), sin(fi), vx, vy, vz, ox, oy, oz);
+        double alpha = sqrt(esc / E);
+        vx = ox * alpha;
+        vy = oy * alpha;
+        vz = oz * alpha;
+        return o;
+    }
+    // ionisation, B = 10 eV (pic2d_enCollisionsSpecificProc.f90:451-629)
+    edp_philox(step, EDP_STREAM_MCC, 2u, seed_hi, id, seed_lo, b2);
+    double u4 = edp_u01(b2[0]), u5 = edp_u01(b2[1]), u6 = edp_u01(b2[2]), u7 = edp_u01(b2[3]);
+    const double B = 10.0;
+    double eej = B * tan(u0 * atan(0.5 * (E - thr) / B));
+    eej = fmax(0.0, fmin(eej, 0.5 * (E - thr)));
+    double esc = fmax(0.0, E - thr - eej);
+    double csc = edp_okh(esc, u1), ksc = acos(csc), ssc = sin(ksc), fsc = u2 * 6.28318530718;
+    double cej = edp_okh(eej, u3), kej = acos(cej), sej = sin(kej), fej = u4 * 6.28318530718;
+    double Vx = vx, Vy = vy, Vz = vz;
+    edp_rotate(csc, ssc, cos(fsc), sin(fsc), Vx, Vy, Vz, ox, oy, oz);
+    double asc = sqrt(esc / E);
+    vx = ox * asc;
+    vy = oy * asc;
+    vz = oz * asc;
+    edp_rotate(cej, sej, cos(fej), sin(fej), Vx, Vy, Vz, ox, oy, oz);
+    double aej = sqrt(eej / E);
+    o.ne[0] = ox * aej;
+    o.ne[1] = oy * aej;
+    o.ne[2] = oz * aej;
+    double f = m.ion_vfactor[ki - 1];
+    o.ni[0] = edp_maxwell(m.maxwell_v, m.rmax, u5) * f;
+    o.ni[1] = edp_maxwell(m.maxwell_v, m.rmax, u6) * f;
+    o.ni[2] = edp_maxwell(m.maxwell_v, m.rmax, u7) * f;
+    o.ion_species = m.ion_species[ki - 1];
+    o.born = (o.ion_species >= 0) ? 1 : 0;
+    return o;
+}
+
+// PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:90-121) for one ion; true on exchange.
+__device__ inline bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, uint32_t step, uint32_t species,
+                                   uint32_t seed_lo, uint32_t seed_hi, double& vx, double& vy, double& vz)
+{
+    double vsq = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+    double en = __dmul_rn(vsq, r.factor_eV);
+    double vabs = __dmul_rn(sqrt(vsq), r.v_scale);
+    double l = __dsub_rn(1.0, __dmul_rn(r.alpha, log(fmax(en, 0.001))));
+    double p = __dmul_rn(__dmul_rn(r.prob_factor, vabs), __dmul_rn(__dmul_rn(r.sigma_1eV, l), l));
+    p = sqrt(__dadd_rn(__dmul_rn(p, p), r.pth2));
+    uint32_t b[4];
+    edp_philox(step, EDP_STREAM_RCX(species), 0u, seed_hi, id, seed_lo, b);
+    if (!(edp_u01(b[0]) <= p)) return false;
+    vx = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[1])) * r.vfactor;
+    vy = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[2])) * r.vfactor;
+    vz = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[3])) * r.vfactor;
+    return true;
+}
+
+// --------------------------------------------------------------------------------- host helpers
+int edp_fail(edp_ctx* c, int code, const std::string& msg);
+int edp_cuda_check(edp_ctx* c, cudaError_t e, const char* what);
+#define EDP_CUDA(ctx, call)                                            \
+    do {                                                               \
+        cudaError_t _e = (call);                                       \
+        if (_e != cudaSuccess) return edp_cuda_check((ctx), _e, #call); \
+    } while (0)
+
+edp_mcc_dev edp_make_mcc_dev(const edp_ctx* c);
+edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
+
+// kernels launched from edp_api.cu, defined in the other translation units
+int edp_launch_push(edp_ctx* c, int species, bool ion_step, bool fuse);
+int edp_launch_collide_en(edp_ctx* c);
+int edp_launch_collide_rcx(edp_ctx* c);
+int edp_launch_append_pending(edp_ctx* c, bool ion_step);
+int edp_launch_append_born_ions(edp_ctx* c);
+int edp_launch_sort(edp_ctx* c, int species);
+int edp_launch_density(edp_ctx* c);
+int edp_launch_fftx(edp_ctx* c);
+int edp_launch_efield(edp_ctx* c);
+int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters);
+int edp_launch_distribute(edp_ctx* c, int species, int per_cell, double factor_convert, int zero_vz, int copy_pos);
+int edp_launch_upload(edp_ctx* c, int species, int64_t n, const double* dx, const double* dy, const double* dvx,
+                      const double* dvy, const double* dvz, const int32_t* dtag, const uint32_t* did);
+int edp_launch_download(edp_ctx* c, int species, int64_t cap, int64_t* n_out, double* x, double* y, double* vx,
+                        double* vy, double* vz, int32_t* tag, uint32_t* id);
+int edp_launch_moments(edp_ctx* c, int species, double out[7]);
+int edp_launch_mcc_choose(edp_ctx* c, int64_t n, const double* E, const double* r, int32_t* out);
+int edp_fields_prepare(edp_ctx* c);   // one-time FFT/CG tables
+int edp_launch_deposit(edp_ctx* c, int species);   // CIC deposit of the whole array without a push

@@ -1,0 +1,430 @@
+// Field part of the cycle:
+//  density   the deposit (fixed point or FP64) -> rho = (sum_s Qs rho_s - rho_e)/N_ppc with the wall factors
+//            of GATHER_ELECTRON_CHARGE_DENSITY (pic2d_ElectronDynamics.f90:1802-1880) and the combination of
+//            SOLVE_POISSON_FFTX_LINSYSY (pic2d_ElectricFieldCalc_FFT_X.f90:72-85)
+//  FFT_X     SOLVE_POISSON_FFTX_LINSYSY (:3-1320): real FFT of every row along x, per-mode tridiagonal solve
+//            along y with the spectral diagonal -2 - 4 pi^2 n^2/N^2 and a_eq of PREPARE_SYS_Y
+//            (pic2d_Prepare_FFTX_SYSY.f90:826-899), inverse FFT. The row transforms are radix-2 in shared
+//            memory, one CTA per row; the Thomas sweeps run one thread per mode with coalesced rows.
+//  E         CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:1324-1547) / CALCULATE_ELECTRIC_FIELD
+//            (pic2d_ElectricFieldCalc_PETSc.F90:360-805), acc_E += E
+//  CG        replacement of SOLVE_POTENTIAL_WITH_PETSC (pic2d_ElectricFieldCalc_PETSc.F90:7-355) on the operator of
+//            SolverInitialization (pic2d_PETSc_Solver.F90:42-1350) with Dirichlet nodes eliminated, FP64 dots.
+#include <cmath>
+#include <vector>
+
+#include "edp_internal.cuh"
+
+namespace {
+
+__global__ void density_kernel(edp_kparams kp, int precision, int nion, const unsigned long long* const* rho_fix,
+                               const double* const* rho_d, const double* qs, double factor_rho, double* out)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
+        double re, ri = 0.0;
+        if (precision == EDP_PREC_MIXED) {
+            re = (double)(long long)rho_fix[0][q] * EDP_FIX_INV;
+            for (int s = 0; s < nion; ++s) ri += qs[s] * ((double)(long long)rho_fix[1 + s][q] * EDP_FIX_INV);
+        } else {
+            re = rho_d[0][q];
+            for (int s = 0; s < nion; ++s) ri += qs[s] * rho_d[1 + s][q];
+        }
+        double f = 1.0;
+        if (kp.periodic) {
+            if (j == 0 || j == kp.ncy) f = 2.0;
+        } else {
+            bool ex = (i == 0 || i == kp.ncx), ey = (j == 0 || j == kp.ncy);
+            f = (ex && ey) ? 4.0 : ((ex || ey) ? 2.0 : 1.0);
+        }
+        out[q] = factor_rho * ((ri * f) - (re * f));
+    }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// in-place radix-2 DIT FFT of N complex values already stored in bit-reversed order; sign +1 uses tw, -1 conj(tw)
+__device__ void smem_fft(double2* x, int N, const double2* __restrict__ tw, int sign)
+{
+    for (int len = 2; len <= N; len <<= 1) {
+        const int half = len >> 1, stride = N / len;
+        for (int b = threadIdx.x; b < N / 2; b += blockDim.x) {
+            int grp = b / half, k = b - grp * half;
+            int a = grp * len + k, c = a + half;
+            double2 w = __ldg(&tw[k * stride]);
+            if (sign < 0) w.y = -w.y;
+            double2 t = cmul(w, x[c]);
+            double2 u = x[a];
+            x[a] = make_double2(u.x + t.x, u.y + t.y);
+            x[c] = make_double2(u.x - t.x, u.y - t.y);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int bitrev(int v, int logn) { return (int)(__brev((unsigned)v) >> (32 - logn)); }
+
+__global__ void fftx_forward(edp_kparams kp, const double* __restrict__ rho, double phi_bottom, double phi_top,
+                             const double2* __restrict__ tw, int logn, int nm, double2* __restrict__ spec)
+{
+    extern __shared__ double2 x[];
+    const int N = kp.ncx, j = blockIdx.x;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        double v = rho[(int64_t)j * kp.nxg + i];
+        if (j == 0) v = phi_bottom;
+        if (j == kp.ncy) v = phi_top;
+        x[bitrev(i, logn)] = make_double2(v, 0.0);
+    }
+    __syncthreads();
+    smem_fft(x, N, tw, +1);
+    for (int m = threadIdx.x; m < nm; m += blockDim.x) {
+        double2 v = x[m];
+        if (m == 0 || m == N / 2) v.y = 0.0;
+        spec[(int64_t)j * nm + m] = v;
+    }
+}
+
+// SOLVE_POISSON_FFTX_LINSYSY :690-756, metal walls (a_eq(0) = a_eq(J) = 0)
+__global__ void fftx_thomas(int J, int nm, const double* __restrict__ aeq, double2* __restrict__ spec)
+{
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nm) return;
+    double2 prev = spec[m];  // rhs(0) = transformed wall row
+    for (int j = 1; j <= J - 1; ++j) {
+        double a = aeq[(int64_t)j * nm + m];
+        double2 y = spec[(int64_t)j * nm + m];
+        prev = make_double2((-y.x - prev.x) * a, (-y.y - prev.y) * a);
+        spec[(int64_t)j * nm + m] = prev;
+    }
+    double2 next = spec[(int64_t)J * nm + m];
+    for (int j = J - 1; j >= 0; --j) {
+        double a = aeq[(int64_t)j * nm + m];
+        double2 r = spec[(int64_t)j * nm + m];
+        next = make_double2(r.x - a * next.x, r.y - a * next.y);
+        spec[(int64_t)j * nm + m] = next;
+    }
+}
+
+__global__ void fftx_inverse(edp_kparams kp, const double2* __restrict__ spec, const double2* __restrict__ tw, int logn,
+                             int nm, double* __restrict__ phi)
+{
+    extern __shared__ double2 x[];
+    const int N = kp.ncx, j = blockIdx.x;
+    for (int m = threadIdx.x; m < N; m += blockDim.x) {
+        double2 v;
+        if (m < nm) v = spec[(int64_t)j * nm + m];
+        else {
+            v = spec[(int64_t)j * nm + (N - m)];
+            v.y = -v.y;
+        }
+        x[bitrev(m, logn)] = v;
+    }
+    __syncthreads();
+    smem_fft(x, N, tw, -1);
+    const double inv = 1.0 / N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) phi[(int64_t)j * kp.nxg + i] = x[i].x * inv;
+}
+
+__global__ void efield_kernel(edp_kparams kp, const double* __restrict__ phi, double f2, double f1, int precision,
+                              float2* E2, float2* acc2, double* Ex, double* Ey, double* accx, double* accy)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    const int J = kp.ncy;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
+        auto P = [&](int ii, int jj) { return phi[(int64_t)jj * kp.nxg + ii]; };
+        double ex, ey;
+        if (kp.periodic) {
+            int im = i == 0 ? kp.ncx - 1 : i - 1, ip = i == kp.ncx - 1 ? 0 : i + 1;
+            ex = f2 * (P(im, j) - P(ip, j));
+        } else {
+            if (i == 0) ex = f1 * (P(0, j) - P(1, j));
+            else if (i == kp.ncx) ex = f1 * (P(kp.ncx - 1, j) - P(kp.ncx, j));
+            else ex = f2 * (P(i - 1, j) - P(i + 1, j));
+        }
+        if (j == 0) ey = f1 * (P(i, 0) - P(i, 1));
+        else if (j == J) ey = f1 * (P(i, J - 1) - P(i, J));
+        else ey = f2 * (P(i, j - 1) - P(i, j + 1));
+        if (precision == EDP_PREC_MIXED) {
+            E2[q] = make_float2((float)ex, (float)ey);
+            float2 a = acc2[q];
+            acc2[q] = make_float2(a.x + (float)ex, a.y + (float)ey);
+        } else {
+            Ex[q] = ex;
+            Ey[q] = ey;
+            accx[q] += ex;
+            accy[q] += ey;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------ CG
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+struct CgGeom {
+    edp_kparams kp;
+    double wall[4];
+    double inner[EDP_MAX_INNER];
+};
+
+__device__ __forceinline__ int cg_node_kind(const CgGeom& g, int i, int j, double* val)
+{
+    const edp_kparams& kp = g.kp;
+    for (int n = 0; n < kp.n_inner; ++n)
+        if (i >= kp.ileft[n] && i <= kp.iright[n] && j >= kp.jbottom[n] && j <= kp.jtop[n]) {
+            *val = g.inner[n];
+            return 1;
+        }
+    if (j == 0) { *val = g.wall[0]; return 1; }
+    if (j == kp.ncy) { *val = g.wall[1]; return 1; }
+    if (i == 0) { *val = g.wall[2]; return 1; }
+    if (i == kp.ncx) { *val = g.wall[3]; return 1; }
+    return 0;
+}
+
+// Dirichlet values, RHS with eliminated neighbours, initial guess; accumulates |b|^2
+__global__ void cg_setup(CgGeom g, const double* __restrict__ rho, int warm, const double* __restrict__ x0,
+                         int8_t* kind, double* phi, double* b, double* scal)
+{
+    const edp_kparams& kp = g.kp;
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    double acc = 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
+        double v;
+        int k = cg_node_kind(g, i, j, &v);
+        kind[q] = (int8_t)k;
+        if (k) {
+            phi[q] = v;
+            b[q] = 0.0;
+            continue;
+        }
+        double s = rho[q], d;
+        if (cg_node_kind(g, i - 1, j, &d)) s += d;
+        if (cg_node_kind(g, i + 1, j, &d)) s += d;
+        if (cg_node_kind(g, i, j - 1, &d)) s += d;
+        if (cg_node_kind(g, i, j + 1, &d)) s += d;
+        b[q] = s;
+        phi[q] = (warm == EDP_WARM_ZERO) ? 0.0 : x0[q];
+        acc += s * s;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(&scal[0], acc);
+}
+
+__device__ __forceinline__ double apply_A(const edp_kparams& kp, const int8_t* kind, const double* v, int64_t q)
+{
+    double s = 4.0 * v[q];
+    const int64_t w = kp.nxg;
+    if (!kind[q - 1]) s -= v[q - 1];
+    if (!kind[q + 1]) s -= v[q + 1];
+    if (!kind[q - w]) s -= v[q - w];
+    if (!kind[q + w]) s -= v[q + w];
+    return s;
+}
+
+// r = b - A x, p = r, rr accumulated
+__global__ void cg_residual(edp_kparams kp, const int8_t* kind, const double* x, const double* b, double* r, double* p,
+                            double* rr)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    double acc = 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        if (kind[q]) {
+            r[q] = 0.0;
+            p[q] = 0.0;
+            continue;
+        }
+        double v = b[q] - apply_A(kp, kind, x, q);
+        r[q] = v;
+        p[q] = v;
+        acc += v * v;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(rr, acc);
+}
+
+__global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, double* Ap, double* pAp)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    double acc = 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        if (kind[q]) {
+            Ap[q] = 0.0;
+            continue;
+        }
+        double v = apply_A(kp, kind, p, q);
+        Ap[q] = v;
+        acc += p[q] * v;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(pAp, acc);
+}
+
+__global__ void cg_update(edp_kparams kp, const int8_t* kind, const double* rr, const double* pAp, const double* p,
+                          const double* Ap, double* x, double* r, double* rr_new)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    const double alpha = *rr / *pAp;
+    double acc = 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        if (kind[q]) continue;
+        x[q] += alpha * p[q];
+        double v = r[q] - alpha * Ap[q];
+        r[q] = v;
+        acc += v * v;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(rr_new, acc);
+}
+
+__global__ void cg_direction(edp_kparams kp, const int8_t* kind, const double* rr, const double* rr_new, const double* r,
+                             double* p)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    const double beta = *rr_new / *rr;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        if (!kind[q]) p[q] = r[q] + beta * p[q];
+}
+
+unsigned grid_nodes(const edp_kparams& kp)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 8) g = 148 * 8;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+int edp_fields_prepare(edp_ctx* c)
+{
+    if (c->p.solver != EDP_SOLVER_FFTX) return EDP_OK;
+    const int N = c->p.ncx, J = c->p.ncy;
+    c->nm = N / 2 + 1;
+    std::vector<double2> tw(N / 2);
+    const double PI = 3.141592653589793;
+    for (int k = 0; k < N / 2; ++k) tw[k] = make_double2(std::cos(2.0 * PI * k / N), std::sin(2.0 * PI * k / N));
+    // a_eq of PREPARE_SYS_Y (pic2d_Prepare_FFTX_SYSY.f90:834-899) for metal walls, layout [j][n]
+    std::vector<double> a((size_t)(J + 1) * c->nm);
+    for (int m = 0; m < c->nm; ++m) {
+        double d = -2.0 - 4.0 * PI * PI * (double)m * (double)m / ((double)N * (double)N);
+        a[m] = 0.0;
+        for (int j = 1; j <= J - 1; ++j) a[(size_t)j * c->nm + m] = 1.0 / (d - a[(size_t)(j - 1) * c->nm + m]);
+        a[(size_t)J * c->nm + m] = 0.0;
+    }
+    EDP_CUDA(c, cudaMalloc(&c->twiddle, tw.size() * sizeof(double2)));
+    EDP_CUDA(c, cudaMalloc(&c->aeq, a.size() * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&c->spec, (size_t)(J + 1) * c->nm * sizeof(double2)));
+    EDP_CUDA(c, cudaMemcpy(c->twiddle, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    EDP_CUDA(c, cudaMemcpy(c->aeq, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice));
+    size_t smem = (size_t)N * sizeof(double2);
+    if (smem > 48 * 1024) {
+        EDP_CUDA(c, cudaFuncSetAttribute(fftx_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        EDP_CUDA(c, cudaFuncSetAttribute(fftx_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    return EDP_OK;
+}
+
+int edp_launch_density(edp_ctx* c)
+{
+    struct Ptrs {
+        const unsigned long long* f[EDP_MAX_SPECIES];
+        const double* d[EDP_MAX_SPECIES];
+        double qs[EDP_MAX_ION_SPECIES];
+    } h;
+    for (int s = 0; s < EDP_MAX_SPECIES; ++s) {
+        h.f[s] = c->rho_fix[s];
+        h.d[s] = c->rho_d[s];
+    }
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) h.qs[s] = (double)c->p.ion_charge[s];
+    static_assert(sizeof(Ptrs) <= 4096, "pointer table");
+    Ptrs* d = reinterpret_cast<Ptrs*>(c->dev_small);
+    EDP_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    density_kernel<<<grid_nodes(c->kp), 256, 0, c->stream>>>(c->kp, c->p.precision, c->p.n_ion_species, d->f, d->d,
+                                                             d->qs, 1.0 / c->p.n_of_particles_cell, c->rho_total);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+int edp_launch_fftx(edp_ctx* c)
+{
+    const int N = c->p.ncx;
+    int logn = 0;
+    while ((1 << logn) < N) ++logn;
+    size_t smem = (size_t)N * sizeof(double2);
+    int thr = std::min(512, std::max(32, N / 2));
+    fftx_forward<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->rho_total, c->phi_wall[0], c->phi_wall[1], c->twiddle,
+                                                     logn, c->nm, c->spec);
+    fftx_thomas<<<(c->nm + 127) / 128, 128, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);
+    fftx_inverse<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->spec, c->twiddle, logn, c->nm, c->phi);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+int edp_launch_efield(edp_ctx* c)
+{
+    const double f2 = c->p.f_scale_v / (c->p.e_scale_vm * 2.0 * c->p.delta_x_m);
+    const double f1 = c->p.f_scale_v / (c->p.e_scale_vm * c->p.delta_x_m);
+    efield_kernel<<<grid_nodes(c->kp), 256, 0, c->stream>>>(c->kp, c->phi, f2, f1, c->p.precision, c->E2, c->acc2,
+                                                            c->Ex, c->Ey, c->accx, c->accy);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
+{
+    const edp_kparams& kp = c->kp;
+    CgGeom g;
+    g.kp = kp;
+    for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
+    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    double* scal = nullptr;   // [0] |b|^2, then rr[k] at 1 + 2k, pAp[k] at 2 + 2k
+    const int nscal = 2 * (max_it + 2) + 2;
+    EDP_CUDA(c, cudaMallocAsync(&scal, nscal * sizeof(double), c->stream));
+    EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
+    const unsigned gr = grid_nodes(kp);
+    const double* x0 = (warm == EDP_WARM_PREVIOUS || warm == EDP_WARM_USER) ? c->phi : nullptr;
+    cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, x0 ? x0 : c->phi, c->cg_kind, c->phi, c->cg_b, scal);
+    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
+    double h[2];
+    EDP_CUDA(c, cudaMemcpyAsync(h, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    double bn = std::sqrt(h[0]);
+    if (bn == 0.0) bn = 1.0;
+    double rel = std::sqrt(h[1]) / bn;
+    int it = 0;
+    const int check = 8;
+    while (rel > rtol && it < max_it) {
+        int stop = std::min(max_it, it + check);
+        for (; it < stop; ++it) {
+            double* rr = &scal[1 + 2 * it];
+            double* pAp = &scal[2 + 2 * it];
+            double* rrn = &scal[1 + 2 * (it + 1)];
+            cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp);
+            cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r, rrn);
+            cg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, rrn, c->cg_r, c->cg_p);
+        }
+        EDP_CUDA(c, cudaMemcpyAsync(h, &scal[1 + 2 * it], sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+        rel = std::sqrt(h[0]) / bn;
+    }
+    EDP_CUDA(c, cudaFreeAsync(scal, c->stream));
+    EDP_CUDA(c, cudaGetLastError());
+    c->last_cg_iters = it;
+    c->last_cg_relres = rel;
+    if (iters) *iters = it;
+    return rel <= rtol ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
+}

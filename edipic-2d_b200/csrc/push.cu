@@ -1,0 +1,903 @@
+// Fused push + charge deposit (+ collisions) of EDIPIC-2D's particle cycle on sm_100a.
+//
+//  ADVANCE_ELECTRONS  pic2d_ElectronDynamics.f90:3-513     bilinear E gather, Boris rotation, move, walls
+//  ADVANCE_IONS       pic2d_IonDynamics.f90:3-524          same on acc_E with QM2s and N_subcycles
+//  GATHER_*_CHARGE_DENSITY  pic2d_ElectronDynamics.f90:1597-1639 / pic2d_IonDynamics.f90:1540-2003 (CIC)
+//  PERFORM_ELECTRON_NEUTRAL_COLLISIONS / PERFORM_RESONANT_CHARGE_EXCHANGE in the epilogue when fused.
+//
+// Mixed precision: int32 packed cell (j<<16 | i) + FP32 in-cell offsets and FP32 velocities, 128-bit loads
+// (4 particles per thread). Particles are tile-sorted; one CTA handles a chunk of one tile, stages the
+// field of the tile + halo in shared memory and accumulates the deposit there in 64-bit fixed point
+// (2^32 units per macroparticle) before one flush of global atomics. Particles that left the window
+// (and the unsorted tail of newly appended particles) use global memory directly.
+#include "edp_internal.cuh"
+
+namespace {
+
+struct PushArgs {
+    edp_kparams kp;
+    edp_species_mixed P;
+    const edp_chunk* chunks;
+    int64_t n_chunks;
+    int64_t tail_start;
+    const unsigned long long* n_slots;
+    int64_t tail_groups_per_cta;
+    int64_t tail_ctas;
+    const float2* E;
+    unsigned long long* rho;
+    float K[9];
+    float qh, ez_term, xmul;
+    int use_rot, is_ion, species;
+    int do_mcc, do_rcx;
+    uint32_t step;
+    edp_mcc_dev mcc;
+    edp_rcx_dev rcx;
+    edp_dev_counters* dc;
+    edp_born pend_next;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+};
+
+__device__ __forceinline__ int wrapx(int lx, const edp_kparams& kp)
+{
+    if (kp.periodic) {
+        if (lx >= kp.ncx) lx -= kp.ncx;
+        else if (lx < 0) lx += kp.ncx;
+    }
+    return lx;
+}
+
+// wall classification of the walled domain (SURROUNDED_BY_WALL corners), :212-518
+__device__ __forceinline__ int wall_object(double X, double Y, double xmax, double ymax)
+{
+    if (X < 0.0) {
+        if (Y >= 1.0 && Y <= ymax - 1.0) return 2;
+        if (Y < 1.0) return ((0.0 - X) < (0.0 - Y)) ? 0 : 2;
+        return ((0.0 - X) < (Y - ymax)) ? 1 : 2;
+    }
+    if (X > xmax) {
+        if (Y >= 1.0 && Y <= ymax - 1.0) return 3;
+        if (Y < 1.0) return ((X - xmax) < (0.0 - Y)) ? 0 : 3;
+        return ((X - xmax) < (Y - ymax)) ? 1 : 3;
+    }
+    return (Y > ymax) ? 1 : 0;
+}
+
+__device__ __forceinline__ void record_born(const edp_born& b, unsigned long long* count, unsigned int* eflag,
+                                            double x, double y, const double* v)
+{
+    unsigned long long k = atomicAdd(count, 1ull);
+    if ((int64_t)k >= b.cap) {
+        atomicOr(eflag, EDP_EFLAG_PENDING);
+        return;
+    }
+    b.x[k] = x;
+    b.y[k] = y;
+    b.vx[k] = v[0];
+    b.vy[k] = v[1];
+    b.vz[k] = v[2];
+}
+
+struct Smem {
+    float2 E[EDP_WIN_NODES * EDP_WIN_NODES];
+    unsigned long long R[EDP_WIN_NODES * EDP_WIN_NODES];
+    unsigned long long cnt[32];   // [0..7] hits, [8..15] en kinds, [16] rcx, [17] removed
+};
+
+// One particle: returns false when it was absorbed (the caller stores cell = -1).
+__device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, int& cell,
+                                         float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id)
+{
+    const edp_kparams& kp = a.kp;
+    int i = cell & 0xFFFF, j = cell >> 16;
+    // ---- gather (bilinear, :82-86)
+    int lx = wrapx(i - wx0, kp), ly = j - wy0;
+    bool inw = windowed && (unsigned)lx < EDP_WIN_CELLS && (unsigned)ly < EDP_WIN_CELLS;
+    float2 e00, e10, e01, e11;
+    if (inw) {
+        int b = ly * EDP_WIN_NODES + lx;
+        e00 = s.E[b];
+        e10 = s.E[b + 1];
+        e01 = s.E[b + EDP_WIN_NODES];
+        e11 = s.E[b + EDP_WIN_NODES + 1];
+    } else {
+        int i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+        e00 = __ldg(&a.E[r0 + i]);
+        e10 = __ldg(&a.E[r0 + i1]);
+        e01 = __ldg(&a.E[r1 + i]);
+        e11 = __ldg(&a.E[r1 + i1]);
+    }
+    float axp = ox, axm = 1.0f - ox, ayp = oy, aym = 1.0f - oy;
+    float w00 = axm * aym, w10 = axp * aym, w01 = axm * ayp, w11 = axp * ayp;
+    float EX = e00.x * w00 + e10.x * w10 + e01.x * w01 + e11.x * w11;
+    float EY = e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11;
+    // ---- Boris (:95-130 / ions :99-149)
+    float q = a.qh;
+    if (a.use_rot) {
+        float mx = vx + q * EX, my = vy + q * EY, mz = vz + a.ez_term;
+        float px = a.K[0] * mx + a.K[1] * my + a.K[2] * mz;
+        float py = a.K[3] * mx + a.K[4] * my + a.K[5] * mz;
+        float pz = a.K[6] * mx + a.K[7] * my + a.K[8] * mz;
+        vx = px + q * EX;
+        vy = py + q * EY;
+        vz = pz + a.ez_term;
+    } else if (a.is_ion) {
+        vx = vx + (q + q) * EX;
+        vy = vy + (q + q) * EY;
+        vz = vz + (a.ez_term + a.ez_term);
+    } else {
+        vx = (vx + q * EX) + q * EX;
+        vy = (vy + q * EY) + q * EY;
+        vz = (vz + a.ez_term) + a.ez_term;
+    }
+    // ---- move (:148-149 / :154-155)
+    float nx = ox + vx * a.xmul, ny = oy + vy * a.xmul;
+    float fx = floorf(nx), fy = floorf(ny);
+    int ni = i + (int)fx, nj = j + (int)fy;
+    nx -= fx;
+    ny -= fy;
+    if (nx >= 1.0f) { nx -= 1.0f; ++ni; }
+    if (ny >= 1.0f) { ny -= 1.0f; ++nj; }
+    // ---- inner objects (:160-172): strictly inside
+    for (int n = 0; n < kp.n_inner; ++n) {
+        bool in = (ni > kp.ileft[n] || (ni == kp.ileft[n] && nx > 0.0f)) && ni < kp.iright[n] &&
+                  (nj > kp.jbottom[n] || (nj == kp.jbottom[n] && ny > 0.0f)) && nj < kp.jtop[n];
+        if (in) {
+            atomicAdd(&s.cnt[4 + n], 1ull);
+            return false;
+        }
+    }
+    // ---- domain boundaries (:174-511)
+    if (kp.periodic) {
+        if (ni < 0) ni += kp.ncx;
+        else if (ni >= kp.ncx) ni -= kp.ncx;
+        if (nj < 0) { atomicAdd(&s.cnt[0], 1ull); return false; }
+        if (nj > kp.ncy || (nj == kp.ncy && ny > 0.0f)) { atomicAdd(&s.cnt[1], 1ull); return false; }
+    } else {
+        bool outx = ni < 0 || ni > kp.ncx || (ni == kp.ncx && nx > 0.0f);
+        bool outy = nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f);
+        if (outx || outy) {
+            int obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
+            atomicAdd(&s.cnt[obj], 1ull);
+            return false;
+        }
+        if (ni == kp.ncx) { ni = kp.ncx - 1; nx = 1.0f; }   // X == c_X_area_max (:68)
+    }
+    if (nj == kp.ncy) { nj = kp.ncy - 1; ny = 1.0f; }       // Y == c_Y_area_max (:69)
+    cell = (nj << 16) | ni;
+    ox = nx;
+    oy = ny;
+    // ---- deposit (:1597-1639): exact FP64 weights of the FP32 offsets, rounded to 2^-32
+    double dx = (double)nx, dy = (double)ny;
+    double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
+    long long q00 = __double2ll_rn(vij * EDP_FIX_ONE);
+    long long q10 = __double2ll_rn(vip1j * EDP_FIX_ONE);
+    long long q01 = __double2ll_rn(vijp1 * EDP_FIX_ONE);
+    long long q11 = 4294967296LL - q00 - q10 - q01;
+    int dlx = wrapx(ni - wx0, kp), dly = nj - wy0;
+    if (windowed && (unsigned)dlx < EDP_WIN_CELLS && (unsigned)dly < EDP_WIN_CELLS) {
+        int b = dly * EDP_WIN_NODES + dlx;
+        atomicAdd(&s.R[b], (unsigned long long)q00);
+        atomicAdd(&s.R[b + 1], (unsigned long long)q10);
+        atomicAdd(&s.R[b + EDP_WIN_NODES], (unsigned long long)q01);
+        atomicAdd(&s.R[b + EDP_WIN_NODES + 1], (unsigned long long)q11);
+    } else {
+        int i1 = ni + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        int64_t r0 = (int64_t)nj * kp.nxg, r1 = r0 + kp.nxg;
+        atomicAdd(&a.rho[r0 + ni], (unsigned long long)q00);
+        atomicAdd(&a.rho[r0 + i1], (unsigned long long)q10);
+        atomicAdd(&a.rho[r1 + ni], (unsigned long long)q01);
+        atomicAdd(&a.rho[r1 + i1], (unsigned long long)q11);
+    }
+    // ---- collisions in the epilogue (same variates as the separate passes)
+    if (a.do_mcc) {
+        double dvx = vx, dvy = vy, dvz = vz;
+        edp_mcc_out o = edp_mcc_electron(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, dvx, dvy, dvz);
+        if (o.kind_index) {
+            vx = (float)dvx;
+            vy = (float)dvy;
+            vz = (float)dvz;
+            atomicAdd(&s.cnt[8 + o.kind_index - 1], 1ull);
+            if (o.born) {
+                double X = (double)ni + dx, Y = (double)nj + dy;
+                record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+                record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y,
+                            o.ni);
+            }
+        }
+    }
+    if (a.do_rcx) {
+        double dvx = vx, dvy = vy, dvz = vz;
+        if (edp_rcx_ion(a.rcx, id, a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, dvx, dvy, dvz)) {
+            vx = (float)dvx;
+            vy = (float)dvy;
+            vz = (float)dvz;
+            atomicAdd(&s.cnt[16], 1ull);
+        }
+    }
+    return true;
+}
+
+// four consecutive slots [4g, 4g+4) restricted to [lo, hi)
+__device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, int64_t g,
+                                           int64_t lo, int64_t hi)
+{
+    const int64_t base = g * EDP_ITEMS;
+    const bool full = base >= lo && base + EDP_ITEMS <= hi;
+    int c[4];
+    float ox[4], oy[4], vx[4], vy[4], vz[4];
+    uint32_t id[4];
+    if (full) {
+        int4 c4 = __ldcs(reinterpret_cast<const int4*>(a.P.cell) + g);
+        float4 ox4 = __ldcs(reinterpret_cast<const float4*>(a.P.ox) + g);
+        float4 oy4 = __ldcs(reinterpret_cast<const float4*>(a.P.oy) + g);
+        float4 vx4 = __ldcs(reinterpret_cast<const float4*>(a.P.vx) + g);
+        float4 vy4 = __ldcs(reinterpret_cast<const float4*>(a.P.vy) + g);
+        float4 vz4 = __ldcs(reinterpret_cast<const float4*>(a.P.vz) + g);
+        c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
+        ox[0] = ox4.x; ox[1] = ox4.y; ox[2] = ox4.z; ox[3] = ox4.w;
+        oy[0] = oy4.x; oy[1] = oy4.y; oy[2] = oy4.z; oy[3] = oy4.w;
+        vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
+        vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
+        vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
+        if (a.do_mcc || a.do_rcx) {
+            uint4 id4 = __ldcs(reinterpret_cast<const uint4*>(a.P.id) + g);
+            id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
+        } else {
+            id[0] = id[1] = id[2] = id[3] = 0u;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < EDP_ITEMS; ++e) {
+            int64_t k = base + e;
+            bool ok = k >= lo && k < hi;
+            c[e] = ok ? a.P.cell[k] : -1;
+            ox[e] = ok ? a.P.ox[k] : 0.f;
+            oy[e] = ok ? a.P.oy[k] : 0.f;
+            vx[e] = ok ? a.P.vx[k] : 0.f;
+            vy[e] = ok ? a.P.vy[k] : 0.f;
+            vz[e] = ok ? a.P.vz[k] : 0.f;
+            id[e] = ok ? a.P.id[k] : 0u;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < EDP_ITEMS; ++e) {
+        if (c[e] < 0) continue;
+        if (!push_one(a, s, windowed, wx0, wy0, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e])) {
+            c[e] = -1;
+            atomicAdd(&s.cnt[17], 1ull);
+        }
+    }
+    if (full) {
+        __stcs(reinterpret_cast<int4*>(a.P.cell) + g, make_int4(c[0], c[1], c[2], c[3]));
+        __stcs(reinterpret_cast<float4*>(a.P.ox) + g, make_float4(ox[0], ox[1], ox[2], ox[3]));
+        __stcs(reinterpret_cast<float4*>(a.P.oy) + g, make_float4(oy[0], oy[1], oy[2], oy[3]));
+        __stcs(reinterpret_cast<float4*>(a.P.vx) + g, make_float4(vx[0], vx[1], vx[2], vx[3]));
+        __stcs(reinterpret_cast<float4*>(a.P.vy) + g, make_float4(vy[0], vy[1], vy[2], vy[3]));
+        __stcs(reinterpret_cast<float4*>(a.P.vz) + g, make_float4(vz[0], vz[1], vz[2], vz[3]));
+    } else {
+#pragma unroll
+        for (int e = 0; e < EDP_ITEMS; ++e) {
+            int64_t k = base + e;
+            if (k < lo || k >= hi) continue;
+            a.P.cell[k] = c[e];
+            if (c[e] < 0) continue;
+            a.P.ox[k] = ox[e];
+            a.P.oy[k] = oy[e];
+            a.P.vx[k] = vx[e];
+            a.P.vy[k] = vy[e];
+            a.P.vz[k] = vz[e];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(EDP_PUSH_THREADS) push_mixed_kernel(PushArgs a)
+{
+    __shared__ Smem s;
+    const edp_kparams& kp = a.kp;
+    if (threadIdx.x < 32) s.cnt[threadIdx.x] = 0ull;
+    const bool windowed = blockIdx.x < a.n_chunks;
+    int64_t lo, hi;
+    int wx0 = 0, wy0 = 0;
+    if (windowed) {
+        edp_chunk ch = a.chunks[blockIdx.x];
+        lo = ch.start;
+        hi = ch.end;
+        wx0 = ch.wx0;
+        wy0 = ch.wy0;
+        for (int t = threadIdx.x; t < EDP_WIN_NODES * EDP_WIN_NODES; t += blockDim.x) {
+            int lx = t % EDP_WIN_NODES, ly = t / EDP_WIN_NODES;
+            int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
+            bool ok = gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg;
+            s.E[t] = ok ? __ldg(&a.E[(int64_t)gy * kp.nxg + gx]) : make_float2(0.f, 0.f);
+            s.R[t] = 0ull;
+        }
+    } else {
+        lo = a.tail_start;
+        hi = (int64_t)*a.n_slots;
+    }
+    __syncthreads();
+    if (windowed) {
+        for (int64_t g = lo / EDP_ITEMS + threadIdx.x; g * EDP_ITEMS < hi; g += blockDim.x)
+            push_group(a, s, true, wx0, wy0, g, lo, hi);
+    } else {
+        int64_t t = blockIdx.x - a.n_chunks;
+        int64_t g0 = lo / EDP_ITEMS;
+        for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * EDP_ITEMS < hi; g += a.tail_ctas * blockDim.x)
+            push_group(a, s, false, 0, 0, g, lo, hi);
+    }
+    __syncthreads();
+    if (windowed) {
+        for (int t = threadIdx.x; t < EDP_WIN_NODES * EDP_WIN_NODES; t += blockDim.x) {
+            unsigned long long v = s.R[t];
+            if (v == 0ull) continue;
+            int lx = t % EDP_WIN_NODES, ly = t / EDP_WIN_NODES;
+            int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
+            if (gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg) atomicAdd(&a.rho[(int64_t)gy * kp.nxg + gx], v);
+            else atomicOr(&a.dc->error_flags, EDP_EFLAG_BOUNDS);
+        }
+    }
+    if (threadIdx.x < 32) {
+        unsigned long long v = s.cnt[threadIdx.x];
+        if (v) {
+            int k = threadIdx.x;
+            if (k < 8) atomicAdd(a.is_ion ? &a.dc->i_hits[k] : &a.dc->e_hits[k], v);
+            else if (k < 16) {
+                atomicAdd(&a.dc->en_coll[k - 8], v);
+                atomicAdd(&a.dc->en_coll_step[k - 8], v);
+            } else if (k == 16) {
+                atomicAdd(&a.dc->rcx[a.species - 1], v);
+                atomicAdd(&a.dc->rcx_step[a.species - 1], v);
+            } else if (k == 17) {
+                atomicAdd(&a.dc->n_live[a.species], (unsigned long long)(-(long long)v));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------- FP64 path
+struct PushArgs64 {
+    edp_kparams kp;
+    edp_species_fp64 P;
+    const unsigned long long* n_slots;
+    const double *Ex, *Ey;
+    double* rho;
+    double K[9];
+    double qh, ez_term;
+    int xmul, use_rot, is_ion, species, do_mcc, do_rcx;
+    uint32_t step;
+    edp_mcc_dev mcc;
+    edp_rcx_dev rcx;
+    edp_dev_counters* dc;
+    edp_born pend_next;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+};
+
+// The plain FP64 cycle: one particle per thread, the reference's arithmetic in FP64, global atomics.
+__global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
+{
+    __shared__ unsigned long long cnt[32];
+    const edp_kparams& kp = a.kp;
+    if (threadIdx.x < 32) cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int64_t n = (int64_t)*a.n_slots;
+    const double xmax = kp.periodic ? (double)kp.ncx : (double)kp.ncx, ymax = (double)kp.ncy;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double X = a.P.x[k];
+        if (X < -1.0e29) continue;
+        double Y = a.P.y[k];
+        int i = (int)X, j = (int)Y;
+        if (!kp.periodic && X == xmax) i = kp.ncx - 1;
+        if (Y == ymax) j = kp.ncy - 1;
+        int i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+        double axp = X - (double)i, axm = 1.0 - axp, ayp = Y - (double)j, aym = 1.0 - ayp;
+        double EX = a.Ex[r0 + i] * axm * aym + a.Ex[r0 + i1] * axp * aym + a.Ex[r1 + i] * axm * ayp +
+                    a.Ex[r1 + i1] * axp * ayp;
+        double EY = a.Ey[r0 + i] * axm * aym + a.Ey[r0 + i1] * axp * aym + a.Ey[r1 + i] * axm * ayp +
+                    a.Ey[r1 + i1] * axp * ayp;
+        double vx = a.P.vx[k], vy = a.P.vy[k], vz = a.P.vz[k];
+        double q = a.qh;
+        if (a.use_rot) {
+            double mx = vx + q * EX, my = vy + q * EY, mz = vz + a.ez_term;
+            double px = a.K[0] * mx + a.K[1] * my + a.K[2] * mz;
+            double py = a.K[3] * mx + a.K[4] * my + a.K[5] * mz;
+            double pz = a.K[6] * mx + a.K[7] * my + a.K[8] * mz;
+            vx = px + q * EX;
+            vy = py + q * EY;
+            vz = pz + a.ez_term;
+        } else if (a.is_ion) {
+            vx = vx + (q + q) * EX;
+            vy = vy + (q + q) * EY;
+            vz = vz + (a.ez_term + a.ez_term);
+        } else {
+            vx = (vx + q * EX) + q * EX;
+            vy = (vy + q * EY) + q * EY;
+            vz = (vz + a.ez_term) + a.ez_term;
+        }
+        X = X + vx * a.xmul;
+        Y = Y + vy * a.xmul;
+        int obj = -1;
+        for (int n2 = 0; n2 < kp.n_inner; ++n2) {
+            if (X <= (double)kp.ileft[n2] || X >= (double)kp.iright[n2]) continue;
+            if (Y <= (double)kp.jbottom[n2] || Y >= (double)kp.jtop[n2]) continue;
+            obj = 4 + n2;
+            break;
+        }
+        if (obj < 0) {
+            if (kp.periodic) {
+                if (X < 0.0) X += (double)kp.ncx;
+                else if (X >= (double)kp.ncx) X -= (double)kp.ncx;
+                if (Y < 0.0) obj = 0;
+                else if (Y > ymax) obj = 1;
+            } else if (X < 0.0 || X > xmax || Y < 0.0 || Y > ymax) {
+                obj = wall_object(X, Y, xmax, ymax);
+            }
+        }
+        if (obj >= 0) {
+            a.P.x[k] = -1.0e30;
+            atomicAdd(&cnt[obj], 1ull);
+            atomicAdd(&cnt[17], 1ull);
+            continue;
+        }
+        // deposit
+        i = (int)X;
+        j = (int)Y;
+        if (!kp.periodic && X == xmax) i = kp.ncx - 1;
+        if (Y == ymax) j = kp.ncy - 1;
+        i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        r0 = (int64_t)j * kp.nxg;
+        r1 = r0 + kp.nxg;
+        double dx = X - (double)i, dy = Y - (double)j;
+        double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
+        atomicAdd(&a.rho[r0 + i], vij);
+        atomicAdd(&a.rho[r0 + i1], vip1j);
+        atomicAdd(&a.rho[r1 + i], vijp1);
+        atomicAdd(&a.rho[r1 + i1], 1.0 - vij - vip1j - vijp1);
+        if (a.do_mcc) {
+            edp_mcc_out o = edp_mcc_electron(a.mcc, a.P.id[k], a.step, kp.seed_lo, kp.seed_hi, vx, vy, vz);
+            if (o.kind_index) {
+                atomicAdd(&cnt[8 + o.kind_index - 1], 1ull);
+                if (o.born) {
+                    record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+                    record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags,
+                                X, Y, o.ni);
+                }
+            }
+        }
+        if (a.do_rcx) {
+            if (edp_rcx_ion(a.rcx, a.P.id[k], a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, vx, vy, vz))
+                atomicAdd(&cnt[16], 1ull);
+        }
+        a.P.x[k] = X;
+        a.P.y[k] = Y;
+        a.P.vx[k] = vx;
+        a.P.vy[k] = vy;
+        a.P.vz[k] = vz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned long long v = cnt[threadIdx.x];
+        if (v) {
+            int k = threadIdx.x;
+            if (k < 8) atomicAdd(a.is_ion ? &a.dc->i_hits[k] : &a.dc->e_hits[k], v);
+            else if (k < 16) {
+                atomicAdd(&a.dc->en_coll[k - 8], v);
+                atomicAdd(&a.dc->en_coll_step[k - 8], v);
+            } else if (k == 16) {
+                atomicAdd(&a.dc->rcx[a.species - 1], v);
+                atomicAdd(&a.dc->rcx_step[a.species - 1], v);
+            } else if (k == 17) {
+                atomicAdd(&a.dc->n_live[a.species], (unsigned long long)(-(long long)v));
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------------------- separate collision passes
+struct CollArgs {
+    edp_kparams kp;
+    int precision, species;
+    edp_species_mixed Pm;
+    edp_species_fp64 Pd;
+    const unsigned long long* n_slots;
+    uint32_t step;
+    edp_mcc_dev mcc;
+    edp_rcx_dev rcx;
+    edp_dev_counters* dc;
+    edp_born pend_next;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+};
+
+// PERFORM_ELECTRON_NEUTRAL_COLLISIONS as its own pass over the electron array
+__global__ void collide_en_kernel(CollArgs a)
+{
+    __shared__ unsigned long long cnt[EDP_MAX_COLPROC];
+    if (threadIdx.x < EDP_MAX_COLPROC) cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int64_t n = (int64_t)*a.n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double vx, vy, vz, X, Y;
+        uint32_t id;
+        if (a.precision == EDP_PREC_MIXED) {
+            int c = a.Pm.cell[k];
+            if (c < 0) continue;
+            vx = a.Pm.vx[k];
+            vy = a.Pm.vy[k];
+            vz = a.Pm.vz[k];
+            X = (double)(c & 0xFFFF) + (double)a.Pm.ox[k];
+            Y = (double)(c >> 16) + (double)a.Pm.oy[k];
+            id = a.Pm.id[k];
+        } else {
+            X = a.Pd.x[k];
+            if (X < -1.0e29) continue;
+            Y = a.Pd.y[k];
+            vx = a.Pd.vx[k];
+            vy = a.Pd.vy[k];
+            vz = a.Pd.vz[k];
+            id = a.Pd.id[k];
+        }
+        edp_mcc_out o = edp_mcc_electron(a.mcc, id, a.step, a.kp.seed_lo, a.kp.seed_hi, vx, vy, vz);
+        if (!o.kind_index) continue;
+        atomicAdd(&cnt[o.kind_index - 1], 1ull);
+        if (a.precision == EDP_PREC_MIXED) {
+            a.Pm.vx[k] = (float)vx;
+            a.Pm.vy[k] = (float)vy;
+            a.Pm.vz[k] = (float)vz;
+        } else {
+            a.Pd.vx[k] = vx;
+            a.Pd.vy[k] = vy;
+            a.Pd.vz[k] = vz;
+        }
+        if (o.born) {
+            record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+            record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y, o.ni);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < EDP_MAX_COLPROC && cnt[threadIdx.x]) {
+        atomicAdd(&a.dc->en_coll[threadIdx.x], cnt[threadIdx.x]);
+        atomicAdd(&a.dc->en_coll_step[threadIdx.x], cnt[threadIdx.x]);
+    }
+}
+
+// PERFORM_RESONANT_CHARGE_EXCHANGE as its own pass over one ion species
+__global__ void collide_rcx_kernel(CollArgs a)
+{
+    __shared__ unsigned long long cnt;
+    if (threadIdx.x == 0) cnt = 0ull;
+    __syncthreads();
+    const int64_t n = (int64_t)*a.n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double vx, vy, vz;
+        uint32_t id;
+        if (a.precision == EDP_PREC_MIXED) {
+            if (a.Pm.cell[k] < 0) continue;
+            vx = a.Pm.vx[k];
+            vy = a.Pm.vy[k];
+            vz = a.Pm.vz[k];
+            id = a.Pm.id[k];
+        } else {
+            if (a.Pd.x[k] < -1.0e29) continue;
+            vx = a.Pd.vx[k];
+            vy = a.Pd.vy[k];
+            vz = a.Pd.vz[k];
+            id = a.Pd.id[k];
+        }
+        if (!edp_rcx_ion(a.rcx, id, a.step, (uint32_t)(a.species - 1), a.kp.seed_lo, a.kp.seed_hi, vx, vy, vz)) continue;
+        atomicAdd(&cnt, 1ull);
+        if (a.precision == EDP_PREC_MIXED) {
+            a.Pm.vx[k] = (float)vx;
+            a.Pm.vy[k] = (float)vy;
+            a.Pm.vz[k] = (float)vz;
+        } else {
+            a.Pd.vx[k] = vx;
+            a.Pd.vy[k] = vy;
+            a.Pd.vz[k] = vz;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && cnt) {
+        atomicAdd(&a.dc->rcx[a.species - 1], cnt);
+        atomicAdd(&a.dc->rcx_step[a.species - 1], cnt);
+    }
+}
+
+// ------------------------------------------------------------------------------------- appending
+struct AppendArgs {
+    edp_kparams kp;
+    int precision, species, do_mcc;
+    edp_species_mixed Pm;
+    edp_species_fp64 Pd;
+    int64_t cap;
+    edp_born src;
+    const unsigned long long* src_count;
+    unsigned long long* n_slots;
+    unsigned long long* n_live;
+    unsigned long long* next_id;
+    unsigned long long* rho_fix;
+    double* rho_d;
+    uint32_t step;
+    edp_mcc_dev mcc;
+    edp_dev_counters* dc;
+    edp_born pend_next;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+};
+
+// PROCESS_ADDED_ELECTRONS / PROCESS_ADDED_IONS (pic2d_ElectronDynamics.f90:1429-1531, pic2d_IonDynamics.f90:1468-1537):
+// the add list joins the main array and is deposited; added electrons take part in this step's MCC.
+__global__ void append_kernel(AppendArgs a)
+{
+    __shared__ unsigned long long cnt[EDP_MAX_COLPROC];
+    if (threadIdx.x < EDP_MAX_COLPROC) cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+    const edp_kparams& kp = a.kp;
+    const int64_t n = (int64_t)*a.src_count;
+    const int64_t nread = n < a.src.cap ? n : a.src.cap;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nread; k += (int64_t)gridDim.x * blockDim.x) {
+        double X = a.src.x[k], Y = a.src.y[k];
+        double vx = a.src.vx[k], vy = a.src.vy[k], vz = a.src.vz[k];
+        uint32_t id = (uint32_t)atomicAdd(a.next_id, 1ull);
+        if (a.do_mcc) {
+            edp_mcc_out o = edp_mcc_electron(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, vx, vy, vz);
+            if (o.kind_index) {
+                atomicAdd(&cnt[o.kind_index - 1], 1ull);
+                if (o.born) {
+                    record_born(a.pend_next, &a.dc->pend_e_count[1], &a.dc->error_flags, X, Y, o.ne);
+                    record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags,
+                                X, Y, o.ni);
+                }
+            }
+        }
+        unsigned long long slot = atomicAdd(a.n_slots, 1ull);
+        if ((int64_t)slot >= a.cap) {
+            atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
+            continue;
+        }
+        atomicAdd(a.n_live, 1ull);
+        int i = (int)X, j = (int)Y;
+        if (!kp.periodic && i == kp.ncx) i = kp.ncx - 1;
+        if (j == kp.ncy) j = kp.ncy - 1;
+        if (kp.periodic && i >= kp.ncx) i -= kp.ncx;
+        double dx = X - (double)((int)X), dy = Y - (double)j;
+        if (!kp.periodic && (int)X == kp.ncx) dx = 1.0;
+        int i1 = i + 1;
+        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+        if (a.precision == EDP_PREC_MIXED) {
+            float fx = (float)dx, fy = (float)dy;
+            a.Pm.cell[slot] = (j << 16) | i;
+            a.Pm.ox[slot] = fx;
+            a.Pm.oy[slot] = fy;
+            a.Pm.vx[slot] = (float)vx;
+            a.Pm.vy[slot] = (float)vy;
+            a.Pm.vz[slot] = (float)vz;
+            a.Pm.id[slot] = id;
+            a.Pm.tag[slot] = 0;
+            double ddx = fx, ddy = fy;
+            double vij = (1.0 - ddx) * (1.0 - ddy), vip1j = ddx * (1.0 - ddy), vijp1 = (1.0 - ddx) * ddy;
+            long long q00 = __double2ll_rn(vij * EDP_FIX_ONE), q10 = __double2ll_rn(vip1j * EDP_FIX_ONE);
+            long long q01 = __double2ll_rn(vijp1 * EDP_FIX_ONE), q11 = 4294967296LL - q00 - q10 - q01;
+            atomicAdd(&a.rho_fix[r0 + i], (unsigned long long)q00);
+            atomicAdd(&a.rho_fix[r0 + i1], (unsigned long long)q10);
+            atomicAdd(&a.rho_fix[r1 + i], (unsigned long long)q01);
+            atomicAdd(&a.rho_fix[r1 + i1], (unsigned long long)q11);
+        } else {
+            a.Pd.x[slot] = (double)i + dx;
+            a.Pd.y[slot] = Y;
+            a.Pd.vx[slot] = vx;
+            a.Pd.vy[slot] = vy;
+            a.Pd.vz[slot] = vz;
+            a.Pd.id[slot] = id;
+            a.Pd.tag[slot] = 0;
+            double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
+            atomicAdd(&a.rho_d[r0 + i], vij);
+            atomicAdd(&a.rho_d[r0 + i1], vip1j);
+            atomicAdd(&a.rho_d[r1 + i], vijp1);
+            atomicAdd(&a.rho_d[r1 + i1], 1.0 - vij - vip1j - vijp1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < EDP_MAX_COLPROC && cnt[threadIdx.x]) {
+        atomicAdd(&a.dc->en_coll[threadIdx.x], cnt[threadIdx.x]);
+        atomicAdd(&a.dc->en_coll_step[threadIdx.x], cnt[threadIdx.x]);
+    }
+}
+
+void fill_rot(const edp_ctx* c, int species, float* Kf, double* Kd)
+{
+    for (int q = 0; q < 9; ++q) {
+        if (Kf) Kf[q] = (float)c->K[species][q];
+        if (Kd) Kd[q] = c->K[species][q];
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------- launch
+int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
+{
+    const edp_params& p = c->p;
+    const bool is_ion = sp > 0;
+    const int s = sp - 1;
+    const double qh = is_ion ? 0.5 * p.ion_charge[s] / p.ion_mass_me[s] : -0.5;
+    double ez_term;
+    int use_rot;
+    if (!is_ion) {
+        ez_term = -0.5 * p.ez;
+        use_rot = (p.bx != 0.0 || p.by != 0.0 || p.bz != 0.0);
+    } else {
+        ez_term = p.ions_sense_ez ? qh * p.ez * p.n_subcycles : 0.0;
+        use_rot = p.ions_sense_b && (p.bx != 0.0 || p.by != 0.0 || p.bz != 0.0);
+    }
+    const bool do_mcc = fuse && !is_ion && ion_step && c->tab.en_on;
+    const bool do_rcx = fuse && is_ion && ion_step && c->tab.rcx_on[s];
+    const int pn = c->pend_cur ^ 1;
+    if (p.precision == EDP_PREC_MIXED) {
+        PushArgs a;
+        memset(&a, 0, sizeof(a));
+        a.kp = c->kp;
+        a.P = c->pm[sp];
+        a.chunks = c->chunks[sp];
+        a.n_chunks = c->n_chunks[sp];
+        a.tail_start = c->sorted_end[sp];
+        a.n_slots = &c->dc->n_slots[sp];
+        a.E = is_ion ? c->acc2 : c->E2;
+        a.rho = c->rho_fix[sp];
+        fill_rot(c, sp, a.K, nullptr);
+        a.qh = (float)qh;
+        a.ez_term = (float)ez_term;
+        a.xmul = is_ion ? (float)p.n_subcycles : 1.0f;
+        a.use_rot = use_rot;
+        a.is_ion = is_ion;
+        a.species = sp;
+        a.do_mcc = do_mcc;
+        a.do_rcx = do_rcx;
+        a.step = (uint32_t)c->t_cntr;
+        if (do_mcc) a.mcc = edp_make_mcc_dev(c);
+        if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
+        a.dc = c->dc;
+        a.pend_next = c->pend_e[pn];
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+        int64_t tail = c->host_slots[sp] - c->sorted_end[sp];
+        if (tail < 0) tail = 0;
+        int64_t per_cta = (int64_t)EDP_PUSH_THREADS * EDP_ITEMS * 8;
+        a.tail_ctas = (tail + per_cta - 1) / per_cta;
+        if (a.tail_ctas < 1) a.tail_ctas = 1;
+        int64_t grid = a.n_chunks + a.tail_ctas;
+        push_mixed_kernel<<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
+    } else {
+        PushArgs64 a;
+        memset(&a, 0, sizeof(a));
+        a.kp = c->kp;
+        a.P = c->pd[sp];
+        a.n_slots = &c->dc->n_slots[sp];
+        a.Ex = is_ion ? c->accx : c->Ex;
+        a.Ey = is_ion ? c->accy : c->Ey;
+        a.rho = c->rho_d[sp];
+        fill_rot(c, sp, nullptr, a.K);
+        a.qh = qh;
+        a.ez_term = ez_term;
+        a.xmul = is_ion ? p.n_subcycles : 1;
+        a.use_rot = use_rot;
+        a.is_ion = is_ion;
+        a.species = sp;
+        a.do_mcc = do_mcc;
+        a.do_rcx = do_rcx;
+        a.step = (uint32_t)c->t_cntr;
+        if (do_mcc) a.mcc = edp_make_mcc_dev(c);
+        if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
+        a.dc = c->dc;
+        a.pend_next = c->pend_e[pn];
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+        int64_t n = c->host_slots[sp];
+        int64_t grid = (n + 255) / 256;
+        if (grid > 148 * 64) grid = 148 * 64;
+        if (grid < 1) grid = 1;
+        push_fp64_kernel<<<(unsigned)grid, 256, 0, c->stream>>>(a);
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+static CollArgs coll_args(edp_ctx* c, int sp)
+{
+    CollArgs a;
+    memset(&a, 0, sizeof(a));
+    a.kp = c->kp;
+    a.precision = c->p.precision;
+    a.species = sp;
+    a.Pm = c->pm[sp];
+    a.Pd = c->pd[sp];
+    a.n_slots = &c->dc->n_slots[sp];
+    a.step = (uint32_t)c->t_cntr;
+    a.dc = c->dc;
+    a.pend_next = c->pend_e[c->pend_cur ^ 1];
+    for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+    return a;
+}
+
+static unsigned grid_for(int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    if (g < 1) g = 1;
+    return (unsigned)g;
+}
+
+int edp_launch_collide_en(edp_ctx* c)
+{
+    if (!c->tab.en_on) return EDP_OK;
+    CollArgs a = coll_args(c, 0);
+    a.mcc = edp_make_mcc_dev(c);
+    collide_en_kernel<<<grid_for(c->host_slots[0]), 256, 0, c->stream>>>(a);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+int edp_launch_collide_rcx(edp_ctx* c)
+{
+    for (int s = 0; s < c->p.n_ion_species; ++s) {
+        if (!c->tab.rcx_on[s]) continue;
+        CollArgs a = coll_args(c, 1 + s);
+        a.rcx = edp_make_rcx_dev(c, s);
+        collide_rcx_kernel<<<grid_for(c->host_slots[1 + s]), 256, 0, c->stream>>>(a);
+        EDP_CUDA(c, cudaGetLastError());
+    }
+    return EDP_OK;
+}
+
+static AppendArgs append_args(edp_ctx* c, int sp)
+{
+    AppendArgs a;
+    memset(&a, 0, sizeof(a));
+    a.kp = c->kp;
+    a.precision = c->p.precision;
+    a.species = sp;
+    a.Pm = c->pm[sp];
+    a.Pd = c->pd[sp];
+    a.cap = c->cap[sp];
+    a.n_slots = &c->dc->n_slots[sp];
+    a.n_live = &c->dc->n_live[sp];
+    a.next_id = &c->dc->next_id[sp];
+    a.rho_fix = c->rho_fix[sp];
+    a.rho_d = c->rho_d[sp];
+    a.step = (uint32_t)c->t_cntr;
+    a.dc = c->dc;
+    for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+    return a;
+}
+
+// electrons born last step join the array after this step's push (PROCESS_ADDED_ELECTRONS, MainProgram:259/:316)
+int edp_launch_append_pending(edp_ctx* c, bool ion_step)
+{
+    const int cur = c->pend_cur;
+    AppendArgs a = append_args(c, 0);
+    a.src = c->pend_e[cur];
+    a.src_count = &c->dc->pend_e_count[1];   // the list filled during the previous step
+    a.do_mcc = ion_step && c->tab.en_on;
+    if (a.do_mcc) a.mcc = edp_make_mcc_dev(c);
+    // electrons born from these go to the list being filled this step, counted in pend_e_count[0]
+    a.pend_next = c->pend_e[cur ^ 1];
+    append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
+    EDP_CUDA(c, cudaGetLastError());
+    c->host_slots[0] += c->born_cap;
+    return EDP_OK;
+}
+
+int edp_launch_append_born_ions(edp_ctx* c)
+{
+    for (int s = 0; s < c->p.n_ion_species; ++s) {
+        AppendArgs a = append_args(c, 1 + s);
+        a.src = c->born_i[s];
+        a.src_count = &c->dc->born_i_count[s];
+        append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
+        EDP_CUDA(c, cudaGetLastError());
+        c->host_slots[1 + s] += c->born_cap;
+    }
+    return EDP_OK;
+}

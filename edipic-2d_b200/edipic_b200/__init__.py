@@ -1,0 +1,252 @@
+"""Host-side mirror of EDIPIC-2D's per-step particle-cycle interface on one B200.
+
+The reference drives its hot path through argument-less Fortran subroutines called in a fixed order from
+MainProg (src/pic2d_MainProgram.f90:151-309). `Simulation` exposes the same steps under the same names, each
+a thin call into the C ABI of libedipic_b200.so (include/edipic_gpu.h); there is no CPU implementation behind
+them, and a missing library or GPU raises instead of falling back.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS,
+                   PREC_FP64, PREC_MIXED, SOLVER_CG, SOLVER_FFTX, WARM_PREVIOUS, WARM_USER, WARM_ZERO, Counters,
+                   Params, Tables)
+
+__all__ = ["Simulation", "EdpError", "read_deck", "library", "Params", "Tables", "Counters", "ELECTRONS", "IONS",
+           "PREC_MIXED", "PREC_FP64", "SOLVER_FFTX", "SOLVER_CG", "FIELD_EX", "FIELD_EY", "FIELD_ACC_EX",
+           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER"]
+
+_lib = None
+
+
+def library():
+    """The loaded libedipic_b200.so (loaded once)."""
+    global _lib
+    if _lib is None:
+        _lib = _abi.load()
+    return _lib
+
+
+class EdpError(RuntimeError):
+    def __init__(self, code, where, message=""):
+        self.code = code
+        super().__init__(f"{where}: {_abi.ERROR_NAMES.get(code, code)} {message}".strip())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+class Deck:
+    """A parsed input-deck directory (init_*.dat files), as INITIATE_PARAMETERS and the collision set-up read it.
+    Keeps the C-side table arrays alive while params/tables are in use."""
+
+    def __init__(self, directory):
+        self.lib = library()
+        self.handle = C.c_void_p()
+        self.params = Params()
+        self.tables = Tables()
+        rc = self.lib.edp_deck_read(str(directory).encode(), C.byref(self.handle), C.byref(self.params),
+                                    C.byref(self.tables))
+        if rc != 0:
+            raise EdpError(rc, "edp_deck_read", str(directory))
+        te, ne, tev, npl = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        ti = (C.c_double * _abi.MAX_ION)()
+        nmv = C.c_int32()
+        maxt = C.c_int64()
+        self.lib.edp_deck_initial_plasma(self.handle, C.byref(te), C.byref(ne), ti, C.byref(tev), C.byref(nmv),
+                                         C.byref(npl), C.byref(maxt))
+        self.init_te_ev, self.init_ne_m3, self.t_e_ev = te.value, ne.value, tev.value
+        self.init_ti_ev = [ti[s] for s in range(_abi.MAX_ION)]
+        self.n_max_vel, self.n_plasma_m3, self.max_t_cntr = nmv.value, npl.value, maxt.value
+
+    def close(self):
+        if self.handle:
+            self.lib.edp_deck_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_deck(directory):
+    return Deck(directory)
+
+
+class Simulation:
+    """One device context. Method names follow the reference subroutines they replace."""
+
+    def __init__(self, deck, precision=PREC_MIXED, sort_every=None, fuse_collisions=True, capacity=None, seed=None):
+        self.lib = library()
+        self.deck = deck if isinstance(deck, Deck) else Deck(deck)
+        p = Params.from_buffer_copy(self.deck.params)
+        p.precision = precision
+        if sort_every is not None:
+            p.sort_every = sort_every
+        p.fuse_collisions = 1 if fuse_collisions else 0
+        if capacity is not None:
+            for s, v in enumerate(capacity):
+                p.capacity[s] = int(v)
+        if seed is not None:
+            p.seed = int(seed)
+        self.params = p
+        self.ctx = C.c_void_p()
+        rc = self.lib.edp_init(C.byref(p), C.byref(self.deck.tables), C.byref(self.ctx))
+        if rc != 0:
+            raise EdpError(rc, "edp_init")
+        self.periodic = bool(p.periodic_x)
+        self.nx_ref = p.ncx + 2 if self.periodic else p.ncx + 1
+        self.ny_ref = p.ncy + 1
+
+    # ------------------------------------------------------------------------------------ plumbing
+    def _check(self, rc, where):
+        if rc != 0:
+            buf = C.create_string_buffer(512)
+            self.lib.edp_last_error(self.ctx, buf, 512)
+            raise EdpError(rc, where, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if self.ctx:
+            self.lib.edp_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        self._check(self.lib.edp_synchronize(self.ctx), "edp_synchronize")
+
+    # ------------------------------------------------------------------------------------ particles
+    def distribute_particles(self, per_cell, init_te_ev=None, init_ti_ev=None):
+        """DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325) on the device: per_cell electrons and
+        ions per cell, ions at the electron positions, Maxwellian velocities of the deck's initial temperatures."""
+        d = self.deck
+        te = d.init_te_ev if init_te_ev is None else init_te_ev
+        fconv_e = np.sqrt(te / d.t_e_ev) / d.n_max_vel
+        self._check(self.lib.edp_distribute_particles(self.ctx, ELECTRONS, int(per_cell), fconv_e, 0, 0),
+                    "edp_distribute_particles")
+        for s in range(self.params.n_ion_species):
+            ti = d.init_ti_ev[s] if init_ti_ev is None else init_ti_ev
+            fconv_i = np.sqrt(ti / d.t_e_ev) / (d.n_max_vel * np.sqrt(self.params.ion_mass_me[s]))
+            self._check(self.lib.edp_distribute_particles(self.ctx, IONS + s, int(per_cell), fconv_i, 1, 1),
+                        "edp_distribute_particles")
+
+    def upload_particles(self, species, x, y, vx, vy, vz, tag=None, ids=None):
+        cols = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, vx, vy, vz)]
+        n = len(cols[0])
+        t = None if tag is None else np.ascontiguousarray(tag, dtype=np.int32)
+        i = None if ids is None else np.ascontiguousarray(ids, dtype=np.uint32)
+        self._check(self.lib.edp_upload_particles(
+            self.ctx, species, n, *[_dp(a) for a in cols],
+            t.ctypes.data_as(C.POINTER(C.c_int32)) if t is not None else None,
+            i.ctypes.data_as(C.POINTER(C.c_uint32)) if i is not None else None), "edp_upload_particles")
+
+    def download_particles(self, species, cap=None):
+        if cap is None:
+            cap = self.counters().n_particles[species] + 16
+        out = {k: np.zeros(cap) for k in ("x", "y", "vx", "vy", "vz")}
+        out["tag"] = np.zeros(cap, dtype=np.int32)
+        out["id"] = np.zeros(cap, dtype=np.uint32)
+        n = C.c_int64()
+        self._check(self.lib.edp_download_particles(
+            self.ctx, species, cap, C.byref(n), *[_dp(out[k]) for k in ("x", "y", "vx", "vy", "vz")],
+            out["tag"].ctypes.data_as(C.POINTER(C.c_int32)), out["id"].ctypes.data_as(C.POINTER(C.c_uint32))),
+            "edp_download_particles")
+        return {k: v[:n.value] for k, v in out.items()}
+
+    # ------------------------------------------------------------------------------------ per-step cycle
+    def _node_array(self):
+        return np.zeros((self.ny_ref, self.nx_ref))
+
+    def gather_electron_charge_density(self):
+        """GATHER_ELECTRON_CHARGE_DENSITY: c_rho on the reference node grid (after fold and wall factors)."""
+        out = self._node_array()
+        self._check(self.lib.edp_gather_charge_density(self.ctx, ELECTRONS, _dp(out)), "edp_gather_charge_density")
+        return out
+
+    def gather_ion_charge_density(self, species=0):
+        """GATHER_ION_CHARGE_DENSITY: Qs-weighted c_rho_i of one ion species."""
+        out = self._node_array()
+        self._check(self.lib.edp_gather_charge_density(self.ctx, IONS + species, _dp(out)),
+                    "edp_gather_charge_density")
+        return out
+
+    def update_wall_potentials(self, t_cntr):
+        self._check(self.lib.edp_update_wall_potentials(self.ctx, int(t_cntr)), "edp_update_wall_potentials")
+
+    def solve_poisson_fftx_linsysy(self, want_phi=False):
+        """SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY."""
+        out = self._node_array() if want_phi else None
+        self._check(self.lib.edp_field_fftx(self.ctx, _dp(out)), "edp_field_fftx")
+        return out
+
+    def solve_potential_with_cg(self, rtol=1e-8, max_it=20000, warm_start=WARM_PREVIOUS):
+        """SOLVE_POTENTIAL_WITH_PETSC + CALCULATE_ELECTRIC_FIELD, with the device CG; returns iterations."""
+        it = C.c_int32()
+        self._check(self.lib.edp_field_cg(self.ctx, rtol, max_it, warm_start, C.byref(it)), "edp_field_cg")
+        return it.value
+
+    def advance_electrons(self):
+        self._check(self.lib.edp_advance_electrons(self.ctx), "edp_advance_electrons")
+
+    def advance_ions(self):
+        self._check(self.lib.edp_advance_ions(self.ctx), "edp_advance_ions")
+
+    def perform_electron_neutral_collisions(self):
+        cnt = (C.c_int64 * _abi.MAX_COLPROC)()
+        self._check(self.lib.edp_collide_en(self.ctx, cnt), "edp_collide_en")
+        return np.array(cnt[:], dtype=np.int64)
+
+    def perform_resonant_charge_exchange(self):
+        n = C.c_int64()
+        self._check(self.lib.edp_collide_rcx(self.ctx, C.byref(n)), "edp_collide_rcx")
+        return n.value
+
+    def end_ion_cycle(self):
+        """PROCESS_ADDED_IONS + CLEAR_ACCUMULATED_FIELDS; advances T_cntr."""
+        self._check(self.lib.edp_end_ion_cycle(self.ctx), "edp_end_ion_cycle")
+
+    def step(self, n=1):
+        self._check(self.lib.edp_step(self.ctx, int(n)), "edp_step")
+
+    # ------------------------------------------------------------------------------------ diagnostics
+    def counters(self):
+        c = Counters()
+        self._check(self.lib.edp_query_counters(self.ctx, C.byref(c)), "edp_query_counters")
+        return c
+
+    def field(self, which):
+        out = self._node_array()
+        self._check(self.lib.edp_get_field(self.ctx, which, _dp(out)), "edp_get_field")
+        return out
+
+    def set_field(self, which, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.ny_ref, self.nx_ref)
+        self._check(self.lib.edp_set_field(self.ctx, which, _dp(a)), "edp_set_field")
+
+    def moments(self, species):
+        out = np.zeros(7)
+        self._check(self.lib.edp_moments(self.ctx, species, _dp(out)), "edp_moments")
+        return out
+
+    def mcc_choose(self, energy_ev, r):
+        e = np.ascontiguousarray(energy_ev, dtype=np.float64)
+        rr = np.ascontiguousarray(r, dtype=np.float64)
+        out = np.zeros(len(e), dtype=np.int32)
+        self._check(self.lib.edp_mcc_choose(self.ctx, len(e), _dp(e), _dp(rr), out.ctypes.data_as(C.POINTER(C.c_int32))),
+                    "edp_mcc_choose")
+        return out

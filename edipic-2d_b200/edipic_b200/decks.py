@@ -1,0 +1,200 @@
+"""Synthetic input decks for the benchmark configurations, written in the reference's fixed-column format.
+
+Each file follows the edit descriptors with which EDIPIC-2D reads it (init_configuration.dat:
+pic2d_CurProblemValues.f90:157-330; init_simcontrol.dat :830-845; init_particles.dat :1005-1031;
+init_extfields.dat pic2d_ExternalFields.f90:36-72; init_bo_NN.dat pic2d_Setup.f90:76-99; neutral decks
+pic2d_enCollisionsGeneralProc.f90:63-190; RCX pic2d_inCollisionsGeneralProc.f90:56-60), so the same directory
+can be read by the reference and by edp_deck_read. Cross sections are analytic synthetic shapes (not
+measured data) tabulated on 200 log-spaced energies.
+
+Normalisation: dx = 0.1 mm and dt = dx / (N_max_vel v_Te) are reached with N_of_cells_debye = 1 and a scale
+temperature/density chosen for them (T_scale = 1.9741945 eV, N_scale = 2.1820009e16 m^-3); the per-cell count of
+the scale density, N_of_particles_cell, is the integer nearest to N_scale * ppc / n_init.
+"""
+import math
+import os
+
+import numpy as np
+
+T_SCALE_EV = 1.9741945
+N_SCALE_M3 = 2.1820009e16
+E_EXC_EV = 11.55
+E_ION_EV = 15.76
+
+CONFIGS = {
+    # name: (ncx, ncy, periodic, ppc, n_init, dt_s, steps, B_gauss (Bx, By), inner object, top RF (V, MHz))
+    "cfg0": dict(ncx=128, ncy=128, periodic=True, ppc=64, n_init=1.0e16, dt=5e-12, steps=1000, bx=0.0, by=0.0),
+    "cfg1": dict(ncx=1024, ncy=1024, periodic=True, ppc=200, n_init=1.0e16, dt=5e-12, steps=200,
+                 bx=100.0 * math.cos(math.radians(30.0)), by=100.0 * math.sin(math.radians(30.0))),
+    "cfg2": dict(ncx=512, ncy=512, periodic=False, ppc=100, n_init=1.0e16, dt=5e-12, steps=2000, bx=0.0, by=0.0,
+                 inner=(224, 112, 288, 144, -100.0)),
+    "cfg4": dict(ncx=2048, ncy=512, periodic=True, ppc=100, n_init=5.0e15, dt=1e-11, steps=100000, bx=0.0, by=0.0,
+                 top_rf=(200.0, 13.56)),
+}
+
+
+def sigma_elastic(e):
+    return 1.0e-19 / (1.0 + e / 15.0) + 5.0e-21
+
+
+def sigma_lotz(e, eth, c):
+    x = np.maximum(e / eth, 1.0)
+    return c * np.log(x) / x
+
+
+def _blocks(n_total):
+    """Split n_total cells into (blocks, cells per block) with at most 999 cells per block (the i3 field)."""
+    for nb in range(1, n_total + 1):
+        if n_total % nb == 0 and n_total // nb <= 999:
+            return nb, n_total // nb
+    raise ValueError(n_total)
+
+
+def _segments():
+    # energy grid of the collision probability table: (upper boundary, resolution) [eV]
+    return 0.0, [(0.1, 0.01), (1.0, 0.02), (10.0, 0.05), (30.0, 0.05), (100.0, 0.5), (1000.0, 5.0)]
+
+
+def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
+               collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None):
+    cfg = dict(CONFIGS[name])
+    ncx = ncx or cfg["ncx"]
+    ncy = ncy or cfg["ncy"]
+    ppc = ppc or cfg["ppc"]
+    steps = steps or cfg["steps"]
+    bx = cfg["bx"] if bx is None else bx
+    by = cfg["by"] if by is None else by
+    inner = cfg.get("inner") if inner is None else (inner or None)
+    periodic = cfg["periodic"]
+    dt = cfg["dt"]
+    os.makedirs(directory, exist_ok=True)
+    dx = 1.0e-4
+    v_te = math.sqrt(2.0 * T_SCALE_EV * 1.602189e-19 / 9.109534e-31)
+    n_max_vel = int(round(dx / dt / v_te))
+    n_ppc = int(round(N_SCALE_M3 * ppc / cfg["n_init"]))
+    nx_total = ncx if periodic else ncx - 1
+    ny_total = ncy - 1
+    nbx, ngx = _blocks(nx_total)
+    nby, ngy = _blocks(ny_total)
+    gmi, gmj = nx_total + 1, ny_total + 1
+    w = lambda fn, lines: open(os.path.join(directory, fn), "w").write("\n".join(lines) + "\n")
+
+    objs = []   # (type, [segments])
+    if periodic:
+        objs = [(2, [(0, 0, 0, gmj)]), (1, [(0, gmj, gmi, gmj)]), (2, [(gmi, 0, gmi, gmj)]), (1, [(0, 0, gmi, 0)])]
+    else:
+        objs = [(1, [(0, 0, 0, gmj)]), (1, [(0, gmj, gmi, gmj)]), (1, [(gmi, 0, gmi, gmj)]), (1, [(0, 0, gmi, 0)])]
+    inner_list = [inner] if inner else []
+    cf = [
+        "---dddd.ddddddd----- scale electron temperature [eV]", f"   {T_SCALE_EV:12.7f}",
+        "---+d.dddddddE+dd--- scale electron density [m^-3]", f"   {N_SCALE_M3:14.7E}",
+        "---ddd---------- cells per scale Debye length", f"   {1:3d}",
+        "---ddd---------- maximal expected velocity [scale thermal velocities]", f"   {n_max_vel:3d}",
+        "---ddd---------- blocks along X", f"   {nbx:3d}",
+        "---ddd---------- blocks along Y", f"   {nby:3d}",
+        "---ddd---------- cells along X in a block", f"   {ngx:3d}",
+        "---ddd---------- cells along Y in a block", f"   {ngy:3d}",
+        "--dddd---------- macroparticles per cell for the scale density", f"  {n_ppc:4d}",
+        "-----d---------- blocks in a cluster along X", f"     {min(nbx, 9):1d}",
+        "-----d---------- blocks in a cluster along Y", f"     {min(nby, 9):1d}",
+        "---ddd---ddd---- boundary objects // inner objects", f"   {len(objs):3d}   {len(inner_list):3d}",
+    ]
+    for k, (ty, segs) in enumerate(objs):
+        cf += [f"===dd===dd=== object type, number of segments // #{k + 1}", f"   {ty:2d}   {len(segs):2d}",
+               "---dddddd---dddddd---dddddd---dddddd--- segment start X/Y end X/Y"]
+        cf += [f"   {a:6d}   {b:6d}   {c:6d}   {d:6d}" for (a, b, c, d) in segs]
+    for (il, jb, ir, jt, _phi) in inner_list:
+        cf += ["===dd=== object type", f"   {1:2d}",
+               "---dddddd---dddddd---dddddd---dddddd--- left bottom X/Y, right top X/Y",
+               f"   {il:6d}   {jb:6d}   {ir:6d}   {jt:6d}"]
+    w("init_configuration.dat", cf)
+
+    w("init_simcontrol.dat", [
+        "---ddddddd.ddd----- simulation time [ns]", f"   {steps * dt * 1e9:11.3f}",
+        "--------dd--------- electron sub-cycles per ion cycle (odd)", f"        {n_subcycles:2d}",
+        "------dddd--------- ion cycles between cluster load balancing", f"      {10:4d}",
+        "------dddd--------- cluster balancing events between global balancing", f"      {10:4d}",
+        "---ddddddd--------- ion cycles between checkpoints", f"   {0:7d}",
+        "---------d--------- use checkpoint", f"         {0:1d}",
+        "--dddddddd--------- time step of the checkpoint", f"  {0:8d}",
+    ])
+    w("init_particles.dat", [
+        "---dddd.ddd----- initial electron temperature [eV]", f"   {2.0:8.3f}",
+        "---+d.dddE+dd--- initial electron density [m^-3]", f"   {cfg['n_init']:10.3E}",
+        "------d--------- number of ion species", f"      {1:1d}",
+        "---ddd.d---+d---dddd.ddd---ddd.dd-- ion mass / charge / temperature / concentration",
+        f"   {40.0:5.1f}   {1:2d}   {0.03:8.3f}   {100.0:6.2f}",
+        "---ddddddddd---- seed", f"   {seed:9d}",
+    ])
+    w("init_extfields.dat", [
+        "---ddddd.ddd--- X-magnetic field [Gauss]", f"   {bx:9.3f}",
+        "---ddddd.ddd--- Y-magnetic field [Gauss]", f"   {by:9.3f}",
+        "--------------- Z-magnetic field profile",
+        "---ddddd.ddd--- y_Bmax [cm]", f"   {0.0:9.3f}",
+        "---ddddd.ddd--- BZ at y=0 [Gauss]", f"   {0.0:9.3f}",
+        "---ddddd.ddd--- BZ at y_Bmax [Gauss]", f"   {0.0:9.3f}",
+        "---ddddd.ddd--- BZ at y=Lsys [Gauss]", f"   {0.0:9.3f}",
+        "---ddddd.ddd--- decay length below y_Bmax [cm]", f"   {1.0:9.3f}",
+        "---ddddd.ddd--- decay length above y_Bmax [cm]", f"   {1.0:9.3f}",
+        "---ddddd.ddd--- Z-electric field [V/cm]", f"   {0.0:9.3f}",
+        "-------d------- ions sense magnetic field", f"       {0:1d}",
+        "-------d------- ions sense Z-electric field", f"       {0:1d}",
+    ])
+
+    def bo(n, phi, amp=0.0, mhz=0.0):
+        w(f"init_bo_{n:02d}.dat", [
+            "------AAAAAA--- material", "      METAL1",
+            "---ddddd.ddd--- constant potential [V]", f"   {phi:9.3f}",
+            "---ddddd.ddd--- amplitude of oscillations [V]", f"   {amp:9.3f}",
+            "---ddddd.ddd--- frequency [MHz]", f"   {mhz:9.3f}",
+            "---ddddd.ddd--- phase [deg]", f"   {0.0:9.3f}",
+            "---ddddd.ddd--- electrons injected per step", f"   {0.0:9.3f}",
+            "-------d------- emission model", f"       {0:1d}",
+            "----dddd.ddd--- emitted temperature normal [eV]", f"    {0.0:8.3f}",
+            "----dddd.ddd--- emitted temperature parallel [eV]", f"    {0.0:8.3f}",
+            "----dddd.ddd--- beam energy [eV]", f"    {0.0:8.3f}",
+            "-------d------- save collided ions", f"       {0:1d}",
+            "-------d------- save collided electrons", f"       {0:1d}",
+        ])
+    wp = wall_potentials or {}
+    for k, (ty, _s) in enumerate(objs):
+        if ty == 1:
+            amp, mhz = (0.0, 0.0)
+            if k == 1 and cfg.get("top_rf"):
+                amp, mhz = cfg["top_rf"]
+            bo(k + 1, wp.get(k + 1, 0.0), amp, mhz)
+    for q, (_a, _b, _c, _d, phi) in enumerate(inner_list):
+        bo(len(objs) + q + 1, phi)
+
+    if not collisions:
+        w("init_neutrals.dat", ["----------dd--- number of neutral species", f"          {0:2d}"])
+        return directory
+    t_gas_k = 0.03 * 1.602189e-19 / 1.38064852e-23
+    w("init_neutrals.dat", [
+        "----------dd--- number of neutral species", f"          {1:2d}",
+        "------AAAAAA--- neutral gas code", "      Argon0",
+        "--#d.dddE#dd--- density [m^-3]", f"  {3.2e21:10.3E}",
+        "-----ddddd.d--- temperature [K]", f"     {t_gas_k:7.1f}",
+    ])
+    e0, segs = _segments()
+    nl = ["---ddd.ddd--- mass [amu]", f"   {39.948:7.3f}", "--------dd--- number of collisional processes",
+          f"        {3:2d}"]
+    for k, ty in enumerate((10, 20, 30)):
+        nl += [f"---dd--d--dd--d- collision #{k + 1} :: type / activated / ion species / save",
+               f"   {ty:2d}  {1:1d}  {(1 if ty == 30 else 0):2d}  {0:1d}"]
+    nl += ["--------dd--- number of energy segments", f"        {len(segs):2d}",
+           "--ddddd.ddd------------- minimal energy [eV]", f"  {e0:9.3f}"]
+    for k, (up, st) in enumerate(segs):
+        nl += [f"--ddddd.ddd---ddd.ddd--- segment {k + 1} :: upper boundary / resolution [eV]", f"  {up:9.3f}   {st:7.3f}"]
+    w("init_neutral_Argon0.dat", nl)
+    tables = {
+        (1, 10): (np.logspace(-2, 3, 200), sigma_elastic),
+        (2, 20): (np.logspace(math.log10(E_EXC_EV), 3, 200), lambda e: sigma_lotz(e, E_EXC_EV, 5.0e-20)),
+        (3, 30): (np.logspace(math.log10(E_ION_EV), 3, 200), lambda e: sigma_lotz(e, E_ION_EV, 8.0e-20)),
+    }
+    for (pid, ty), (en, fn) in tables.items():
+        rows = [f"  {len(en):4d}"] + [f"    {e:9.3f}  {float(fn(e)):10.3E}" for e in en]
+        w(f"init_neutral_Argon0_crsect_coll_id_{pid:02d}_type_{ty:02d}.dat", rows)
+    if rcx:
+        w("init_neutral_Argon0_rcx_param.dat", ["ion species / sigma at 1 eV [m^2] / alpha", "1  5.0e-19  0.0"])
+    return directory

@@ -1,0 +1,222 @@
+/*
+ * edipic_gpu.h -- C ABI of the B200 particle cycle of EDIPIC-2D (sm_100a).
+ *
+ * The reference's hot path is a set of argument-less Fortran subroutines acting on module globals and
+ * called from MainProg in a fixed order (src/pic2d_MainProgram.f90:151-309). Each entry point below
+ * replaces one of them; the reference routine is cited beside it. A Fortran host binds these functions
+ * through ISO_C_BINDING (edipic-2d_b200/fortran/edipic_gpu_mod.f90); every argument is a plain pointer,
+ * integer or double.
+ *
+ * Conventions
+ *  - Every function returns EDP_OK (0) or a negative EDP_ERR_* code and never aborts the process.
+ *    edp_last_error() returns the message of the last failure on a context.
+ *  - Device work is ordered on the context's CUDA stream. Entry points that return host data synchronise;
+ *    the others return as soon as their work is queued unless edp_set_sync(ctx, 1) was called.
+ *  - Node arrays exchanged with the host use the reference's cluster layout, x fastest:
+ *      periodic-x domain : (ncx+2) x (ncy+1) nodes, columns ncx and ncx+1 repeat columns 0 and 1
+ *                          (the overlap cell of a self-connected periodic cluster);
+ *      walled domain     : (ncx+1) x (ncy+1) nodes.
+ *  - Positions are in cells, velocities in cells per time step, fields in E_scale, potentials in F_scale
+ *    (pic2d_CurProblemValues.f90:719-723, 893-900).
+ *  - One context per GPU and host thread; a context is not thread safe.
+ */
+#ifndef EDIPIC_GPU_H
+#define EDIPIC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDP_ABI_VERSION 1
+
+enum edp_status {
+    EDP_OK = 0,
+    EDP_ERR_ARG = -1,            /* invalid argument or configuration */
+    EDP_ERR_CUDA = -2,           /* CUDA runtime error (allocation, launch) */
+    EDP_ERR_CAPACITY = -3,       /* particle or add-list capacity exceeded on the device */
+    EDP_ERR_BOUNDS = -4,         /* a particle was found outside the domain (ADVANCE_* Error-1/-2 checks) */
+    EDP_ERR_NOT_CONVERGED = -5,  /* CG did not reach the tolerance within max_it */
+    EDP_ERR_TIMEOUT = -6,        /* a bounded device-side wait gave up */
+    EDP_ERR_STATE = -7,          /* call out of order (e.g. solve before upload) */
+    EDP_ERR_IO = -8              /* deck file missing or malformed */
+};
+
+enum edp_precision { EDP_PREC_MIXED = 0, EDP_PREC_FP64 = 1 };
+enum edp_solver { EDP_SOLVER_FFTX = 0, EDP_SOLVER_CG = 1 };
+enum edp_species { EDP_ELECTRONS = 0, EDP_IONS = 1 /* ion species s is EDP_IONS + s */ };
+enum edp_field {
+    EDP_FIELD_EX = 0, EDP_FIELD_EY = 1, EDP_FIELD_ACC_EX = 2, EDP_FIELD_ACC_EY = 3,
+    EDP_FIELD_PHI = 4, EDP_FIELD_RHO_TOTAL = 5
+};
+enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2 };
+
+#define EDP_MAX_ION_SPECIES 4
+#define EDP_MAX_INNER 4
+#define EDP_MAX_COLPROC 8
+#define EDP_MAX_SEGMENTS 32
+
+/* Boundary objects: sides 0 below, 1 above, 2 left, 3 right; inner metal rectangles 4.. . */
+#define EDP_N_HIT_COUNTERS (4 + EDP_MAX_INNER)
+
+/* Problem description. Values are those of the reference's module data after INITIATE_PARAMETERS
+ * (pic2d_CurProblemValues.f90:59-1255); the deck reader below fills it from init_*.dat files. */
+typedef struct edp_params {
+    int32_t abi_version;            /* EDP_ABI_VERSION */
+    int32_t ncx, ncy;               /* cells: period N along x (periodic) or global_maximal_i; global_maximal_j */
+    int32_t periodic_x;             /* 1: self-connected periodic cluster with metal walls below/above */
+    int32_t n_subcycles;            /* N_subcycles (odd) */
+    int32_t n_of_particles_cell;    /* N_of_particles_cell, density normalisation */
+    double delta_t_s, delta_x_m;
+    double v_scale_ms, e_scale_vm, b_scale_t, f_scale_v;
+    double bx, by, bz, ez;          /* uniform external fields, normalised (Bx_ext/B_scale ...) */
+    int32_t ions_sense_b, ions_sense_ez;
+    int32_t n_ion_species;
+    int32_t ion_charge[EDP_MAX_ION_SPECIES];        /* Qs */
+    double ion_mass_me[EDP_MAX_ION_SPECIES];        /* Ms = M_i / m_e */
+    /* metal boundary potentials (normalised), phi = phi_const + phi_var*sin(omega*T + phase)
+       (UPDATE_WALL_POTENTIALS, pic2d_WallPotentials.f90:1-93; omega in rad per step) */
+    double wall_phi_const[4], wall_phi_var[4], wall_omega[4], wall_phase[4];
+    int32_t n_inner;
+    int32_t inner_ileft[EDP_MAX_INNER], inner_jbottom[EDP_MAX_INNER];
+    int32_t inner_iright[EDP_MAX_INNER], inner_jtop[EDP_MAX_INNER];
+    double inner_phi[EDP_MAX_INNER];
+    uint64_t seed;                  /* Philox key for all device random streams */
+    int32_t precision;              /* edp_precision */
+    int32_t solver;                 /* edp_solver */
+    int32_t sort_every;             /* cell sort period in steps (mixed precision), 0 = never */
+    int32_t fuse_collisions;        /* 1: MCC/RCX run in the push epilogue (same variates as the separate pass) */
+    int64_t capacity[1 + EDP_MAX_ION_SPECIES];      /* particle slots per species (0 = automatic) */
+} edp_params;
+
+/* Collision and sampling tables, as built on the host by INITIATE_ELECTRON_NEUTRAL_COLLISIONS
+ * (pic2d_enCollisionsGeneralProc.f90:5-325), INITIATE_ION_NEUTRAL_COLLISIONS
+ * (pic2d_inCollisionsGeneralProc.f90:3-90) and PrepareMaxwellDistribIntegral
+ * (pic2d_ElectronWallCollisions.f90:835-929). One neutral species. */
+typedef struct edp_tables {
+    int32_t en_on;                       /* electron-neutral collisions active */
+    int32_t n_act;                       /* N_of_activated_colproc */
+    int32_t n_seg, n_values;             /* N_of_energy_segments, N_of_energy_values */
+    double seg_value[EDP_MAX_SEGMENTS + 1];
+    double seg_step[EDP_MAX_SEGMENTS];
+    int32_t seg_index[EDP_MAX_SEGMENTS + 1];
+    const double* energy_eV;             /* [n_values+1] */
+    const double* prob;                  /* prob_colproc_energy, [(n_values+1)*n_act], prob[i*n_act + p-1] */
+    double max_colliding_fraction;
+    int32_t colproc_type[EDP_MAX_COLPROC];          /* 10, 11, 20, 30 */
+    double threshold_eV[EDP_MAX_COLPROC];
+    int32_t ion_species_produced[EDP_MAX_COLPROC];  /* 1-based, ionisation only */
+    double ion_velocity_factor[EDP_MAX_COLPROC];
+    double neutral_mass_amu;
+    double energy_factor_eV;             /* 0.5 m_e V_scale^2 / e */
+    /* resonant charge exchange per ion species */
+    int32_t rcx_on[EDP_MAX_ION_SPECIES];
+    double rcx_prob_factor;              /* n_gas * dt * N_subcycles */
+    double rcx_sigma_1eV, rcx_alpha;
+    double rcx_probab_thermal[EDP_MAX_ION_SPECIES];
+    double rcx_vfactor[EDP_MAX_ION_SPECIES];
+    /* Maxwellian inverse CDF v(0:R_max) */
+    int32_t maxwell_rmax;
+    const double* maxwell_v;
+} edp_tables;
+
+/* Counters of one step (COLLECT_PARTICLE_BOUNDARY_HITS, collision counters, particle totals). */
+typedef struct edp_counters {
+    int64_t n_particles[1 + EDP_MAX_ION_SPECIES];           /* live particles */
+    int64_t electron_hits[EDP_N_HIT_COUNTERS];              /* whole_object(n)%electron_hit_count, cumulative */
+    int64_t ion_hits[EDP_N_HIT_COUNTERS];
+    int64_t en_collisions[EDP_MAX_COLPROC];                 /* collision_e_neutral(1)%counter(p), cumulative */
+    int64_t rcx_collisions[EDP_MAX_ION_SPECIES];
+    int64_t step;                                           /* T_cntr */
+    int32_t cg_iterations;                                  /* last CG solve */
+    double cg_relres;
+    int32_t error_flags;                                    /* device error word (bit set per EDP_ERR_*) */
+} edp_counters;
+
+typedef struct edp_ctx edp_ctx;
+
+/* ---- set-up / tear-down ------------------------------------------------------------------------- */
+/* after INITIATE_*_COLLISIONS (pic2d_MainProgram.f90:36-60): copies params and tables to the device */
+int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out);
+/* end of MainProg (pic2d_MainProgram.f90:414-419) */
+int edp_destroy(edp_ctx* ctx);
+int edp_last_error(const edp_ctx* ctx, char* buf, size_t len);
+int edp_set_sync(edp_ctx* ctx, int sync);
+int edp_synchronize(edp_ctx* ctx);
+
+/* ---- particles ----------------------------------------------------------------------------------- */
+/* after DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325) or a checkpoint read: the host's
+ * AoS TYPE particle arrays, split into columns. ids may be NULL (then 0..n-1 are assigned). */
+int edp_upload_particles(edp_ctx* ctx, int species, int64_t n, const double* x, const double* y,
+                         const double* vx, const double* vy, const double* vz, const int32_t* tag,
+                         const uint32_t* id);
+/* for checkpoints/snapshots: copies live particles back (compacted), n_out receives the count */
+int edp_download_particles(edp_ctx* ctx, int species, int64_t cap, int64_t* n_out, double* x, double* y,
+                           double* vx, double* vy, double* vz, int32_t* tag, uint32_t* id);
+/* DISTRIBUTE_PARTICLES on the device: per_cell particles in every cell, uniform positions, Maxwellian
+ * velocities of width factor_convert (sqrt(T_init/T_scale)/N_max_vel [/sqrt(Ms)]), vz zeroed when
+ * zero_vz (ions, :3298). Ion species s takes the positions of the electrons when copy_positions. */
+int edp_distribute_particles(edp_ctx* ctx, int species, int32_t per_cell, double factor_convert,
+                             int32_t zero_vz, int32_t copy_positions_from_electrons);
+
+/* ---- per-step cycle ------------------------------------------------------------------------------ */
+/* GATHER_ELECTRON_CHARGE_DENSITY (pic2d_ElectronDynamics.f90:1535-1975) / GATHER_ION_CHARGE_DENSITY
+ * (pic2d_IonDynamics.f90:1540-2003). The deposit itself is fused into the pushes; this call only
+ * converts the accumulated fixed-point density to FP64 with the periodic fold and wall factors and,
+ * when rho_out != NULL, copies it to the host (species EDP_ELECTRONS: c_rho; EDP_IONS: c_rho_i, Qs-weighted). */
+int edp_gather_charge_density(edp_ctx* ctx, int species, double* rho_out);
+/* UPDATE_WALL_POTENTIALS (pic2d_WallPotentials.f90:1-56) for step T_cntr */
+int edp_update_wall_potentials(edp_ctx* ctx, int64_t t_cntr);
+/* SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY
+ * (pic2d_ElectricFieldCalc_FFT_X.f90:3-1547): phi_out may be NULL */
+int edp_field_fftx(edp_ctx* ctx, double* phi_out);
+/* SOLVE_POTENTIAL_WITH_PETSC + CALCULATE_ELECTRIC_FIELD (pic2d_ElectricFieldCalc_PETSc.F90:7-805,
+ * pic2d_PETSc_Solver.F90:31-40): preconditioned CG to rtol on the same operator, FP64 dots. */
+int edp_field_cg(edp_ctx* ctx, double rtol, int32_t max_it, int32_t warm_start, int32_t* iters_out);
+/* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
+ * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
+int edp_advance_electrons(edp_ctx* ctx);
+/* ADVANCE_IONS (pic2d_IonDynamics.f90:3-524), fused with the ion deposit and, when fused, with RCX */
+int edp_advance_ions(edp_ctx* ctx);
+/* PERFORM_ELECTRON_NEUTRAL_COLLISIONS (pic2d_enCollisionsGeneralProc.f90:332-654): a separate pass unless
+ * the push already did it; counters_out[p] receives this step's count of process p (may be NULL) */
+int edp_collide_en(edp_ctx* ctx, int64_t* counters_out);
+/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126) */
+int edp_collide_rcx(edp_ctx* ctx, int64_t* count_out);
+/* PROCESS_ADDED_IONS + CLEAR_ACCUMULATED_FIELDS (pic2d_IonDynamics.f90:1468-1537,
+ * pic2d_ElectricFieldCalc_PETSc.F90:809-829): appends ions born this step, clears acc_E, advances T_cntr */
+int edp_end_ion_cycle(edp_ctx* ctx);
+/* One or more whole steps of pic2d_MainProgram.f90:151-309 in order (convenience for drivers). */
+int edp_step(edp_ctx* ctx, int32_t nsteps);
+
+/* ---- diagnostics / test access -------------------------------------------------------------------- */
+int edp_query_counters(edp_ctx* ctx, edp_counters* out);
+/* node arrays in the reference layout (see Conventions) */
+int edp_get_field(edp_ctx* ctx, int which, double* out);
+int edp_set_field(edp_ctx* ctx, int which, const double* in);
+/* FP64 sums of report_total_number_of_particles (pic2d_Diagnostics.f90:321-460): N, sum vx, vy, vz,
+ * sum vx^2, vy^2, vz^2 for one species */
+int edp_moments(edp_ctx* ctx, int species, double out[7]);
+/* kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:447-485) evaluated on the device for given
+ * (energy, r) pairs: kind_out[k] = indx_coll (n_act+1 = null collision) */
+int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const double* r, int32_t* kind_out);
+
+/* ---- deck reader (host side of INITIATE_PARAMETERS and the collision set-up) --------------------- */
+/* Reads init_configuration.dat, init_simcontrol.dat, init_particles.dat, init_extfields.dat,
+ * init_bo_NN.dat, init_neutrals.dat, init_neutral_<NAME>.dat, its cross-section files and
+ * init_neutral_<NAME>_rcx_param.dat from directory dir (pic2d_CurProblemValues.f90:157-1031,
+ * pic2d_ExternalFields.f90:3-195, pic2d_Setup.f90:60-100, pic2d_enCollisionsGeneralProc.f90:5-325,
+ * pic2d_inCollisionsGeneralProc.f90:3-90). The deck owns the table arrays that t points into. */
+typedef struct edp_deck edp_deck;
+int edp_deck_read(const char* dir, edp_deck** out, edp_params* p, edp_tables* t);
+/* initial plasma of init_particles.dat: init_Te_eV, init_Ne_m3, init_Ti_eV(s), T_e_eV, N_max_vel ... */
+int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_ne_m3, double* init_ti_ev,
+                            double* t_e_ev, int32_t* n_max_vel, double* n_plasma_m3, int64_t* max_t_cntr);
+int edp_deck_free(edp_deck* d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDIPIC_GPU_H */

@@ -1,0 +1,947 @@
+// ORACLE (test infrastructure only): CPU FP64 restatement of EDIPIC-2D's per-step particle cycle.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load liboracle.so; the
+// product library never links or calls it. Each function names the reference routine it restates.
+// Built with -ffp-contract=off so the multiply/add order written here is the order executed.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// physical constants of pic2d_Modules.f90:161-168
+const double E_CL = 1.602189e-19;
+const double M_E_KG = 9.109534e-31;
+const double PI = 3.141592653589793;
+
+inline int64_t node(const oracle_geom_t* g, int i, int j) { return (int64_t)j * oracle_nx_nodes(g) + i; }
+
+struct Area {
+    double xmin, xmax, ymin, ymax;
+    int ixmax, jymax;  // c_indx_x_max, c_indx_y_max
+};
+
+Area area_of(const oracle_geom_t* g)
+{
+    Area a;
+    a.xmin = 0.0;
+    a.ymin = 0.0;
+    a.ixmax = g->periodic ? g->ncx + 1 : g->ncx;
+    a.jymax = g->ncy;
+    a.xmax = (double)a.ixmax;
+    a.ymax = (double)a.jymax;
+    return a;
+}
+
+inline void remove_particle(oracle_parts_t* p, int64_t k)
+{
+    // REMOVE_ELECTRON (pic2d_ElectronDynamics.f90:517-555): the last particle takes slot k
+    int64_t last = p->n - 1;
+    if (k < last) {
+        p->x[k] = p->x[last];
+        p->y[k] = p->y[last];
+        p->vx[k] = p->vx[last];
+        p->vy[k] = p->vy[last];
+        p->vz[k] = p->vz[last];
+        p->tag[k] = p->tag[last];
+        p->id[k] = p->id[last];
+    }
+    p->n = last;
+}
+
+inline double uniform(uint32_t x) { return ((double)x + 0.5) * 0x1p-32; }
+
+void philox_block(uint32_t id, uint64_t seed, uint32_t step, uint32_t stream, uint32_t block, uint32_t out[4])
+{
+    uint32_t ctr[4] = {step, stream, block, (uint32_t)(seed >> 32)};
+    uint32_t key[2] = {id, (uint32_t)seed};
+    oracle_philox4x32_10(ctr, key, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t oracle_nx_nodes(const oracle_geom_t* g) { return g->periodic ? g->ncx + 2 : g->ncx + 1; }
+
+// ------------------------------------------------------------------------------------------- push
+// ADVANCE_ELECTRONS pic2d_ElectronDynamics.f90:3-513 and ADVANCE_IONS pic2d_IonDynamics.f90:3-524 for a
+// single cluster covering the domain. Object numbering for hits: 0 below, 1 above, 2 left, 3 right, 4+k inner.
+void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                 oracle_parts_t* p, int64_t* hits)
+{
+    const Area a = area_of(g);
+    const double L = (double)g->ncx;  // L_period_X
+    int64_t k = 0;
+    while (k < p->n) {
+        double X = p->x[k], Y = p->y[k];
+        int i = (int)X, j = (int)Y;
+        if (X == a.xmax) i = a.ixmax - 1;
+        if (Y == a.ymax) j = a.jymax - 1;
+        double ax_ip1 = X - (double)i, ax_i = 1.0 - ax_ip1;
+        double ay_jp1 = Y - (double)j, ay_j = 1.0 - ay_jp1;
+        const double* fx = EX;
+        const double* fy = EY;
+        double E_X = fx[node(g, i, j)] * ax_i * ay_j + fx[node(g, i + 1, j)] * ax_ip1 * ay_j +
+                     fx[node(g, i, j + 1)] * ax_i * ay_jp1 + fx[node(g, i + 1, j + 1)] * ax_ip1 * ay_jp1;
+        double E_Y = fy[node(g, i, j)] * ax_i * ay_j + fy[node(g, i + 1, j)] * ax_ip1 * ay_j +
+                     fy[node(g, i, j + 1)] * ax_i * ay_jp1 + fy[node(g, i + 1, j + 1)] * ax_ip1 * ay_jp1;
+        double vx = p->vx[k], vy = p->vy[k], vz = p->vz[k];
+        if (!sp->is_ion) {
+            double E_Z = sp->ez;
+            double alfa_x = -0.5 * sp->bx, alfa_y = -0.5 * sp->by, alfa_z = -0.5 * sp->bz;
+            double ax2 = alfa_x * alfa_x, ay2 = alfa_y * alfa_y, az2 = alfa_z * alfa_z;
+            double theta2 = ax2 + ay2 + az2;
+            double inv = 1.0 / (1.0 + theta2);
+            double K11 = (1.0 - theta2 + 2.0 * ax2) * inv, K12 = 2.0 * (alfa_x * alfa_y + alfa_z) * inv,
+                   K13 = 2.0 * (alfa_x * alfa_z - alfa_y) * inv;
+            double K21 = 2.0 * (alfa_x * alfa_y - alfa_z) * inv, K22 = (1.0 - theta2 + 2.0 * ay2) * inv,
+                   K23 = 2.0 * (alfa_y * alfa_z + alfa_x) * inv;
+            double K31 = 2.0 * (alfa_x * alfa_z + alfa_y) * inv, K32 = 2.0 * (alfa_y * alfa_z - alfa_x) * inv,
+                   K33 = (1.0 - theta2 + 2.0 * az2) * inv;
+            double VXm = vx - 0.5 * E_X, VYm = vy - 0.5 * E_Y, VZm = vz - 0.5 * E_Z;
+            double VXp = K11 * VXm + K12 * VYm + K13 * VZm;
+            double VYp = K21 * VXm + K22 * VYm + K23 * VZm;
+            double VZp = K31 * VXm + K32 * VYm + K33 * VZm;
+            vx = VXp - 0.5 * E_X;
+            vy = VYp - 0.5 * E_Y;
+            vz = VZp - 0.5 * E_Z;
+            X = X + vx;
+            Y = Y + vy;
+        } else {
+            double E_Z = sp->ions_sense_ez ? sp->ez * sp->nsub : 0.0;
+            double q = sp->qm2;
+            if (sp->ions_sense_b) {
+                double qn = q * sp->nsub;
+                double alfa_x = qn * sp->bx, alfa_y = qn * sp->by, alfa_z = qn * sp->bz;
+                double ax2 = alfa_x * alfa_x, ay2 = alfa_y * alfa_y, az2 = alfa_z * alfa_z;
+                double theta2 = ax2 + ay2 + az2;
+                double inv = 1.0 / (1.0 + theta2);
+                double K11 = (1.0 - theta2 + 2.0 * ax2) * inv, K12 = 2.0 * (alfa_x * alfa_y + alfa_z) * inv,
+                       K13 = 2.0 * (alfa_x * alfa_z - alfa_y) * inv;
+                double K21 = 2.0 * (alfa_x * alfa_y - alfa_z) * inv, K22 = (1.0 - theta2 + 2.0 * ay2) * inv,
+                       K23 = 2.0 * (alfa_y * alfa_z + alfa_x) * inv;
+                double K31 = 2.0 * (alfa_x * alfa_z + alfa_y) * inv, K32 = 2.0 * (alfa_y * alfa_z - alfa_x) * inv,
+                       K33 = (1.0 - theta2 + 2.0 * az2) * inv;
+                double VXm = vx + q * E_X, VYm = vy + q * E_Y, VZm = vz + q * E_Z;
+                double VXp = K11 * VXm + K12 * VYm + K13 * VZm;
+                double VYp = K21 * VXm + K22 * VYm + K23 * VZm;
+                double VZp = K31 * VXm + K32 * VYm + K33 * VZm;
+                vx = VXp + q * E_X;
+                vy = VYp + q * E_Y;
+                vz = VZp + q * E_Z;
+            } else {
+                vx = vx + (q + q) * E_X;
+                vy = vy + (q + q) * E_Y;
+                vz = vz + (q + q) * E_Z;
+            }
+            X = X + vx * sp->nsub;
+            Y = Y + vy * sp->nsub;
+        }
+        p->vx[k] = vx;
+        p->vy[k] = vy;
+        p->vz[k] = vz;
+
+        // inner objects (:160-172): strictly inside the rectangle
+        bool hit_inner = false;
+        for (int n = 0; n < g->n_inner; ++n) {
+            if (X <= (double)g->ileft[n] || X >= (double)g->iright[n]) continue;
+            if (Y <= (double)g->jbottom[n] || Y >= (double)g->jtop[n]) continue;
+            hits[4 + n]++;
+            hit_inner = true;
+            break;
+        }
+        if (hit_inner) {
+            remove_particle(p, k);
+            continue;
+        }
+        if (X >= a.xmin && X <= a.xmax && Y >= a.ymin && Y <= a.ymax) {
+            p->x[k] = X;
+            p->y[k] = Y;
+            ++k;
+            continue;
+        }
+        if (g->periodic) {
+            // self-connected periodic cluster (:185-210, :304-330, :430-443, :476-488)
+            if (X < a.xmin) X += L;
+            else if (X > a.xmax) X -= L;
+            if (Y < a.ymin) {
+                hits[0]++;
+                remove_particle(p, k);
+            } else if (Y > a.ymax) {
+                hits[1]++;
+                remove_particle(p, k);
+            } else {
+                p->x[k] = X;
+                p->y[k] = Y;
+                ++k;
+            }
+            continue;
+        }
+        // walls on four sides, corners of type SURROUNDED_BY_WALL (:212-300, :332-420, :445-474, :490-518)
+        int obj;
+        if (X < a.xmin) {
+            if (Y >= a.ymin + 1.0 && Y <= a.ymax - 1.0) obj = 2;
+            else if (Y < a.ymin + 1.0) obj = ((a.xmin - X) < (a.ymin - Y)) ? 0 : 2;
+            else obj = ((a.xmin - X) < (Y - a.ymax)) ? 1 : 2;
+        } else if (X > a.xmax) {
+            if (Y >= a.ymin + 1.0 && Y <= a.ymax - 1.0) obj = 3;
+            else if (Y < a.ymin + 1.0) obj = ((X - a.xmax) < (a.ymin - Y)) ? 0 : 3;
+            else obj = ((X - a.xmax) < (Y - a.ymax)) ? 1 : 3;
+        } else if (Y > a.ymax) {
+            obj = 1;
+        } else {
+            obj = 0;
+        }
+        hits[obj]++;
+        remove_particle(p, k);
+    }
+}
+
+// GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1597-1639 (the CIC loop; weight = Qs for ions)
+void oracle_deposit(const oracle_geom_t* g, const oracle_parts_t* p, double weight, double* rho)
+{
+    const Area a = area_of(g);
+    const int64_t nn = (int64_t)oracle_nx_nodes(g) * (g->ncy + 1);
+    std::fill(rho, rho + nn, 0.0);
+    for (int64_t k = 0; k < p->n; ++k) {
+        double X = p->x[k], Y = p->y[k];
+        int i = (int)X, j = (int)Y;
+        if (X == a.xmax) i = a.ixmax - 1;
+        if (Y == a.ymax) j = a.jymax - 1;
+        double ax_ip1 = X - (double)i, ax_i = 1.0 - ax_ip1;
+        double ay_jp1 = Y - (double)j, ay_j = 1.0 - ay_jp1;
+        double vij = ax_i * ay_j, vip1j = ax_ip1 * ay_j, vijp1 = ax_i * ay_jp1;
+        rho[node(g, i, j)] += weight * vij;
+        rho[node(g, i + 1, j)] += weight * vip1j;
+        rho[node(g, i, j + 1)] += weight * vijp1;
+        rho[node(g, i + 1, j + 1)] += weight * (1.0 - vij - vip1j - vijp1);
+    }
+}
+
+// periodic fold :1661-1667 and wall factors :1802-1880
+void oracle_fold_and_wall_scale(const oracle_geom_t* g, double* rho)
+{
+    const int nx = oracle_nx_nodes(g);
+    const int imax = nx - 1, jmax = g->ncy;
+    if (g->periodic) {
+        for (int j = 0; j <= jmax; ++j) {
+            rho[node(g, 1, j)] += rho[node(g, imax, j)];
+            rho[node(g, imax - 1, j)] += rho[node(g, 0, j)];
+            rho[node(g, 0, j)] = rho[node(g, imax - 1, j)];
+            rho[node(g, imax, j)] = rho[node(g, 1, j)];
+        }
+        for (int i = 0; i <= imax; ++i) {
+            rho[node(g, i, jmax)] *= 2.0;
+            rho[node(g, i, 0)] *= 2.0;
+        }
+        return;
+    }
+    for (int j = 1; j <= jmax - 1; ++j) {
+        rho[node(g, 0, j)] *= 2.0;
+        rho[node(g, imax, j)] *= 2.0;
+    }
+    for (int i = 1; i <= imax - 1; ++i) {
+        rho[node(g, i, jmax)] *= 2.0;
+        rho[node(g, i, 0)] *= 2.0;
+    }
+    rho[node(g, 0, 0)] *= 4.0;
+    rho[node(g, 0, jmax)] *= 4.0;
+    rho[node(g, imax, 0)] *= 4.0;
+    rho[node(g, imax, jmax)] *= 4.0;
+}
+
+// ---------------------------------------------------------------------------------- Maxwell sampler
+// PrepareMaxwellDistribIntegral pic2d_ElectronWallCollisions.f90:835-929 (U_max = 3, R_max = 9000,
+// R_max_inj = 4500 from pic2d_Modules.f90:949-951)
+void oracle_maxwell_tables(double* v, double* v_inj)
+{
+    const double U_max = 3.0;
+    const int R_max = 9000, R_max_inj = 4500;
+    std::vector<double> F(180004, 0.0);
+    {
+        const int N = 180000;
+        const double Vmin = -U_max, Vmax = U_max, dV = (Vmax - Vmin) / N;
+        F[0] = 0.0;
+        for (int i = 1; i <= N + 3; ++i) {
+            double u = Vmin + ((double)i - 0.5) * dV;
+            F[i] = F[i - 1] + std::exp(-(u * u));
+        }
+        double t = F[N];
+        for (int i = 0; i <= N + 3; ++i) F[i] = F[i] * R_max / t;
+        v[0] = Vmin;
+        int count = 0;
+        for (int i = 1; i <= N + 3; ++i) {
+            if ((int)F[i] - count == 1) {
+                ++count;
+                v[count] = Vmin + i * dV;
+                if (count == R_max) break;
+            }
+        }
+    }
+    {
+        const int N = 90000;
+        const double Vmin = 0.0, Vmax = U_max, dV = (Vmax - Vmin) / N;
+        std::fill(F.begin(), F.end(), 0.0);
+        for (int i = 1; i <= N + 3; ++i) {
+            double t = Vmin + ((double)(float)i - 0.5) * dV;
+            F[i] = F[i - 1] + std::exp(-(t * t)) * t;
+        }
+        double t = F[N];
+        for (int i = 1; i <= N + 3; ++i) F[i] = F[i] * R_max_inj / t;
+        v_inj[0] = Vmin;
+        int count = 0;
+        for (int i = 1; i <= N + 3; ++i) {
+            if ((int)F[i] - count == 1) {
+                ++count;
+                v_inj[count] = Vmin + i * dV;
+                if (count == R_max_inj) break;
+            }
+        }
+    }
+}
+
+// GetMaxwellVelocity :961-985
+double oracle_maxwell_sample(const double* v, double u)
+{
+    const int R_max = 9000;
+    double R = R_max * u;
+    int indx = (int)R;
+    if (indx < R_max) return v[indx] + (R - indx) * (v[indx + 1] - v[indx]);
+    return v[R_max];
+}
+
+// --------------------------------------------------------------------------- e-n collision table
+// frequency_of_en_collision pic2d_enCollisionsSpecificProc.f90:4-57
+double oracle_en_frequency(const oracle_crsect_t* cs, double energy_eV, double n_m3, int32_t nsub, double dt_s)
+{
+    const int N = cs->n_points;
+    const double* e = cs->energy_eV;
+    const double* s = cs->crsect_m2;
+    double f;
+    if (energy_eV >= e[N - 1]) {
+        f = s[N - 1] * std::sqrt(2.0 * energy_eV * E_CL / M_E_KG);
+    } else if (energy_eV < e[0]) {
+        f = (cs->type < 20) ? s[0] * std::sqrt(2.0 * energy_eV * E_CL / M_E_KG) : 0.0;
+    } else {
+        int j;  // 1-based in the reference, 0-based here
+        for (j = 0; j < N - 1; ++j)
+            if (energy_eV >= e[j] && energy_eV < e[j + 1]) break;
+        j = std::min(j, N - 2);
+        double ej = e[j], ejp1 = e[j + 1];
+        double fj = s[j] * std::sqrt(2.0 * ej * E_CL / M_E_KG);
+        double fjp1 = s[j + 1] * std::sqrt(2.0 * ejp1 * E_CL / M_E_KG);
+        f = fj + (fjp1 - fj) * (energy_eV - ej) / (ejp1 - ej);
+    }
+    return f * n_m3 * nsub * dt_s;
+}
+
+// energy grid of INITIATE_ELECTRON_NEUTRAL_COLLISIONS pic2d_enCollisionsGeneralProc.f90:236-279
+int32_t oracle_mcc_n_values(int32_t n_seg, const double* seg_value, const double* seg_step)
+{
+    int32_t n = 0;
+    for (int i = 1; i <= n_seg; ++i) n += (int32_t)((seg_value[i] - seg_value[i - 1]) / seg_step[i - 1] + 0.001);
+    return n;
+}
+
+// probability table :281-322
+void oracle_mcc_build(oracle_mcc_table_t* t, int32_t n_act, const oracle_crsect_t* cs, double n_m3, int32_t nsub,
+                      double dt_s)
+{
+    t->n_act = n_act;
+    t->n_values = oracle_mcc_n_values(t->n_seg, t->seg_value, t->seg_step);
+    t->seg_index[0] = 0;
+    for (int i = 1; i <= t->n_seg; ++i)
+        t->seg_index[i] =
+            t->seg_index[i - 1] + (int32_t)((t->seg_value[i] - t->seg_value[i - 1]) / t->seg_step[i - 1] + 0.001);
+    t->energy_eV[0] = t->seg_value[0];
+    for (int i = 1; i <= t->n_seg; ++i) {
+        for (int j = t->seg_index[i - 1] + 1; j <= t->seg_index[i] - 1; ++j)
+            t->energy_eV[j] = t->seg_value[i - 1] + (j - t->seg_index[i - 1]) * t->seg_step[i - 1];
+        t->energy_eV[t->seg_index[i]] = t->seg_value[i];
+    }
+    const int NV = t->n_values;
+    double* P = t->prob;
+    for (int ie = 0; ie <= NV; ++ie) {
+        double en = t->energy_eV[ie];
+        P[(int64_t)ie * n_act + 0] = oracle_en_frequency(&cs[0], en, n_m3, nsub, dt_s);
+        for (int p = 1; p < n_act; ++p)
+            P[(int64_t)ie * n_act + p] = P[(int64_t)ie * n_act + p - 1] + oracle_en_frequency(&cs[p], en, n_m3, nsub, dt_s);
+    }
+    int imax = 0;
+    for (int ie = 1; ie <= NV; ++ie)
+        if (P[(int64_t)ie * n_act + n_act - 1] > P[(int64_t)imax * n_act + n_act - 1]) imax = ie;
+    double pmax = P[(int64_t)imax * n_act + n_act - 1];
+    t->max_colliding_fraction = 1.0 - std::exp(-pmax);
+    for (int ie = 0; ie <= NV; ++ie)
+        for (int p = 0; p < n_act; ++p) {
+            double v = P[(int64_t)ie * n_act + p] / pmax;
+            P[(int64_t)ie * n_act + p] = std::max(0.0, std::min(1.0, v));
+        }
+    P[(int64_t)imax * n_act + n_act - 1] = 1.0;
+    for (int ie = 0; ie <= NV; ++ie)
+        for (int p = 0; p < n_act - 1; ++p)
+            P[(int64_t)ie * n_act + p + 1] = std::max(P[(int64_t)ie * n_act + p], P[(int64_t)ie * n_act + p + 1]);
+    for (int p = 0; p < n_act; ++p) {
+        t->type[p] = cs[p].type;
+        t->threshold_eV[p] = (cs[p].type >= 20) ? cs[p].energy_eV[0] : 0.0;
+    }
+}
+
+// kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS :451-485. The weighted threshold is formed with
+// explicit fused multiply-adds (fma(a1, P1, a0*P0)) so that the GPU kernels can reproduce it bit for bit.
+int32_t oracle_mcc_choose(const oracle_mcc_table_t* t, double energy_eV, double r)
+{
+    const int na = t->n_act;
+    int indx;
+    double a0, a1;
+    if (energy_eV >= t->seg_value[t->n_seg]) {
+        indx = t->n_values - 1;
+        a1 = 1.0;
+        a0 = 0.0;
+    } else if (energy_eV < t->seg_value[0]) {
+        indx = 0;
+        a1 = 0.0;
+        a0 = 1.0;
+    } else {
+        int seg = 1;
+        for (int i = t->n_seg - 1; i >= 0; --i)
+            if (energy_eV >= t->seg_value[i]) {
+                seg = i + 1;
+                break;
+            }
+        double step = t->seg_step[seg - 1];
+        double fi = (double)t->seg_index[seg - 1] + (energy_eV - t->seg_value[seg - 1]) / step;
+        indx = (int)fi;
+        indx = std::max(0, std::min(indx, t->n_values - 1));
+        a1 = (energy_eV - t->energy_eV[indx]) / step;
+        a0 = 1.0 - a1;
+    }
+    int k;
+    for (k = na; k >= 1; --k) {
+        double thr = std::fma(a1, t->prob[(int64_t)(indx + 1) * na + k - 1], a0 * t->prob[(int64_t)indx * na + k - 1]);
+        if (r > thr) break;
+    }
+    return k + 1;
+}
+
+// velocity rotation common to en_Collision_* (e.g. pic2d_enCollisionsSpecificProc.f90:117-144)
+static void rotate(double cosk, double sink, double cosf, double sinf, const double* v, double* out)
+{
+    double Vx = v[0], Vy = v[1], Vz = v[2];
+    double V = std::sqrt(Vx * Vx + Vy * Vy + Vz * Vz);
+    double Vxy = std::sqrt(Vx * Vx + Vy * Vy);
+    if (Vxy > 1.0e-20) {
+        double a = Vx / Vxy, b = Vy / Vxy;
+        out[0] = Vx * cosk + (sinf * V * b + cosf * Vz * a) * sink;
+        out[1] = Vy * cosk - (sinf * V * a - cosf * Vz * b) * sink;
+        out[2] = Vz * cosk - Vxy * cosf * sink;
+    } else {
+        out[0] = std::fabs(Vz) * sink * cosf;
+        out[1] = std::fabs(Vz) * sink * sinf;
+        out[2] = Vz * cosk;
+    }
+}
+
+static double clampc(double c) { return std::max(std::min(0.999999999999, c), -0.999999999999); }
+static double okhrimovskyy(double e, double R) { return 1.0 - 2.0 * R / (1.0 + 8.0 * (e / 27.21) * (1.0 - R)); }
+
+// en_Collision_Elastic_10 :61-183, _Elastic_11 :187-269, _Inelastic_20 :273-394, _Ionization_30 :398-639
+int32_t oracle_en_scatter(int32_t kind, double energy_eV, double threshold_eV, double neutral_mass_amu,
+                          double ion_velocity_factor, const double* maxwell_v, const double* u, double* v,
+                          double* new_e, double* new_i)
+{
+    double out[3];
+    if (kind == 10 || kind == 11) {
+        double c = (kind == 10) ? okhrimovskyy(energy_eV, u[0]) : 1.0 - 2.0 * u[0];
+        c = clampc(c);
+        double ksi = std::acos(c), s = std::sin(ksi);
+        double fi = u[1] * 6.28318530718;
+        rotate(c, s, std::cos(fi), std::sin(fi), v, out);
+        double alpha = std::sqrt(1.0 - (0.001097161 / neutral_mass_amu) * (1.0 - c));
+        v[0] = out[0] * alpha;
+        v[1] = out[1] * alpha;
+        v[2] = out[2] * alpha;
+        return 0;
+    }
+    if (kind == 20) {
+        if (energy_eV <= threshold_eV) return 0;
+        double esc = std::max(0.0, energy_eV - threshold_eV);
+        double c = clampc(okhrimovskyy(esc, u[0]));
+        double ksi = std::acos(c), s = std::sin(ksi);
+        double fi = u[1] * 6.28318530718;
+        rotate(c, s, std::cos(fi), std::sin(fi), v, out);
+        double alpha = std::sqrt(esc / energy_eV);
+        v[0] = out[0] * alpha;
+        v[1] = out[1] * alpha;
+        v[2] = out[2] * alpha;
+        return 0;
+    }
+    // kind 30, ionisation with B = 10 eV (:451)
+    if (energy_eV <= threshold_eV) return 0;
+    const double B = 10.0;
+    double eej = B * std::tan(u[0] * std::atan(0.5 * (energy_eV - threshold_eV) / B));
+    eej = std::max(0.0, std::min(eej, 0.5 * (energy_eV - threshold_eV)));
+    double esc = std::max(0.0, energy_eV - threshold_eV - eej);
+    double csc = clampc(okhrimovskyy(esc, u[1]));
+    double ksc = std::acos(csc), ssc = std::sin(ksc);
+    double fsc = u[2] * 6.28318530718;
+    double cej = clampc(okhrimovskyy(eej, u[3]));
+    double kej = std::acos(cej), sej = std::sin(kej);
+    double fej = u[4] * 6.28318530718;
+    double vin[3] = {v[0], v[1], v[2]};
+    double osc[3], oej[3];
+    rotate(csc, ssc, std::cos(fsc), std::sin(fsc), vin, osc);
+    double asc = std::sqrt(esc / energy_eV);
+    v[0] = osc[0] * asc;
+    v[1] = osc[1] * asc;
+    v[2] = osc[2] * asc;
+    rotate(cej, sej, std::cos(fej), std::sin(fej), vin, oej);
+    double aej = std::sqrt(eej / energy_eV);
+    new_e[0] = oej[0] * aej;
+    new_e[1] = oej[1] * aej;
+    new_e[2] = oej[2] * aej;
+    new_i[0] = oracle_maxwell_sample(maxwell_v, u[5]) * ion_velocity_factor;
+    new_i[1] = oracle_maxwell_sample(maxwell_v, u[6]) * ion_velocity_factor;
+    new_i[2] = oracle_maxwell_sample(maxwell_v, u[7]) * ion_velocity_factor;
+    return 1;
+}
+
+static void append(oracle_parts_t* p, int64_t cap, double x, double y, const double* v, uint32_t id)
+{
+    if (p->n >= cap) return;
+    int64_t k = p->n++;
+    p->x[k] = x;
+    p->y[k] = y;
+    p->vx[k] = v[0];
+    p->vy[k] = v[1];
+    p->vz[k] = v[2];
+    p->tag[k] = 0;
+    p->id[k] = id;
+}
+
+// PERFORM_ELECTRON_NEUTRAL_COLLISIONS :332-485 with a per-particle Bernoulli(P_max) selection in place of the
+// binary-tree draw of floor(P_max N) distinct particles; kind choice and scattering as in the reference.
+void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
+                       oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters)
+{
+    const double pmax = tab->max_colliding_fraction;
+    for (int64_t k = 0; k < e->n; ++k) {
+        uint32_t b0[4];
+        philox_block(e->id[k], c->seed, c->step, 0u, 0u, b0);
+        if (!(uniform(b0[0]) < pmax)) continue;
+        double r = uniform(b0[1]);
+        double vx = e->vx[k], vy = e->vy[k], vz = e->vz[k];
+        double v2 = std::fma(vz, vz, std::fma(vy, vy, vx * vx));
+        double en = v2 * c->energy_factor_eV;
+        int kind_index = oracle_mcc_choose(tab, en, r);
+        if (kind_index > tab->n_act) continue;
+        uint32_t b1[4], b2[4];
+        philox_block(e->id[k], c->seed, c->step, 0u, 1u, b1);
+        philox_block(e->id[k], c->seed, c->step, 0u, 2u, b2);
+        double u[8] = {uniform(b1[0]), uniform(b1[1]), uniform(b1[2]), uniform(b1[3]),
+                       uniform(b2[0]), uniform(b2[1]), uniform(b2[2]), uniform(b2[3])};
+        double v[3] = {vx, vy, vz}, ne[3], ni[3];
+        int kind = tab->type[kind_index - 1];
+        int born = oracle_en_scatter(kind, en, tab->threshold_eV[kind_index - 1], c->neutral_mass_amu,
+                                     c->ion_velocity_factor, c->maxwell_v, u, v, ne, ni);
+        // en_Collision_Inelastic_20 / _Ionization_30 return before counting when below threshold
+        if ((kind == 20 || kind == 30) && en <= tab->threshold_eV[kind_index - 1]) continue;
+        e->vx[k] = v[0];
+        e->vy[k] = v[1];
+        e->vz[k] = v[2];
+        counters[kind_index - 1]++;
+        if (born) {
+            append(born_e, cap_born, e->x[k], e->y[k], ne, 0u);
+            append(born_i, cap_born, e->x[k], e->y[k], ni, 0u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------ RCX
+// calculate_thermal_cx_probab pic2d_inCollisionsSpecificProc.f90:4-31 with sigma_rcx_m2 :35-44
+double oracle_rcx_probab_thermal(double sigma_1eV, double alpha, double T_K, double n_m3, double Ms, double dt_s,
+                                 int32_t nsub)
+{
+    const double KB = 1.38064852e-23;
+    double Tgas_eV = T_K * KB / E_CL;
+    double e = std::max(1.5 * Tgas_eV, 0.001);
+    double l = 1.0 - alpha * std::log(e);
+    double sig = sigma_1eV * l * l;
+    double vmean = std::sqrt(2.54647908947033 * Tgas_eV * E_CL / (Ms * M_E_KG));
+    return n_m3 * sig * vmean * dt_s * nsub;
+}
+
+// PERFORM_RESONANT_CHARGE_EXCHANGE :48-126
+int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint32_t species, oracle_parts_t* ions)
+{
+    int64_t count = 0;
+    double pt2 = r->probab_thermal * r->probab_thermal;
+    for (int64_t k = 0; k < ions->n; ++k) {
+        double vx = ions->vx[k], vy = ions->vy[k], vz = ions->vz[k];
+        double vsq = vx * vx + vy * vy + vz * vz;
+        double en = vsq * r->factor_eV;
+        double vabs = std::sqrt(vsq) * r->v_scale_ms;
+        double l = 1.0 - r->alpha * std::log(std::max(en, 0.001));
+        double p = r->prob_factor * vabs * (r->sigma_1eV * l * l);
+        p = std::sqrt(p * p + pt2);
+        uint32_t b[4];
+        philox_block(ions->id[k], c->seed, c->step, 1u + (species << 8), 0u, b);
+        if (uniform(b[0]) <= p) {
+            ions->vx[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[1])) * r->vfactor;
+            ions->vy[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[2])) * r->vfactor;
+            ions->vz[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[3])) * r->vfactor;
+            ++count;
+        }
+    }
+    return count;
+}
+
+// ------------------------------------------------------------------------------------- FFT_X solve
+// Radix-2 complex FFT (Danielson-Lanczos, iterative, bit reversal), sign = +1 forward kernel exp(+2 pi i jk/N)
+// as in FOUR1_8 (pic2d_ElectricFieldCalc_FFT_X.f90:1648-1710); twiddles are evaluated directly.
+static void fft_complex(std::vector<double>& re, std::vector<double>& im, int sign)
+{
+    const int n = (int)re.size();
+    for (int i = 1, j = 0; i < n; ++i) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            std::swap(re[i], re[j]);
+            std::swap(im[i], im[j]);
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const int half = len >> 1;
+        for (int k = 0; k < half; ++k) {
+            double ang = sign * 2.0 * PI * k / len;
+            double wr = std::cos(ang), wi = std::sin(ang);
+            for (int s = 0; s < n; s += len) {
+                int a = s + k, b = a + half;
+                double tr = wr * re[b] - wi * im[b];
+                double ti = wr * im[b] + wi * re[b];
+                re[b] = re[a] - tr;
+                im[b] = im[a] - ti;
+                re[a] += tr;
+                im[a] += ti;
+            }
+        }
+    }
+}
+
+// SOLVE_POISSON_FFTX_LINSYSY :66-1320 (single cluster, metal walls): row FFT, per-mode Thomas with the spectral
+// diagonal -2 - 4 pi^2 n^2/N^2 and a_eq of PREPARE_SYS_Y (pic2d_Prepare_FFTX_SYSY.f90:834-899), inverse FFT.
+void oracle_fftx_solve(const oracle_geom_t* g, const double* rho, double phi_bottom, double phi_top, double* phi)
+{
+    const int N = g->ncx, J = g->ncy, nx = oracle_nx_nodes(g);
+    const int nm = N / 2 + 1;
+    std::vector<double> Fre((size_t)(J + 1) * nm), Fim((size_t)(J + 1) * nm);
+    std::vector<double> re(N), im(N);
+    for (int j = 0; j <= J; ++j) {
+        for (int i = 0; i < N; ++i) {
+            // xband(1:N-1) = c_rho(1:N-1), xband(0) = c_rho(N) (:155-262)
+            double v = (i == 0) ? rho[node(g, N, j)] : rho[node(g, i, j)];
+            if (j == 0) v = phi_bottom;
+            if (j == J) v = phi_top;
+            re[i] = v;
+            im[i] = 0.0;
+        }
+        fft_complex(re, im, +1);
+        for (int m = 0; m < nm; ++m) {
+            Fre[(size_t)j * nm + m] = re[m];
+            Fim[(size_t)j * nm + m] = (m == 0 || m == N / 2) ? 0.0 : im[m];
+        }
+    }
+    std::vector<double> aeq(J + 1), rr(J + 1), ri(J + 1);
+    for (int m = 0; m < nm; ++m) {
+        double d = -2.0 - 4.0 * PI * PI * (double)m * (double)m / ((double)N * (double)N);
+        aeq[0] = 0.0;
+        for (int j = 1; j <= J - 1; ++j) aeq[j] = 1.0 / (d - aeq[j - 1]);
+        aeq[J] = 0.0;
+        rr[0] = Fre[m];
+        ri[0] = Fim[m];
+        for (int j = 1; j <= J - 1; ++j) {
+            rr[j] = (-Fre[(size_t)j * nm + m] - rr[j - 1]) * aeq[j];
+            ri[j] = (-Fim[(size_t)j * nm + m] - ri[j - 1]) * aeq[j];
+        }
+        rr[J] = Fre[(size_t)J * nm + m];
+        ri[J] = Fim[(size_t)J * nm + m];
+        Fre[(size_t)J * nm + m] = rr[J];
+        Fim[(size_t)J * nm + m] = ri[J];
+        for (int j = J - 1; j >= 0; --j) {
+            Fre[(size_t)j * nm + m] = rr[j] - aeq[j] * Fre[(size_t)(j + 1) * nm + m];
+            Fim[(size_t)j * nm + m] = ri[j] - aeq[j] * Fim[(size_t)(j + 1) * nm + m];
+        }
+    }
+    for (int j = 0; j <= J; ++j) {
+        for (int m = 0; m < nm; ++m) {
+            re[m] = Fre[(size_t)j * nm + m];
+            im[m] = Fim[(size_t)j * nm + m];
+        }
+        for (int m = nm; m < N; ++m) {  // Hermitian completion of the real signal's spectrum
+            re[m] = re[N - m];
+            im[m] = -im[N - m];
+        }
+        fft_complex(re, im, -1);
+        for (int i = 0; i < N; ++i) phi[node(g, i, j)] = re[i] / N;
+        phi[node(g, N, j)] = phi[node(g, 0, j)];
+        phi[node(g, N + 1, j)] = phi[node(g, 1, j)];
+        (void)nx;
+    }
+}
+
+// CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY :1341-1545 (periodic) and CALCULATE_ELECTRIC_FIELD
+// (pic2d_ElectricFieldCalc_PETSc.F90:385-452, walls everywhere)
+void oracle_efield(const oracle_geom_t* g, const double* phi, double f2, double f1, double* ex, double* ey,
+                   double* acc_ex, double* acc_ey)
+{
+    const int nx = oracle_nx_nodes(g), imax = nx - 1, J = g->ncy;
+    auto P = [&](int i, int j) { return phi[node(g, i, j)]; };
+    for (int j = 0; j <= J; ++j)
+        for (int i = 0; i <= imax; ++i) {
+            double EXv = 0.0, EYv = 0.0;
+            if (g->periodic) {
+                int ii = i;
+                if (i == 0) ii = imax - 1;          // E(0) = E(N)  (left neighbour copy)
+                if (i == imax) ii = 1;              // E(N+1) = E(1)
+                EXv = f2 * (P(ii - 1, j) - P(ii + 1, j));
+                if (j == 0) EYv = f1 * (P(ii, 0) - P(ii, 1));
+                else if (j == J) EYv = f1 * (P(ii, J - 1) - P(ii, J));
+                else EYv = f2 * (P(ii, j - 1) - P(ii, j + 1));
+            } else {
+                if (i == 0) EXv = f1 * (P(0, j) - P(1, j));
+                else if (i == imax) EXv = f1 * (P(imax - 1, j) - P(imax, j));
+                else EXv = f2 * (P(i - 1, j) - P(i + 1, j));
+                if (j == 0) EYv = f1 * (P(i, 0) - P(i, 1));
+                else if (j == J) EYv = f1 * (P(i, J - 1) - P(i, J));
+                else EYv = f2 * (P(i, j - 1) - P(i, j + 1));
+            }
+            ex[node(g, i, j)] = EXv;
+            ey[node(g, i, j)] = EYv;
+            if (acc_ex) {
+                acc_ex[node(g, i, j)] += EXv;
+                acc_ey[node(g, i, j)] += EYv;
+            }
+        }
+}
+
+// ------------------------------------------------------------------------------------------- CG
+static int node_kind(const oracle_geom_t* g, int i, int j, int* inner)
+{
+    // 0 unknown, 1 wall (0 below, 1 above, 2 left, 3 right via *inner = -1-side), 2 inner metal (index in *inner)
+    const int imax = g->ncx, J = g->ncy;
+    for (int n = 0; n < g->n_inner; ++n)
+        if (i >= g->ileft[n] && i <= g->iright[n] && j >= g->jbottom[n] && j <= g->jtop[n]) {
+            *inner = n;
+            return 2;
+        }
+    if (j == 0) { *inner = -1; return 1; }
+    if (j == J) { *inner = -2; return 1; }
+    if (i == 0) { *inner = -3; return 1; }
+    if (i == imax) { *inner = -4; return 1; }
+    return 0;
+}
+
+int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho, const double* wall_phi, const double* inner_phi,
+                        double rtol, int32_t max_it, double* phi, double* relres_out)
+{
+    const int nx = oracle_nx_nodes(g), J = g->ncy;
+    const int64_t nn = (int64_t)nx * (J + 1);
+    std::vector<int8_t> kind(nn);
+    for (int j = 0; j <= J; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int w = 0;
+            int k = node_kind(g, i, j, &w);
+            kind[node(g, i, j)] = (int8_t)k;
+            if (k == 1) phi[node(g, i, j)] = wall_phi[-1 - w];
+            if (k == 2) phi[node(g, i, j)] = inner_phi[w];
+        }
+    // A = -(5-point Laplacian) on unknown nodes, b = rho + Dirichlet neighbours
+    std::vector<double> b(nn, 0.0), x(nn, 0.0), r(nn, 0.0), p(nn, 0.0), Ap(nn, 0.0);
+    const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+    for (int j = 1; j < J; ++j)
+        for (int i = 1; i < nx - 1; ++i) {
+            int64_t q = node(g, i, j);
+            if (kind[q]) continue;
+            double s = rho[q];
+            for (int d = 0; d < 4; ++d) {
+                int64_t q2 = node(g, i + di[d], j + dj[d]);
+                if (kind[q2]) s += phi[q2];
+            }
+            b[q] = s;
+            x[q] = phi[q];
+        }
+    auto apply = [&](const std::vector<double>& in, std::vector<double>& out) {
+        for (int j = 1; j < J; ++j)
+            for (int i = 1; i < nx - 1; ++i) {
+                int64_t q = node(g, i, j);
+                if (kind[q]) continue;
+                double s = 4.0 * in[q];
+                for (int d = 0; d < 4; ++d) {
+                    int64_t q2 = node(g, i + di[d], j + dj[d]);
+                    if (!kind[q2]) s -= in[q2];
+                }
+                out[q] = s;
+            }
+    };
+    apply(x, Ap);
+    double bn = 0.0, rr = 0.0;
+    for (int64_t q = 0; q < nn; ++q)
+        if (!kind[q]) {
+            r[q] = b[q] - Ap[q];
+            p[q] = r[q];
+            bn += b[q] * b[q];
+            rr += r[q] * r[q];
+        }
+    bn = std::sqrt(bn);
+    if (bn == 0.0) bn = 1.0;
+    int it = 0;
+    double rel = std::sqrt(rr) / bn;
+    while (rel > rtol && it < max_it) {
+        apply(p, Ap);
+        double pAp = 0.0;
+        for (int64_t q = 0; q < nn; ++q)
+            if (!kind[q]) pAp += p[q] * Ap[q];
+        double alpha = rr / pAp;
+        double rr2 = 0.0;
+        for (int64_t q = 0; q < nn; ++q)
+            if (!kind[q]) {
+                x[q] += alpha * p[q];
+                r[q] -= alpha * Ap[q];
+                rr2 += r[q] * r[q];
+            }
+        double beta = rr2 / rr;
+        rr = rr2;
+        for (int64_t q = 0; q < nn; ++q)
+            if (!kind[q]) p[q] = r[q] + beta * p[q];
+        ++it;
+        rel = std::sqrt(rr) / bn;
+    }
+    for (int64_t q = 0; q < nn; ++q)
+        if (!kind[q]) phi[q] = x[q];
+    if (relres_out) *relres_out = rel;
+    return rel <= rtol ? it : -1;
+}
+
+// ----------------------------------------------------------------------------------- whole cycle
+static void deposit_threads(const oracle_geom_t* g, const oracle_parts_t* p, double w, double* rho, int nthreads)
+{
+    const int64_t nn = (int64_t)oracle_nx_nodes(g) * (g->ncy + 1);
+#ifdef _OPENMP
+    if (nthreads > 1) {
+        std::vector<std::vector<double>> part(nthreads, std::vector<double>(nn, 0.0));
+#pragma omp parallel num_threads(nthreads)
+        {
+            int t = omp_get_thread_num();
+            int64_t lo = p->n * t / nthreads, hi = p->n * (t + 1) / nthreads;
+            oracle_parts_t sub = *p;
+            sub.x += lo; sub.y += lo; sub.vx += lo; sub.vy += lo; sub.vz += lo; sub.tag += lo; sub.id += lo;
+            sub.n = hi - lo;
+            oracle_deposit(g, &sub, w, part[t].data());
+        }
+        std::fill(rho, rho + nn, 0.0);
+        for (int t = 0; t < nthreads; ++t)
+            for (int64_t q = 0; q < nn; ++q) rho[q] += part[t][q];
+        return;
+    }
+#endif
+    (void)nthreads;
+    oracle_deposit(g, p, w, rho);
+}
+
+// push in thread-sized slices; each slice compacts itself, slices are then concatenated in order
+static void push_threads(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                         oracle_parts_t* p, int64_t* hits, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads > 1) {
+        std::vector<int64_t> lo(nthreads), cnt(nthreads);
+        std::vector<std::vector<int64_t>> h(nthreads, std::vector<int64_t>(8, 0));
+#pragma omp parallel num_threads(nthreads)
+        {
+            int t = omp_get_thread_num();
+            int64_t a = p->n * t / nthreads, b = p->n * (t + 1) / nthreads;
+            oracle_parts_t sub = *p;
+            sub.x += a; sub.y += a; sub.vx += a; sub.vy += a; sub.vz += a; sub.tag += a; sub.id += a;
+            sub.n = b - a;
+            oracle_push(g, sp, EX, EY, &sub, h[t].data());
+            lo[t] = a;
+            cnt[t] = sub.n;
+        }
+        int64_t w = cnt[0];
+        for (int t = 1; t < nthreads; ++t) {
+            std::memmove(p->x + w, p->x + lo[t], cnt[t] * sizeof(double));
+            std::memmove(p->y + w, p->y + lo[t], cnt[t] * sizeof(double));
+            std::memmove(p->vx + w, p->vx + lo[t], cnt[t] * sizeof(double));
+            std::memmove(p->vy + w, p->vy + lo[t], cnt[t] * sizeof(double));
+            std::memmove(p->vz + w, p->vz + lo[t], cnt[t] * sizeof(double));
+            std::memmove(p->tag + w, p->tag + lo[t], cnt[t] * sizeof(int32_t));
+            std::memmove(p->id + w, p->id + lo[t], cnt[t] * sizeof(uint32_t));
+            w += cnt[t];
+        }
+        p->n = w;
+        for (int t = 0; t < nthreads; ++t)
+            for (int o = 0; o < 8; ++o) hits[o] += h[t][o];
+        return;
+    }
+#endif
+    (void)nthreads;
+    oracle_push(g, sp, EX, EY, p, hits);
+}
+
+int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* ion, int64_t cap_e, int64_t cap_i,
+                          double* work, int64_t* counters)
+{
+    const oracle_geom_t* g = &c->geom;
+    const int64_t nn = (int64_t)oracle_nx_nodes(g) * (g->ncy + 1);
+    double* rho_e = work;
+    double* rho_i = work + nn;
+    double* rho = work + 2 * nn;
+    double* phi = work + 3 * nn;
+    double* ex = work + 4 * nn;
+    double* ey = work + 5 * nn;
+    int64_t processed = e->n + ion->n;
+    // GATHER_ION_CHARGE_DENSITY / GATHER_ELECTRON_CHARGE_DENSITY (MainProgram:151-157)
+    deposit_threads(g, ion, c->ion_charge, rho_i, c->nthreads);
+    oracle_fold_and_wall_scale(g, rho_i);
+    deposit_threads(g, e, 1.0, rho_e, c->nthreads);
+    oracle_fold_and_wall_scale(g, rho_e);
+    for (int64_t q = 0; q < nn; ++q) rho[q] = c->factor_rho * (rho_i[q] - rho_e[q]);
+    // SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:182-191); acc_E == E for N_sub = 1
+    oracle_fftx_solve(g, rho, c->phi_bottom, c->phi_top, phi);
+    oracle_efield(g, phi, c->factor2_E, c->factor1_E, ex, ey, nullptr, nullptr);
+    // ADVANCE_ELECTRONS_PLUS (:210), then the add list left by the previous step's ionisation joins the array
+    push_threads(g, &c->e_sp, ex, ey, e, counters + 8, c->nthreads);
+    for (int64_t k = 0; k < c->pend_e.n && e->n < cap_e; ++k) {
+        double v[3] = {c->pend_e.vx[k], c->pend_e.vy[k], c->pend_e.vz[k]};
+        append(e, cap_e, c->pend_e.x[k], c->pend_e.y[k], v, c->pend_e.id[k]);
+    }
+    c->pend_e.n = 0;
+    // ADVANCE_IONS_PLUS (:231)
+    push_threads(g, &c->i_sp, ex, ey, ion, counters + 8, c->nthreads);
+    // PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:275), PERFORM_RESONANT_CHARGE_EXCHANGE (:287)
+    c->born_e.n = 0;
+    c->born_i.n = 0;
+    if (c->mcc) oracle_mcc_philox(c->mcc, &c->mcc_ctx, e, &c->born_e, &c->born_i, c->cap_born, counters);
+    if (c->rcx_on) counters[4] += oracle_rcx_philox(&c->rcx, &c->mcc_ctx, 0u, ion);
+    // PROCESS_ADDED_IONS (:300); born electrons wait in the add list for one step
+    for (int64_t k = 0; k < c->born_i.n; ++k) {
+        double v[3] = {c->born_i.vx[k], c->born_i.vy[k], c->born_i.vz[k]};
+        append(ion, cap_i, c->born_i.x[k], c->born_i.y[k], v, c->born_i.id[k]);
+    }
+    for (int64_t k = 0; k < c->born_e.n; ++k) {
+        double v[3] = {c->born_e.vx[k], c->born_e.vy[k], c->born_e.vz[k]};
+        append(&c->pend_e, c->cap_born, c->born_e.x[k], c->born_e.y[k], v, c->born_e.id[k]);
+    }
+    c->mcc_ctx.step++;
+    return processed;
+}
+
+}  // extern "C"

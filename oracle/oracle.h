@@ -1,0 +1,187 @@
+/*
+ * ORACLE (test infrastructure only): CPU FP64 restatement of EDIPIC-2D's per-step particle cycle.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load liboracle.so.
+ * The product library never links or calls it.
+ *
+ * Every function cites the reference routine it restates (paths relative to the EDIPIC-2D tree).
+ */
+#ifndef EDIPIC_ORACLE_H
+#define EDIPIC_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- random numbers (oracle_rng.c) */
+typedef struct { uint32_t v[624]; int i; } oracle_well_t;
+void   oracle_well_set_state(oracle_well_t* s, const uint32_t* words, int index);
+void   oracle_well_seed(oracle_well_t* s, int32_t seed);
+double oracle_well_next(oracle_well_t* s);
+void   oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* ---------------------------------------------------------------- geometry
+ * Node (i,j) of the reference's cluster arrays, one cluster covering the whole domain.
+ *  periodic != 0 : self-connected periodic-x cluster, nodes i = 0..ncx+1 (node ncx+1 overlaps node 1,
+ *                  node 0 overlaps node ncx), metal walls at j = 0 (object 0) and j = ncy (object 1).
+ *  periodic == 0 : walls on four sides, nodes i = 0..ncx; objects 0 below, 1 above, 2 left, 3 right.
+ *  inner objects k = 0..n_inner-1 are metal rectangles [ileft,iright]x[jbottom,jtop] (object 4+k).
+ */
+typedef struct {
+    int32_t ncx, ncy, periodic, n_inner;
+    int32_t ileft[4], jbottom[4], iright[4], jtop[4];
+} oracle_geom_t;
+
+int32_t oracle_nx_nodes(const oracle_geom_t* g);   /* ncx+2 (periodic) or ncx+1 */
+
+/* external fields and species constants (normalised as in pic2d_ExternalFields.f90:75-110) */
+typedef struct {
+    double bx, by, bz, ez;      /* B in units of B_scale, Ez in E_scale */
+    int32_t is_ion;             /* 0 electrons, 1 ions */
+    double qm2;                 /* ions: QM2s = 0.5*Qs/Ms */
+    int32_t nsub;               /* N_subcycles */
+    int32_t ions_sense_b, ions_sense_ez;
+} oracle_species_t;
+
+/* particle array in SoA FP64 form, the reference's TYPE particle split into columns */
+typedef struct {
+    int64_t n;
+    double *x, *y, *vx, *vy, *vz;
+    int32_t* tag;
+    uint32_t* id;
+} oracle_parts_t;
+
+/* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513) / ADVANCE_IONS (pic2d_IonDynamics.f90:3-524):
+ * one push of every particle with the field (EX,EY) on the node grid, wall/inner-object absorption with
+ * swap-with-last removal (REMOVE_ELECTRON :517-555) and hit counting per object. */
+void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                 oracle_parts_t* p, int64_t* hits);
+
+/* CIC deposit of GATHER_ELECTRON_CHARGE_DENSITY (pic2d_ElectronDynamics.f90:1597-1639) into rho
+ * (zeroed here), scaled by weight (ions: Qs). No fold, no wall factors. */
+void oracle_deposit(const oracle_geom_t* g, const oracle_parts_t* p, double weight, double* rho);
+/* periodic fold (:1661-1667) and wall factors (:1802-1880) */
+void oracle_fold_and_wall_scale(const oracle_geom_t* g, double* rho);
+
+/* ---------------------------------------------------------------- Maxwell sampler */
+/* PrepareMaxwellDistribIntegral (pic2d_ElectronWallCollisions.f90:835-929); v[0..9000], v_inj[0..4500] */
+void   oracle_maxwell_tables(double* v, double* v_inj);
+/* GetMaxwellVelocity (:961-985) driven by one uniform variate */
+double oracle_maxwell_sample(const double* v, double u);
+
+/* ---------------------------------------------------------------- electron-neutral collisions */
+typedef struct {
+    int32_t n_points;
+    const double* energy_eV;
+    const double* crsect_m2;
+    int32_t type;               /* 10, 11, 20, 30 */
+} oracle_crsect_t;
+
+typedef struct {
+    int32_t n_act, n_seg, n_values;
+    double seg_value[33];       /* energy_segment_boundary_value(0:n_seg) */
+    double seg_step[32];        /* energy_segment_step(1:n_seg) -> [0..n_seg-1] */
+    int32_t seg_index[33];      /* energy_segment_boundary_index(0:n_seg) */
+    double* energy_eV;          /* [n_values+1], caller-owned */
+    double* prob;               /* [(n_values+1) * n_act], prob[i*n_act + (p-1)], caller-owned */
+    double max_colliding_fraction;
+    int32_t type[8];
+    double threshold_eV[8];
+} oracle_mcc_table_t;
+
+/* frequency_of_en_collision (pic2d_enCollisionsSpecificProc.f90:4-57) */
+double oracle_en_frequency(const oracle_crsect_t* cs, double energy_eV, double n_m3, int32_t nsub, double dt_s);
+/* INITIATE_ELECTRON_NEUTRAL_COLLISIONS table part (pic2d_enCollisionsGeneralProc.f90:236-322).
+ * tab->seg_* must be set; tab->energy_eV / tab->prob must point to arrays of the right size
+ * (query the size with oracle_mcc_n_values first). */
+int32_t oracle_mcc_n_values(int32_t n_seg, const double* seg_value, const double* seg_step);
+void oracle_mcc_build(oracle_mcc_table_t* tab, int32_t n_act, const oracle_crsect_t* cs,
+                      double n_m3, int32_t nsub, double dt_s);
+/* collision kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:447-485): returns indx_coll in 1..n_act,
+ * or n_act+1 for the null collision */
+int32_t oracle_mcc_choose(const oracle_mcc_table_t* tab, double energy_eV, double r);
+
+/* scattering of en_Collision_* (pic2d_enCollisionsSpecificProc.f90:61-639) given its uniform variates.
+ * kind 10/11/20: u[0] angle, u[1] azimuth. kind 30: u[0] ejected energy, u[1..2] scattered electron angles,
+ * u[3..4] ejected electron angles, u[5..7] ion Maxwellian. Returns 1 when a new electron+ion were produced
+ * (their velocities in new_e[3], new_i[3]), 0 otherwise. v[3] is updated in place. */
+int32_t oracle_en_scatter(int32_t kind, double energy_eV, double threshold_eV, double neutral_mass_amu,
+                          double ion_velocity_factor, const double* maxwell_v, const double* u,
+                          double* v, double* new_e, double* new_i);
+
+/* Per-particle null-collision MCC driven by Philox4x32-10, the variate layout shared with the GPU kernels:
+ *   key = {id, seed_lo}, counter = {step, stream, block, seed_hi}; u = (x + 0.5) * 2^-32.
+ *   electrons, stream 0: block0 = {select, kind r, density n, -}, block1/2 = scattering variates.
+ * Ionisation products are appended to *born_e / *born_i (capacity checked). counters[k] counts kind k+1. */
+typedef struct {
+    uint64_t seed;
+    uint32_t step;
+    double energy_factor_eV;   /* m_e V_scale^2 / (2 e) */
+    double neutral_mass_amu;
+    double ion_velocity_factor;
+    const double* maxwell_v;
+} oracle_mcc_ctx_t;
+void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
+                       oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters);
+
+/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126), Philox stream 1, block0 =
+ * {hit, Mx, My, Mz}. Returns the number of exchanges. */
+typedef struct {
+    double prob_factor;        /* ngas * dt * N_subcycles */
+    double v_scale_ms;
+    double factor_eV;          /* Ms * energy_factor_eV */
+    double sigma_1eV, alpha;
+    double probab_thermal;     /* calculate_thermal_cx_probab :4-31 */
+    double vfactor;
+} oracle_rcx_t;
+double oracle_rcx_probab_thermal(double sigma_1eV, double alpha, double T_K, double n_m3, double Ms,
+                                 double dt_s, int32_t nsub);
+int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint32_t species, oracle_parts_t* ions);
+
+/* ---------------------------------------------------------------- field solvers */
+/* SOLVE_POISSON_FFTX_LINSYSY (pic2d_ElectricFieldCalc_FFT_X.f90:3-1320) for the periodic geometry:
+ * rho_total = factor_rho*(rho_i - rho_e) on the reference node grid (after fold/wall factors);
+ * phi_bottom/phi_top the metal wall potentials (normalised). Output phi on the node grid
+ * (columns ncx, ncx+1 filled with the periodic copies). */
+void oracle_fftx_solve(const oracle_geom_t* g, const double* rho_total, double phi_bottom, double phi_top, double* phi);
+
+/* CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:1324-1547) and CALCULATE_ELECTRIC_FIELD (ElectricFieldCalc_PETSc.F90:360-805):
+ * E = -grad(phi) * factor, central inside, one-sided on walls; acc += E when acc_ex != NULL. */
+void oracle_efield(const oracle_geom_t* g, const double* phi, double factor2, double factor1,
+                   double* ex, double* ey, double* acc_ex, double* acc_ey);
+
+/* The PETSc operator of SolverInitialization (pic2d_PETSc_Solver.F90:42-1350) for eps = 1 with metal walls and
+ * metal inner objects (Dirichlet identity rows) and the RHS of SOLVE_POTENTIAL_WITH_PETSC
+ * (ElectricFieldCalc_PETSc.F90:38-186), solved in FP64 by CG on the Dirichlet-eliminated SPD system.
+ * phi holds the initial guess on entry (node grid); returns iterations, or -1 if not converged. */
+int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho_total, const double* wall_phi /*4*/,
+                        const double* inner_phi, double rtol, int32_t max_it, double* phi, double* relres_out);
+
+/* ---------------------------------------------------------------- whole cycle (CPU baseline) */
+typedef struct {
+    oracle_geom_t geom;
+    oracle_species_t e_sp, i_sp;
+    double factor_rho;          /* 1/N_of_particles_cell */
+    double ion_charge;          /* Qs */
+    double factor2_E, factor1_E;
+    double phi_bottom, phi_top;
+    const oracle_mcc_table_t* mcc;
+    oracle_mcc_ctx_t mcc_ctx;
+    oracle_rcx_t rcx;
+    int32_t rcx_on;
+    int32_t nthreads;
+    /* electrons born by ionisation wait one step in an add list before they join the main array
+       (they are appended by PROCESS_ADDED_ELECTRONS of the next step, pic2d_MainProgram.f90:259/:316) */
+    oracle_parts_t pend_e, born_e, born_i;
+    int64_t cap_born;
+} oracle_cycle_t;
+
+/* one electron+ion step with N_subcycles == 1 in the order of pic2d_MainProgram.f90:151-309:
+ * gather densities, FFT_X solve, E, push electrons, push ions, MCC, RCX, append born particles.
+ * Particle arrays must have room for the appended particles (cap). Returns particles processed. */
+int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* i, int64_t cap_e, int64_t cap_i,
+                          double* work /* 7 * node grid */, int64_t* counters /* [16] */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
