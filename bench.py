@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Throughput of EDIPIC-2D's per-step particle cycle (push + MCC + deposit, with the FFT_X field solve) on B200.
+
+Workload (default): the 1024x1024-cell periodic-x plasma with 200 electrons and 200 Ar+ per cell
+(419,430,400 particles), B = 10 mT at 30 degrees in plane, e-Ar (elastic, excitation, ionisation) and Ar+-Ar
+charge exchange, N_subcycles = 1, mixed precision (int32 cell + FP32 offsets/velocities, int64 fixed-point
+deposit), tile sort every 20 steps. Synthetic deck and initial plasma (no dataset is involved).
+
+One step = one pass of MainProg's cycle (pic2d_MainProgram.f90:151-309): density, FFT_X solve and E, electron
+push+deposit+MCC, ion push+deposit+RCX, appends. value = (electrons + ions) * steps / device time of the timed
+steps (CUDA events on the library's stream). e2e = the same steps driven through the C ABI in the call order
+a Fortran host uses, with the per-step host reads of the collision counters.
+
+--impl reference times the CPU restatement of the reference routines (the oracle: the reference's Fortran
+cannot be built in this image) on the host cores, on a bounded sample of the same workload.
+Multi-GPU (torchrun): independent replicas, one per GPU (weak scaling), device time max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "edipic-2d_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "particle-steps/s (push+MCC+deposit); Poisson ms/step learned vs plain, 1×B200"
+BYTES_PER_PARTICLE_STEP = {"mixed": 52, "fp64": 84}
+
+
+def workload_desc(args):
+    return (f"{args.config}: {args.cells_x}x{args.cells_y} cells, {args.ppc} e- + {args.ppc} Ar+ per cell, "
+            f"{'B 10 mT at 30 deg, ' if args.config == 'cfg1' else ''}e-Ar MCC + Ar+-Ar RCX, FFT_X, "
+            f"{args.precision} precision, sort every {args.sort_every}")
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, n in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(args, deck_dir, seconds=15.0):
+    """The oracle's cycle (FP64, OpenMP on all host threads) on a bounded sample of the workload: the same
+    physics and particles per cell on a smaller periodic grid, stepped for about `seconds`."""
+    import numpy as np
+
+    import pyoracle
+    from edipic_b200 import decks, read_deck
+    ncx, ncy = 128, 64
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.write_deck(tmp, args.config, ncx=ncx, ncy=ncy, ppc=args.ppc)
+        dk = read_deck(d)
+        p, t = dk.params, dk.tables
+        rng = np.random.default_rng(0)
+        n = ncx * ncy * args.ppc
+        x = rng.uniform(0, ncx, n)
+        y = rng.uniform(0, ncy, n)
+        ve = rng.normal(0, np.sqrt(2.0 / dk.t_e_ev / 2.0) / dk.n_max_vel, (3, n))
+        vi = rng.normal(0, np.sqrt(0.03 / dk.t_e_ev / 2.0 / p.ion_mass_me[0]) / dk.n_max_vel, (3, n))
+        threads = os.cpu_count() or 1
+        oc = pyoracle.OracleCycle(d, p, t, (x, y, ve[0], ve[1], ve[2]), (x, y, vi[0], vi[1], vi[2]), seed=1,
+                                  nthreads=threads)
+        oc.step(1)
+        done, steps, t0 = 0, 0, time.perf_counter()
+        while True:
+            done += oc.step(1)
+            steps += 1
+            el = time.perf_counter() - t0
+            if el > seconds or steps >= 200:
+                break
+    return {"value": done / el, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{ncx}x{ncy} cells x {args.ppc}+{args.ppc} per cell ({2 * n} particles), {steps} steps, "
+                      f"{el:.1f} s, FP64 oracle cycle incl. FFT_X"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from edipic_b200 import decks
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc)
+        cb = cpu_baseline(args, d, seconds=30.0)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(args), "reference_arm": "CPU restatement of the reference routines "
+                       "(the reference's Fortran/MPI/PETSc cannot be built in this image)"},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation, decks
+    tmp = tempfile.mkdtemp(prefix=f"edp_bench_{rank}_")
+    d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc, seed=rank)
+    prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    sim = Simulation(d, precision=prec, sort_every=args.sort_every, fuse_collisions=True, seed=1000 + rank)
+    lib, ctx = sim.lib, sim.ctx
+    sim.distribute_particles(args.ppc)
+    sptr = C.c_void_p()
+    lib.edp_get_stream(ctx, C.byref(sptr))
+    stream = torch.cuda.ExternalStream(sptr.value)
+    chk = sim._check
+
+    def step_plain(ev=None):
+        t = sim.counters_cache_t if hasattr(sim, "counters_cache_t") else 0
+        chk(lib.edp_update_wall_potentials(ctx, t), "wall")
+        if ev:
+            ev[0].record(stream)
+        chk(lib.edp_field_fftx(ctx, None), "fftx")
+        if ev:
+            ev[1].record(stream)
+        chk(lib.edp_advance_electrons(ctx), "adv_e")
+        chk(lib.edp_advance_ions(ctx), "adv_i")
+        if ev:
+            ev[2].record(stream)
+        chk(lib.edp_collide_en(ctx, None), "en")
+        chk(lib.edp_collide_rcx(ctx, None), "rcx")
+        chk(lib.edp_end_ion_cycle(ctx), "end")
+        sim.counters_cache_t = t + 1
+
+    for _ in range(args.warmup):
+        step_plain()
+    c0 = sim.counters()
+    n0 = c0.n_particles[0] + c0.n_particles[1]
+    launches0 = c0.kernel_launches
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local if world > 1 else 0)
+    clocks.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(args.steps):
+        step_plain(evs[k])
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    c1 = sim.counters()
+    n1 = c1.n_particles[0] + c1.n_particles[1]
+    launches = c1.kernel_launches - launches0
+    t_total = start.elapsed_time(end) / 1e3
+    t_field = sum(e[0].elapsed_time(e[1]) for e in evs) / 1e3
+    t_push = sum(e[1].elapsed_time(e[2]) for e in evs) / 1e3
+    if dist:
+        tt = torch.tensor([t_total, t_field, t_push], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total, t_field, t_push = tt.tolist()
+        cnt = torch.tensor([float(n0 + n1)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(cnt)
+        nsum = cnt.item()
+    else:
+        nsum = float(n0 + n1)
+    particle_steps = 0.5 * nsum * args.steps
+    value = particle_steps / t_total
+
+    # end to end: the drop-in call order of a Fortran host (pic2d_MainProgram.f90:151-309) with its per-step reads
+    e2e_steps = max(2, min(args.steps, 10))
+    cnt_buf = (C.c_int64 * 8)()
+    rcx_buf = C.c_int64()
+    rho_host = None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es.record(stream)
+    for _ in range(e2e_steps):
+        t = sim.counters_cache_t
+        chk(lib.edp_gather_charge_density(ctx, IONS, rho_host), "gi")
+        chk(lib.edp_gather_charge_density(ctx, ELECTRONS, rho_host), "ge")
+        chk(lib.edp_update_wall_potentials(ctx, t), "wall")
+        chk(lib.edp_field_fftx(ctx, None), "fftx")
+        chk(lib.edp_advance_electrons(ctx), "adv_e")
+        chk(lib.edp_advance_ions(ctx), "adv_i")
+        chk(lib.edp_collide_en(ctx, cnt_buf), "en")
+        chk(lib.edp_collide_rcx(ctx, C.byref(rcx_buf)), "rcx")
+        chk(lib.edp_end_ion_cycle(ctx), "end")
+        sim.counters_cache_t = t + 1
+    ee.record(stream)
+    ee.synchronize()
+    t_e2e = es.elapsed_time(ee) / 1e3
+    c2 = sim.counters()
+    n2 = c2.n_particles[0] + c2.n_particles[1]
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = tt.item()
+        cnt = torch.tensor([float(n1 + n2)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(cnt)
+        ne2e = cnt.item()
+    else:
+        ne2e = float(n1 + n2)
+    e2e = 0.5 * ne2e * e2e_steps / t_e2e
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        bpp = BYTES_PER_PARTICLE_STEP[args.precision]
+        per_gpu_particles = 0.5 * (n0 + n1)
+        achieved = per_gpu_particles * bpp * args.steps / t_push / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "push_traffic.json")) as f:
+                tr = json.load(f)
+            traffic = tr["dram_bytes_per_particle"][args.precision] * per_gpu_particles
+        except Exception:
+            pass
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 particles / i64 fixed-point density / f64 field" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": workload_desc(args), "cells": [args.cells_x, args.cells_y],
+                       "particles_per_gpu": int(per_gpu_particles), "parallelism": f"replicas x{world}",
+                       "l2": "particle arrays (>10 GB) exceed L2 each step"},
+            "poisson_ms_per_step": 1e3 * t_field / args.steps,
+            "push_ms_per_step": 1e3 * t_push / args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "basis": f"{bpp} B/particle-step algorithmic, electron+ion push kernels "
+                                  f"(push+deposit+collisions), peak {peak_kind}"},
+            "clocks": clk, "gpu_launches": int(launches),
+            "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * 8 + 8,
+                    "path": "C ABI call sequence of the Fortran host with per-step counter reads"},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(args, d)
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="cfg1")
+    ap.add_argument("--cells", type=int, nargs=2, default=None, metavar=("NX", "NY"))
+    ap.add_argument("--ppc", type=int, default=None)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--sort-every", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    from edipic_b200 import decks
+    cfg = decks.CONFIGS[args.config]
+    args.cells_x, args.cells_y = args.cells if args.cells else (cfg["ncx"], cfg["ncy"])
+    args.ppc = args.ppc or cfg["ppc"]
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

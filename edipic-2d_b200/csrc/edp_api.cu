@@ -471,6 +471,7 @@ int after_particles_changed(edp_ctx* c, int sp)
     // live count, then the initial sort and the deposit the first field solve needs
     c->hc->n_live[sp] = 0;
     EDP_CUDA(c, cudaMemsetAsync(&c->dc->n_live[sp], 0, sizeof(unsigned long long), c->stream));
+    ++c->launches;
     count_live_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->kp, c->p.precision, c->pm[sp], c->pd[sp],
                                                                           c->host_slots[sp], &c->dc->n_live[sp]);
     EDP_CUDA(c, cudaGetLastError());
@@ -487,6 +488,7 @@ int after_particles_changed(edp_ctx* c, int sp)
 
 int edp_launch_deposit(edp_ctx* c, int sp)
 {
+    ++c->launches;
     if (c->p.precision == EDP_PREC_MIXED)
         deposit_mixed_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->kp, c->pm[sp], &c->dc->n_slots[sp],
                                                                                  c->rho_fix[sp]);
@@ -668,6 +670,13 @@ int edp_set_sync(edp_ctx* c, int sync)
     return EDP_OK;
 }
 
+int edp_get_stream(edp_ctx* c, void** out)
+{
+    if (!c || !out) return EDP_ERR_ARG;
+    *out = (void*)c->stream;
+    return EDP_OK;
+}
+
 int edp_synchronize(edp_ctx* c)
 {
     if (!c) return EDP_ERR_ARG;
@@ -694,6 +703,7 @@ int edp_upload_particles(edp_ctx* c, int sp, int64_t n, const double* x, const d
         if (n) EDP_CUDA(c, cudaMemcpyAsync(dbuf + q * nn, cols[q], n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if (tag && n) EDP_CUDA(c, cudaMemcpyAsync(tbuf, tag, n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
     if (id && n) EDP_CUDA(c, cudaMemcpyAsync(ibuf, id, n * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+        ++c->launches;
     if (n)
         upload_kernel<<<grid_of(n), 256, 0, c->stream>>>(c->kp, c->p.precision, n, 0, dbuf, dbuf + nn, dbuf + 2 * nn,
                                                          dbuf + 3 * nn, dbuf + 4 * nn, tag ? tbuf : nullptr,
@@ -728,6 +738,7 @@ int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv,
         return edp_fail(c, EDP_ERR_STATE, "ions copy electron positions: same per_cell, before the electron sort");
     TRY(alloc_species(c, sp, n));
     const int64_t base_id = 0;
+    ++c->launches;
     distribute_kernel<<<grid_of(n, 148 * 64), 256, 0, c->stream>>>(
         c->kp, c->p.precision, sp, per_cell, fconv, zero_vz, copy_pos, c->maxwell_v, c->tab.maxwell_rmax, base_id,
         c->pm[sp], c->pd[sp], c->pm[0], c->pd[0], n);
@@ -740,6 +751,7 @@ int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv,
     if (sp == 0 && copy_pos == 0) {
         c->hc->n_live[sp] = 0;
         EDP_CUDA(c, cudaMemsetAsync(&c->dc->n_live[sp], 0, sizeof(unsigned long long), c->stream));
+        ++c->launches;
         count_live_kernel<<<grid_of(n), 256, 0, c->stream>>>(c->kp, c->p.precision, c->pm[sp], c->pd[sp], n,
                                                              &c->dc->n_live[sp]);
         TRY(zero_density(c, sp));
@@ -837,8 +849,10 @@ int edp_gather_charge_density(edp_ctx* c, int sp, double* rho_out)
     EDP_CUDA(c, cudaMalloc(&tmp, (int64_t)c->kp.nxg * c->kp.nyg * sizeof(double)));
     EDP_CUDA(c, cudaMalloc(&ref, nref * sizeof(double)));
     double wgt = sp == 0 ? 1.0 : (double)c->p.ion_charge[sp - 1];
+    ++c->launches;
     species_density_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, c->p.precision, c->rho_fix[sp], c->rho_d[sp],
                                                                   wgt, tmp);
+    ++c->launches;
     expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, tmp, nullptr, 0, ref, w);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemcpyAsync(rho_out, ref, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -886,6 +900,7 @@ int edp_advance_electrons(edp_ctx* c)
     if (!c->uploaded[0]) return edp_fail(c, EDP_ERR_STATE, "electrons not uploaded");
     const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
     const bool fuse = c->p.fuse_collisions != 0;
+    ++c->launches;
     reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
     TRY(zero_density(c, 0));
     TRY(edp_launch_push(c, 0, ion_step, fuse));
@@ -944,6 +959,7 @@ int edp_end_ion_cycle(edp_ctx* c)
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
     if (ion_step) {
         TRY(edp_launch_append_born_ions(c));
+        ++c->launches;
         reset_born_ions_kernel<<<1, 1, 0, c->stream>>>(c->dc);
         if (c->p.precision == EDP_PREC_MIXED) {
             EDP_CUDA(c, cudaMemsetAsync(c->acc2, 0, nn * sizeof(float2), c->stream));
@@ -955,6 +971,7 @@ int edp_end_ion_cycle(edp_ctx* c)
     } else {
         c->n_sub_phase++;
     }
+    ++c->launches;
     rotate_pending_kernel<<<1, 1, 0, c->stream>>>(c->dc, c->p.n_ion_species);
     EDP_CUDA(c, cudaGetLastError());
     c->pend_cur ^= 1;
@@ -1010,6 +1027,7 @@ int edp_query_counters(edp_ctx* c, edp_counters* out)
     out->cg_iterations = c->last_cg_iters;
     out->cg_relres = c->last_cg_relres;
     out->error_flags = (int32_t)c->hc->error_flags;
+    out->kernel_launches = c->launches;
     for (int s = 0; s < c->nspec; ++s) c->host_slots[s] = std::max<int64_t>((int64_t)c->hc->n_slots[s], 0);
     if (c->hc->error_flags & EDP_EFLAG_CAPACITY) return edp_fail(c, EDP_ERR_CAPACITY, "particle capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
@@ -1025,6 +1043,7 @@ int edp_get_field(edp_ctx* c, int which, double* out)
     double* ref = nullptr;
     EDP_CUDA(c, cudaMalloc(&ref, nref * sizeof(double)));
     const bool mixed = c->p.precision == EDP_PREC_MIXED;
+    ++c->launches;
     switch (which) {
     case EDP_FIELD_EX: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->Ex, c->E2, 0, ref, w); break;
     case EDP_FIELD_EY: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->Ey, c->E2, 1, ref, w); break;
@@ -1051,6 +1070,7 @@ int edp_set_field(edp_ctx* c, int which, const double* in)
     EDP_CUDA(c, cudaMemcpyAsync(ref, in, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     const bool mixed = c->p.precision == EDP_PREC_MIXED;
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    ++c->launches;
     switch (which) {
     case EDP_FIELD_EX: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->Ex, c->E2, 0); break;
     case EDP_FIELD_EY: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->Ey, c->E2, 1); break;
@@ -1072,6 +1092,7 @@ int edp_moments(edp_ctx* c, int sp, double out[7])
     double* d = nullptr;
     EDP_CUDA(c, cudaMalloc(&d, 7 * sizeof(double)));
     EDP_CUDA(c, cudaMemsetAsync(d, 0, 7 * sizeof(double), c->stream));
+    ++c->launches;
     moments_kernel<<<grid_of(c->host_slots[sp]), 256, 0, c->stream>>>(c->p.precision, c->pm[sp], c->pd[sp],
                                                                        &c->dc->n_slots[sp], d);
     EDP_CUDA(c, cudaGetLastError());
@@ -1093,6 +1114,7 @@ int edp_mcc_choose(edp_ctx* c, int64_t n, const double* E, const double* r, int3
     EDP_CUDA(c, cudaMalloc(&dout, n * sizeof(int32_t)));
     EDP_CUDA(c, cudaMemcpyAsync(dE, E, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     EDP_CUDA(c, cudaMemcpyAsync(dr, r, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ++c->launches;
     mcc_choose_kernel<<<grid_of(n), 256, 0, c->stream>>>(edp_make_mcc_dev(c), n, dE, dr, dout);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemcpyAsync(out, dout, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));

@@ -147,6 +147,7 @@ struct edp_ctx {
     double K[EDP_MAX_SPECIES][9];
     void* dev_small = nullptr;        // 4 KB device block for kernel pointer tables
     double phi_wall[4];               // current wall potentials (normalised)
+    int64_t launches = 0;             // kernels launched (reported by edp_query_counters)
 };
 
 // ------------------------------------------------------------------------------------------ Philox

@@ -353,6 +353,7 @@ int edp_launch_density(edp_ctx* c)
     static_assert(sizeof(Ptrs) <= 4096, "pointer table");
     Ptrs* d = reinterpret_cast<Ptrs*>(c->dev_small);
     EDP_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    ++c->launches;
     density_kernel<<<grid_nodes(c->kp), 256, 0, c->stream>>>(c->kp, c->p.precision, c->p.n_ion_species, d->f, d->d,
                                                              d->qs, 1.0 / c->p.n_of_particles_cell, c->rho_total);
     EDP_CUDA(c, cudaGetLastError());
@@ -366,9 +367,12 @@ int edp_launch_fftx(edp_ctx* c)
     while ((1 << logn) < N) ++logn;
     size_t smem = (size_t)N * sizeof(double2);
     int thr = std::min(512, std::max(32, N / 2));
+    ++c->launches;
     fftx_forward<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->rho_total, c->phi_wall[0], c->phi_wall[1], c->twiddle,
                                                      logn, c->nm, c->spec);
+    ++c->launches;
     fftx_thomas<<<(c->nm + 127) / 128, 128, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);
+    ++c->launches;
     fftx_inverse<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->spec, c->twiddle, logn, c->nm, c->phi);
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
@@ -378,6 +382,7 @@ int edp_launch_efield(edp_ctx* c)
 {
     const double f2 = c->p.f_scale_v / (c->p.e_scale_vm * 2.0 * c->p.delta_x_m);
     const double f1 = c->p.f_scale_v / (c->p.e_scale_vm * c->p.delta_x_m);
+    ++c->launches;
     efield_kernel<<<grid_nodes(c->kp), 256, 0, c->stream>>>(c->kp, c->phi, f2, f1, c->p.precision, c->E2, c->acc2,
                                                             c->Ex, c->Ey, c->accx, c->accy);
     EDP_CUDA(c, cudaGetLastError());
@@ -397,7 +402,9 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
     const unsigned gr = grid_nodes(kp);
     const double* x0 = (warm == EDP_WARM_PREVIOUS || warm == EDP_WARM_USER) ? c->phi : nullptr;
+    ++c->launches;
     cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, x0 ? x0 : c->phi, c->cg_kind, c->phi, c->cg_b, scal);
+    ++c->launches;
     cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
     double h[2];
     EDP_CUDA(c, cudaMemcpyAsync(h, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -413,8 +420,11 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
             double* rr = &scal[1 + 2 * it];
             double* pAp = &scal[2 + 2 * it];
             double* rrn = &scal[1 + 2 * (it + 1)];
+            ++c->launches;
             cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp);
+            ++c->launches;
             cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r, rrn);
+            ++c->launches;
             cg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, rrn, c->cg_r, c->cg_p);
         }
         EDP_CUDA(c, cudaMemcpyAsync(h, &scal[1 + 2 * it], sizeof(double), cudaMemcpyDeviceToHost, c->stream));

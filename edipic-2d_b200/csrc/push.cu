@@ -769,6 +769,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.tail_ctas = (tail + per_cta - 1) / per_cta;
         if (a.tail_ctas < 1) a.tail_ctas = 1;
         int64_t grid = a.n_chunks + a.tail_ctas;
+        ++c->launches;
         push_mixed_kernel<<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
     } else {
         PushArgs64 a;
@@ -798,6 +799,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         int64_t grid = (n + 255) / 256;
         if (grid > 148 * 64) grid = 148 * 64;
         if (grid < 1) grid = 1;
+        ++c->launches;
         push_fp64_kernel<<<(unsigned)grid, 256, 0, c->stream>>>(a);
     }
     EDP_CUDA(c, cudaGetLastError());
@@ -834,6 +836,7 @@ int edp_launch_collide_en(edp_ctx* c)
     if (!c->tab.en_on) return EDP_OK;
     CollArgs a = coll_args(c, 0);
     a.mcc = edp_make_mcc_dev(c);
+    ++c->launches;
     collide_en_kernel<<<grid_for(c->host_slots[0]), 256, 0, c->stream>>>(a);
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
@@ -845,6 +848,7 @@ int edp_launch_collide_rcx(edp_ctx* c)
         if (!c->tab.rcx_on[s]) continue;
         CollArgs a = coll_args(c, 1 + s);
         a.rcx = edp_make_rcx_dev(c, s);
+        ++c->launches;
         collide_rcx_kernel<<<grid_for(c->host_slots[1 + s]), 256, 0, c->stream>>>(a);
         EDP_CUDA(c, cudaGetLastError());
     }
@@ -883,6 +887,7 @@ int edp_launch_append_pending(edp_ctx* c, bool ion_step)
     if (a.do_mcc) a.mcc = edp_make_mcc_dev(c);
     // electrons born from these go to the list being filled this step, counted in pend_e_count[0]
     a.pend_next = c->pend_e[cur ^ 1];
+    ++c->launches;
     append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
     EDP_CUDA(c, cudaGetLastError());
     c->host_slots[0] += c->born_cap;
@@ -895,6 +900,7 @@ int edp_launch_append_born_ions(edp_ctx* c)
         AppendArgs a = append_args(c, 1 + s);
         a.src = c->born_i[s];
         a.src_count = &c->dc->born_i_count[s];
+        ++c->launches;
         append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
         EDP_CUDA(c, cudaGetLastError());
         c->host_slots[1 + s] += c->born_cap;

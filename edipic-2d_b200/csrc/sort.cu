@@ -127,18 +127,26 @@ int edp_launch_sort(edp_ctx* c, int sp)
     const int64_t nslots = std::max<int64_t>(c->host_slots[sp], 1);
     unsigned grid = (unsigned)std::min<int64_t>((nslots + 255) / 256, 148 * 16);
     EDP_CUDA(c, cudaMemsetAsync(c->sort_count, 0, nkeys * sizeof(uint32_t), c->stream));
+    ++c->launches;
     hist_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp].cell, &c->dc->n_slots[sp], c->ntx, c->sort_count);
     const int64_t nb = (nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK;
     unsigned long long* bsum = c->scan_tmp;
     unsigned long long* total = c->scan_tmp + nb;
     unsigned long long* cursor = c->scan_tmp + nb + 1;
     unsigned long long* starts = cursor + nkeys;
+    ++c->launches;
     scan_local<<<(unsigned)nb, 256, 0, c->stream>>>(c->sort_count, c->sort_offset, bsum, nkeys);
+    ++c->launches;
     scan_sums<<<1, 32, 0, c->stream>>>(bsum, nb, total);
+    ++c->launches;
     scan_add<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, bsum, nkeys);
+    ++c->launches;
     copy_u64<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(cursor, c->sort_offset, nkeys);
+    ++c->launches;
     scatter_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp], c->pm_alt[sp], &c->dc->n_slots[sp], c->ntx, cursor);
+    ++c->launches;
     tile_starts<<<(unsigned)((ntiles + 1 + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, ntiles, total, starts);
+    ++c->launches;
     set_slots<<<1, 1, 0, c->stream>>>(&c->dc->n_slots[sp], &c->dc->n_live[sp], total);
     EDP_CUDA(c, cudaGetLastError());
     std::swap(c->pm[sp], c->pm_alt[sp]);

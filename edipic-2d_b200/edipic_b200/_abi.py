@@ -70,7 +70,7 @@ class Counters(C.Structure):
         ("n_particles", C.c_int64 * MAX_SPECIES), ("electron_hits", C.c_int64 * N_HIT),
         ("ion_hits", C.c_int64 * N_HIT), ("en_collisions", C.c_int64 * MAX_COLPROC),
         ("rcx_collisions", C.c_int64 * MAX_ION), ("step", C.c_int64), ("cg_iterations", C.c_int32),
-        ("cg_relres", C.c_double), ("error_flags", C.c_int32),
+        ("cg_relres", C.c_double), ("error_flags", C.c_int32), ("kernel_launches", C.c_int64),
     ]
 
 
@@ -87,6 +87,7 @@ SIGNATURES = {
     "edp_last_error": [_CTX, C.c_char_p, C.c_size_t],
     "edp_set_sync": [_CTX, C.c_int],
     "edp_synchronize": [_CTX],
+    "edp_get_stream": [_CTX, P(C.c_void_p)],
     "edp_upload_particles": [_CTX, C.c_int, C.c_int64, _D, _D, _D, _D, _D, _I32, _U32],
     "edp_download_particles": [_CTX, C.c_int, C.c_int64, _I64, _D, _D, _D, _D, _D, _I32, _U32],
     "edp_distribute_particles": [_CTX, C.c_int, C.c_int32, C.c_double, C.c_int32, C.c_int32],

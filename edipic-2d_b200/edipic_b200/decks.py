@@ -56,7 +56,7 @@ def _segments():
 
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
-               collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None):
+               collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21):
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -173,7 +173,7 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
     w("init_neutrals.dat", [
         "----------dd--- number of neutral species", f"          {1:2d}",
         "------AAAAAA--- neutral gas code", "      Argon0",
-        "--#d.dddE#dd--- density [m^-3]", f"  {3.2e21:10.3E}",
+        "--#d.dddE#dd--- density [m^-3]", f"  {n_gas:10.3E}",
         "-----ddddd.d--- temperature [K]", f"     {t_gas_k:7.1f}",
     ])
     e0, segs = _segments()

@@ -133,6 +133,7 @@ typedef struct edp_counters {
     int32_t cg_iterations;                                  /* last CG solve */
     double cg_relres;
     int32_t error_flags;                                    /* device error word (bit set per EDP_ERR_*) */
+    int64_t kernel_launches;                                /* kernels this context launched so far */
 } edp_counters;
 
 typedef struct edp_ctx edp_ctx;
@@ -145,6 +146,8 @@ int edp_destroy(edp_ctx* ctx);
 int edp_last_error(const edp_ctx* ctx, char* buf, size_t len);
 int edp_set_sync(edp_ctx* ctx, int sync);
 int edp_synchronize(edp_ctx* ctx);
+/* the context's CUDA stream (a cudaStream_t), e.g. to record timing events on it */
+int edp_get_stream(edp_ctx* ctx, void** stream_out);
 
 /* ---- particles ----------------------------------------------------------------------------------- */
 /* after DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325) or a checkpoint read: the host's

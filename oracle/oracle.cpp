@@ -528,11 +528,11 @@ static void append(oracle_parts_t* p, int64_t cap, double x, double y, const dou
 
 // PERFORM_ELECTRON_NEUTRAL_COLLISIONS :332-485 with a per-particle Bernoulli(P_max) selection in place of the
 // binary-tree draw of floor(P_max N) distinct particles; kind choice and scattering as in the reference.
-void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
-                       oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters)
+static void mcc_range(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e, int64_t lo,
+                      int64_t hi, std::vector<double>* out, int64_t* counters)
 {
     const double pmax = tab->max_colliding_fraction;
-    for (int64_t k = 0; k < e->n; ++k) {
+    for (int64_t k = lo; k < hi; ++k) {
         uint32_t b0[4];
         philox_block(e->id[k], c->seed, c->step, 0u, 0u, b0);
         if (!(uniform(b0[0]) < pmax)) continue;
@@ -558,8 +558,38 @@ void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c,
         e->vz[k] = v[2];
         counters[kind_index - 1]++;
         if (born) {
-            append(born_e, cap_born, e->x[k], e->y[k], ne, 0u);
-            append(born_i, cap_born, e->x[k], e->y[k], ni, 0u);
+            double rec[8] = {e->x[k], e->y[k], ne[0], ne[1], ne[2], ni[0], ni[1], ni[2]};
+            out->insert(out->end(), rec, rec + 8);
+        }
+    }
+}
+
+// Per-particle null-collision MCC; thread slices keep their ionisation products in order, so the add lists are
+// the same as in a serial pass.
+void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
+                       oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters)
+{
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    std::vector<std::vector<double>> born(nt);
+    std::vector<std::vector<int64_t>> cnt(nt, std::vector<int64_t>(8, 0));
+#pragma omp parallel num_threads(nt)
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        int64_t lo = e->n * t / nt, hi = e->n * (t + 1) / nt;
+        mcc_range(tab, c, e, lo, hi, &born[t], cnt[t].data());
+    }
+    for (int t = 0; t < nt; ++t) {
+        for (int q = 0; q < 8; ++q) counters[q] += cnt[t][q];
+        for (size_t r = 0; r < born[t].size(); r += 8) {
+            const double* b = &born[t][r];
+            append(born_e, cap_born, b[0], b[1], b + 2, 0u);
+            append(born_i, cap_born, b[0], b[1], b + 5, 0u);
         }
     }
 }
@@ -583,6 +613,7 @@ int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint
 {
     int64_t count = 0;
     double pt2 = r->probab_thermal * r->probab_thermal;
+#pragma omp parallel for reduction(+ : count) schedule(static)
     for (int64_t k = 0; k < ions->n; ++k) {
         double vx = ions->vx[k], vy = ions->vy[k], vz = ions->vz[k];
         double vsq = vx * vx + vy * vy + vz * vz;
@@ -901,6 +932,9 @@ int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* 
 {
     const oracle_geom_t* g = &c->geom;
     const int64_t nn = (int64_t)oracle_nx_nodes(g) * (g->ncy + 1);
+#ifdef _OPENMP
+    omp_set_num_threads(c->nthreads > 0 ? c->nthreads : 1);
+#endif
     double* rho_e = work;
     double* rho_i = work + nn;
     double* rho = work + 2 * nn;

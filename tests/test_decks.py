@@ -1,0 +1,99 @@
+"""The product's deck reader (edp_deck_read, C++) against the oracle's independent reading of the same files:
+normalisation, geometry and the e-n collision probability table (bit for bit), RCX constants and the Maxwell
+table. Runs without a GPU."""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle
+from edipic_b200 import decks, read_deck
+
+REFERENCE = "/root/reference"
+
+
+@pytest.fixture(scope="module", params=["cfg0", "cfg1", "cfg2", "cfg4"])
+def deck(request, tmp_path_factory):
+    d = decks.write_deck(str(tmp_path_factory.mktemp(request.param)), request.param)
+    return request.param, d, read_deck(d)
+
+
+def test_normalisation(deck):
+    name, _d, dk = deck
+    p = dk.params
+    assert math.isclose(p.delta_x_m, 1e-4, rel_tol=1e-6)
+    assert math.isclose(p.delta_t_s, decks.CONFIGS[name]["dt"], rel_tol=1e-4)
+    assert p.ncx == decks.CONFIGS[name]["ncx"] and p.ncy == decks.CONFIGS[name]["ncy"]
+    assert p.periodic_x == (1 if decks.CONFIGS[name]["periodic"] else 0)
+    # E_scale = m_e V_scale/(e dt), B_scale = m_e/(e dt), F_scale = e N dx^2/eps0 (pic2d_CurProblemValues.f90:893-900)
+    assert math.isclose(p.b_scale_t, 9.109534e-31 / (1.602189e-19 * p.delta_t_s), rel_tol=1e-12)
+    assert math.isclose(p.e_scale_vm, p.b_scale_t * p.v_scale_ms, rel_tol=1e-12)
+
+
+def test_mcc_table_matches_oracle_bitwise(deck):
+    _name, d, dk = deck
+    t, p = dk.tables, dk.params
+    neu = pyoracle.read_neutral_deck(d)
+    ot = pyoracle.MccTables(neu, p.n_subcycles, p.delta_t_s)
+    assert t.en_on == 1 and t.n_act == ot.t.n_act == 3
+    assert t.n_values == ot.t.n_values
+    assert t.max_colliding_fraction == ot.t.max_colliding_fraction
+    nv = t.n_values
+    e = np.ctypeslib.as_array(t.energy_eV, shape=(nv + 1,))
+    pr = np.ctypeslib.as_array(t.prob, shape=((nv + 1) * t.n_act,))
+    assert np.array_equal(e, ot.energy)
+    assert np.array_equal(pr, ot.prob)
+    assert [t.seg_index[i] for i in range(t.n_seg + 1)] == [ot.t.seg_index[i] for i in range(t.n_seg + 1)]
+    assert [t.threshold_eV[i] for i in range(3)] == [0.0, 11.55, 15.76]
+    # cumulative, normalised, non-decreasing (:300-322)
+    P = pr.reshape(nv + 1, 3)
+    assert np.all(np.diff(P, axis=1) >= 0) and P.max() == 1.0 and P.min() >= 0.0
+
+
+def test_rcx_and_maxwell_match_oracle(deck):
+    _name, d, dk = deck
+    t, p = dk.tables, dk.params
+    neu = pyoracle.read_neutral_deck(d)
+    pt = pyoracle.lib().oracle_rcx_probab_thermal(5.0e-19, 0.0, neu["t_k"], neu["n_m3"], p.ion_mass_me[0],
+                                                  p.delta_t_s, p.n_subcycles)
+    assert t.rcx_on[0] == 1
+    assert math.isclose(t.rcx_probab_thermal[0], pt, rel_tol=1e-13)
+    v, _vi = pyoracle.maxwell_tables()
+    mv = np.ctypeslib.as_array(t.maxwell_v, shape=(t.maxwell_rmax + 1,))
+    assert np.array_equal(mv, v)
+
+
+def test_missing_deck_is_an_io_error(tmp_path):
+    from edipic_b200 import EdpError
+    with pytest.raises(EdpError) as e:
+        read_deck(str(tmp_path))
+    assert e.value.code == -8
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference example decks not present")
+def test_reference_example_decks_parse_or_are_rejected_cleanly():
+    """The reference's own example decks: the supported subset (metal/periodic walls, metal inner objects) parses;
+    decks with dielectric walls or vacuum gaps are rejected with EDP_ERR_IO rather than misread."""
+    from edipic_b200 import EdpError
+    seen = 0
+    for name in sorted(os.listdir(REFERENCE)):
+        d = os.path.join(REFERENCE, name)
+        if not (name.startswith("input_data") and os.path.isdir(d)):
+            continue
+        seen += 1
+        try:
+            dk = read_deck(d)
+        except EdpError as e:
+            assert e.code == -8
+            continue
+        p = dk.params
+        assert p.ncx > 0 and p.ncy > 0 and p.delta_t_s > 0
+        if dk.tables.en_on:
+            neu = pyoracle.read_neutral_deck(d)
+            ot = pyoracle.MccTables(neu, p.n_subcycles, p.delta_t_s)
+            nv = dk.tables.n_values
+            pr = np.ctypeslib.as_array(dk.tables.prob, shape=((nv + 1) * dk.tables.n_act,))
+            assert np.array_equal(pr, ot.prob), name
+    assert seen == 11

@@ -1,0 +1,94 @@
+"""Whole steps of the cycle (MainProg order: densities, FFT_X, E, electron push, ion push, MCC, RCX, appends):
+the FP64 device cycle against the oracle's cycle, determinism of the fixed-point deposit under re-sorting, and
+the fused collision epilogue against the separate collision passes."""
+import numpy as np
+import pytest
+
+import pyoracle
+from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation
+from gpu_common import match_by_id, oracle_geom, periodic_dx, random_particles, small_deck
+
+
+def _plasma(sim, precision, n_per_cell=16, seed=21):
+    p = sim.params
+    n = p.ncx * p.ncy * n_per_cell
+    e = random_particles(sim, n, seed=seed, precision=precision, fast_fraction=0.01)
+    ivs = np.random.default_rng(seed + 1).normal(0, 0.0005, (3, n))
+    if precision == PREC_MIXED:
+        ivs = ivs.astype(np.float32).astype(np.float64)
+    sim.upload_particles(ELECTRONS, *e, ids=np.arange(n, dtype=np.uint32))
+    sim.upload_particles(IONS, e[0], e[1], ivs[0], ivs[1], ivs[2], ids=np.arange(n, dtype=np.uint32))
+    return e, ivs
+
+
+@pytest.mark.gpu
+def test_fp64_cycle_matches_oracle_cycle(tmp_path):
+    d = small_deck(tmp_path, "periodic", ncx=32, ncy=32, n_gas=5.0e22)
+    steps = 1   # born particles get atomically assigned ids afterwards, so one step compares exactly
+    with Simulation(d, precision=PREC_FP64, seed=3) as sim:
+        p, t = sim.params, sim.deck.tables
+        e, ivs = _plasma(sim, PREC_FP64, n_per_cell=24)
+        sim.step(steps)
+        c = sim.counters()
+        ge = sim.download_particles(ELECTRONS)
+        gi = sim.download_particles(IONS)
+    n = e[0].size
+    oc = pyoracle.OracleCycle(d, p, t, e, (e[0], e[1], ivs[0], ivs[1], ivs[2]), seed=3)
+    oc.step(steps)
+    counters, pe, pi = oc.counters, oc.pe, oc.pi
+    assert list(c.en_collisions[:3]) == list(counters[:3])
+    assert c.rcx_collisions[0] == counters[4]
+    assert c.n_particles[0] == pe.n and c.n_particles[1] == pi.n
+    for got, ref in ((ge, pe.arrays()), (gi, pi.arrays())):
+        keep_g = got["id"] < n
+        keep_r = ref["id"] < n
+        a = {k: v[keep_g] for k, v in got.items()}
+        b = {k: v[keep_r] for k, v in ref.items()}
+        ia, ib = match_by_id(a, b)
+        assert np.abs(periodic_dx(a["x"][ia] - b["x"][ib], p.ncx)).max() < 1e-9
+        assert np.abs(a["y"][ia] - b["y"][ib]).max() < 1e-9
+        assert np.abs(a["vx"][ia] - b["vx"][ib]).max() < 1e-9
+
+
+@pytest.mark.gpu
+def test_sorting_does_not_change_the_state(tmp_path):
+    """The fixed-point deposit is order independent and the push is per particle, so the state after several steps
+    with periodic re-sorting is bit-identical to the unsorted run."""
+    d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, collisions=False, bx=86.6, by=50.0)
+    out = []
+    for sort_every in (0, 3):
+        with Simulation(d, precision=PREC_MIXED, sort_every=sort_every) as sim:
+            _plasma(sim, PREC_MIXED, n_per_cell=20)
+            sim.step(10)
+            out.append((sim.download_particles(ELECTRONS), sim.download_particles(IONS),
+                        sim.gather_electron_charge_density(), sim.counters()))
+    (e0, i0, r0, c0), (e1, i1, r1, c1) = out
+    assert np.array_equal(r0, r1)
+    for a, b in ((e0, e1), (i0, i1)):
+        ia, ib = match_by_id(a, b)
+        for k in ("x", "y", "vx", "vy", "vz"):
+            assert np.array_equal(a[k][ia], b[k][ib])
+    assert list(c0.electron_hits) == list(c1.electron_hits)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_fused_collisions_equal_separate_passes(tmp_path, precision):
+    d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, n_gas=1.0e23)
+    out = []
+    for fuse in (False, True):
+        with Simulation(d, precision=precision, sort_every=4, fuse_collisions=fuse, seed=11) as sim:
+            _plasma(sim, precision, n_per_cell=20)
+            sim.step(3)
+            c = sim.counters()
+            out.append((sim.download_particles(ELECTRONS), list(c.en_collisions[:3]), c.rcx_collisions[0],
+                        list(c.n_particles[:2])))
+    (a, ca, ra, na), (b, cb, rb, nb) = out
+    assert ca == cb and ra == rb and na == nb
+    assert min(ca) > 0
+    keep_a, keep_b = a["id"] < 64 * 48 * 20, b["id"] < 64 * 48 * 20
+    a = {k: v[keep_a] for k, v in a.items()}
+    b = {k: v[keep_b] for k, v in b.items()}
+    ia, ib = match_by_id(a, b)
+    for k in ("vx", "vy", "vz"):
+        assert np.abs(a[k][ia] - b[k][ib]).max() < 1e-6

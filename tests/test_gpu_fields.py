@@ -1,0 +1,68 @@
+"""Field solves on the device against the oracle on the same charge density: FFT_X (SOLVE_POISSON_FFTX_LINSYSY)
+to 1e-9 of max|phi|, E from phi, and the CG replacement of the PETSc solve to the discrete operator's solution."""
+import numpy as np
+import pytest
+
+import pyoracle
+from edipic_b200 import (ELECTRONS, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS, PREC_FP64, PREC_MIXED,
+                         Simulation, WARM_ZERO)
+from gpu_common import oracle_geom, random_particles, small_deck
+
+
+def _load_plasma(sim, precision, seed=4):
+    n = sim.params.ncx * sim.params.ncy * 12
+    xe = random_particles(sim, n, seed=seed, precision=precision)
+    xi = random_particles(sim, n // 2, seed=seed + 1, precision=precision, vscale=0.001)
+    sim.upload_particles(ELECTRONS, *xe)
+    sim.upload_particles(IONS, *xi)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+@pytest.mark.parametrize("ncx,ncy", [(64, 48), (256, 40)])
+def test_fftx_matches_oracle(tmp_path, precision, ncx, ncy):
+    d = small_deck(tmp_path, "periodic", ncx=ncx, ncy=ncy, wall_potentials={2: 30.0, 4: -10.0})
+    with Simulation(d, precision=precision, sort_every=0) as sim:
+        _load_plasma(sim, precision)
+        p = sim.params
+        phi = sim.solve_poisson_fftx_linsysy(want_phi=True)
+        rho_e = sim.gather_electron_charge_density()
+        rho_i = sim.gather_ion_charge_density()
+        rho_t = sim.field(FIELD_RHO_TOTAL)
+        ex, ey = sim.field(FIELD_EX), sim.field(FIELD_EY)
+    g = oracle_geom(sim)
+    rho = (rho_i - rho_e) / p.n_of_particles_cell
+    assert np.allclose(rho_t, rho, rtol=0, atol=1e-12 * max(1.0, np.abs(rho).max()))
+    ref = pyoracle.fftx_solve(g, rho, p.wall_phi_const[0], p.wall_phi_const[1])
+    assert np.abs(phi - ref).max() <= 1e-9 * np.abs(ref).max()
+    f2 = p.f_scale_v / (p.e_scale_vm * 2.0 * p.delta_x_m)
+    f1 = p.f_scale_v / (p.e_scale_vm * p.delta_x_m)
+    rex, rey = pyoracle.efield(g, phi, f2, f1)
+    tol = (1e-6 if precision == PREC_MIXED else 1e-12) * max(np.abs(rex).max(), np.abs(rey).max())
+    assert np.abs(ex - rex).max() <= tol and np.abs(ey - rey).max() <= tol
+    # the discrete operator of the reference: phi_{j-1} + phi_{j+1} + (spectral x) = -rho inside
+    assert abs(phi[0, 5] - p.wall_phi_const[0]) < 1e-9 and abs(phi[-1, 5] - p.wall_phi_const[1]) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_cg_matches_oracle(tmp_path, precision):
+    d = small_deck(tmp_path, "walled", ncx=96, ncy=80, inner=(30, 20, 60, 36, -100.0))
+    with Simulation(d, precision=precision, sort_every=0) as sim:
+        _load_plasma(sim, precision)
+        p = sim.params
+        it = sim.solve_potential_with_cg(rtol=1e-12, max_it=20000, warm_start=WARM_ZERO)
+        phi = sim.field(FIELD_PHI)
+        rho_t = sim.field(FIELD_RHO_TOTAL)
+        ex = sim.field(FIELD_EX)
+        it2 = sim.solve_potential_with_cg(rtol=1e-8, max_it=20000)   # warm start from the converged phi
+    g = oracle_geom(sim)
+    ref, it_ref, rel = pyoracle.cg_solve(g, rho_t, [0.0, 0.0, 0.0, 0.0], [p.inner_phi[0]], rtol=1e-13)
+    assert it_ref > 0 and rel < 1e-13
+    assert np.abs(phi - ref).max() <= 1e-8 * np.abs(ref).max()
+    assert it > 10 and it2 <= 2
+    assert np.allclose(phi[20:37, 30:61], p.inner_phi[0])
+    f2 = p.f_scale_v / (p.e_scale_vm * 2.0 * p.delta_x_m)
+    f1 = p.f_scale_v / (p.e_scale_vm * p.delta_x_m)
+    rex, _ = pyoracle.efield(g, phi, f2, f1)
+    assert np.abs(ex - rex).max() <= (1e-6 if precision == PREC_MIXED else 1e-12) * np.abs(rex).max()
