@@ -588,8 +588,9 @@ void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c,
         for (int q = 0; q < 8; ++q) counters[q] += cnt[t][q];
         for (size_t r = 0; r < born[t].size(); r += 8) {
             const double* b = &born[t][r];
-            append(born_e, cap_born, b[0], b[1], b + 2, 0u);
-            append(born_i, cap_born, b[0], b[1], b + 5, 0u);
+            // born particles carry no id of the parent run (marked 0xFFFFFFFF); the device numbers them itself
+            append(born_e, cap_born, b[0], b[1], b + 2, 0xFFFFFFFFu);
+            append(born_i, cap_born, b[0], b[1], b + 5, 0xFFFFFFFFu);
         }
     }
 }
