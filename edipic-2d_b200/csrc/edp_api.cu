@@ -39,6 +39,7 @@ edp_mcc_dev edp_make_mcc_dev(const edp_ctx* c)
     }
     for (int i = 0; i < t.n_seg; ++i) m.seg_step[i] = t.seg_step[i];
     m.pmax = t.max_colliding_fraction;
+    m.pmax_x = (unsigned long long)std::ceil(std::ldexp(t.max_colliding_fraction, 32) - 0.5);
     for (int p = 0; p < EDP_MAX_COLPROC; ++p) {
         m.type[p] = t.colproc_type[p];
         m.thr[p] = t.threshold_eV[p];
@@ -66,6 +67,8 @@ edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s)
     r.alpha = t.rcx_alpha;
     r.pth2 = t.rcx_probab_thermal[s] * t.rcx_probab_thermal[s];
     r.vfactor = t.rcx_vfactor[s];
+    double k = (r.prob_factor * ((r.sigma_1eV * 1.0) * 1.0)) * r.v_scale;
+    r.k2 = k * k;
     return r;
 }
 
@@ -155,6 +158,18 @@ int alloc_species(edp_ctx* c, int sp, int64_t n)
             TRY(dalloc(c, &e.vy, bc));
             TRY(dalloc(c, &e.vz, bc));
         }
+        edp_born_dev h[2];
+        for (int b = 0; b < 2; ++b) {
+            h[b].pend_next = c->pend_e[b];
+            for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) h[b].born_i[s] = c->born_i[s];
+        }
+        TRY(dalloc(c, &c->born_dev, 2));
+        EDP_CUDA(c, cudaMemcpy(c->born_dev, h, sizeof(h), cudaMemcpyHostToDevice));
+        // selection list of the fused collision test: P_max of the electrons on average, with headroom
+        double pm = c->tab.en_on ? c->tab.max_colliding_fraction : 0.0;
+        c->sel_cap = std::max<int64_t>(65536, (int64_t)((double)cap * std::min(1.0, 2.0 * pm + 0.01)));
+        TRY(dalloc(c, &c->sel_list, c->sel_cap));
+        TRY(dalloc(c, &c->sel_count, 1));
     }
     return EDP_OK;
 }
@@ -612,6 +627,11 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
     c->tab.prob = nullptr;
     c->tab.energy_eV = nullptr;
     c->tab.maxwell_v = nullptr;
+    {
+        edp_mcc_dev m = edp_make_mcc_dev(c);
+        if ((r = dalloc(c, &c->mcc_dev, 1))) return fail(r);
+        cudaMemcpy(c->mcc_dev, &m, sizeof(m), cudaMemcpyHostToDevice);
+    }
     if ((r = edp_fields_prepare(c))) return fail(r);
     for (int s = 0; s < 4; ++s) c->phi_wall[s] = p->wall_phi_const[s] + p->wall_phi_var[s] * std::sin(p->wall_phase[s]);
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDP_ERR_CUDA);
@@ -649,7 +669,7 @@ int edp_destroy(edp_ctx* c)
     F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
     F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
     F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v);
-    F(c->dc); F(c->dev_small);
+    F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

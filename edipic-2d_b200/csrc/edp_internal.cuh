@@ -72,6 +72,14 @@ struct edp_born {
     int64_t cap = 0;
 };
 
+struct edp_mcc_dev;
+
+// add lists as seen by the kernels: the electron list filled this step and the ion lists
+struct edp_born_dev {
+    edp_born pend_next;
+    edp_born born_i[EDP_MAX_ION_SPECIES];
+};
+
 // constant parameters handed to kernels by value
 struct edp_kparams {
     int32_t ncx, ncy, periodic, nxg, nyg;     // nxg = node columns stored (ncx periodic, ncx+1 walled)
@@ -137,6 +145,11 @@ struct edp_ctx {
     double* mcc_prob = nullptr;
     double* mcc_energy = nullptr;
     double* maxwell_v = nullptr;
+    edp_mcc_dev* mcc_dev = nullptr;  // device copy of the collision table descriptor
+    edp_born_dev* born_dev = nullptr; // [2]: add-list descriptors for pend_cur^1 == 0 and == 1
+    uint32_t* sel_list = nullptr;     // electron slots selected for a collision in the fused push
+    unsigned long long* sel_count = nullptr;
+    int64_t sel_cap = 0;
     edp_tables tab;                   // scalar part (pointers are host pointers; device copies above)
     int32_t host_n_act = 0;
 
@@ -195,6 +208,7 @@ struct edp_mcc_dev {
     double seg_step[EDP_MAX_SEGMENTS];
     int32_t seg_index[EDP_MAX_SEGMENTS + 1];
     double pmax;
+    unsigned long long pmax_x;              // (x + 1/2) 2^-32 < pmax  <=>  x < pmax_x, for 32-bit Philox words x
     int32_t type[EDP_MAX_COLPROC];
     double thr[EDP_MAX_COLPROC];
     int32_t ion_species[EDP_MAX_COLPROC];   // 0-based, -1 none
@@ -207,6 +221,7 @@ struct edp_rcx_dev {
     const double* maxwell_v;
     int32_t on, rmax;
     double prob_factor, v_scale, factor_eV, sigma_1eV, alpha, pth2, vfactor;
+    double k2;   // (n_gas dt N_sub sigma V_scale)^2, the energy-independent factor when alpha == 0
 };
 
 // GetMaxwellVelocity (pic2d_ElectronWallCollisions.f90:961-985)
@@ -287,25 +302,36 @@ struct edp_mcc_out {
     int ion_species;
 };
 
-// PERFORM_ELECTRON_NEUTRAL_COLLISIONS + en_Collision_* (pic2d_enCollisionsSpecificProc.f90:61-639) for one
-// electron with Philox stream 0 (block 0 = select, kind, density; blocks 1-2 = scattering variates).
-__device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id, uint32_t step, uint32_t seed_lo,
-                                               uint32_t seed_hi, double& vx, double& vy, double& vz)
+// Selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS as a per-electron Bernoulli(P_max) test on Philox stream 0,
+// block 0 = {select, kind r, density n, -}. Returns the kind variate r when selected.
+__device__ __forceinline__ bool edp_mcc_select(const edp_mcc_dev* m, uint32_t id, uint32_t step, uint32_t seed_lo,
+                                               uint32_t seed_hi, double& r)
 {
-    edp_mcc_out o;
-    o.kind_index = 0;
-    o.born = 0;
     uint32_t b0[4];
     edp_philox(step, EDP_STREAM_MCC, 0u, seed_hi, id, seed_lo, b0);
-    if (!(edp_u01(b0[0]) < m.pmax)) return o;
-    double r = edp_u01(b0[1]);
+    if ((unsigned long long)b0[0] >= m->pmax_x) return false;
+    r = edp_u01(b0[1]);
+    return true;
+}
+
+// Kind choice and scattering of one selected electron (en_Collision_*, pic2d_enCollisionsSpecificProc.f90:61-639),
+// blocks 1-2 of Philox stream 0 hold the scattering variates. Out of line: it runs for P_max of the electrons.
+static __device__ __noinline__ void edp_mcc_collide(const edp_mcc_dev* mp, uint32_t id, uint32_t step,
+                                                    uint32_t seed_lo, uint32_t seed_hi, double r, double* v,
+                                                    edp_mcc_out* out)
+{
+    const edp_mcc_dev& m = *mp;
+    edp_mcc_out& o = *out;
+    o.kind_index = 0;
+    o.born = 0;
+    double vx = v[0], vy = v[1], vz = v[2];
     double v2 = __fma_rn(vz, vz, __fma_rn(vy, vy, __dmul_rn(vx, vx)));
     double E = __dmul_rn(v2, m.energy_factor);
     int ki = edp_mcc_choose_dev(m, E, r);
-    if (ki > m.n_act) return o;
+    if (ki > m.n_act) return;
     int kind = m.type[ki - 1];
     double thr = m.thr[ki - 1];
-    if ((kind == 20 || kind == 30) && E <= thr) return o;
+    if ((kind == 20 || kind == 30) && E <= thr) return;
     uint32_t b1[4], b2[4];
     edp_philox(step, EDP_STREAM_MCC, 1u, seed_hi, id, seed_lo, b1);
     double u0 = edp_u01(b1[0]), u1 = edp_u01(b1[1]), u2 = edp_u01(b1[2]), u3 = edp_u01(b1[3]);
@@ -316,10 +342,10 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id
         double ks = acos(c), s = sin(ks), fi = u1 * 6.28318530718;
         edp_rotate(c, s, cos(fi), sin(fi), vx, vy, vz, ox, oy, oz);
         double alpha = sqrt(1.0 - (0.001097161 / m.mass_amu) * (1.0 - c));
-        vx = ox * alpha;
-        vy = oy * alpha;
-        vz = oz * alpha;
-        return o;
+        v[0] = ox * alpha;
+        v[1] = oy * alpha;
+        v[2] = oz * alpha;
+        return;
     }
     if (kind == 20) {
         double esc = fmax(0.0, E - thr);
@@ -327,10 +353,10 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id
         double ks = acos(c), s = sin(ks), fi = u1 * 6.28318530718;
         edp_rotate(c, s, cos(fi), sin(fi), vx, vy, vz, ox, oy, oz);
         double alpha = sqrt(esc / E);
-        vx = ox * alpha;
-        vy = oy * alpha;
-        vz = oz * alpha;
-        return o;
+        v[0] = ox * alpha;
+        v[1] = oy * alpha;
+        v[2] = oz * alpha;
+        return;
     }
     // ionisation, B = 10 eV (pic2d_enCollisionsSpecificProc.f90:451-629)
     edp_philox(step, EDP_STREAM_MCC, 2u, seed_hi, id, seed_lo, b2);
@@ -341,13 +367,12 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id
     double esc = fmax(0.0, E - thr - eej);
     double csc = edp_okh(esc, u1), ksc = acos(csc), ssc = sin(ksc), fsc = u2 * 6.28318530718;
     double cej = edp_okh(eej, u3), kej = acos(cej), sej = sin(kej), fej = u4 * 6.28318530718;
-    double Vx = vx, Vy = vy, Vz = vz;
-    edp_rotate(csc, ssc, cos(fsc), sin(fsc), Vx, Vy, Vz, ox, oy, oz);
+    edp_rotate(csc, ssc, cos(fsc), sin(fsc), vx, vy, vz, ox, oy, oz);
     double asc = sqrt(esc / E);
-    vx = ox * asc;
-    vy = oy * asc;
-    vz = oz * asc;
-    edp_rotate(cej, sej, cos(fej), sin(fej), Vx, Vy, Vz, ox, oy, oz);
+    v[0] = ox * asc;
+    v[1] = oy * asc;
+    v[2] = oz * asc;
+    edp_rotate(cej, sej, cos(fej), sin(fej), vx, vy, vz, ox, oy, oz);
     double aej = sqrt(eej / E);
     o.ne[0] = ox * aej;
     o.ne[1] = oy * aej;
@@ -358,22 +383,42 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev& m, uint32_t id
     o.ni[2] = edp_maxwell(m.maxwell_v, m.rmax, u7) * f;
     o.ion_species = m.ion_species[ki - 1];
     o.born = (o.ion_species >= 0) ? 1 : 0;
+}
+
+// PERFORM_ELECTRON_NEUTRAL_COLLISIONS + en_Collision_* for one electron (the separate passes)
+__device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev* m, uint32_t id, uint32_t step, uint32_t seed_lo,
+                                               uint32_t seed_hi, double& vx, double& vy, double& vz)
+{
+    edp_mcc_out o;
+    o.kind_index = 0;
+    o.born = 0;
+    double r;
+    if (!edp_mcc_select(m, id, step, seed_lo, seed_hi, r)) return o;
+    double v[3] = {vx, vy, vz};
+    edp_mcc_collide(m, id, step, seed_lo, seed_hi, r, v, &o);
+    vx = v[0];
+    vy = v[1];
+    vz = v[2];
     return o;
 }
 
 // PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:90-121) for one ion; true on exchange.
-__device__ inline bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, uint32_t step, uint32_t species,
-                                   uint32_t seed_lo, uint32_t seed_hi, double& vx, double& vy, double& vz)
+// The test r <= sqrt(P^2 + P_th^2), P = n dt N_sub |v| V_scale sigma(E), is evaluated as r^2 <= P^2 + P_th^2.
+__device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, uint32_t step, uint32_t species,
+                                            uint32_t seed_lo, uint32_t seed_hi, double& vx, double& vy, double& vz)
 {
     double vsq = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
-    double en = __dmul_rn(vsq, r.factor_eV);
-    double vabs = __dmul_rn(sqrt(vsq), r.v_scale);
-    double l = __dsub_rn(1.0, __dmul_rn(r.alpha, log(fmax(en, 0.001))));
-    double p = __dmul_rn(__dmul_rn(r.prob_factor, vabs), __dmul_rn(__dmul_rn(r.sigma_1eV, l), l));
-    p = sqrt(__dadd_rn(__dmul_rn(p, p), r.pth2));
+    double k2 = r.k2;
+    if (r.alpha != 0.0) {
+        double l = __dsub_rn(1.0, __dmul_rn(r.alpha, log(fmax(__dmul_rn(vsq, r.factor_eV), 0.001))));
+        double k = __dmul_rn(__dmul_rn(r.prob_factor, __dmul_rn(__dmul_rn(r.sigma_1eV, l), l)), r.v_scale);
+        k2 = __dmul_rn(k, k);
+    }
+    double p2 = __dadd_rn(__dmul_rn(k2, vsq), r.pth2);
     uint32_t b[4];
     edp_philox(step, EDP_STREAM_RCX(species), 0u, seed_hi, id, seed_lo, b);
-    if (!(edp_u01(b[0]) <= p)) return false;
+    double u = edp_u01(b[0]);
+    if (!(__dmul_rn(u, u) <= p2)) return false;
     vx = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[1])) * r.vfactor;
     vy = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[2])) * r.vfactor;
     vz = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[3])) * r.vfactor;

@@ -21,20 +21,19 @@ struct PushArgs {
     int64_t n_chunks;
     int64_t tail_start;
     const unsigned long long* n_slots;
-    int64_t tail_groups_per_cta;
     int64_t tail_ctas;
     const float2* E;
     unsigned long long* rho;
     float K[9];
     float qh, ez_term, xmul;
-    int use_rot, is_ion, species;
-    int do_mcc, do_rcx;
+    int use_rot, species, do_coll;
     uint32_t step;
-    edp_mcc_dev mcc;
+    const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
-    edp_born pend_next;
-    edp_born born_i[EDP_MAX_ION_SPECIES];
+    uint32_t* sel_list;
+    unsigned long long* sel_count;
+    int64_t sel_cap;
 };
 
 __device__ __forceinline__ int wrapx(int lx, const edp_kparams& kp)
@@ -77,23 +76,68 @@ __device__ __forceinline__ void record_born(const edp_born& b, unsigned long lon
     b.vz[k] = v[2];
 }
 
+// Shared state of one CTA of the mixed push: field window, density window and per-CTA counters.
+// The fixed-point density (2^32 units per macroparticle) is kept as two 32-bit accumulators per node,
+// hi = sum(q >> 16) and lo = sum(q & 0xFFFF), so that every shared update is a native 32-bit atomic;
+// a CTA handles at most EDP_CHUNK particles, which bounds both sums below 2^30.
+#define EDP_SEL_SMEM 1024
 struct Smem {
     float2 E[EDP_WIN_NODES * EDP_WIN_NODES];
-    unsigned long long R[EDP_WIN_NODES * EDP_WIN_NODES];
+    int hi[EDP_WIN_NODES * EDP_WIN_NODES];
+    unsigned lo[EDP_WIN_NODES * EDP_WIN_NODES];
     unsigned long long cnt[32];   // [0..7] hits, [8..15] en kinds, [16] rcx, [17] removed
+    uint32_t sel[EDP_SEL_SMEM];   // slots selected for an electron-neutral collision
+    unsigned nsel;
 };
 
-// One particle: returns false when it was absorbed (the caller stores cell = -1).
-__device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, int& cell,
-                                         float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id)
+// deposit of consecutive particles of one thread that land in the same cell, merged in registers
+struct DepAcc {
+    int b;   // window index of the (i, j) node, -1 when empty
+    long long q00, q10, q01, q11;
+};
+
+__device__ __forceinline__ void smem_add(Smem& s, int n, long long q)
+{
+    atomicAdd(&s.hi[n], (int)(q >> 16));
+    atomicAdd(&s.lo[n], (unsigned)(q & 0xFFFF));
+}
+
+__device__ __forceinline__ void dep_flush(Smem& s, DepAcc& d)
+{
+    if (d.b < 0) return;
+    smem_add(s, d.b, d.q00);
+    smem_add(s, d.b + 1, d.q10);
+    smem_add(s, d.b + EDP_WIN_NODES, d.q01);
+    smem_add(s, d.b + EDP_WIN_NODES + 1, d.q11);
+    d.b = -1;
+}
+
+// Electrons selected for a collision in the push epilogue: slot indices gathered per CTA in shared memory and
+// appended to a global list that collide_selected_kernel scatters (the same Philox variates as the separate pass).
+__device__ __forceinline__ void select_slot(const PushArgs& a, Smem& s, uint32_t slot)
+{
+    unsigned q = atomicAdd(&s.nsel, 1u);
+    if (q < EDP_SEL_SMEM) {
+        s.sel[q] = slot;
+        return;
+    }
+    unsigned long long g = atomicAdd(a.sel_count, 1ull);
+    if ((int64_t)g < a.sel_cap) a.sel_list[g] = slot;
+    else atomicOr(&a.dc->error_flags, EDP_EFLAG_PENDING);
+}
+
+// One particle. Returns false when it was absorbed (the caller stores cell = -1).
+template <bool ION>
+__device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, DepAcc& acc,
+                                         int& cell, float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id,
+                                         uint32_t slot)
 {
     const edp_kparams& kp = a.kp;
     int i = cell & 0xFFFF, j = cell >> 16;
     // ---- gather (bilinear, :82-86)
     int lx = wrapx(i - wx0, kp), ly = j - wy0;
-    bool inw = windowed && (unsigned)lx < EDP_WIN_CELLS && (unsigned)ly < EDP_WIN_CELLS;
     float2 e00, e10, e01, e11;
-    if (inw) {
+    if (windowed && (unsigned)lx < EDP_WIN_CELLS && (unsigned)ly < EDP_WIN_CELLS) {
         int b = ly * EDP_WIN_NODES + lx;
         e00 = s.E[b];
         e10 = s.E[b + 1];
@@ -113,7 +157,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     float EX = e00.x * w00 + e10.x * w10 + e01.x * w01 + e11.x * w11;
     float EY = e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11;
     // ---- Boris (:95-130 / ions :99-149)
-    float q = a.qh;
+    const float q = a.qh;
     if (a.use_rot) {
         float mx = vx + q * EX, my = vy + q * EY, mz = vz + a.ez_term;
         float px = a.K[0] * mx + a.K[1] * my + a.K[2] * mz;
@@ -122,7 +166,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         vx = px + q * EX;
         vy = py + q * EY;
         vz = pz + a.ez_term;
-    } else if (a.is_ion) {
+    } else if (ION) {
         vx = vx + (q + q) * EX;
         vy = vy + (q + q) * EY;
         vz = vz + (a.ez_term + a.ez_term);
@@ -168,20 +212,29 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     cell = (nj << 16) | ni;
     ox = nx;
     oy = ny;
-    // ---- deposit (:1597-1639): exact FP64 weights of the FP32 offsets, rounded to 2^-32
-    double dx = (double)nx, dy = (double)ny;
-    double vij = (1.0 - dx) * (1.0 - dy), vip1j = dx * (1.0 - dy), vijp1 = (1.0 - dx) * dy;
-    long long q00 = __double2ll_rn(vij * EDP_FIX_ONE);
-    long long q10 = __double2ll_rn(vip1j * EDP_FIX_ONE);
-    long long q01 = __double2ll_rn(vijp1 * EDP_FIX_ONE);
-    long long q11 = 4294967296LL - q00 - q10 - q01;
-    int dlx = wrapx(ni - wx0, kp), dly = nj - wy0;
+    // ---- deposit (:1597-1639): exact FP64 weights of the FP32 offsets, rounded to 2^-32; the fourth weight
+    // takes the remainder so that every particle deposits exactly 2^32 units
+    const double dx = (double)nx, dy = (double)ny;
+    const long long q00 = __double2ll_rn((1.0 - dx) * (1.0 - dy) * EDP_FIX_ONE);
+    const long long q10 = __double2ll_rn(dx * (1.0 - dy) * EDP_FIX_ONE);
+    const long long q01 = __double2ll_rn((1.0 - dx) * dy * EDP_FIX_ONE);
+    const long long q11 = 4294967296LL - q00 - q10 - q01;
+    const int dlx = wrapx(ni - wx0, kp), dly = nj - wy0;
     if (windowed && (unsigned)dlx < EDP_WIN_CELLS && (unsigned)dly < EDP_WIN_CELLS) {
-        int b = dly * EDP_WIN_NODES + dlx;
-        atomicAdd(&s.R[b], (unsigned long long)q00);
-        atomicAdd(&s.R[b + 1], (unsigned long long)q10);
-        atomicAdd(&s.R[b + EDP_WIN_NODES], (unsigned long long)q01);
-        atomicAdd(&s.R[b + EDP_WIN_NODES + 1], (unsigned long long)q11);
+        const int b = dly * EDP_WIN_NODES + dlx;
+        if (b != acc.b) {
+            dep_flush(s, acc);
+            acc.b = b;
+            acc.q00 = q00;
+            acc.q10 = q10;
+            acc.q01 = q01;
+            acc.q11 = q11;
+        } else {
+            acc.q00 += q00;
+            acc.q10 += q10;
+            acc.q01 += q01;
+            acc.q11 += q11;
+        }
     } else {
         int i1 = ni + 1;
         if (kp.periodic && i1 == kp.ncx) i1 = 0;
@@ -191,24 +244,12 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         atomicAdd(&a.rho[r1 + ni], (unsigned long long)q01);
         atomicAdd(&a.rho[r1 + i1], (unsigned long long)q11);
     }
-    // ---- collisions in the epilogue (same variates as the separate passes)
-    if (a.do_mcc) {
-        double dvx = vx, dvy = vy, dvz = vz;
-        edp_mcc_out o = edp_mcc_electron(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, dvx, dvy, dvz);
-        if (o.kind_index) {
-            vx = (float)dvx;
-            vy = (float)dvy;
-            vz = (float)dvz;
-            atomicAdd(&s.cnt[8 + o.kind_index - 1], 1ull);
-            if (o.born) {
-                double X = (double)ni + dx, Y = (double)nj + dy;
-                record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
-                record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y,
-                            o.ni);
-            }
-        }
+    // ---- collisions in the epilogue, with the variates of the separate passes
+    if (!ION && a.do_coll) {
+        double r;
+        if (edp_mcc_select(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, r)) select_slot(a, s, slot);
     }
-    if (a.do_rcx) {
+    if (ION && a.do_coll) {
         double dvx = vx, dvy = vy, dvz = vz;
         if (edp_rcx_ion(a.rcx, id, a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, dvx, dvy, dvz)) {
             vx = (float)dvx;
@@ -221,6 +262,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
 }
 
 // four consecutive slots [4g, 4g+4) restricted to [lo, hi)
+template <bool ION>
 __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, int64_t g,
                                            int64_t lo, int64_t hi)
 {
@@ -242,7 +284,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
         vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
         vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
         vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
-        if (a.do_mcc || a.do_rcx) {
+        if (a.do_coll) {
             uint4 id4 = __ldcs(reinterpret_cast<const uint4*>(a.P.id) + g);
             id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
         } else {
@@ -262,14 +304,18 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
             id[e] = ok ? a.P.id[k] : 0u;
         }
     }
+    DepAcc acc;
+    acc.b = -1;
 #pragma unroll
     for (int e = 0; e < EDP_ITEMS; ++e) {
         if (c[e] < 0) continue;
-        if (!push_one(a, s, windowed, wx0, wy0, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e])) {
+        if (!push_one<ION>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                            (uint32_t)(base + e))) {
             c[e] = -1;
             atomicAdd(&s.cnt[17], 1ull);
         }
     }
+    dep_flush(s, acc);
     if (full) {
         __stcs(reinterpret_cast<int4*>(a.P.cell) + g, make_int4(c[0], c[1], c[2], c[3]));
         __stcs(reinterpret_cast<float4*>(a.P.ox) + g, make_float4(ox[0], ox[1], ox[2], ox[3]));
@@ -293,11 +339,13 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
     }
 }
 
-__global__ void __launch_bounds__(EDP_PUSH_THREADS) push_mixed_kernel(PushArgs a)
+template <bool ION>
+__global__ void __launch_bounds__(EDP_PUSH_THREADS, 3) push_mixed_kernel(PushArgs a)
 {
     __shared__ Smem s;
     const edp_kparams& kp = a.kp;
     if (threadIdx.x < 32) s.cnt[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) s.nsel = 0u;
     const bool windowed = blockIdx.x < a.n_chunks;
     int64_t lo, hi;
     int wx0 = 0, wy0 = 0;
@@ -312,7 +360,8 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS) push_mixed_kernel(PushArgs a
             int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
             bool ok = gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg;
             s.E[t] = ok ? __ldg(&a.E[(int64_t)gy * kp.nxg + gx]) : make_float2(0.f, 0.f);
-            s.R[t] = 0ull;
+            s.hi[t] = 0;
+            s.lo[t] = 0u;
         }
     } else {
         lo = a.tail_start;
@@ -321,29 +370,41 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS) push_mixed_kernel(PushArgs a
     __syncthreads();
     if (windowed) {
         for (int64_t g = lo / EDP_ITEMS + threadIdx.x; g * EDP_ITEMS < hi; g += blockDim.x)
-            push_group(a, s, true, wx0, wy0, g, lo, hi);
+            push_group<ION>(a, s, true, wx0, wy0, g, lo, hi);
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
         int64_t g0 = lo / EDP_ITEMS;
         for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * EDP_ITEMS < hi; g += a.tail_ctas * blockDim.x)
-            push_group(a, s, false, 0, 0, g, lo, hi);
+            push_group<ION>(a, s, false, 0, 0, g, lo, hi);
     }
     __syncthreads();
     if (windowed) {
         for (int t = threadIdx.x; t < EDP_WIN_NODES * EDP_WIN_NODES; t += blockDim.x) {
-            unsigned long long v = s.R[t];
-            if (v == 0ull) continue;
+            long long v = (long long)s.hi[t] * 65536LL + (long long)s.lo[t];
+            if (v == 0) continue;
             int lx = t % EDP_WIN_NODES, ly = t / EDP_WIN_NODES;
             int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
-            if (gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg) atomicAdd(&a.rho[(int64_t)gy * kp.nxg + gx], v);
+            if (gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg)
+                atomicAdd(&a.rho[(int64_t)gy * kp.nxg + gx], (unsigned long long)v);
             else atomicOr(&a.dc->error_flags, EDP_EFLAG_BOUNDS);
+        }
+    }
+    if (!ION) {
+        __shared__ unsigned long long sel_base;
+        const unsigned nsel = min(s.nsel, (unsigned)EDP_SEL_SMEM);
+        if (threadIdx.x == 0 && nsel) sel_base = atomicAdd(a.sel_count, (unsigned long long)nsel);
+        __syncthreads();
+        for (unsigned q = threadIdx.x; q < nsel; q += blockDim.x) {
+            unsigned long long g = sel_base + q;
+            if ((int64_t)g < a.sel_cap) a.sel_list[g] = s.sel[q];
+            else atomicOr(&a.dc->error_flags, EDP_EFLAG_PENDING);
         }
     }
     if (threadIdx.x < 32) {
         unsigned long long v = s.cnt[threadIdx.x];
         if (v) {
             int k = threadIdx.x;
-            if (k < 8) atomicAdd(a.is_ion ? &a.dc->i_hits[k] : &a.dc->e_hits[k], v);
+            if (k < 8) atomicAdd(ION ? &a.dc->i_hits[k] : &a.dc->e_hits[k], v);
             else if (k < 16) {
                 atomicAdd(&a.dc->en_coll[k - 8], v);
                 atomicAdd(&a.dc->en_coll_step[k - 8], v);
@@ -354,6 +415,57 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS) push_mixed_kernel(PushArgs a
                 atomicAdd(&a.dc->n_live[a.species], (unsigned long long)(-(long long)v));
             }
         }
+    }
+}
+
+struct SelArgs {
+    edp_kparams kp;
+    edp_species_mixed P;
+    const uint32_t* sel_list;
+    const unsigned long long* sel_count;
+    int64_t sel_cap;
+    uint32_t step;
+    const edp_mcc_dev* mcc;
+    const edp_born_dev* born;
+    edp_dev_counters* dc;
+};
+
+// kind choice and scattering of the electrons the push selected (PERFORM_ELECTRON_NEUTRAL_COLLISIONS :447-485 and
+// en_Collision_*), on the post-push velocities, with the selection's kind variate recomputed from Philox block 0
+__global__ void __launch_bounds__(256) collide_selected_kernel(SelArgs a)
+{
+    __shared__ unsigned long long cnt[EDP_MAX_COLPROC];
+    if (threadIdx.x < EDP_MAX_COLPROC) cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+    unsigned long long n = *a.sel_count;
+    if ((int64_t)n > a.sel_cap) n = (unsigned long long)a.sel_cap;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < (int64_t)n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t slot = a.sel_list[k];
+        const uint32_t id = a.P.id[slot];
+        double r;
+        if (!edp_mcc_select(a.mcc, id, a.step, a.kp.seed_lo, a.kp.seed_hi, r)) continue;
+        double v[3] = {(double)a.P.vx[slot], (double)a.P.vy[slot], (double)a.P.vz[slot]};
+        edp_mcc_out o;
+        edp_mcc_collide(a.mcc, id, a.step, a.kp.seed_lo, a.kp.seed_hi, r, v, &o);
+        if (!o.kind_index) continue;
+        a.P.vx[slot] = (float)v[0];
+        a.P.vy[slot] = (float)v[1];
+        a.P.vz[slot] = (float)v[2];
+        atomicAdd(&cnt[o.kind_index - 1], 1ull);
+        if (o.born) {
+            const int c = a.P.cell[slot];
+            const double X = (double)(c & 0xFFFF) + (double)a.P.ox[slot];
+            const double Y = (double)(c >> 16) + (double)a.P.oy[slot];
+            record_born(a.born->pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+            record_born(a.born->born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y,
+                        o.ni);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < EDP_MAX_COLPROC && cnt[threadIdx.x]) {
+        atomicAdd(&a.dc->en_coll[threadIdx.x], cnt[threadIdx.x]);
+        atomicAdd(&a.dc->en_coll_step[threadIdx.x], cnt[threadIdx.x]);
     }
 }
 
@@ -368,7 +480,7 @@ struct PushArgs64 {
     double qh, ez_term;
     int xmul, use_rot, is_ion, species, do_mcc, do_rcx;
     uint32_t step;
-    edp_mcc_dev mcc;
+    const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
     edp_born pend_next;
@@ -506,7 +618,7 @@ struct CollArgs {
     edp_species_fp64 Pd;
     const unsigned long long* n_slots;
     uint32_t step;
-    edp_mcc_dev mcc;
+    const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
     edp_born pend_next;
@@ -622,7 +734,7 @@ struct AppendArgs {
     unsigned long long* rho_fix;
     double* rho_d;
     uint32_t step;
-    edp_mcc_dev mcc;
+    const edp_mcc_dev* mcc;
     edp_dev_counters* dc;
     edp_born pend_next;
     edp_born born_i[EDP_MAX_ION_SPECIES];
@@ -753,16 +865,16 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.ez_term = (float)ez_term;
         a.xmul = is_ion ? (float)p.n_subcycles : 1.0f;
         a.use_rot = use_rot;
-        a.is_ion = is_ion;
         a.species = sp;
-        a.do_mcc = do_mcc;
-        a.do_rcx = do_rcx;
+        a.do_coll = do_mcc || do_rcx;
         a.step = (uint32_t)c->t_cntr;
-        if (do_mcc) a.mcc = edp_make_mcc_dev(c);
+        a.mcc = c->mcc_dev;
         if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
         a.dc = c->dc;
-        a.pend_next = c->pend_e[pn];
-        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+        a.sel_list = c->sel_list;
+        a.sel_count = c->sel_count;
+        a.sel_cap = c->sel_cap;
+        if (do_mcc) EDP_CUDA(c, cudaMemsetAsync(c->sel_count, 0, sizeof(unsigned long long), c->stream));
         int64_t tail = c->host_slots[sp] - c->sorted_end[sp];
         if (tail < 0) tail = 0;
         int64_t per_cta = (int64_t)EDP_PUSH_THREADS * EDP_ITEMS * 8;
@@ -770,7 +882,23 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         if (a.tail_ctas < 1) a.tail_ctas = 1;
         int64_t grid = a.n_chunks + a.tail_ctas;
         ++c->launches;
-        push_mixed_kernel<<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
+        if (is_ion) push_mixed_kernel<true><<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
+        else push_mixed_kernel<false><<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
+        if (do_mcc) {
+            SelArgs b;
+            memset(&b, 0, sizeof(b));
+            b.kp = c->kp;
+            b.P = c->pm[sp];
+            b.sel_list = c->sel_list;
+            b.sel_count = c->sel_count;
+            b.sel_cap = c->sel_cap;
+            b.step = (uint32_t)c->t_cntr;
+            b.mcc = c->mcc_dev;
+            b.born = c->born_dev + pn;
+            b.dc = c->dc;
+            ++c->launches;
+            collide_selected_kernel<<<148 * 4, 256, 0, c->stream>>>(b);
+        }
     } else {
         PushArgs64 a;
         memset(&a, 0, sizeof(a));
@@ -790,7 +918,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.do_mcc = do_mcc;
         a.do_rcx = do_rcx;
         a.step = (uint32_t)c->t_cntr;
-        if (do_mcc) a.mcc = edp_make_mcc_dev(c);
+        a.mcc = c->mcc_dev;
         if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
         a.dc = c->dc;
         a.pend_next = c->pend_e[pn];
@@ -835,7 +963,7 @@ int edp_launch_collide_en(edp_ctx* c)
 {
     if (!c->tab.en_on) return EDP_OK;
     CollArgs a = coll_args(c, 0);
-    a.mcc = edp_make_mcc_dev(c);
+    a.mcc = c->mcc_dev;
     ++c->launches;
     collide_en_kernel<<<grid_for(c->host_slots[0]), 256, 0, c->stream>>>(a);
     EDP_CUDA(c, cudaGetLastError());
@@ -884,7 +1012,7 @@ int edp_launch_append_pending(edp_ctx* c, bool ion_step)
     a.src = c->pend_e[cur];
     a.src_count = &c->dc->pend_e_count[1];   // the list filled during the previous step
     a.do_mcc = ion_step && c->tab.en_on;
-    if (a.do_mcc) a.mcc = edp_make_mcc_dev(c);
+    a.mcc = c->mcc_dev;
     // electrons born from these go to the list being filled this step, counted in pend_e_count[0]
     a.pend_next = c->pend_e[cur ^ 1];
     ++c->launches;

@@ -617,15 +617,17 @@ int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint
 #pragma omp parallel for reduction(+ : count) schedule(static)
     for (int64_t k = 0; k < ions->n; ++k) {
         double vx = ions->vx[k], vy = ions->vy[k], vz = ions->vz[k];
+        // probab_rcx = n dt N_sub |v| V_scale sigma(E); hit when r <= sqrt(probab_rcx^2 + P_th^2), written here as
+        // r^2 <= (n dt N_sub sigma(E) V_scale)^2 |v|^2 + P_th^2 (the same test without the two square roots)
         double vsq = vx * vx + vy * vy + vz * vz;
-        double en = vsq * r->factor_eV;
-        double vabs = std::sqrt(vsq) * r->v_scale_ms;
-        double l = 1.0 - r->alpha * std::log(std::max(en, 0.001));
-        double p = r->prob_factor * vabs * (r->sigma_1eV * l * l);
-        p = std::sqrt(p * p + pt2);
+        double l = 1.0;
+        if (r->alpha != 0.0) l = 1.0 - r->alpha * std::log(std::max(vsq * r->factor_eV, 0.001));
+        double kf = (r->prob_factor * ((r->sigma_1eV * l) * l)) * r->v_scale_ms;
+        double p2 = (kf * kf) * vsq + pt2;
         uint32_t b[4];
         philox_block(ions->id[k], c->seed, c->step, 1u + (species << 8), 0u, b);
-        if (uniform(b[0]) <= p) {
+        double u = uniform(b[0]);
+        if (u * u <= p2) {
             ions->vx[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[1])) * r->vfactor;
             ions->vy[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[2])) * r->vfactor;
             ions->vz[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[3])) * r->vfactor;
