@@ -106,6 +106,8 @@ SIGNATURES = {
     "edp_set_field": [_CTX, C.c_int, _D],
     "edp_moments": [_CTX, C.c_int, _D],
     "edp_mcc_choose": [_CTX, C.c_int64, _D, _D, _I32],
+    "edp_poisson_fftx_noalloc": [C.c_int32, C.c_int32, C.c_void_p, C.c_double, C.c_double, C.c_void_p,
+                                 C.c_void_p],
     "edp_deck_read": [C.c_char_p, P(C.c_void_p), P(Params), P(Tables)],
     "edp_deck_initial_plasma": [C.c_void_p, _D, _D, _D, _D, _I32, _D, _I64],
     "edp_deck_free": [C.c_void_p],

@@ -206,6 +206,23 @@ int edp_moments(edp_ctx* ctx, int species, double out[7]);
  * (energy, r) pairs: kind_out[k] = indx_coll (n_act+1 = null collision) */
 int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const double* r, int32_t* kind_out);
 
+/* ---- allocation-free FFT_X solve ------------------------------------------------------------------ */
+/* No counterpart in the reference. For callers that cannot allocate device memory (a host whose GPU memory is
+ * owned by another runtime or pool, or that must not allocate once running): solves the FFT_X Poisson problem
+ * of SOLVE_POISSON_FFTX_LINSYSY for metal walls without any allocation. rho_dev (input) and phi_dev (output)
+ * are device buffers of the caller in the periodic reference layout, (ncx+2) x (ncy+1) FP64 nodes x fastest,
+ * rho_dev holding factor_rho*(rho_i - rho_e); phi_bottom/phi_top are the normalised wall potentials; stream is
+ * a cudaStream_t (NULL = default stream). The workspace is a file-scope device array of
+ * EDP_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps until exit; (ncy+1)*(ncx/2+1)*24 +
+ * ncx*8 bytes plus up to 512 bytes of section alignment must fit in it, else EDP_ERR_CAPACITY (1024 x 1023
+ * cells fit). The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make it before any stream capture. All calls share
+ * the array, so calls that overlap on the GPU race: order them on one stream. Work is queued on the stream and
+ * the call returns without synchronising. */
+#define EDP_NOALLOC_SCRATCH_BYTES (8u << 20)
+int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* rho_dev, double phi_bottom, double phi_top,
+                             double* phi_dev, void* stream);
+
 /* ---- deck reader (host side of INITIATE_PARAMETERS and the collision set-up) --------------------- */
 /* Reads init_configuration.dat, init_simcontrol.dat, init_particles.dat, init_extfields.dat,
  * init_bo_NN.dat, init_neutrals.dat, init_neutral_<NAME>.dat, its cross-section files and
