@@ -231,7 +231,7 @@ def run_ours(args):
     value = particle_steps / t_total
 
     # end to end: the drop-in call order of a Fortran host (pic2d_MainProgram.f90:151-309) with its per-step reads
-    e2e_steps = max(2, min(args.steps, 10))
+    e2e_steps = args.steps
     cnt_buf = (C.c_int64 * 8)()
     rcx_buf = C.c_int64()
     rho_host = None

@@ -85,25 +85,78 @@ __global__ void fftx_forward(edp_kparams kp, const double* __restrict__ rho, dou
     }
 }
 
-// SOLVE_POISSON_FFTX_LINSYSY :690-756, metal walls (a_eq(0) = a_eq(J) = 0)
+// SOLVE_POISSON_FFTX_LINSYSY :690-756 for metal walls (a_eq(0) = a_eq(J) = 0). The forward sweep
+//   rr(j) = (-y(j) - rr(j-1)) a(j),  j = 1..J-1,  rr(0) = y(0)
+// and the back substitution phi(j) = rr(j) - a(j) phi(j+1), phi(J) = y(J), are first-order affine recurrences.
+// One warp solves one mode: lane l composes the maps of its segment of rows, a shuffle scan over the lanes gives
+// each segment its incoming value, and the lane re-sweeps its rows. Same recurrence, reassociated.
+struct Aff {   // x -> c + b x, complex c, real b
+    double cx, cy, b;
+};
+
+__device__ __forceinline__ Aff aff_after(const Aff& late, const Aff& early)   // late o early
+{
+    return Aff{late.cx + late.b * early.cx, late.cy + late.b * early.cy, late.b * early.b};
+}
+
+__device__ __forceinline__ Aff shfl_aff(const Aff& a, int src, bool up, int off)
+{
+    Aff r;
+    r.cx = up ? __shfl_up_sync(0xFFFFFFFFu, a.cx, off) : __shfl_down_sync(0xFFFFFFFFu, a.cx, off);
+    r.cy = up ? __shfl_up_sync(0xFFFFFFFFu, a.cy, off) : __shfl_down_sync(0xFFFFFFFFu, a.cy, off);
+    r.b = up ? __shfl_up_sync(0xFFFFFFFFu, a.b, off) : __shfl_down_sync(0xFFFFFFFFu, a.b, off);
+    (void)src;
+    return r;
+}
+
 __global__ void fftx_thomas(int J, int nm, const double* __restrict__ aeq, double2* __restrict__ spec)
 {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nm) return;
-    double2 prev = spec[m];  // rhs(0) = transformed wall row
-    for (int j = 1; j <= J - 1; ++j) {
-        double a = aeq[(int64_t)j * nm + m];
-        double2 y = spec[(int64_t)j * nm + m];
+    const int m = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (m >= nm) return;   // whole warps
+    const int n = J - 1, per = (n + 31) / 32;
+    const int j0 = 1 + lane * per, j1 = min(j0 + per, J);   // interior rows [j0, j1) of this lane
+    // ---- forward sweep: compose rr(j) = -a y(j) + (-a) rr(j-1) over the segment
+    Aff f{0.0, 0.0, 1.0};
+    for (int j = j0; j < j1; ++j) {
+        const double a = aeq[(int64_t)j * nm + m];
+        const double2 y = spec[(int64_t)j * nm + m];
+        f = aff_after(Aff{-a * y.x, -a * y.y, -a}, f);
+    }
+    for (int off = 1; off < 32; off <<= 1) {   // inclusive scan, lane l = segments 0..l
+        Aff p = shfl_aff(f, lane - off, true, off);
+        if (lane >= off) f = aff_after(f, p);
+    }
+    const double2 rr0 = spec[m];   // transformed wall row
+    Aff ex = shfl_aff(f, lane - 1, true, 1);
+    double2 prev = lane == 0 ? rr0 : make_double2(ex.cx + ex.b * rr0.x, ex.cy + ex.b * rr0.y);
+    for (int j = j0; j < j1; ++j) {
+        const double a = aeq[(int64_t)j * nm + m];
+        const double2 y = spec[(int64_t)j * nm + m];
         prev = make_double2((-y.x - prev.x) * a, (-y.y - prev.y) * a);
         spec[(int64_t)j * nm + m] = prev;
     }
-    double2 next = spec[(int64_t)J * nm + m];
-    for (int j = J - 1; j >= 0; --j) {
-        double a = aeq[(int64_t)j * nm + m];
-        double2 r = spec[(int64_t)j * nm + m];
+    // ---- back substitution: phi(j) = rr(j) + (-a(j)) phi(j+1), segments composed from the top
+    Aff g{0.0, 0.0, 1.0};
+    for (int j = j1 - 1; j >= j0; --j) {
+        const double a = aeq[(int64_t)j * nm + m];
+        const double2 r = spec[(int64_t)j * nm + m];
+        g = aff_after(Aff{r.x, r.y, -a}, g);
+    }
+    for (int off = 1; off < 32; off <<= 1) {   // inclusive scan from lane 31 down: lane l = segments l..31
+        Aff p = shfl_aff(g, lane + off, false, off);
+        if (lane + off < 32) g = aff_after(g, p);
+    }
+    const double2 phiJ = spec[(int64_t)J * nm + m];
+    Aff ey = shfl_aff(g, lane + 1, false, 1);
+    double2 next = lane == 31 ? phiJ : make_double2(ey.cx + ey.b * phiJ.x, ey.cy + ey.b * phiJ.y);
+    for (int j = j1 - 1; j >= j0; --j) {
+        const double a = aeq[(int64_t)j * nm + m];
+        const double2 r = spec[(int64_t)j * nm + m];
         next = make_double2(r.x - a * next.x, r.y - a * next.y);
         spec[(int64_t)j * nm + m] = next;
     }
+    // row 0 keeps rr(0) = phi(0) since a_eq(0) = 0
 }
 
 __global__ void fftx_inverse(edp_kparams kp, const double2* __restrict__ spec, const double2* __restrict__ tw, int logn,
@@ -371,7 +424,7 @@ int edp_launch_fftx(edp_ctx* c)
     fftx_forward<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->rho_total, c->phi_wall[0], c->phi_wall[1], c->twiddle,
                                                      logn, c->nm, c->spec);
     ++c->launches;
-    fftx_thomas<<<(c->nm + 127) / 128, 128, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);
+    fftx_thomas<<<(c->nm + 7) / 8, 256, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);   // a warp per mode
     ++c->launches;
     fftx_inverse<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->spec, c->twiddle, logn, c->nm, c->phi);
     EDP_CUDA(c, cudaGetLastError());

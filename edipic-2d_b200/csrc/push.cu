@@ -340,7 +340,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
 }
 
 template <bool ION>
-__global__ void __launch_bounds__(EDP_PUSH_THREADS, 3) push_mixed_kernel(PushArgs a)
+__global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArgs a)   // 64 registers, no spills
 {
     __shared__ Smem s;
     const edp_kparams& kp = a.kp;
