@@ -125,7 +125,7 @@ def cpu_baseline(args, deck_dir, seconds=15.0):
             done += oc.step(1)
             steps += 1
             el = time.perf_counter() - t0
-            if el > seconds or steps >= 200:
+            if el > seconds or steps >= 5000:
                 break
     return {"value": done / el, "unit": "particle-steps/s", "cores": threads, "kind": "port",
             "sample": f"{ncx}x{ncy} cells x {args.ppc}+{args.ppc} per cell ({2 * n} particles), {steps} steps, "

@@ -610,9 +610,9 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
     c->ntx = (p->ncx + EDP_TILE - 1) / EDP_TILE;
     c->nty = (p->ncy + EDP_TILE - 1) / EDP_TILE;
     if (p->precision == EDP_PREC_MIXED) {
-        int64_t ntiles = (int64_t)c->ntx * c->nty, nkeys = ntiles * 256, nb = (nkeys + 2047) / 2048;
+        int64_t ntiles = (int64_t)c->ntx * c->nty, nkeys = ntiles * 256;
         if ((r = dalloc(c, &c->sort_count, nkeys + 1)) || (r = dalloc(c, &c->sort_offset, nkeys + 1)) ||
-            (r = dalloc(c, &c->scan_tmp, nb + 1 + nkeys + ntiles + 2)))
+            (r = dalloc(c, &c->scan_tmp, 2 * ntiles + nkeys + 4)))
             return fail(r);
     }
     // tables

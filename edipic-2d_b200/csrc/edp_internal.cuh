@@ -190,6 +190,30 @@ __host__ __device__ inline void edp_philox(uint32_t c0, uint32_t c1, uint32_t c2
     out[3] = c3;
 }
 
+// Philox2x32-10 (Salmon et al. SC'11): 64-bit counter {c0, c1}, 32-bit key, multiplier 0xD256D193,
+// Weyl increment 0x9E3779B9
+__host__ __device__ inline void edp_philox2x32(uint32_t c0, uint32_t c1, uint32_t k, uint32_t out[2])
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
+#else
+        uint64_t p = (uint64_t)0xD256D193u * c0;
+        uint32_t hi = (uint32_t)(p >> 32), lo = (uint32_t)p;
+#endif
+        c0 = hi ^ k ^ c1;
+        c1 = lo;
+        k += 0x9E3779B9u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+}
+
+// counter words of the Philox2x32 decision draws (xor-ed into the low seed word)
+#define EDP_SEL_MCC 0x4D430000u
+#define EDP_SEL_RCX(s) (0x52430000u | (uint32_t)(s))
+
 // uniform in (0,1), exactly representable: (x + 1/2) 2^-32
 __host__ __device__ inline double edp_u01(uint32_t x) { return ((double)x + 0.5) * 2.3283064365386962890625e-10; }
 
@@ -302,15 +326,17 @@ struct edp_mcc_out {
     int ion_species;
 };
 
-// Selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS as a per-electron Bernoulli(P_max) test on Philox stream 0,
-// block 0 = {select, kind r, density n, -}. Returns the kind variate r when selected.
+// Selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS as a per-electron Bernoulli(P_max) test. The per-particle
+// decision draws come from Philox2x32-10 (key = id, counter = {step, seed_lo ^ EDP_SEL_MCC}): word 0 is the
+// selection variate, word 1 the kind variate r. Returns r when selected.
 __device__ __forceinline__ bool edp_mcc_select(const edp_mcc_dev* m, uint32_t id, uint32_t step, uint32_t seed_lo,
                                                uint32_t seed_hi, double& r)
 {
-    uint32_t b0[4];
-    edp_philox(step, EDP_STREAM_MCC, 0u, seed_hi, id, seed_lo, b0);
-    if ((unsigned long long)b0[0] >= m->pmax_x) return false;
-    r = edp_u01(b0[1]);
+    (void)seed_hi;
+    uint32_t w[2];
+    edp_philox2x32(step, seed_lo ^ EDP_SEL_MCC, id, w);
+    if ((unsigned long long)w[0] >= m->pmax_x) return false;
+    r = edp_u01(w[1]);
     return true;
 }
 
@@ -415,13 +441,15 @@ __device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, u
         k2 = __dmul_rn(k, k);
     }
     double p2 = __dadd_rn(__dmul_rn(k2, vsq), r.pth2);
-    uint32_t b[4];
-    edp_philox(step, EDP_STREAM_RCX(species), 0u, seed_hi, id, seed_lo, b);
-    double u = edp_u01(b[0]);
+    uint32_t w[2];
+    edp_philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id, w);
+    double u = edp_u01(w[0]);
     if (!(__dmul_rn(u, u) <= p2)) return false;
-    vx = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[1])) * r.vfactor;
-    vy = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[2])) * r.vfactor;
-    vz = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[3])) * r.vfactor;
+    uint32_t b[4];
+    edp_philox(step, EDP_STREAM_RCX(species), 1u, seed_hi, id, seed_lo, b);
+    vx = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[0])) * r.vfactor;
+    vy = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[1])) * r.vfactor;
+    vz = edp_maxwell(r.maxwell_v, r.rmax, edp_u01(b[2])) * r.vfactor;
     return true;
 }
 

@@ -126,8 +126,16 @@ __device__ __forceinline__ void select_slot(const PushArgs& a, Smem& s, uint32_t
     else atomicOr(&a.dc->error_flags, EDP_EFLAG_PENDING);
 }
 
+// column offset inside a window; periodic domains have a power-of-two period (the FFT_X length)
+template <bool PER>
+__device__ __forceinline__ int win_dx(int d, const edp_kparams& kp)
+{
+    return PER ? (d & (kp.ncx - 1)) : d;
+}
+
 // One particle. Returns false when it was absorbed (the caller stores cell = -1).
-template <bool ION>
+// ION: ion species (acc_E, RCX) instead of electrons (E, MCC selection); PER: periodic x; ROT: Boris rotation.
+template <bool ION, bool PER, bool ROT>
 __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, DepAcc& acc,
                                          int& cell, float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id,
                                          uint32_t slot)
@@ -135,7 +143,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     const edp_kparams& kp = a.kp;
     int i = cell & 0xFFFF, j = cell >> 16;
     // ---- gather (bilinear, :82-86)
-    int lx = wrapx(i - wx0, kp), ly = j - wy0;
+    int lx = win_dx<PER>(i - wx0, kp), ly = j - wy0;
     float2 e00, e10, e01, e11;
     if (windowed && (unsigned)lx < EDP_WIN_CELLS && (unsigned)ly < EDP_WIN_CELLS) {
         int b = ly * EDP_WIN_NODES + lx;
@@ -145,7 +153,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         e11 = s.E[b + EDP_WIN_NODES + 1];
     } else {
         int i1 = i + 1;
-        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        if (PER && i1 == kp.ncx) i1 = 0;
         int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
         e00 = __ldg(&a.E[r0 + i]);
         e10 = __ldg(&a.E[r0 + i1]);
@@ -158,7 +166,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     float EY = e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11;
     // ---- Boris (:95-130 / ions :99-149)
     const float q = a.qh;
-    if (a.use_rot) {
+    if (ROT) {
         float mx = vx + q * EX, my = vy + q * EY, mz = vz + a.ez_term;
         float px = a.K[0] * mx + a.K[1] * my + a.K[2] * mz;
         float py = a.K[3] * mx + a.K[4] * my + a.K[5] * mz;
@@ -193,7 +201,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         }
     }
     // ---- domain boundaries (:174-511)
-    if (kp.periodic) {
+    if (PER) {
         if (ni < 0) ni += kp.ncx;
         else if (ni >= kp.ncx) ni -= kp.ncx;
         if (nj < 0) { atomicAdd(&s.cnt[0], 1ull); return false; }
@@ -214,12 +222,14 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     oy = ny;
     // ---- deposit (:1597-1639): exact FP64 weights of the FP32 offsets, rounded to 2^-32; the fourth weight
     // takes the remainder so that every particle deposits exactly 2^32 units
-    const double dx = (double)nx, dy = (double)ny;
-    const long long q00 = __double2ll_rn((1.0 - dx) * (1.0 - dy) * EDP_FIX_ONE);
-    const long long q10 = __double2ll_rn(dx * (1.0 - dy) * EDP_FIX_ONE);
-    const long long q01 = __double2ll_rn((1.0 - dx) * dy * EDP_FIX_ONE);
+    // (the 2^32 scaling is exact, so folding it into one factor rounds the same way)
+    const double dx = (double)nx, dy = (double)ny, mxd = 1.0 - dx;
+    const double A = (1.0 - dy) * EDP_FIX_ONE, B = dy * EDP_FIX_ONE;
+    const long long q00 = __double2ll_rn(mxd * A);
+    const long long q10 = __double2ll_rn(dx * A);
+    const long long q01 = __double2ll_rn(mxd * B);
     const long long q11 = 4294967296LL - q00 - q10 - q01;
-    const int dlx = wrapx(ni - wx0, kp), dly = nj - wy0;
+    const int dlx = win_dx<PER>(ni - wx0, kp), dly = nj - wy0;
     if (windowed && (unsigned)dlx < EDP_WIN_CELLS && (unsigned)dly < EDP_WIN_CELLS) {
         const int b = dly * EDP_WIN_NODES + dlx;
         if (b != acc.b) {
@@ -237,7 +247,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         }
     } else {
         int i1 = ni + 1;
-        if (kp.periodic && i1 == kp.ncx) i1 = 0;
+        if (PER && i1 == kp.ncx) i1 = 0;
         int64_t r0 = (int64_t)nj * kp.nxg, r1 = r0 + kp.nxg;
         atomicAdd(&a.rho[r0 + ni], (unsigned long long)q00);
         atomicAdd(&a.rho[r0 + i1], (unsigned long long)q10);
@@ -261,13 +271,15 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     return true;
 }
 
-// four consecutive slots [4g, 4g+4) restricted to [lo, hi)
-template <bool ION>
-__device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, int64_t g,
-                                           int64_t lo, int64_t hi)
+// four consecutive slots [4g, 4g+4). WIN: a sorted chunk, always whole groups (tiles are padded to multiples of
+// EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted to [lo, hi).
+template <bool ION, bool PER, bool ROT, bool WIN>
+__device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
+                                           int64_t hi)
 {
     const int64_t base = g * EDP_ITEMS;
-    const bool full = base >= lo && base + EDP_ITEMS <= hi;
+    const bool full = WIN || (base >= lo && base + EDP_ITEMS <= hi);
+    const bool windowed = WIN;
     int c[4];
     float ox[4], oy[4], vx[4], vy[4], vz[4];
     uint32_t id[4];
@@ -309,8 +321,8 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
 #pragma unroll
     for (int e = 0; e < EDP_ITEMS; ++e) {
         if (c[e] < 0) continue;
-        if (!push_one<ION>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                            (uint32_t)(base + e))) {
+        if (!push_one<ION, PER, ROT>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                                     (uint32_t)(base + e))) {
             c[e] = -1;
             atomicAdd(&s.cnt[17], 1ull);
         }
@@ -339,7 +351,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, bool wind
     }
 }
 
-template <bool ION>
+template <bool ION, bool PER, bool ROT>
 __global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArgs a)   // 64 registers, no spills
 {
     __shared__ Smem s;
@@ -370,12 +382,12 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArg
     __syncthreads();
     if (windowed) {
         for (int64_t g = lo / EDP_ITEMS + threadIdx.x; g * EDP_ITEMS < hi; g += blockDim.x)
-            push_group<ION>(a, s, true, wx0, wy0, g, lo, hi);
+            push_group<ION, PER, ROT, true>(a, s, wx0, wy0, g, lo, hi);
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
         int64_t g0 = lo / EDP_ITEMS;
         for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * EDP_ITEMS < hi; g += a.tail_ctas * blockDim.x)
-            push_group<ION>(a, s, false, 0, 0, g, lo, hi);
+            push_group<ION, PER, ROT, false>(a, s, 0, 0, g, lo, hi);
     }
     __syncthreads();
     if (windowed) {
@@ -882,8 +894,18 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         if (a.tail_ctas < 1) a.tail_ctas = 1;
         int64_t grid = a.n_chunks + a.tail_ctas;
         ++c->launches;
-        if (is_ion) push_mixed_kernel<true><<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
-        else push_mixed_kernel<false><<<(unsigned)grid, EDP_PUSH_THREADS, 0, c->stream>>>(a);
+        const unsigned gr = (unsigned)grid;
+        const int variant = (is_ion ? 4 : 0) | (c->kp.periodic ? 2 : 0) | (use_rot ? 1 : 0);
+        switch (variant) {
+        case 0: push_mixed_kernel<false, false, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 1: push_mixed_kernel<false, false, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 2: push_mixed_kernel<false, true, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 3: push_mixed_kernel<false, true, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 4: push_mixed_kernel<true, false, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 5: push_mixed_kernel<true, false, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        case 6: push_mixed_kernel<true, true, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        default: push_mixed_kernel<true, true, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        }
         if (do_mcc) {
             SelArgs b;
             memset(&b, 0, sizeof(b));

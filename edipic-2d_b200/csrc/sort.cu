@@ -1,7 +1,8 @@
 // Cell sort of the mixed-precision particle arrays (no reference analogue: EDIPIC-2D keeps particles in
 // arrival order). Counting sort on a tile-major cell key, so that every EDP_TILE x EDP_TILE tile is one
 // contiguous slot range and, inside it, particles of one cell are adjacent. Dead slots are dropped, which
-// is also the compaction of particles removed at walls since the last sort.
+// is also the compaction of particles removed at walls since the last sort. Each tile's range is padded with
+// dead slots to a multiple of EDP_ITEMS, so the push reads and writes every tile in whole 128-bit groups.
 #include <algorithm>
 #include <vector>
 
@@ -29,51 +30,73 @@ __global__ void hist_kernel(const int32_t* __restrict__ cell, const unsigned lon
     }
 }
 
-// exclusive scan, three phases: per-block scan (2048 keys), scan of block sums, add
-#define SCAN_BLOCK 2048
-__global__ void scan_local(const uint32_t* __restrict__ in, unsigned long long* __restrict__ out,
-                           unsigned long long* __restrict__ bsum, int64_t n)
+// exclusive scan of the 256 cell counts of one tile (one CTA per tile); tile_total[t] = live particles in it
+__global__ void tile_scan_kernel(const uint32_t* __restrict__ count, unsigned long long* __restrict__ local,
+                                 unsigned long long* __restrict__ tile_total)
 {
-    __shared__ unsigned long long s[SCAN_BLOCK];
-    const int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK;
-    for (int t = threadIdx.x; t < SCAN_BLOCK; t += blockDim.x) s[t] = (base + t < n) ? in[base + t] : 0ull;
+    __shared__ unsigned warp_sum[8];
+    const int t = blockIdx.x, k = threadIdx.x, lane = k & 31, w = k >> 5;
+    const unsigned v = count[(int64_t)t * 256 + k];
+    unsigned x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[w] = x;
     __syncthreads();
-    for (int off = 1; off < SCAN_BLOCK; off <<= 1) {
-        unsigned long long v[SCAN_BLOCK / 256];
-        int q = 0;
-        for (int t = threadIdx.x; t < SCAN_BLOCK; t += blockDim.x, ++q) v[q] = (t >= off) ? s[t - off] : 0ull;
-        __syncthreads();
-        q = 0;
-        for (int t = threadIdx.x; t < SCAN_BLOCK; t += blockDim.x, ++q) s[t] += v[q];
-        __syncthreads();
+    unsigned base = 0;
+    for (int q = 0; q < w; ++q) base += warp_sum[q];
+    local[(int64_t)t * 256 + k] = (unsigned long long)(base + x - v);
+    if (k == 255) tile_total[t] = (unsigned long long)(base + x);
+}
+
+// exclusive scan over the tiles of the padded tile sizes (one CTA); tile_base[ntiles] = padded total,
+// live = number of live particles
+__global__ void tiles_scan_kernel(const unsigned long long* __restrict__ tile_total, int64_t ntiles,
+                                  unsigned long long* __restrict__ tile_base, unsigned long long* live)
+{
+    __shared__ unsigned long long part[1024];
+    const int64_t per = (ntiles + blockDim.x - 1) / blockDim.x;
+    const int64_t t0 = threadIdx.x * per, t1 = min(t0 + per, ntiles);
+    unsigned long long s = 0, l = 0;
+    for (int64_t t = t0; t < t1; ++t) {
+        unsigned long long v = tile_total[t];
+        s += (v + (EDP_ITEMS - 1)) & ~(unsigned long long)(EDP_ITEMS - 1);
+        l += v;
     }
-    for (int t = threadIdx.x; t < SCAN_BLOCK; t += blockDim.x)
-        if (base + t < n) out[base + t] = (t == 0) ? 0ull : s[t - 1];
-    if (threadIdx.x == 0) bsum[blockIdx.x] = s[SCAN_BLOCK - 1];
-}
-
-__global__ void scan_sums(unsigned long long* bsum, int64_t nb, unsigned long long* total)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long acc = 0;
-    for (int64_t b = 0; b < nb; ++b) {
-        unsigned long long v = bsum[b];
-        bsum[b] = acc;
-        acc += v;
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long acc = 0;
+        for (int q = 0; q < (int)blockDim.x; ++q) {
+            unsigned long long v = part[q];
+            part[q] = acc;
+            acc += v;
+        }
+        tile_base[ntiles] = acc;
     }
-    *total = acc;
+    __syncthreads();
+    unsigned long long acc = part[threadIdx.x];
+    for (int64_t t = t0; t < t1; ++t) {
+        tile_base[t] = acc;
+        acc += (tile_total[t] + (EDP_ITEMS - 1)) & ~(unsigned long long)(EDP_ITEMS - 1);
+    }
+    // live total
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xFFFFFFFFu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(live, l);
 }
 
-__global__ void scan_add(unsigned long long* out, const unsigned long long* bsum, int64_t n)
+// scatter cursors = tile base + offset inside the tile; padding slots at each tile's end marked dead
+__global__ void cursor_kernel(const unsigned long long* __restrict__ local, const unsigned long long* __restrict__ tile_base,
+                              const unsigned long long* __restrict__ tile_total, int64_t ntiles,
+                              unsigned long long* __restrict__ cursor, int32_t* __restrict__ dst_cell)
 {
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) out[k] += bsum[k / SCAN_BLOCK];
-}
-
-__global__ void copy_u64(unsigned long long* dst, const unsigned long long* src, int64_t n)
-{
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) dst[k] = src[k];
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ntiles * 256) cursor[k] = tile_base[k >> 8] + local[k];
+    if (k < ntiles) {
+        const unsigned long long e = tile_base[k] + tile_total[k];
+        for (unsigned long long q = e; q < tile_base[k + 1]; ++q) dst_cell[q] = -1;
+    }
 }
 
 __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, const unsigned long long* n_slots,
@@ -103,18 +126,11 @@ __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, con
     }
 }
 
-__global__ void tile_starts(const unsigned long long* offset, int64_t ntiles, const unsigned long long* total,
-                            unsigned long long* out)
-{
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ntiles) out[t] = offset[t << 8];
-    if (t == ntiles) out[t] = *total;
-}
-
-__global__ void set_slots(unsigned long long* n_slots, unsigned long long* n_live, const unsigned long long* total)
+__global__ void set_slots(unsigned long long* n_slots, unsigned long long* n_live, const unsigned long long* total,
+                          const unsigned long long* live)
 {
     *n_slots = *total;
-    *n_live = *total;
+    *n_live = *live;
 }
 
 }  // namespace
@@ -126,34 +142,34 @@ int edp_launch_sort(edp_ctx* c, int sp)
     const int64_t nkeys = ntiles * 256;
     const int64_t nslots = std::max<int64_t>(c->host_slots[sp], 1);
     unsigned grid = (unsigned)std::min<int64_t>((nslots + 255) / 256, 148 * 16);
+    // scratch layout: tile_total[ntiles] | tile_base[ntiles+1] | cursor[nkeys] | live[1]
+    unsigned long long* tile_total = c->scan_tmp;
+    unsigned long long* tile_base = tile_total + ntiles;
+    unsigned long long* cursor = tile_base + ntiles + 1;
+    unsigned long long* live = cursor + nkeys;
     EDP_CUDA(c, cudaMemsetAsync(c->sort_count, 0, nkeys * sizeof(uint32_t), c->stream));
+    EDP_CUDA(c, cudaMemsetAsync(live, 0, sizeof(unsigned long long), c->stream));
     ++c->launches;
     hist_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp].cell, &c->dc->n_slots[sp], c->ntx, c->sort_count);
-    const int64_t nb = (nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK;
-    unsigned long long* bsum = c->scan_tmp;
-    unsigned long long* total = c->scan_tmp + nb;
-    unsigned long long* cursor = c->scan_tmp + nb + 1;
-    unsigned long long* starts = cursor + nkeys;
     ++c->launches;
-    scan_local<<<(unsigned)nb, 256, 0, c->stream>>>(c->sort_count, c->sort_offset, bsum, nkeys);
+    tile_scan_kernel<<<(unsigned)ntiles, 256, 0, c->stream>>>(c->sort_count, c->sort_offset, tile_total);
     ++c->launches;
-    scan_sums<<<1, 32, 0, c->stream>>>(bsum, nb, total);
+    tiles_scan_kernel<<<1, 1024, 0, c->stream>>>(tile_total, ntiles, tile_base, live);
     ++c->launches;
-    scan_add<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, bsum, nkeys);
-    ++c->launches;
-    copy_u64<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(cursor, c->sort_offset, nkeys);
+    cursor_kernel<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, tile_base, tile_total,
+                                                                           ntiles, cursor, c->pm_alt[sp].cell);
     ++c->launches;
     scatter_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp], c->pm_alt[sp], &c->dc->n_slots[sp], c->ntx, cursor);
     ++c->launches;
-    tile_starts<<<(unsigned)((ntiles + 1 + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, ntiles, total, starts);
-    ++c->launches;
-    set_slots<<<1, 1, 0, c->stream>>>(&c->dc->n_slots[sp], &c->dc->n_live[sp], total);
+    set_slots<<<1, 1, 0, c->stream>>>(&c->dc->n_slots[sp], &c->dc->n_live[sp], tile_base + ntiles, live);
     EDP_CUDA(c, cudaGetLastError());
     std::swap(c->pm[sp], c->pm_alt[sp]);
     std::vector<unsigned long long> h(ntiles + 1);
-    EDP_CUDA(c, cudaMemcpyAsync(h.data(), starts, (ntiles + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    EDP_CUDA(c, cudaMemcpyAsync(h.data(), tile_base, (ntiles + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if ((int64_t)h[ntiles] > c->cap[sp])
+        return edp_fail(c, EDP_ERR_CAPACITY, "sorted particles with tile padding exceed the capacity");
     std::vector<edp_chunk> ch;
     ch.reserve(ntiles * 2);
     for (int64_t t = 0; t < ntiles; ++t) {

@@ -57,6 +57,12 @@ inline void remove_particle(oracle_parts_t* p, int64_t k)
 
 inline double uniform(uint32_t x) { return ((double)x + 0.5) * 0x1p-32; }
 
+void philox_decision(uint32_t id, uint64_t seed, uint32_t step, uint32_t tag, uint32_t out[2])
+{
+    uint32_t ctr[2] = {step, (uint32_t)seed ^ tag};
+    oracle_philox2x32_10(ctr, id, out);
+}
+
 void philox_block(uint32_t id, uint64_t seed, uint32_t step, uint32_t stream, uint32_t block, uint32_t out[4])
 {
     uint32_t ctr[4] = {step, stream, block, (uint32_t)(seed >> 32)};
@@ -533,10 +539,10 @@ static void mcc_range(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, 
 {
     const double pmax = tab->max_colliding_fraction;
     for (int64_t k = lo; k < hi; ++k) {
-        uint32_t b0[4];
-        philox_block(e->id[k], c->seed, c->step, 0u, 0u, b0);
-        if (!(uniform(b0[0]) < pmax)) continue;
-        double r = uniform(b0[1]);
+        uint32_t w[2];
+        philox_decision(e->id[k], c->seed, c->step, 0x4D430000u, w);
+        if (!(uniform(w[0]) < pmax)) continue;
+        double r = uniform(w[1]);
         double vx = e->vx[k], vy = e->vy[k], vz = e->vz[k];
         double v2 = std::fma(vz, vz, std::fma(vy, vy, vx * vx));
         double en = v2 * c->energy_factor_eV;
@@ -624,13 +630,15 @@ int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint
         if (r->alpha != 0.0) l = 1.0 - r->alpha * std::log(std::max(vsq * r->factor_eV, 0.001));
         double kf = (r->prob_factor * ((r->sigma_1eV * l) * l)) * r->v_scale_ms;
         double p2 = (kf * kf) * vsq + pt2;
-        uint32_t b[4];
-        philox_block(ions->id[k], c->seed, c->step, 1u + (species << 8), 0u, b);
-        double u = uniform(b[0]);
+        uint32_t w[2];
+        philox_decision(ions->id[k], c->seed, c->step, 0x52430000u | species, w);
+        double u = uniform(w[0]);
         if (u * u <= p2) {
-            ions->vx[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[1])) * r->vfactor;
-            ions->vy[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[2])) * r->vfactor;
-            ions->vz[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[3])) * r->vfactor;
+            uint32_t b[4];
+            philox_block(ions->id[k], c->seed, c->step, 1u + (species << 8), 1u, b);
+            ions->vx[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[0])) * r->vfactor;
+            ions->vy[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[1])) * r->vfactor;
+            ions->vz[k] = oracle_maxwell_sample(c->maxwell_v, uniform(b[2])) * r->vfactor;
             ++count;
         }
     }

@@ -18,6 +18,7 @@ void   oracle_well_set_state(oracle_well_t* s, const uint32_t* words, int index)
 void   oracle_well_seed(oracle_well_t* s, int32_t seed);
 double oracle_well_next(oracle_well_t* s);
 void   oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void   oracle_philox2x32_10(const uint32_t ctr[2], uint32_t key, uint32_t out[2]);
 
 /* ---------------------------------------------------------------- geometry
  * Node (i,j) of the reference's cluster arrays, one cluster covering the whole domain.
@@ -109,8 +110,9 @@ int32_t oracle_en_scatter(int32_t kind, double energy_eV, double threshold_eV, d
                           double* v, double* new_e, double* new_i);
 
 /* Per-particle null-collision MCC driven by Philox4x32-10, the variate layout shared with the GPU kernels:
- *   key = {id, seed_lo}, counter = {step, stream, block, seed_hi}; u = (x + 0.5) * 2^-32.
- *   electrons, stream 0: block0 = {select, kind r, density n, -}, block1/2 = scattering variates.
+ *   decision draws: Philox2x32-10, key = id, counter = {step, seed_lo ^ 0x4D430000}: {select, kind r};
+ *   scattering variates: Philox4x32-10, key = {id, seed_lo}, counter = {step, 0, block 1/2, seed_hi};
+ *   u = (x + 0.5) * 2^-32.
  * Ionisation products are appended to *born_e / *born_i (capacity checked). counters[k] counts kind k+1. */
 typedef struct {
     uint64_t seed;
@@ -123,8 +125,9 @@ typedef struct {
 void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
                        oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters);
 
-/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126), Philox stream 1, block0 =
- * {hit, Mx, My, Mz}. Returns the number of exchanges. */
+/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126): hit variate from Philox2x32-10
+ * (key = id, counter = {step, seed_lo ^ (0x52430000 | species)}), Maxwellian from Philox4x32-10 block 1 of stream
+ * 1 + (species << 8). Returns the number of exchanges. */
 typedef struct {
     double prob_factor;        /* ngas * dt * N_subcycles */
     double v_scale_ms;

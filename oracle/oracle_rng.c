@@ -108,3 +108,20 @@ void oracle_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], ui
     }
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
+
+/* Philox2x32-10 of the same paper: 64-bit counter, 32-bit key, multiplier 0xD256D193, Weyl increment
+ * 0x9E3779B9. The device cycle uses it for the per-particle decision draws. */
+void oracle_philox2x32_10(const uint32_t ctr_in[2], uint32_t key, uint32_t out[2])
+{
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], k = key;
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi, lo;
+        mulhilo(0xD256D193u, c0, &hi, &lo);
+        uint32_t n0 = hi ^ k ^ c1;
+        c1 = lo;
+        c0 = n0;
+        k += 0x9E3779B9u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+}

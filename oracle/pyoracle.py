@@ -82,6 +82,7 @@ def lib():
             "oracle_well_seed": ([C.POINTER(Well), C.c_int32], None),
             "oracle_well_next": ([C.POINTER(Well)], C.c_double),
             "oracle_philox4x32_10": ([_U32, _U32, _U32], None),
+            "oracle_philox2x32_10": ([_U32, C.c_uint32, _U32], None),
             "oracle_nx_nodes": ([C.POINTER(Geom)], C.c_int32),
             "oracle_push": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
@@ -125,6 +126,12 @@ def well_stream(seed, n):
 def philox(ctr, key):
     out = (C.c_uint32 * 4)()
     lib().oracle_philox4x32_10((C.c_uint32 * 4)(*ctr), (C.c_uint32 * 2)(*key), out)
+    return tuple(out)
+
+
+def philox2x32(ctr, key):
+    out = (C.c_uint32 * 2)()
+    lib().oracle_philox2x32_10((C.c_uint32 * 2)(*ctr), key, out)
     return tuple(out)
 
 

@@ -45,3 +45,12 @@ def test_well_range():
 ])
 def test_philox_known_answers(ctr, key, expect):
     assert pyoracle.philox(ctr, key) == expect
+
+
+@pytest.mark.parametrize("ctr,key,expect", [
+    ((0, 0), 0, (0xff1dae59, 0x6cd10df2)),
+    ((0xffffffff, 0xffffffff), 0xffffffff, (0x2c3f628b, 0xab4fd7ad)),
+    ((0x243f6a88, 0x85a308d3), 0x13198a2e, (0xdd7ce038, 0xf62a4c12)),
+])
+def test_philox2x32_known_answers(ctr, key, expect):
+    assert pyoracle.philox2x32(ctr, key) == expect
