@@ -140,8 +140,8 @@ int alloc_species(edp_ctx* c, int sp, int64_t n)
         // add lists for ionisation products: a small fraction of the electron capacity
         int64_t bc = std::max<int64_t>(65536, cap / 64);
         c->born_cap = bc;
-        for (int b = 0; b < 2; ++b) {
-            edp_born& e = c->pend_e[b];
+        {
+            edp_born& e = c->born_e;
             e.cap = bc;
             TRY(dalloc(c, &e.x, bc));
             TRY(dalloc(c, &e.y, bc));
@@ -158,13 +158,11 @@ int alloc_species(edp_ctx* c, int sp, int64_t n)
             TRY(dalloc(c, &e.vy, bc));
             TRY(dalloc(c, &e.vz, bc));
         }
-        edp_born_dev h[2];
-        for (int b = 0; b < 2; ++b) {
-            h[b].pend_next = c->pend_e[b];
-            for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) h[b].born_i[s] = c->born_i[s];
-        }
-        TRY(dalloc(c, &c->born_dev, 2));
-        EDP_CUDA(c, cudaMemcpy(c->born_dev, h, sizeof(h), cudaMemcpyHostToDevice));
+        edp_born_dev h;
+        h.born_e = c->born_e;
+        for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) h.born_i[s] = c->born_i[s];
+        TRY(dalloc(c, &c->born_dev, 1));
+        EDP_CUDA(c, cudaMemcpy(c->born_dev, &h, sizeof(h), cudaMemcpyHostToDevice));
         // selection list of the fused collision test: P_max of the electrons on average, with headroom
         double pm = c->tab.en_on ? c->tab.max_colliding_fraction : 0.0;
         c->sel_cap = std::max<int64_t>(65536, (int64_t)((double)cap * std::min(1.0, 2.0 * pm + 0.01)));
@@ -401,14 +399,9 @@ __global__ void mcc_choose_kernel(edp_mcc_dev m, int64_t n, const double* E, con
         out[k] = edp_mcc_choose_dev(m, E[k], r[k]);
 }
 
-__global__ void rotate_pending_kernel(edp_dev_counters* dc, int n_ion)
+__global__ void reset_born_kernel(edp_dev_counters* dc)
 {
-    dc->pend_e_count[1] = dc->pend_e_count[0];
-    dc->pend_e_count[0] = 0ull;
-}
-
-__global__ void reset_born_ions_kernel(edp_dev_counters* dc)
-{
+    dc->born_e_count = 0ull;
     for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) dc->born_i_count[s] = 0ull;
 }
 
@@ -656,8 +649,8 @@ int edp_destroy(edp_ctx* c)
         F(c->rho_fix[s]);
         F(c->rho_d[s]);
     }
-    for (int b = 0; b < 2; ++b) {
-        edp_born& e = c->pend_e[b];
+    {
+        edp_born& e = c->born_e;
         F(e.x); F(e.y); F(e.vx); F(e.vy); F(e.vz);
     }
     for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) {
@@ -924,7 +917,6 @@ int edp_advance_electrons(edp_ctx* c)
     reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
     TRY(zero_density(c, 0));
     TRY(edp_launch_push(c, 0, ion_step, fuse));
-    TRY(edp_launch_append_pending(c, ion_step && fuse));
     return finish_sync(c);
 }
 
@@ -978,9 +970,10 @@ int edp_end_ion_cycle(edp_ctx* c)
     const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
     if (ion_step) {
-        TRY(edp_launch_append_born_ions(c));
+        // collisions run only on ion steps, so only then can the add lists hold anything
+        TRY(edp_launch_append_born(c));
         ++c->launches;
-        reset_born_ions_kernel<<<1, 1, 0, c->stream>>>(c->dc);
+        reset_born_kernel<<<1, 1, 0, c->stream>>>(c->dc);
         if (c->p.precision == EDP_PREC_MIXED) {
             EDP_CUDA(c, cudaMemsetAsync(c->acc2, 0, nn * sizeof(float2), c->stream));
         } else {
@@ -991,10 +984,7 @@ int edp_end_ion_cycle(edp_ctx* c)
     } else {
         c->n_sub_phase++;
     }
-    ++c->launches;
-    rotate_pending_kernel<<<1, 1, 0, c->stream>>>(c->dc, c->p.n_ion_species);
     EDP_CUDA(c, cudaGetLastError());
-    c->pend_cur ^= 1;
     c->t_cntr++;
     c->steps_since_sort++;
     if (c->p.precision == EDP_PREC_MIXED && c->p.sort_every > 0 && c->steps_since_sort >= c->p.sort_every &&

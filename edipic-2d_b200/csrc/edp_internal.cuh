@@ -45,7 +45,7 @@ struct edp_dev_counters {
     unsigned long long en_coll_step[EDP_MAX_COLPROC];
     unsigned long long rcx[EDP_MAX_ION_SPECIES];
     unsigned long long rcx_step[EDP_MAX_ION_SPECIES];
-    unsigned long long pend_e_count[2];            // electrons born by ionisation (double buffer)
+    unsigned long long born_e_count;               // electrons born by ionisation this step
     unsigned long long born_i_count[EDP_MAX_ION_SPECIES];
     unsigned long long next_id[EDP_MAX_SPECIES];
     unsigned int error_flags;
@@ -74,9 +74,9 @@ struct edp_born {
 
 struct edp_mcc_dev;
 
-// add lists as seen by the kernels: the electron list filled this step and the ion lists
+// add lists as seen by the kernels
 struct edp_born_dev {
-    edp_born pend_next;
+    edp_born born_e;
     edp_born born_i[EDP_MAX_ION_SPECIES];
 };
 
@@ -108,8 +108,7 @@ struct edp_ctx {
     // particles
     edp_species_mixed pm[EDP_MAX_SPECIES], pm_alt[EDP_MAX_SPECIES];
     edp_species_fp64 pd[EDP_MAX_SPECIES];
-    edp_born pend_e[2];           // [cur] appended this step, [cur^1] filled this step
-    int pend_cur = 0;
+    edp_born born_e;              // ionisation electrons of this step (joined at the end of the step)
     edp_born born_i[EDP_MAX_ION_SPECIES];
     int64_t born_cap = 0;
 
@@ -146,7 +145,7 @@ struct edp_ctx {
     double* mcc_energy = nullptr;
     double* maxwell_v = nullptr;
     edp_mcc_dev* mcc_dev = nullptr;  // device copy of the collision table descriptor
-    edp_born_dev* born_dev = nullptr; // [2]: add-list descriptors for pend_cur^1 == 0 and == 1
+    edp_born_dev* born_dev = nullptr; // device copy of the add-list descriptors
     uint32_t* sel_list = nullptr;     // electron slots selected for a collision in the fused push
     unsigned long long* sel_count = nullptr;
     int64_t sel_cap = 0;
@@ -469,8 +468,7 @@ edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
 int edp_launch_push(edp_ctx* c, int species, bool ion_step, bool fuse);
 int edp_launch_collide_en(edp_ctx* c);
 int edp_launch_collide_rcx(edp_ctx* c);
-int edp_launch_append_pending(edp_ctx* c, bool ion_step);
-int edp_launch_append_born_ions(edp_ctx* c);
+int edp_launch_append_born(edp_ctx* c);
 int edp_launch_sort(edp_ctx* c, int species);
 int edp_launch_density(edp_ctx* c);
 int edp_launch_fftx(edp_ctx* c);

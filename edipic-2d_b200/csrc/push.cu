@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(256) collide_selected_kernel(SelArgs a)
             const int c = a.P.cell[slot];
             const double X = (double)(c & 0xFFFF) + (double)a.P.ox[slot];
             const double Y = (double)(c >> 16) + (double)a.P.oy[slot];
-            record_born(a.born->pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+            record_born(a.born->born_e, &a.dc->born_e_count, &a.dc->error_flags, X, Y, o.ne);
             record_born(a.born->born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y,
                         o.ni);
         }
@@ -495,7 +495,7 @@ struct PushArgs64 {
     const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
-    edp_born pend_next;
+    edp_born born_e;
     edp_born born_i[EDP_MAX_ION_SPECIES];
 };
 
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             if (o.kind_index) {
                 atomicAdd(&cnt[8 + o.kind_index - 1], 1ull);
                 if (o.born) {
-                    record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+                    record_born(a.born_e, &a.dc->born_e_count, &a.dc->error_flags, X, Y, o.ne);
                     record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags,
                                 X, Y, o.ni);
                 }
@@ -633,7 +633,7 @@ struct CollArgs {
     const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
-    edp_born pend_next;
+    edp_born born_e;
     edp_born born_i[EDP_MAX_ION_SPECIES];
 };
 
@@ -678,7 +678,7 @@ __global__ void collide_en_kernel(CollArgs a)
             a.Pd.vz[k] = vz;
         }
         if (o.born) {
-            record_born(a.pend_next, &a.dc->pend_e_count[0], &a.dc->error_flags, X, Y, o.ne);
+            record_born(a.born_e, &a.dc->born_e_count, &a.dc->error_flags, X, Y, o.ne);
             record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags, X, Y, o.ni);
         }
     }
@@ -734,7 +734,7 @@ __global__ void collide_rcx_kernel(CollArgs a)
 // ------------------------------------------------------------------------------------- appending
 struct AppendArgs {
     edp_kparams kp;
-    int precision, species, do_mcc;
+    int precision, species;
     edp_species_mixed Pm;
     edp_species_fp64 Pd;
     int64_t cap;
@@ -745,20 +745,15 @@ struct AppendArgs {
     unsigned long long* next_id;
     unsigned long long* rho_fix;
     double* rho_d;
-    uint32_t step;
-    const edp_mcc_dev* mcc;
     edp_dev_counters* dc;
-    edp_born pend_next;
-    edp_born born_i[EDP_MAX_ION_SPECIES];
 };
 
-// PROCESS_ADDED_ELECTRONS / PROCESS_ADDED_IONS (pic2d_ElectronDynamics.f90:1429-1531, pic2d_IonDynamics.f90:1468-1537):
-// the add list joins the main array and is deposited; added electrons take part in this step's MCC.
+// PROCESS_ADDED_ELECTRONS / PROCESS_ADDED_IONS (pic2d_ElectronDynamics.f90:1429-1531,
+// pic2d_IonDynamics.f90:1468-1537), called at the end of the step (pic2d_MainProgram.f90:300, :363): the add list
+// joins the main array and is deposited at its birth positions into the density the next step's field solve uses
+// (the density GATHER_*_CHARGE_DENSITY takes at the start of the next step).
 __global__ void append_kernel(AppendArgs a)
 {
-    __shared__ unsigned long long cnt[EDP_MAX_COLPROC];
-    if (threadIdx.x < EDP_MAX_COLPROC) cnt[threadIdx.x] = 0ull;
-    __syncthreads();
     const edp_kparams& kp = a.kp;
     const int64_t n = (int64_t)*a.src_count;
     const int64_t nread = n < a.src.cap ? n : a.src.cap;
@@ -766,17 +761,6 @@ __global__ void append_kernel(AppendArgs a)
         double X = a.src.x[k], Y = a.src.y[k];
         double vx = a.src.vx[k], vy = a.src.vy[k], vz = a.src.vz[k];
         uint32_t id = (uint32_t)atomicAdd(a.next_id, 1ull);
-        if (a.do_mcc) {
-            edp_mcc_out o = edp_mcc_electron(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, vx, vy, vz);
-            if (o.kind_index) {
-                atomicAdd(&cnt[o.kind_index - 1], 1ull);
-                if (o.born) {
-                    record_born(a.pend_next, &a.dc->pend_e_count[1], &a.dc->error_flags, X, Y, o.ne);
-                    record_born(a.born_i[o.ion_species], &a.dc->born_i_count[o.ion_species], &a.dc->error_flags,
-                                X, Y, o.ni);
-                }
-            }
-        }
         unsigned long long slot = atomicAdd(a.n_slots, 1ull);
         if ((int64_t)slot >= a.cap) {
             atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
@@ -791,7 +775,7 @@ __global__ void append_kernel(AppendArgs a)
         if (!kp.periodic && (int)X == kp.ncx) dx = 1.0;
         int i1 = i + 1;
         if (kp.periodic && i1 == kp.ncx) i1 = 0;
-        int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
+    int64_t r0 = (int64_t)j * kp.nxg, r1 = r0 + kp.nxg;
         if (a.precision == EDP_PREC_MIXED) {
             float fx = (float)dx, fy = (float)dy;
             a.Pm.cell[slot] = (j << 16) | i;
@@ -825,11 +809,6 @@ __global__ void append_kernel(AppendArgs a)
             atomicAdd(&a.rho_d[r1 + i1], 1.0 - vij - vip1j - vijp1);
         }
     }
-    __syncthreads();
-    if (threadIdx.x < EDP_MAX_COLPROC && cnt[threadIdx.x]) {
-        atomicAdd(&a.dc->en_coll[threadIdx.x], cnt[threadIdx.x]);
-        atomicAdd(&a.dc->en_coll_step[threadIdx.x], cnt[threadIdx.x]);
-    }
 }
 
 void fill_rot(const edp_ctx* c, int species, float* Kf, double* Kd)
@@ -860,7 +839,6 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
     }
     const bool do_mcc = fuse && !is_ion && ion_step && c->tab.en_on;
     const bool do_rcx = fuse && is_ion && ion_step && c->tab.rcx_on[s];
-    const int pn = c->pend_cur ^ 1;
     if (p.precision == EDP_PREC_MIXED) {
         PushArgs a;
         memset(&a, 0, sizeof(a));
@@ -916,7 +894,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
             b.sel_cap = c->sel_cap;
             b.step = (uint32_t)c->t_cntr;
             b.mcc = c->mcc_dev;
-            b.born = c->born_dev + pn;
+            b.born = c->born_dev;
             b.dc = c->dc;
             ++c->launches;
             collide_selected_kernel<<<148 * 4, 256, 0, c->stream>>>(b);
@@ -943,7 +921,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.mcc = c->mcc_dev;
         if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
         a.dc = c->dc;
-        a.pend_next = c->pend_e[pn];
+        a.born_e = c->born_e;
         for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
         int64_t n = c->host_slots[sp];
         int64_t grid = (n + 255) / 256;
@@ -968,7 +946,7 @@ static CollArgs coll_args(edp_ctx* c, int sp)
     a.n_slots = &c->dc->n_slots[sp];
     a.step = (uint32_t)c->t_cntr;
     a.dc = c->dc;
-    a.pend_next = c->pend_e[c->pend_cur ^ 1];
+    a.born_e = c->born_e;
     for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
     return a;
 }
@@ -1020,33 +998,16 @@ static AppendArgs append_args(edp_ctx* c, int sp)
     a.next_id = &c->dc->next_id[sp];
     a.rho_fix = c->rho_fix[sp];
     a.rho_d = c->rho_d[sp];
-    a.step = (uint32_t)c->t_cntr;
     a.dc = c->dc;
-    for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
     return a;
 }
 
-// electrons born last step join the array after this step's push (PROCESS_ADDED_ELECTRONS, MainProgram:259/:316)
-int edp_launch_append_pending(edp_ctx* c, bool ion_step)
-{
-    const int cur = c->pend_cur;
-    AppendArgs a = append_args(c, 0);
-    a.src = c->pend_e[cur];
-    a.src_count = &c->dc->pend_e_count[1];   // the list filled during the previous step
-    a.do_mcc = ion_step && c->tab.en_on;
-    a.mcc = c->mcc_dev;
-    // electrons born from these go to the list being filled this step, counted in pend_e_count[0]
-    a.pend_next = c->pend_e[cur ^ 1];
-    ++c->launches;
-    append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
-    EDP_CUDA(c, cudaGetLastError());
-    c->host_slots[0] += c->born_cap;
-    return EDP_OK;
-}
-
-int edp_launch_append_born_ions(edp_ctx* c)
+// the add lists of this step's ionisations join their arrays: ions (PROCESS_ADDED_IONS, pic2d_MainProgram.f90:300),
+// then electrons (PROCESS_ADDED_ELECTRONS, :363)
+int edp_launch_append_born(edp_ctx* c)
 {
     for (int s = 0; s < c->p.n_ion_species; ++s) {
+        if (!c->uploaded[1 + s]) continue;
         AppendArgs a = append_args(c, 1 + s);
         a.src = c->born_i[s];
         a.src_count = &c->dc->born_i_count[s];
@@ -1055,5 +1016,12 @@ int edp_launch_append_born_ions(edp_ctx* c)
         EDP_CUDA(c, cudaGetLastError());
         c->host_slots[1 + s] += c->born_cap;
     }
+    AppendArgs a = append_args(c, 0);
+    a.src = c->born_e;
+    a.src_count = &c->dc->born_e_count;
+    ++c->launches;
+    append_kernel<<<148 * 2, 256, 0, c->stream>>>(a);
+    EDP_CUDA(c, cudaGetLastError());
+    c->host_slots[0] += c->born_cap;
     return EDP_OK;
 }

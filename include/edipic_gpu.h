@@ -188,8 +188,10 @@ int edp_advance_ions(edp_ctx* ctx);
 int edp_collide_en(edp_ctx* ctx, int64_t* counters_out);
 /* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126) */
 int edp_collide_rcx(edp_ctx* ctx, int64_t* count_out);
-/* PROCESS_ADDED_IONS + CLEAR_ACCUMULATED_FIELDS (pic2d_IonDynamics.f90:1468-1537,
- * pic2d_ElectricFieldCalc_PETSc.F90:809-829): appends ions born this step, clears acc_E, advances T_cntr */
+/* End of a time step, called every step. On ion steps: PROCESS_ADDED_IONS (pic2d_MainProgram.f90:300,
+ * pic2d_IonDynamics.f90:1468-1537), CLEAR_ACCUMULATED_FIELDS (:306, pic2d_ElectricFieldCalc_PETSc.F90:809-829) and
+ * PROCESS_ADDED_ELECTRONS (:363, pic2d_ElectronDynamics.f90:1429-1531): the ions and electrons born by this step's
+ * ionisations join their arrays and the next step's density. Every step: advances T_cntr and runs the periodic sort. */
 int edp_end_ion_cycle(edp_ctx* ctx);
 /* One or more whole steps of pic2d_MainProgram.f90:151-309 in order (convenience for drivers). */
 int edp_step(edp_ctx* ctx, int32_t nsteps);

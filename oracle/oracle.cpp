@@ -962,13 +962,8 @@ int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* 
     // SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:182-191); acc_E == E for N_sub = 1
     oracle_fftx_solve(g, rho, c->phi_bottom, c->phi_top, phi);
     oracle_efield(g, phi, c->factor2_E, c->factor1_E, ex, ey, nullptr, nullptr);
-    // ADVANCE_ELECTRONS_PLUS (:210), then the add list left by the previous step's ionisation joins the array
+    // ADVANCE_ELECTRONS_PLUS (:210)
     push_threads(g, &c->e_sp, ex, ey, e, counters + 8, c->nthreads);
-    for (int64_t k = 0; k < c->pend_e.n && e->n < cap_e; ++k) {
-        double v[3] = {c->pend_e.vx[k], c->pend_e.vy[k], c->pend_e.vz[k]};
-        append(e, cap_e, c->pend_e.x[k], c->pend_e.y[k], v, c->pend_e.id[k]);
-    }
-    c->pend_e.n = 0;
     // ADVANCE_IONS_PLUS (:231)
     push_threads(g, &c->i_sp, ex, ey, ion, counters + 8, c->nthreads);
     // PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:275), PERFORM_RESONANT_CHARGE_EXCHANGE (:287)
@@ -976,14 +971,14 @@ int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* 
     c->born_i.n = 0;
     if (c->mcc) oracle_mcc_philox(c->mcc, &c->mcc_ctx, e, &c->born_e, &c->born_i, c->cap_born, counters);
     if (c->rcx_on) counters[4] += oracle_rcx_philox(&c->rcx, &c->mcc_ctx, 0u, ion);
-    // PROCESS_ADDED_IONS (:300); born electrons wait in the add list for one step
+    // PROCESS_ADDED_IONS (:300), then PROCESS_ADDED_ELECTRONS (:363)
     for (int64_t k = 0; k < c->born_i.n; ++k) {
         double v[3] = {c->born_i.vx[k], c->born_i.vy[k], c->born_i.vz[k]};
-        append(ion, cap_i, c->born_i.x[k], c->born_i.y[k], v, c->born_i.id[k]);
+        append(ion, cap_i, c->born_i.x[k], c->born_i.y[k], v, c->next_id_i++);
     }
     for (int64_t k = 0; k < c->born_e.n; ++k) {
         double v[3] = {c->born_e.vx[k], c->born_e.vy[k], c->born_e.vz[k]};
-        append(&c->pend_e, c->cap_born, c->born_e.x[k], c->born_e.y[k], v, c->born_e.id[k]);
+        append(e, cap_e, c->born_e.x[k], c->born_e.y[k], v, c->next_id_e++);
     }
     c->mcc_ctx.step++;
     return processed;

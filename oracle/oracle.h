@@ -172,14 +172,15 @@ typedef struct {
     oracle_rcx_t rcx;
     int32_t rcx_on;
     int32_t nthreads;
-    /* electrons born by ionisation wait one step in an add list before they join the main array
-       (they are appended by PROCESS_ADDED_ELECTRONS of the next step, pic2d_MainProgram.f90:259/:316) */
-    oracle_parts_t pend_e, born_e, born_i;
+    /* add lists of this step's ionisations; both join their arrays at the end of the step
+       (PROCESS_ADDED_IONS, pic2d_MainProgram.f90:300; PROCESS_ADDED_ELECTRONS, :363) */
+    oracle_parts_t born_e, born_i;
     int64_t cap_born;
+    uint32_t next_id_e, next_id_i;  /* id of the next particle that joins (max id + 1 at the start) */
 } oracle_cycle_t;
 
-/* one electron+ion step with N_subcycles == 1 in the order of pic2d_MainProgram.f90:151-309:
- * gather densities, FFT_X solve, E, push electrons, push ions, MCC, RCX, append born particles.
+/* one electron+ion step with N_subcycles == 1 in the order of pic2d_MainProgram.f90:151-363:
+ * gather densities, FFT_X solve, E, push electrons, push ions, MCC, RCX, append born ions, append born electrons.
  * Particle arrays must have room for the appended particles (cap). Returns particles processed. */
 int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* i, int64_t cap_e, int64_t cap_i,
                           double* work /* 7 * node grid */, int64_t* counters /* [16] */);

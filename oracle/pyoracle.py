@@ -66,7 +66,8 @@ class Cycle(C.Structure):
                 ("ion_charge", C.c_double), ("factor2_E", C.c_double), ("factor1_E", C.c_double),
                 ("phi_bottom", C.c_double), ("phi_top", C.c_double), ("mcc", C.POINTER(MccTable)),
                 ("mcc_ctx", MccCtx), ("rcx", Rcx), ("rcx_on", C.c_int32), ("nthreads", C.c_int32),
-                ("pend_e", Parts), ("born_e", Parts), ("born_i", Parts), ("cap_born", C.c_int64)]
+                ("born_e", Parts), ("born_i", Parts), ("cap_born", C.c_int64),
+                ("next_id_e", C.c_uint32), ("next_id_i", C.c_uint32)]
 
 
 _lib = None
@@ -305,7 +306,7 @@ class OracleCycle:
         self.pi = ParticleSet(*ions[:5], ids=ions[5] if len(ions) > 5 else None, cap=int(n_i * cap_factor) + 1024)
         nb = max(n_e // 4, 4096)
         mk = lambda: ParticleSet(*(np.zeros(0),) * 5, cap=nb)
-        self.pend, self.be, self.bi = mk(), mk(), mk()
+        self.be, self.bi = mk(), mk()
         self.neu = read_neutral_deck(deck_dir)
         self.mcc = MccTables(self.neu, p.n_subcycles, p.delta_t_s)
         self.mv, _ = maxwell_tables()
@@ -327,7 +328,9 @@ class OracleCycle:
                     t.rcx_alpha, t.rcx_probab_thermal[0], t.rcx_vfactor[0])
         c.rcx_on = int(t.rcx_on[0])
         c.nthreads = nthreads
-        c.pend_e, c.born_e, c.born_i, c.cap_born = self.pend.s, self.be.s, self.bi.s, nb
+        c.born_e, c.born_i, c.cap_born = self.be.s, self.bi.s, nb
+        c.next_id_e = int(self.pe.id[:n_e].max()) + 1 if n_e else 0
+        c.next_id_i = int(self.pi.id[:n_i].max()) + 1 if n_i else 0
         self.c = c
         ny, nx = nodes_shape(g)
         self.work = np.zeros(7 * nx * ny)
