@@ -132,6 +132,73 @@ def cpu_baseline(args, deck_dir, seconds=15.0):
                       f"{el:.1f} s, FP64 oracle cycle incl. FFT_X"}
 
 
+def fp64_cycle_leg(args, stream_of):
+    """The same workload through the plain FP64 device path (84 B per particle-step, no sort): the comparison the
+    mixed-precision cycle is quoted against."""
+    from edipic_b200 import PREC_FP64, Simulation, decks
+    import torch
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc)
+        with Simulation(d, precision=PREC_FP64, sort_every=0, fuse_collisions=True, seed=1000) as sim:
+            sim.distribute_particles(args.ppc)
+            stream = stream_of(sim)
+            for _ in range(3):
+                sim.step(1)
+            c0 = sim.counters()
+            steps = 10
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            sim.step(steps)
+            b.record(stream)
+            b.synchronize()
+            t = a.elapsed_time(b) / 1e3
+            c1 = sim.counters()
+    n = 0.5 * (c0.n_particles[0] + c0.n_particles[1] + c1.n_particles[0] + c1.n_particles[1])
+    return {"value": n * steps / t, "unit": "particle-steps/s", "ms_per_step": 1e3 * t / steps, "steps": steps,
+            "path": "FP64 particles and FP64 atomic deposit, same kernels' FP64 variants, whole cycle incl. FFT_X"}
+
+
+def poisson_leg(args, stream_of, warmup=10, steps=30):
+    """Poisson ms/step on the inner-object geometry (512 x 512 cells, metal walls at 0 V, a 64 x 32-cell metal
+    rectangle at -100 V centred at (256, 128), 100 e- + 100 Ar+ per cell, the full collision set): each step of the
+    cycle solves with CG to a 1e-8 relative residual from the previous step's potential. Timed by CUDA events
+    around each solve (density, CG with its convergence reads, E)."""
+    from edipic_b200 import PRECOND_MG, PRECOND_NONE, Simulation, decks
+    import torch
+    out = {"workload": "cfg2: 512x512 cells, inner metal rectangle 64x32 cells at -100 V, 100+100 per cell, "
+                       "CG to 1e-8 relative residual, previous-step warm start", "rtol": 1e-8}
+    for name, pc in (("plain_mg", PRECOND_MG), ("plain_nopc", PRECOND_NONE)):
+        with tempfile.TemporaryDirectory() as tmp:
+            d = decks.write_deck(tmp, "cfg2")
+            with Simulation(d, sort_every=20, fuse_collisions=True, seed=2000) as sim:
+                sim.set_cg_preconditioner(pc)
+                sim.distribute_particles(100)
+                stream = stream_of(sim)
+                lib, ctx, chk = sim.lib, sim.ctx, sim._check
+                it = C.c_int32()
+                times, iters = [], []
+                for k in range(warmup + steps):
+                    chk(lib.edp_update_wall_potentials(ctx, k), "wall")
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    chk(lib.edp_field_cg(ctx, 1e-8, 200000, 1, C.byref(it)), "cg")
+                    b.record(stream)
+                    chk(lib.edp_advance_electrons(ctx), "adv_e")
+                    chk(lib.edp_advance_ions(ctx), "adv_i")
+                    chk(lib.edp_collide_en(ctx, None), "en")
+                    chk(lib.edp_collide_rcx(ctx, None), "rcx")
+                    chk(lib.edp_end_ion_cycle(ctx), "end")
+                    if k >= warmup:
+                        b.synchronize()
+                        times.append(a.elapsed_time(b))
+                        iters.append(it.value)
+        out[name] = {"ms_per_step": sum(times) / len(times), "cg_iterations_mean": sum(iters) / len(iters),
+                     "cg_iterations_max": max(iters), "steps": steps,
+                     "preconditioner": "multigrid V(2,2) RB-GS" if pc == PRECOND_MG else "none (Jacobi = plain)"}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -300,10 +367,19 @@ def run_ours(args):
                     "d2h_bytes_per_step": 8 * 8 + 8,
                     "path": "C ABI call sequence of the Fortran host with per-step counter reads"},
         }
+    sim.close()
+    if rank == 0:
+        def stream_of(s):
+            ptr = C.c_void_p()
+            s.lib.edp_get_stream(s.ctx, C.byref(ptr))
+            return torch.cuda.ExternalStream(ptr.value)
+        if not args.no_extra_legs and world == 1:
+            line["fp64_gpu_cycle"] = fp64_cycle_leg(args, stream_of)
+            line["fp64_gpu_cycle"]["mixed_over_fp64"] = value / line["fp64_gpu_cycle"]["value"]
+            line["poisson"] = poisson_leg(args, stream_of)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args, d)
         print(json.dumps(line), flush=True)
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -321,6 +397,7 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--sort-every", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true", help="skip the FP64-cycle and Poisson legs")
     args = ap.parse_args()
     from edipic_b200 import decks
     cfg = decks.CONFIGS[args.config]

@@ -626,6 +626,7 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
         cudaMemcpy(c->mcc_dev, &m, sizeof(m), cudaMemcpyHostToDevice);
     }
     if ((r = edp_fields_prepare(c))) return fail(r);
+    if (p->solver == EDP_SOLVER_CG && (r = edp_mg_setup(c))) return fail(r);
     for (int s = 0; s < 4; ++s) c->phi_wall[s] = p->wall_phi_const[s] + p->wall_phi_var[s] * std::sin(p->wall_phase[s]);
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDP_ERR_CUDA);
     *out = c;
@@ -661,6 +662,7 @@ int edp_destroy(edp_ctx* c)
     F(c->E2); F(c->acc2); F(c->Ex); F(c->Ey); F(c->accx); F(c->accy);
     F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
     F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
+    edp_mg_free(c);
     F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v);
     F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
@@ -892,6 +894,14 @@ int edp_field_fftx(edp_ctx* c, double* phi_out)
     TRY(edp_launch_efield(c));
     if (phi_out) TRY(edp_get_field(c, EDP_FIELD_PHI, phi_out));
     return finish_sync(c);
+}
+
+int edp_set_cg_preconditioner(edp_ctx* c, int32_t kind)
+{
+    if (!c || (kind != EDP_PRECOND_NONE && kind != EDP_PRECOND_MG)) return edp_fail(c, EDP_ERR_ARG, "preconditioner");
+    if (kind == EDP_PRECOND_MG && c->mg_nlev == 0) return edp_fail(c, EDP_ERR_STATE, "context was not set up for CG");
+    c->precond = kind;
+    return EDP_OK;
 }
 
 int edp_field_cg(edp_ctx* c, double rtol, int32_t max_it, int32_t warm, int32_t* iters_out)

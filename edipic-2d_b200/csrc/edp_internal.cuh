@@ -74,6 +74,15 @@ struct edp_born {
 
 struct edp_mcc_dev;
 
+// one level of the multigrid preconditioner: (nx+1) x (ny+1) nodes, x fastest, spacing 2^level
+#define EDP_MG_MAX_LEVELS 16
+struct edp_mg_level {
+    int32_t nx = 0, ny = 0;
+    double* u = nullptr;      // correction (level 0: the preconditioned residual z)
+    double* f = nullptr;      // right-hand side (level 0: the CG residual r)
+    int8_t* mask = nullptr;   // 1: Dirichlet node, correction fixed at 0
+};
+
 // add lists as seen by the kernels
 struct edp_born_dev {
     edp_born born_e;
@@ -137,8 +146,13 @@ struct edp_ctx {
     // CG workspace
     double *cg_b = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_z = nullptr;
     int8_t* cg_kind = nullptr;        // 0 unknown, 1 Dirichlet
+    int32_t precond = 1;              // edp_precond
+    int32_t mg_nlev = 0, mg_lc = 0;   // multigrid levels; levels >= mg_lc run inside one CTA
+    edp_mg_level mg[EDP_MG_MAX_LEVELS];
+    size_t mg_smem = 0;               // shared memory of the coarse-level kernel
     int32_t last_cg_iters = 0;
     double last_cg_relres = 0.0;
+    double last_cg_relres0 = 0.0;     // relative residual of the initial guess
 
     // tables
     double* mcc_prob = nullptr;
@@ -474,6 +488,9 @@ int edp_launch_density(edp_ctx* c);
 int edp_launch_fftx(edp_ctx* c);
 int edp_launch_efield(edp_ctx* c);
 int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters);
+int edp_mg_setup(edp_ctx* c);                                  // level hierarchy and masks (CG contexts)
+int edp_mg_apply(edp_ctx* c, const double* r, double* z);     // z = M^-1 r, one symmetric V-cycle
+void edp_mg_free(edp_ctx* c);
 int edp_launch_distribute(edp_ctx* c, int species, int per_cell, double factor_convert, int zero_vz, int copy_pos);
 int edp_launch_upload(edp_ctx* c, int species, int64_t n, const double* dx, const double* dy, const double* dvx,
                       const double* dvy, const double* dvz, const int32_t* dtag, const uint32_t* did);

@@ -343,13 +343,25 @@ __global__ void cg_update(edp_kparams kp, const int8_t* kind, const double* rr, 
     if (threadIdx.x == 0) atomicAdd(rr_new, acc);
 }
 
-__global__ void cg_direction(edp_kparams kp, const int8_t* kind, const double* rr, const double* rr_new, const double* r,
-                             double* p)
+// sum of a.b over the unknown nodes
+__global__ void pcg_dot(edp_kparams kp, const int8_t* kind, const double* a, const double* b, double* out)
 {
     int64_t n = (int64_t)kp.nxg * kp.nyg;
-    const double beta = *rr_new / *rr;
+    double acc = 0.0;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        if (!kind[q]) p[q] = r[q] + beta * p[q];
+        if (!kind[q]) acc += a[q] * b[q];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(out, acc);
+}
+
+// p = z + (rz / rz_old) p; rz_old == nullptr starts a new direction sequence (p = z)
+__global__ void pcg_direction(edp_kparams kp, const int8_t* kind, const double* rz, const double* rz_old,
+                              const double* z, double* p)
+{
+    int64_t n = (int64_t)kp.nxg * kp.nyg;
+    const double beta = rz_old ? *rz / *rz_old : 0.0;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        p[q] = kind[q] ? 0.0 : z[q] + beta * p[q];
 }
 
 unsigned grid_nodes(const edp_kparams& kp)
@@ -445,14 +457,18 @@ int edp_launch_efield(edp_ctx* c)
 int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
 {
     const edp_kparams& kp = c->kp;
+    const bool mg = c->precond == EDP_PRECOND_MG && c->mg_nlev > 0;
     CgGeom g;
     g.kp = kp;
     for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
     for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
-    double* scal = nullptr;   // [0] |b|^2, then rr[k] at 1 + 2k, pAp[k] at 2 + 2k
-    const int nscal = 2 * (max_it + 2) + 2;
+    // scalars: [0] |b|^2, [1] r.r before iteration 0; iteration k keeps r.z at 2+4k, p.Ap at 3+4k and the
+    // residual norm^2 after it at 4(k+1)
+    double* scal = nullptr;
+    const int nscal = 4 * (max_it + 2);
     EDP_CUDA(c, cudaMallocAsync(&scal, nscal * sizeof(double), c->stream));
     EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
+    auto rr_at = [&](int k) { return k == 0 ? scal + 1 : scal + 4 * k; };
     const unsigned gr = grid_nodes(kp);
     const double* x0 = (warm == EDP_WARM_PREVIOUS || warm == EDP_WARM_USER) ? c->phi : nullptr;
     ++c->launches;
@@ -465,29 +481,53 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     double bn = std::sqrt(h[0]);
     if (bn == 0.0) bn = 1.0;
     double rel = std::sqrt(h[1]) / bn;
-    int it = 0;
-    const int check = 8;
-    while (rel > rtol && it < max_it) {
-        int stop = std::min(max_it, it + check);
-        for (; it < stop; ++it) {
-            double* rr = &scal[1 + 2 * it];
-            double* pAp = &scal[2 + 2 * it];
-            double* rrn = &scal[1 + 2 * (it + 1)];
+    c->last_cg_relres0 = rel;
+    int it = 0, done_at = rel <= rtol ? 0 : -1;
+    const int check = mg ? 2 : 8;
+    std::vector<double> blk(4 * check + 4);
+    while (done_at < 0 && it < max_it) {
+        const int stop = std::min(max_it, it + check);
+        for (int k = it; k < stop; ++k) {
+            double* rz = scal + 2 + 4 * k;
+            double* pAp = scal + 3 + 4 * k;
+            if (mg) {
+                const int e = edp_mg_apply(c, c->cg_r, c->cg_z);
+                if (e != EDP_OK) {
+                    cudaFreeAsync(scal, c->stream);
+                    return e;
+                }
+                ++c->launches;
+                pcg_dot<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_r, c->cg_z, rz);
+                ++c->launches;
+                pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, k ? scal + 2 + 4 * (k - 1) : nullptr,
+                                                         c->cg_z, c->cg_p);
+            } else {
+                rz = rr_at(k);
+                if (k) {
+                    ++c->launches;
+                    pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rr_at(k - 1), c->cg_r, c->cg_p);
+                }
+            }
             ++c->launches;
             cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp);
             ++c->launches;
-            cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r, rrn);
-            ++c->launches;
-            cg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rr, rrn, c->cg_r, c->cg_p);
+            cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r,
+                                                 rr_at(k + 1));
         }
-        EDP_CUDA(c, cudaMemcpyAsync(h, &scal[1 + 2 * it], sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        // residual norms after iterations it+1 .. stop; the iteration count is the first that met rtol
+        const int n = 4 * (stop - it) - 3;
+        EDP_CUDA(c, cudaMemcpyAsync(blk.data(), rr_at(it + 1), n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         EDP_CUDA(c, cudaStreamSynchronize(c->stream));
-        rel = std::sqrt(h[0]) / bn;
+        for (int k = it + 1; k <= stop && done_at < 0; ++k)
+            if (std::sqrt(blk[4 * (k - it - 1)]) / bn <= rtol) done_at = k;
+        rel = std::sqrt(blk[4 * (stop - it - 1)]) / bn;   // the solution carries the whole block
+        it = stop;
     }
     EDP_CUDA(c, cudaFreeAsync(scal, c->stream));
     EDP_CUDA(c, cudaGetLastError());
-    c->last_cg_iters = it;
+    const int reported = done_at >= 0 ? done_at : it;
+    c->last_cg_iters = reported;
     c->last_cg_relres = rel;
-    if (iters) *iters = it;
-    return rel <= rtol ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
+    if (iters) *iters = reported;
+    return done_at >= 0 ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
 }

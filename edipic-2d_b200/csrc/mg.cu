@@ -1,0 +1,333 @@
+// Geometric multigrid V-cycle used as the preconditioner of the CG solve that replaces the PETSc path
+// (pic2d_ElectricFieldCalc_PETSc.F90:7-355; pic2d_PETSc_Solver.F90:42-1350 builds the same 5-point operator with
+// Dirichlet rows for the walls and the metal inner objects and solves it with GMRES + BoomerAMG).
+//
+// Operator on level l (spacing h = 2^l finest cells): (4 u_ij - sum of the 4 neighbours) / h^2 on unknown nodes,
+// Dirichlet nodes (walls, inner objects) carry a zero correction. A coarse node (I, J) is the fine node (2I, 2J) and
+// is Dirichlet when that node is. Restriction is full weighting (1/16 [1 2 1; 2 4 2; 1 2 1]) of the masked residual,
+// prolongation is bilinear into unknown nodes, so R = P^T / 4. Smoothing is red-black Gauss-Seidel: nu sweeps red
+// then black on the way down and nu sweeps black then red on the way up, the adjoint order, and the coarsest level
+// gets a palindromic sequence of sweeps. With a zero initial guess on every level the V-cycle is therefore a
+// symmetric positive definite operator, as preconditioned CG requires.
+//
+// Levels whose node count is small run inside one CTA from shared memory (one launch for the whole bottom of
+// the cycle); the finer levels are one launch per half sweep, restriction and prolongation.
+#include "edp_internal.cuh"
+
+#include <vector>
+
+namespace {
+
+constexpr int kNu = 2;                 // RB sweeps before and after the coarse correction
+constexpr int kCoarsestSweeps = 24;    // RB sweep pairs on the coarsest level
+constexpr int kCtaNodes = 4225;        // levels with at most this many nodes (65 x 65) run in the coarse CTA
+constexpr int kCoarseThreads = 1024;
+
+struct Lev {
+    double* u;
+    const double* f;
+    const int8_t* mask;
+    int nx, ny;
+    double h2;
+};
+
+// one half sweep of red-black Gauss-Seidel over the nodes with (i + j) % 2 == color. With first, the level starts
+// from a zero correction: nodes of the colour take h^2 f / 4 and every other node is set to zero.
+__device__ __forceinline__ void half_sweep(const Lev& L, int color, bool first, int64_t t0, int64_t stride)
+{
+    const int w = L.nx + 1;
+    if (first) {
+        const int64_t n = (int64_t)w * (L.ny + 1);
+        for (int64_t q = t0; q < n; q += stride) {
+            const int i = (int)(q % w), j = (int)(q / w);
+            double v = 0.0;
+            if (!L.mask[q] && ((i + j) & 1) == color) v = 0.25 * L.h2 * L.f[q];
+            L.u[q] = v;
+        }
+        return;
+    }
+    const int hw = (w + 1) >> 1;
+    const int64_t n = (int64_t)hw * (L.ny + 1);
+    for (int64_t k = t0; k < n; k += stride) {
+        const int j = (int)(k / hw);
+        const int i = 2 * (int)(k % hw) + ((j + color) & 1);
+        if (i > L.nx) continue;
+        const int64_t q = (int64_t)j * w + i;
+        if (L.mask[q]) continue;   // walls are Dirichlet, so every unknown node has four in-range neighbours
+        L.u[q] = 0.25 * (L.h2 * L.f[q] + L.u[q - 1] + L.u[q + 1] + L.u[q - w] + L.u[q + w]);
+    }
+}
+
+__device__ __forceinline__ double residual_at(const Lev& L, int64_t q)
+{
+    if (L.mask[q]) return 0.0;
+    const int w = L.nx + 1;
+    return L.f[q] - (4.0 * L.u[q] - L.u[q - 1] - L.u[q + 1] - L.u[q - w] - L.u[q + w]) / L.h2;
+}
+
+// coarse right-hand side = full weighting of the fine residual
+__device__ __forceinline__ void restrict_to(const Lev& F, double* fc, const int8_t* maskc, int nxc, int nyc,
+                                            int64_t t0, int64_t stride)
+{
+    const int wc = nxc + 1, w = F.nx + 1;
+    const int64_t n = (int64_t)wc * (nyc + 1);
+    for (int64_t Q = t0; Q < n; Q += stride) {
+        if (maskc[Q]) {
+            fc[Q] = 0.0;
+            continue;
+        }
+        const int I = (int)(Q % wc), J = (int)(Q / wc);
+        const int64_t q = (int64_t)(2 * J) * w + 2 * I;
+        double s = 4.0 * residual_at(F, q);
+        s += 2.0 * (residual_at(F, q - 1) + residual_at(F, q + 1) + residual_at(F, q - w) + residual_at(F, q + w));
+        s += residual_at(F, q - w - 1) + residual_at(F, q - w + 1) + residual_at(F, q + w - 1) + residual_at(F, q + w + 1);
+        fc[Q] = s * 0.0625;
+    }
+}
+
+// fine correction += bilinear interpolation of the coarse correction (unknown fine nodes only)
+__device__ __forceinline__ void prolong_add(const Lev& F, const double* uc, int nxc, int64_t t0, int64_t stride)
+{
+    const int w = F.nx + 1, wc = nxc + 1;
+    const int64_t n = (int64_t)w * (F.ny + 1);
+    for (int64_t q = t0; q < n; q += stride) {
+        if (F.mask[q]) continue;
+        const int i = (int)(q % w), j = (int)(q / w);
+        const int I = i >> 1, J = j >> 1;
+        const int64_t Q = (int64_t)J * wc + I;
+        double e;
+        if (!(i & 1) && !(j & 1)) e = uc[Q];
+        else if (!(j & 1)) e = 0.5 * (uc[Q] + uc[Q + 1]);
+        else if (!(i & 1)) e = 0.5 * (uc[Q] + uc[Q + wc]);
+        else e = 0.25 * (uc[Q] + uc[Q + 1] + uc[Q + wc] + uc[Q + wc + 1]);
+        F.u[q] += e;
+    }
+}
+
+__global__ void mg_sweep_kernel(Lev L, int color, int first)
+{
+    half_sweep(L, color, first != 0, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+__global__ void mg_restrict_kernel(Lev F, double* fc, const int8_t* maskc, int nxc, int nyc)
+{
+    restrict_to(F, fc, maskc, nxc, nyc, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                (int64_t)gridDim.x * blockDim.x);
+}
+
+__global__ void mg_prolong_kernel(Lev F, const double* uc, int nxc)
+{
+    prolong_add(F, uc, nxc, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+struct CoarseArgs {
+    int nlev;                             // levels handled here: lc .. lc + nlev - 1
+    int nx[EDP_MG_MAX_LEVELS], ny[EDP_MG_MAX_LEVELS];
+    double h2[EDP_MG_MAX_LEVELS];
+    const int8_t* mask[EDP_MG_MAX_LEVELS];
+    const double* f_in;                   // right-hand side of the top level here
+    double* u_out;                        // its correction
+};
+
+// The bottom of the V-cycle in one CTA: every level lives in shared memory, phases are separated by barriers.
+__global__ void __launch_bounds__(kCoarseThreads, 1) mg_coarse_kernel(CoarseArgs a)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    Lev L[EDP_MG_MAX_LEVELS];
+    size_t off = 0;
+    for (int l = 0; l < a.nlev; ++l) {
+        const int64_t n = (int64_t)(a.nx[l] + 1) * (a.ny[l] + 1);
+        L[l].u = reinterpret_cast<double*>(sm + off);
+        off += n * sizeof(double);
+        L[l].f = reinterpret_cast<const double*>(sm + off);
+        off += n * sizeof(double);
+        L[l].mask = reinterpret_cast<const int8_t*>(sm + off);
+        off += (n + 15) & ~(int64_t)15;
+        L[l].nx = a.nx[l];
+        L[l].ny = a.ny[l];
+        L[l].h2 = a.h2[l];
+    }
+    const int t = threadIdx.x, T = blockDim.x;
+    for (int l = 0; l < a.nlev; ++l) {
+        const int64_t n = (int64_t)(a.nx[l] + 1) * (a.ny[l] + 1);
+        int8_t* m = const_cast<int8_t*>(L[l].mask);
+        for (int64_t q = t; q < n; q += T) m[q] = a.mask[l][q];
+    }
+    {
+        const int64_t n = (int64_t)(a.nx[0] + 1) * (a.ny[0] + 1);
+        double* f0 = const_cast<double*>(L[0].f);
+        for (int64_t q = t; q < n; q += T) f0[q] = a.f_in[q];
+    }
+    __syncthreads();
+    const int last = a.nlev - 1;
+    for (int l = 0; l < last; ++l) {
+        for (int s = 0; s < kNu; ++s) {
+            half_sweep(L[l], 0, s == 0, t, T);
+            __syncthreads();
+            half_sweep(L[l], 1, false, t, T);
+            __syncthreads();
+        }
+        restrict_to(L[l], const_cast<double*>(L[l + 1].f), L[l + 1].mask, a.nx[l + 1], a.ny[l + 1], t, T);
+        __syncthreads();
+    }
+    for (int s = 0; s < kCoarsestSweeps; ++s) {
+        half_sweep(L[last], 0, s == 0, t, T);
+        __syncthreads();
+        half_sweep(L[last], 1, false, t, T);
+        __syncthreads();
+    }
+    for (int s = 0; s < kCoarsestSweeps; ++s) {
+        half_sweep(L[last], 1, false, t, T);
+        __syncthreads();
+        half_sweep(L[last], 0, false, t, T);
+        __syncthreads();
+    }
+    for (int l = last - 1; l >= 0; --l) {
+        prolong_add(L[l], L[l + 1].u, a.nx[l + 1], t, T);
+        __syncthreads();
+        for (int s = 0; s < kNu; ++s) {
+            half_sweep(L[l], 1, false, t, T);
+            __syncthreads();
+            half_sweep(L[l], 0, false, t, T);
+            __syncthreads();
+        }
+    }
+    const int64_t n = (int64_t)(a.nx[0] + 1) * (a.ny[0] + 1);
+    for (int64_t q = t; q < n; q += T) a.u_out[q] = L[0].u[q];
+}
+
+unsigned grid_of_nodes(int nx, int ny)
+{
+    int64_t n = (int64_t)(nx + 1) * (ny + 1);
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 8) g = 148 * 8;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+Lev lev_of(const edp_ctx* c, int l, double* u, const double* f)
+{
+    Lev L;
+    L.u = u;
+    L.f = f;
+    L.mask = c->mg[l].mask;
+    L.nx = c->mg[l].nx;
+    L.ny = c->mg[l].ny;
+    L.h2 = (double)(1 << l) * (double)(1 << l);
+    return L;
+}
+
+}  // namespace
+
+int edp_mg_setup(edp_ctx* c)
+{
+    const edp_params& p = c->p;
+    // levels: halve while both cell counts stay even and the coarse grid keeps at least 2 x 2 cells
+    int nl = 1;
+    c->mg[0].nx = p.ncx;
+    c->mg[0].ny = p.ncy;
+    while (nl < EDP_MG_MAX_LEVELS) {
+        const int nx = c->mg[nl - 1].nx, ny = c->mg[nl - 1].ny;
+        if ((nx & 1) || (ny & 1) || nx < 4 || ny < 4) break;
+        c->mg[nl].nx = nx / 2;
+        c->mg[nl].ny = ny / 2;
+        ++nl;
+    }
+    c->mg_nlev = nl;
+    int lc = 0;
+    while (lc < nl && (int64_t)(c->mg[lc].nx + 1) * (c->mg[lc].ny + 1) > kCtaNodes) ++lc;
+    if (lc == nl) lc = nl - 1;   // the coarsest level is large (odd sizes): it still runs in the CTA
+    c->mg_lc = lc;
+    size_t smem = 0;
+    for (int l = lc; l < nl; ++l) {
+        const size_t n = (size_t)(c->mg[l].nx + 1) * (c->mg[l].ny + 1);
+        smem += 2 * n * sizeof(double) + ((n + 15) & ~(size_t)15);
+    }
+    if (smem > 220 * 1024) {   // cell counts without enough factors of 2: plain CG only
+        c->mg_nlev = 0;
+        c->precond = EDP_PRECOND_NONE;
+        return EDP_OK;
+    }
+    c->mg_smem = smem;
+    EDP_CUDA(c, cudaFuncSetAttribute(mg_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // Dirichlet masks: walls, and the metal inner objects, of the finest node at (2^l I, 2^l J)
+    for (int l = 0; l < nl; ++l) {
+        edp_mg_level& m = c->mg[l];
+        const int w = m.nx + 1;
+        const size_t n = (size_t)w * (m.ny + 1);
+        std::vector<int8_t> h(n);
+        for (int J = 0; J <= m.ny; ++J)
+            for (int I = 0; I <= m.nx; ++I) {
+                const int i = I << l, j = J << l;
+                int8_t k = (i == 0 || j == 0 || i == p.ncx || j == p.ncy) ? 1 : 0;
+                for (int o = 0; o < p.n_inner; ++o)
+                    if (i >= p.inner_ileft[o] && i <= p.inner_iright[o] && j >= p.inner_jbottom[o] && j <= p.inner_jtop[o])
+                        k = 1;
+                h[(size_t)J * w + I] = k;
+            }
+        EDP_CUDA(c, cudaMalloc(&m.mask, n));
+        EDP_CUDA(c, cudaMemcpy(m.mask, h.data(), n, cudaMemcpyHostToDevice));
+        if (l > 0) {
+            EDP_CUDA(c, cudaMalloc(&m.u, n * sizeof(double)));
+            EDP_CUDA(c, cudaMalloc(&m.f, n * sizeof(double)));
+        }
+    }
+    return EDP_OK;
+}
+
+void edp_mg_free(edp_ctx* c)
+{
+    for (int l = 0; l < c->mg_nlev; ++l) {
+        cudaFree(c->mg[l].mask);
+        if (l > 0) {
+            cudaFree(c->mg[l].u);
+            cudaFree(c->mg[l].f);
+        }
+        c->mg[l] = edp_mg_level();
+    }
+    c->mg_nlev = 0;
+}
+
+int edp_mg_apply(edp_ctx* c, const double* r, double* z)
+{
+    const int nl = c->mg_nlev, lc = c->mg_lc;
+    auto u_of = [&](int l) { return l == 0 ? z : c->mg[l].u; };
+    auto f_of = [&](int l) { return l == 0 ? r : (const double*)c->mg[l].f; };
+    for (int l = 0; l < lc; ++l) {
+        Lev L = lev_of(c, l, u_of(l), f_of(l));
+        const unsigned g = grid_of_nodes(L.nx, L.ny);
+        for (int s = 0; s < kNu; ++s) {
+            c->launches += 2;
+            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 0, s == 0);
+            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 1, 0);
+        }
+        ++c->launches;
+        mg_restrict_kernel<<<grid_of_nodes(c->mg[l + 1].nx, c->mg[l + 1].ny), 256, 0, c->stream>>>(
+            L, c->mg[l + 1].f, c->mg[l + 1].mask, c->mg[l + 1].nx, c->mg[l + 1].ny);
+    }
+    CoarseArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nlev = nl - lc;
+    for (int l = lc; l < nl; ++l) {
+        a.nx[l - lc] = c->mg[l].nx;
+        a.ny[l - lc] = c->mg[l].ny;
+        a.h2[l - lc] = (double)(1 << l) * (double)(1 << l);
+        a.mask[l - lc] = c->mg[l].mask;
+    }
+    a.f_in = f_of(lc);
+    a.u_out = u_of(lc);
+    ++c->launches;
+    mg_coarse_kernel<<<1, kCoarseThreads, c->mg_smem, c->stream>>>(a);
+    for (int l = lc - 1; l >= 0; --l) {
+        Lev L = lev_of(c, l, u_of(l), f_of(l));
+        const unsigned g = grid_of_nodes(L.nx, L.ny);
+        ++c->launches;
+        mg_prolong_kernel<<<g, 256, 0, c->stream>>>(L, c->mg[l + 1].u, c->mg[l + 1].nx);
+        for (int s = 0; s < kNu; ++s) {
+            c->launches += 2;
+            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 1, 0);
+            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 0, 0);
+        }
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}

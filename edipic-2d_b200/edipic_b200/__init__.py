@@ -11,12 +11,14 @@ import numpy as np
 
 from . import _abi
 from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS,
-                   PREC_FP64, PREC_MIXED, SOLVER_CG, SOLVER_FFTX, WARM_PREVIOUS, WARM_USER, WARM_ZERO, Counters,
+                   PREC_FP64, PREC_MIXED, PRECOND_MG, PRECOND_NONE, SOLVER_CG, SOLVER_FFTX, WARM_PREVIOUS, WARM_USER,
+                   WARM_ZERO, Counters,
                    Params, Tables)
 
 __all__ = ["Simulation", "EdpError", "read_deck", "library", "Params", "Tables", "Counters", "ELECTRONS", "IONS",
            "PREC_MIXED", "PREC_FP64", "SOLVER_FFTX", "SOLVER_CG", "FIELD_EX", "FIELD_EY", "FIELD_ACC_EX",
-           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER"]
+           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER", "PRECOND_NONE",
+           "PRECOND_MG"]
 
 _lib = None
 
@@ -199,6 +201,10 @@ class Simulation:
         it = C.c_int32()
         self._check(self.lib.edp_field_cg(self.ctx, rtol, max_it, warm_start, C.byref(it)), "edp_field_cg")
         return it.value
+
+    def set_cg_preconditioner(self, kind):
+        """PRECOND_MG (default): a multigrid V-cycle per CG iteration; PRECOND_NONE: plain CG."""
+        self._check(self.lib.edp_set_cg_preconditioner(self.ctx, kind), "edp_set_cg_preconditioner")
 
     def advance_electrons(self):
         self._check(self.lib.edp_advance_electrons(self.ctx), "edp_advance_electrons")

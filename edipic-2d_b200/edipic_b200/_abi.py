@@ -21,6 +21,7 @@ SOLVER_FFTX, SOLVER_CG = 0, 1
 ELECTRONS, IONS = 0, 1
 FIELD_EX, FIELD_EY, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_PHI, FIELD_RHO_TOTAL = range(6)
 WARM_ZERO, WARM_PREVIOUS, WARM_USER = 0, 1, 2
+PRECOND_NONE, PRECOND_MG = 0, 1
 
 ERROR_NAMES = {
     ERR_ARG: "EDP_ERR_ARG", ERR_CUDA: "EDP_ERR_CUDA", ERR_CAPACITY: "EDP_ERR_CAPACITY",
@@ -95,6 +96,7 @@ SIGNATURES = {
     "edp_update_wall_potentials": [_CTX, C.c_int64],
     "edp_field_fftx": [_CTX, _D],
     "edp_field_cg": [_CTX, C.c_double, C.c_int32, C.c_int32, _I32],
+    "edp_set_cg_preconditioner": [_CTX, C.c_int32],
     "edp_advance_electrons": [_CTX],
     "edp_advance_ions": [_CTX],
     "edp_collide_en": [_CTX, _I64],

@@ -125,8 +125,6 @@ int read_deck(const std::string& dir, edp_deck* d)
     memset(&t, 0, sizeof(t));
     p.abi_version = EDP_ABI_VERSION;
     std::string L;
-    long long iv;
-    double rv;
     // ---- init_configuration.dat (pic2d_CurProblemValues.f90:157-330)
     Lines cf(dir + "/init_configuration.dat");
     if (!cf.ok) return EDP_ERR_IO;

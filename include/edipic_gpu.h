@@ -52,6 +52,9 @@ enum edp_field {
     EDP_FIELD_PHI = 4, EDP_FIELD_RHO_TOTAL = 5
 };
 enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2 };
+/* preconditioner of edp_field_cg: NONE is Jacobi, which is plain CG here because the operator's diagonal is
+ * constant; MG (the default) is one symmetric geometric-multigrid V-cycle per iteration */
+enum edp_precond { EDP_PRECOND_NONE = 0, EDP_PRECOND_MG = 1 };
 
 #define EDP_MAX_ION_SPECIES 4
 #define EDP_MAX_INNER 4
@@ -176,8 +179,12 @@ int edp_update_wall_potentials(edp_ctx* ctx, int64_t t_cntr);
  * (pic2d_ElectricFieldCalc_FFT_X.f90:3-1547): phi_out may be NULL */
 int edp_field_fftx(edp_ctx* ctx, double* phi_out);
 /* SOLVE_POTENTIAL_WITH_PETSC + CALCULATE_ELECTRIC_FIELD (pic2d_ElectricFieldCalc_PETSc.F90:7-805,
- * pic2d_PETSc_Solver.F90:31-40): preconditioned CG to rtol on the same operator, FP64 dots. */
+ * pic2d_PETSc_Solver.F90:31-40): preconditioned CG on the same operator, FP64 dots, until the relative residual
+ * |b - A phi| / |b| <= rtol. iters_out receives the first iteration that met rtol (the potential may carry up to
+ * one more convergence-check block of iterations). */
 int edp_field_cg(edp_ctx* ctx, double rtol, int32_t max_it, int32_t warm_start, int32_t* iters_out);
+/* selects the preconditioner of edp_field_cg (edp_precond) */
+int edp_set_cg_preconditioner(edp_ctx* ctx, int32_t kind);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
  * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
 int edp_advance_electrons(edp_ctx* ctx);
