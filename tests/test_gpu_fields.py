@@ -62,7 +62,7 @@ def test_cg_matches_oracle(tmp_path, precision, precond):
     ref, it_ref, rel = pyoracle.cg_solve(g, rho_t, [0.0, 0.0, 0.0, 0.0], [p.inner_phi[0]], rtol=1e-13)
     assert it_ref > 0 and rel < 1e-13
     assert np.abs(phi - ref).max() <= 1e-8 * np.abs(ref).max()
-    assert it > 10 and it2 <= 2
+    assert it > (3 if precond == PRECOND_MG else 10) and it2 <= 2
     assert np.allclose(phi[20:37, 30:61], p.inner_phi[0])
     f2 = p.f_scale_v / (p.e_scale_vm * 2.0 * p.delta_x_m)
     f1 = p.f_scale_v / (p.e_scale_vm * p.delta_x_m)
