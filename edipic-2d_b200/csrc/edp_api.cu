@@ -82,12 +82,6 @@ int dalloc(edp_ctx* c, T** p, size_t n)
     return EDP_OK;
 }
 
-#define TRY(x)                        \
-    do {                              \
-        int _r = (x);                 \
-        if (_r != EDP_OK) return _r;  \
-    } while (0)
-
 // Boris rotation matrix K11..K33 (pic2d_ElectronDynamics.f90:91-113) for uniform B
 void rotation(double ax, double ay, double az, double* K)
 {
@@ -663,6 +657,7 @@ int edp_destroy(edp_ctx* c)
     F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
     F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
     edp_mg_free(c);
+    edp_warmstart_free(c);
     F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v);
     F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
@@ -906,7 +901,8 @@ int edp_set_cg_preconditioner(edp_ctx* c, int32_t kind)
 
 int edp_field_cg(edp_ctx* c, double rtol, int32_t max_it, int32_t warm, int32_t* iters_out)
 {
-    if (!c || max_it < 1 || !(rtol > 0.0)) return edp_fail(c, EDP_ERR_ARG, "edp_field_cg");
+    if (!c || max_it < 1 || !(rtol > 0.0) || warm < EDP_WARM_ZERO || warm > EDP_WARM_LEARNED)
+        return edp_fail(c, EDP_ERR_ARG, "edp_field_cg");
     if (c->p.solver != EDP_SOLVER_CG) return edp_fail(c, EDP_ERR_STATE, "context was not set up for CG");
     TRY(edp_launch_density(c));
     int it = 0;

@@ -73,6 +73,7 @@ struct edp_born {
 };
 
 struct edp_mcc_dev;
+struct edp_warmstart;   // learned warm start of the CG solve (warmstart.cu)
 
 // one level of the multigrid preconditioner: (nx+1) x (ny+1) nodes, x fastest, spacing 2^level
 #define EDP_MG_MAX_LEVELS 16
@@ -150,6 +151,8 @@ struct edp_ctx {
     int32_t mg_nlev = 0, mg_lc = 0;   // multigrid levels; levels >= mg_lc run inside one CTA
     edp_mg_level mg[EDP_MG_MAX_LEVELS];
     size_t mg_smem = 0;               // shared memory of the coarse-level kernel
+    edp_warmstart* ws = nullptr;      // network of the learned warm start, once loaded
+    int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     int32_t last_cg_iters = 0;
     double last_cg_relres = 0.0;
     double last_cg_relres0 = 0.0;     // relative residual of the initial guess
@@ -474,6 +477,11 @@ int edp_cuda_check(edp_ctx* c, cudaError_t e, const char* what);
         cudaError_t _e = (call);                                       \
         if (_e != cudaSuccess) return edp_cuda_check((ctx), _e, #call); \
     } while (0)
+#define TRY(x)                       \
+    do {                             \
+        int _r = (x);                \
+        if (_r != EDP_OK) return _r; \
+    } while (0)
 
 edp_mcc_dev edp_make_mcc_dev(const edp_ctx* c);
 edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
@@ -491,6 +499,12 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters);
 int edp_mg_setup(edp_ctx* c);                                  // level hierarchy and masks (CG contexts)
 int edp_mg_apply(edp_ctx* c, const double* r, double* z);     // z = M^-1 r, one symmetric V-cycle
 void edp_mg_free(edp_ctx* c);
+void edp_warmstart_free(edp_ctx* c);
+int edp_warmstart_forward(edp_ctx* c, const double* rr0);   // guess from the residual in cg_r
+int edp_warmstart_residual(edp_ctx* c);                     // residual of the guess
+const double* edp_warmstart_rr(edp_ctx* c);                 // device |r|^2 of the guess
+cudaError_t edp_warmstart_accept(edp_ctx* c, double* rr_dst);
+const double* edp_warmstart_guess(edp_ctx* c);
 int edp_launch_distribute(edp_ctx* c, int species, int per_cell, double factor_convert, int zero_vz, int copy_pos);
 int edp_launch_upload(edp_ctx* c, int species, int64_t n, const double* dx, const double* dy, const double* dvx,
                       const double* dvy, const double* dvz, const int32_t* dtag, const uint32_t* did);

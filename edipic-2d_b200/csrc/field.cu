@@ -470,17 +470,36 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
     auto rr_at = [&](int k) { return k == 0 ? scal + 1 : scal + 4 * k; };
     const unsigned gr = grid_nodes(kp);
-    const double* x0 = (warm == EDP_WARM_PREVIOUS || warm == EDP_WARM_USER) ? c->phi : nullptr;
+    const bool learned = warm == EDP_WARM_LEARNED;
+    if (learned && !c->ws) {
+        cudaFreeAsync(scal, c->stream);
+        return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
+    }
     ++c->launches;
-    cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, x0 ? x0 : c->phi, c->cg_kind, c->phi, c->cg_b, scal);
+    cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
     ++c->launches;
     cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
-    double h[2];
+    if (learned) {
+        int e = edp_warmstart_forward(c, &scal[1]);
+        if (e == EDP_OK) e = edp_warmstart_residual(c);
+        if (e != EDP_OK) {
+            cudaFreeAsync(scal, c->stream);
+            return e;
+        }
+    }
+    double h[3] = {0.0, 0.0, 0.0};
     EDP_CUDA(c, cudaMemcpyAsync(h, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (learned) EDP_CUDA(c, cudaMemcpyAsync(h + 2, edp_warmstart_rr(c), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
     double bn = std::sqrt(h[0]);
     if (bn == 0.0) bn = 1.0;
     double rel = std::sqrt(h[1]) / bn;
+    c->last_ws_used = 0;
+    if (learned && h[2] < h[1]) {   // the network's guess has the smaller residual: start from it
+        EDP_CUDA(c, edp_warmstart_accept(c, &scal[1]));
+        rel = std::sqrt(h[2]) / bn;
+        c->last_ws_used = 1;
+    }
     c->last_cg_relres0 = rel;
     int it = 0, done_at = rel <= rtol ? 0 : -1;
     const int check = mg ? 2 : 8;
@@ -530,4 +549,38 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     c->last_cg_relres = rel;
     if (iters) *iters = reported;
     return done_at >= 0 ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
+}
+
+// The network's guess for the current density without solving: guess_out (node layout) and the residual norms of
+// the previous potential and of the guess. The potential itself is left unchanged.
+extern "C" int edp_warmstart_predict(edp_ctx* c, double* guess_out, double* res_out)
+{
+    if (!c || !guess_out || !res_out) return EDP_ERR_ARG;
+    if (c->p.solver != EDP_SOLVER_CG) return edp_fail(c, EDP_ERR_STATE, "context was not set up for CG");
+    if (!c->ws) return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
+    TRY(edp_launch_density(c));
+    const edp_kparams& kp = c->kp;
+    CgGeom g;
+    g.kp = kp;
+    for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
+    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    double* scal = nullptr;
+    EDP_CUDA(c, cudaMallocAsync(&scal, 2 * sizeof(double), c->stream));
+    EDP_CUDA(c, cudaMemsetAsync(scal, 0, 2 * sizeof(double), c->stream));
+    const unsigned gr = grid_nodes(kp);
+    c->launches += 2;
+    cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, EDP_WARM_PREVIOUS, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
+    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
+    TRY(edp_warmstart_forward(c, &scal[1]));
+    TRY(edp_warmstart_residual(c));
+    double h[2];
+    EDP_CUDA(c, cudaMemcpyAsync(&h[0], &scal[1], sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaMemcpyAsync(&h[1], edp_warmstart_rr(c), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    const size_t nb = (size_t)kp.nxg * kp.nyg * sizeof(double);
+    EDP_CUDA(c, cudaMemcpyAsync(guess_out, edp_warmstart_guess(c), nb, cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaFreeAsync(scal, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    res_out[0] = std::sqrt(h[0]);
+    res_out[1] = std::sqrt(h[1]);
+    return EDP_OK;
 }

@@ -1,0 +1,674 @@
+// Kernels of the learned warm start of the CG solve: a 4-level convolutional encoder-decoder that maps the
+// residual of the previous potential against the new charge density to a potential update.
+//
+// Tensors are NHWC: activations BF16 [images][h][w][channels], 3x3 convolution weights BF16 [c_out][3][3][c_in]
+// (tap = 3 ky + kx, offsets ky - 1, kx - 1), biases and all gradients of weights FP32. Convolutions are implicit
+// GEMMs on the BF16 tensor cores with FP32 accumulation:
+//   forward  y[p][n]      = act(sum_{tap, c} x[p + off(tap)][c] w[n][tap][c] + b[n])       M = pixels, N = c_out
+//   dgrad    dx[p][c]     = sum_{tap', n} dz[p + off(tap')][n] w[n][8 - tap'][c]          (the forward kernel on
+//                           the flipped, transposed weight copy)
+//   wgrad    dw[n][tap][c] += sum_p dz[p][n] x[p + off(tap)][c]                            M = c_out, K = pixels
+// Pixels outside the image read zero (padding 1). The input of a forward convolution may be the channel
+// concatenation of two tensors (the decoder's upsampled path and the encoder's skip), read in place.
+#include "edp_internal.cuh"
+
+#include <cuda_bf16.h>
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid)
+{
+    const int sz = valid ? 16 : 0;   // 0: zero-fill the 16 bytes
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// byte offset of 16-byte chunk c of row r in a tile whose rows hold `cpr` chunks (4: 64 B rows, 8: 128 B rows);
+// the XOR spreads the 8 rows an ldmatrix reads over all 32 banks
+__device__ __forceinline__ int swz(int r, int c, int cpr)
+{
+    const int x = cpr == 8 ? (r & 7) : ((r >> 1) & 3);
+    return r * cpr * 16 + ((c ^ x) << 4);
+}
+
+// ------------------------------------------------------------------------------------------ forward / dgrad
+struct ConvArgs {
+    int nimg, h, w;
+    const bf16* x1;   // [P][c1]
+    int c1;
+    const bf16* x2;   // [P][c2] or null
+    int c2;
+    const bf16* wt;   // [cout][9][c1 + c2]
+    const float* bias;
+    int cout;
+    int relu;
+    bf16* y;          // [P][cout]
+};
+
+constexpr int kBM = 128, kBK = 32, kStages = 3, kConvThreads = 256;
+
+template <int BN>
+__global__ void __launch_bounds__(kConvThreads) conv3x3_fwd_kernel(ConvArgs a)
+{
+    constexpr int WARPS_N = BN / 32, WARPS_M = 8 / WARPS_N;
+    constexpr int WM = kBM / WARPS_M;          // 32 (BN 64) or 16 (BN 32)
+    constexpr int MI = WM / 16, NI = 4;        // m16 tiles and n8 tiles per warp
+    constexpr int A_BYTES = kBM * kBK * 2, B_BYTES = BN * kBK * 2;
+    __shared__ __align__(128) unsigned char sm[kStages * (A_BYTES + B_BYTES)];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp % WARPS_M, wn = warp / WARPS_M;
+    const int64_t P = (int64_t)a.nimg * a.h * a.w;
+    const int64_t m0 = (int64_t)blockIdx.x * kBM;
+    const int n0 = blockIdx.y * BN;
+    const int cin = a.c1 + a.c2;
+    const int kc = cin / kBK;
+    const int KT = 9 * kc;
+
+    // the two A rows this thread loads: pixel coordinates
+    int ay[2], ax[2], ab[2], arow[2], achk[2];
+    bool aval[2];
+    for (int i = 0; i < 2; ++i) {
+        const int idx = tid + kConvThreads * i;
+        arow[i] = idx >> 2;
+        achk[i] = idx & 3;
+        const int64_t p = m0 + arow[i];
+        aval[i] = p < P;
+        const int64_t pp = aval[i] ? p : 0;
+        ax[i] = (int)(pp % a.w);
+        ay[i] = (int)((pp / a.w) % a.h);
+        ab[i] = (int)(pp / ((int64_t)a.w * a.h));
+    }
+
+    auto load_stage = [&](int s, int kt) {
+        unsigned char* As = sm + s * (A_BYTES + B_BYTES);
+        unsigned char* Bs = As + A_BYTES;
+        const int tap = kt / kc, cc = kt % kc;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const int ci0 = cc * kBK;
+        const bf16* src;
+        int cs, cof;
+        if (ci0 < a.c1) { src = a.x1; cs = a.c1; cof = ci0; }
+        else { src = a.x2; cs = a.c2; cof = ci0 - a.c1; }
+        for (int i = 0; i < 2; ++i) {
+            const int yy = ay[i] + dy, xx = ax[i] + dx;
+            const bool ok = aval[i] && yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            const bf16* g = ok ? src + (((int64_t)ab[i] * a.h + yy) * a.w + xx) * cs + cof + achk[i] * 8 : src;
+            cp_async16(smem_u32(As + swz(arow[i], achk[i], 4)), g, ok);
+        }
+        for (int idx = tid; idx < BN * 4; idx += kConvThreads) {
+            const int r = idx >> 2, c = idx & 3;
+            const bf16* g = a.wt + ((int64_t)(n0 + r) * 9 + tap) * cin + ci0 + c * 8;
+            cp_async16(smem_u32(Bs + swz(r, c, 4)), g, true);
+        }
+    };
+
+    float acc[MI][NI][4];
+    for (int i = 0; i < MI; ++i)
+        for (int j = 0; j < NI; ++j)
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
+
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
+        cp_async_commit();
+        const unsigned char* As = sm + (kt % kStages) * (A_BYTES + B_BYTES);
+        const unsigned char* Bs = As + A_BYTES;
+        for (int ks = 0; ks < 2; ++ks) {
+            uint32_t af[MI][4], bfr[NI][2];
+            for (int i = 0; i < MI; ++i) {
+                const int r = wm * WM + i * 16 + (lane & 15);
+                ldsm_x4(smem_u32(As + swz(r, 2 * ks + (lane >> 4), 4)), af[i][0], af[i][1], af[i][2], af[i][3]);
+            }
+            for (int j = 0; j < NI / 2; ++j) {
+                const int r = wn * 32 + j * 16 + (lane & 7) + ((lane >> 4) << 3);
+                ldsm_x4(smem_u32(Bs + swz(r, 2 * ks + ((lane >> 3) & 1), 4)), bfr[2 * j][0], bfr[2 * j][1],
+                        bfr[2 * j + 1][0], bfr[2 * j + 1][1]);
+            }
+            for (int i = 0; i < MI; ++i)
+                for (int j = 0; j < NI; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+        }
+    }
+    cp_async_wait<0>();
+
+    const int g = lane >> 2, t = lane & 3;
+    for (int i = 0; i < MI; ++i)
+        for (int j = 0; j < NI; ++j) {
+            const int n = n0 + wn * 32 + j * 8 + 2 * t;
+            const float b0 = a.bias ? a.bias[n] : 0.0f, b1 = a.bias ? a.bias[n + 1] : 0.0f;
+            for (int hlf = 0; hlf < 2; ++hlf) {
+                const int64_t p = m0 + wm * WM + i * 16 + g + 8 * hlf;
+                if (p >= P) continue;
+                float v0 = acc[i][j][2 * hlf] + b0, v1 = acc[i][j][2 * hlf + 1] + b1;
+                if (a.relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                *reinterpret_cast<__nv_bfloat162*>(a.y + p * a.cout + n) = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+}
+
+// wt_t[c][8 - tap][n] = wt[n][tap][c]: the weights of the data gradient
+__global__ void flip_transpose_kernel(const bf16* __restrict__ wt, int cout, int cin, bf16* __restrict__ out)
+{
+    const int64_t total = (int64_t)cout * 9 * cin;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(q % cin);
+        const int tap = (int)((q / cin) % 9);
+        const int n = (int)(q / ((int64_t)cin * 9));
+        out[((int64_t)c * 9 + (8 - tap)) * cout + n] = wt[q];
+    }
+}
+
+// ------------------------------------------------------------------------------------------ weight gradient
+struct WgradArgs {
+    int nimg, h, w;
+    const bf16* x;    // [P][cin] (a concatenated input is passed as x1 | x2 split at c1)
+    int c1;
+    const bf16* x2;
+    int c2;
+    const bf16* dz;   // [P][cout]
+    int cout;
+    float* dw;        // [cout][9][cin], accumulated
+    int64_t pix_per_cta;
+};
+
+constexpr int kWK = 32;   // pixels per K step
+
+template <int BM, int BN>
+__global__ void __launch_bounds__((BM / 32) * (BN / 16) * 32) conv3x3_wgrad_kernel(WgradArgs a)
+{
+    constexpr int WARPS_M = BM / 32, WARPS_N = BN / 16, NT = WARPS_M * WARPS_N * 32;
+    constexpr int A_CPR = BM / 8, B_CPR = BN / 8;               // 16-byte chunks per smem row (4 or 8)
+    constexpr int A_BYTES = kWK * BM * 2, B_BYTES = kWK * BN * 2;
+    __shared__ __align__(128) unsigned char sm[kStages * (A_BYTES + B_BYTES)];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp % WARPS_M, wn = warp / WARPS_M;
+    const int cin = a.c1 + a.c2;
+    const int ntile_c = cin / BN, ntile_o = a.cout / BM;
+    int tile = blockIdx.y;
+    const int co0 = (tile % ntile_o) * BM;
+    tile /= ntile_o;
+    const int ci0 = (tile % ntile_c) * BN;
+    const int tap = tile / ntile_c;
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const int64_t P = (int64_t)a.nimg * a.h * a.w;
+    const int64_t p_begin = (int64_t)blockIdx.x * a.pix_per_cta;
+    int64_t p_end = p_begin + a.pix_per_cta;
+    if (p_end > P) p_end = P;
+    if (p_begin >= p_end) return;
+    const int KT = (int)((p_end - p_begin + kWK - 1) / kWK);
+    const bf16* xs;
+    int xcs, xco;
+    if (ci0 < a.c1) { xs = a.x; xcs = a.c1; xco = ci0; }
+    else { xs = a.x2; xcs = a.c2; xco = ci0 - a.c1; }
+
+    auto load_stage = [&](int s, int kt) {
+        unsigned char* As = sm + s * (A_BYTES + B_BYTES);
+        unsigned char* Bs = As + A_BYTES;
+        const int64_t pk = p_begin + (int64_t)kt * kWK;
+        for (int idx = tid; idx < kWK * A_CPR; idx += NT) {
+            const int r = idx / A_CPR, c = idx % A_CPR;
+            const int64_t p = pk + r;
+            const bool ok = p < p_end;
+            const bf16* g = ok ? a.dz + p * a.cout + co0 + c * 8 : a.dz;
+            cp_async16(smem_u32(As + swz(r, c, A_CPR)), g, ok);
+        }
+        for (int idx = tid; idx < kWK * B_CPR; idx += NT) {
+            const int r = idx / B_CPR, c = idx % B_CPR;
+            const int64_t p = pk + r;
+            bool ok = p < p_end;
+            const bf16* g = xs;
+            if (ok) {
+                const int x = (int)(p % a.w), y = (int)((p / a.w) % a.h);
+                const int64_t b = p / ((int64_t)a.w * a.h);
+                const int yy = y + dy, xx = x + dx;
+                ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+                if (ok) g = xs + ((b * a.h + yy) * a.w + xx) * xcs + xco + c * 8;
+            }
+            cp_async16(smem_u32(Bs + swz(r, c, B_CPR)), g, ok);
+        }
+    };
+
+    float acc[2][2][4];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
+
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
+        cp_async_commit();
+        const unsigned char* As = sm + (kt % kStages) * (A_BYTES + B_BYTES);
+        const unsigned char* Bs = As + A_BYTES;
+        for (int ks = 0; ks < 2; ++ks) {
+            const int kb = ks * 16;
+            uint32_t af[2][4], bfr[2][2];
+            for (int i = 0; i < 2; ++i) {   // A (m = c_out, k = pixel) stored [k][m]: transposed loads
+                const int r = kb + (lane & 7) + ((lane >> 4) << 3);
+                const int m = wm * 32 + i * 16 + (((lane >> 3) & 1) << 3);
+                ldsm_x4_t(smem_u32(As + swz(r, m >> 3, A_CPR)), af[i][0], af[i][1], af[i][2], af[i][3]);
+            }
+            {   // B (k = pixel, n = c_in) stored [k][n]: transposed loads, two n8 tiles
+                const int r = kb + (lane & 7) + (((lane >> 3) & 1) << 3);
+                const int n = wn * 16 + ((lane >> 4) << 3);
+                ldsm_x4_t(smem_u32(Bs + swz(r, n >> 3, B_CPR)), bfr[0][0], bfr[0][1], bfr[1][0], bfr[1][1]);
+            }
+            for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 2; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+        }
+    }
+    cp_async_wait<0>();
+
+    const int g = lane >> 2, t = lane & 3;
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int q = 0; q < 4; ++q) {
+                const int co = co0 + wm * 32 + i * 16 + g + 8 * (q >> 1);
+                const int ci = ci0 + wn * 16 + j * 8 + 2 * t + (q & 1);
+                atomicAdd(&a.dw[((int64_t)co * 9 + tap) * cin + ci], acc[i][j][q]);
+            }
+}
+
+// db[n] += sum_p dz[p][n]
+__global__ void bias_grad_kernel(const bf16* __restrict__ dz, int64_t P, int cout, float* db)
+{
+    extern __shared__ float red[];
+    const int c = threadIdx.x % cout, lanes = blockDim.x / cout, l = threadIdx.x / cout;
+    float s = 0.0f;
+    if (threadIdx.x < lanes * cout)
+        for (int64_t p = (int64_t)blockIdx.x * lanes + l; p < P; p += (int64_t)gridDim.x * lanes)
+            s += __bfloat162float(dz[p * cout + c]);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x < cout) {
+        float t = 0.0f;
+        for (int k = 0; k < lanes; ++k) t += red[k * cout + threadIdx.x];
+        atomicAdd(&db[threadIdx.x], t);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ glue
+// 2x2 average pooling, NHWC, h and w even
+__global__ void pool_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, bf16* __restrict__ y)
+{
+    const int ho = h / 2, wo = w / 2;
+    const int64_t total = (int64_t)nimg * ho * wo * c;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(q % c);
+        int64_t r = q / c;
+        const int X = (int)(r % wo);
+        r /= wo;
+        const int Y = (int)(r % ho);
+        const int64_t b = r / ho;
+        const int64_t s = ((b * h + 2 * Y) * w + 2 * X) * c + ch;
+        const float v = __bfloat162float(x[s]) + __bfloat162float(x[s + c]) + __bfloat162float(x[s + (int64_t)w * c]) +
+                        __bfloat162float(x[s + (int64_t)w * c + c]);
+        y[q] = __float2bfloat16(0.25f * v);
+    }
+}
+
+// dx (+)= pool backward of dy: every input pixel gets a quarter of its output's gradient
+__global__ void pool_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, bf16* __restrict__ dx,
+                                int accumulate)
+{
+    const int64_t total = (int64_t)nimg * h * w * c;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(q % c);
+        int64_t r = q / c;
+        const int x = (int)(r % w);
+        r /= w;
+        const int y = (int)(r % h);
+        const int64_t b = r / h;
+        float v = 0.25f * __bfloat162float(dy[((b * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch]);
+        if (accumulate) v += __bfloat162float(dx[q]);
+        dx[q] = __float2bfloat16(v);
+    }
+}
+
+// nearest 2x upsampling, NHWC (h, w: output size)
+__global__ void up_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, bf16* __restrict__ y)
+{
+    const int64_t total = (int64_t)nimg * h * w * c;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(q % c);
+        int64_t r = q / c;
+        const int xx = (int)(r % w);
+        r /= w;
+        const int yy = (int)(r % h);
+        const int64_t b = r / h;
+        y[q] = x[((b * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch];
+    }
+}
+
+// dx = sum of the four output gradients of each input pixel; dy has cs channels of which the first c are read
+__global__ void up_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, int cs, bf16* __restrict__ dx)
+{
+    const int ho = h / 2, wo = w / 2;
+    const int64_t total = (int64_t)nimg * ho * wo * c;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(q % c);
+        int64_t r = q / c;
+        const int X = (int)(r % wo);
+        r /= wo;
+        const int Y = (int)(r % ho);
+        const int64_t b = r / ho;
+        const int64_t s = ((b * h + 2 * Y) * w + 2 * X) * cs + ch;
+        const float v = __bfloat162float(dy[s]) + __bfloat162float(dy[s + cs]) +
+                        __bfloat162float(dy[s + (int64_t)w * cs]) + __bfloat162float(dy[s + (int64_t)w * cs + cs]);
+        dx[q] = __float2bfloat16(v);
+    }
+}
+
+// dz = dy * (y > 0) (ReLU backward through the layer's own output); dy may have cs >= c channels (first c read,
+// starting at channel offset co), with an optional second term dy2 [P][c] added first
+__global__ void relu_bwd_kernel(const bf16* __restrict__ dy, int cs, int co, const bf16* __restrict__ dy2,
+                                const bf16* __restrict__ y, int64_t P, int c, bf16* __restrict__ dz)
+{
+    const int64_t total = P * c;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(q % c);
+        const int64_t p = q / c;
+        float v = __bfloat162float(dy[p * cs + co + ch]);
+        if (dy2) v += __bfloat162float(dy2[q]);
+        dz[q] = __float2bfloat16(__bfloat162float(y[q]) > 0.0f ? v : 0.0f);
+    }
+}
+
+// head: out[p] = sum_{tap, c} x[p + off(tap)][c] wh[tap][c] + bh   (c_out = 1, FP32)
+__global__ void head_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, const float* __restrict__ wh,
+                                const float* __restrict__ bhp, float* __restrict__ out)
+{
+    const int64_t P = (int64_t)nimg * h * w;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % w), yy = (int)((p / w) % h);
+        const int64_t b = p / ((int64_t)w * h);
+        float s = *bhp;
+        for (int tap = 0; tap < 9; ++tap) {
+            const int y2 = yy + tap / 3 - 1, x2 = xx + tap % 3 - 1;
+            if (y2 < 0 || y2 >= h || x2 < 0 || x2 >= w) continue;
+            const bf16* xp = x + ((b * h + y2) * w + x2) * c;
+            const float* wp = wh + tap * c;
+            for (int k = 0; k < c; k += 2) {
+                const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(xp + k));
+                s += v.x * wp[k] + v.y * wp[k + 1];
+            }
+        }
+        out[p] = s;
+    }
+}
+
+// head backward: dx[p][c] = sum_tap dout[p - off(tap)] wh[tap][c]; dwh[tap][c] += sum_p dout[p] x[p + off(tap)][c];
+// dbh += sum_p dout[p]. A thread owns one channel pair (the grid stride is a multiple of c / 2) and keeps its
+// weight-gradient partial sums in registers.
+__global__ void head_bwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, const float* __restrict__ wh,
+                                const float* __restrict__ dout, bf16* __restrict__ dx, float* dwh, float* dbh)
+{
+    extern __shared__ float part[];   // [9 * c + 1]
+    for (int k = threadIdx.x; k < 9 * c + 1; k += blockDim.x) part[k] = 0.0f;
+    __syncthreads();
+    const int64_t P = (int64_t)nimg * h * w;
+    const int cp = c / 2;
+    const int64_t total = P * cp;
+    float gw[9][2], gb = 0.0f;
+    for (int tap = 0; tap < 9; ++tap) gw[tap][0] = gw[tap][1] = 0.0f;
+    const int k = 2 * (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) % cp);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = q / cp;
+        const int xx = (int)(p % w), yy = (int)((p / w) % h);
+        const int64_t b = p / ((int64_t)w * h);
+        float g0 = 0.0f, g1 = 0.0f;
+        const float d = dout[p];
+        for (int tap = 0; tap < 9; ++tap) {
+            const int oy = tap / 3 - 1, ox = tap % 3 - 1;
+            // data gradient: the output pixel p - off(tap) read this pixel through tap
+            const int ys = yy - oy, xs = xx - ox;
+            if (ys >= 0 && ys < h && xs >= 0 && xs < w) {
+                const float dd = dout[(b * h + ys) * w + xs];
+                g0 += dd * wh[tap * c + k];
+                g1 += dd * wh[tap * c + k + 1];
+            }
+            // weight gradient: this output pixel reads p + off(tap)
+            const int y2 = yy + oy, x2 = xx + ox;
+            if (y2 >= 0 && y2 < h && x2 >= 0 && x2 < w) {
+                const float2 v =
+                    __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(x + ((b * h + y2) * w + x2) * c + k));
+                gw[tap][0] += d * v.x;
+                gw[tap][1] += d * v.y;
+            }
+        }
+        if (dx) *reinterpret_cast<__nv_bfloat162*>(dx + p * c + k) = __floats2bfloat162_rn(g0, g1);
+        if (k == 0) gb += d;
+    }
+    for (int tap = 0; tap < 9; ++tap) {
+        atomicAdd(&part[tap * c + k], gw[tap][0]);
+        atomicAdd(&part[tap * c + k + 1], gw[tap][1]);
+    }
+    if (k == 0) atomicAdd(&part[9 * c], gb);
+    __syncthreads();
+    for (int j = threadIdx.x; j < 9 * c; j += blockDim.x) atomicAdd(&dwh[j], part[j]);
+    if (threadIdx.x == 0) atomicAdd(dbh, part[9 * c]);
+}
+
+// Adam step on FP32 master parameters; the BF16 copies of the convolution weights are rewritten
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float c1,
+                            float c2, bf16* __restrict__ p_bf16)
+{
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.0f - b1) * gq;
+        const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        const float pq = p[q] - lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+        p[q] = pq;
+        if (p_bf16) p_bf16[q] = __float2bfloat16(pq);
+    }
+}
+
+unsigned grid_for(int64_t n, int per = 256)
+{
+    int64_t g = (n + per - 1) / per;
+    if (g > 148 * 16) g = 148 * 16;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------ C ABI
+extern "C" {
+
+int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
+                       const void* wt, const float* bias, int32_t cout, int32_t relu, void* y, void* stream)
+{
+    if (nimg < 1 || h < 1 || w < 1 || !x1 || !wt || !y || c1 < 32 || c1 % 32 || c2 < 0 || c2 % 32 || (c2 && !x2) ||
+        cout < 32 || cout % 32)
+        return EDP_ERR_ARG;
+    ConvArgs a;
+    a.nimg = nimg;
+    a.h = h;
+    a.w = w;
+    a.x1 = (const bf16*)x1;
+    a.c1 = c1;
+    a.x2 = (const bf16*)x2;
+    a.c2 = c2;
+    a.wt = (const bf16*)wt;
+    a.bias = bias;
+    a.cout = cout;
+    a.relu = relu;
+    a.y = (bf16*)y;
+    const int64_t P = (int64_t)nimg * h * w;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cout % 64 == 0) {
+        dim3 grid((unsigned)((P + kBM - 1) / kBM), cout / 64);
+        conv3x3_fwd_kernel<64><<<grid, kConvThreads, 0, s>>>(a);
+    } else {
+        dim3 grid((unsigned)((P + kBM - 1) / kBM), cout / 32);
+        conv3x3_fwd_kernel<32><<<grid, kConvThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream)
+{
+    if (!wt || !out || cout < 1 || cin < 1) return EDP_ERR_ARG;
+    flip_transpose_kernel<<<grid_for((int64_t)cout * 9 * cin), 256, 0, (cudaStream_t)stream>>>(
+        (const bf16*)wt, cout, cin, (bf16*)out);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
+                         const void* dz, int32_t cout, float* dw, float* db, void* stream)
+{
+    if (nimg < 1 || h < 1 || w < 1 || !x1 || !dz || !dw || c1 < 32 || c1 % 32 || c2 < 0 || c2 % 32 ||
+        (c2 && !x2) || cout < 32 || cout % 32)
+        return EDP_ERR_ARG;
+    WgradArgs a;
+    a.nimg = nimg;
+    a.h = h;
+    a.w = w;
+    a.x = (const bf16*)x1;
+    a.c1 = c1;
+    a.x2 = (const bf16*)x2;
+    a.c2 = c2;
+    a.dz = (const bf16*)dz;
+    a.cout = cout;
+    a.dw = dw;
+    const int64_t P = (int64_t)nimg * h * w;
+    const int cin = c1 + c2;
+    const int bm = cout % 64 == 0 ? 64 : 32;
+    // the input-channel tile must not straddle the two concatenated tensors
+    const int bn = (cin % 64 == 0 && c1 % 64 == 0) ? 64 : 32;
+    const int64_t tiles = (int64_t)(cout / bm) * 9 * (cin / bn);
+    // K split: about 4 CTAs per SM overall, at least 1024 pixels per CTA
+    int64_t per = (P * tiles + 148 * 4 - 1) / (148 * 4);
+    if (per < 1024) per = 1024;
+    per = (per + kWK - 1) / kWK * kWK;
+    a.pix_per_cta = per;
+    dim3 grid((unsigned)((P + per - 1) / per), (unsigned)tiles);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (bm == 64 && bn == 64) conv3x3_wgrad_kernel<64, 64><<<grid, 256, 0, s>>>(a);
+    else if (bm == 64) conv3x3_wgrad_kernel<64, 32><<<grid, 128, 0, s>>>(a);
+    else if (bn == 64) conv3x3_wgrad_kernel<32, 64><<<grid, 128, 0, s>>>(a);
+    else conv3x3_wgrad_kernel<32, 32><<<grid, 64, 0, s>>>(a);
+    if (db) {
+        const int lanes = 1024 / cout;
+        bias_grad_kernel<<<grid_for(P, 1024), lanes * cout, lanes * cout * sizeof(float), s>>>((const bf16*)dz, P,
+                                                                                            cout, db);
+    }
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream)
+{
+    if (h % 2 || w % 2 || !x || !y) return EDP_ERR_ARG;
+    pool_fwd_kernel<<<grid_for((int64_t)nimg * h * w * c / 4), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, nimg, h,
+                                                                                            w, c, (bf16*)y);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* dy, void* dx, int32_t accumulate,
+                    void* stream)
+{
+    if (h % 2 || w % 2 || !dy || !dx) return EDP_ERR_ARG;
+    pool_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c), 256, 0, (cudaStream_t)stream>>>((const bf16*)dy, nimg, h, w,
+                                                                                        c, (bf16*)dx, accumulate);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream)
+{
+    if (h % 2 || w % 2 || !x || !y) return EDP_ERR_ARG;
+    up_fwd_kernel<<<grid_for((int64_t)nimg * h * w * c), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, nimg, h, w, c,
+                                                                                      (bf16*)y);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, const void* dy, void* dx,
+                        void* stream)
+{
+    if (h % 2 || w % 2 || !dy || !dx || cs < c) return EDP_ERR_ARG;
+    up_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c / 4), 256, 0, (cudaStream_t)stream>>>((const bf16*)dy, nimg, h,
+                                                                                          w, c, cs, (bf16*)dx);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_relu_bwd(int64_t P, int32_t c, const void* dy, int32_t cs, int32_t co, const void* dy2, const void* y,
+                    void* dz, void* stream)
+{
+    if (!dy || !y || !dz || cs < co + c) return EDP_ERR_ARG;
+    relu_bwd_kernel<<<grid_for(P * c), 256, 0, (cudaStream_t)stream>>>((const bf16*)dy, cs, co, (const bf16*)dy2,
+                                                                       (const bf16*)y, P, c, (bf16*)dz);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_head_fwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, const float* wh, const float* bh,
+                    float* out, void* stream)
+{
+    if (!x || !wh || !bh || !out || c % 2) return EDP_ERR_ARG;
+    head_fwd_kernel<<<grid_for((int64_t)nimg * h * w), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, nimg, h, w, c,
+                                                                                    wh, bh, out);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_head_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, const float* wh, const float* dout,
+                    void* dx, float* dwh, float* dbh, void* stream)
+{
+    if (!x || !wh || !dout || !dwh || !dbh || c % 2 || 256 % (c / 2)) return EDP_ERR_ARG;
+    head_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c / 2), 256, (9 * c + 1) * sizeof(float),
+                      (cudaStream_t)stream>>>((const bf16*)x, nimg, h, w, c, wh, dout, (bf16*)dx, dwh, dbh);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+int edp_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                int32_t step, void* p_bf16, void* stream)
+{
+    if (!p || !g || !m || !v || n < 1 || step < 1) return EDP_ERR_ARG;
+    const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+    adam_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, beta1, beta2, eps, c1, c2,
+                                                               (bf16*)p_bf16);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+}  // extern "C"

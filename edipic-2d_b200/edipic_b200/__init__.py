@@ -11,14 +11,14 @@ import numpy as np
 
 from . import _abi
 from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS,
-                   PREC_FP64, PREC_MIXED, PRECOND_MG, PRECOND_NONE, SOLVER_CG, SOLVER_FFTX, WARM_PREVIOUS, WARM_USER,
-                   WARM_ZERO, Counters,
+                   PREC_FP64, PREC_MIXED, PRECOND_MG, PRECOND_NONE, SOLVER_CG, SOLVER_FFTX, WARM_LEARNED, WARM_PREVIOUS,
+                   WARM_USER, WARM_ZERO, Counters,
                    Params, Tables)
 
 __all__ = ["Simulation", "EdpError", "read_deck", "library", "Params", "Tables", "Counters", "ELECTRONS", "IONS",
            "PREC_MIXED", "PREC_FP64", "SOLVER_FFTX", "SOLVER_CG", "FIELD_EX", "FIELD_EY", "FIELD_ACC_EX",
-           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER", "PRECOND_NONE",
-           "PRECOND_MG"]
+           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER", "WARM_LEARNED",
+           "PRECOND_NONE", "PRECOND_MG"]
 
 _lib = None
 
@@ -201,6 +201,20 @@ class Simulation:
         it = C.c_int32()
         self._check(self.lib.edp_field_cg(self.ctx, rtol, max_it, warm_start, C.byref(it)), "edp_field_cg")
         return it.value
+
+    def load_warm_start(self, theta):
+        """Loads the learned warm start's FP32 parameter vector (edipic_b200.warmstart.param_layout order)."""
+        a = np.ascontiguousarray(theta, dtype=np.float32)
+        self._check(self.lib.edp_warmstart_load(self.ctx, a.ctypes.data_as(C.POINTER(C.c_float)), a.size),
+                    "edp_warmstart_load")
+
+    def predict_warm_start(self):
+        """The network's guess for the current density (node layout) and the residual norms of the previous
+        potential and of the guess."""
+        g = self._node_array()
+        res = np.zeros(2)
+        self._check(self.lib.edp_warmstart_predict(self.ctx, _dp(g), _dp(res)), "edp_warmstart_predict")
+        return g, res
 
     def set_cg_preconditioner(self, kind):
         """PRECOND_MG (default): a multigrid V-cycle per CG iteration; PRECOND_NONE: plain CG."""

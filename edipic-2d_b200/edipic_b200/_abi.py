@@ -22,6 +22,7 @@ ELECTRONS, IONS = 0, 1
 FIELD_EX, FIELD_EY, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_PHI, FIELD_RHO_TOTAL = range(6)
 WARM_ZERO, WARM_PREVIOUS, WARM_USER = 0, 1, 2
 PRECOND_NONE, PRECOND_MG = 0, 1
+WARM_LEARNED = 3
 
 ERROR_NAMES = {
     ERR_ARG: "EDP_ERR_ARG", ERR_CUDA: "EDP_ERR_CUDA", ERR_CAPACITY: "EDP_ERR_CAPACITY",
@@ -110,6 +111,26 @@ SIGNATURES = {
     "edp_mcc_choose": [_CTX, C.c_int64, _D, _D, _I32],
     "edp_poisson_fftx_noalloc": [C.c_int32, C.c_int32, C.c_void_p, C.c_double, C.c_double, C.c_void_p,
                                  C.c_void_p],
+    "edp_warmstart_load": [_CTX, P(C.c_float), C.c_int64],
+    "edp_warmstart_predict": [_CTX, _D, _D],
+    "edp_nn_conv3x3_fwd": [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                           C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
+    "edp_nn_flip_transpose": [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
+    "edp_nn_conv3x3_wgrad": [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                             C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+    "edp_nn_pool": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+    "edp_nn_pool_bwd": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+    "edp_nn_upsample": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
+    "edp_nn_upsample_bwd": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                            C.c_void_p],
+    "edp_nn_relu_bwd": [C.c_int64, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                        C.c_void_p],
+    "edp_nn_head_fwd": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                        C.c_void_p],
+    "edp_nn_head_bwd": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                        C.c_void_p, C.c_void_p, C.c_void_p],
+    "edp_nn_adam": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_float,
+                    C.c_float, C.c_int32, C.c_void_p, C.c_void_p],
     "edp_deck_read": [C.c_char_p, P(C.c_void_p), P(Params), P(Tables)],
     "edp_deck_initial_plasma": [C.c_void_p, _D, _D, _D, _D, _I32, _D, _I64],
     "edp_deck_free": [C.c_void_p],

@@ -51,7 +51,10 @@ enum edp_field {
     EDP_FIELD_EX = 0, EDP_FIELD_EY = 1, EDP_FIELD_ACC_EX = 2, EDP_FIELD_ACC_EY = 3,
     EDP_FIELD_PHI = 4, EDP_FIELD_RHO_TOTAL = 5
 };
-enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2 };
+/* initial guess of edp_field_cg. LEARNED: the previous potential plus the update the loaded network
+ * (edp_warmstart_load) predicts from its residual against the new density; the previous potential is kept
+ * whenever the prediction's residual is not smaller. */
+enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2, EDP_WARM_LEARNED = 3 };
 /* preconditioner of edp_field_cg: NONE is Jacobi, which is plain CG here because the operator's diagonal is
  * constant; MG (the default) is one symmetric geometric-multigrid V-cycle per iteration */
 enum edp_precond { EDP_PRECOND_NONE = 0, EDP_PRECOND_MG = 1 };
@@ -231,6 +234,45 @@ int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const doubl
 #define EDP_NOALLOC_SCRATCH_BYTES (8u << 20)
 int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* rho_dev, double phi_bottom, double phi_top,
                              double* phi_dev, void* stream);
+
+/* ---- learned warm start of the CG solve ----------------------------------------------------------- */
+/* No counterpart in the reference (its PETSc solve always starts from zero). A 4-level convolutional
+ * encoder-decoder (channels 32-64-128-256, 3x3 kernels, 2x2 average pooling, nearest upsampling, skip
+ * concatenation, ReLU; BF16 weights and activations, FP32 accumulation) maps the residual r0 = b - A phi_prev of
+ * the previous potential, divided by its RMS s, and the Dirichlet mask to the update (phi - phi_prev) / (s K),
+ * K = L^2 / (2 pi^2) with L the larger cell count. blob holds FP32 parameters in the order
+ * EDP_WARMSTART_LAYERS lists: per convolution the weights [c_out][3][3][c_in] then the biases [c_out]; last the
+ * head's weights [3][3][32] and bias. */
+#define EDP_WARMSTART_N_CONV 14
+#define EDP_WARMSTART_LAYERS {{32, 32}, {32, 32}, {32, 64}, {64, 64}, {64, 128}, {128, 128}, {128, 256}, \
+                              {256, 256}, {384, 128}, {128, 128}, {192, 64}, {64, 64}, {96, 32}, {32, 32}}
+int edp_warmstart_load(edp_ctx* ctx, const float* blob, int64_t n_floats);
+/* the network's forward pass on the current residual: fills guess_out (reference node layout) with
+ * phi_prev + predicted update; the residual norms of phi_prev and of the guess go to res_out[0..1] */
+int edp_warmstart_predict(edp_ctx* ctx, double* guess_out, double* res_out);
+
+/* Kernels of the network, on caller-owned device memory and a caller stream (cudaStream_t), for training.
+ * Activations are NHWC BF16, c1, c2 and c_out multiples of 32 (c2 may be 0: one input tensor). */
+int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
+                       const void* wt, const float* bias, int32_t cout, int32_t relu, void* y, void* stream);
+int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream);
+int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
+                         const void* dz, int32_t cout, float* dw, float* db, void* stream);
+int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream);
+int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* dy, void* dx, int32_t accumulate,
+                    void* stream);
+int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream);
+int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, const void* dy, void* dx,
+                        void* stream);
+int edp_nn_relu_bwd(int64_t npix, int32_t c, const void* dy, int32_t cs, int32_t co, const void* dy2, const void* y,
+                    void* dz, void* stream);
+/* head: the 3x3 convolution to one FP32 output channel; bh points to its bias on the device */
+int edp_nn_head_fwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, const float* wh, const float* bh,
+                    float* out, void* stream);
+int edp_nn_head_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, const float* wh, const float* dout,
+                    void* dx, float* dwh, float* dbh, void* stream);
+int edp_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                int32_t step, void* p_bf16, void* stream);
 
 /* ---- deck reader (host side of INITIATE_PARAMETERS and the collision set-up) --------------------- */
 /* Reads init_configuration.dat, init_simcontrol.dat, init_particles.dat, init_extfields.dat,

@@ -1,0 +1,235 @@
+"""The learned warm start's network on the device against the oracle (oracle/nn_oracle.py): every kernel on
+BF16-rounded inputs, the whole forward and backward pass of the training wrapper, the C-ABI inference inside the CG
+solve against the training forward pass, and what a trained network gains over the previous-step warm start."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import nn_oracle as O
+from edipic_b200 import (FIELD_PHI, FIELD_RHO_TOTAL, PRECOND_MG, PRECOND_NONE, WARM_LEARNED, WARM_PREVIOUS,
+                         Simulation, decks, library, warmstart)
+
+torch = pytest.importorskip("torch")
+
+
+def _bf(a):
+    return torch.tensor(np.asarray(a, dtype=np.float32), device="cuda").to(torch.bfloat16)
+
+
+def _f32(a):
+    return torch.tensor(np.asarray(a, dtype=np.float32), device="cuda")
+
+
+def _np(t):
+    return t.detach().float().cpu().numpy().astype(np.float64)
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 0, 128), (256, 128, 128), (64, 32, 32), (128, 0, 96)])
+def test_conv_kernels_match_oracle(c1, c2, cout):
+    lib = library()
+    rng = np.random.default_rng(c1 + c2 + cout)
+    n, h, w = 2, 16, 24
+    x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
+    x2 = O.bf16(rng.normal(0, 1, (n, h, w, c2))) if c2 else None
+    cin = c1 + c2
+    wt = O.bf16(rng.normal(0, 1.0 / np.sqrt(9 * cin), (cout, 9, cin)))
+    b = rng.normal(0, 0.1, cout).astype(np.float32).astype(np.float64)
+    xin = x1 if c2 == 0 else np.concatenate([x1, x2], axis=-1)
+    tx1, tx2, tw, tb = _bf(x1), (_bf(x2) if c2 else None), _bf(wt), _f32(b)
+    y = torch.empty((n, h, w, cout), device="cuda", dtype=torch.bfloat16)
+    for relu in (0, 1):
+        assert lib.edp_nn_conv3x3_fwd(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tw), _p(tb), cout, relu, _p(y),
+                                      _stream()) == 0
+        ref = O.conv_fwd(xin, wt, b, relu=bool(relu))
+        assert _rel(_np(y), ref) < 8e-3   # BF16 output rounding
+    # data gradient: the forward kernel on the flipped, transposed weights
+    dz = O.bf16(rng.normal(0, 1, (n, h, w, cout)))
+    tdz = _bf(dz)
+    wtt = torch.empty((cin, 9, cout), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_flip_transpose(_p(tw), cout, cin, _p(wtt), _stream()) == 0
+    dx = torch.empty((n, h, w, cin), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_conv3x3_fwd(n, h, w, _p(tdz), cout, None, 0, _p(wtt), None, cin, 0, _p(dx), _stream()) == 0
+    assert _rel(_np(dx), O.conv_dgrad(dz, wt)) < 8e-3
+    # weight and bias gradients (FP32, accumulated)
+    dw = torch.zeros((cout, 9, cin), device="cuda", dtype=torch.float32)
+    db = torch.zeros(cout, device="cuda", dtype=torch.float32)
+    assert lib.edp_nn_conv3x3_wgrad(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tdz), cout, _p(dw), _p(db), _stream()) == 0
+    rw, rb = O.conv_wgrad(xin, dz)
+    assert _rel(_np(dw), rw) < 1e-5 and _rel(_np(db), rb) < 1e-5
+
+
+@pytest.mark.gpu
+def test_glue_kernels_match_oracle():
+    lib = library()
+    rng = np.random.default_rng(5)
+    n, h, w, c = 2, 16, 24, 64
+    x = O.bf16(rng.normal(0, 1, (n, h, w, c)))
+    tx = _bf(x)
+    y = torch.empty((n, h // 2, w // 2, c), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_pool(n, h, w, c, _p(tx), _p(y), _stream()) == 0
+    assert _rel(_np(y), O.pool(x)) < 5e-3
+    dy = O.bf16(rng.normal(0, 1, (n, h // 2, w // 2, c)))
+    dx = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_pool_bwd(n, h, w, c, _p(_bf(dy)), _p(dx), 0, _stream()) == 0
+    assert np.array_equal(_np(dx), O.pool_bwd(dy))
+    u = torch.empty((n, 2 * h, 2 * w, c), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_upsample(n, 2 * h, 2 * w, c, _p(tx), _p(u), _stream()) == 0
+    assert np.array_equal(_np(u), O.up(x))
+    du = O.bf16(rng.normal(0, 1, (n, 2 * h, 2 * w, c)))
+    dxu = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_upsample_bwd(n, 2 * h, 2 * w, c, c, _p(_bf(du)), _p(dxu), _stream()) == 0
+    assert _rel(_np(dxu), O.up_bwd(du)) < 5e-3
+    yy = O.bf16(rng.normal(0, 1, (n, h, w, c)))
+    dz = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
+    assert lib.edp_nn_relu_bwd(n * h * w, c, _p(tx), c, 0, None, _p(_bf(yy)), _p(dz), _stream()) == 0
+    assert np.array_equal(_np(dz), np.where(yy > 0, x, 0.0))
+    # head (32 channels to one FP32 output)
+    xh = O.bf16(rng.normal(0, 1, (n, h, w, 32)))
+    wh = rng.normal(0, 0.1, 9 * 32).astype(np.float32).astype(np.float64)
+    bh = np.array([0.25], dtype=np.float32)
+    out = torch.empty((n, h, w), device="cuda", dtype=torch.float32)
+    twh, tbh = _f32(wh), _f32(bh)
+    assert lib.edp_nn_head_fwd(n, h, w, 32, _p(_bf(xh)), _p(twh), _p(tbh), _p(out), _stream()) == 0
+    assert _rel(_np(out), O.head_fwd(xh, wh, 0.25)) < 1e-5
+    dout = rng.normal(0, 1, (n, h, w)).astype(np.float32).astype(np.float64)
+    dxh = torch.empty((n, h, w, 32), device="cuda", dtype=torch.bfloat16)
+    dwh = torch.zeros(9 * 32, device="cuda", dtype=torch.float32)
+    dbh = torch.zeros(1, device="cuda", dtype=torch.float32)
+    assert lib.edp_nn_head_bwd(n, h, w, 32, _p(_bf(xh)), _p(twh), _p(_f32(dout)), _p(dxh), _p(dwh), _p(dbh),
+                               _stream()) == 0
+    rdx, rdw, rdb = O.head_bwd(xh, wh, dout)
+    assert _rel(_np(dxh), rdx) < 5e-3 and _rel(_np(dwh), rdw) < 1e-5 and abs(float(dbh[0]) - rdb) < 1e-4 * abs(rdb) + 1e-4
+
+
+@pytest.mark.gpu
+def test_network_gradient_matches_oracle():
+    """Forward and backward of the training wrapper (torch.autograd.Function over the device kernels) against the
+    oracle's BF16-emulating FP64 pass on the same parameters and input."""
+    rng = np.random.default_rng(7)
+    theta = warmstart.init_params(seed=3)
+    theta[warmstart.param_layout()[1][0]:] *= 10.0   # a livelier head than at initialisation
+    x = O.bf16(rng.normal(0, 1, (2, 16, 24, 32)))
+    net = warmstart.WarmStartNet(theta)
+    out = net.forward(_bf(x))
+    dout = rng.normal(0, 1, tuple(out.shape))
+    (out * _f32(dout)).sum().backward()
+    g = _np(net.theta.grad)
+    rout, tape = O.net_forward(theta.astype(np.float64), x)
+    rg = O.net_backward(theta.astype(np.float64), tape, dout)
+    assert _rel(_np(out), rout) < 2e-2
+    cos = float(np.dot(g, rg) / (np.linalg.norm(g) * np.linalg.norm(rg)))
+    assert cos > 0.999
+    convs, (wh, bh), _ = warmstart.param_layout()
+    for (wo, bo, ci, co) in convs:
+        assert np.linalg.norm(g[wo:bo] - rg[wo:bo]) <= 5e-2 * np.linalg.norm(rg[wo:bo]) + 1e-6
+    assert np.linalg.norm(g[wh:bh] - rg[wh:bh]) <= 2e-2 * np.linalg.norm(rg[wh:bh])
+
+
+def _input_from_fields(rho_t, phi, unk, K):
+    """The network input and s of the library's inference, rebuilt on the host from rho_total and phi."""
+    ny, nx = phi.shape
+    H, W = warmstart.padded(ny), warmstart.padded(nx)
+    p = np.pad(phi, 1)
+    r0 = (rho_t - 4.0 * phi + p[1:-1, :-2] + p[1:-1, 2:] + p[:-2, 1:-1] + p[2:, 1:-1]) * unk
+    s = np.sqrt((r0 ** 2).sum() / unk.sum())
+    x = np.zeros((1, H, W, 32))
+    x[0, :ny, :nx, 0] = r0 / s
+    m = np.ones((H, W))
+    m[:ny, :nx] = 1.0 - unk
+    x[0, :, :, 1] = m
+    return x, s
+
+
+def _unknowns(p):
+    ny, nx = p.ncy + 1, p.ncx + 1
+    unk = np.zeros((ny, nx))
+    unk[1:-1, 1:-1] = 1.0
+    for o in range(p.n_inner):
+        unk[p.inner_jbottom[o]:p.inner_jtop[o] + 1, p.inner_ileft[o]:p.inner_iright[o] + 1] = 0.0
+    return unk
+
+
+@pytest.mark.gpu
+def test_library_inference_matches_training_forward(tmp_path):
+    d = decks.write_deck(str(tmp_path), "cfg2", ncx=64, ncy=48, ppc=16, inner=(20, 12, 36, 20, -100.0))
+    theta = warmstart.init_params(seed=11)
+    theta[warmstart.param_layout()[1][0]:] *= 10.0
+    with Simulation(d, sort_every=20) as sim:
+        p = sim.params
+        sim.distribute_particles(16)
+        sim.solve_potential_with_cg(rtol=1e-10)
+        for _ in range(2):
+            sim.advance_electrons()
+            sim.advance_ions()
+            sim.end_ion_cycle()
+        sim.load_warm_start(theta)
+        guess, res = sim.predict_warm_start()
+        phi = sim.field(FIELD_PHI)
+        rho_t = sim.field(FIELD_RHO_TOTAL)
+    unk = _unknowns(p)
+    K = warmstart.k_factor(p.ncx, p.ncy)
+    x, s = _input_from_fields(rho_t, phi, unk, K)
+    net = warmstart.WarmStartNet(theta)
+    with torch.no_grad():
+        out = _np(net.forward(_bf(x)))[0]
+    ny, nx = phi.shape
+    upd = s * K * out[:ny, :nx] * unk
+    assert np.abs(guess - phi - upd).max() <= 2e-2 * np.abs(upd).max()
+    assert np.allclose(guess[unk == 0], phi[unk == 0])
+    assert res[0] > 0 and np.isfinite(res[1])
+
+
+@pytest.mark.gpu
+def test_trained_warm_start_reduces_cg_work(tmp_path):
+    """Trained on the potential updates of short plain runs of one geometry family, the network's start has a
+    smaller residual than the previous potential on a held-out run, and CG needs fewer iterations from it."""
+    dirs = []
+    geo = [(20, 20, 36, 28, -100.0), (26, 30, 42, 38, -150.0), (16, 34, 32, 42, -60.0), (24, 22, 40, 30, -120.0)]
+    for k, g in enumerate(geo):
+        dirs.append(decks.write_deck(str(tmp_path / f"d{k}"), "cfg2", ncx=64, ncy=64, ppc=16, inner=g, seed=k))
+    torch.manual_seed(0)
+    dphi, unk = warmstart.generate_samples(dirs[:3], steps_per_deck=24, warmup=4)
+    K = warmstart.k_factor(64, 64)
+    net = warmstart.WarmStartNet(seed=0)
+    hist = warmstart.train(net, dphi, unk, K, steps=400, batch=8, lr=1e-3)
+    theta = net.blob()
+    its = {}
+    ratios = []
+    for mode in (WARM_PREVIOUS, WARM_LEARNED):
+        for pc in (PRECOND_NONE, PRECOND_MG):
+            with Simulation(dirs[3], sort_every=20, seed=5) as sim:
+                sim.set_cg_preconditioner(pc)
+                sim.load_warm_start(theta)
+                sim.distribute_particles(16)
+                n = []
+                for k in range(16):
+                    if mode == WARM_LEARNED and pc == PRECOND_NONE and k >= 4:
+                        _, res = sim.predict_warm_start()
+                        ratios.append(res[1] / res[0])
+                    it = sim.solve_potential_with_cg(rtol=1e-8, max_it=100000, warm_start=mode)
+                    if k >= 4:
+                        n.append(it)
+                    sim.advance_electrons()
+                    sim.advance_ions()
+                    sim.perform_electron_neutral_collisions()
+                    sim.perform_resonant_charge_exchange()
+                    sim.end_ion_cycle()
+                its[(mode, pc)] = float(np.mean(n))
+    print("train history", hist[-1:] if hist else None, "iterations", its, "residual ratio", np.mean(ratios))
+    assert np.mean(ratios) < 0.5
+    assert its[(WARM_LEARNED, PRECOND_NONE)] < its[(WARM_PREVIOUS, PRECOND_NONE)]
+    assert its[(WARM_LEARNED, PRECOND_MG)] <= its[(WARM_PREVIOUS, PRECOND_MG)] + 0.5
