@@ -164,15 +164,27 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
     rectangle at -100 V centred at (256, 128), 100 e- + 100 Ar+ per cell, the full collision set): each step of the
     cycle solves with CG to a 1e-8 relative residual from the previous step's potential. Timed by CUDA events
     around each solve (density, CG with its convergence reads, E)."""
-    from edipic_b200 import PRECOND_MG, PRECOND_NONE, Simulation, decks
+    from edipic_b200 import PRECOND_MG, PRECOND_NONE, WARM_LEARNED, WARM_PREVIOUS, Simulation, decks, warmstart
     import torch
     out = {"workload": "cfg2: 512x512 cells, inner metal rectangle 64x32 cells at -100 V, 100+100 per cell, "
-                       "CG to 1e-8 relative residual, previous-step warm start", "rtol": 1e-8}
-    for name, pc in (("plain_mg", PRECOND_MG), ("plain_nopc", PRECOND_NONE)):
+                       "CG to 1e-8 relative residual, previous-step (plain) or learned warm start", "rtol": 1e-8}
+    theta = None
+    wpath = os.path.join(ROOT, "edipic-2d_b200", "weights", "warmstart_cfg3.npz")
+    if os.path.exists(wpath):
+        theta = warmstart.load_blob(wpath)
+        out["weights"] = os.path.relpath(wpath, ROOT)
+    runs = [("plain_mg", PRECOND_MG, WARM_PREVIOUS), ("plain_nopc", PRECOND_NONE, WARM_PREVIOUS)]
+    if theta is not None:
+        runs += [("learned_mg", PRECOND_MG, WARM_LEARNED), ("learned_nopc", PRECOND_NONE, WARM_LEARNED)]
+    else:
+        out["learned"] = {"unavailable": "no trained weights (edipic_b200.train_warmstart writes them)"}
+    for name, pc, warm in runs:
         with tempfile.TemporaryDirectory() as tmp:
             d = decks.write_deck(tmp, "cfg2")
             with Simulation(d, sort_every=20, fuse_collisions=True, seed=2000) as sim:
                 sim.set_cg_preconditioner(pc)
+                if theta is not None:
+                    sim.load_warm_start(theta)
                 sim.distribute_particles(100)
                 stream = stream_of(sim)
                 lib, ctx, chk = sim.lib, sim.ctx, sim._check
@@ -182,7 +194,7 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
                     chk(lib.edp_update_wall_potentials(ctx, k), "wall")
                     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                     a.record(stream)
-                    chk(lib.edp_field_cg(ctx, 1e-8, 200000, 1, C.byref(it)), "cg")
+                    chk(lib.edp_field_cg(ctx, 1e-8, 200000, warm if k > 0 else WARM_PREVIOUS, C.byref(it)), "cg")
                     b.record(stream)
                     chk(lib.edp_advance_electrons(ctx), "adv_e")
                     chk(lib.edp_advance_ions(ctx), "adv_i")
@@ -195,7 +207,14 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
                         iters.append(it.value)
         out[name] = {"ms_per_step": sum(times) / len(times), "cg_iterations_mean": sum(iters) / len(iters),
                      "cg_iterations_max": max(iters), "steps": steps,
-                     "preconditioner": "multigrid V(2,2) RB-GS" if pc == PRECOND_MG else "none (Jacobi = plain)"}
+                     "preconditioner": "multigrid V(2,2) RB-GS" if pc == PRECOND_MG else "none (Jacobi = plain)",
+                     "warm_start": "learned" if warm == WARM_LEARNED else "previous step"}
+    for pcn in ("mg", "nopc"):
+        if f"learned_{pcn}" in out:
+            pl, le = out[f"plain_{pcn}"], out[f"learned_{pcn}"]
+            out[f"learned_over_plain_{pcn}"] = {
+                "cg_iteration_ratio": pl["cg_iterations_mean"] / max(le["cg_iterations_mean"], 1e-9),
+                "ms_ratio": pl["ms_per_step"] / le["ms_per_step"]}
     return out
 
 

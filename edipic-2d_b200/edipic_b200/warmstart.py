@@ -313,3 +313,44 @@ def generate_samples(deck_dirs, steps_per_deck, warmup=4, precision=None, rtol=1
     dphi = torch.tensor(np.stack(out_d), device="cuda")
     unk = torch.tensor(np.stack(out_u), device="cuda")
     return dphi, unk
+
+
+# ------------------------------------------------------------------------------------------ cfg3 family
+def cfg3_geometries(n, seed=0, ncx=512, ncy=512):
+    """Object rectangles of the learned-warm-start training set: 64 x 32 cells centred at (256, 128) jittered by up to
+    +-64 cells per axis, biased uniformly in [-200, 0] V (scaled to the grid when it is not 512 x 512)."""
+    rng = np.random.default_rng(seed)
+    sx, sy = ncx / 512.0, ncy / 512.0
+    out = []
+    for _ in range(n):
+        cx = int(round((256 + rng.uniform(-64, 64)) * sx))
+        cy = int(round((128 + rng.uniform(-64, 64)) * sy))
+        hw, hh = max(1, int(round(32 * sx))), max(1, int(round(16 * sy)))
+        out.append((cx - hw, cy - hh, cx + hw, cy + hh, float(rng.uniform(-200.0, 0.0))))
+    return out
+
+
+def save_blob(path, theta):
+    """Convolution weights as BF16 bits (the device uses them as BF16), biases and head as FP32."""
+    convs, (wh, bh), n = param_layout()
+    theta = np.asarray(theta, dtype=np.float32)
+    wmask = np.zeros(n, dtype=bool)
+    for (wo, bo, ci, co) in convs:
+        wmask[wo:bo] = True
+    bits = theta[wmask].view(np.uint32)
+    bits = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16).astype(np.uint16)
+    np.savez_compressed(path, w_bf16=bits, rest_f32=theta[~wmask], n=np.int64(n))
+
+
+def load_blob(path):
+    z = np.load(path)
+    convs, _, n = param_layout()
+    if int(z["n"]) != n:
+        raise ValueError(f"{path}: {int(z['n'])} parameters, the network has {n}")
+    wmask = np.zeros(n, dtype=bool)
+    for (wo, bo, ci, co) in convs:
+        wmask[wo:bo] = True
+    theta = np.zeros(n, dtype=np.float32)
+    theta[wmask] = (z["w_bf16"].astype(np.uint32) << 16).view(np.float32)
+    theta[~wmask] = z["rest_f32"]
+    return theta
