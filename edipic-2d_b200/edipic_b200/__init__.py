@@ -263,6 +263,14 @@ class Simulation:
         self._check(self.lib.edp_moments(self.ctx, species, _dp(out)), "edp_moments")
         return out
 
+    def collect_moments(self, species):
+        """COLLECT_ELECTRON_MOMENTS / COLLECT_ION_MOMENTS: [13, ny, nx] FP32 in the reference node layout (N, VX,
+        VY, VZ, WX, WY, WZ, VXVY, VXVZ, VYVZ, QX, QY, QZ)."""
+        out = np.zeros((13, self.ny_ref, self.nx_ref), dtype=np.float32)
+        self._check(self.lib.edp_collect_moments(self.ctx, species, out.ctypes.data_as(C.POINTER(C.c_float))),
+                    "edp_collect_moments")
+        return out
+
     def mcc_choose(self, energy_ev, r):
         e = np.ascontiguousarray(energy_ev, dtype=np.float64)
         rr = np.ascontiguousarray(r, dtype=np.float64)

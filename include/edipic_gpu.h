@@ -214,6 +214,11 @@ int edp_set_field(edp_ctx* ctx, int which, const double* in);
 /* FP64 sums of report_total_number_of_particles (pic2d_Diagnostics.f90:321-460): N, sum vx, vy, vz,
  * sum vx^2, vy^2, vz^2 for one species */
 int edp_moments(edp_ctx* ctx, int species, double out[7]);
+/* COLLECT_ELECTRON_MOMENTS (pic2d_ElectronMoments.f90:3-425; what ADVANCE_ELECTRONS_PLUS deposits on a snapshot
+ * step, before the push) / COLLECT_ION_MOMENTS (pic2d_IonMoments.f90:3-348) with the current field: 13 node grids
+ * in the reference layout, out[m][j][i], m = N, VX, VY, VZ, WX, WY, WZ, VXVY, VXVZ, VYVZ, QX, QY, QZ (cs_N ...
+ * cs_QZ after normalisation and ADJUST_DENSITY_AT_WALL_BOUNDARIES). */
+int edp_collect_moments(edp_ctx* ctx, int species, float* out);
 /* kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:447-485) evaluated on the device for given
  * (energy, r) pairs: kind_out[k] = indx_coll (n_act+1 = null collision) */
 int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const double* r, int32_t* kind_out);

@@ -232,6 +232,120 @@ void oracle_deposit(const oracle_geom_t* g, const oracle_parts_t* p, double weig
 }
 
 // periodic fold :1661-1667 and wall factors :1802-1880
+// COLLECT_ELECTRON_MOMENTS (pic2d_ElectronMoments.f90:3-425) and COLLECT_ION_MOMENTS (pic2d_IonMoments.f90:3-348):
+// 13 CIC-weighted node sums at the particles' current positions (weights in REAL arithmetic :148-157), of the
+// velocity v = (VX, VY, VZ) for ions (pic2d_IonMoments.f90:154-166) and, for electrons, of the mean of the stored
+// velocity and its Boris update with the current field (:159-243); overlap columns folded
+// (SYNCHRONIZE_MOMENTS_IN_OVERLAP_NODES, :353 and :428-), normalised per node (:356-419) and the density scaled at
+// the walls (ADJUST_DENSITY_AT_WALL_BOUNDARIES :422 and :1829-1934, one cluster: flat walls x2, corners x4). out[m * nodes + node], m = N, VX, VY, VZ, WX, WY, WZ,
+// VXVY, VXVZ, VYVZ, QX, QY, QZ. Sums are kept in FP64 (the reference keeps REAL).
+void oracle_collect_moments(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                            const oracle_parts_t* p, double* out)
+{
+    const Area a = area_of(g);
+    const int nx = oracle_nx_nodes(g);
+    const int64_t nn = (int64_t)nx * (g->ncy + 1);
+    for (int64_t q = 0; q < 13 * nn; ++q) out[q] = 0.0;
+    for (int64_t k = 0; k < p->n; ++k) {
+        const double X = p->x[k], Y = p->y[k];
+        int i = (int)X, j = (int)Y;
+        if (X == a.xmax) i = a.ixmax - 1;
+        if (Y == a.ymax) j = a.jymax - 1;
+        const float ax_ip1 = (float)(X - (double)i), ax_i = 1.0f - ax_ip1;
+        const float ay_jp1 = (float)(Y - (double)j), ay_j = 1.0f - ay_jp1;
+        const float vij = ax_i * ay_j, vip1j = ax_ip1 * ay_j, vijp1 = ax_i * ay_jp1;
+        const float vip1jp1 = 1.0f - vij - vip1j - vijp1;
+        double ux = p->vx[k], uy = p->vy[k], uz = p->vz[k];
+        if (!sp->is_ion) {
+            const double dx1 = X - (double)i, dx0 = 1.0 - dx1, dy1 = Y - (double)j, dy0 = 1.0 - dy1;
+            const double E_X = EX[node(g, i, j)] * dx0 * dy0 + EX[node(g, i + 1, j)] * dx1 * dy0 +
+                               EX[node(g, i, j + 1)] * dx0 * dy1 + EX[node(g, i + 1, j + 1)] * dx1 * dy1;
+            const double E_Y = EY[node(g, i, j)] * dx0 * dy0 + EY[node(g, i + 1, j)] * dx1 * dy0 +
+                               EY[node(g, i, j + 1)] * dx0 * dy1 + EY[node(g, i + 1, j + 1)] * dx1 * dy1;
+            const double E_Z = sp->ez;
+            const double alfa_x = -0.5 * sp->bx, alfa_y = -0.5 * sp->by, alfa_z = -0.5 * sp->bz;
+            const double ax2 = alfa_x * alfa_x, ay2 = alfa_y * alfa_y, az2 = alfa_z * alfa_z;
+            const double theta2 = ax2 + ay2 + az2, inv = 1.0 / (1.0 + theta2);
+            const double K11 = (1.0 - theta2 + 2.0 * ax2) * inv, K12 = 2.0 * (alfa_x * alfa_y + alfa_z) * inv,
+                         K13 = 2.0 * (alfa_x * alfa_z - alfa_y) * inv;
+            const double K21 = 2.0 * (alfa_x * alfa_y - alfa_z) * inv, K22 = (1.0 - theta2 + 2.0 * ay2) * inv,
+                         K23 = 2.0 * (alfa_y * alfa_z + alfa_x) * inv;
+            const double K31 = 2.0 * (alfa_x * alfa_z + alfa_y) * inv, K32 = 2.0 * (alfa_y * alfa_z - alfa_x) * inv,
+                         K33 = (1.0 - theta2 + 2.0 * az2) * inv;
+            const double VXm = ux - 0.5 * E_X, VYm = uy - 0.5 * E_Y, VZm = uz - 0.5 * E_Z;
+            const double nvx = K11 * VXm + K12 * VYm + K13 * VZm - 0.5 * E_X;
+            const double nvy = K21 * VXm + K22 * VYm + K23 * VZm - 0.5 * E_Y;
+            const double nvz = K31 * VXm + K32 * VYm + K33 * VZm - 0.5 * E_Z;
+            ux = 0.5 * (ux + nvx);
+            uy = 0.5 * (uy + nvy);
+            uz = 0.5 * (uz + nvz);
+        }
+        const float rvx = (float)ux, rvy = (float)uy, rvz = (float)uz;
+        const float rvx2 = rvx * rvx, rvy2 = rvy * rvy, rvz2 = rvz * rvz;
+        const float v2 = rvx2 + rvy2 + rvz2;
+        const float m[13] = {1.0f, rvx, rvy, rvz, rvx2, rvy2, rvz2, rvx * rvy, rvx * rvz, rvy * rvz,
+                             v2 * rvx, v2 * rvy, v2 * rvz};
+        const int64_t n00 = node(g, i, j), n10 = node(g, i + 1, j), n01 = node(g, i, j + 1), n11 = node(g, i + 1, j + 1);
+        for (int q = 0; q < 13; ++q) {
+            double* o = out + q * nn;
+            o[n00] += (double)(m[q] * vij);
+            o[n10] += (double)(m[q] * vip1j);
+            o[n01] += (double)(m[q] * vijp1);
+            o[n11] += (double)(m[q] * vip1jp1);
+        }
+    }
+    if (g->periodic) {   // overlap columns, as the density fold
+        const int imax = nx - 1;
+        for (int q = 0; q < 13; ++q) {
+            double* o = out + q * nn;
+            for (int j = 0; j <= g->ncy; ++j) {
+                o[node(g, 1, j)] += o[node(g, imax, j)];
+                o[node(g, imax - 1, j)] += o[node(g, 0, j)];
+                o[node(g, 0, j)] = o[node(g, imax - 1, j)];
+                o[node(g, imax, j)] = o[node(g, 1, j)];
+            }
+        }
+    }
+    for (int64_t nd = 0; nd < nn; ++nd) {
+        double* c[13];
+        for (int q = 0; q < 13; ++q) c[q] = out + q * nn + nd;
+        if (*c[0] > 1.0e-9) {
+            const double inv_N = 1.0 / *c[0];
+            for (int q = 1; q <= 6; ++q) *c[q] *= inv_N;
+            for (int q = 7; q <= 9; ++q) *c[q] = 2.0 * *c[q] * inv_N;
+            const double vx = *c[1], vy = *c[2], vz = *c[3], wx = *c[4], wy = *c[5], wz = *c[6];
+            double t = vx * vx + vy * vy + vz * vz;
+            t = t + t - wx - wy - wz;
+            *c[10] = *c[10] * inv_N + (t - wx - wx) * vx - *c[7] * vy - *c[8] * vz;
+            *c[11] = *c[11] * inv_N - *c[7] * vx + (t - wy - wy) * vy - *c[9] * vz;
+            *c[12] = *c[12] * inv_N - *c[8] * vx - *c[9] * vy + (t - wz - wz) * vz;
+        } else {
+            for (int q = 0; q < 13; ++q) *c[q] = 0.0;
+        }
+    }
+    double* N = out;
+    const int imax = nx - 1, jmax = g->ncy;
+    if (g->periodic) {
+        for (int i = 0; i <= imax; ++i) {
+            N[node(g, i, jmax)] *= 2.0;
+            N[node(g, i, 0)] *= 2.0;
+        }
+        return;
+    }
+    for (int j = 1; j <= jmax - 1; ++j) {
+        N[node(g, 0, j)] *= 2.0;
+        N[node(g, imax, j)] *= 2.0;
+    }
+    for (int i = 1; i <= imax - 1; ++i) {
+        N[node(g, i, jmax)] *= 2.0;
+        N[node(g, i, 0)] *= 2.0;
+    }
+    N[node(g, 0, 0)] *= 4.0;
+    N[node(g, 0, jmax)] *= 4.0;
+    N[node(g, imax, 0)] *= 4.0;
+    N[node(g, imax, jmax)] *= 4.0;
+}
+
 void oracle_fold_and_wall_scale(const oracle_geom_t* g, double* rho)
 {
     const int nx = oracle_nx_nodes(g);

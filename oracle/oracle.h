@@ -62,6 +62,11 @@ void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const doubl
 void oracle_deposit(const oracle_geom_t* g, const oracle_parts_t* p, double weight, double* rho);
 /* periodic fold (:1661-1667) and wall factors (:1802-1880) */
 void oracle_fold_and_wall_scale(const oracle_geom_t* g, double* rho);
+/* COLLECT_ELECTRON_MOMENTS (pic2d_ElectronMoments.f90:3-425) / COLLECT_ION_MOMENTS (pic2d_IonMoments.f90:3-348)
+ * with the overlap fold, normalisation and ADJUST_DENSITY_AT_WALL_BOUNDARIES: out[13 * nodes] (N, VX, VY, VZ,
+ * WX, WY, WZ, VXVY, VXVZ, VYVZ, QX, QY, QZ); EX/EY are used for electrons only. */
+void oracle_collect_moments(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                            const oracle_parts_t* p, double* out);
 
 /* ---------------------------------------------------------------- Maxwell sampler */
 /* PrepareMaxwellDistribIntegral (pic2d_ElectronWallCollisions.f90:835-929); v[0..9000], v_inj[0..4500] */

@@ -88,6 +88,7 @@ def lib():
             "oracle_push": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
             "oracle_fold_and_wall_scale": ([C.POINTER(Geom), _D], None),
+            "oracle_collect_moments": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _D], None),
             "oracle_maxwell_tables": ([_D, _D], None),
             "oracle_maxwell_sample": ([_D, C.c_double], C.c_double),
             "oracle_en_frequency": ([C.POINTER(Crsect), C.c_double, C.c_double, C.c_int32, C.c_double], C.c_double),
@@ -194,6 +195,17 @@ def deposit(g, parts, weight=1.0, fold=True):
     if fold:
         lib().oracle_fold_and_wall_scale(C.byref(g), dp(rho))
     return rho
+
+
+def collect_moments(g, sp, ex, ey, parts):
+    """COLLECT_ELECTRON_MOMENTS / COLLECT_ION_MOMENTS: [13, ny, nx] (N, VX, VY, VZ, WX, WY, WZ, VXVY, VXVZ, VYVZ,
+    QX, QY, QZ)."""
+    ny, nx = nodes_shape(g)
+    out = np.zeros((13, ny, nx))
+    ex = np.ascontiguousarray(ex if ex is not None else np.zeros((ny, nx)))
+    ey = np.ascontiguousarray(ey if ey is not None else np.zeros((ny, nx)))
+    lib().oracle_collect_moments(C.byref(g), C.byref(sp), dp(ex), dp(ey), C.byref(parts.s), dp(out))
+    return out
 
 
 def fftx_solve(g, rho_total, phi_bottom=0.0, phi_top=0.0):
