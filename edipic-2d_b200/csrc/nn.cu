@@ -182,6 +182,204 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_fwd_kernel(ConvArgs a)
         }
 }
 
+// ------------------------------------------------------------------------------------------ forward on tcgen05
+// The same implicit GEMM on the 5th-generation tensor cores: a CTA owns 128 pixels x BN output channels, its FP32
+// accumulator lives in tensor memory (BN columns x 128 lanes). K = 9 c_in runs in 64-wide stages (4 MMAs of
+// K = 16 each); a stage holds A (128 rows) and B (BN rows) of 128 bytes each in the K-major 128-byte-swizzled layout
+// (8-row atoms of 1024 bytes, 16-byte chunk index XOR row % 8). The 128 threads gather the stage with cp.async
+// (zero-fill for padding and for K past 9 c_in), thread 0 issues the MMAs and commits them to the stage's mbarrier,
+// which frees the stage for the gather kernel-stages later. Every wait is bounded: on timeout the kernel raises
+// *err, still waits (bounded) for its MMAs, frees its tensor memory and returns.
+constexpr int kTcThreads = 128, kTcStages = 4, kTcBK = 64;
+constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls; a healthy wait ends far sooner
+
+struct TcArgs {
+    ConvArgs c;
+    int* err;
+};
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
+{
+    // start address >> 4 | leading offset 16 B (unused by swizzled K-major) | stride 1024 B between 8-row atoms |
+    // descriptor version 1 | layout SWIZZLE_128B
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P;\n\t}\n"
+                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta)
+{
+    constexpr int A_BYTES = 128 * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+    extern __shared__ unsigned char dsm[];
+    __shared__ __align__(8) uint64_t bars[kTcStages];
+    __shared__ uint32_t tmem_base_sh;
+    const ConvArgs& a = ta.c;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (smem_u32(dsm) + 1023u) & ~1023u;   // swizzle atoms need 1024-byte alignment
+    const int64_t P = (int64_t)a.nimg * a.h * a.w;
+    const int64_t m0 = (int64_t)blockIdx.x * 128;
+    const int n0 = blockIdx.y * BN;
+    const int cin = a.c1 + a.c2, K = 9 * cin;
+    const int KT = (K + kTcBK - 1) / kTcBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0)
+        for (int s = 0; s < kTcStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])));
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    // this thread gathers A row `tid` (one pixel) of every stage
+    const int64_t p_row = m0 + tid;
+    const bool row_ok = p_row < P;
+    const int64_t pp = row_ok ? p_row : 0;
+    const int rx = (int)(pp % a.w), ry = (int)((pp / a.w) % a.h);
+    const int64_t rb = pp / ((int64_t)a.w * a.h);
+
+    auto load_stage = [&](int s, int kt) {
+        const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
+        const int k0 = kt * kTcBK;
+        int tap = k0 / cin;
+        for (int c = 0; c < 8; ++c) {
+            const int k = k0 + 8 * c;
+            if (k - tap * cin >= cin) ++tap;
+            const int ci = k - tap * cin;
+            bool ok = row_ok && k < K;
+            const bf16* g = a.x1;
+            if (ok) {
+                const int yy = ry + tap / 3 - 1, xx = rx + tap % 3 - 1;
+                ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+                if (ok) {
+                    const int64_t pix = (rb * a.h + yy) * a.w + xx;
+                    g = ci < a.c1 ? a.x1 + pix * a.c1 + ci : a.x2 + pix * a.c2 + (ci - a.c1);
+                }
+            }
+            cp_async16(As + tid * 128 + ((c ^ (tid & 7)) << 4), g, ok);
+        }
+        for (int idx = tid; idx < BN * 8; idx += kTcThreads) {
+            const int r = idx >> 3, c = idx & 7;
+            const int k = k0 + 8 * c;
+            const bool ok = k < K;
+            const bf16* g = ok ? a.wt + (int64_t)(n0 + r) * K + k : a.wt;
+            cp_async16(Bs + r * 128 + ((c ^ (r & 7)) << 4), g, ok);
+        }
+    };
+
+    bool timed_out = false;
+    for (int s = 0; s < kTcStages - 1; ++s) {
+        if (s < KT) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < KT; ++kt) {
+        const int s = kt % kTcStages;
+        cp_async_wait<kTcStages - 2>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // gathered bytes -> tensor-core reads
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
+            for (int ks = 0; ks < kTcBK / 16; ++ks) {
+                const uint64_t da = umma_desc_sw128(As + 32 * ks), db = umma_desc_sw128(Bs + 32 * ks);
+                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                             ::"r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         ::"r"(smem_u32(&bars[s])) : "memory");
+        }
+        const int nxt = kt + kTcStages - 1;
+        if (nxt < KT) {
+            if (kt >= 1 && !timed_out) {   // the stage refilled now was read by the MMAs of chunk kt - 1
+                const int sp = (kt - 1) % kTcStages;
+                if (!mbar_wait(smem_u32(&bars[sp]), (uint32_t)(((kt - 1) / kTcStages) & 1))) timed_out = true;
+            }
+            load_stage(nxt % kTcStages, nxt);
+        }
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+    // all MMAs of this CTA are done once the last commit has arrived
+    const bool done = mbar_wait(smem_u32(&bars[(KT - 1) % kTcStages]), (uint32_t)(((KT - 1) / kTcStages) & 1));
+    if (!done || timed_out) {
+        if (tid == 0) atomicExch(ta.err, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (done) {
+        // epilogue: warp w owns tensor-memory lanes (pixels) 32 w .. 32 w + 31
+        const int64_t p = m0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                         " [%16];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                           "=r"(r[14]), "=r"(r[15])
+                         : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (p < P) {
+                uint32_t pk[8];
+                for (int q = 0; q < 8; ++q) {
+                    const int n = n0 + c0 + 2 * q;
+                    float v0 = __uint_as_float(r[2 * q]) + (a.bias ? a.bias[n] : 0.0f);
+                    float v1 = __uint_as_float(r[2 * q + 1]) + (a.bias ? a.bias[n + 1] : 0.0f);
+                    if (a.relu) {
+                        v0 = fmaxf(v0, 0.0f);
+                        v1 = fmaxf(v1, 0.0f);
+                    }
+                    __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+                    pk[q] = *reinterpret_cast<uint32_t*>(&h);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.cout + n0 + c0);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+template <int BN>
+int launch_tc(const ConvArgs& c, int* err, cudaStream_t s)
+{
+    constexpr int SMEM = kTcStages * (128 * 128 + BN * 128) + 1024;
+    if (cudaFuncSetAttribute(conv3x3_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
+        cudaSuccess)
+        return EDP_ERR_CUDA;
+    const int64_t P = (int64_t)c.nimg * c.h * c.w;
+    TcArgs ta;
+    ta.c = c;
+    ta.err = err;
+    dim3 grid((unsigned)((P + 127) / 128), c.cout / BN);
+    conv3x3_fwd_tc_kernel<BN><<<grid, kTcThreads, SMEM, s>>>(ta);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
 // wt_t[c][8 - tap][n] = wt[n][tap][c]: the weights of the data gradient
 __global__ void flip_transpose_kernel(const bf16* __restrict__ wt, int cout, int cin, bf16* __restrict__ out)
 {
@@ -507,6 +705,19 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
     }
 }
 
+// one device word per GPU for the bounded waits of the tcgen05 kernels
+int* tc_error_word()
+{
+    static int* words[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!words[dev]) {
+        if (cudaMalloc(&words[dev], sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(words[dev], 0, sizeof(int)) != cudaSuccess) return nullptr;
+    }
+    return words[dev];
+}
+
 unsigned grid_for(int64_t n, int per = 256)
 {
     int64_t g = (n + per - 1) / per;
@@ -523,7 +734,7 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
                        const void* wt, const float* bias, int32_t cout, int32_t relu, void* y, void* stream)
 {
     if (nimg < 1 || h < 1 || w < 1 || !x1 || !wt || !y || c1 < 32 || c1 % 32 || c2 < 0 || c2 % 32 || (c2 && !x2) ||
-        cout < 32 || cout % 32)
+        cout < 32 || cout % 32 || c1 + c2 > 1024)
         return EDP_ERR_ARG;
     ConvArgs a;
     a.nimg = nimg;
@@ -538,16 +749,31 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
     a.cout = cout;
     a.relu = relu;
     a.y = (bf16*)y;
-    const int64_t P = (int64_t)nimg * h * w;
     cudaStream_t s = (cudaStream_t)stream;
-    if (cout % 64 == 0) {
-        dim3 grid((unsigned)((P + kBM - 1) / kBM), cout / 64);
-        conv3x3_fwd_kernel<64><<<grid, kConvThreads, 0, s>>>(a);
-    } else {
-        dim3 grid((unsigned)((P + kBM - 1) / kBM), cout / 32);
-        conv3x3_fwd_kernel<32><<<grid, kConvThreads, 0, s>>>(a);
+    int* err = tc_error_word();
+    if (!err) return EDP_ERR_CUDA;
+    switch (cout) {   // one CTA covers all output channels (two halves above 256)
+    case 32: return launch_tc<32>(a, err, s);
+    case 64: return launch_tc<64>(a, err, s);
+    case 96: return launch_tc<96>(a, err, s);
+    case 128: return launch_tc<128>(a, err, s);
+    case 192: return launch_tc<192>(a, err, s);
+    case 256: return launch_tc<256>(a, err, s);
+    case 384: return launch_tc<192>(a, err, s);
+    default: return EDP_ERR_ARG;
     }
-    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+/* bounded-wait error word of the tcgen05 kernels: nonzero once a wait gave up; reading clears it */
+int edp_nn_error(int32_t* out)
+{
+    int* err = tc_error_word();
+    if (!err || !out) return EDP_ERR_ARG;
+    int h = 0;
+    if (cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return EDP_ERR_CUDA;
+    if (h && cudaMemset(err, 0, sizeof(int)) != cudaSuccess) return EDP_ERR_CUDA;
+    *out = h;
+    return EDP_OK;
 }
 
 int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream)

@@ -261,6 +261,8 @@ int edp_warmstart_predict(edp_ctx* ctx, double* guess_out, double* res_out);
 int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
                        const void* wt, const float* bias, int32_t cout, int32_t relu, void* y, void* stream);
 int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream);
+/* nonzero in *out when a bounded wait of the tensor-core convolution gave up since the last call (then cleared) */
+int edp_nn_error(int32_t* out);
 int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
                          const void* dz, int32_t cout, float* dw, float* db, void* stream);
 int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream);

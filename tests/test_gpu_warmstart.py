@@ -38,11 +38,15 @@ def _rel(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 0, 128), (256, 128, 128), (64, 32, 32), (128, 0, 96)])
-def test_conv_kernels_match_oracle(c1, c2, cout):
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 0, 128), (256, 128, 128), (64, 32, 32), (128, 0, 96),
+                                        (128, 0, 256), (64, 128, 64)])
+@pytest.mark.parametrize("n,h,w", [(2, 16, 24), (1, 13, 21)])
+def test_conv_kernels_match_oracle(c1, c2, cout, n, h, w):
+    """Forward (tcgen05 tensor cores, one CTA per 128 pixels and all output channels), data gradient through the
+    same kernel on the flipped weights, weight and bias gradients; pixel counts that do and do not fill the last
+    128-pixel tile."""
     lib = library()
-    rng = np.random.default_rng(c1 + c2 + cout)
-    n, h, w = 2, 16, 24
+    rng = np.random.default_rng(c1 + c2 + cout + h)
     x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
     x2 = O.bf16(rng.normal(0, 1, (n, h, w, c2))) if c2 else None
     cin = c1 + c2
@@ -70,6 +74,8 @@ def test_conv_kernels_match_oracle(c1, c2, cout):
     assert lib.edp_nn_conv3x3_wgrad(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tdz), cout, _p(dw), _p(db), _stream()) == 0
     rw, rb = O.conv_wgrad(xin, dz)
     assert _rel(_np(dw), rw) < 1e-5 and _rel(_np(db), rb) < 1e-5
+    flag = C.c_int32(-1)
+    assert lib.edp_nn_error(C.byref(flag)) == 0 and flag.value == 0
 
 
 @pytest.mark.gpu
