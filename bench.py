@@ -159,6 +159,65 @@ def fp64_cycle_leg(args, stream_of):
             "path": "FP64 particles and FP64 atomic deposit, same kernels' FP64 variants, whole cycle incl. FFT_X"}
 
 
+def network_leg():
+    """The learned warm start's convolutions on the tensor cores: each of the 14 layers of the encoder-decoder timed
+    alone at the inference shape (one 520 x 520 image, the padded 513 x 513 node grid) and at the training shape
+    (4 images), and the whole forward pass. FLOPs = 2 x pixels x 9 x c_in x c_out per layer."""
+    import torch
+    from edipic_b200 import library, warmstart
+    lib = library()
+    H = W = 520
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        peak, peak_kind = 1590.0, "fallback"
+    scale = [1, 1, 2, 2, 4, 4, 8, 8, 4, 4, 2, 2, 1, 1]
+    net = warmstart.WarmStartNet(seed=0)
+    out = {"shape": f"{H}x{W}", "peak_tflops": peak, "peak_kind": peak_kind}
+    st = torch.cuda.current_stream()
+    for nb in (1, 4):
+        tot_t, tot_f, per = 0.0, 0.0, []
+        for l, (ci, co) in enumerate(warmstart.LAYERS):
+            h, w = H // scale[l], W // scale[l]
+            x = torch.randn(nb, h, w, ci, device="cuda").to(torch.bfloat16)
+            y = torch.empty(nb, h, w, co, device="cuda", dtype=torch.bfloat16)
+            wo, bo, _, _ = net.convs[l]
+            wb, bb = net.theta_bf[wo:bo], net.theta[bo:bo + co].detach()
+            args = (nb, h, w, C.c_void_p(x.data_ptr()), ci, None, 0, C.c_void_p(wb.data_ptr()),
+                    C.c_void_p(bb.data_ptr()), co, 1, C.c_void_p(y.data_ptr()), C.c_void_p(st.cuda_stream))
+            for _ in range(3):
+                lib.edp_nn_conv3x3_fwd(*args)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 20
+            e0.record(st)
+            for _ in range(reps):
+                lib.edp_nn_conv3x3_fwd(*args)
+            e1.record(st)
+            e1.synchronize()
+            t = e0.elapsed_time(e1) / 1e3 / reps
+            f = 2.0 * nb * h * w * 9 * ci * co
+            tot_t += t
+            tot_f += f
+            per.append({"layer": l, "cin": ci, "cout": co, "hw": [h, w], "us": 1e6 * t, "tflops": f / t / 1e12})
+        x = torch.randn(nb, H, W, 32, device="cuda").to(torch.bfloat16)
+        with torch.no_grad():
+            for _ in range(3):
+                net.forward(x)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(10):
+                net.forward(x)
+            e1.record(st)
+            e1.synchronize()
+        fwd = e0.elapsed_time(e1) / 10
+        out[f"batch{nb}"] = {"conv_ms": 1e3 * tot_t, "conv_gflop": tot_f / 1e9, "conv_tflops": tot_f / tot_t / 1e12,
+                             "frac": tot_f / tot_t / 1e12 / peak, "forward_ms": fwd, "layers": per}
+    return out
+
+
 def poisson_leg(args, stream_of, warmup=10, steps=30):
     """Poisson ms/step on the inner-object geometry (512 x 512 cells, metal walls at 0 V, a 64 x 32-cell metal
     rectangle at -100 V centred at (256, 128), 100 e- + 100 Ar+ per cell, the full collision set): each step of the
@@ -396,6 +455,13 @@ def run_ours(args):
             line["fp64_gpu_cycle"] = fp64_cycle_leg(args, stream_of)
             line["fp64_gpu_cycle"]["mixed_over_fp64"] = value / line["fp64_gpu_cycle"]["value"]
             line["poisson"] = poisson_leg(args, stream_of)
+            line["network"] = network_leg()
+            line["roofline_conv"] = {"bound": "tensor", "achieved": line["network"]["batch4"]["conv_tflops"],
+                                     "peak": line["network"]["peak_tflops"], "unit": "TFLOP/s",
+                                     "frac": line["network"]["batch4"]["frac"], "traffic": None,
+                                     "basis": "14 tcgen05 convolutions of the warm-start network, 4 x 520 x 520, "
+                                              "2 x pixels x 9 x c_in x c_out FLOPs, peak bf16 "
+                                              + line["network"]["peak_kind"]}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args, d)
         print(json.dumps(line), flush=True)

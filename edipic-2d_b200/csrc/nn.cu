@@ -73,124 +73,17 @@ struct ConvArgs {
     bf16* y;          // [P][cout]
 };
 
-constexpr int kBM = 128, kBK = 32, kStages = 3, kConvThreads = 256;
-
-template <int BN>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_fwd_kernel(ConvArgs a)
-{
-    constexpr int WARPS_N = BN / 32, WARPS_M = 8 / WARPS_N;
-    constexpr int WM = kBM / WARPS_M;          // 32 (BN 64) or 16 (BN 32)
-    constexpr int MI = WM / 16, NI = 4;        // m16 tiles and n8 tiles per warp
-    constexpr int A_BYTES = kBM * kBK * 2, B_BYTES = BN * kBK * 2;
-    __shared__ __align__(128) unsigned char sm[kStages * (A_BYTES + B_BYTES)];
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp % WARPS_M, wn = warp / WARPS_M;
-    const int64_t P = (int64_t)a.nimg * a.h * a.w;
-    const int64_t m0 = (int64_t)blockIdx.x * kBM;
-    const int n0 = blockIdx.y * BN;
-    const int cin = a.c1 + a.c2;
-    const int kc = cin / kBK;
-    const int KT = 9 * kc;
-
-    // the two A rows this thread loads: pixel coordinates
-    int ay[2], ax[2], ab[2], arow[2], achk[2];
-    bool aval[2];
-    for (int i = 0; i < 2; ++i) {
-        const int idx = tid + kConvThreads * i;
-        arow[i] = idx >> 2;
-        achk[i] = idx & 3;
-        const int64_t p = m0 + arow[i];
-        aval[i] = p < P;
-        const int64_t pp = aval[i] ? p : 0;
-        ax[i] = (int)(pp % a.w);
-        ay[i] = (int)((pp / a.w) % a.h);
-        ab[i] = (int)(pp / ((int64_t)a.w * a.h));
-    }
-
-    auto load_stage = [&](int s, int kt) {
-        unsigned char* As = sm + s * (A_BYTES + B_BYTES);
-        unsigned char* Bs = As + A_BYTES;
-        const int tap = kt / kc, cc = kt % kc;
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-        const int ci0 = cc * kBK;
-        const bf16* src;
-        int cs, cof;
-        if (ci0 < a.c1) { src = a.x1; cs = a.c1; cof = ci0; }
-        else { src = a.x2; cs = a.c2; cof = ci0 - a.c1; }
-        for (int i = 0; i < 2; ++i) {
-            const int yy = ay[i] + dy, xx = ax[i] + dx;
-            const bool ok = aval[i] && yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
-            const bf16* g = ok ? src + (((int64_t)ab[i] * a.h + yy) * a.w + xx) * cs + cof + achk[i] * 8 : src;
-            cp_async16(smem_u32(As + swz(arow[i], achk[i], 4)), g, ok);
-        }
-        for (int idx = tid; idx < BN * 4; idx += kConvThreads) {
-            const int r = idx >> 2, c = idx & 3;
-            const bf16* g = a.wt + ((int64_t)(n0 + r) * 9 + tap) * cin + ci0 + c * 8;
-            cp_async16(smem_u32(Bs + swz(r, c, 4)), g, true);
-        }
-    };
-
-    float acc[MI][NI][4];
-    for (int i = 0; i < MI; ++i)
-        for (int j = 0; j < NI; ++j)
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
-
-    for (int s = 0; s < kStages - 1; ++s) {
-        if (s < KT) load_stage(s, s);
-        cp_async_commit();
-    }
-    for (int kt = 0; kt < KT; ++kt) {
-        cp_async_wait<kStages - 2>();
-        __syncthreads();
-        if (kt + kStages - 1 < KT) load_stage((kt + kStages - 1) % kStages, kt + kStages - 1);
-        cp_async_commit();
-        const unsigned char* As = sm + (kt % kStages) * (A_BYTES + B_BYTES);
-        const unsigned char* Bs = As + A_BYTES;
-        for (int ks = 0; ks < 2; ++ks) {
-            uint32_t af[MI][4], bfr[NI][2];
-            for (int i = 0; i < MI; ++i) {
-                const int r = wm * WM + i * 16 + (lane & 15);
-                ldsm_x4(smem_u32(As + swz(r, 2 * ks + (lane >> 4), 4)), af[i][0], af[i][1], af[i][2], af[i][3]);
-            }
-            for (int j = 0; j < NI / 2; ++j) {
-                const int r = wn * 32 + j * 16 + (lane & 7) + ((lane >> 4) << 3);
-                ldsm_x4(smem_u32(Bs + swz(r, 2 * ks + ((lane >> 3) & 1), 4)), bfr[2 * j][0], bfr[2 * j][1],
-                        bfr[2 * j + 1][0], bfr[2 * j + 1][1]);
-            }
-            for (int i = 0; i < MI; ++i)
-                for (int j = 0; j < NI; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
-        }
-    }
-    cp_async_wait<0>();
-
-    const int g = lane >> 2, t = lane & 3;
-    for (int i = 0; i < MI; ++i)
-        for (int j = 0; j < NI; ++j) {
-            const int n = n0 + wn * 32 + j * 8 + 2 * t;
-            const float b0 = a.bias ? a.bias[n] : 0.0f, b1 = a.bias ? a.bias[n + 1] : 0.0f;
-            for (int hlf = 0; hlf < 2; ++hlf) {
-                const int64_t p = m0 + wm * WM + i * 16 + g + 8 * hlf;
-                if (p >= P) continue;
-                float v0 = acc[i][j][2 * hlf] + b0, v1 = acc[i][j][2 * hlf + 1] + b1;
-                if (a.relu) {
-                    v0 = fmaxf(v0, 0.0f);
-                    v1 = fmaxf(v1, 0.0f);
-                }
-                *reinterpret_cast<__nv_bfloat162*>(a.y + p * a.cout + n) = __floats2bfloat162_rn(v0, v1);
-            }
-        }
-}
+constexpr int kStages = 3;   // cp.async pipeline depth of the weight-gradient kernel
 
 // ------------------------------------------------------------------------------------------ forward on tcgen05
 // The same implicit GEMM on the 5th-generation tensor cores: a CTA owns 128 pixels x BN output channels, its FP32
 // accumulator lives in tensor memory (BN columns x 128 lanes). K = 9 c_in runs in 64-wide stages (4 MMAs of
 // K = 16 each); a stage holds A (128 rows) and B (BN rows) of 128 bytes each in the K-major 128-byte-swizzled layout
-// (8-row atoms of 1024 bytes, 16-byte chunk index XOR row % 8). The 128 threads gather the stage with cp.async
+// (8-row atoms of 1024 bytes, 16-byte chunk index XOR row % 8). The 256 threads gather the stage with cp.async
 // (zero-fill for padding and for K past 9 c_in), thread 0 issues the MMAs and commits them to the stage's mbarrier,
-// which frees the stage for the gather kernel-stages later. Every wait is bounded: on timeout the kernel raises
-// *err, still waits (bounded) for its MMAs, frees its tensor memory and returns.
-constexpr int kTcThreads = 128, kTcStages = 4, kTcBK = 64;
+// which frees the stage for a later gather. Every wait is bounded: on timeout the kernel raises *err, still waits
+// (bounded) for its MMAs, frees its tensor memory and returns.
+constexpr int kTcThreads = 256, kTcBK = 64;
 constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls; a healthy wait ends far sooner
 
 struct TcArgs {
@@ -218,15 +111,20 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     return false;
 }
 
+// Stage kt: chunk kt of K (64 wide) is gathered two stages ahead (cp.async, two threads per pixel row, four 16-byte
+// pieces each); thread 0 issues its 4 MMAs once everybody's pieces landed, and before a stage is refilled thread 0
+// alone waits for the MMAs that read it (two chunks back) while the other threads sleep in the block barrier.
 template <int BN>
 __global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta)
 {
+    constexpr int STAGES = 4, AHEAD = 2;   // chunks gathered ahead; two chunks of MMAs stay in flight
     constexpr int A_BYTES = 128 * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
     constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
     extern __shared__ unsigned char dsm[];
-    __shared__ __align__(8) uint64_t bars[kTcStages];
+    __shared__ __align__(8) uint64_t bars[STAGES];
     __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
     const ConvArgs& a = ta.c;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (smem_u32(dsm) + 1023u) & ~1023u;   // swizzle atoms need 1024-byte alignment
@@ -241,59 +139,76 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
-    if (tid == 0)
-        for (int s = 0; s < kTcStages; ++s)
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int s = 0; s < STAGES; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])));
+    }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
 
-    // this thread gathers A row `tid` (one pixel) of every stage
-    const int64_t p_row = m0 + tid;
+    // this thread gathers half (pieces 4 h .. 4 h + 3) of A row `row` (one pixel) of every stage
+    const int row = tid >> 1, half = tid & 1;
+    const int64_t p_row = m0 + row;
     const bool row_ok = p_row < P;
-    const int64_t pp = row_ok ? p_row : 0;
-    const int rx = (int)(pp % a.w), ry = (int)((pp / a.w) % a.h);
-    const int64_t rb = pp / ((int64_t)a.w * a.h);
+    const int64_t pix0 = row_ok ? p_row : 0;   // tap t reads pix0 + (t / 3 - 1) w + (t % 3 - 1)
+    uint32_t tap_ok = 0;                       // bit t: the pixel under tap t lies inside the image
+    if (row_ok) {
+        const int rx = (int)(pix0 % a.w), ry = (int)((pix0 / a.w) % a.h);
+        for (int t = 0; t < 9; ++t) {
+            const int yy = ry + t / 3 - 1, xx = rx + t % 3 - 1;
+            if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w) tap_ok |= 1u << t;
+        }
+    }
+    const uint32_t a_row = (uint32_t)row * 128u;
+    const int rsw = row & 7;
 
     auto load_stage = [&](int s, int kt) {
         const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
-        const int k0 = kt * kTcBK;
+        const int k0 = kt * kTcBK + 32 * half;
         int tap = k0 / cin;
-        for (int c = 0; c < 8; ++c) {
-            const int k = k0 + 8 * c;
-            if (k - tap * cin >= cin) ++tap;
-            const int ci = k - tap * cin;
-            bool ok = row_ok && k < K;
+        int ci = k0 - tap * cin;
+        for (int c = 0; c < 4; ++c) {
+            if (ci >= cin) {
+                ci -= cin;
+                ++tap;
+            }
+            const bool ok = tap < 9 && ((tap_ok >> tap) & 1u);
             const bf16* g = a.x1;
             if (ok) {
-                const int yy = ry + tap / 3 - 1, xx = rx + tap % 3 - 1;
-                ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
-                if (ok) {
-                    const int64_t pix = (rb * a.h + yy) * a.w + xx;
-                    g = ci < a.c1 ? a.x1 + pix * a.c1 + ci : a.x2 + pix * a.c2 + (ci - a.c1);
-                }
+                const int64_t pix = pix0 + (int64_t)(tap / 3 - 1) * a.w + (tap % 3 - 1);
+                g = ci < a.c1 ? a.x1 + pix * a.c1 + ci : a.x2 + pix * a.c2 + (ci - a.c1);
             }
-            cp_async16(As + tid * 128 + ((c ^ (tid & 7)) << 4), g, ok);
+            const int cc = 4 * half + c;
+            cp_async16(As + a_row + ((cc ^ rsw) << 4), g, ok);
+            ci += 8;
         }
+        const int k00 = kt * kTcBK;
         for (int idx = tid; idx < BN * 8; idx += kTcThreads) {
             const int r = idx >> 3, c = idx & 7;
-            const int k = k0 + 8 * c;
+            const int k = k00 + 8 * c;
             const bool ok = k < K;
             const bf16* g = ok ? a.wt + (int64_t)(n0 + r) * K + k : a.wt;
             cp_async16(Bs + r * 128 + ((c ^ (r & 7)) << 4), g, ok);
         }
     };
 
-    bool timed_out = false;
-    for (int s = 0; s < kTcStages - 1; ++s) {
+    for (int s = 0; s < AHEAD; ++s) {
         if (s < KT) load_stage(s, s);
         cp_async_commit();
     }
     for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt % kTcStages;
-        cp_async_wait<kTcStages - 2>();
+        const int s = kt % STAGES;
+        cp_async_wait<AHEAD - 1>();
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // gathered bytes -> tensor-core reads
+        const int nxt = kt + AHEAD;
+        if (tid == 0 && nxt < KT && nxt >= STAGES && fail_sh == 0) {
+            // the stage chunk nxt refills was read by the MMAs of chunk nxt - STAGES
+            const int old = nxt - STAGES;
+            if (!mbar_wait(smem_u32(&bars[old % STAGES]), (uint32_t)((old / STAGES) & 1))) fail_sh = 1;
+        }
         __syncthreads();
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -308,34 +223,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                          ::"r"(smem_u32(&bars[s])) : "memory");
         }
-        const int nxt = kt + kTcStages - 1;
-        if (nxt < KT) {
-            if (kt >= 1 && !timed_out) {   // the stage refilled now was read by the MMAs of chunk kt - 1
-                const int sp = (kt - 1) % kTcStages;
-                if (!mbar_wait(smem_u32(&bars[sp]), (uint32_t)(((kt - 1) / kTcStages) & 1))) timed_out = true;
-            }
-            load_stage(nxt % kTcStages, nxt);
-        }
+        if (nxt < KT) load_stage(nxt % STAGES, nxt);
         cp_async_commit();
     }
     cp_async_wait<0>();
-    // all MMAs of this CTA are done once the last commit has arrived
-    const bool done = mbar_wait(smem_u32(&bars[(KT - 1) % kTcStages]), (uint32_t)(((KT - 1) / kTcStages) & 1));
-    if (!done || timed_out) {
-        if (tid == 0) atomicExch(ta.err, 1);
+    // all MMAs of this CTA are done once the last commit has arrived (commits complete in order)
+    if (tid == 0) {
+        const int last = KT - 1;
+        if (!mbar_wait(smem_u32(&bars[last % STAGES]), (uint32_t)((last / STAGES) & 1))) fail_sh = 2;
+        if (fail_sh) atomicExch(ta.err, 1);
     }
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (done) {
-        // epilogue: warp w owns tensor-memory lanes (pixels) 32 w .. 32 w + 31
-        const int64_t p = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+    if (fail_sh != 2) {
+        // epilogue: warp w reads tensor-memory lanes (pixels) 32 (w % 4) .. + 31, column half w / 4
+        const int wl = warp & 3, wh = warp >> 2;
+        const int cols = BN / 2;
+        const int64_t p = m0 + wl * 32 + lane;
+        for (int c0 = wh * cols; c0 < (wh + 1) * cols; c0 += 16) {
             uint32_t r[16];
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
                          " [%16];\n"
                          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
                            "=r"(r[14]), "=r"(r[15])
-                         : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+                         : "r"(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             if (p < P) {
                 uint32_t pk[8];
@@ -367,7 +279,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta
 template <int BN>
 int launch_tc(const ConvArgs& c, int* err, cudaStream_t s)
 {
-    constexpr int SMEM = kTcStages * (128 * 128 + BN * 128) + 1024;
+    constexpr int SMEM = 4 * (128 * 128 + BN * 128) + 1024;
     if (cudaFuncSetAttribute(conv3x3_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
         cudaSuccess)
         return EDP_ERR_CUDA;
