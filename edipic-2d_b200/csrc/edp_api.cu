@@ -1048,6 +1048,7 @@ int edp_query_counters(edp_ctx* c, edp_counters* out)
     if (c->hc->error_flags & EDP_EFLAG_CAPACITY) return edp_fail(c, EDP_ERR_CAPACITY, "particle capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "particle outside the domain");
+    if (c->hc->error_flags & EDP_EFLAG_TIMEOUT) return edp_fail(c, EDP_ERR_TIMEOUT, "a bounded device wait gave up");
     return EDP_OK;
 }
 

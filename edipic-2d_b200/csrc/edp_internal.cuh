@@ -29,6 +29,7 @@
 #define EDP_EFLAG_CAPACITY 1
 #define EDP_EFLAG_BOUNDS 2
 #define EDP_EFLAG_PENDING 4
+#define EDP_EFLAG_TIMEOUT 8   // a bounded device-side wait gave up
 
 struct edp_chunk {      // one CTA work item of the sorted push
     int64_t start, end; // slot range
