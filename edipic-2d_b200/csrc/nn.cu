@@ -280,9 +280,15 @@ template <int BN>
 int launch_tc(const ConvArgs& c, int* err, cudaStream_t s)
 {
     constexpr int SMEM = 4 * (128 * 128 + BN * 128) + 1024;
-    if (cudaFuncSetAttribute(conv3x3_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
-        cudaSuccess)
-        return EDP_ERR_CUDA;
+    static bool configured[64] = {false};   // the shared-memory opt-in, once per device and tile width
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(conv3x3_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
+            cudaSuccess)
+            return EDP_ERR_CUDA;
+        configured[dev] = true;
+    }
     const int64_t P = (int64_t)c.nimg * c.h * c.w;
     TcArgs ta;
     ta.c = c;
