@@ -12,6 +12,7 @@
 // concatenation of two tensors (the decoder's upsampled path and the encoder's skip), read in place.
 #include "edp_internal.cuh"
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 namespace {
@@ -296,6 +297,261 @@ int launch_tc(const ConvArgs& c, int* err, cudaStream_t s)
     dim3 grid((unsigned)((P + 127) / 128), c.cout / BN);
     conv3x3_fwd_tc_kernel<BN><<<grid, kTcThreads, SMEM, s>>>(ta);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------------------------------ forward on TMA + tcgen05
+// The same implicit GEMM with both operands brought in by the tensor memory access unit. A CTA owns a 16 x 8-pixel
+// patch of one image (128 rows of A) and BN output channels. K runs in chunks of CW channels of one tap
+// (CW = 64, or 32 when c_in or the concatenation split is not a multiple of 64): A is the 4-D box
+// (CW channels, 16 x, 8 y, 1 image) at (c, x0 + dx, y0 + dy, n) of the NHWC activations, zero-filled where the
+// patch leaves the image, B the 2-D box (CW, BN) at (k, n0) of the [c_out][9 c_in] weights; both arrive in the
+// K-major swizzled layout the MMA descriptors name (128-byte swizzle for CW = 64, 64-byte for CW = 32). Thread 0
+// issues the copies (expect-tx on the stage's full barrier) and the MMAs (committed to the stage's empty barrier);
+// the other warps join for the epilogue. Every wait is bounded.
+struct TmaArgs {
+    int nimg, h, w, c1, c2, cout, relu, tiles_x, tiles_y;
+    const float* bias;
+    bf16* y;
+    int* err;
+};
+
+template <int BN, int CW>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    conv3x3_fwd_tma_kernel(const __grid_constant__ CUtensorMap mx1, const __grid_constant__ CUtensorMap mx2,
+                           const __grid_constant__ CUtensorMap mw, TmaArgs ta)
+{
+    constexpr int STAGES = 4;
+    constexpr int A_BYTES = 128 * CW * 2, B_BYTES = BN * CW * 2, STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+    // K-major descriptor: 8-row atoms of 8 x (CW * 2) bytes, layout 2 = 128-byte swizzle, 4 = 64-byte swizzle
+    constexpr uint64_t DESC_HI = ((uint64_t)((8 * CW * 2) >> 4) << 32) | ((uint64_t)1 << 46) |
+                                 ((uint64_t)(CW == 64 ? 2 : 4) << 61) | ((uint64_t)1 << 16);
+    extern __shared__ unsigned char dsm[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (smem_u32(dsm) + 1023u) & ~1023u;
+    const int tile = blockIdx.x;
+    const int tx = tile % ta.tiles_x, ty = (tile / ta.tiles_x) % ta.tiles_y, img = tile / (ta.tiles_x * ta.tiles_y);
+    const int x0 = tx * 16, y0 = ty * 8;
+    const int n0 = blockIdx.y * BN;
+    const int cin = ta.c1 + ta.c2;
+    const int KT = 9 * cin / CW;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    if (tid == 0) {
+        auto issue = [&](int kt) {
+            const int s = kt % STAGES;
+            const uint32_t As = base + s * STAGE, Bs = As + A_BYTES, fb = smem_u32(&full[s]);
+            const int k0 = kt * CW, tap = k0 / cin, ci = k0 - tap * cin;
+            const int xx = x0 + tap % 3 - 1, yy = y0 + tap / 3 - 1;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(STAGE) : "memory");
+            const CUtensorMap* ma = ci < ta.c1 ? &mx1 : &mx2;
+            const int ca = ci < ta.c1 ? ci : ci - ta.c1;
+            asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                         ::"r"(As), "l"(ma), "r"(ca), "r"(xx), "r"(yy), "r"(img), "r"(fb) : "memory");
+            asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                         ::"r"(Bs), "l"(&mw), "r"(k0), "r"(n0), "r"(fb) : "memory");
+        };
+        int issued = 0;
+        for (; issued < STAGES - 1 && issued < KT; ++issued) issue(issued);
+        int kt = 0;
+        for (; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((kt / STAGES) & 1))) {
+                fail_sh = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
+            for (int ks = 0; ks < CW / 16; ++ks) {
+                const uint64_t da = DESC_HI | (uint64_t)(((As + 32 * ks) >> 4) & 0x3FFFu);
+                const uint64_t db = DESC_HI | (uint64_t)(((Bs + 32 * ks) >> 4) & 0x3FFFu);
+                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                             ::"r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         ::"r"(smem_u32(&empty[s])) : "memory");
+            if (issued < KT) {   // chunk `issued` reuses the stage of chunk issued - STAGES = kt - 1
+                const int old = issued - STAGES;
+                if (old >= 0 && !mbar_wait(smem_u32(&empty[old % STAGES]), (uint32_t)((old / STAGES) & 1))) {
+                    fail_sh = 1;
+                    ++kt;
+                    break;
+                }
+                issue(issued++);
+            }
+        }
+        // copies in flight and the last MMAs finish before the epilogue reads or the CTA leaves
+        for (int q = kt; q < issued; ++q) mbar_wait(smem_u32(&full[q % STAGES]), (uint32_t)((q / STAGES) & 1));
+        if (kt > 0 && !mbar_wait(smem_u32(&empty[(kt - 1) % STAGES]), (uint32_t)(((kt - 1) / STAGES) & 1)))
+            fail_sh = 2;
+        if (fail_sh) atomicExch(ta.err, 1);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (fail_sh == 0) {
+        // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (patch rows), column half w / 4
+        const int wl = warp & 3, wh = warp >> 2;
+        const int cols = BN / 2;
+        const int r = wl * 32 + lane;
+        const int px = x0 + (r & 15), py = y0 + (r >> 4);
+        const bool inside = px < ta.w && py < ta.h;
+        const int64_t p = ((int64_t)img * ta.h + py) * ta.w + px;
+        for (int c0 = wh * cols; c0 < (wh + 1) * cols; c0 += 16) {
+            uint32_t v[16];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                         " [%16];\n"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                           "=r"(v[14]), "=r"(v[15])
+                         : "r"(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (inside) {
+                uint32_t pk[8];
+                for (int q = 0; q < 8; ++q) {
+                    const int n = n0 + c0 + 2 * q;
+                    float v0 = __uint_as_float(v[2 * q]) + (ta.bias ? ta.bias[n] : 0.0f);
+                    float v1 = __uint_as_float(v[2 * q + 1]) + (ta.bias ? ta.bias[n + 1] : 0.0f);
+                    if (ta.relu) {
+                        v0 = fmaxf(v0, 0.0f);
+                        v1 = fmaxf(v1, 0.0f);
+                    }
+                    __nv_bfloat162 h2 = __floats2bfloat162_rn(v0, v1);
+                    pk[q] = *reinterpret_cast<uint32_t*>(&h2);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(ta.y + p * ta.cout + n0 + c0);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// NHWC activations with c channels: dims (c, w, h, n), box (cw, 16, 8, 1)
+bool map_act(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int cw)
+{
+    EncodeTiledFn f = encode_fn();
+    if (!f) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
+    const cuuint32_t box[4] = {(cuuint32_t)cw, 16, 8, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, cw == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// weights [cout][k]: dims (k, cout), box (cw, bn)
+bool map_wt(CUtensorMap* m, const void* wt, int k, int cout, int cw, int bn)
+{
+    EncodeTiledFn f = encode_fn();
+    if (!f) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)cout};
+    const cuuint64_t strides[1] = {(cuuint64_t)k * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)cw, (cuuint32_t)bn};
+    const cuuint32_t estr[2] = {1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(wt), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, cw == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int CW>
+int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
+{
+    constexpr int SMEM = 4 * (128 * CW * 2 + BN * CW * 2) + 1024;
+    static bool configured[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(conv3x3_fwd_tma_kernel<BN, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
+            cudaSuccess)
+            return EDP_ERR_CUDA;
+        configured[dev] = true;
+    }
+    CUtensorMap m1, m2, mw;
+    if (!map_act(&m1, c.x1, c.nimg, c.h, c.w, c.c1, CW)) return EDP_ERR_CUDA;
+    if (c.c2 > 0) {
+        if (!map_act(&m2, c.x2, c.nimg, c.h, c.w, c.c2, CW)) return EDP_ERR_CUDA;
+    } else {
+        m2 = m1;
+    }
+    if (!map_wt(&mw, c.wt, 9 * (c.c1 + c.c2), c.cout, CW, BN)) return EDP_ERR_CUDA;
+    TmaArgs ta;
+    ta.nimg = c.nimg;
+    ta.h = c.h;
+    ta.w = c.w;
+    ta.c1 = c.c1;
+    ta.c2 = c.c2;
+    ta.cout = c.cout;
+    ta.relu = c.relu;
+    ta.tiles_x = (c.w + 15) / 16;
+    ta.tiles_y = (c.h + 7) / 8;
+    ta.bias = c.bias;
+    ta.y = c.y;
+    ta.err = err;
+    dim3 grid((unsigned)(ta.tiles_x * ta.tiles_y * c.nimg), c.cout / BN);
+    conv3x3_fwd_tma_kernel<BN, CW><<<grid, kTcThreads, SMEM, s>>>(m1, m2, mw, ta);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+template <int CW>
+int launch_tma_cout(const ConvArgs& a, int* err, cudaStream_t s)
+{
+    switch (a.cout) {   // one CTA covers all output channels (two halves above 256)
+    case 32: return launch_tma<32, CW>(a, err, s);
+    case 64: return launch_tma<64, CW>(a, err, s);
+    case 96: return launch_tma<96, CW>(a, err, s);
+    case 128: return launch_tma<128, CW>(a, err, s);
+    case 192: return launch_tma<192, CW>(a, err, s);
+    case 256: return launch_tma<256, CW>(a, err, s);
+    case 384: return launch_tma<192, CW>(a, err, s);
+    default: return EDP_ERR_ARG;
+    }
 }
 
 // wt_t[c][8 - tap][n] = wt[n][tap][c]: the weights of the data gradient
@@ -670,16 +926,9 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
     cudaStream_t s = (cudaStream_t)stream;
     int* err = tc_error_word();
     if (!err) return EDP_ERR_CUDA;
-    switch (cout) {   // one CTA covers all output channels (two halves above 256)
-    case 32: return launch_tc<32>(a, err, s);
-    case 64: return launch_tc<64>(a, err, s);
-    case 96: return launch_tc<96>(a, err, s);
-    case 128: return launch_tc<128>(a, err, s);
-    case 192: return launch_tc<192>(a, err, s);
-    case 256: return launch_tc<256>(a, err, s);
-    case 384: return launch_tc<192>(a, err, s);
-    default: return EDP_ERR_ARG;
-    }
+    // 64-channel chunks when neither c_in nor the concatenation split breaks them, else 32
+    if (c1 % 64 == 0 && c2 % 64 == 0) return launch_tma_cout<64>(a, err, s);
+    return launch_tma_cout<32>(a, err, s);
 }
 
 /* bounded-wait error word of the tcgen05 kernels: nonzero once a wait gave up; reading clears it */
