@@ -3,7 +3,8 @@
 //
 // Tensors are NHWC: activations BF16 [images][h][w][channels], 3x3 convolution weights BF16 [c_out][3][3][c_in]
 // (tap = 3 ky + kx, offsets ky - 1, kx - 1), biases and all gradients of weights FP32. Convolutions are implicit
-// GEMMs on the BF16 tensor cores with FP32 accumulation:
+// GEMMs on the BF16 tensor cores with FP32 accumulation; the forward (and through it the data gradient) runs on
+// tcgen05 with TMA-loaded operands and tensor-memory accumulators, the weight gradient on mma.sync:
 //   forward  y[p][n]      = act(sum_{tap, c} x[p + off(tap)][c] w[n][tap][c] + b[n])       M = pixels, N = c_out
 //   dgrad    dx[p][c]     = sum_{tap', n} dz[p + off(tap')][n] w[n][8 - tap'][c]          (the forward kernel on
 //                           the flipped, transposed weight copy)
@@ -76,29 +77,9 @@ struct ConvArgs {
 
 constexpr int kStages = 3;   // cp.async pipeline depth of the weight-gradient kernel
 
-// ------------------------------------------------------------------------------------------ forward on tcgen05
-// The same implicit GEMM on the 5th-generation tensor cores: a CTA owns 128 pixels x BN output channels, its FP32
-// accumulator lives in tensor memory (BN columns x 128 lanes). K = 9 c_in runs in 64-wide stages (4 MMAs of
-// K = 16 each); a stage holds A (128 rows) and B (BN rows) of 128 bytes each in the K-major 128-byte-swizzled layout
-// (8-row atoms of 1024 bytes, 16-byte chunk index XOR row % 8). The 256 threads gather the stage with cp.async
-// (zero-fill for padding and for K past 9 c_in), thread 0 issues the MMAs and commits them to the stage's mbarrier,
-// which frees the stage for a later gather. Every wait is bounded: on timeout the kernel raises *err, still waits
-// (bounded) for its MMAs, frees its tensor memory and returns.
-constexpr int kTcThreads = 256, kTcBK = 64;
+// ------------------------------------------------------------------------------------------ tcgen05 helpers
+constexpr int kTcThreads = 256;
 constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls; a healthy wait ends far sooner
-
-struct TcArgs {
-    ConvArgs c;
-    int* err;
-};
-
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
-{
-    // start address >> 4 | leading offset 16 B (unused by swizzled K-major) | stride 1024 B between 8-row atoms |
-    // descriptor version 1 | layout SWIZZLE_128B
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 {
@@ -110,193 +91,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
         if (done) return true;
     }
     return false;
-}
-
-// Stage kt: chunk kt of K (64 wide) is gathered two stages ahead (cp.async, two threads per pixel row, four 16-byte
-// pieces each); thread 0 issues its 4 MMAs once everybody's pieces landed, and before a stage is refilled thread 0
-// alone waits for the MMAs that read it (two chunks back) while the other threads sleep in the block barrier.
-template <int BN>
-__global__ void __launch_bounds__(kTcThreads, 1) conv3x3_fwd_tc_kernel(TcArgs ta)
-{
-    constexpr int STAGES = 4, AHEAD = 2;   // chunks gathered ahead; two chunks of MMAs stay in flight
-    constexpr int A_BYTES = 128 * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
-    constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
-    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
-    extern __shared__ unsigned char dsm[];
-    __shared__ __align__(8) uint64_t bars[STAGES];
-    __shared__ uint32_t tmem_base_sh;
-    __shared__ int fail_sh;
-    const ConvArgs& a = ta.c;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t base = (smem_u32(dsm) + 1023u) & ~1023u;   // swizzle atoms need 1024-byte alignment
-    const int64_t P = (int64_t)a.nimg * a.h * a.w;
-    const int64_t m0 = (int64_t)blockIdx.x * 128;
-    const int n0 = blockIdx.y * BN;
-    const int cin = a.c1 + a.c2, K = 9 * cin;
-    const int KT = (K + kTcBK - 1) / kTcBK;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
-    }
-    if (tid == 0) {
-        fail_sh = 0;
-        for (int s = 0; s < STAGES; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])));
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem = tmem_base_sh;
-
-    // this thread gathers half (pieces 4 h .. 4 h + 3) of A row `row` (one pixel) of every stage
-    const int row = tid >> 1, half = tid & 1;
-    const int64_t p_row = m0 + row;
-    const bool row_ok = p_row < P;
-    const int64_t pix0 = row_ok ? p_row : 0;   // tap t reads pix0 + (t / 3 - 1) w + (t % 3 - 1)
-    uint32_t tap_ok = 0;                       // bit t: the pixel under tap t lies inside the image
-    if (row_ok) {
-        const int rx = (int)(pix0 % a.w), ry = (int)((pix0 / a.w) % a.h);
-        for (int t = 0; t < 9; ++t) {
-            const int yy = ry + t / 3 - 1, xx = rx + t % 3 - 1;
-            if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w) tap_ok |= 1u << t;
-        }
-    }
-    const uint32_t a_row = (uint32_t)row * 128u;
-    const int rsw = row & 7;
-
-    auto load_stage = [&](int s, int kt) {
-        const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
-        const int k0 = kt * kTcBK + 32 * half;
-        int tap = k0 / cin;
-        int ci = k0 - tap * cin;
-        for (int c = 0; c < 4; ++c) {
-            if (ci >= cin) {
-                ci -= cin;
-                ++tap;
-            }
-            const bool ok = tap < 9 && ((tap_ok >> tap) & 1u);
-            const bf16* g = a.x1;
-            if (ok) {
-                const int64_t pix = pix0 + (int64_t)(tap / 3 - 1) * a.w + (tap % 3 - 1);
-                g = ci < a.c1 ? a.x1 + pix * a.c1 + ci : a.x2 + pix * a.c2 + (ci - a.c1);
-            }
-            const int cc = 4 * half + c;
-            cp_async16(As + a_row + ((cc ^ rsw) << 4), g, ok);
-            ci += 8;
-        }
-        const int k00 = kt * kTcBK;
-        for (int idx = tid; idx < BN * 8; idx += kTcThreads) {
-            const int r = idx >> 3, c = idx & 7;
-            const int k = k00 + 8 * c;
-            const bool ok = k < K;
-            const bf16* g = ok ? a.wt + (int64_t)(n0 + r) * K + k : a.wt;
-            cp_async16(Bs + r * 128 + ((c ^ (r & 7)) << 4), g, ok);
-        }
-    };
-
-    for (int s = 0; s < AHEAD; ++s) {
-        if (s < KT) load_stage(s, s);
-        cp_async_commit();
-    }
-    for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt % STAGES;
-        cp_async_wait<AHEAD - 1>();
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // gathered bytes -> tensor-core reads
-        const int nxt = kt + AHEAD;
-        if (tid == 0 && nxt < KT && nxt >= STAGES && fail_sh == 0) {
-            // the stage chunk nxt refills was read by the MMAs of chunk nxt - STAGES
-            const int old = nxt - STAGES;
-            if (!mbar_wait(smem_u32(&bars[old % STAGES]), (uint32_t)((old / STAGES) & 1))) fail_sh = 1;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t As = base + s * STAGE, Bs = As + A_BYTES;
-            for (int ks = 0; ks < kTcBK / 16; ++ks) {
-                const uint64_t da = umma_desc_sw128(As + 32 * ks), db = umma_desc_sw128(Bs + 32 * ks);
-                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
-                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-                             ::"r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(acc));
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
-                         ::"r"(smem_u32(&bars[s])) : "memory");
-        }
-        if (nxt < KT) load_stage(nxt % STAGES, nxt);
-        cp_async_commit();
-    }
-    cp_async_wait<0>();
-    // all MMAs of this CTA are done once the last commit has arrived (commits complete in order)
-    if (tid == 0) {
-        const int last = KT - 1;
-        if (!mbar_wait(smem_u32(&bars[last % STAGES]), (uint32_t)((last / STAGES) & 1))) fail_sh = 2;
-        if (fail_sh) atomicExch(ta.err, 1);
-    }
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (fail_sh != 2) {
-        // epilogue: warp w reads tensor-memory lanes (pixels) 32 (w % 4) .. + 31, column half w / 4
-        const int wl = warp & 3, wh = warp >> 2;
-        const int cols = BN / 2;
-        const int64_t p = m0 + wl * 32 + lane;
-        for (int c0 = wh * cols; c0 < (wh + 1) * cols; c0 += 16) {
-            uint32_t r[16];
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
-                         " [%16];\n"
-                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                           "=r"(r[14]), "=r"(r[15])
-                         : "r"(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            if (p < P) {
-                uint32_t pk[8];
-                for (int q = 0; q < 8; ++q) {
-                    const int n = n0 + c0 + 2 * q;
-                    float v0 = __uint_as_float(r[2 * q]) + (a.bias ? a.bias[n] : 0.0f);
-                    float v1 = __uint_as_float(r[2 * q + 1]) + (a.bias ? a.bias[n + 1] : 0.0f);
-                    if (a.relu) {
-                        v0 = fmaxf(v0, 0.0f);
-                        v1 = fmaxf(v1, 0.0f);
-                    }
-                    __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
-                    pk[q] = *reinterpret_cast<uint32_t*>(&h);
-                }
-                uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.cout + n0 + c0);
-                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-            }
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    if (warp == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
-    }
-}
-
-template <int BN>
-int launch_tc(const ConvArgs& c, int* err, cudaStream_t s)
-{
-    constexpr int SMEM = 4 * (128 * 128 + BN * 128) + 1024;
-    static bool configured[64] = {false};   // the shared-memory opt-in, once per device and tile width
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
-    if (!configured[dev]) {
-        if (cudaFuncSetAttribute(conv3x3_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
-            cudaSuccess)
-            return EDP_ERR_CUDA;
-        configured[dev] = true;
-    }
-    const int64_t P = (int64_t)c.nimg * c.h * c.w;
-    TcArgs ta;
-    ta.c = c;
-    ta.err = err;
-    dim3 grid((unsigned)((P + 127) / 128), c.cout / BN);
-    conv3x3_fwd_tc_kernel<BN><<<grid, kTcThreads, SMEM, s>>>(ta);
-    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
 // ------------------------------------------------------------------------------------------ forward on TMA + tcgen05
