@@ -354,3 +354,34 @@ def load_blob(path):
     theta[wmask] = (z["w_bf16"].astype(np.uint32) << 16).view(np.float32)
     theta[~wmask] = z["rest_f32"]
     return theta
+
+
+# ------------------------------------------------------------------------------------------ layer timing
+def time_layer(cin, cout, h, w, nimg, reps=10):
+    """CUDA-event time (us) and TFLOP/s of one forward convolution of the network's kind on random data."""
+    torch = _torch()
+    lib = library()
+    st = torch.cuda.current_stream()
+    x = torch.randn(nimg, h, w, cin, device="cuda").to(torch.bfloat16)
+    y = torch.empty(nimg, h, w, cout, device="cuda", dtype=torch.bfloat16)
+    wt = (torch.randn(cout, 9, cin, device="cuda") * 0.05).to(torch.bfloat16)
+    b = torch.zeros(cout, device="cuda")
+    args = (nimg, h, w, _ptr(x), cin, None, 0, _ptr(wt), _ptr(b), cout, 1, _ptr(y), C.c_void_p(st.cuda_stream))
+    for _ in range(3):
+        _check(lib.edp_nn_conv3x3_fwd(*args), "conv3x3_fwd")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        lib.edp_nn_conv3x3_fwd(*args)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / reps * 1e-3
+    return t * 1e6, 2.0 * nimg * h * w * 9 * cin * cout / t / 1e12
+
+
+if __name__ == "__main__":
+    # python -m edipic_b200.warmstart CIN COUT H W IMAGES: times one convolution layer
+    import sys
+    a = [int(v) for v in sys.argv[1:6]]
+    us, tf = time_layer(*a)
+    print(f"{a[0]}->{a[1]} {a[4]}x{a[2]}x{a[3]}: {us:.1f} us, {tf:.1f} TFLOP/s")
