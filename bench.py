@@ -230,12 +230,15 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
     theta = None
     wpath = os.path.join(ROOT, "edipic-2d_b200", "weights", "warmstart_cfg3.npz")
     if os.path.exists(wpath):
-        theta = warmstart.load_blob(wpath)
-        out["weights"] = os.path.relpath(wpath, ROOT)
+        try:
+            theta = warmstart.load_blob(wpath)
+            out["weights"] = os.path.relpath(wpath, ROOT)
+        except ValueError as e:   # parameters of another network layout
+            out["learned"] = {"unavailable": str(e)}
     runs = [("plain_mg", PRECOND_MG, WARM_PREVIOUS), ("plain_nopc", PRECOND_NONE, WARM_PREVIOUS)]
     if theta is not None:
         runs += [("learned_mg", PRECOND_MG, WARM_LEARNED), ("learned_nopc", PRECOND_NONE, WARM_LEARNED)]
-    else:
+    elif "learned" not in out:
         out["learned"] = {"unavailable": "no trained weights (edipic_b200.train_warmstart writes them)"}
     for name, pc, warm in runs:
         with tempfile.TemporaryDirectory() as tmp:

@@ -1,8 +1,8 @@
 // Learned warm start of the CG solve (no counterpart in the reference, whose PETSc solve starts from zero):
 // the encoder-decoder of nn.cu run on the residual of the previous potential. The network sees the node grid as
 // an image padded to multiples of 8 (three 2x2 poolings): channel 0 = r0 / s at unknown nodes, channel 1 = 1 at
-// Dirichlet nodes and padding, channels 2..31 = 0; its FP32 output o gives the guess phi_prev + s K o at unknown
-// nodes (s = RMS of r0 over the unknowns, K = L^2 / (2 pi^2)). The guess is used only when its residual is
+// Dirichlet nodes and padding, channels 2..31 = 0; its two FP32 heads o0, o1 give the guess phi_prev + s (K o0 + o1)
+// at unknown nodes (s = RMS of r0 over the unknowns, K = L^2 / (2 pi^2)). The guess is used only when its residual is
 // smaller than the previous potential's; CG then iterates to the same tolerance either way.
 #include "edp_internal.cuh"
 
@@ -19,12 +19,13 @@ struct edp_warmstart {
     int64_t n_unknown = 0;
     bf16* w[EDP_WARMSTART_N_CONV] = {nullptr};
     float* b[EDP_WARMSTART_N_CONV] = {nullptr};
-    float* wh = nullptr;       // [9][32] then the bias
+    float* wh = nullptr;       // two heads, each [9][32] then the bias
     // activations (NHWC BF16)
     bf16 *in = nullptr, *e0 = nullptr, *s0 = nullptr, *p0 = nullptr, *e1 = nullptr, *s1 = nullptr, *p1 = nullptr;
     bf16 *e2 = nullptr, *s2 = nullptr, *p2 = nullptr, *ba = nullptr, *bb = nullptr, *u2 = nullptr, *d2a = nullptr;
     bf16 *d2b = nullptr, *u1 = nullptr, *d1a = nullptr, *d1b = nullptr, *u0 = nullptr, *d0a = nullptr, *d0b = nullptr;
-    float* out = nullptr;
+    float* out = nullptr;      // head 0 (smooth, scaled by K)
+    float* out1 = nullptr;     // head 1 (grid scale)
     double* guess = nullptr;   // node grid
     double* r1 = nullptr;
     double* p1n = nullptr;
@@ -62,14 +63,16 @@ __global__ void ws_input_kernel(edp_kparams kp, const int8_t* __restrict__ kind,
 }
 
 __global__ void ws_guess_kernel(edp_kparams kp, const int8_t* __restrict__ kind, const double* __restrict__ phi,
-                                const float* __restrict__ out, const double* __restrict__ rr0, double n_unknown,
-                                double K, int W, double* __restrict__ guess)
+                                const float* __restrict__ out, const float* __restrict__ out1,
+                                const double* __restrict__ rr0, double n_unknown, double K, int W,
+                                double* __restrict__ guess)
 {
     const double s = (*rr0 > 0.0) ? sqrt(*rr0 / n_unknown) : 1.0;
     const int64_t n = (int64_t)kp.nxg * kp.nyg;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(q % kp.nxg), j = (int)(q / kp.nxg);
-        guess[q] = kind[q] ? phi[q] : phi[q] + s * K * (double)out[(int64_t)j * W + i];
+        const int64_t pix = (int64_t)j * W + i;
+        guess[q] = kind[q] ? phi[q] : phi[q] + s * (K * (double)out[pix] + (double)out1[pix]);
     }
 }
 
@@ -142,7 +145,7 @@ void edp_warmstart_free(edp_ctx* c)
     }
     void* bufs[] = {ws->wh, ws->in, ws->e0, ws->s0, ws->p0, ws->e1, ws->s1, ws->p1, ws->e2, ws->s2, ws->p2, ws->ba,
                     ws->bb, ws->u2, ws->d2a, ws->d2b, ws->u1, ws->d1a, ws->d1b, ws->u0, ws->d0a, ws->d0b, ws->out,
-                    ws->guess, ws->r1, ws->p1n, ws->scal};
+                    ws->out1, ws->guess, ws->r1, ws->p1n, ws->scal};
     for (void* q : bufs) cudaFree(q);
     delete ws;
     c->ws = nullptr;
@@ -185,9 +188,11 @@ int edp_warmstart_forward(edp_ctx* c, const double* rr0)
     TRY(conv(c, 13, H, W, ws->d0a, 32, nullptr, 0, ws->d0b));
     c->launches += 1;
     TRY(edp_nn_head_fwd(1, H, W, 32, ws->d0b, ws->wh, ws->wh + 9 * 32, ws->out, c->stream));
+    c->launches += 1;
+    TRY(edp_nn_head_fwd(1, H, W, 32, ws->d0b, ws->wh + 9 * 32 + 1, ws->wh + 2 * 9 * 32 + 1, ws->out1, c->stream));
     ++c->launches;
     ws_guess_kernel<<<grid_n((int64_t)kp.nxg * kp.nyg), 256, 0, c->stream>>>(
-        kp, c->cg_kind, c->phi, ws->out, rr0, (double)ws->n_unknown, ws->K, W, ws->guess);
+        kp, c->cg_kind, c->phi, ws->out, ws->out1, rr0, (double)ws->n_unknown, ws->K, W, ws->guess);
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
 }
@@ -225,7 +230,7 @@ extern "C" int edp_warmstart_load(edp_ctx* c, const float* blob, int64_t n)
 {
     if (!c || !blob) return EDP_ERR_ARG;
     if (c->p.solver != EDP_SOLVER_CG) return edp_fail(c, EDP_ERR_STATE, "the learned warm start is for CG contexts");
-    int64_t need = 9 * 32 + 1;
+    int64_t need = 2 * (9 * 32 + 1);
     for (int l = 0; l < EDP_WARMSTART_N_CONV; ++l) need += (int64_t)9 * kLayers[l][0] * kLayers[l][1] + kLayers[l][1];
     if (n != need) return edp_fail(c, EDP_ERR_ARG, "warm-start parameter count does not match the network");
     edp_warmstart_free(c);
@@ -260,8 +265,8 @@ extern "C" int edp_warmstart_load(edp_ctx* c, const float* blob, int64_t n)
         EDP_CUDA(c, cudaMemcpy(ws->b[l], q, kLayers[l][1] * sizeof(float), cudaMemcpyHostToDevice));
         q += kLayers[l][1];
     }
-    EDP_CUDA(c, cudaMalloc(&ws->wh, (9 * 32 + 1) * sizeof(float)));
-    EDP_CUDA(c, cudaMemcpy(ws->wh, q, (9 * 32 + 1) * sizeof(float), cudaMemcpyHostToDevice));
+    EDP_CUDA(c, cudaMalloc(&ws->wh, 2 * (9 * 32 + 1) * sizeof(float)));
+    EDP_CUDA(c, cudaMemcpy(ws->wh, q, 2 * (9 * 32 + 1) * sizeof(float), cudaMemcpyHostToDevice));
     const int64_t p0 = (int64_t)ws->H * ws->W, p1 = p0 / 4, p2 = p0 / 16, p3 = p0 / 64;
     auto act = [&](bf16** ptr, int64_t pix, int ch) -> int {
         EDP_CUDA(c, cudaMalloc(ptr, pix * ch * sizeof(bf16)));
@@ -290,6 +295,7 @@ extern "C" int edp_warmstart_load(edp_ctx* c, const float* blob, int64_t n)
     TRY(act(&ws->d0b, p0, 32));
     const int64_t nn = (int64_t)kp.nxg * kp.nyg;
     EDP_CUDA(c, cudaMalloc(&ws->out, p0 * sizeof(float)));
+    EDP_CUDA(c, cudaMalloc(&ws->out1, p0 * sizeof(float)));
     EDP_CUDA(c, cudaMalloc(&ws->guess, nn * sizeof(double)));
     EDP_CUDA(c, cudaMalloc(&ws->r1, nn * sizeof(double)));
     EDP_CUDA(c, cudaMalloc(&ws->p1n, nn * sizeof(double)));

@@ -4,8 +4,10 @@ starts from zero; SOLVE_POTENTIAL_WITH_PETSC, src/pic2d_ElectricFieldCalc_PETSc.
 A 4-level convolutional encoder-decoder (channels 32-64-128-256, 3x3 kernels, 2x2 average pooling, nearest
 upsampling, skip concatenation, ReLU, BF16 weights and activations with FP32 accumulation; LAYERS below) maps the
 residual r0 = b - A phi_prev of the previous potential against the new charge density, divided by its RMS s, and the
-Dirichlet mask to the update (phi - phi_prev) / (s K), K = L^2 / (2 pi^2). Since A phi = b, r0 = A (phi - phi_prev):
-a training sample is one potential update of a plain run.
+Dirichlet mask to the update (phi - phi_prev) / s = K o0 + o1 through two FP32 heads, K = L^2 / (2 pi^2): o0 carries
+the smooth part (the inverse Laplacian grows like L^2 on the longest wavelengths) and o1 the grid-scale part, so both
+stay O(1) inside the BF16 network. Since A phi = b, r0 = A (phi - phi_prev): a training sample is one potential update
+of a plain run.
 
 Training runs on the device kernels of libedipic_b200.so (edp_nn_*) behind torch.autograd.Function wrappers; torch
 holds the tensors and chains the backward pass, the loss is torch arithmetic, and the Adam step is the library's.
@@ -24,13 +26,20 @@ HEAD_C = 32
 IN_C = 32   # input channels: residual / s, Dirichlet mask, zeros
 
 
+N_HEADS = 2   # smooth (scaled by K) and grid-scale outputs
+
+
 def param_layout():
-    """[(w_offset, b_offset, cin, cout)] per convolution and (wh_offset, bh_offset) of the head."""
+    """[(w_offset, b_offset, cin, cout)] per convolution, [(wh_offset, bh_offset)] per head, total count."""
     out, off = [], 0
     for ci, co in LAYERS:
         out.append((off, off + 9 * ci * co, ci, co))
         off += 9 * ci * co + co
-    return out, (off, off + 9 * HEAD_C), off + 9 * HEAD_C + 1
+    heads = []
+    for _ in range(N_HEADS):
+        heads.append((off, off + 9 * HEAD_C))
+        off += 9 * HEAD_C + 1
+    return out, heads, off
 
 
 def n_params():
@@ -40,11 +49,12 @@ def n_params():
 def init_params(seed=0):
     """He-normal convolution weights, zero biases, a small head."""
     rng = np.random.default_rng(seed)
-    convs, (wh, bh), n = param_layout()
+    convs, heads, n = param_layout()
     theta = np.zeros(n, dtype=np.float32)
     for (wo, bo, ci, co) in convs:
         theta[wo:bo] = rng.normal(0.0, math.sqrt(2.0 / (9 * ci)), 9 * ci * co)
-    theta[wh:bh] = rng.normal(0.0, 0.1 * math.sqrt(1.0 / (9 * HEAD_C)), 9 * HEAD_C)
+    for (wh, bh) in heads:
+        theta[wh:bh] = rng.normal(0.0, 0.1 * math.sqrt(1.0 / (9 * HEAD_C)), 9 * HEAD_C)
     return theta
 
 
@@ -187,7 +197,7 @@ class WarmStartNet:
         self.m = torch.zeros_like(self.theta.detach())
         self.v = torch.zeros_like(self.theta.detach())
         self.steps = 0
-        self.convs, (self.wh, self.bh), _ = param_layout()
+        self.convs, self.heads, _ = param_layout()
         self.Conv3x3, self.Pool, self.Up, self.Head = _fns()
 
     def _conv(self, l, x1, x2=None, relu=1):
@@ -198,7 +208,7 @@ class WarmStartNet:
         return self.Conv3x3.apply(x1, x2, w32, b32, wbf, co, relu)
 
     def forward(self, x):
-        """x: [images, H, W, 32] BF16 (H, W multiples of 8) -> [images, H, W] FP32."""
+        """x: [images, H, W, 32] BF16 (H, W multiples of 8) -> (o0, o1), each [images, H, W] FP32."""
         P, U = self.Pool.apply, self.Up.apply
         s0 = self._conv(1, self._conv(0, x))
         s1 = self._conv(3, self._conv(2, P(s0)))
@@ -207,7 +217,7 @@ class WarmStartNet:
         d2 = self._conv(9, self._conv(8, U(bb), s2))
         d1 = self._conv(11, self._conv(10, U(d2), s1))
         d0 = self._conv(13, self._conv(12, U(d1), s0))
-        return self.Head.apply(d0, self.theta[self.wh:self.bh], self.theta[self.bh:self.bh + 1])
+        return tuple(self.Head.apply(d0, self.theta[wh:bh], self.theta[bh:bh + 1]) for (wh, bh) in self.heads)
 
     def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
         torch = _torch()
@@ -248,8 +258,8 @@ def make_batch(dphi, unk):
 
 def losses(out, rhat, t, unk, K):
     """Per-sample relative residual |r0 - A u|^2 / |r0|^2 and relative energy-norm error |t - u|_A^2 / |t|_A^2 of
-    the normalised update u = K out, as the CG start phi_prev + s u would see them."""
-    u = K * out * unk
+    the normalised update u = K o0 + o1, as the CG start phi_prev + s u would see them."""
+    u = (K * out[0] + out[1]) * unk
     r1 = rhat - stencil(u, unk)
     lr = (r1 * r1).sum(dim=(1, 2)) / (rhat * rhat).sum(dim=(1, 2)).clamp_min(1e-30)
     e = (t - u) * unk
@@ -332,7 +342,7 @@ def cfg3_geometries(n, seed=0, ncx=512, ncy=512):
 
 def save_blob(path, theta):
     """Convolution weights as BF16 bits (the device uses them as BF16), biases and head as FP32."""
-    convs, (wh, bh), n = param_layout()
+    convs, _, n = param_layout()
     theta = np.asarray(theta, dtype=np.float32)
     wmask = np.zeros(n, dtype=bool)
     for (wo, bo, ci, co) in convs:

@@ -244,10 +244,10 @@ int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* rho_dev, do
 /* No counterpart in the reference (its PETSc solve always starts from zero). A 4-level convolutional
  * encoder-decoder (channels 32-64-128-256, 3x3 kernels, 2x2 average pooling, nearest upsampling, skip
  * concatenation, ReLU; BF16 weights and activations, FP32 accumulation) maps the residual r0 = b - A phi_prev of
- * the previous potential, divided by its RMS s, and the Dirichlet mask to the update (phi - phi_prev) / (s K),
- * K = L^2 / (2 pi^2) with L the larger cell count. blob holds FP32 parameters in the order
- * EDP_WARMSTART_LAYERS lists: per convolution the weights [c_out][3][3][c_in] then the biases [c_out]; last the
- * head's weights [3][3][32] and bias. */
+ * the previous potential, divided by its RMS s, and the Dirichlet mask to the update (phi - phi_prev) / s =
+ * K o0 + o1 of its two FP32 heads, K = L^2 / (2 pi^2) with L the larger cell count. blob holds FP32 parameters in
+ * the order EDP_WARMSTART_LAYERS lists: per convolution the weights [c_out][3][3][c_in] then the biases [c_out];
+ * last the two heads, each weights [3][3][32] and bias. */
 #define EDP_WARMSTART_N_CONV 14
 #define EDP_WARMSTART_LAYERS {{32, 32}, {32, 32}, {32, 64}, {64, 64}, {64, 128}, {128, 128}, {128, 256}, \
                               {256, 256}, {384, 128}, {128, 128}, {192, 64}, {64, 64}, {96, 32}, {32, 32}}

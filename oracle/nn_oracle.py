@@ -102,8 +102,11 @@ def unpack(theta):
         b = theta[off:off + co].astype(np.float64)
         off += co
         convs.append((w, b))
-    wh = theta[off:off + 9 * 32].astype(np.float64)
-    return convs, wh, float(theta[off + 9 * 32])
+    heads = []
+    for _ in range(2):
+        heads.append((theta[off:off + 9 * 32].astype(np.float64), float(theta[off + 9 * 32])))
+        off += 9 * 32 + 1
+    return convs, heads
 
 
 def _exact(a):
@@ -114,7 +117,7 @@ def net_forward(theta, x, quantize=True):
     """The encoder-decoder on x [N, H, W, 32]; with quantize, BF16 weights and BF16-rounded stored activations as
     on the device (FP64 arithmetic otherwise exact). Returns the output and the tape for net_backward."""
     bf16 = globals()["bf16"] if quantize else _exact
-    convs, wh, bh = unpack(theta)
+    convs, heads = unpack(theta)
     wq = [(bf16(w), b) for w, b in convs]
     tape = {"q": quantize}
 
@@ -131,21 +134,26 @@ def net_forward(theta, x, quantize=True):
     d2 = conv(9, conv(8, up(bb), s2))
     d1 = conv(11, conv(10, up(d2), s1))
     d0 = conv(13, conv(12, up(d1), s0))
-    out = head_fwd(d0, wh, bh)
+    out = [head_fwd(d0, wh, bh) for wh, bh in heads]
     tape["head"] = d0
     if quantize:
-        out = out.astype(np.float32).astype(np.float64)
-    return out, (tape, wq, wh)
+        out = [o.astype(np.float32).astype(np.float64) for o in out]
+    return out, (tape, wq, heads)
 
 
 def net_backward(theta, tape_all, dout):
-    """Gradient of sum(out * dout) with respect to theta (same order), BF16-rounded data gradients as stored on
-    the device."""
-    tape, wq, wh = tape_all
+    """Gradient of sum_h sum(out[h] * dout[h]) with respect to theta (same order), BF16-rounded data gradients as
+    stored on the device."""
+    tape, wq, heads = tape_all
     bf16 = globals()["bf16"] if tape["q"] else _exact
     grads = [None] * len(LAYERS)
     d0 = tape["head"]
-    g, gwh, gbh = head_bwd(d0, wh, dout)
+    g = 0.0
+    ghead = []
+    for (wh, _), do in zip(heads, dout):
+        gx, gwh, gbh = head_bwd(d0, wh, do)
+        g = g + gx
+        ghead.append((gwh, gbh))
     g = bf16(g)
 
     def conv_back(l, dy, need_dx=True):
@@ -182,6 +190,7 @@ def net_backward(theta, tape_all, dout):
     for dw, db in grads:
         out.append(dw.reshape(-1))
         out.append(db)
-    out.append(gwh)
-    out.append(np.array([gbh]))
+    for gwh, gbh in ghead:
+        out.append(gwh)
+        out.append(np.array([gbh]))
     return np.concatenate(out)

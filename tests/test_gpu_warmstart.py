@@ -129,24 +129,26 @@ def test_network_gradient_matches_oracle():
     oracle's own BF16-emulating pass from it, for the output, the whole gradient and every layer."""
     rng = np.random.default_rng(7)
     theta = warmstart.init_params(seed=3)
-    theta[warmstart.param_layout()[1][0]:] *= 10.0   # a livelier head than at initialisation
+    heads0 = warmstart.param_layout()[1][0][0]
+    theta[heads0:] *= 10.0   # livelier heads than at initialisation
     x = O.bf16(rng.normal(0, 1, (2, 16, 24, 32)))
     net = warmstart.WarmStartNet(theta)
     out = net.forward(_bf(x))
-    dout = rng.normal(0, 1, tuple(out.shape))
-    (out * _f32(dout)).sum().backward()
+    dout = [rng.normal(0, 1, tuple(o.shape)) for o in out]
+    sum((o * _f32(d)).sum() for o, d in zip(out, dout)).backward()
     g = _np(net.theta.grad)
     t64 = theta.astype(np.float64)
     rout_q, tape_q = O.net_forward(t64, x, quantize=True)
     rg_q = O.net_backward(t64, tape_q, dout)
     rout, tape = O.net_forward(t64, x, quantize=False)
     rg = O.net_backward(t64, tape, dout)
-    assert np.linalg.norm(_np(out) - rout) <= 2.0 * np.linalg.norm(rout_q - rout) + 1e-6 * np.linalg.norm(rout)
+    for o, rq, r in zip(out, rout_q, rout):
+        assert np.linalg.norm(_np(o) - r) <= 2.0 * np.linalg.norm(rq - r) + 1e-6 * np.linalg.norm(r)
     assert np.linalg.norm(g - rg) <= 2.0 * np.linalg.norm(rg_q - rg) + 1e-6 * np.linalg.norm(rg)
     cos = float(np.dot(g, rg) / (np.linalg.norm(g) * np.linalg.norm(rg)))
     assert cos > 0.99
-    convs, (wh, bh), _ = warmstart.param_layout()
-    for (wo, bo, ci, co) in convs + [(wh, bh, 32, 1)]:
+    convs, heads, _ = warmstart.param_layout()
+    for (wo, bo, ci, co) in convs + [(wh, bh, 32, 1) for (wh, bh) in heads]:
         err, noise = np.linalg.norm(g[wo:bo] - rg[wo:bo]), np.linalg.norm(rg_q[wo:bo] - rg[wo:bo])
         assert err <= 2.0 * noise + 1e-4 * np.linalg.norm(rg[wo:bo]) + 1e-9
 
@@ -179,7 +181,7 @@ def _unknowns(p):
 def test_library_inference_matches_training_forward(tmp_path):
     d = decks.write_deck(str(tmp_path), "cfg2", ncx=64, ncy=48, ppc=16, inner=(20, 12, 36, 20, -100.0))
     theta = warmstart.init_params(seed=11)
-    theta[warmstart.param_layout()[1][0]:] *= 10.0
+    theta[warmstart.param_layout()[1][0][0]:] *= 10.0
     with Simulation(d, sort_every=20) as sim:
         p = sim.params
         sim.distribute_particles(16)
@@ -197,9 +199,9 @@ def test_library_inference_matches_training_forward(tmp_path):
     x, s = _input_from_fields(rho_t, phi, unk, K)
     net = warmstart.WarmStartNet(theta)
     with torch.no_grad():
-        out = _np(net.forward(_bf(x)))[0]
+        o0, o1 = (_np(o)[0] for o in net.forward(_bf(x)))
     ny, nx = phi.shape
-    upd = s * K * out[:ny, :nx] * unk
+    upd = s * (K * o0[:ny, :nx] + o1[:ny, :nx]) * unk
     assert np.abs(guess - phi - upd).max() <= 2e-2 * np.abs(upd).max()
     assert np.allclose(guess[unk == 0], phi[unk == 0])
     assert res[0] > 0 and np.isfinite(res[1])

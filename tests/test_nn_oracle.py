@@ -8,11 +8,11 @@ import nn_oracle as O
 
 def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(0)
-    n = sum(9 * ci * co + co for ci, co in O.LAYERS) + 9 * 32 + 1
+    n = sum(9 * ci * co + co for ci, co in O.LAYERS) + 2 * (9 * 32 + 1)
     theta = rng.normal(0, 1, n) * 0.2
     x = rng.normal(0, 1, (1, 8, 8, 32))
     out, tape = O.net_forward(theta, x, quantize=False)
-    dout = rng.normal(0, 1, out.shape)
+    dout = [rng.normal(0, 1, o.shape) for o in out]
     g = O.net_backward(theta, tape, dout)
     live = np.flatnonzero(np.abs(g) > 1e-3 * np.abs(g).max())
     checked = 0
@@ -21,7 +21,8 @@ def test_oracle_backward_matches_finite_differences():
         tp, tm = theta.copy(), theta.copy()
         tp[k] += e
         tm[k] -= e
-        fd = ((O.net_forward(tp, x, False)[0] - O.net_forward(tm, x, False)[0]) * dout).sum() / (2 * e)
+        op, om = O.net_forward(tp, x, False)[0], O.net_forward(tm, x, False)[0]
+        fd = sum(((a - b) * d).sum() for a, b, d in zip(op, om, dout)) / (2 * e)
         assert abs(g[k] - fd) <= 1e-5 * abs(fd) + 1e-8
         checked += 1
     assert checked == 10
