@@ -47,14 +47,15 @@ def n_params():
 
 
 def init_params(seed=0):
-    """He-normal convolution weights, zero biases, a small head."""
+    """He-normal convolution weights and zero biases; the K-scaled head starts at zero (K is ~10^4 on a 512-cell
+    grid, so a random start would swamp the first updates), the grid-scale head small."""
     rng = np.random.default_rng(seed)
     convs, heads, n = param_layout()
     theta = np.zeros(n, dtype=np.float32)
     for (wo, bo, ci, co) in convs:
         theta[wo:bo] = rng.normal(0.0, math.sqrt(2.0 / (9 * ci)), 9 * ci * co)
-    for (wh, bh) in heads:
-        theta[wh:bh] = rng.normal(0.0, 0.1 * math.sqrt(1.0 / (9 * HEAD_C)), 9 * HEAD_C)
+    wh, bh = heads[1]
+    theta[wh:bh] = rng.normal(0.0, 0.1 * math.sqrt(1.0 / (9 * HEAD_C)), 9 * HEAD_C)
     return theta
 
 
