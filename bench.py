@@ -161,12 +161,13 @@ def fp64_cycle_leg(args, stream_of):
 
 def network_leg():
     """The learned warm start's convolutions on the tensor cores: each of the 14 layers of the encoder-decoder timed
-    alone at the inference shape (one 520 x 520 image, the padded 513 x 513 node grid) and at the training shape
+    alone at the inference shape (one image of the 513 x 513-node grid padded to 576 x 576) and at the training shape
     (4 images), and the whole forward pass. FLOPs = 2 x pixels x 9 x c_in x c_out per layer."""
+    # (the image is the 513 x 513-node grid padded to a multiple of 64)
     import torch
     from edipic_b200 import library, warmstart
     lib = library()
-    H = W = 520
+    H = W = warmstart.padded(513)   # the 513 x 513-node grid of the inner-object geometry
     peak = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -174,7 +175,8 @@ def network_leg():
         peak_kind = "measured"
     except Exception:
         peak, peak_kind = 1590.0, "fallback"
-    scale = [1, 1, 2, 2, 4, 4, 8, 8, 4, 4, 2, 2, 1, 1]
+    p = warmstart.POOL
+    scale = [1, 1, p, p, p ** 2, p ** 2, p ** 3, p ** 3, p ** 2, p ** 2, p, p, 1, 1]
     net = warmstart.WarmStartNet(seed=0)
     out = {"shape": f"{H}x{W}", "peak_tflops": peak, "peak_kind": peak_kind}
     st = torch.cuda.current_stream()
@@ -462,7 +464,7 @@ def run_ours(args):
             line["roofline_conv"] = {"bound": "tensor", "achieved": line["network"]["batch4"]["conv_tflops"],
                                      "peak": line["network"]["peak_tflops"], "unit": "TFLOP/s",
                                      "frac": line["network"]["batch4"]["frac"], "traffic": None,
-                                     "basis": "14 tcgen05 convolutions of the warm-start network, 4 x 520 x 520, "
+                                     "basis": "14 tcgen05 convolutions of the warm-start network, 4 x 576 x 576, "
                                               "2 x pixels x 9 x c_in x c_out FLOPs, peak bf16 "
                                               + line["network"]["peak_kind"]}
         if not args.no_cpu_baseline and world == 1:

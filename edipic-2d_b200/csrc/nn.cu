@@ -495,10 +495,12 @@ __global__ void bias_grad_kernel(const bf16* __restrict__ dz, int64_t P, int cou
 }
 
 // ------------------------------------------------------------------------------------------ glue
-// 2x2 average pooling, NHWC, h and w even
-__global__ void pool_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, bf16* __restrict__ y)
+// f x f average pooling, NHWC, h and w multiples of f (f = 2 or 4)
+__global__ void pool_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, int f,
+                                bf16* __restrict__ y)
 {
-    const int ho = h / 2, wo = w / 2;
+    const int ho = h / f, wo = w / f;
+    const float inv = 1.0f / (float)(f * f);
     const int64_t total = (int64_t)nimg * ho * wo * c;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int ch = (int)(q % c);
@@ -507,17 +509,18 @@ __global__ void pool_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int
         r /= wo;
         const int Y = (int)(r % ho);
         const int64_t b = r / ho;
-        const int64_t s = ((b * h + 2 * Y) * w + 2 * X) * c + ch;
-        const float v = __bfloat162float(x[s]) + __bfloat162float(x[s + c]) + __bfloat162float(x[s + (int64_t)w * c]) +
-                        __bfloat162float(x[s + (int64_t)w * c + c]);
-        y[q] = __float2bfloat16(0.25f * v);
+        float v = 0.0f;
+        for (int dy = 0; dy < f; ++dy)
+            for (int dx = 0; dx < f; ++dx) v += __bfloat162float(x[((b * h + f * Y + dy) * w + f * X + dx) * c + ch]);
+        y[q] = __float2bfloat16(inv * v);
     }
 }
 
-// dx (+)= pool backward of dy: every input pixel gets a quarter of its output's gradient
-__global__ void pool_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, bf16* __restrict__ dx,
-                                int accumulate)
+// dx (+)= pool backward of dy: every input pixel gets 1 / f^2 of its output's gradient
+__global__ void pool_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, int f,
+                                bf16* __restrict__ dx, int accumulate)
 {
+    const float inv = 1.0f / (float)(f * f);
     const int64_t total = (int64_t)nimg * h * w * c;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int ch = (int)(q % c);
@@ -526,14 +529,14 @@ __global__ void pool_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, in
         r /= w;
         const int y = (int)(r % h);
         const int64_t b = r / h;
-        float v = 0.25f * __bfloat162float(dy[((b * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch]);
+        float v = inv * __bfloat162float(dy[((b * (h / f) + y / f) * (w / f) + x / f) * c + ch]);
         if (accumulate) v += __bfloat162float(dx[q]);
         dx[q] = __float2bfloat16(v);
     }
 }
 
-// nearest 2x upsampling, NHWC (h, w: output size)
-__global__ void up_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, bf16* __restrict__ y)
+// nearest f x upsampling, NHWC (h, w: output size)
+__global__ void up_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w, int c, int f, bf16* __restrict__ y)
 {
     const int64_t total = (int64_t)nimg * h * w * c;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -543,14 +546,15 @@ __global__ void up_fwd_kernel(const bf16* __restrict__ x, int nimg, int h, int w
         r /= w;
         const int yy = (int)(r % h);
         const int64_t b = r / h;
-        y[q] = x[((b * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch];
+        y[q] = x[((b * (h / f) + yy / f) * (w / f) + xx / f) * c + ch];
     }
 }
 
-// dx = sum of the four output gradients of each input pixel; dy has cs channels of which the first c are read
-__global__ void up_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, int cs, bf16* __restrict__ dx)
+// dx = sum of the f^2 output gradients of each input pixel; dy has cs channels of which the first c are read
+__global__ void up_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int w, int c, int cs, int f,
+                              bf16* __restrict__ dx)
 {
-    const int ho = h / 2, wo = w / 2;
+    const int ho = h / f, wo = w / f;
     const int64_t total = (int64_t)nimg * ho * wo * c;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int ch = (int)(q % c);
@@ -559,9 +563,10 @@ __global__ void up_bwd_kernel(const bf16* __restrict__ dy, int nimg, int h, int 
         r /= wo;
         const int Y = (int)(r % ho);
         const int64_t b = r / ho;
-        const int64_t s = ((b * h + 2 * Y) * w + 2 * X) * cs + ch;
-        const float v = __bfloat162float(dy[s]) + __bfloat162float(dy[s + cs]) +
-                        __bfloat162float(dy[s + (int64_t)w * cs]) + __bfloat162float(dy[s + (int64_t)w * cs + cs]);
+        float v = 0.0f;
+        for (int dyy = 0; dyy < f; ++dyy)
+            for (int dxx = 0; dxx < f; ++dxx)
+                v += __bfloat162float(dy[((b * h + f * Y + dyy) * w + f * X + dxx) * cs + ch]);
         dx[q] = __float2bfloat16(v);
     }
 }
@@ -787,37 +792,37 @@ int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
-int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream)
+int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream)
 {
-    if (h % 2 || w % 2 || !x || !y) return EDP_ERR_ARG;
-    pool_fwd_kernel<<<grid_for((int64_t)nimg * h * w * c / 4), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, nimg, h,
-                                                                                            w, c, (bf16*)y);
+    if ((f != 2 && f != 4) || h % f || w % f || !x || !y) return EDP_ERR_ARG;
+    pool_fwd_kernel<<<grid_for((int64_t)nimg * h * w * c / (f * f)), 256, 0, (cudaStream_t)stream>>>(
+        (const bf16*)x, nimg, h, w, c, f, (bf16*)y);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
-int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* dy, void* dx, int32_t accumulate,
-                    void* stream)
+int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* dy, void* dx,
+                    int32_t accumulate, void* stream)
 {
-    if (h % 2 || w % 2 || !dy || !dx) return EDP_ERR_ARG;
-    pool_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c), 256, 0, (cudaStream_t)stream>>>((const bf16*)dy, nimg, h, w,
-                                                                                        c, (bf16*)dx, accumulate);
+    if ((f != 2 && f != 4) || h % f || w % f || !dy || !dx) return EDP_ERR_ARG;
+    pool_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c), 256, 0, (cudaStream_t)stream>>>(
+        (const bf16*)dy, nimg, h, w, c, f, (bf16*)dx, accumulate);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
-int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream)
+int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream)
 {
-    if (h % 2 || w % 2 || !x || !y) return EDP_ERR_ARG;
+    if ((f != 2 && f != 4) || h % f || w % f || !x || !y) return EDP_ERR_ARG;
     up_fwd_kernel<<<grid_for((int64_t)nimg * h * w * c), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, nimg, h, w, c,
-                                                                                      (bf16*)y);
+                                                                                      f, (bf16*)y);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
-int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, const void* dy, void* dx,
+int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, int32_t f, const void* dy, void* dx,
                         void* stream)
 {
-    if (h % 2 || w % 2 || !dy || !dx || cs < c) return EDP_ERR_ARG;
-    up_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c / 4), 256, 0, (cudaStream_t)stream>>>((const bf16*)dy, nimg, h,
-                                                                                          w, c, cs, (bf16*)dx);
+    if ((f != 2 && f != 4) || h % f || w % f || !dy || !dx || cs < c) return EDP_ERR_ARG;
+    up_bwd_kernel<<<grid_for((int64_t)nimg * h * w * c / (f * f)), 256, 0, (cudaStream_t)stream>>>(
+        (const bf16*)dy, nimg, h, w, c, cs, f, (bf16*)dx);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 

@@ -1,6 +1,6 @@
 // Learned warm start of the CG solve (no counterpart in the reference, whose PETSc solve starts from zero):
 // the encoder-decoder of nn.cu run on the residual of the previous potential. The network sees the node grid as
-// an image padded to multiples of 8 (three 2x2 poolings): channel 0 = r0 / s at unknown nodes, channel 1 = 1 at
+// an image padded to multiples of 64 (three 4x4 poolings): channel 0 = r0 / s at unknown nodes, channel 1 = 1 at
 // Dirichlet nodes and padding, channels 2..31 = 0; its two FP32 heads o0, o1 give the guess phi_prev + s (K o0 + o1)
 // at unknown nodes (s = RMS of r0 over the unknowns, K = L^2 / (2 pi^2)). The guess is used only when its residual is
 // smaller than the previous potential's; CG then iterates to the same tolerance either way.
@@ -163,27 +163,27 @@ int edp_warmstart_forward(edp_ctx* c, const double* rr0)
     TRY(conv(c, 0, H, W, ws->in, 32, nullptr, 0, ws->e0));
     TRY(conv(c, 1, H, W, ws->e0, 32, nullptr, 0, ws->s0));
     c->launches += 1;
-    TRY(edp_nn_pool(1, H, W, 32, ws->s0, ws->p0, c->stream));
-    TRY(conv(c, 2, H / 2, W / 2, ws->p0, 32, nullptr, 0, ws->e1));
-    TRY(conv(c, 3, H / 2, W / 2, ws->e1, 64, nullptr, 0, ws->s1));
+    TRY(edp_nn_pool(1, H, W, 32, 4, ws->s0, ws->p0, c->stream));
+    TRY(conv(c, 2, H / 4, W / 4, ws->p0, 32, nullptr, 0, ws->e1));
+    TRY(conv(c, 3, H / 4, W / 4, ws->e1, 64, nullptr, 0, ws->s1));
     c->launches += 1;
-    TRY(edp_nn_pool(1, H / 2, W / 2, 64, ws->s1, ws->p1, c->stream));
-    TRY(conv(c, 4, H / 4, W / 4, ws->p1, 64, nullptr, 0, ws->e2));
-    TRY(conv(c, 5, H / 4, W / 4, ws->e2, 128, nullptr, 0, ws->s2));
+    TRY(edp_nn_pool(1, H / 4, W / 4, 64, 4, ws->s1, ws->p1, c->stream));
+    TRY(conv(c, 4, H / 16, W / 16, ws->p1, 64, nullptr, 0, ws->e2));
+    TRY(conv(c, 5, H / 16, W / 16, ws->e2, 128, nullptr, 0, ws->s2));
     c->launches += 1;
-    TRY(edp_nn_pool(1, H / 4, W / 4, 128, ws->s2, ws->p2, c->stream));
-    TRY(conv(c, 6, H / 8, W / 8, ws->p2, 128, nullptr, 0, ws->ba));
-    TRY(conv(c, 7, H / 8, W / 8, ws->ba, 256, nullptr, 0, ws->bb));
+    TRY(edp_nn_pool(1, H / 16, W / 16, 128, 4, ws->s2, ws->p2, c->stream));
+    TRY(conv(c, 6, H / 64, W / 64, ws->p2, 128, nullptr, 0, ws->ba));
+    TRY(conv(c, 7, H / 64, W / 64, ws->ba, 256, nullptr, 0, ws->bb));
     c->launches += 1;
-    TRY(edp_nn_upsample(1, H / 4, W / 4, 256, ws->bb, ws->u2, c->stream));
-    TRY(conv(c, 8, H / 4, W / 4, ws->u2, 256, ws->s2, 128, ws->d2a));
-    TRY(conv(c, 9, H / 4, W / 4, ws->d2a, 128, nullptr, 0, ws->d2b));
+    TRY(edp_nn_upsample(1, H / 16, W / 16, 256, 4, ws->bb, ws->u2, c->stream));
+    TRY(conv(c, 8, H / 16, W / 16, ws->u2, 256, ws->s2, 128, ws->d2a));
+    TRY(conv(c, 9, H / 16, W / 16, ws->d2a, 128, nullptr, 0, ws->d2b));
     c->launches += 1;
-    TRY(edp_nn_upsample(1, H / 2, W / 2, 128, ws->d2b, ws->u1, c->stream));
-    TRY(conv(c, 10, H / 2, W / 2, ws->u1, 128, ws->s1, 64, ws->d1a));
-    TRY(conv(c, 11, H / 2, W / 2, ws->d1a, 64, nullptr, 0, ws->d1b));
+    TRY(edp_nn_upsample(1, H / 4, W / 4, 128, 4, ws->d2b, ws->u1, c->stream));
+    TRY(conv(c, 10, H / 4, W / 4, ws->u1, 128, ws->s1, 64, ws->d1a));
+    TRY(conv(c, 11, H / 4, W / 4, ws->d1a, 64, nullptr, 0, ws->d1b));
     c->launches += 1;
-    TRY(edp_nn_upsample(1, H, W, 64, ws->d1b, ws->u0, c->stream));
+    TRY(edp_nn_upsample(1, H, W, 64, 4, ws->d1b, ws->u0, c->stream));
     TRY(conv(c, 12, H, W, ws->u0, 64, ws->s0, 32, ws->d0a));
     TRY(conv(c, 13, H, W, ws->d0a, 32, nullptr, 0, ws->d0b));
     c->launches += 1;
@@ -237,8 +237,8 @@ extern "C" int edp_warmstart_load(edp_ctx* c, const float* blob, int64_t n)
     edp_warmstart* ws = new edp_warmstart();
     c->ws = ws;
     const edp_kparams& kp = c->kp;
-    ws->H = (kp.nyg + 7) / 8 * 8;
-    ws->W = (kp.nxg + 7) / 8 * 8;
+    ws->H = (kp.nyg + 63) / 64 * 64;
+    ws->W = (kp.nxg + 63) / 64 * 64;
     const double L = (double)std::max(c->p.ncx, c->p.ncy);
     ws->K = L * L / (2.0 * 3.141592653589793 * 3.141592653589793);
     // unknown nodes: not on a wall, not in an inner object
@@ -267,7 +267,7 @@ extern "C" int edp_warmstart_load(edp_ctx* c, const float* blob, int64_t n)
     }
     EDP_CUDA(c, cudaMalloc(&ws->wh, 2 * (9 * 32 + 1) * sizeof(float)));
     EDP_CUDA(c, cudaMemcpy(ws->wh, q, 2 * (9 * 32 + 1) * sizeof(float), cudaMemcpyHostToDevice));
-    const int64_t p0 = (int64_t)ws->H * ws->W, p1 = p0 / 4, p2 = p0 / 16, p3 = p0 / 64;
+    const int64_t p0 = (int64_t)ws->H * ws->W, p1 = p0 / 16, p2 = p0 / 256, p3 = p0 / 4096;
     auto act = [&](bf16** ptr, int64_t pix, int ch) -> int {
         EDP_CUDA(c, cudaMalloc(ptr, pix * ch * sizeof(bf16)));
         return EDP_OK;

@@ -1,8 +1,8 @@
 """Learned warm start of the CG solve that replaces the PETSc path (no counterpart in the reference, whose solve
 starts from zero; SOLVE_POTENTIAL_WITH_PETSC, src/pic2d_ElectricFieldCalc_PETSc.F90:7-355).
 
-A 4-level convolutional encoder-decoder (channels 32-64-128-256, 3x3 kernels, 2x2 average pooling, nearest
-upsampling, skip concatenation, ReLU, BF16 weights and activations with FP32 accumulation; LAYERS below) maps the
+A 4-level convolutional encoder-decoder (channels 32-64-128-256, 3x3 kernels, 4x4 average pooling so that the
+bottleneck sees the whole domain, nearest upsampling, skip concatenation, ReLU, BF16 weights and activations with FP32 accumulation; LAYERS below) maps the
 residual r0 = b - A phi_prev of the previous potential against the new charge density, divided by its RMS s, and the
 Dirichlet mask to the update (phi - phi_prev) / s = K o0 + o1 through two FP32 heads, K = L^2 / (2 pi^2): o0 carries
 the smooth part (the inverse Laplacian grows like L^2 on the longest wavelengths) and o1 the grid-scale part, so both
@@ -24,6 +24,7 @@ LAYERS = [(32, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128), (128, 2
           (128, 128), (192, 64), (64, 64), (96, 32), (32, 32)]
 HEAD_C = 32
 IN_C = 32   # input channels: residual / s, Dirichlet mask, zeros
+POOL = 4    # pooling / upsampling factor per level
 
 
 N_HEADS = 2   # smooth (scaled by K) and grid-scale outputs
@@ -60,7 +61,9 @@ def init_params(seed=0):
 
 
 def padded(n):
-    return (n + 7) // 8 * 8
+    """grid size of the network image: three poolings by POOL"""
+    m = POOL ** 3
+    return (n + m - 1) // m * m
 
 
 def k_factor(ncx, ncy):
@@ -133,8 +136,8 @@ def _fns():
         @staticmethod
         def forward(ctx, x):
             n, h, w, c = x.shape
-            y = torch.empty((n, h // 2, w // 2, c), device=x.device, dtype=torch.bfloat16)
-            _check(lib.edp_nn_pool(n, h, w, c, _ptr(x), _ptr(y), stream()), "pool")
+            y = torch.empty((n, h // POOL, w // POOL, c), device=x.device, dtype=torch.bfloat16)
+            _check(lib.edp_nn_pool(n, h, w, c, POOL, _ptr(x), _ptr(y), stream()), "pool")
             ctx.dims = (n, h, w, c)
             return y
 
@@ -142,23 +145,24 @@ def _fns():
         def backward(ctx, dy):
             n, h, w, c = ctx.dims
             dx = torch.empty((n, h, w, c), device=dy.device, dtype=torch.bfloat16)
-            _check(lib.edp_nn_pool_bwd(n, h, w, c, _ptr(dy.contiguous()), _ptr(dx), 0, stream()), "pool_bwd")
+            _check(lib.edp_nn_pool_bwd(n, h, w, c, POOL, _ptr(dy.contiguous()), _ptr(dx), 0, stream()), "pool_bwd")
             return dx
 
     class Up(torch.autograd.Function):
         @staticmethod
         def forward(ctx, x):
             n, h, w, c = x.shape
-            y = torch.empty((n, 2 * h, 2 * w, c), device=x.device, dtype=torch.bfloat16)
-            _check(lib.edp_nn_upsample(n, 2 * h, 2 * w, c, _ptr(x), _ptr(y), stream()), "upsample")
-            ctx.dims = (n, 2 * h, 2 * w, c)
+            y = torch.empty((n, POOL * h, POOL * w, c), device=x.device, dtype=torch.bfloat16)
+            _check(lib.edp_nn_upsample(n, POOL * h, POOL * w, c, POOL, _ptr(x), _ptr(y), stream()), "upsample")
+            ctx.dims = (n, POOL * h, POOL * w, c)
             return y
 
         @staticmethod
         def backward(ctx, dy):
             n, h, w, c = ctx.dims
-            dx = torch.empty((n, h // 2, w // 2, c), device=dy.device, dtype=torch.bfloat16)
-            _check(lib.edp_nn_upsample_bwd(n, h, w, c, c, _ptr(dy.contiguous()), _ptr(dx), stream()), "upsample_bwd")
+            dx = torch.empty((n, h // POOL, w // POOL, c), device=dy.device, dtype=torch.bfloat16)
+            _check(lib.edp_nn_upsample_bwd(n, h, w, c, c, POOL, _ptr(dy.contiguous()), _ptr(dx), stream()),
+                   "upsample_bwd")
             return dx
 
     class Head(torch.autograd.Function):
@@ -209,7 +213,7 @@ class WarmStartNet:
         return self.Conv3x3.apply(x1, x2, w32, b32, wbf, co, relu)
 
     def forward(self, x):
-        """x: [images, H, W, 32] BF16 (H, W multiples of 8) -> (o0, o1), each [images, H, W] FP32."""
+        """x: [images, H, W, 32] BF16 (H, W multiples of 64) -> (o0, o1), each [images, H, W] FP32."""
         P, U = self.Pool.apply, self.Up.apply
         s0 = self._conv(1, self._conv(0, x))
         s1 = self._conv(3, self._conv(2, P(s0)))

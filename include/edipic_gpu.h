@@ -242,10 +242,11 @@ int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* rho_dev, do
 
 /* ---- learned warm start of the CG solve ----------------------------------------------------------- */
 /* No counterpart in the reference (its PETSc solve always starts from zero). A 4-level convolutional
- * encoder-decoder (channels 32-64-128-256, 3x3 kernels, 2x2 average pooling, nearest upsampling, skip
+ * encoder-decoder (channels 32-64-128-256, 3x3 kernels, 4x4 average pooling, nearest upsampling, skip
  * concatenation, ReLU; BF16 weights and activations, FP32 accumulation) maps the residual r0 = b - A phi_prev of
  * the previous potential, divided by its RMS s, and the Dirichlet mask to the update (phi - phi_prev) / s =
- * K o0 + o1 of its two FP32 heads, K = L^2 / (2 pi^2) with L the larger cell count. blob holds FP32 parameters in
+ * K o0 + o1 of its two FP32 heads, K = L^2 / (2 pi^2) with L the larger cell count. Each level pools 4 x 4, so the
+ * 9 x 9 bottleneck of a 513-node grid (padded to 576) sees the whole domain. blob holds FP32 parameters in
  * the order EDP_WARMSTART_LAYERS lists: per convolution the weights [c_out][3][3][c_in] then the biases [c_out];
  * last the two heads, each weights [3][3][32] and bias. */
 #define EDP_WARMSTART_N_CONV 14
@@ -265,11 +266,12 @@ int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, 
 int edp_nn_error(int32_t* out);
 int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
                          const void* dz, int32_t cout, float* dw, float* db, void* stream);
-int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream);
-int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* dy, void* dx, int32_t accumulate,
-                    void* stream);
-int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, const void* x, void* y, void* stream);
-int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, const void* dy, void* dx,
+/* f x f average pooling (h, w: input size) and nearest f x upsampling (h, w: output size), f = 2 or 4 */
+int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream);
+int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* dy, void* dx,
+                    int32_t accumulate, void* stream);
+int edp_nn_upsample(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream);
+int edp_nn_upsample_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t cs, int32_t f, const void* dy, void* dx,
                         void* stream);
 int edp_nn_relu_bwd(int64_t npix, int32_t c, const void* dy, int32_t cs, int32_t co, const void* dy2, const void* y,
                     void* dz, void* stream);

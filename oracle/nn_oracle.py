@@ -1,5 +1,5 @@
 """Oracle (test infrastructure only: imported by tests, never by the library) for the learned warm start's network:
-FP64 numpy restatements of the 3x3 convolution (forward, data gradient, weight and bias gradients), 2x2 average
+FP64 numpy restatements of the 3x3 convolution (forward, data gradient, weight and bias gradients), f x f average
 pooling, nearest upsampling, the FP32 head, and the whole encoder-decoder forward and backward pass with the
 activations rounded to BF16 where the device stores them.
 
@@ -60,22 +60,25 @@ def conv_wgrad(x, dz):
     return dw, dzf.sum(axis=0)
 
 
-def pool(x):
+POOL = 4   # pooling / upsampling factor of the network
+
+
+def pool(x, f=POOL):
     n, h, w, c = x.shape
-    return 0.25 * x.reshape(n, h // 2, 2, w // 2, 2, c).sum(axis=(2, 4))
+    return x.reshape(n, h // f, f, w // f, f, c).sum(axis=(2, 4)) / (f * f)
 
 
-def pool_bwd(dy):
-    return 0.25 * np.repeat(np.repeat(dy, 2, axis=1), 2, axis=2)
+def pool_bwd(dy, f=POOL):
+    return np.repeat(np.repeat(dy, f, axis=1), f, axis=2) / (f * f)
 
 
-def up(x):
-    return np.repeat(np.repeat(x, 2, axis=1), 2, axis=2)
+def up(x, f=POOL):
+    return np.repeat(np.repeat(x, f, axis=1), f, axis=2)
 
 
-def up_bwd(dy):
+def up_bwd(dy, f=POOL):
     n, h, w, c = dy.shape
-    return dy.reshape(n, h // 2, 2, w // 2, 2, c).sum(axis=(2, 4))
+    return dy.reshape(n, h // f, f, w // f, f, c).sum(axis=(2, 4))
 
 
 def head_fwd(x, wh, bh):

@@ -85,20 +85,21 @@ def test_glue_kernels_match_oracle():
     n, h, w, c = 2, 16, 24, 64
     x = O.bf16(rng.normal(0, 1, (n, h, w, c)))
     tx = _bf(x)
-    y = torch.empty((n, h // 2, w // 2, c), device="cuda", dtype=torch.bfloat16)
-    assert lib.edp_nn_pool(n, h, w, c, _p(tx), _p(y), _stream()) == 0
-    assert _rel(_np(y), O.pool(x)) < 5e-3
-    dy = O.bf16(rng.normal(0, 1, (n, h // 2, w // 2, c)))
-    dx = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
-    assert lib.edp_nn_pool_bwd(n, h, w, c, _p(_bf(dy)), _p(dx), 0, _stream()) == 0
-    assert np.array_equal(_np(dx), O.pool_bwd(dy))
-    u = torch.empty((n, 2 * h, 2 * w, c), device="cuda", dtype=torch.bfloat16)
-    assert lib.edp_nn_upsample(n, 2 * h, 2 * w, c, _p(tx), _p(u), _stream()) == 0
-    assert np.array_equal(_np(u), O.up(x))
-    du = O.bf16(rng.normal(0, 1, (n, 2 * h, 2 * w, c)))
-    dxu = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
-    assert lib.edp_nn_upsample_bwd(n, 2 * h, 2 * w, c, c, _p(_bf(du)), _p(dxu), _stream()) == 0
-    assert _rel(_np(dxu), O.up_bwd(du)) < 5e-3
+    for f in (2, 4):
+        y = torch.empty((n, h // f, w // f, c), device="cuda", dtype=torch.bfloat16)
+        assert lib.edp_nn_pool(n, h, w, c, f, _p(tx), _p(y), _stream()) == 0
+        assert _rel(_np(y), O.pool(x, f)) < 5e-3
+        dy = O.bf16(rng.normal(0, 1, (n, h // f, w // f, c)))
+        dx = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
+        assert lib.edp_nn_pool_bwd(n, h, w, c, f, _p(_bf(dy)), _p(dx), 0, _stream()) == 0
+        assert _rel(_np(dx), O.pool_bwd(dy, f)) < 5e-3
+        u = torch.empty((n, f * h, f * w, c), device="cuda", dtype=torch.bfloat16)
+        assert lib.edp_nn_upsample(n, f * h, f * w, c, f, _p(tx), _p(u), _stream()) == 0
+        assert np.array_equal(_np(u), O.up(x, f))
+        du = O.bf16(rng.normal(0, 1, (n, f * h, f * w, c)))
+        dxu = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
+        assert lib.edp_nn_upsample_bwd(n, f * h, f * w, c, c, f, _p(_bf(du)), _p(dxu), _stream()) == 0
+        assert _rel(_np(dxu), O.up_bwd(du, f)) < 5e-3
     yy = O.bf16(rng.normal(0, 1, (n, h, w, c)))
     dz = torch.empty((n, h, w, c), device="cuda", dtype=torch.bfloat16)
     assert lib.edp_nn_relu_bwd(n * h * w, c, _p(tx), c, 0, None, _p(_bf(yy)), _p(dz), _stream()) == 0
@@ -131,7 +132,7 @@ def test_network_gradient_matches_oracle():
     theta = warmstart.init_params(seed=3)
     heads0 = warmstart.param_layout()[1][0][0]
     theta[heads0:] *= 10.0   # livelier heads than at initialisation
-    x = O.bf16(rng.normal(0, 1, (2, 16, 24, 32)))
+    x = O.bf16(rng.normal(0, 1, (1, 64, 128, 32)))
     net = warmstart.WarmStartNet(theta)
     out = net.forward(_bf(x))
     dout = [rng.normal(0, 1, tuple(o.shape)) for o in out]

@@ -10,13 +10,13 @@ def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(0)
     n = sum(9 * ci * co + co for ci, co in O.LAYERS) + 2 * (9 * 32 + 1)
     theta = rng.normal(0, 1, n) * 0.2
-    x = rng.normal(0, 1, (1, 8, 8, 32))
+    x = rng.normal(0, 1, (1, 64, 64, 32))
     out, tape = O.net_forward(theta, x, quantize=False)
     dout = [rng.normal(0, 1, o.shape) for o in out]
     g = O.net_backward(theta, tape, dout)
     live = np.flatnonzero(np.abs(g) > 1e-3 * np.abs(g).max())
     checked = 0
-    for k in rng.choice(live, 10, replace=False):
+    for k in rng.choice(live, 6, replace=False):
         e = 1e-5
         tp, tm = theta.copy(), theta.copy()
         tp[k] += e
@@ -25,7 +25,7 @@ def test_oracle_backward_matches_finite_differences():
         fd = sum(((a - b) * d).sum() for a, b, d in zip(op, om, dout)) / (2 * e)
         assert abs(g[k] - fd) <= 1e-5 * abs(fd) + 1e-8
         checked += 1
-    assert checked == 10
+    assert checked == 6
 
 
 def test_bf16_rounding_matches_torch():
