@@ -43,6 +43,13 @@ def main():
                                  inner=g, seed=args.seed + k) for k, g in enumerate(geo)]
         dphi, unk = warmstart.generate_samples(dirs, args.steps, warmup=args.warmup)
     t1 = time.time()
+    # how white the residuals are: relative residual after one Jacobi step u = r0 / 4 (0.25 for white noise, near 1
+    # for fields smooth on the grid scale), on the first samples
+    with torch.no_grad():
+        x, rhat, t = warmstart.make_batch(dphi[:8], unk[:8])
+        jac = warmstart.stencil(rhat / 4.0, unk[:8])
+        jr = ((rhat - jac) ** 2).sum(dim=(1, 2)) / (rhat ** 2).sum(dim=(1, 2))
+        print("jacobi residual ratio of the samples:", [round(float(v), 4) for v in jr], flush=True)
     K = warmstart.k_factor(args.cells, args.cells)
     net = warmstart.WarmStartNet(seed=args.seed)
     hist = warmstart.train(net, dphi, unk, K, steps=args.train_steps, batch=args.batch, lr=args.lr,

@@ -255,7 +255,7 @@ def make_batch(dphi, unk):
     n_unk = unk.sum(dim=(1, 2)).clamp_min(1.0)
     s = torch.sqrt((r0 * r0).sum(dim=(1, 2)) / n_unk).clamp_min(1e-30)
     rhat = r0 / s[:, None, None]
-    x = torch.zeros(dphi.shape + (IN_C,), device=dphi.device, dtype=torch.bfloat16)
+    x = torch.zeros(tuple(dphi.shape) + (IN_C,), device=dphi.device, dtype=torch.bfloat16)
     x[..., 0] = rhat.to(torch.bfloat16)
     x[..., 1] = (1.0 - unk).to(torch.bfloat16)
     return x, rhat, dphi / s[:, None, None]
@@ -264,7 +264,7 @@ def make_batch(dphi, unk):
 def losses(out, rhat, t, unk, K):
     """Per-sample relative residual |r0 - A u|^2 / |r0|^2 and relative energy-norm error |t - u|_A^2 / |t|_A^2 of
     the normalised update u = K o0 + o1, as the CG start phi_prev + s u would see them."""
-    u = (K * out[0] + out[1]) * unk
+    u = (K * out[0].double() + out[1].double()) * unk
     r1 = rhat - stencil(u, unk)
     lr = (r1 * r1).sum(dim=(1, 2)) / (rhat * rhat).sum(dim=(1, 2)).clamp_min(1e-30)
     e = (t - u) * unk
@@ -295,7 +295,8 @@ def train(net, dphi, unk, K, steps=500, batch=4, lr=1e-3, seed=0, log=None):
 def generate_samples(deck_dirs, steps_per_deck, warmup=4, precision=None, rtol=1e-10, ppc=None):
     """Potential updates of plain runs: for every deck, the cycle is stepped with CG (multigrid preconditioner,
     previous-step warm start, tolerance rtol) and phi_n - phi_(n-1) is kept for every step after warmup.
-    Returns (dphi [N, H, W] FP32, unk [N, H, W] FP32) on the device, padded to multiples of 8."""
+    Returns (dphi [N, H, W] FP64, unk [N, H, W] FP64) on the device, padded for the network (FP64 keeps the residual
+    A dphi of smooth updates free of cancellation)."""
     torch = _torch()
     from . import FIELD_PHI, PREC_MIXED, Simulation
     out_d, out_u = [], []
@@ -305,7 +306,7 @@ def generate_samples(deck_dirs, steps_per_deck, warmup=4, precision=None, rtol=1
             sim.distribute_particles(ppc or p.n_of_particles_cell)
             ny, nx = p.ncy + 1, p.ncx + 1
             H, W = padded(ny), padded(nx)
-            unk = np.zeros((H, W), dtype=np.float32)
+            unk = np.zeros((H, W), dtype=np.float64)
             unk[1:ny - 1, 1:nx - 1] = 1.0
             for o in range(p.n_inner):
                 unk[p.inner_jbottom[o]:p.inner_jtop[o] + 1, p.inner_ileft[o]:p.inner_iright[o] + 1] = 0.0
@@ -315,7 +316,7 @@ def generate_samples(deck_dirs, steps_per_deck, warmup=4, precision=None, rtol=1
                 sim.solve_potential_with_cg(rtol=rtol, max_it=100000)
                 phi = sim.field(FIELD_PHI)
                 if prev is not None and k >= warmup:
-                    dp = np.zeros((H, W), dtype=np.float32)
+                    dp = np.zeros((H, W), dtype=np.float64)
                     dp[:ny, :nx] = (phi - prev) * unk[:ny, :nx]
                     out_d.append(dp)
                     out_u.append(unk)
