@@ -14,7 +14,8 @@ module edipic_gpu
   integer(c_int), parameter :: EDP_MAX_ION_SPECIES = 4, EDP_MAX_INNER = 4, EDP_MAX_COLPROC = 8, EDP_MAX_SEGMENTS = 32
   integer(c_int), parameter :: EDP_PREC_MIXED = 0, EDP_PREC_FP64 = 1, EDP_SOLVER_FFTX = 0, EDP_SOLVER_CG = 1
   integer(c_int), parameter :: EDP_ELECTRONS = 0, EDP_IONS = 1
-  integer(c_int), parameter :: EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1
+  integer(c_int), parameter :: EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_LEARNED = 3
+  integer(c_int), parameter :: EDP_PRECOND_NONE = 0, EDP_PRECOND_MG = 1
 
   type, bind(C) :: edp_params
      integer(c_int32_t) :: abi_version, ncx, ncy, periodic_x, n_subcycles, n_of_particles_cell
@@ -136,6 +137,23 @@ module edipic_gpu
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
      end function edp_end_ion_cycle
+     integer(c_int) function edp_set_cg_preconditioner(ctx, kind) bind(C, name="edp_set_cg_preconditioner")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: kind
+     end function edp_set_cg_preconditioner
+     integer(c_int) function edp_warmstart_load(ctx, blob, n) bind(C, name="edp_warmstart_load")
+       import :: c_ptr, c_int, c_int64_t, c_float
+       type(c_ptr), value :: ctx
+       real(c_float), intent(in) :: blob(*)
+       integer(c_int64_t), value :: n
+     end function edp_warmstart_load
+     integer(c_int) function edp_collect_moments(ctx, species, out) bind(C, name="edp_collect_moments")
+       import :: c_ptr, c_int, c_float
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: species
+       real(c_float), intent(out) :: out(*)
+     end function edp_collect_moments
      integer(c_int) function edp_query_counters(ctx, c) bind(C, name="edp_query_counters")
        import :: c_ptr, c_int, edp_counters
        type(c_ptr), value :: ctx
@@ -177,6 +195,13 @@ contains
   subroutine GPU_PERFORM_RESONANT_CHARGE_EXCHANGE
     call edp_check(edp_collide_rcx(edp_context, c_null_ptr), 'PERFORM_RESONANT_CHARGE_EXCHANGE')
   end subroutine GPU_PERFORM_RESONANT_CHARGE_EXCHANGE
+
+  ! COLLECT_ELECTRON_MOMENTS (and the moments branch of ADVANCE_ELECTRONS_PLUS, called before the push on a
+  ! snapshot step): the 13 grids cs_N, cs_VX, ... cs_QZ, each (c_indx_x_min:c_indx_x_max, c_indx_y_min:c_indx_y_max)
+  subroutine GPU_COLLECT_ELECTRON_MOMENTS(moments)
+    real(c_float), intent(out) :: moments(:,:,:)   ! (nodes x, nodes y, 13)
+    call edp_check(edp_collect_moments(edp_context, EDP_ELECTRONS, moments), 'COLLECT_ELECTRON_MOMENTS')
+  end subroutine GPU_COLLECT_ELECTRON_MOMENTS
 
   ! called at the end of every time step: on ion steps it is PROCESS_ADDED_IONS + CLEAR_ACCUMULATED_FIELDS,
   ! on every step it moves the ionisation add list and advances T_cntr
