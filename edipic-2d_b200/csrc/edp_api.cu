@@ -658,7 +658,9 @@ int edp_destroy(edp_ctx* c)
     F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
     edp_mg_free(c);
     edp_warmstart_free(c);
-    F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v);
+    F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v); F(c->maxwell_inj); F(c->emit_dev);
+    delete c->emit_h;
+    F(c->hits.x); F(c->hits.y); F(c->hits.vx); F(c->hits.vy); F(c->hits.vz); F(c->hits.id); F(c->hits.ws);
     F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -899,6 +901,71 @@ int edp_set_cg_preconditioner(edp_ctx* c, int32_t kind)
     return EDP_OK;
 }
 
+// GetInjMaxwellVelocity's table v_inj(0:R_max_inj) for the flux-weighted half-Maxwellian t exp(-t^2), t >= 0
+// (PrepareMaxwellDistribIntegral, pic2d_ElectronWallCollisions.f90:889-915): the inverse of its running integral at
+// R_max_inj equal steps.
+static std::vector<double> injection_maxwell_table(int rmax)
+{
+    const int n = 90000;
+    const double vmin = 0.0, dv = 3.0 / n;
+    std::vector<double> F(n + 4, 0.0), v(rmax + 1, 0.0);
+    for (int i = 1; i <= n + 3; ++i) {
+        const double t = vmin + ((double)(float)i - 0.5) * dv;
+        F[i] = F[i - 1] + std::exp(-(t * t)) * t;
+    }
+    const double tot = F[n];
+    v[0] = vmin;
+    int count = 0;
+    for (int i = 1; i <= n + 3 && count < rmax; ++i)
+        if ((int)(F[i] * rmax / tot) - count == 1) v[++count] = vmin + i * dv;
+    return v;
+}
+
+int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double yield, double emin_ev, double emax_ev,
+                         double t_emit_ev)
+{
+    if (!c || wall < 0 || wall > 3 || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
+        !(emax_ev > emin_ev) || !(t_emit_ev >= 0.0))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_emission");
+    if (!c->emit_h) {
+        const int rmax_inj = 4500;
+        std::vector<double> v = injection_maxwell_table(rmax_inj);
+        TRY(dalloc(c, &c->maxwell_inj, rmax_inj + 1));
+        EDP_CUDA(c, cudaMemcpy(c->maxwell_inj, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        TRY(dalloc(c, &c->emit_dev, 1));
+        edp_hits& h = c->hits;
+        h.cap = std::max<int64_t>(65536, c->born_cap);   // the electron add list's size, once allocated
+        TRY(dalloc(c, &h.x, h.cap));
+        TRY(dalloc(c, &h.y, h.cap));
+        TRY(dalloc(c, &h.vx, h.cap));
+        TRY(dalloc(c, &h.vy, h.cap));
+        TRY(dalloc(c, &h.vz, h.cap));
+        TRY(dalloc(c, &h.id, h.cap));
+        TRY(dalloc(c, &h.ws, h.cap));
+        c->emit_h = new edp_emit_dev();
+        memset(c->emit_h, 0, sizeof(edp_emit_dev));
+        c->emit_h->maxwell_v = c->maxwell_v;
+        c->emit_h->rmax = c->tab.maxwell_rmax;
+        c->emit_h->maxwell_inj = c->maxwell_inj;
+        c->emit_h->rmax_inj = rmax_inj;
+    }
+    edp_emit_dev& h = *c->emit_h;
+    const int s = ion_species - 1;
+    const double ef = c->tab.energy_factor_eV;
+    h.on[wall][s] = yield > 0.0;
+    h.yield[wall][s] = yield;
+    h.emin[wall][s] = emin_ev / ef;
+    h.emax[wall][s] = emax_ev / ef;
+    h.fconv[wall][s] = std::sqrt(t_emit_ev / ef);
+    h.ms[s] = c->p.ion_mass_me[s];
+    c->emit_on = 0;
+    for (int w = 0; w < 4; ++w)
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) c->emit_on |= h.on[w][q];
+    EDP_CUDA(c, cudaMemcpyAsync(c->emit_dev, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
 int edp_field_cg(edp_ctx* c, double rtol, int32_t max_it, int32_t warm, int32_t* iters_out)
 {
     if (!c || max_it < 1 || !(rtol > 0.0) || warm < EDP_WARM_ZERO || warm > EDP_WARM_LEARNED)
@@ -937,6 +1004,7 @@ int edp_advance_ions(edp_ctx* c)
         TRY(zero_density(c, 1 + s));
         TRY(edp_launch_push(c, 1 + s, true, fuse));
     }
+    if (c->emit_on) TRY(edp_launch_ion_emission(c));
     return finish_sync(c);
 }
 
@@ -1049,6 +1117,15 @@ int edp_query_counters(edp_ctx* c, edp_counters* out)
     if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "particle outside the domain");
     if (c->hc->error_flags & EDP_EFLAG_TIMEOUT) return edp_fail(c, EDP_ERR_TIMEOUT, "a bounded device wait gave up");
+    return EDP_OK;
+}
+
+int edp_query_emission(edp_ctx* c, int64_t* out)
+{
+    if (!c || !out) return EDP_ERR_ARG;
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    EDP_CUDA(c, cudaMemcpy(c->hc, c->dc, sizeof(edp_dev_counters), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < EDP_N_HIT_COUNTERS; ++k) out[k] = (int64_t)c->hc->e_emit[k];
     return EDP_OK;
 }
 

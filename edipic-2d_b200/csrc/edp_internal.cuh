@@ -41,12 +41,14 @@ struct edp_dev_counters {
     unsigned long long n_slots[EDP_MAX_SPECIES];   // high-water slot count (append cursor)
     unsigned long long n_live[EDP_MAX_SPECIES];
     unsigned long long e_hits[EDP_N_HIT_COUNTERS];
+    unsigned long long e_emit[EDP_N_HIT_COUNTERS];   // electrons emitted by each object (ion impacts)
     unsigned long long i_hits[EDP_N_HIT_COUNTERS];
     unsigned long long en_coll[EDP_MAX_COLPROC];
     unsigned long long en_coll_step[EDP_MAX_COLPROC];
     unsigned long long rcx[EDP_MAX_ION_SPECIES];
     unsigned long long rcx_step[EDP_MAX_ION_SPECIES];
     unsigned long long born_e_count;               // electrons born by ionisation this step
+    unsigned long long hit_count;                  // records in the wall-hit list
     unsigned long long born_i_count[EDP_MAX_ION_SPECIES];
     unsigned long long next_id[EDP_MAX_SPECIES];
     unsigned int error_flags;
@@ -73,8 +75,17 @@ struct edp_born {
     int64_t cap = 0;
 };
 
+// wall hits of ions while ion-induced electron emission is on: position, velocity, id, wall | species << 8
+struct edp_hits {
+    double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    uint32_t* id = nullptr;
+    int32_t* ws = nullptr;
+    int64_t cap = 0;
+};
+
 struct edp_mcc_dev;
 struct edp_warmstart;   // learned warm start of the CG solve (warmstart.cu)
+struct edp_emit_dev;    // ion-induced electron emission parameters (below)
 
 // one level of the multigrid preconditioner: (nx+1) x (ny+1) nodes, x fastest, spacing 2^level
 #define EDP_MG_MAX_LEVELS 16
@@ -153,6 +164,11 @@ struct edp_ctx {
     edp_mg_level mg[EDP_MG_MAX_LEVELS];
     size_t mg_smem = 0;               // shared memory of the coarse-level kernel
     edp_warmstart* ws = nullptr;      // network of the learned warm start, once loaded
+    edp_emit_dev* emit_dev = nullptr; // ion-induced electron emission (device copy of emit_h)
+    edp_emit_dev* emit_h = nullptr;   // host copy
+    edp_hits hits;                    // ion wall hits of the current ion step
+    int emit_on = 0;
+    double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
     int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     int32_t last_cg_iters = 0;
     double last_cg_relres = 0.0;
@@ -238,6 +254,7 @@ __host__ __device__ inline double edp_u01(uint32_t x) { return ((double)x + 0.5)
 #define EDP_STREAM_MCC 0u
 #define EDP_STREAM_RCX(s) (1u + ((uint32_t)(s) << 8))
 #define EDP_STREAM_INIT(sp) (2u + ((uint32_t)(sp) << 8))
+#define EDP_STREAM_EMIT(s) (0x45450000u + (uint32_t)(s))   // ion-induced electron emission, ion species s
 
 // --------------------------------------------------------------------------- collision tables (device)
 struct edp_mcc_dev {
@@ -489,6 +506,7 @@ edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
 
 // kernels launched from edp_api.cu, defined in the other translation units
 int edp_launch_push(edp_ctx* c, int species, bool ion_step, bool fuse);
+int edp_launch_ion_emission(edp_ctx* c);
 int edp_launch_collide_en(edp_ctx* c);
 int edp_launch_collide_rcx(edp_ctx* c);
 int edp_launch_append_born(edp_ctx* c);
@@ -515,3 +533,91 @@ int edp_launch_moments(edp_ctx* c, int species, double out[7]);
 int edp_launch_mcc_choose(edp_ctx* c, int64_t n, const double* E, const double* r, int32_t* out);
 int edp_fields_prepare(edp_ctx* c);   // one-time FFT/CG tables
 int edp_launch_deposit(edp_ctx* c, int species);   // CIC deposit of the whole array without a push
+
+// ------------------------------------------------------------------------------ ion-induced electron emission
+// Parameters of PROCESS_ION_INDUCED_ELECTRON_EMISSION (pic2d_IonEmissions.f90:1-56) for the four domain walls
+// (0 below, 1 above, 2 left, 3 right) and each ion species, as read from init_material_*.dat
+// (pic2d_Materials.f90:165-188): a constant yield for impact energies in (emin, emax), energies in the code's units
+// (an ion's energy is Ms v^2, an electron's v^2), and the velocity factor sqrt(T_emit / energy_factor_eV) of the
+// emitted electrons (= sqrt(T_emit / T_e) / N_max_vel, :188).
+struct edp_emit_dev {
+    int on[4][EDP_MAX_ION_SPECIES];
+    double yield[4][EDP_MAX_ION_SPECIES];
+    double emin[4][EDP_MAX_ION_SPECIES], emax[4][EDP_MAX_ION_SPECIES];
+    double fconv[4][EDP_MAX_ION_SPECIES];
+    double ms[EDP_MAX_ION_SPECIES];
+    const double* maxwell_v;   // GetMaxwellVelocity table, rmax + 1 values
+    const double* maxwell_inj; // GetInjMaxwellVelocity table, rmax_inj + 1 values
+    int rmax, rmax_inj;
+};
+
+// GetInjMaxwellVelocity (pic2d_ElectronWallCollisions.f90:933-957) driven by one uniform variate
+__device__ inline double edp_maxwell_inj(const double* v, int rmax, double u)
+{
+    double R = rmax * u;
+    int indx = (int)R;
+    if (indx < rmax) return __ldg(&v[indx]) + (R - indx) * (__ldg(&v[indx + 1]) - __ldg(&v[indx]));
+    return __ldg(&v[rmax]);
+}
+
+// PROCESS_ION_INDUCED_ELECTRON_EMISSION + INJECT_ION_IMPACT_EXTRACTED_ELECTRON (pic2d_IonEmissions.f90:1-342) for an
+// ion of species s absorbed by wall `wall` at (x, y) (the tangential coordinate already inside the domain) with
+// velocity v. Variates: Philox4x32-10, key {id, seed_lo}, counter {step, EDP_STREAM_EMIT(s), block, seed_hi};
+// block 0 word 0 decides the fractional part of the yield, block 1 + e words 0, 1, 2 give electron e's normal
+// (injection) component and its two tangential components in x, y, z order. Emitted electrons start 1e-6 inside the
+// wall and go to `out` (the electron add list). Returns the number emitted.
+template <class Out>
+__device__ __noinline__ int edp_emit_electrons(const edp_emit_dev* em, int s, int wall, double x, double y,
+                                               double vx, double vy, double vz, uint32_t id, uint32_t step,
+                                               uint32_t seed_lo, uint32_t seed_hi, double xmax, double ymax, Out out)
+{
+    if (!em->on[wall][s]) return 0;
+    double energy = em->ms[s] * (vx * vx + vy * vy + vz * vz);
+    if (energy <= em->emin[wall][s] || energy >= em->emax[wall][s]) return 0;
+    double coef = em->yield[wall][s];
+    if (coef == 0.0) return 0;
+    energy = fmax(0.0, energy - em->emin[wall][s]);
+    const double f = em->fconv[wall][s];
+    int n = 0, e = 0;
+    auto inject = [&]() {
+        if (energy <= 0.0) return;
+        uint32_t w[4];
+        edp_philox(step, EDP_STREAM_EMIT(s), 1u + (uint32_t)e, seed_hi, id, seed_lo, w);
+        ++e;
+        const double un = edp_maxwell_inj(em->maxwell_inj, em->rmax_inj, edp_u01(w[0]));
+        const double t1 = edp_maxwell(em->maxwell_v, em->rmax, edp_u01(w[1]));
+        const double t2 = edp_maxwell(em->maxwell_v, em->rmax, edp_u01(w[2]));
+        double nx, ny, nvx, nvy, nvz;
+        switch (wall) {
+        case 0: nx = x; ny = 1.0e-6; nvx = t1; nvy = un; nvz = t2; break;            // below (dirflag 4)
+        case 1: nx = x; ny = ymax - 1.0e-6; nvx = t1; nvy = -un; nvz = t2; break;    // above (dirflag 2)
+        case 2: nx = 1.0e-6; ny = y; nvx = un; nvy = t1; nvz = t2; break;            // left (dirflag 1)
+        default: nx = xmax - 1.0e-6; ny = y; nvx = -un; nvy = t1; nvz = t2; break;   // right (dirflag 3)
+        }
+        nvx *= f;
+        nvy *= f;
+        nvz *= f;
+        const double en = nvx * nvx + nvy * nvy + nvz * nvz;
+        if (en > energy) {   // the electron takes what is left of the ion's energy
+            const double alpha = sqrt(energy / en);
+            nvx *= alpha;
+            nvy *= alpha;
+            nvz *= alpha;
+            energy = 0.0;
+        } else {
+            energy -= en;
+        }
+        const double v3[3] = {nvx, nvy, nvz};
+        out(nx, ny, v3);
+        ++n;
+    };
+    while (coef >= 1.0) {
+        inject();
+        coef -= 1.0;
+    }
+    if (coef == 0.0) return n;
+    uint32_t w0[4];
+    edp_philox(step, EDP_STREAM_EMIT(s), 0u, seed_hi, id, seed_lo, w0);
+    if (edp_u01(w0[0]) < coef) inject();
+    return n;
+}

@@ -34,6 +34,8 @@ struct PushArgs {
     uint32_t* sel_list;
     unsigned long long* sel_count;
     int64_t sel_cap;
+    edp_hits hits;                 // wall-hit list of ion-induced electron emission
+    int emit_on;
 };
 
 __device__ __forceinline__ int wrapx(int lx, const edp_kparams& kp)
@@ -74,6 +76,25 @@ __device__ __forceinline__ void record_born(const edp_born& b, unsigned long lon
     b.vx[k] = v[0];
     b.vy[k] = v[1];
     b.vz[k] = v[2];
+}
+
+// An ion absorbed by a domain wall while ion-induced electron emission is on: its record goes to the wall-hit list
+// (the emission itself runs in ion_emission_kernel after the push, so that the push keeps no call frame).
+__device__ __forceinline__ void record_hit(const edp_hits& h, edp_dev_counters* dc, int wall, int s, double x,
+                                           double y, double vx, double vy, double vz, uint32_t id)
+{
+    unsigned long long k = atomicAdd(&dc->hit_count, 1ull);
+    if ((int64_t)k >= h.cap) {
+        atomicOr(&dc->error_flags, EDP_EFLAG_PENDING);
+        return;
+    }
+    h.x[k] = x;
+    h.y[k] = y;
+    h.vx[k] = vx;
+    h.vy[k] = vy;
+    h.vz[k] = vz;
+    h.id[k] = id;
+    h.ws[k] = wall | (s << 8);
 }
 
 // Shared state of one CTA of the mixed push: field window, density window and per-CTA counters.
@@ -204,14 +225,23 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     if (PER) {
         if (ni < 0) ni += kp.ncx;
         else if (ni >= kp.ncx) ni -= kp.ncx;
-        if (nj < 0) { atomicAdd(&s.cnt[0], 1ull); return false; }
-        if (nj > kp.ncy || (nj == kp.ncy && ny > 0.0f)) { atomicAdd(&s.cnt[1], 1ull); return false; }
+        if (nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f)) {
+            const int wall = nj < 0 ? 0 : 1;
+            atomicAdd(&s.cnt[wall], 1ull);
+            if (ION && a.emit_on)
+                record_hit(a.hits, a.dc, wall, a.species - 1, (double)ni + (double)nx, (double)nj + (double)ny, vx,
+                           vy, vz, id);
+            return false;
+        }
     } else {
         bool outx = ni < 0 || ni > kp.ncx || (ni == kp.ncx && nx > 0.0f);
         bool outy = nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f);
         if (outx || outy) {
             int obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
             atomicAdd(&s.cnt[obj], 1ull);
+            if (ION && a.emit_on)
+                record_hit(a.hits, a.dc, obj, a.species - 1, (double)ni + (double)nx, (double)nj + (double)ny, vx,
+                           vy, vz, id);
             return false;
         }
         if (ni == kp.ncx) { ni = kp.ncx - 1; nx = 1.0f; }   // X == c_X_area_max (:68)
@@ -296,7 +326,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
         vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
         vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
         vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
-        if (a.do_coll) {
+        if (a.do_coll || (ION && a.emit_on)) {
             uint4 id4 = __ldcs(reinterpret_cast<const uint4*>(a.P.id) + g);
             id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
         } else {
@@ -497,6 +527,8 @@ struct PushArgs64 {
     edp_dev_counters* dc;
     edp_born born_e;
     edp_born born_i[EDP_MAX_ION_SPECIES];
+    edp_hits hits;              // wall-hit list of ion-induced electron emission
+    int emit_on;
 };
 
 // The plain FP64 cycle: one particle per thread, the reference's arithmetic in FP64, global atomics.
@@ -565,6 +597,8 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             a.P.x[k] = -1.0e30;
             atomicAdd(&cnt[obj], 1ull);
             atomicAdd(&cnt[17], 1ull);
+            if (a.is_ion && a.emit_on && obj < 4)
+                record_hit(a.hits, a.dc, obj, a.species - 1, X, Y, vx, vy, vz, a.P.id[k]);
             continue;
         }
         // deposit
@@ -864,6 +898,8 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.sel_list = c->sel_list;
         a.sel_count = c->sel_count;
         a.sel_cap = c->sel_cap;
+        a.hits = c->hits;
+        a.emit_on = is_ion && c->emit_on;
         if (do_mcc) EDP_CUDA(c, cudaMemsetAsync(c->sel_count, 0, sizeof(unsigned long long), c->stream));
         int64_t tail = c->host_slots[sp] - c->sorted_end[sp];
         if (tail < 0) tail = 0;
@@ -923,6 +959,8 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.dc = c->dc;
         a.born_e = c->born_e;
         for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
+        a.hits = c->hits;
+        a.emit_on = is_ion && c->emit_on;
         int64_t n = c->host_slots[sp];
         int64_t grid = (n + 255) / 256;
         if (grid > 148 * 64) grid = 148 * 64;
@@ -931,6 +969,34 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         push_fp64_kernel<<<(unsigned)grid, 256, 0, c->stream>>>(a);
     }
     EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+// PROCESS_ION_INDUCED_ELECTRON_EMISSION for every recorded wall hit of this ion step. PROCESS_ION_COLL_WITH_BOUNDARY_*
+// (pic2d_IonWallCollisions.f90:63-303) first clamps the coordinate along the wall into the domain.
+__global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp_emit_dev* em, edp_born born_e,
+                                                           edp_dev_counters* dc, edp_kparams kp, uint32_t step)
+{
+    const int64_t n = min((int64_t)dc->hit_count, h.cap);
+    const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int ws = h.ws[k], wall = ws & 255, s = ws >> 8;
+        const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
+        const int m = edp_emit_electrons(em, s, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
+                                         kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
+                                             record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
+                                         });
+        if (m) atomicAdd(&dc->e_emit[wall], (unsigned long long)m);
+    }
+}
+
+int edp_launch_ion_emission(edp_ctx* c)
+{
+    ++c->launches;
+    ion_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->emit_dev, c->born_e, c->dc, c->kp,
+                                                      (uint32_t)c->t_cntr);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));
     return EDP_OK;
 }
 

@@ -63,6 +63,13 @@ class Deck:
         self.init_te_ev, self.init_ne_m3, self.t_e_ev = te.value, ne.value, tev.value
         self.init_ti_ev = [ti[s] for s in range(_abi.MAX_ION)]
         self.n_max_vel, self.n_plasma_m3, self.max_t_cntr = nmv.value, npl.value, maxt.value
+        # ion-induced electron emission of the walls' materials: {(wall, ion species): (yield, E_min, E_max, T)}
+        self.ion_emission = {}
+        buf = (C.c_double * 4)()
+        for wall in range(4):
+            for s in range(1, self.params.n_ion_species + 1):
+                if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
+                    self.ion_emission[(wall, s)] = tuple(buf)
 
     def close(self):
         if self.handle:
@@ -104,6 +111,8 @@ class Simulation:
         self.periodic = bool(p.periodic_x)
         self.nx_ref = p.ncx + 2 if self.periodic else p.ncx + 1
         self.ny_ref = p.ncy + 1
+        for (wall, s), (yld, e0, e1, t) in self.deck.ion_emission.items():
+            self.set_ion_emission(wall, s, yld, e0, e1, t)
 
     # ------------------------------------------------------------------------------------ plumbing
     def _check(self, rc, where):
@@ -219,6 +228,19 @@ class Simulation:
     def set_cg_preconditioner(self, kind):
         """PRECOND_MG (default): a multigrid V-cycle per CG iteration; PRECOND_NONE: plain CG."""
         self._check(self.lib.edp_set_cg_preconditioner(self.ctx, kind), "edp_set_cg_preconditioner")
+
+    def set_ion_emission(self, wall, ion_species, yield_, emin_ev, emax_ev, t_emit_ev):
+        """Ion-induced electron emission of a domain wall (0 below, 1 above, 2 left, 3 right) for an ion species
+        (1-based): PROCESS_ION_INDUCED_ELECTRON_EMISSION (pic2d_IonEmissions.f90:1-348). yield_ 0 turns it off."""
+        self._check(self.lib.edp_set_ion_emission(self.ctx, wall, ion_species, yield_, emin_ev, emax_ev, t_emit_ev),
+                    "edp_set_ion_emission")
+
+    def emission_counts(self):
+        """Electrons emitted by ion impacts on each object (walls 0-3, then inner objects), cumulative."""
+        out = np.zeros(4 + _abi.MAX_INNER, np.int64)
+        self._check(self.lib.edp_query_emission(self.ctx, out.ctypes.data_as(C.POINTER(C.c_int64))),
+                    "edp_query_emission")
+        return out
 
     def advance_electrons(self):
         self._check(self.lib.edp_advance_electrons(self.ctx), "edp_advance_electrons")

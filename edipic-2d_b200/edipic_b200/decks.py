@@ -29,7 +29,7 @@ CONFIGS = {
     "cfg2": dict(ncx=512, ncy=512, periodic=False, ppc=100, n_init=1.0e16, dt=5e-12, steps=2000, bx=0.0, by=0.0,
                  inner=(224, 112, 288, 144, -100.0)),
     "cfg4": dict(ncx=2048, ncy=512, periodic=True, ppc=100, n_init=5.0e15, dt=1e-11, steps=100000, bx=0.0, by=0.0,
-                 top_rf=(200.0, 13.56)),
+                 top_rf=(200.0, 13.56), ion_emission=(0.1, 0.0, 10000.0, 2.0)),
 }
 
 
@@ -56,7 +56,10 @@ def _segments():
 
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
-               collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21):
+               collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
+               ion_emission=None):
+    """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
+    (the wall material METAL1), False for none, None for the configuration's default."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -156,6 +159,55 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
             "-------d------- save collided ions", f"       {0:1d}",
             "-------d------- save collided electrons", f"       {0:1d}",
         ])
+    iee = cfg.get("ion_emission") if ion_emission is None else (ion_emission or None)
+    # init_material_METAL1.dat in the layout PREPARE_WALL_MATERIALS reads (pic2d_Materials.f90:79-188): electron
+    # reflection and secondary emission off, ion-material model 2 (ion-induced emission) or 0 (absorption)
+    mat = [
+        "------dd.ddd- dielectric constant", f"      {1.0:6.3f}",
+        "=======d===== elastic electron reflection model", f"       {0:1d}",
+        "-------d----- elastic electron reflection type", f"       {0:1d}",
+        "------------- elastic reflection, model 1",
+        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
+        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
+        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "------------- elastic reflection, model 2",
+        "--dddddd.ddd- threshold [eV]", f"  {0.0:10.3f}",
+        "--dddddd.ddd- energy of the maximum [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- maximum", f"       {0.0:5.3f}",
+        "--dddddd.ddd- decay scale [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- high-energy fraction", f"       {0.0:5.3f}",
+        "=======d===== inelastic electron reflection model", f"       {0:1d}",
+        "------------- inelastic reflection, model 1",
+        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
+        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
+        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "------------- inelastic reflection, model 2",
+        "-------d.ddd- fraction", f"       {0.0:5.3f}",
+        "=======d===== true secondary emission model", f"       {0:1d}",
+        "--dddddd.ddd- temperature [eV]", f"  {0.0:10.3f}",
+        "------------- true secondary emission, model 1",
+        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
+        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
+        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "------------- true secondary emission, model 2",
+        "--dddddd.ddd- threshold [eV]", f"  {0.0:10.3f}",
+        "--dddddd.ddd- energy of the maximum [eV]", f"  {0.0:10.3f}",
+        "------dd.ddd- maximum", f"      {0.0:6.3f}",
+        "-------d.ddd- smoothness", f"       {0.0:5.3f}",
+        "=======d===== ION-MATERIAL INTERACTION MODEL (0 absorb, 1 reflect, 2 ion-induced electron emission)",
+        f"       {2 if iee else 0:1d}",
+    ]
+    if iee:
+        yld, e0, e1, t = iee
+        for s in range(1):   # one ion species (Ar+)
+            mat += [
+                f"------------- ION-INDUCED ELECTRON EMISSION, ION SPECIES {s + 1}",
+                "-------d.ddd- coefficient", f"       {yld:5.3f}",
+                "--dddddd.ddd- E_min [eV]", f"  {e0:10.3f}",
+                "--dddddd.ddd- E_max [eV]", f"  {e1:10.3f}",
+                "--dddddd.ddd- temperature of emitted electrons [eV]", f"  {t:10.3f}",
+            ]
+    w("init_material_METAL1.dat", mat)
     wp = wall_potentials or {}
     for k, (ty, _s) in enumerate(objs):
         if ty == 1:

@@ -142,6 +142,19 @@ module edipic_gpu
        type(c_ptr), value :: ctx
        integer(c_int32_t), value :: kind
      end function edp_set_cg_preconditioner
+     ! PREPARE_WALL_MATERIALS (pic2d_Materials.f90:150-188) passes each wall's ion-induced emission here
+     integer(c_int) function edp_set_ion_emission(ctx, wall, ion_species, yield, emin_ev, emax_ev, t_emit_ev) &
+          bind(C, name="edp_set_ion_emission")
+       import :: c_ptr, c_int, c_int32_t, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: wall, ion_species
+       real(c_double), value :: yield, emin_ev, emax_ev, t_emit_ev
+     end function edp_set_ion_emission
+     integer(c_int) function edp_query_emission(ctx, counts) bind(C, name="edp_query_emission")
+       import :: c_ptr, c_int, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), intent(out) :: counts(*)
+     end function edp_query_emission
      integer(c_int) function edp_warmstart_load(ctx, blob, n) bind(C, name="edp_warmstart_load")
        import :: c_ptr, c_int, c_int64_t, c_float
        type(c_ptr), value :: ctx

@@ -113,6 +113,8 @@ struct edp_deck {
     double init_te = 0, init_ne = 0, init_ti[EDP_MAX_ION_SPECIES] = {0}, t_e = 0, n_plasma = 0;
     int32_t n_max_vel = 0;
     int64_t max_t_cntr = 0;
+    // ion-induced electron emission of the four walls per ion species: yield, E_min [eV], E_max [eV], T [eV]
+    double ii_ee[4][EDP_MAX_ION_SPECIES][4] = {};
 };
 
 namespace {
@@ -277,6 +279,41 @@ int read_deck(const std::string& dir, edp_deck* d)
         if (side_obj[s] >= 0 &&
             !read_bo(side_obj[s], &p.wall_phi_const[s], &p.wall_phi_var[s], &p.wall_omega[s], &p.wall_phase[s]))
             return EDP_ERR_IO;
+    // ---- wall materials (material name: init_bo_NN.dat line 2, (6x,A6), pic2d_Setup.f90:77; properties
+    // init_material_<NAME>.dat, PREPARE_WALL_MATERIALS pic2d_Materials.f90:1-200). Only the ion-material interaction
+    // model is used: 2 = ion-induced electron emission with, per ion species, a constant coefficient between
+    // E_min and E_max and the temperature of the emitted electrons. A missing file means default materials.
+    for (int w = 0; w < 4; ++w) {
+        if (side_obj[w] < 0) continue;
+        char name[32];
+        snprintf(name, sizeof(name), "/init_bo_%02d.dat", side_obj[w] + 1);
+        Lines bf(dir + name);
+        if (!bf.ok || !bf.next(L) || !bf.next(L)) continue;
+        const std::string mat = (L + "      ").substr(6, 6);   // the six characters of the A6 field
+        if (mat == "      ") continue;
+        Lines mf(dir + "/init_material_" + mat + ".dat");
+        if (!mf.ok) continue;
+        bool found = false;
+        while (mf.next(L))
+            if (L.find("ION-MATERIAL INTERACTION MODEL") != std::string::npos) {
+                found = true;
+                break;
+            }
+        long long flag = 0;
+        if (!found || !mf.next(L) || !fint(L, 7, 1, &flag)) continue;
+        if (flag != 2) continue;
+        for (int s = 0; s < (int)p.n_ion_species; ++s) {
+            double yv = 0, e0 = 0, e1 = 0, te = 0;
+            bool ok = mf.next(L) && mf.next(L) && mf.next(L) && freal(L, 7, 5, &yv) && mf.next(L) && mf.next(L) &&
+                      freal(L, 2, 10, &e0) && mf.next(L) && mf.next(L) && freal(L, 2, 10, &e1) && mf.next(L) &&
+                      mf.next(L) && freal(L, 2, 10, &te);
+            if (!ok) return EDP_ERR_IO;
+            d->ii_ee[w][s][0] = yv;
+            d->ii_ee[w][s][1] = e0;
+            d->ii_ee[w][s][2] = e1;
+            d->ii_ee[w][s][3] = te;
+        }
+    }
     if (nio > EDP_MAX_INNER) return EDP_ERR_IO;
     p.n_inner = (int32_t)nio;
     for (int n = 0; n < nio; ++n) {
@@ -475,6 +512,13 @@ int edp_deck_initial_plasma(const edp_deck* d, double* te, double* ne, double* t
     if (nmv) *nmv = d->n_max_vel;
     if (np) *np = d->n_plasma;
     if (maxt) *maxt = d->max_t_cntr;
+    return EDP_OK;
+}
+
+int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out)
+{
+    if (!d || !out || wall < 0 || wall > 3 || ion_species < 1 || ion_species > EDP_MAX_ION_SPECIES) return EDP_ERR_ARG;
+    for (int k = 0; k < 4; ++k) out[k] = d->ii_ee[wall][ion_species - 1][k];
     return EDP_OK;
 }
 

@@ -188,6 +188,13 @@ int edp_field_fftx(edp_ctx* ctx, double* phi_out);
 int edp_field_cg(edp_ctx* ctx, double rtol, int32_t max_it, int32_t warm_start, int32_t* iters_out);
 /* selects the preconditioner of edp_field_cg (edp_precond) */
 int edp_set_cg_preconditioner(edp_ctx* ctx, int32_t kind);
+/* Ion-induced electron emission of a domain wall (ion-material interaction model 2, pic2d_Materials.f90:150-188;
+ * PROCESS_ION_INDUCED_ELECTRON_EMISSION, pic2d_IonEmissions.f90:1-348): ions of ion_species (1-based) absorbed by
+ * wall (0 below, 1 above, 2 left, 3 right) with energy in (emin_ev, emax_ev) emit on average `yield` electrons with
+ * temperature t_emit_ev, within the ion's energy. The emitted electrons join the electron arrays at the end of the
+ * step (edp_end_ion_cycle) and are counted per wall (edp_query_emission). yield 0 switches the wall off. */
+int edp_set_ion_emission(edp_ctx* ctx, int32_t wall, int32_t ion_species, double yield, double emin_ev,
+                         double emax_ev, double t_emit_ev);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
  * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
 int edp_advance_electrons(edp_ctx* ctx);
@@ -208,6 +215,8 @@ int edp_step(edp_ctx* ctx, int32_t nsteps);
 
 /* ---- diagnostics / test access -------------------------------------------------------------------- */
 int edp_query_counters(edp_ctx* ctx, edp_counters* out);
+/* electrons emitted by ion impacts on each object since the start (out[EDP_N_HIT_COUNTERS], walls first) */
+int edp_query_emission(edp_ctx* ctx, int64_t* out);
 /* node arrays in the reference layout (see Conventions) */
 int edp_get_field(edp_ctx* ctx, int which, double* out);
 int edp_set_field(edp_ctx* ctx, int which, const double* in);
@@ -294,6 +303,10 @@ int edp_deck_read(const char* dir, edp_deck** out, edp_params* p, edp_tables* t)
 /* initial plasma of init_particles.dat: init_Te_eV, init_Ne_m3, init_Ti_eV(s), T_e_eV, N_max_vel ... */
 int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_ne_m3, double* init_ti_ev,
                             double* t_e_ev, int32_t* n_max_vel, double* n_plasma_m3, int64_t* max_t_cntr);
+/* ion-induced electron emission of wall (0 below, 1 above, 2 left, 3 right) for ion_species (1-based), from the
+ * wall's init_material_<NAME>.dat: out = {yield, E_min [eV], E_max [eV], T_emit [eV]}, all 0 when the wall's
+ * material has no emission (pic2d_Materials.f90:150-188) */
+int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out);
 int edp_deck_free(edp_deck* d);
 
 #ifdef __cplusplus

@@ -82,6 +82,20 @@ int32_t oracle_nx_nodes(const oracle_geom_t* g) { return g->periodic ? g->ncx + 
 void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
                  oracle_parts_t* p, int64_t* hits)
 {
+    int64_t n_hit = 0;
+    oracle_push_hits(g, sp, EX, EY, p, hits, nullptr, 0, &n_hit);
+}
+
+void oracle_push_hits(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                      oracle_parts_t* p, int64_t* hits, double* hit_rows, int64_t cap, int64_t* n_hit)
+{
+    auto record = [&](int obj, double X, double Y, int64_t k) {
+        if (hit_rows && *n_hit < cap) {
+            double* r = hit_rows + 7 * *n_hit;
+            r[0] = obj; r[1] = X; r[2] = Y; r[3] = p->vx[k]; r[4] = p->vy[k]; r[5] = p->vz[k]; r[6] = p->id[k];
+        }
+        ++*n_hit;
+    };
     const Area a = area_of(g);
     const double L = (double)g->ncx;  // L_period_X
     int64_t k = 0;
@@ -179,9 +193,11 @@ void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const doubl
             else if (X > a.xmax) X -= L;
             if (Y < a.ymin) {
                 hits[0]++;
+                record(0, X, Y, k);
                 remove_particle(p, k);
             } else if (Y > a.ymax) {
                 hits[1]++;
+                record(1, X, Y, k);
                 remove_particle(p, k);
             } else {
                 p->x[k] = X;
@@ -206,6 +222,7 @@ void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const doubl
             obj = 0;
         }
         hits[obj]++;
+        record(obj, X, Y, k);
         remove_particle(p, k);
     }
 }
@@ -435,6 +452,81 @@ double oracle_maxwell_sample(const double* v, double u)
     int indx = (int)R;
     if (indx < R_max) return v[indx] + (R - indx) * (v[indx + 1] - v[indx]);
     return v[R_max];
+}
+
+// GetInjMaxwellVelocity pic2d_ElectronWallCollisions.f90:933-957
+static double maxwell_inj_sample(const double* v, double u)
+{
+    const int R_max_inj = 4500;
+    double R = R_max_inj * u;
+    int indx = (int)R;
+    if (indx < R_max_inj) return v[indx] + (R - indx) * (v[indx + 1] - v[indx]);
+    return v[R_max_inj];
+}
+
+// PROCESS_ION_INDUCED_ELECTRON_EMISSION pic2d_IonEmissions.f90:1-89 (Coeff_ii_EE_True :350-372 is the constant
+// yield inside (minE, maxE); the angle of incidence is computed there but not used) and
+// INJECT_ION_IMPACT_EXTRACTED_ELECTRON :91-348 for the domain walls (m > 0): position 1e-6 inside the wall,
+// normal component from the injection distribution, tangential ones Maxwellian, all times the conversion factor,
+// scaled down to the ion's remaining energy when above it.
+int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, double y, double vx, double vy,
+                            double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
+                            double* out, int32_t cap)
+{
+    if (!em->on[wall]) return 0;
+    x = std::min(std::max(x, 0.0), xmax);
+    y = std::min(std::max(y, 0.0), ymax);
+    double energy_inc = em->ms * (vx * vx + vy * vy + vz * vz);
+    if (energy_inc <= em->emin[wall]) return 0;
+    if (energy_inc >= em->emax[wall]) return 0;
+    double coef_total = em->yield[wall];
+    if (coef_total == 0.0) return 0;
+    energy_inc = std::max(0.0, energy_inc - em->emin[wall]);
+    const uint32_t stream = 0x45450000u + em->species;
+    int32_t n = 0;
+    uint32_t block = 1;
+    auto inject = [&]() {
+        if (energy_inc <= 0.0) return;
+        uint32_t w[4];
+        philox_block(id, seed, step, stream, block++, w);
+        double un = maxwell_inj_sample(em->maxwell_inj, uniform(w[0]));
+        double t1 = oracle_maxwell_sample(em->maxwell_v, uniform(w[1]));
+        double t2 = oracle_maxwell_sample(em->maxwell_v, uniform(w[2]));
+        double xn, yn, v[3];
+        if (wall == 2) {        // left, dirflag 1
+            xn = 1.0e-6; yn = y; v[0] = un; v[1] = t1; v[2] = t2;
+        } else if (wall == 3) { // right, dirflag 3
+            xn = xmax - 1.0e-6; yn = y; v[0] = -un; v[1] = t1; v[2] = t2;
+        } else if (wall == 0) { // below, dirflag 4
+            xn = x; yn = 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2;
+        } else {                // above, dirflag 2
+            xn = x; yn = ymax - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2;
+        }
+        const double f = em->fconv[wall];
+        for (double& c : v) c *= f;
+        double energy_new = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (energy_new > energy_inc) {
+            double alpha = std::sqrt(energy_inc / energy_new);
+            for (double& c : v) c *= alpha;
+            energy_inc = 0.0;
+        } else {
+            energy_inc -= energy_new;
+        }
+        if (n < cap) {
+            double* r = out + 5 * n;
+            r[0] = xn; r[1] = yn; r[2] = v[0]; r[3] = v[1]; r[4] = v[2];
+        }
+        ++n;
+    };
+    while (coef_total >= 1.0) {
+        inject();
+        coef_total -= 1.0;
+    }
+    if (coef_total == 0.0) return n;
+    uint32_t w0[4];
+    philox_block(id, seed, step, stream, 0u, w0);
+    if (uniform(w0[0]) < coef_total) inject();
+    return n;
 }
 
 // --------------------------------------------------------------------------- e-n collision table

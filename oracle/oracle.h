@@ -57,6 +57,12 @@ typedef struct {
 void oracle_push(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
                  oracle_parts_t* p, int64_t* hits);
 
+/* oracle_push that also records each domain-wall absorption (objects 0-3) as 7 doubles
+ * {wall, X, Y, vx, vy, vz, id}: the position after the move (X wrapped on the periodic cluster) and the pushed
+ * velocity, in push order; at most cap rows, *n_hit receives the number of absorptions. */
+void oracle_push_hits(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
+                      oracle_parts_t* p, int64_t* hits, double* hit_rows, int64_t cap, int64_t* n_hit);
+
 /* CIC deposit of GATHER_ELECTRON_CHARGE_DENSITY (pic2d_ElectronDynamics.f90:1597-1639) into rho
  * (zeroed here), scaled by weight (ions: Qs). No fold, no wall factors. */
 void oracle_deposit(const oracle_geom_t* g, const oracle_parts_t* p, double weight, double* rho);
@@ -73,6 +79,28 @@ void oracle_collect_moments(const oracle_geom_t* g, const oracle_species_t* sp, 
 void   oracle_maxwell_tables(double* v, double* v_inj);
 /* GetMaxwellVelocity (:961-985) driven by one uniform variate */
 double oracle_maxwell_sample(const double* v, double u);
+
+/* ---------------------------------------------------------------- ion-induced electron emission */
+/* one ion species at the four domain walls (0 below, 1 above, 2 left, 3 right), in code units
+ * (pic2d_Materials.f90:165-188): yield between emin and emax (energies Ms v^2), fconv = sqrt(T_emit/T_e)/N_max_vel */
+typedef struct {
+    int32_t on[4];
+    double yield[4], emin[4], emax[4], fconv[4];
+    double ms;
+    uint32_t species;            /* 0-based ion species */
+    const double* maxwell_v;     /* v[0..9000] */
+    const double* maxwell_inj;   /* v_inj[0..4500] */
+} oracle_emit_t;
+/* PROCESS_ION_INDUCED_ELECTRON_EMISSION and INJECT_ION_IMPACT_EXTRACTED_ELECTRON (pic2d_IonEmissions.f90:1-348)
+ * for an ion absorbed by `wall` at (x, y) (PROCESS_ION_COLL_WITH_BOUNDARY_*, pic2d_IonWallCollisions.f90:63-303,
+ * clamps the coordinate along the wall into [0, xmax] x [0, ymax] first; done here) with velocity v. Writes the
+ * emitted electrons as rows {x, y, vx, vy, vz} (room for cap rows) and returns their number. Variates:
+ * Philox4x32-10, key {id, seed_lo}, counter {step, 0x45450000 + species, block, seed_hi}; block 0 word 0 draws
+ * the fractional part of the yield, block 1 + e words 0, 1, 2 the normal speed of electron e (GetInjMaxwellVelocity)
+ * and its two tangential components (GetMaxwellVelocity) in x, y, z order. */
+int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, double y, double vx, double vy,
+                            double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
+                            double* out, int32_t cap);
 
 /* ---------------------------------------------------------------- electron-neutral collisions */
 typedef struct {

@@ -73,6 +73,12 @@ class Cycle(C.Structure):
 _lib = None
 
 
+class Emit(C.Structure):
+    _fields_ = [("on", C.c_int32 * 4), ("yld", C.c_double * 4), ("emin", C.c_double * 4),
+                ("emax", C.c_double * 4), ("fconv", C.c_double * 4), ("ms", C.c_double), ("species", C.c_uint32),
+                ("maxwell_v", _D), ("maxwell_inj", _D)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -86,6 +92,11 @@ def lib():
             "oracle_philox2x32_10": ([_U32, C.c_uint32, _U32], None),
             "oracle_nx_nodes": ([C.POINTER(Geom)], C.c_int32),
             "oracle_push": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64], None),
+            "oracle_push_hits": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64, _D,
+                                  C.c_int64, _I64], None),
+            "oracle_ion_emission": ([C.POINTER(Emit), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, C.c_double, C.c_double, _D,
+                                     C.c_int32], C.c_int32),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
             "oracle_fold_and_wall_scale": ([C.POINTER(Geom), _D], None),
             "oracle_collect_moments": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _D], None),
@@ -187,6 +198,43 @@ def push(g, sp, ex, ey, parts):
     lib().oracle_push(C.byref(g), C.byref(sp), dp(np.ascontiguousarray(ex)), dp(np.ascontiguousarray(ey)),
                       C.byref(parts.s), hits.ctypes.data_as(_I64))
     return hits
+
+
+def push_hits(g, sp, ex, ey, parts, cap=1 << 20):
+    """oracle_push plus the wall-hit rows {wall, X, Y, vx, vy, vz, id} of every domain-wall absorption."""
+    hits = np.zeros(8, dtype=np.int64)
+    rows = np.zeros((cap, 7))
+    n = C.c_int64(0)
+    lib().oracle_push_hits(C.byref(g), C.byref(sp), dp(np.ascontiguousarray(ex)), dp(np.ascontiguousarray(ey)),
+                           C.byref(parts.s), hits.ctypes.data_as(_I64), dp(rows), cap, C.byref(n))
+    assert n.value <= cap
+    return hits, rows[:n.value].copy()
+
+
+class IonEmission:
+    """Ion-induced electron emission of one ion species at the four walls (oracle_ion_emission). Energies in eV are
+    converted with energy_factor_ev (0.5 m_e V_scale^2 / e); t_emit in eV the same way."""
+
+    def __init__(self, walls, ms, energy_factor_ev, species=0):
+        self.v, self.vi = maxwell_tables()
+        self.s = Emit()
+        for w, (yld, e0, e1, t) in walls.items():
+            self.s.on[w] = 1 if yld > 0 else 0
+            self.s.yld[w] = yld
+            self.s.emin[w] = e0 / energy_factor_ev
+            self.s.emax[w] = e1 / energy_factor_ev
+            self.s.fconv[w] = np.sqrt(t / energy_factor_ev)
+        self.s.ms = ms
+        self.s.species = species
+        self.s.maxwell_v = dp(self.v)
+        self.s.maxwell_inj = dp(self.vi)
+
+    def emit(self, wall, x, y, vx, vy, vz, ident, seed, step, xmax, ymax, cap=64):
+        out = np.zeros((cap, 5))
+        n = lib().oracle_ion_emission(C.byref(self.s), int(wall), x, y, vx, vy, vz, int(ident), seed, step, xmax,
+                                      ymax, dp(out), cap)
+        assert n <= cap
+        return out[:n]
 
 
 def deposit(g, parts, weight=1.0, fold=True):

@@ -97,3 +97,30 @@ def test_reference_example_decks_parse_or_are_rejected_cleanly():
             pr = np.ctypeslib.as_array(dk.tables.prob, shape=((nv + 1) * dk.tables.n_act,))
             assert np.array_equal(pr, ot.prob), name
     assert seen == 11
+
+
+def test_wall_material_ion_emission(tmp_path):
+    """init_material_<NAME>.dat of the walls: ion-material model 2 gives the ion-induced emission parameters per
+    wall and ion species (pic2d_Materials.f90:150-188); model 0 gives none."""
+    d = read_deck(decks.write_deck(str(tmp_path / "a"), "cfg4", ncx=64, ncy=32, ppc=4))
+    assert d.ion_emission == {(0, 1): (0.1, 0.0, 10000.0, 2.0), (1, 1): (0.1, 0.0, 10000.0, 2.0)}
+    d = read_deck(decks.write_deck(str(tmp_path / "b"), "cfg2", ncx=64, ncy=32, ppc=4,
+                                   ion_emission=(1.25, 5.0, 500.0, 1.5)))
+    assert d.ion_emission == {(w, 1): (1.25, 5.0, 500.0, 1.5) for w in range(4)}
+    d = read_deck(decks.write_deck(str(tmp_path / "c"), "cfg0", ncx=64, ncy=32, ppc=4))
+    assert d.ion_emission == {}
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference example decks not present")
+def test_reference_ion_emission_deck():
+    """The reference's periodic ion-induced emission example: both walls' material file read as text here must give
+    the reader's values."""
+    d = os.path.join(REFERENCE, "input_data_dc_periodic_ion_induced_EE")
+    lines = open(os.path.join(d, "init_material_METAL2.dat")).read().splitlines()
+    k = next(i for i, L in enumerate(lines) if "ION-MATERIAL INTERACTION MODEL" in L)
+    assert int(lines[k + 1][7:8]) == 2
+    want = (float(lines[k + 4][7:12]), float(lines[k + 6][2:12]), float(lines[k + 8][2:12]),
+            float(lines[k + 10][2:12]))
+    got = read_deck(d).ion_emission
+    assert got == {(0, 1): want, (1, 1): want}
+    assert want == (0.2, 100.0, 10000.0, 2.0)

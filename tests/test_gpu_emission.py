@@ -1,0 +1,110 @@
+"""Ion-induced electron emission (PROCESS_ION_INDUCED_ELECTRON_EMISSION, pic2d_IonEmissions.f90:1-348) on the
+device against the oracle: ions launched into the walls, one ion push, the electrons emitted by each absorbed ion
+(count per wall, positions 1e-6 inside the wall, velocities from the injection and Maxwell tables scaled to the
+emission temperature and to the ion's energy budget), appended to the electrons at the end of the step."""
+import numpy as np
+import pytest
+
+import pyoracle
+from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation
+from gpu_common import oracle_geom, small_deck
+
+
+def wall_ions(sim, n, seed, precision):
+    """Ions within one step of a wall, moving into it (bottom/top; left/right too on the walled domain)."""
+    p = sim.params
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, p.ncx, n)
+    y = rng.uniform(0.0, p.ncy, n)
+    v = rng.normal(0.0, 0.001, (3, n))
+    out = 0.0005 + np.abs(rng.normal(0.0, 0.0015, n))
+    side = rng.integers(0, 2 if sim.periodic else 4, n)
+    d = rng.uniform(0.0, 0.003, n)
+    lo, hi = side == 0, side == 1
+    y[lo], v[1][lo] = d[lo], -out[lo]
+    y[hi], v[1][hi] = p.ncy - 1e-4 - d[hi], out[hi]
+    if not sim.periodic:
+        le, ri = side == 2, side == 3
+        x[le], v[0][le] = d[le], -out[le]
+        x[ri], v[0][ri] = p.ncx - 1e-4 - d[ri], out[ri]
+    if precision == PREC_MIXED:
+        i, j = np.floor(x), np.floor(y)
+        x = i + (x - i).astype(np.float32).astype(np.float64)
+        y = j + (y - j).astype(np.float32).astype(np.float64)
+        v = v.astype(np.float32).astype(np.float64)
+    return x, y, v[0], v[1], v[2]
+
+
+def pair_rows(a, b, scale):
+    """Nearest-neighbour pairing of the rows of a and b (same count, columns divided by scale); the pairing must be
+    one to one. Returns the largest distance (max norm) of a pair."""
+    from scipy.spatial import cKDTree
+
+    assert a.shape == b.shape, (a.shape, b.shape)
+    if a.size == 0:
+        return 0.0
+    d, j = cKDTree(b / scale).query(a / scale, p=np.inf)
+    assert np.unique(j).size == j.size, "rows do not pair one to one"
+    return float(d.max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,sort_every", [(PREC_MIXED, 0), (PREC_MIXED, 4), (PREC_FP64, 0)])
+@pytest.mark.parametrize("geometry", ["periodic", "walled"])
+def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry):
+    kw = {"inner": False} if geometry == "walled" else {}
+    d = small_deck(tmp_path, geometry, ion_emission=False, **kw)
+    with Simulation(d, precision=precision, sort_every=sort_every, fuse_collisions=False) as sim:
+        p = sim.params
+        ef = sim.deck.tables.energy_factor_eV
+        ms = p.ion_mass_me[0]
+        n = 8000
+        x, y, vx, vy, vz = wall_ions(sim, n, seed=5, precision=precision)
+        e_ev = ms * (vx * vx + vy * vy + vz * vz) * ef
+        e0, e1 = np.percentile(e_ev, 15), np.percentile(e_ev, 85)
+        walls = {w: (2.3 if w % 2 == 0 else 0.6, e0, e1, 20.0) for w in range(2 if sim.periodic else 4)}
+        for w, (yld, a, b, t) in walls.items():
+            sim.set_ion_emission(w, 1, yld, a, b, t)
+        ne = 16
+        sim.upload_particles(ELECTRONS, x[:ne], y[:ne], 0 * vx[:ne], 0 * vy[:ne], 0 * vz[:ne],
+                             ids=np.arange(ne, dtype=np.uint32) + 500000)
+        ids = np.arange(n, dtype=np.uint32) * 5 + 3
+        sim.upload_particles(IONS, x, y, vx, vy, vz, ids=ids)
+        step = sim.counters().step
+        sim.advance_ions()
+        emitted = sim.emission_counts()
+        c = sim.counters()
+        sim.end_ion_cycle()
+        el = sim.download_particles(ELECTRONS)
+
+    new = el["id"] >= 0
+    new &= ~np.isin(el["id"], np.arange(ne, dtype=np.uint32) + 500000)
+    got = np.stack([el[k][new] for k in ("x", "y", "vx", "vy", "vz")], axis=1)
+
+    g = oracle_geom(sim)
+    sp = pyoracle.Species(p.bx, p.by, p.bz, p.ez, 1, 0.5 * p.ion_charge[0] / p.ion_mass_me[0], p.n_subcycles,
+                          p.ions_sense_b, p.ions_sense_ez)
+    ps = pyoracle.ParticleSet(x, y, vx, vy, vz, ids=ids)
+    zero = np.zeros((sim.ny_ref, sim.nx_ref))
+    hits, rows = pyoracle.push_hits(g, sp, zero, zero, ps)
+    em = pyoracle.IonEmission(walls, ms, ef)
+    ref, per_wall = [], np.zeros(8, np.int64)
+    for r in rows:
+        out = em.emit(int(r[0]), r[1], r[2], r[3], r[4], r[5], int(r[6]), p.seed, step, float(p.ncx), float(p.ncy))
+        per_wall[int(r[0])] += len(out)
+        ref.append(out)
+    ref = np.concatenate(ref) if ref else np.zeros((0, 5))
+
+    assert np.array_equal(np.array(c.ion_hits[:8]), hits), (list(c.ion_hits[:8]), hits)
+    assert np.array_equal(emitted, per_wall), (emitted, per_wall)
+    assert per_wall.sum() > 500
+    assert got.shape == ref.shape
+    vscale = np.abs(ref[:, 2:]).max()
+    scale = np.array([1.0, 1.0, vscale, vscale, vscale])
+    tol = 2e-6 if precision == PREC_MIXED else 1e-12
+    assert pair_rows(ref, got, scale) <= tol
+    # the electrons start 1e-6 inside the wall they came from
+    on_wall = (np.abs(ref[:, 1] - 1e-6) < 1e-9) | (np.abs(ref[:, 1] - (p.ncy - 1e-6)) < 1e-9)
+    if not sim.periodic:
+        on_wall |= (np.abs(ref[:, 0] - 1e-6) < 1e-9) | (np.abs(ref[:, 0] - (p.ncx - 1e-6)) < 1e-9)
+    assert on_wall.all()
