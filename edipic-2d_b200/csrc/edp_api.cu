@@ -921,12 +921,10 @@ static std::vector<double> injection_maxwell_table(int rmax)
     return v;
 }
 
-int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double yield, double emin_ev, double emax_ev,
-                         double t_emit_ev)
+// device state of the ion-wall interactions, made on first use: the wall-hit list, the injection table and the
+// parameter block
+static int wall_state(edp_ctx* c)
 {
-    if (!c || wall < 0 || wall > 3 || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
-        !(emax_ev > emin_ev) || !(t_emit_ev >= 0.0))
-        return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_emission");
     if (!c->emit_h) {
         const int rmax_inj = 4500;
         std::vector<double> v = injection_maxwell_table(rmax_inj);
@@ -949,6 +947,29 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
         c->emit_h->maxwell_inj = c->maxwell_inj;
         c->emit_h->rmax_inj = rmax_inj;
     }
+    return EDP_OK;
+}
+
+static int upload_wall_state(edp_ctx* c)
+{
+    const edp_emit_dev& h = *c->emit_h;
+    c->emit_on = 0;
+    for (int w = 0; w < 4; ++w) {
+        c->emit_on |= h.reflect[w];
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) c->emit_on |= h.on[w][q];
+    }
+    EDP_CUDA(c, cudaMemcpyAsync(c->emit_dev, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
+int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double yield, double emin_ev, double emax_ev,
+                         double t_emit_ev)
+{
+    if (!c || wall < 0 || wall > 3 || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
+        !(emax_ev > emin_ev) || !(t_emit_ev >= 0.0))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_emission");
+    TRY(wall_state(c));
     edp_emit_dev& h = *c->emit_h;
     const int s = ion_species - 1;
     const double ef = c->tab.energy_factor_eV;
@@ -958,12 +979,15 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
     h.emax[wall][s] = emax_ev / ef;
     h.fconv[wall][s] = std::sqrt(t_emit_ev / ef);
     h.ms[s] = c->p.ion_mass_me[s];
-    c->emit_on = 0;
-    for (int w = 0; w < 4; ++w)
-        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) c->emit_on |= h.on[w][q];
-    EDP_CUDA(c, cudaMemcpyAsync(c->emit_dev, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
-    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
-    return EDP_OK;
+    return upload_wall_state(c);
+}
+
+int edp_set_ion_reflection(edp_ctx* c, int32_t wall, int32_t on)
+{
+    if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
+    TRY(wall_state(c));
+    c->emit_h->reflect[wall] = on ? 1 : 0;
+    return upload_wall_state(c);
 }
 
 int edp_field_cg(edp_ctx* c, double rtol, int32_t max_it, int32_t warm, int32_t* iters_out)

@@ -167,7 +167,7 @@ struct edp_ctx {
     edp_emit_dev* emit_dev = nullptr; // ion-induced electron emission (device copy of emit_h)
     edp_emit_dev* emit_h = nullptr;   // host copy
     edp_hits hits;                    // ion wall hits of the current ion step
-    int emit_on = 0;
+    int emit_on = 0;                  // wall hits are recorded: some wall emits or reflects
     double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
     int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     int32_t last_cg_iters = 0;
@@ -541,6 +541,7 @@ int edp_launch_deposit(edp_ctx* c, int species);   // CIC deposit of the whole a
 // (an ion's energy is Ms v^2, an electron's v^2), and the velocity factor sqrt(T_emit / energy_factor_eV) of the
 // emitted electrons (= sqrt(T_emit / T_e) / N_max_vel, :188).
 struct edp_emit_dev {
+    int reflect[4];            // ion-material model 1: the wall reflects every ion specularly
     int on[4][EDP_MAX_ION_SPECIES];
     double yield[4][EDP_MAX_ION_SPECIES];
     double emin[4][EDP_MAX_ION_SPECIES], emax[4][EDP_MAX_ION_SPECIES];

@@ -972,9 +972,11 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
     return EDP_OK;
 }
 
-// PROCESS_ION_INDUCED_ELECTRON_EMISSION for every recorded wall hit of this ion step. PROCESS_ION_COLL_WITH_BOUNDARY_*
-// (pic2d_IonWallCollisions.f90:63-303) first clamps the coordinate along the wall into the domain.
-__global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp_emit_dev* em, edp_born born_e,
+// The wall interaction of every recorded ion hit of this ion step (PROCESS_ION_COLL_WITH_BOUNDARY_*,
+// pic2d_IonWallCollisions.f90:3-303, which first clamps the coordinate along the wall into the domain): a reflecting
+// wall returns the ion specularly, 1e-6 inside the wall, through the ion add list (INJECT_REFLECTED_ION,
+// pic2d_IonEmissions.f90:374-492); otherwise PROCESS_ION_INDUCED_ELECTRON_EMISSION.
+__global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp_emit_dev* em, edp_born_dev* born,
                                                            edp_dev_counters* dc, edp_kparams kp, uint32_t step)
 {
     const int64_t n = min((int64_t)dc->hit_count, h.cap);
@@ -982,6 +984,19 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int ws = h.ws[k], wall = ws & 255, s = ws >> 8;
         const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
+        if (em->reflect[wall]) {
+            double v[3] = {h.vx[k], h.vy[k], h.vz[k]};
+            double nx = x, ny = y;
+            switch (wall) {
+            case 0: ny = 1.0e-6; v[1] = -v[1]; break;
+            case 1: ny = ymax - 1.0e-6; v[1] = -v[1]; break;
+            case 2: nx = 1.0e-6; v[0] = -v[0]; break;
+            default: nx = xmax - 1.0e-6; v[0] = -v[0]; break;
+            }
+            record_born(born->born_i[s], &dc->born_i_count[s], &dc->error_flags, nx, ny, v);
+            continue;
+        }
+        const edp_born born_e = born->born_e;
         const int m = edp_emit_electrons(em, s, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
                                          kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
                                              record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
@@ -993,7 +1008,7 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
 int edp_launch_ion_emission(edp_ctx* c)
 {
     ++c->launches;
-    ion_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->emit_dev, c->born_e, c->dc, c->kp,
+    ion_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->emit_dev, c->born_dev, c->dc, c->kp,
                                                       (uint32_t)c->t_cntr);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));

@@ -65,8 +65,12 @@ class Deck:
         self.n_max_vel, self.n_plasma_m3, self.max_t_cntr = nmv.value, npl.value, maxt.value
         # ion-induced electron emission of the walls' materials: {(wall, ion species): (yield, E_min, E_max, T)}
         self.ion_emission = {}
+        self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission
         buf = (C.c_double * 4)()
+        model = C.c_int32()
         for wall in range(4):
+            if self.lib.edp_deck_ion_wall_model(self.handle, wall, C.byref(model)) == 0:
+                self.ion_wall_model[wall] = model.value
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(wall, s)] = tuple(buf)
@@ -113,6 +117,9 @@ class Simulation:
         self.ny_ref = p.ncy + 1
         for (wall, s), (yld, e0, e1, t) in self.deck.ion_emission.items():
             self.set_ion_emission(wall, s, yld, e0, e1, t)
+        for wall, model in enumerate(self.deck.ion_wall_model):
+            if model == 1:
+                self.set_ion_reflection(wall, True)
 
     # ------------------------------------------------------------------------------------ plumbing
     def _check(self, rc, where):
@@ -234,6 +241,11 @@ class Simulation:
         (1-based): PROCESS_ION_INDUCED_ELECTRON_EMISSION (pic2d_IonEmissions.f90:1-348). yield_ 0 turns it off."""
         self._check(self.lib.edp_set_ion_emission(self.ctx, wall, ion_species, yield_, emin_ev, emax_ev, t_emit_ev),
                     "edp_set_ion_emission")
+
+    def set_ion_reflection(self, wall, on=True):
+        """Ion-material model 1: the wall reflects every ion specularly (INJECT_REFLECTED_ION,
+        pic2d_IonEmissions.f90:374-492)."""
+        self._check(self.lib.edp_set_ion_reflection(self.ctx, wall, 1 if on else 0), "edp_set_ion_reflection")
 
     def emission_counts(self):
         """Electrons emitted by ion impacts on each object (walls 0-3, then inner objects), cumulative."""

@@ -100,6 +100,7 @@ SIGNATURES = {
     "edp_set_cg_preconditioner": [_CTX, C.c_int32],
     "edp_set_ion_emission": [_CTX, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double],
     "edp_query_emission": [_CTX, _I64],
+    "edp_set_ion_reflection": [_CTX, C.c_int32, C.c_int32],
     "edp_advance_electrons": [_CTX],
     "edp_advance_ions": [_CTX],
     "edp_collide_en": [_CTX, _I64],
@@ -139,6 +140,7 @@ SIGNATURES = {
     "edp_deck_read": [C.c_char_p, P(C.c_void_p), P(Params), P(Tables)],
     "edp_deck_initial_plasma": [C.c_void_p, _D, _D, _D, _D, _I32, _D, _I64],
     "edp_deck_ion_emission": [C.c_void_p, C.c_int32, C.c_int32, _D],
+    "edp_deck_ion_wall_model": [C.c_void_p, C.c_int32, _I32],
     "edp_deck_free": [C.c_void_p],
 }
 

@@ -57,9 +57,10 @@ def _segments():
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
-               ion_emission=None):
+               ion_emission=None, ion_reflection=False):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
-    (the wall material METAL1), False for none, None for the configuration's default."""
+    (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
+    reflect all ions specularly instead (ion-material model 1)."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -195,8 +196,10 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         "------dd.ddd- maximum", f"      {0.0:6.3f}",
         "-------d.ddd- smoothness", f"       {0.0:5.3f}",
         "=======d===== ION-MATERIAL INTERACTION MODEL (0 absorb, 1 reflect, 2 ion-induced electron emission)",
-        f"       {2 if iee else 0:1d}",
+        f"       {1 if ion_reflection else (2 if iee else 0):1d}",
     ]
+    if ion_reflection:
+        iee = None
     if iee:
         yld, e0, e1, t = iee
         for s in range(1):   # one ion species (Ar+)

@@ -5,6 +5,7 @@
 // Supported deck subset: one cluster covering the domain (any block count), boundary objects that are metal
 // walls (type 1) or periodic pipes (type 2) on the four sides, metal rectangular inner objects, uniform external
 // B and Ez, one neutral species with e-n processes of types 10/11/20/30 and resonant charge exchange.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -115,6 +116,7 @@ struct edp_deck {
     int64_t max_t_cntr = 0;
     // ion-induced electron emission of the four walls per ion species: yield, E_min [eV], E_max [eV], T [eV]
     double ii_ee[4][EDP_MAX_ION_SPECIES][4] = {};
+    int32_t ion_model[4] = {};   // ion-material interaction model of each wall's material
 };
 
 namespace {
@@ -301,6 +303,8 @@ int read_deck(const std::string& dir, edp_deck* d)
             }
         long long flag = 0;
         if (!found || !mf.next(L) || !fint(L, 7, 1, &flag)) continue;
+        flag = std::max(0LL, std::min(flag, 2LL));   // MAX(0, MIN(flag, 2)), :153
+        d->ion_model[w] = (int32_t)flag;
         if (flag != 2) continue;
         for (int s = 0; s < (int)p.n_ion_species; ++s) {
             double yv = 0, e0 = 0, e1 = 0, te = 0;
@@ -519,6 +523,13 @@ int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, 
 {
     if (!d || !out || wall < 0 || wall > 3 || ion_species < 1 || ion_species > EDP_MAX_ION_SPECIES) return EDP_ERR_ARG;
     for (int k = 0; k < 4; ++k) out[k] = d->ii_ee[wall][ion_species - 1][k];
+    return EDP_OK;
+}
+
+int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model)
+{
+    if (!d || !model || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    *model = d->ion_model[wall];
     return EDP_OK;
 }
 

@@ -195,6 +195,11 @@ int edp_set_cg_preconditioner(edp_ctx* ctx, int32_t kind);
  * step (edp_end_ion_cycle) and are counted per wall (edp_query_emission). yield 0 switches the wall off. */
 int edp_set_ion_emission(edp_ctx* ctx, int32_t wall, int32_t ion_species, double yield, double emin_ev,
                          double emax_ev, double t_emit_ev);
+/* Ion-material model 1 (pic2d_Materials.f90:159-161): wall (0 below, 1 above, 2 left, 3 right) reflects every ion
+ * specularly (INJECT_REFLECTED_ION, pic2d_IonEmissions.f90:374-492). The hit is counted, and the ion returns 1e-6
+ * inside the wall with the normal velocity reversed, through the ion add list at the end of the step. Reflection
+ * takes precedence over emission on the same wall. on = 0 restores absorption. */
+int edp_set_ion_reflection(edp_ctx* ctx, int32_t wall, int32_t on);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
  * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
 int edp_advance_electrons(edp_ctx* ctx);
@@ -307,6 +312,8 @@ int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_
  * wall's init_material_<NAME>.dat: out = {yield, E_min [eV], E_max [eV], T_emit [eV]}, all 0 when the wall's
  * material has no emission (pic2d_Materials.f90:150-188) */
 int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out);
+/* ion-material interaction model of wall's material (0 absorption, 1 specular reflection, 2 ion-induced emission) */
+int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
 int edp_deck_free(edp_deck* d);
 
 #ifdef __cplusplus

@@ -529,6 +529,19 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
     return n;
 }
 
+// INJECT_REFLECTED_ION pic2d_IonEmissions.f90:374-430 (m > 0, the domain walls)
+void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,
+                        double* out)
+{
+    x = std::min(std::max(x, 0.0), xmax);
+    y = std::min(std::max(y, 0.0), ymax);
+    out[0] = x; out[1] = y; out[2] = vx; out[3] = vy; out[4] = vz;
+    if (wall == 2) { out[0] = 1.0e-6; out[2] = -vx; }
+    else if (wall == 3) { out[0] = xmax - 1.0e-6; out[2] = -vx; }
+    else if (wall == 0) { out[1] = 1.0e-6; out[3] = -vy; }
+    else { out[1] = ymax - 1.0e-6; out[3] = -vy; }
+}
+
 // --------------------------------------------------------------------------- e-n collision table
 // frequency_of_en_collision pic2d_enCollisionsSpecificProc.f90:4-57
 double oracle_en_frequency(const oracle_crsect_t* cs, double energy_eV, double n_m3, int32_t nsub, double dt_s)

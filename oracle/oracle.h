@@ -102,6 +102,11 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
                             double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
                             double* out, int32_t cap);
 
+/* INJECT_REFLECTED_ION (pic2d_IonEmissions.f90:374-492) for a domain wall: the ion returns 1e-6 inside the wall
+ * (coordinate along the wall clamped into the domain) with its normal velocity reversed; out = {x, y, vx, vy, vz} */
+void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,
+                        double* out);
+
 /* ---------------------------------------------------------------- electron-neutral collisions */
 typedef struct {
     int32_t n_points;

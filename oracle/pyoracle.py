@@ -97,6 +97,8 @@ def lib():
             "oracle_ion_emission": ([C.POINTER(Emit), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, C.c_double, C.c_double, _D,
                                      C.c_int32], C.c_int32),
+            "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, _D], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
             "oracle_fold_and_wall_scale": ([C.POINTER(Geom), _D], None),
             "oracle_collect_moments": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _D], None),
@@ -235,6 +237,12 @@ class IonEmission:
                                       ymax, dp(out), cap)
         assert n <= cap
         return out[:n]
+
+
+def ion_reflect(wall, x, y, vx, vy, vz, xmax, ymax):
+    out = np.zeros(5)
+    lib().oracle_ion_reflect(int(wall), x, y, vx, vy, vz, xmax, ymax, dp(out))
+    return out
 
 
 def deposit(g, parts, weight=1.0, fold=True):

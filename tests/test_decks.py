@@ -124,3 +124,11 @@ def test_reference_ion_emission_deck():
     got = read_deck(d).ion_emission
     assert got == {(0, 1): want, (1, 1): want}
     assert want == (0.2, 100.0, 10000.0, 2.0)
+
+
+def test_wall_material_ion_reflection(tmp_path):
+    d = read_deck(decks.write_deck(str(tmp_path / "r"), "cfg2", ncx=64, ncy=32, ppc=4, ion_reflection=True))
+    assert d.ion_wall_model == [1, 1, 1, 1]
+    assert d.ion_emission == {}
+    d = read_deck(decks.write_deck(str(tmp_path / "e"), "cfg4", ncx=64, ncy=32, ppc=4))
+    assert d.ion_wall_model == [2, 2, 0, 0]

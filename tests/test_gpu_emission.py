@@ -1,7 +1,10 @@
-"""Ion-induced electron emission (PROCESS_ION_INDUCED_ELECTRON_EMISSION, pic2d_IonEmissions.f90:1-348) on the
-device against the oracle: ions launched into the walls, one ion push, the electrons emitted by each absorbed ion
-(count per wall, positions 1e-6 inside the wall, velocities from the injection and Maxwell tables scaled to the
-emission temperature and to the ion's energy budget), appended to the electrons at the end of the step."""
+"""Ion-wall interactions on the device against the oracle: ions launched into the walls, one ion push, then
+* ion-induced electron emission (PROCESS_ION_INDUCED_ELECTRON_EMISSION, pic2d_IonEmissions.f90:1-348): the electrons
+  emitted by each absorbed ion (count per wall, positions 1e-6 inside the wall, velocities from the injection and
+  Maxwell tables scaled to the emission temperature and to the ion's energy budget), appended to the electrons at
+  the end of the step;
+* specular reflection (INJECT_REFLECTED_ION, :374-492) on the walls with ion-material model 1: the reflected ions
+  appended to the ions at the end of the step."""
 import numpy as np
 import pytest
 
@@ -51,7 +54,8 @@ def pair_rows(a, b, scale):
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision,sort_every", [(PREC_MIXED, 0), (PREC_MIXED, 4), (PREC_FP64, 0)])
 @pytest.mark.parametrize("geometry", ["periodic", "walled"])
-def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry):
+@pytest.mark.parametrize("reflect", [False, True])
+def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry, reflect):
     kw = {"inner": False} if geometry == "walled" else {}
     d = small_deck(tmp_path, geometry, ion_emission=False, **kw)
     with Simulation(d, precision=precision, sort_every=sort_every, fuse_collisions=False) as sim:
@@ -65,6 +69,10 @@ def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry):
         walls = {w: (2.3 if w % 2 == 0 else 0.6, e0, e1, 20.0) for w in range(2 if sim.periodic else 4)}
         for w, (yld, a, b, t) in walls.items():
             sim.set_ion_emission(w, 1, yld, a, b, t)
+        # with reflection: the walls below and on the left reflect (and keep their emission parameters unused)
+        reflecting = {0, 2} if reflect else set()
+        for w in reflecting:
+            sim.set_ion_reflection(w, True)
         ne = 16
         sim.upload_particles(ELECTRONS, x[:ne], y[:ne], 0 * vx[:ne], 0 * vy[:ne], 0 * vz[:ne],
                              ids=np.arange(ne, dtype=np.uint32) + 500000)
@@ -76,6 +84,7 @@ def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry):
         c = sim.counters()
         sim.end_ion_cycle()
         el = sim.download_particles(ELECTRONS)
+        io = sim.download_particles(IONS)
 
     new = el["id"] >= 0
     new &= ~np.isin(el["id"], np.arange(ne, dtype=np.uint32) + 500000)
@@ -88,14 +97,26 @@ def test_ion_emission_matches_oracle(tmp_path, precision, sort_every, geometry):
     zero = np.zeros((sim.ny_ref, sim.nx_ref))
     hits, rows = pyoracle.push_hits(g, sp, zero, zero, ps)
     em = pyoracle.IonEmission(walls, ms, ef)
-    ref, per_wall = [], np.zeros(8, np.int64)
+    ref, per_wall, refl = [], np.zeros(8, np.int64), []
     for r in rows:
+        if int(r[0]) in reflecting:
+            refl.append(pyoracle.ion_reflect(int(r[0]), r[1], r[2], r[3], r[4], r[5], float(p.ncx), float(p.ncy)))
+            continue
         out = em.emit(int(r[0]), r[1], r[2], r[3], r[4], r[5], int(r[6]), p.seed, step, float(p.ncx), float(p.ncy))
         per_wall[int(r[0])] += len(out)
         ref.append(out)
     ref = np.concatenate(ref) if ref else np.zeros((0, 5))
 
     assert np.array_equal(np.array(c.ion_hits[:8]), hits), (list(c.ion_hits[:8]), hits)
+    # reflected ions: the ions that are not original
+    back = ~np.isin(io["id"], ids)
+    got_i = np.stack([io[k][back] for k in ("x", "y", "vx", "vy", "vz")], axis=1)
+    ref_i = np.array(refl).reshape(-1, 5)
+    assert (len(ref_i) > 300) == reflect
+    assert got_i.shape == ref_i.shape
+    if reflect:
+        vs = np.abs(ref_i[:, 2:]).max()
+        assert pair_rows(ref_i, got_i, np.array([1.0, 1.0, vs, vs, vs])) <= (2e-6 if precision == PREC_MIXED else 1e-12)
     assert np.array_equal(emitted, per_wall), (emitted, per_wall)
     assert per_wall.sum() > 500
     assert got.shape == ref.shape
