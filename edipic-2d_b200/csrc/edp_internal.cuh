@@ -57,7 +57,7 @@ struct edp_dev_counters {
 };
 
 struct edp_species_mixed {
-    int32_t* cell = nullptr;   // linear cell j*ncx + i, -1 dead
+    int32_t* cell = nullptr;   // cell (j << 16) | i, -1 dead
     float *ox = nullptr, *oy = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     uint32_t* id = nullptr;
     int32_t* tag = nullptr;

@@ -1,0 +1,171 @@
+// Velocity distribution functions: CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393)
+// on the particles in HBM, for one cluster over the whole domain.
+//
+// The domain is split into nbx x nby boxes at X = i * ncx / nbx, Y = j * ncy / nby (xsplit/ysplit, :63-75). Each
+// velocity component is binned as INT(v * fvc), one less for v < 0 (:99-117), with fvc = N_max_vel * N_vbins
+// (* sqrt(Ms) for ions, :74 of the ion routine), bins vmin = -N_max_vel_s * N_vbins .. vmax = -vmin - 1. A particle with
+// any component outside that range is skipped and counted (:101-118). Counts: 1D histograms of vx, vy, vz per box
+// and, when asked, the 2D vx-vy histogram per box (:122-136).
+//
+// One CTA keeps private copies of the histograms in shared memory when they fit (the 1D ones always do at the
+// reference's sizes) and adds them to the global counts once; otherwise it adds each count to global memory.
+#include <algorithm>
+
+#include "edp_internal.cuh"
+
+namespace {
+
+constexpr int kMaxBoxes = 16;   // per direction (the deck's i1 fields allow 9)
+
+struct VdfArgs {
+    int precision;
+    edp_species_mixed m;
+    edp_species_fp64 d;
+    const unsigned long long* n_slots;
+    int nbx, nby, nbox;
+    double xsplit[kMaxBoxes], ysplit[kMaxBoxes];
+    double fvc;
+    int vmin, vmax, reclen;
+    unsigned* h1;            // [3][nbox][reclen], global
+    unsigned* h2;            // [nbox][reclen (vy)][reclen (vx)], global, or null
+    int h1_shared, h2_shared;
+    unsigned long long* skipped;
+};
+
+// the bin of one velocity component, or INT_MIN when out of range (the reference's INT of a value beyond the
+// integer range is not defined; such values are far outside every bin range and count as skipped)
+__device__ __forceinline__ int vbin(double v, double fvc, int vmin, int vmax)
+{
+    const double t = v * fvc;
+    if (!(fabs(t) < 1073741824.0)) return INT_MIN;
+    int b = (int)t;
+    if (v < 0.0) b -= 1;
+    return (b < vmin || b > vmax) ? INT_MIN : b;
+}
+
+__global__ void __launch_bounds__(256) vdf_kernel(VdfArgs a)
+{
+    extern __shared__ unsigned sh[];
+    const int n1 = 3 * a.nbox * a.reclen;
+    const int64_t n2 = (int64_t)a.nbox * a.reclen * a.reclen;
+    unsigned* s1 = sh;
+    unsigned* s2 = sh + (a.h1_shared ? n1 : 0);
+    if (a.h1_shared)
+        for (int q = threadIdx.x; q < n1; q += blockDim.x) s1[q] = 0u;
+    if (a.h2 && a.h2_shared)
+        for (int64_t q = threadIdx.x; q < n2; q += blockDim.x) s2[q] = 0u;
+    __shared__ unsigned long long skip_cta;
+    if (threadIdx.x == 0) skip_cta = 0ull;
+    __syncthreads();
+    unsigned* h1 = a.h1_shared ? s1 : a.h1;
+    unsigned* h2 = a.h2 ? (a.h2_shared ? s2 : a.h2) : nullptr;
+    unsigned long long skip = 0ull;
+    const int64_t n = (int64_t)*a.n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double X, Y, vx, vy, vz;
+        if (a.precision == EDP_PREC_MIXED) {
+            const int cell = a.m.cell[k];
+            if (cell < 0) continue;
+            X = (double)(cell & 0xFFFF) + (double)a.m.ox[k];
+            Y = (double)(cell >> 16) + (double)a.m.oy[k];
+            vx = a.m.vx[k];
+            vy = a.m.vy[k];
+            vz = a.m.vz[k];
+        } else {
+            X = a.d.x[k];
+            if (X < -1.0e29) continue;
+            Y = a.d.y[k];
+            vx = a.d.vx[k];
+            vy = a.d.vy[k];
+            vz = a.d.vz[k];
+        }
+        int ib = a.nbx - 1;
+        for (int i = 0; i < a.nbx - 1; ++i)
+            if (X < a.xsplit[i]) { ib = i; break; }
+        int jb = a.nby - 1;
+        for (int j = 0; j < a.nby - 1; ++j)
+            if (Y < a.ysplit[j]) { jb = j; break; }
+        const int box = ib + jb * a.nbx;
+        const int bx = vbin(vx, a.fvc, a.vmin, a.vmax);
+        const int by = bx == INT_MIN ? INT_MIN : vbin(vy, a.fvc, a.vmin, a.vmax);
+        const int bz = by == INT_MIN ? INT_MIN : vbin(vz, a.fvc, a.vmin, a.vmax);
+        if (bz == INT_MIN) {
+            ++skip;
+            continue;
+        }
+        const int base = box * a.reclen - a.vmin;
+        atomicAdd(&h1[base + bx], 1u);
+        atomicAdd(&h1[a.nbox * a.reclen + base + by], 1u);
+        atomicAdd(&h1[2 * a.nbox * a.reclen + base + bz], 1u);
+        if (h2) atomicAdd(&h2[((int64_t)box * a.reclen + (by - a.vmin)) * a.reclen + (bx - a.vmin)], 1u);
+    }
+    if (skip) atomicAdd(&skip_cta, skip);
+    __syncthreads();
+    if (threadIdx.x == 0 && skip_cta) atomicAdd(a.skipped, skip_cta);
+    if (a.h1_shared)
+        for (int q = threadIdx.x; q < n1; q += blockDim.x)
+            if (s1[q]) atomicAdd(&a.h1[q], s1[q]);
+    if (a.h2 && a.h2_shared)
+        for (int64_t q = threadIdx.x; q < n2; q += blockDim.x)
+            if (s2[q]) atomicAdd(&a.h2[q], s2[q]);
+}
+
+}  // namespace
+
+extern "C" int edp_calculate_vdf(edp_ctx* c, int species, int32_t n_max_vel, int32_t nbox_x, int32_t nbox_y,
+                                 int32_t n_max_vel_s, int32_t n_vbins, int32_t* vdf1d, int32_t* vdf2d,
+                                 int64_t* skipped)
+{
+    if (!c || !vdf1d || species < 0 || species >= c->nspec || n_max_vel < 1 || nbox_x < 1 || nbox_y < 1 ||
+        nbox_x > kMaxBoxes || nbox_y > kMaxBoxes || n_max_vel_s < 1 || n_vbins < 1 ||
+        (int64_t)n_max_vel_s * n_vbins > (1 << 20))
+        return edp_fail(c, EDP_ERR_ARG, "edp_calculate_vdf");
+    if (!c->uploaded[species]) return edp_fail(c, EDP_ERR_STATE, "species not uploaded");
+    VdfArgs a;
+    memset(&a, 0, sizeof(a));
+    a.precision = c->p.precision;
+    a.m = c->pm[species];
+    a.d = c->pd[species];
+    a.n_slots = &c->dc->n_slots[species];
+    a.nbx = nbox_x;
+    a.nby = nbox_y;
+    a.nbox = nbox_x * nbox_y;
+    // xsplit(i) = c_X_area_min + DBLE(i) * (c_X_area_max - c_X_area_min) / N_vdfbox_x (:65-67), one cluster
+    for (int i = 1; i < nbox_x; ++i) a.xsplit[i - 1] = 0.0 + (double)i * (double)c->p.ncx / nbox_x;
+    for (int j = 1; j < nbox_y; ++j) a.ysplit[j - 1] = 0.0 + (double)j * (double)c->p.ncy / nbox_y;
+    a.fvc = (double)(n_max_vel * n_vbins);
+    if (species > 0) a.fvc *= std::sqrt(c->p.ion_mass_me[species - 1]);
+    a.vmin = -n_max_vel_s * n_vbins;
+    a.vmax = n_max_vel_s * n_vbins - 1;
+    a.reclen = 2 * n_max_vel_s * n_vbins;
+    const int64_t n1 = 3LL * a.nbox * a.reclen;
+    const int64_t n2 = vdf2d ? (int64_t)a.nbox * a.reclen * a.reclen : 0;
+    if (n2 > ((int64_t)1 << 31)) return edp_fail(c, EDP_ERR_ARG, "edp_calculate_vdf: 2D histogram too large");
+    const int64_t kSmem = 160 * 1024 / 4;   // private copies up to 160 KB per CTA
+    a.h1_shared = n1 <= kSmem;
+    a.h2_shared = vdf2d && a.h1_shared && n1 + n2 <= kSmem;
+    const size_t smem = 4 * (size_t)((a.h1_shared ? n1 : 0) + (a.h2_shared ? n2 : 0));
+    unsigned* buf = nullptr;
+    const size_t bytes = (size_t)(n1 + n2) * 4 + 16;
+    EDP_CUDA(c, cudaMallocAsync(&buf, bytes, c->stream));
+    EDP_CUDA(c, cudaMemsetAsync(buf, 0, bytes, c->stream));
+    a.h1 = buf;
+    a.h2 = vdf2d ? buf + n1 : nullptr;
+    a.skipped = reinterpret_cast<unsigned long long*>(buf + n1 + n2 + ((n1 + n2) & 1));
+    if (smem > 48 * 1024)
+        EDP_CUDA(c, cudaFuncSetAttribute(vdf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // about 64 particles per thread, so that the private copies are flushed rarely
+    const int64_t slots = c->host_slots[species];
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((slots + 256 * 64 - 1) / (256 * 64), 148 * 4));
+    ++c->launches;
+    vdf_kernel<<<(unsigned)grid, 256, smem, c->stream>>>(a);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemcpyAsync(vdf1d, a.h1, n1 * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (vdf2d) EDP_CUDA(c, cudaMemcpyAsync(vdf2d, a.h2, n2 * 4, cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long sk = 0;
+    EDP_CUDA(c, cudaMemcpyAsync(&sk, a.skipped, 8, cudaMemcpyDeviceToHost, c->stream));
+    EDP_CUDA(c, cudaFreeAsync(buf, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (skipped) *skipped = (int64_t)sk;
+    return EDP_OK;
+}

@@ -305,6 +305,22 @@ class Simulation:
                     "edp_collect_moments")
         return out
 
+    def calculate_vdf(self, species, nbox=(1, 1), n_max_vel_s=4, n_vbins=10, two_d=False, n_max_vel=None):
+        """CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393): returns
+        (vdf1d [3, nbox, 2 n_max_vel_s n_vbins] for vx, vy, vz; vdf2d [nbox, vy bin, vx bin] or None; skipped).
+        Box k = ibox + jbox * nbox[0]; bin b covers [b, b + 1) / n_vbins thermal velocities, b from
+        -n_max_vel_s n_vbins. n_max_vel defaults to the deck's velocity scale N_max_vel."""
+        nmv = self.deck.n_max_vel if n_max_vel is None else n_max_vel
+        nb = nbox[0] * nbox[1]
+        rl = 2 * n_max_vel_s * n_vbins
+        v1 = np.zeros((3, nb, rl), dtype=np.int32)
+        v2 = np.zeros((nb, rl, rl), dtype=np.int32) if two_d else None
+        sk = C.c_int64(0)
+        i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32)) if a is not None else None
+        self._check(self.lib.edp_calculate_vdf(self.ctx, species, nmv, nbox[0], nbox[1], n_max_vel_s, n_vbins, i32(v1),
+                                               i32(v2), C.byref(sk)), "edp_calculate_vdf")
+        return v1, v2, sk.value
+
     def mcc_choose(self, energy_ev, r):
         e = np.ascontiguousarray(energy_ev, dtype=np.float64)
         rr = np.ascontiguousarray(r, dtype=np.float64)

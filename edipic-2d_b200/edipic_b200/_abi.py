@@ -113,6 +113,7 @@ SIGNATURES = {
     "edp_moments": [_CTX, C.c_int, _D],
     "edp_mcc_choose": [_CTX, C.c_int64, _D, _D, _I32],
     "edp_collect_moments": [_CTX, C.c_int, P(C.c_float)],
+    "edp_calculate_vdf": [_CTX, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _I32, _I32, _I64],
     "edp_poisson_fftx_noalloc": [C.c_int32, C.c_int32, C.c_void_p, C.c_double, C.c_double, C.c_void_p,
                                  C.c_void_p],
     "edp_warmstart_load": [_CTX, P(C.c_float), C.c_int64],

@@ -233,6 +233,14 @@ int edp_moments(edp_ctx* ctx, int species, double out[7]);
  * in the reference layout, out[m][j][i], m = N, VX, VY, VZ, WX, WY, WZ, VXVY, VXVZ, VYVZ, QX, QY, QZ (cs_N ...
  * cs_QZ after normalisation and ADJUST_DENSITY_AT_WALL_BOUNDARIES). */
 int edp_collect_moments(edp_ctx* ctx, int species, float* out);
+/* CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393) for one species (0 electrons,
+ * s ions), one cluster over the domain: nbox_x x nbox_y boxes (N_vdfbox_x/y of init_snapshots.dat), bins of
+ * 1/n_vbins thermal velocities up to +-n_max_vel_s of them (N_vbins_e/i, N_max_vel_e/i); n_max_vel is the deck's
+ * velocity scale N_max_vel. vdf1d[3][nbox][2 n_max_vel_s n_vbins] = evxdf, evydf, evzdf (isvxdf.. for ions),
+ * box = ibox + jbox nbox_x; vdf2d[nbox][vy bin][vx bin] = evxvydf, or NULL to skip it. skipped receives the
+ * number of particles outside the bins (may be NULL). */
+int edp_calculate_vdf(edp_ctx* ctx, int species, int32_t n_max_vel, int32_t nbox_x, int32_t nbox_y,
+                      int32_t n_max_vel_s, int32_t n_vbins, int32_t* vdf1d, int32_t* vdf2d, int64_t* skipped);
 /* kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:447-485) evaluated on the device for given
  * (energy, r) pairs: kind_out[k] = indx_coll (n_act+1 = null collision) */
 int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const double* r, int32_t* kind_out);

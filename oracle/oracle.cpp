@@ -454,6 +454,51 @@ double oracle_maxwell_sample(const double* v, double u)
     return v[R_max];
 }
 
+// CALCULATE_ELECTRON_VDF pic2d_VelocityDistributions.f90:3-206 (and CALCULATE_ION_VDF :211-393, which differs only in
+// fvc and the per-species layout), the loop over particles of one cluster
+int64_t oracle_vdf(const oracle_parts_t* p, int32_t nbx, int32_t nby, double xmax, double ymax, double fvc,
+                   int32_t vmin, int32_t* h1, int32_t* h2)
+{
+    const int32_t vmax = -vmin - 1, reclen = -2 * vmin, nbox = nbx * nby;
+    std::fill(h1, h1 + 3 * (int64_t)nbox * reclen, 0);
+    if (h2) std::fill(h2, h2 + (int64_t)nbox * reclen * reclen, 0);
+    std::vector<double> xsplit(nbx), ysplit(nby);
+    for (int i = 1; i < nbx; ++i) xsplit[i] = 0.0 + (double)i * (xmax - 0.0) / nbx;
+    for (int j = 1; j < nby; ++j) ysplit[j] = 0.0 + (double)j * (ymax - 0.0) / nby;
+    // INT(v * fvc), one less for negative v; values beyond the integer range count as out of range
+    auto bin = [&](double v, bool* ok) {
+        double t = v * fvc;
+        if (!(std::fabs(t) < 1073741824.0)) { *ok = false; return 0; }
+        int b = (int)t;
+        if (v < 0.0) b -= 1;
+        *ok = b >= vmin && b <= vmax;
+        return b;
+    };
+    int64_t skip = 0;
+    for (int64_t k = 0; k < p->n; ++k) {
+        int ibox = nbx;
+        for (int i = 1; i <= nbx - 1; ++i)
+            if (p->x[k] < xsplit[i]) { ibox = i; break; }
+        int jbox = nby;
+        for (int j = 1; j <= nby - 1; ++j)
+            if (p->y[k] < ysplit[j]) { jbox = j; break; }
+        const int n = (ibox - 1) + (jbox - 1) * nbx;
+        bool ok;
+        int bx = bin(p->vx[k], &ok);
+        if (!ok) { ++skip; continue; }
+        int by = bin(p->vy[k], &ok);
+        if (!ok) { ++skip; continue; }
+        int bz = bin(p->vz[k], &ok);
+        if (!ok) { ++skip; continue; }
+        const int64_t pos1 = (int64_t)n * reclen - vmin;
+        h1[pos1 + bx]++;
+        h1[(int64_t)nbox * reclen + pos1 + by]++;
+        h1[2 * (int64_t)nbox * reclen + pos1 + bz]++;
+        if (h2) h2[((int64_t)n * reclen + (by - vmin)) * reclen + (bx - vmin)]++;
+    }
+    return skip;
+}
+
 // GetInjMaxwellVelocity pic2d_ElectronWallCollisions.f90:933-957
 static double maxwell_inj_sample(const double* v, double u)
 {

@@ -74,6 +74,13 @@ void oracle_fold_and_wall_scale(const oracle_geom_t* g, double* rho);
 void oracle_collect_moments(const oracle_geom_t* g, const oracle_species_t* sp, const double* EX, const double* EY,
                             const oracle_parts_t* p, double* out);
 
+/* CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393) for one cluster over
+ * [0, xmax] x [0, ymax]: nbx x nby boxes, bins INT(v fvc) (minus one for v < 0) in [vmin, -vmin - 1];
+ * h1[3][nbox][reclen] counts vx, vy, vz, h2[nbox][vy][vx] (may be NULL), reclen = -2 vmin. Returns the number of
+ * skipped particles. h1/h2 are zeroed here. */
+int64_t oracle_vdf(const oracle_parts_t* p, int32_t nbx, int32_t nby, double xmax, double ymax, double fvc,
+                   int32_t vmin, int32_t* h1, int32_t* h2);
+
 /* ---------------------------------------------------------------- Maxwell sampler */
 /* PrepareMaxwellDistribIntegral (pic2d_ElectronWallCollisions.f90:835-929); v[0..9000], v_inj[0..4500] */
 void   oracle_maxwell_tables(double* v, double* v_inj);

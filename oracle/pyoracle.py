@@ -97,6 +97,8 @@ def lib():
             "oracle_ion_emission": ([C.POINTER(Emit), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, C.c_double, C.c_double, _D,
                                      C.c_int32], C.c_int32),
+            "oracle_vdf": ([C.POINTER(Parts), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
+                            _I32, _I32], C.c_int64),
             "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _D], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
@@ -237,6 +239,18 @@ class IonEmission:
                                       ymax, dp(out), cap)
         assert n <= cap
         return out[:n]
+
+
+def vdf(parts, nbox, xmax, ymax, fvc, n_max_vel_s, n_vbins, two_d=False):
+    """oracle_vdf: (h1 [3, nbox, reclen], h2 [nbox, reclen, reclen] or None, skipped)."""
+    nb = nbox[0] * nbox[1]
+    vmin = -n_max_vel_s * n_vbins
+    rl = -2 * vmin
+    h1 = np.zeros((3, nb, rl), dtype=np.int32)
+    h2 = np.zeros((nb, rl, rl), dtype=np.int32) if two_d else None
+    i32 = lambda a: a.ctypes.data_as(_I32) if a is not None else None
+    sk = lib().oracle_vdf(C.byref(parts.s), nbox[0], nbox[1], xmax, ymax, fvc, vmin, i32(h1), i32(h2))
+    return h1, h2, sk
 
 
 def ion_reflect(wall, x, y, vx, vy, vz, xmax, ymax):
