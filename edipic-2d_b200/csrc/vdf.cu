@@ -1,11 +1,14 @@
 // Velocity distribution functions: CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393)
 // on the particles in HBM, for one cluster over the whole domain.
 //
-// The domain is split into nbx x nby boxes at X = i * ncx / nbx, Y = j * ncy / nby (xsplit/ysplit, :63-75). Each
-// velocity component is binned as INT(v * fvc), one less for v < 0 (:99-117), with fvc = N_max_vel * N_vbins
-// (* sqrt(Ms) for ions, :74 of the ion routine), bins vmin = -N_max_vel_s * N_vbins .. vmax = -vmin - 1. A particle with
-// any component outside that range is skipped and counted (:101-118). Counts: 1D histograms of vx, vy, vz per box
-// and, when asked, the 2D vx-vy histogram per box (:122-136).
+// The cluster area [0, c_X_area_max] x [0, c_Y_area_max] is split into nbx x nby boxes at X = i * c_X_area_max / nbx,
+// Y = j * c_Y_area_max / nby (xsplit/ysplit, :63-75). c_X_area_max = c_indx_x_max is ncx on a walled domain and
+// ncx + 1 on the self-connected periodic cluster (its overlap node, pic2d_CurProblemValues.f90:1310, :1331);
+// positions here are the periodic images in [0, ncx). Each velocity component is binned as INT(v * fvc), one less
+// for v < 0 (:99-117), with fvc = N_max_vel * N_vbins (* sqrt(Ms) for ions, :74 of the ion routine), bins
+// vmin = -N_max_vel_s * N_vbins .. vmax = -vmin - 1. A particle with any component outside that range is skipped
+// and counted (:101-118). Counts: 1D histograms of vx, vy, vz per box and, when asked, the 2D vx-vy histogram per
+// box (:122-136).
 //
 // One CTA keeps private copies of the histograms in shared memory when they fit (the 1D ones always do at the
 // reference's sizes) and adds them to the global counts once; otherwise it adds each count to global memory.
@@ -131,7 +134,8 @@ extern "C" int edp_calculate_vdf(edp_ctx* c, int species, int32_t n_max_vel, int
     a.nby = nbox_y;
     a.nbox = nbox_x * nbox_y;
     // xsplit(i) = c_X_area_min + DBLE(i) * (c_X_area_max - c_X_area_min) / N_vdfbox_x (:65-67), one cluster
-    for (int i = 1; i < nbox_x; ++i) a.xsplit[i - 1] = 0.0 + (double)i * (double)c->p.ncx / nbox_x;
+    const double xarea = (double)(c->p.periodic_x ? c->p.ncx + 1 : c->p.ncx);
+    for (int i = 1; i < nbox_x; ++i) a.xsplit[i - 1] = 0.0 + (double)i * xarea / nbox_x;
     for (int j = 1; j < nbox_y; ++j) a.ysplit[j - 1] = 0.0 + (double)j * (double)c->p.ncy / nbox_y;
     a.fvc = (double)(n_max_vel * n_vbins);
     if (species > 0) a.fvc *= std::sqrt(c->p.ion_mass_me[species - 1]);

@@ -143,6 +143,11 @@ SIGNATURES = {
     "edp_deck_ion_emission": [C.c_void_p, C.c_int32, C.c_int32, _D],
     "edp_deck_ion_wall_model": [C.c_void_p, C.c_int32, _I32],
     "edp_deck_free": [C.c_void_p],
+    "edp_write_snapshot_2d": [C.c_char_p, P(C.c_float), C.c_int32, C.c_int32, C.c_double],
+    "edp_write_vdf1d": [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                        C.c_int32, C.c_int32, C.c_int32, C.c_double, _D, _I32, _I32],
+    "edp_write_vdf2d": [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,
+                        C.c_double, _I32],
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libedipic_b200.so")

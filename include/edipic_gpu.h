@@ -234,7 +234,8 @@ int edp_moments(edp_ctx* ctx, int species, double out[7]);
  * cs_QZ after normalisation and ADJUST_DENSITY_AT_WALL_BOUNDARIES). */
 int edp_collect_moments(edp_ctx* ctx, int species, float* out);
 /* CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF (pic2d_VelocityDistributions.f90:3-393) for one species (0 electrons,
- * s ions), one cluster over the domain: nbox_x x nbox_y boxes (N_vdfbox_x/y of init_snapshots.dat), bins of
+ * s ions), one cluster over the domain: nbox_x x nbox_y boxes (N_vdfbox_x/y of init_snapshots.dat) splitting
+ * [0, c_X_area_max] x [0, ncy], c_X_area_max = ncx (walled) or ncx + 1 (periodic: the overlap node), bins of
  * 1/n_vbins thermal velocities up to +-n_max_vel_s of them (N_vbins_e/i, N_max_vel_e/i); n_max_vel is the deck's
  * velocity scale N_max_vel. vdf1d[3][nbox][2 n_max_vel_s n_vbins] = evxdf, evydf, evzdf (isvxdf.. for ions),
  * box = ibox + jbox nbox_x; vdf2d[nbox][vy bin][vx bin] = evxvydf, or NULL to skip it. skipped receives the
@@ -323,6 +324,19 @@ int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, 
 /* ion-material interaction model of wall's material (0 absorption, 1 specular reflection, 2 ion-induced emission) */
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
 int edp_deck_free(edp_deck* d);
+
+/* ---- snapshot files (host side of CREATE_SNAPSHOT, pic2d_Snapshots.f90:303-1202), one cluster ---------------- */
+/* SAVE_GLOBAL_2D_ARRAY (:1207-1355): gnuplot binary matrix of REAL values; row 0 = {nx_nodes, x_i = i delta_x_m},
+ * row 1 + j = {j delta_x_m, arr[j][0 .. nx_nodes - 1]}; arr[ny_nodes][nx_nodes] in the reference node layout */
+int edp_write_snapshot_2d(const char* path, const float* arr, int32_t nx_nodes, int32_t ny_nodes, double delta_x_m);
+/* SAVE_ALL_VDF1D (:1359-1544) of edp_calculate_vdf's electron and ion histograms (i1d = [n_spec][3][nbox][bins]);
+ * x_area_max, y_area_max = the cluster's c_X_area_max, c_Y_area_max in cells */
+int edp_write_vdf1d(const char* path, int32_t nbox_x, int32_t nbox_y, double x_area_max, double y_area_max,
+                    double delta_x_m, int32_t n_max_vel_e, int32_t n_vbins_e, int32_t n_max_vel_i, int32_t n_vbins_i,
+                    int32_t n_spec, double t_e_ev, const double* m_i_amu, const int32_t* e1d, const int32_t* i1d);
+/* SAVE_ALL_VDF2D (:1548-1705) of the electron vx-vy histograms */
+int edp_write_vdf2d(const char* path, int32_t nbox_x, int32_t nbox_y, double x_area_max, double y_area_max,
+                    double delta_x_m, int32_t n_max_vel_e, int32_t n_vbins_e, double t_e_ev, const int32_t* e2d);
 
 #ifdef __cplusplus
 }

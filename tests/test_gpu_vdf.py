@@ -40,7 +40,8 @@ def test_vdf_matches_oracle(tmp_path, precision, sort_every, geometry, species):
     ps = pyoracle.ParticleSet(parts["x"], parts["y"], parts["vx"], parts["vy"], parts["vz"])
     for (nbox, nmv, nvb, two_d), (h1, h2, sk) in zip(CASES, got):
         fvc = float(nmv_scale * nvb) * (np.sqrt(p.ion_mass_me[0]) if species == IONS else 1.0)
-        r1, r2, rs = pyoracle.vdf(ps, nbox, float(p.ncx), float(p.ncy), fvc, nmv, nvb, two_d)
+        xarea = float(p.ncx + 1 if sim.periodic else p.ncx)   # c_X_area_max of the one cluster
+        r1, r2, rs = pyoracle.vdf(ps, nbox, xarea, float(p.ncy), fvc, nmv, nvb, two_d)
         assert np.array_equal(h1, r1), (nbox, np.abs(h1 - r1).max())
         assert sk == rs
         assert h1[0].sum() + sk == parts["x"].size
