@@ -1,6 +1,7 @@
 """CREATE_SNAPSHOT from device moments and histograms (edipic_b200.snapshots): on a freshly distributed Maxwellian
 plasma the density file gives the deck's initial density and the temperature files its initial temperatures at
-interior nodes; the density, potential and VDF files hold exactly the device arrays they were made from."""
+interior nodes (the ions' z temperature is zero: they start with vz = 0); the potential and VDF files hold exactly the device arrays they were made from, the density file the
+device moments to FP32 rounding."""
 import numpy as np
 import pytest
 
@@ -27,7 +28,9 @@ def test_snapshot_files(tmp_path, geometry):
     assert len(names) == 38 + 2 and "_0007_Ni_1_m3_2D.bin" in names and "_0007_vdf2d.bin" in names
     sc = snapshots.scales(sim)
     _, _, ne = snapshots.read_2d(out / "_0007_Ne_m3_2D.bin")
-    assert np.array_equal(ne, m[0] * np.float32(sc["N_scale_part_m3"]))
+    # moments are FP32 atomic sums: two calls agree to rounding, not bit for bit
+    ref = m[0] * np.float32(sc["N_scale_part_m3"])
+    assert np.abs(ne - ref).max() <= 1e-5 * np.abs(ref).max()
     _, _, f = snapshots.read_2d(out / "_0007_F_V_2D.bin")
     assert np.array_equal(f, (phi * p.f_scale_v).astype(np.float32))
     inner = (slice(4, -4), slice(4, -4))
@@ -36,7 +39,10 @@ def test_snapshot_files(tmp_path, geometry):
         _, _, t = snapshots.read_2d(out / f"_0007_T{c}e_eV_2D.bin")
         assert abs(np.mean(t[inner]) / deck.init_te_ev - 1.0) < 0.03, (c, np.mean(t[inner]), deck.init_te_ev)
         _, _, ti = snapshots.read_2d(out / f"_0007_T{c}i_1_eV_2D.bin")
-        assert abs(np.mean(ti[inner]) / deck.init_ti_ev[0] - 1.0) < 0.05
+        if c == "Z":   # DISTRIBUTE_PARTICLES starts the ions with vz = 0 (pic2d_CurProblemValues.f90:3298)
+            assert np.all(ti == 0.0)
+        else:
+            assert abs(np.mean(ti[inner]) / deck.init_ti_ev[0] - 1.0) < 0.05, (c, np.mean(ti[inner]))
     raw = np.fromfile(out / "_0007_vdf2d.bin", dtype=np.int32)
     rl = 80
     one = 4 + rl * rl
