@@ -155,6 +155,23 @@ module edipic_gpu
        type(c_ptr), value :: ctx
        integer(c_int64_t), intent(out) :: counts(*)
      end function edp_query_emission
+     ! ion-material model 1 (specular reflection) of a wall
+     integer(c_int) function edp_set_ion_reflection(ctx, wall, on) bind(C, name="edp_set_ion_reflection")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: wall, on
+     end function edp_set_ion_reflection
+     ! CALCULATE_ELECTRON_VDF / CALCULATE_ION_VDF: evdf1d(bins, box, 3) in Fortran order, evxvydf(vx, vy, box)
+     integer(c_int) function edp_calculate_vdf(ctx, species, n_max_vel, nbox_x, nbox_y, n_max_vel_s, n_vbins, &
+          vdf1d, vdf2d, skipped) bind(C, name="edp_calculate_vdf")
+       import :: c_ptr, c_int, c_int32_t, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: species
+       integer(c_int32_t), value :: n_max_vel, nbox_x, nbox_y, n_max_vel_s, n_vbins
+       integer(c_int32_t), intent(out) :: vdf1d(*)
+       type(c_ptr), value :: vdf2d            ! c_loc(evxvydf) or c_null_ptr
+       integer(c_int64_t), intent(out) :: skipped
+     end function edp_calculate_vdf
      integer(c_int) function edp_warmstart_load(ctx, blob, n) bind(C, name="edp_warmstart_load")
        import :: c_ptr, c_int, c_int64_t, c_float
        type(c_ptr), value :: ctx
