@@ -1,6 +1,7 @@
 // C ABI of the EDIPIC-2D B200 particle cycle: context lifecycle, particle I/O, step orchestration.
 // The call order of one step follows MainProg (pic2d_MainProgram.f90:151-309).
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1092,6 +1093,15 @@ int edp_end_ion_cycle(edp_ctx* c)
         c->steps_since_sort = 0;
     }
     return finish_sync(c);
+}
+
+int edp_set_step(edp_ctx* c, int64_t t_cntr)
+{
+    if (!c || t_cntr < 0 || t_cntr > INT32_MAX) return edp_fail(c, EDP_ERR_ARG, "edp_set_step");
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->t_cntr = t_cntr;
+    c->n_sub_phase = 0;
+    return EDP_OK;
 }
 
 int edp_step(edp_ctx* c, int32_t nsteps)

@@ -242,6 +242,10 @@ class Simulation:
         self._check(self.lib.edp_set_ion_emission(self.ctx, wall, ion_species, yield_, emin_ev, emax_ev, t_emit_ev),
                     "edp_set_ion_emission")
 
+    def set_step(self, t_cntr):
+        """Start_T_cntr of a continued run: the next step is t_cntr (at ion sub-cycle 0)."""
+        self._check(self.lib.edp_set_step(self.ctx, int(t_cntr)), "edp_set_step")
+
     def set_ion_reflection(self, wall, on=True):
         """Ion-material model 1: the wall reflects every ion specularly (INJECT_REFLECTED_ION,
         pic2d_IonEmissions.f90:374-492)."""

@@ -107,6 +107,7 @@ SIGNATURES = {
     "edp_collide_rcx": [_CTX, _I64],
     "edp_end_ion_cycle": [_CTX],
     "edp_step": [_CTX, C.c_int32],
+    "edp_set_step": [_CTX, C.c_int64],
     "edp_query_counters": [_CTX, P(Counters)],
     "edp_get_field": [_CTX, C.c_int, _D],
     "edp_set_field": [_CTX, C.c_int, _D],

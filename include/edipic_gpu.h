@@ -215,6 +215,11 @@ int edp_collide_rcx(edp_ctx* ctx, int64_t* count_out);
  * PROCESS_ADDED_ELECTRONS (:363, pic2d_ElectronDynamics.f90:1429-1531): the ions and electrons born by this step's
  * ionisations join their arrays and the next step's density. Every step: advances T_cntr and runs the periodic sort. */
 int edp_end_ion_cycle(edp_ctx* ctx);
+/* Start_T_cntr of a run continued from a checkpoint (READ_CHECKPOINT_POSIX, pic2d_Checkpoints.f90:1002; the loop
+ * of pic2d_MainProgram.f90:98 resumes at the saved T_cntr): the next step is t_cntr, at ion sub-cycle n_sub = 0,
+ * where checkpoints are taken (:103-108). The step counter keys the device's random streams and the wall
+ * potentials. */
+int edp_set_step(edp_ctx* ctx, int64_t t_cntr);
 /* One or more whole steps of pic2d_MainProgram.f90:151-309 in order (convenience for drivers). */
 int edp_step(edp_ctx* ctx, int32_t nsteps);
 
