@@ -1,7 +1,8 @@
 """A run saved to a checkpoint in the reference's layouts and continued in a fresh context: the particles come back
 exactly (positions, velocities, tags; periodic overlap-cell positions folded), the step counter resumes at the saved
-T_cntr, and two further steps without collisions give the same particles as the run that was not interrupted (the
-mixed-precision deposit is fixed point, so the order of the particles does not matter)."""
+T_cntr, and two further steps without collisions give the same particles as the run that was not interrupted: bit
+for bit with the FFT_X solve and the fixed-point deposit (the order of the particles does not matter), to rounding
+otherwise."""
 import os
 
 import numpy as np
@@ -49,7 +50,10 @@ def test_checkpoint_restart(tmp_path, precision, geometry, fmt, nprocs):
     for pa, pb in zip(after_a, after_b):
         ra, rb = rows(pa), rows(pb)
         assert ra.shape == rb.shape
-        if precision == PREC_MIXED:
+        if precision == PREC_MIXED and geometry == "periodic":
             assert np.array_equal(ra, rb)
-        else:   # FP64 atomics sum the density in another order
-            assert np.abs(ra - rb).max() < 1e-9
+        else:
+            # FP64 atomics sum the density in another order; the walled CG solve starts from the previous potential
+            # in the uninterrupted run and from zero after the restart (a checkpoint holds no potential), so the
+            # fields agree to the CG tolerance
+            assert np.abs(ra - rb).max() < (1e-9 if geometry == "periodic" else 1e-6)
