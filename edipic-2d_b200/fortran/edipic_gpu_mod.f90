@@ -155,6 +155,12 @@ module edipic_gpu
        type(c_ptr), value :: ctx
        integer(c_int64_t), intent(out) :: counts(*)
      end function edp_query_emission
+     ! READ_A_CHECKPOINT: the continued run's next step is Start_T_cntr
+     integer(c_int) function edp_set_step(ctx, t_cntr) bind(C, name="edp_set_step")
+       import :: c_ptr, c_int, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), value :: t_cntr
+     end function edp_set_step
      ! ion-material model 1 (specular reflection) of a wall
      integer(c_int) function edp_set_ion_reflection(ctx, wall, on) bind(C, name="edp_set_ion_reflection")
        import :: c_ptr, c_int, c_int32_t
