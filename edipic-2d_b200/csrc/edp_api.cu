@@ -661,6 +661,8 @@ int edp_destroy(edp_ctx* c)
     edp_warmstart_free(c);
     F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v); F(c->maxwell_inj); F(c->emit_dev);
     delete c->emit_h;
+    delete c->see_h;
+    F(c->see_dev);
     F(c->hits.x); F(c->hits.y); F(c->hits.vx); F(c->hits.vy); F(c->hits.vz); F(c->hits.id); F(c->hits.ws);
     F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
@@ -983,6 +985,69 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
     return upload_wall_state(c);
 }
 
+int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp)
+{
+    if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission");
+    if (sp && (sp->elastic_model < 0 || sp->elastic_model > 2 || sp->inelastic_model < 0 || sp->inelastic_model > 2 ||
+               sp->true_model < 0 || sp->true_model > 2))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission: model outside 0-2");
+    TRY(wall_state(c));
+    if (!c->see_h) {
+        TRY(dalloc(c, &c->see_dev, 1));
+        c->see_h = new edp_see_dev();
+        memset(c->see_h, 0, sizeof(edp_see_dev));
+        c->see_h->maxwell_v = c->maxwell_v;
+        c->see_h->rmax = c->tab.maxwell_rmax;
+        c->see_h->maxwell_inj = c->maxwell_inj;
+        c->see_h->rmax_inj = c->emit_h->rmax_inj;
+    }
+    edp_see_wall& w = c->see_h->w[wall];
+    memset(&w, 0, sizeof(w));
+    if (sp && sp->elastic_model + sp->inelastic_model + sp->true_model > 0) {
+        // PREPARE_WALL_MATERIALS, pic2d_Materials.f90:195-244: energies to code units, the emission temperature to
+        // a velocity factor, and the lowest energy at which any model emits
+        const double ef = c->tab.energy_factor_eV;
+        w.on = 1;
+        w.m_el = sp->elastic_model;
+        w.m_in = sp->inelastic_model;
+        w.m_tr = sp->true_model;
+        w.refl_random = sp->elastic_type != 0;
+        w.el_yield = sp->elastic_yield;
+        w.el_emin = sp->elastic_emin_ev / ef;
+        w.el_emax = sp->elastic_emax_ev / ef;
+        w.el_e0 = sp->elastic_e0_ev / ef;
+        w.el_emaxc = sp->elastic_emax_coef_ev / ef;
+        w.el_max = sp->elastic_max;
+        w.el_de = sp->elastic_de_ev / ef;
+        w.el_frac = sp->elastic_frac_classic;
+        w.in_yield = sp->inelastic_yield;
+        w.in_emin = sp->inelastic_emin_ev / ef;
+        w.in_emax = sp->inelastic_emax_ev / ef;
+        w.in_frac = sp->inelastic_frac_classic;
+        w.tr_yield = sp->true_yield;
+        w.tr_emin = sp->true_emin_ev / ef;
+        w.tr_emax = sp->true_emax_ev / ef;
+        w.cl_e0 = sp->classic_e0_ev / ef;
+        w.cl_emax = sp->classic_emax_ev / ef;
+        w.cl_max = sp->classic_max;
+        w.cl_k = sp->classic_k_smooth;
+        w.fconv = std::sqrt(sp->true_t_ev / ef);
+        double lo = 1.0e6 / ef;
+        if (w.m_el == 1) lo = std::min(lo, w.el_emin);
+        if (w.m_el == 2) lo = std::min(lo, w.el_e0);
+        if (w.m_in == 1) lo = std::min(lo, w.in_emin);
+        if (w.m_in == 2) lo = std::min(lo, w.cl_e0);
+        if (w.m_tr == 1) lo = std::min(lo, w.tr_emin);
+        if (w.m_tr == 2) lo = std::min(lo, w.cl_e0);
+        w.lowest = lo;
+    }
+    c->see_on = 0;
+    for (int q = 0; q < 4; ++q) c->see_on |= c->see_h->w[q].on;
+    EDP_CUDA(c, cudaMemcpyAsync(c->see_dev, c->see_h, sizeof(edp_see_dev), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return EDP_OK;
+}
+
 int edp_set_ion_reflection(edp_ctx* c, int32_t wall, int32_t on)
 {
     if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
@@ -1015,6 +1080,7 @@ int edp_advance_electrons(edp_ctx* c)
     reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
     TRY(zero_density(c, 0));
     TRY(edp_launch_push(c, 0, ion_step, fuse));
+    if (c->see_on) TRY(edp_launch_electron_emission(c));
     return finish_sync(c);
 }
 
@@ -1068,11 +1134,14 @@ int edp_end_ion_cycle(edp_ctx* c)
     if (!c) return EDP_ERR_ARG;
     const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
-    if (ion_step) {
-        // collisions run only on ion steps, so only then can the add lists hold anything
+    if (ion_step || c->see_on) {
+        // collisions run only on ion steps, so only then, or when walls emit electrons, can the add lists hold
+        // anything (PROCESS_ADDED_ELECTRONS runs every step, pic2d_MainProgram.f90:363)
         TRY(edp_launch_append_born(c));
         ++c->launches;
         reset_born_kernel<<<1, 1, 0, c->stream>>>(c->dc);
+    }
+    if (ion_step) {
         if (c->p.precision == EDP_PREC_MIXED) {
             EDP_CUDA(c, cudaMemsetAsync(c->acc2, 0, nn * sizeof(float2), c->stream));
         } else {
@@ -1151,6 +1220,8 @@ int edp_query_counters(edp_ctx* c, edp_counters* out)
     if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "particle outside the domain");
     if (c->hc->error_flags & EDP_EFLAG_TIMEOUT) return edp_fail(c, EDP_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (c->hc->error_flags & EDP_EFLAG_SEE_MODEL)
+        return edp_fail(c, EDP_ERR_STATE, "elastic + inelastic emission coefficients above 1 (secondary emission model)");
     return EDP_OK;
 }
 

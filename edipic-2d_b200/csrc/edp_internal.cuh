@@ -30,6 +30,7 @@
 #define EDP_EFLAG_BOUNDS 2
 #define EDP_EFLAG_PENDING 4
 #define EDP_EFLAG_TIMEOUT 8   // a bounded device-side wait gave up
+#define EDP_EFLAG_SEE_MODEL 16   // elastic + inelastic emission coefficients above 1 at some electron impact
 
 struct edp_chunk {      // one CTA work item of the sorted push
     int64_t start, end; // slot range
@@ -75,7 +76,9 @@ struct edp_born {
     int64_t cap = 0;
 };
 
-// wall hits of ions while ion-induced electron emission is on: position, velocity, id, wall | species << 8
+// wall hits of the species being pushed while its walls emit or reflect: position, velocity, id, wall | species << 8
+// (the electron push fills it for electron-induced emission, the ion push for the ion-wall interactions; each push
+// is followed by the kernel that consumes and clears it)
 struct edp_hits {
     double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
     uint32_t* id = nullptr;
@@ -86,6 +89,7 @@ struct edp_hits {
 struct edp_mcc_dev;
 struct edp_warmstart;   // learned warm start of the CG solve (warmstart.cu)
 struct edp_emit_dev;    // ion-induced electron emission parameters (below)
+struct edp_see_dev;     // electron-induced electron emission parameters (below)
 
 // one level of the multigrid preconditioner: (nx+1) x (ny+1) nodes, x fastest, spacing 2^level
 #define EDP_MG_MAX_LEVELS 16
@@ -166,8 +170,11 @@ struct edp_ctx {
     edp_warmstart* ws = nullptr;      // network of the learned warm start, once loaded
     edp_emit_dev* emit_dev = nullptr; // ion-induced electron emission (device copy of emit_h)
     edp_emit_dev* emit_h = nullptr;   // host copy
-    edp_hits hits;                    // ion wall hits of the current ion step
-    int emit_on = 0;                  // wall hits are recorded: some wall emits or reflects
+    edp_hits hits;                    // wall hits of the current push
+    int emit_on = 0;                  // ion wall hits are recorded: some wall emits or reflects ions
+    edp_see_dev* see_dev = nullptr;   // electron-induced electron emission (device copy of see_h)
+    edp_see_dev* see_h = nullptr;
+    int see_on = 0;                   // electron wall hits are recorded
     double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
     int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     int32_t last_cg_iters = 0;
@@ -255,6 +262,7 @@ __host__ __device__ inline double edp_u01(uint32_t x) { return ((double)x + 0.5)
 #define EDP_STREAM_RCX(s) (1u + ((uint32_t)(s) << 8))
 #define EDP_STREAM_INIT(sp) (2u + ((uint32_t)(sp) << 8))
 #define EDP_STREAM_EMIT(s) (0x45450000u + (uint32_t)(s))   // ion-induced electron emission, ion species s
+#define EDP_STREAM_SEE 0x53450000u                          // electron-induced electron emission
 
 // --------------------------------------------------------------------------- collision tables (device)
 struct edp_mcc_dev {
@@ -507,6 +515,7 @@ edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
 // kernels launched from edp_api.cu, defined in the other translation units
 int edp_launch_push(edp_ctx* c, int species, bool ion_step, bool fuse);
 int edp_launch_ion_emission(edp_ctx* c);
+int edp_launch_electron_emission(edp_ctx* c);
 int edp_launch_collide_en(edp_ctx* c);
 int edp_launch_collide_rcx(edp_ctx* c);
 int edp_launch_append_born(edp_ctx* c);
@@ -561,6 +570,41 @@ __device__ inline double edp_maxwell_inj(const double* v, int rmax, double u)
     return __ldg(&v[rmax]);
 }
 
+// One electron emitted with a thermal velocity into the domain from wall `wall` at (x, y) (INJECT_ION_IMPACT_
+// EXTRACTED_ELECTRON, pic2d_IonEmissions.f90:91-348, and INJECT_TRUE_SECONDARY_ELECTRON, pic2d_SEEmission.f90:794-1050,
+// for the domain walls): 1e-6 inside the wall, normal speed from the injection table (variate w0), tangential
+// components from the Maxwell table (w1, w2) in x, y, z order, all times f, then scaled down to the energy left
+// (`energy`, which the electron's energy reduces). Returns false, emitting nothing, when no energy is left.
+__device__ inline bool edp_emit_thermal(const double* maxwell_v, int rmax, const double* maxwell_inj, int rmax_inj,
+                                        int wall, double x, double y, double xmax, double ymax, double f,
+                                        double& energy, const uint32_t w[4], double& nx, double& ny, double v[3])
+{
+    if (energy <= 0.0) return false;
+    const double un = edp_maxwell_inj(maxwell_inj, rmax_inj, edp_u01(w[0]));
+    const double t1 = edp_maxwell(maxwell_v, rmax, edp_u01(w[1]));
+    const double t2 = edp_maxwell(maxwell_v, rmax, edp_u01(w[2]));
+    switch (wall) {
+    case 0: nx = x; ny = 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2; break;            // below (dirflag 4)
+    case 1: nx = x; ny = ymax - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2; break;    // above (dirflag 2)
+    case 2: nx = 1.0e-6; ny = y; v[0] = un; v[1] = t1; v[2] = t2; break;            // left (dirflag 1)
+    default: nx = xmax - 1.0e-6; ny = y; v[0] = -un; v[1] = t1; v[2] = t2; break;   // right (dirflag 3)
+    }
+    v[0] *= f;
+    v[1] *= f;
+    v[2] *= f;
+    const double en = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (en > energy) {   // the electron takes what is left of the primary's energy
+        const double alpha = sqrt(energy / en);
+        v[0] *= alpha;
+        v[1] *= alpha;
+        v[2] *= alpha;
+        energy = 0.0;
+    } else {
+        energy -= en;
+    }
+    return true;
+}
+
 // PROCESS_ION_INDUCED_ELECTRON_EMISSION + INJECT_ION_IMPACT_EXTRACTED_ELECTRON (pic2d_IonEmissions.f90:1-342) for an
 // ion of species s absorbed by wall `wall` at (x, y) (the tangential coordinate already inside the domain) with
 // velocity v. Variates: Philox4x32-10, key {id, seed_lo}, counter {step, EDP_STREAM_EMIT(s), block, seed_hi};
@@ -581,35 +625,15 @@ __device__ __noinline__ int edp_emit_electrons(const edp_emit_dev* em, int s, in
     const double f = em->fconv[wall][s];
     int n = 0, e = 0;
     auto inject = [&]() {
-        if (energy <= 0.0) return;
         uint32_t w[4];
+        if (energy <= 0.0) return;
         edp_philox(step, EDP_STREAM_EMIT(s), 1u + (uint32_t)e, seed_hi, id, seed_lo, w);
+        double nx, ny, v[3];
+        if (!edp_emit_thermal(em->maxwell_v, em->rmax, em->maxwell_inj, em->rmax_inj, wall, x, y, xmax, ymax, f,
+                              energy, w, nx, ny, v))
+            return;
         ++e;
-        const double un = edp_maxwell_inj(em->maxwell_inj, em->rmax_inj, edp_u01(w[0]));
-        const double t1 = edp_maxwell(em->maxwell_v, em->rmax, edp_u01(w[1]));
-        const double t2 = edp_maxwell(em->maxwell_v, em->rmax, edp_u01(w[2]));
-        double nx, ny, nvx, nvy, nvz;
-        switch (wall) {
-        case 0: nx = x; ny = 1.0e-6; nvx = t1; nvy = un; nvz = t2; break;            // below (dirflag 4)
-        case 1: nx = x; ny = ymax - 1.0e-6; nvx = t1; nvy = -un; nvz = t2; break;    // above (dirflag 2)
-        case 2: nx = 1.0e-6; ny = y; nvx = un; nvy = t1; nvz = t2; break;            // left (dirflag 1)
-        default: nx = xmax - 1.0e-6; ny = y; nvx = -un; nvy = t1; nvz = t2; break;   // right (dirflag 3)
-        }
-        nvx *= f;
-        nvy *= f;
-        nvz *= f;
-        const double en = nvx * nvx + nvy * nvy + nvz * nvz;
-        if (en > energy) {   // the electron takes what is left of the ion's energy
-            const double alpha = sqrt(energy / en);
-            nvx *= alpha;
-            nvy *= alpha;
-            nvz *= alpha;
-            energy = 0.0;
-        } else {
-            energy -= en;
-        }
-        const double v3[3] = {nvx, nvy, nvz};
-        out(nx, ny, v3);
+        out(nx, ny, v);
         ++n;
     };
     while (coef >= 1.0) {
@@ -620,5 +644,156 @@ __device__ __noinline__ int edp_emit_electrons(const edp_emit_dev* em, int s, in
     uint32_t w0[4];
     edp_philox(step, EDP_STREAM_EMIT(s), 0u, seed_hi, id, seed_lo, w0);
     if (edp_u01(w0[0]) < coef) inject();
+    return n;
+}
+
+// Electron-induced electron emission of the four domain walls in code units (energies of an electron are v^2):
+// the parameters of edp_see_params converted as PREPARE_WALL_MATERIALS does (pic2d_Materials.f90:195-244).
+struct edp_see_wall {
+    int on, m_el, m_in, m_tr, refl_random;
+    double el_yield, el_emin, el_emax, el_e0, el_emaxc, el_max, el_de, el_frac;
+    double in_yield, in_emin, in_emax, in_frac;
+    double tr_yield, tr_emin, tr_emax;
+    double cl_e0, cl_emax, cl_max, cl_k;
+    double lowest;   // lowest_energy_for_see
+    double fconv;    // factor_convert_seetrue_vinj = sqrt(T_see / T_e) / N_max_vel
+};
+struct edp_see_dev {
+    edp_see_wall w[4];
+    const double* maxwell_v;
+    const double* maxwell_inj;
+    int rmax, rmax_inj;
+};
+
+// Coeff_SEE_Classic (pic2d_SEEmission.f90:1171-1208); its exponent k is a REAL (single precision) variable
+__device__ inline double edp_see_classic(const edp_see_wall& w, double e, double theta)
+{
+    if (!(e > w.cl_e0)) return 0.0;
+    const double emax_t = w.cl_emax * (1.0 + 0.318309886 * w.cl_k * theta * theta);
+    const double v = (e - w.cl_e0) / (emax_t - w.cl_e0);
+    const double cmax = w.cl_max * (1.0 + 0.159154943 * w.cl_k * theta * theta);
+    const double k = v < 1.0 ? (double)0.62f : (double)0.25f;
+    return cmax * pow(v * exp(1.0 - v), k);
+}
+
+// Coeff_SEE_Elastic / _Inelastic / _True (:1054-1167); a model-1 coefficient outside its window is 0
+__device__ inline double edp_see_elastic(const edp_see_wall& w, double e, double theta)
+{
+    if (w.m_el == 1) return (e > w.el_emin && e <= w.el_emax) ? w.el_yield : 0.0;
+    if (w.m_el != 2) return 0.0;
+    if (e >= w.el_emaxc)
+        return w.el_max * exp(-(e - w.el_emaxc) / w.el_de) * (e - w.el_emaxc + w.el_de) / w.el_de +
+               w.el_frac * edp_see_classic(w, e, theta);
+    if (e > w.el_e0)
+        return w.el_max * exp(-(e - w.el_emaxc) / (w.el_emaxc - w.el_e0)) * (e - w.el_e0) / (w.el_emaxc - w.el_e0) +
+               w.el_frac * edp_see_classic(w, e, theta);
+    return 0.0;
+}
+__device__ inline double edp_see_inelastic(const edp_see_wall& w, double e, double theta)
+{
+    if (w.m_in == 1) return (e > w.in_emin && e <= w.in_emax) ? w.in_yield : 0.0;
+    if (w.m_in == 2) return w.in_frac * edp_see_classic(w, e, theta);
+    return 0.0;
+}
+__device__ inline double edp_see_true(const edp_see_wall& w, double e, double theta)
+{
+    if (w.m_tr == 1) return (e > w.tr_emin && e <= w.tr_emax) ? w.tr_yield : 0.0;
+    if (w.m_tr != 2) return 0.0;
+    return fmax(0.0, edp_see_classic(w, e, theta) * (1.0 - w.el_frac - w.in_frac));
+}
+
+// A reflected or backscattered electron of speed `speed` leaving wall `wall` at angle theta from the normal and
+// azimuth fi (INJECT_ELASTIC_REFLECTED_ELECTRON / INJECT_INELASTIC_BACKSCATTERED_ELECTRON for the domain walls)
+__device__ inline void edp_see_scatter(int wall, double x, double y, double xmax, double ymax, double speed,
+                                       double theta, double fi, double& nx, double& ny, double v[3])
+{
+    const double c = speed * cos(theta), s1 = speed * sin(theta) * sin(fi), s2 = speed * sin(theta) * cos(fi);
+    switch (wall) {
+    case 0: nx = x; ny = 1.0e-6; v[0] = s1; v[1] = c; v[2] = s2; break;
+    case 1: nx = x; ny = ymax - 1.0e-6; v[0] = s1; v[1] = -c; v[2] = s2; break;
+    case 2: nx = 1.0e-6; ny = y; v[0] = c; v[1] = s1; v[2] = s2; break;
+    default: nx = xmax - 1.0e-6; ny = y; v[0] = -c; v[1] = s1; v[2] = s2; break;
+    }
+}
+
+// PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION (pic2d_SEEmission.f90:4-151) for an electron absorbed by `wall` at
+// (x, y) (coordinate along the wall already clamped) with velocity v. Variates: Philox4x32-10, key {id, seed_lo},
+// counter {step, EDP_STREAM_SEE, block, seed_hi}. Block 0: word 0 chooses the process, words 1 and 2 the angles
+// (ASIN(R), 2 pi R), word 3 the backscattered speed (sqrt(R)) or the fractional true yield; block 1 + e: true
+// secondary e (as edp_emit_thermal). Emitted electrons go to `out`; returns their number, or -1 when the elastic
+// and inelastic coefficients add up to more than 1 (the reference stops there).
+template <class Out>
+__device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, double x, double y, double vx,
+                                              double vy, double vz, uint32_t id, uint32_t step, uint32_t seed_lo,
+                                              uint32_t seed_hi, double xmax, double ymax, Out out)
+{
+    const edp_see_wall& w = sd->w[wall];
+    if (!w.on) return 0;
+    double e = vx * vx + vy * vy + vz * vz;
+    if (e <= w.lowest) return 0;
+    const double v = sqrt(e);
+    double theta = 0.0;
+    if (v != 0.0) theta = acos(fmin(1.0, fabs(wall >= 2 ? vx : vy) / v));
+    const double ce = edp_see_elastic(w, e, theta), ci = edp_see_inelastic(w, e, theta);
+    if (ce + ci > 1.0) return -1;
+    double ct = edp_see_true(w, e, theta);
+    const double ctot = ce + ci + ct;
+    if (ctot == 0.0) return 0;
+    uint32_t b0[4];
+    edp_philox(step, EDP_STREAM_SEE, 0u, seed_hi, id, seed_lo, b0);
+    const double R = edp_u01(b0[0]);
+    double nx, ny, nv[3];
+    if (R <= ce) {   // INJECT_ELASTIC_REFLECTED_ELECTRON :155-557
+        if (!w.refl_random) {
+            nx = x;
+            ny = y;
+            nv[0] = vx;
+            nv[1] = vy;
+            nv[2] = vz;
+            switch (wall) {
+            case 0: ny = 1.0e-6; nv[1] = -vy; break;
+            case 1: ny = ymax - 1.0e-6; nv[1] = -vy; break;
+            case 2: nx = 1.0e-6; nv[0] = -vx; break;
+            default: nx = xmax - 1.0e-6; nv[0] = -vx; break;
+            }
+        } else {
+            edp_see_scatter(wall, x, y, xmax, ymax, v, asin(fmin(edp_u01(b0[1]), 1.0)),
+                            6.283185307179 * edp_u01(b0[2]), nx, ny, nv);
+        }
+        out(nx, ny, nv);
+        return 1;
+    }
+    if (R > ce && R <= ce + ci) {   // INJECT_INELASTIC_BACKSCATTERED_ELECTRON :561-790
+        const double th = asin(fmin(edp_u01(b0[1]), 1.0)), fi = 6.283185307179 * edp_u01(b0[2]);
+        edp_see_scatter(wall, x, y, xmax, ymax, v * sqrt(edp_u01(b0[3])), th, fi, nx, ny, nv);
+        out(nx, ny, nv);
+        return 1;
+    }
+    if (ct <= 0.0) return 0;
+    double energy = e;
+    if (w.m_tr == 1) energy = fmax(0.0, e - w.tr_emin);
+    else if (w.m_tr == 2) energy = fmax(0.0, e - w.cl_e0);
+    int n = 0, k = 0;
+    auto inject = [&]() {   // INJECT_TRUE_SECONDARY_ELECTRON :794-1050
+        uint32_t wb[4];
+        if (energy <= 0.0) return;
+        edp_philox(step, EDP_STREAM_SEE, 1u + (uint32_t)k, seed_hi, id, seed_lo, wb);
+        if (!edp_emit_thermal(sd->maxwell_v, sd->rmax, sd->maxwell_inj, sd->rmax_inj, wall, x, y, xmax, ymax, w.fconv,
+                              energy, wb, nx, ny, nv))
+            return;
+        ++k;
+        out(nx, ny, nv);
+        ++n;
+    };
+    if (ctot <= 1.0) {
+        if (R > ce + ci && R <= ctot) inject();
+        return n;
+    }
+    ct = ct / (1.0 - (ce + ci));
+    while (ct >= 1.0) {
+        inject();
+        ct -= 1.0;
+    }
+    if (edp_u01(b0[3]) < ct) inject();
     return n;
 }

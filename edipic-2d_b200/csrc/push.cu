@@ -228,9 +228,9 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         if (nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f)) {
             const int wall = nj < 0 ? 0 : 1;
             atomicAdd(&s.cnt[wall], 1ull);
-            if (ION && a.emit_on)
-                record_hit(a.hits, a.dc, wall, a.species - 1, (double)ni + (double)nx, (double)nj + (double)ny, vx,
-                           vy, vz, id);
+            if (a.emit_on)
+                record_hit(a.hits, a.dc, wall, ION ? a.species - 1 : 0, (double)ni + (double)nx,
+                           (double)nj + (double)ny, vx, vy, vz, id);
             return false;
         }
     } else {
@@ -239,9 +239,9 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         if (outx || outy) {
             int obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
             atomicAdd(&s.cnt[obj], 1ull);
-            if (ION && a.emit_on)
-                record_hit(a.hits, a.dc, obj, a.species - 1, (double)ni + (double)nx, (double)nj + (double)ny, vx,
-                           vy, vz, id);
+            if (a.emit_on)
+                record_hit(a.hits, a.dc, obj, ION ? a.species - 1 : 0, (double)ni + (double)nx,
+                           (double)nj + (double)ny, vx, vy, vz, id);
             return false;
         }
         if (ni == kp.ncx) { ni = kp.ncx - 1; nx = 1.0f; }   // X == c_X_area_max (:68)
@@ -326,7 +326,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
         vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
         vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
         vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
-        if (a.do_coll || (ION && a.emit_on)) {
+        if (a.do_coll || a.emit_on) {
             uint4 id4 = __ldcs(reinterpret_cast<const uint4*>(a.P.id) + g);
             id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
         } else {
@@ -597,8 +597,8 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             a.P.x[k] = -1.0e30;
             atomicAdd(&cnt[obj], 1ull);
             atomicAdd(&cnt[17], 1ull);
-            if (a.is_ion && a.emit_on && obj < 4)
-                record_hit(a.hits, a.dc, obj, a.species - 1, X, Y, vx, vy, vz, a.P.id[k]);
+            if (a.emit_on && obj < 4)
+                record_hit(a.hits, a.dc, obj, a.is_ion ? a.species - 1 : 0, X, Y, vx, vy, vz, a.P.id[k]);
             continue;
         }
         // deposit
@@ -899,7 +899,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.sel_count = c->sel_count;
         a.sel_cap = c->sel_cap;
         a.hits = c->hits;
-        a.emit_on = is_ion && c->emit_on;
+        a.emit_on = is_ion ? c->emit_on : c->see_on;
         if (do_mcc) EDP_CUDA(c, cudaMemsetAsync(c->sel_count, 0, sizeof(unsigned long long), c->stream));
         int64_t tail = c->host_slots[sp] - c->sorted_end[sp];
         if (tail < 0) tail = 0;
@@ -960,7 +960,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.born_e = c->born_e;
         for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) a.born_i[q] = c->born_i[q];
         a.hits = c->hits;
-        a.emit_on = is_ion && c->emit_on;
+        a.emit_on = is_ion ? c->emit_on : c->see_on;
         int64_t n = c->host_slots[sp];
         int64_t grid = (n + 255) / 256;
         if (grid > 148 * 64) grid = 148 * 64;
@@ -1003,6 +1003,35 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
                                          });
         if (m) atomicAdd(&dc->e_emit[wall], (unsigned long long)m);
     }
+}
+
+// PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION for every electron wall hit of this step (the coordinate along the wall
+// clamped into the domain first, pic2d_ElectronWallCollisions.f90:21, :93, :165, :237)
+__global__ void __launch_bounds__(256) electron_emission_kernel(edp_hits h, const edp_see_dev* sd, edp_born born_e,
+                                                                edp_dev_counters* dc, edp_kparams kp, uint32_t step)
+{
+    const int64_t n = min((int64_t)dc->hit_count, h.cap);
+    const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int wall = h.ws[k] & 255;
+        const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
+        const int m = edp_see_electrons(sd, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
+                                        kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
+                                            record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
+                                        });
+        if (m < 0) atomicOr(&dc->error_flags, EDP_EFLAG_SEE_MODEL);
+        else if (m) atomicAdd(&dc->e_emit[wall], (unsigned long long)m);
+    }
+}
+
+int edp_launch_electron_emission(edp_ctx* c)
+{
+    ++c->launches;
+    electron_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->see_dev, c->born_e, c->dc, c->kp,
+                                                           (uint32_t)c->t_cntr);
+    EDP_CUDA(c, cudaGetLastError());
+    EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));
+    return EDP_OK;
 }
 
 int edp_launch_ion_emission(edp_ctx* c)

@@ -10,6 +10,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
+from ._abi import SeeParams  # noqa: F401
 from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS,
                    PREC_FP64, PREC_MIXED, PRECOND_MG, PRECOND_NONE, SOLVER_CG, SOLVER_FFTX, WARM_LEARNED, WARM_PREVIOUS,
                    WARM_USER, WARM_ZERO, Counters,
@@ -66,11 +67,15 @@ class Deck:
         # ion-induced electron emission of the walls' materials: {(wall, ion species): (yield, E_min, E_max, T)}
         self.ion_emission = {}
         self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission
+        self.electron_emission = {}           # {wall: SeeParams} of the walls whose material emits electrons
         buf = (C.c_double * 4)()
         model = C.c_int32()
         for wall in range(4):
             if self.lib.edp_deck_ion_wall_model(self.handle, wall, C.byref(model)) == 0:
                 self.ion_wall_model[wall] = model.value
+            see, on = _abi.SeeParams(), C.c_int32()
+            if self.lib.edp_deck_electron_emission(self.handle, wall, C.byref(see), C.byref(on)) == 0 and on.value:
+                self.electron_emission[wall] = see
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(wall, s)] = tuple(buf)
@@ -120,6 +125,8 @@ class Simulation:
         for wall, model in enumerate(self.deck.ion_wall_model):
             if model == 1:
                 self.set_ion_reflection(wall, True)
+        for wall, see in self.deck.electron_emission.items():
+            self.set_electron_emission(wall, see)
 
     # ------------------------------------------------------------------------------------ plumbing
     def _check(self, rc, where):
@@ -251,8 +258,18 @@ class Simulation:
         pic2d_IonEmissions.f90:374-492)."""
         self._check(self.lib.edp_set_ion_reflection(self.ctx, wall, 1 if on else 0), "edp_set_ion_reflection")
 
+    def set_electron_emission(self, wall, params=None, **kw):
+        """Electron-induced electron emission of a wall (PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION,
+        pic2d_SEEmission.f90:4-151): params is a SeeParams, or its fields as keywords; None (and no keywords)
+        switches the wall off."""
+        if params is None and kw:
+            params = _abi.SeeParams(**kw)
+        self._check(self.lib.edp_set_electron_emission(self.ctx, wall, C.byref(params) if params is not None else None),
+                    "edp_set_electron_emission")
+
     def emission_counts(self):
-        """Electrons emitted by ion impacts on each object (walls 0-3, then inner objects), cumulative."""
+        """Electrons emitted by each object (walls 0-3, then inner objects; ion and electron impacts), cumulative:
+        electron_emit_count."""
         out = np.zeros(4 + _abi.MAX_INNER, np.int64)
         self._check(self.lib.edp_query_emission(self.ctx, out.ctypes.data_as(C.POINTER(C.c_int64))),
                     "edp_query_emission")

@@ -67,6 +67,16 @@ class Tables(C.Structure):
     ]
 
 
+class SeeParams(C.Structure):
+    """edp_see_params: electron-induced emission of one wall material, energies in eV."""
+    _fields_ = [("elastic_model", C.c_int32), ("elastic_type", C.c_int32), ("inelastic_model", C.c_int32),
+                ("true_model", C.c_int32)] + [(n, C.c_double) for n in (
+                    "elastic_yield", "elastic_emin_ev", "elastic_emax_ev", "elastic_e0_ev", "elastic_emax_coef_ev",
+                    "elastic_max", "elastic_de_ev", "elastic_frac_classic", "inelastic_yield", "inelastic_emin_ev",
+                    "inelastic_emax_ev", "inelastic_frac_classic", "true_t_ev", "true_yield", "true_emin_ev",
+                    "true_emax_ev", "classic_e0_ev", "classic_emax_ev", "classic_max", "classic_k_smooth")]
+
+
 class Counters(C.Structure):
     _fields_ = [
         ("n_particles", C.c_int64 * MAX_SPECIES), ("electron_hits", C.c_int64 * N_HIT),
@@ -101,6 +111,7 @@ SIGNATURES = {
     "edp_set_ion_emission": [_CTX, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double],
     "edp_query_emission": [_CTX, _I64],
     "edp_set_ion_reflection": [_CTX, C.c_int32, C.c_int32],
+    "edp_set_electron_emission": [_CTX, C.c_int32, P(SeeParams)],
     "edp_advance_electrons": [_CTX],
     "edp_advance_ions": [_CTX],
     "edp_collide_en": [_CTX, _I64],
@@ -143,6 +154,7 @@ SIGNATURES = {
     "edp_deck_initial_plasma": [C.c_void_p, _D, _D, _D, _D, _I32, _D, _I64],
     "edp_deck_ion_emission": [C.c_void_p, C.c_int32, C.c_int32, _D],
     "edp_deck_ion_wall_model": [C.c_void_p, C.c_int32, _I32],
+    "edp_deck_electron_emission": [C.c_void_p, C.c_int32, P(SeeParams), _I32],
     "edp_deck_free": [C.c_void_p],
     "edp_write_snapshot_2d": [C.c_char_p, P(C.c_float), C.c_int32, C.c_int32, C.c_double],
     "edp_write_vdf1d": [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,

@@ -33,6 +33,14 @@ CONFIGS = {
 }
 
 
+# electron-induced emission of the wall material, all three models off (fields of edp_see_params)
+SEE_OFF = dict(elastic_model=0, elastic_type=0, inelastic_model=0, true_model=0, elastic_yield=0.0,
+               elastic_emin_ev=0.0, elastic_emax_ev=0.0, elastic_e0_ev=0.0, elastic_emax_coef_ev=0.0, elastic_max=0.0,
+               elastic_de_ev=0.0, elastic_frac_classic=0.0, inelastic_yield=0.0, inelastic_emin_ev=0.0,
+               inelastic_emax_ev=0.0, inelastic_frac_classic=0.0, true_t_ev=0.0, true_yield=0.0, true_emin_ev=0.0,
+               true_emax_ev=0.0, classic_e0_ev=0.0, classic_emax_ev=0.0, classic_max=0.0, classic_k_smooth=0.0)
+
+
 def sigma_elastic(e):
     return 1.0e-19 / (1.0 + e / 15.0) + 5.0e-21
 
@@ -57,10 +65,11 @@ def _segments():
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
-               ion_emission=None, ion_reflection=False):
+               ion_emission=None, ion_reflection=False, electron_emission=None):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
-    reflect all ions specularly instead (ion-material model 1)."""
+    reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
+    and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -163,38 +172,41 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
     iee = cfg.get("ion_emission") if ion_emission is None else (ion_emission or None)
     # init_material_METAL1.dat in the layout PREPARE_WALL_MATERIALS reads (pic2d_Materials.f90:79-188): electron
     # reflection and secondary emission off, ion-material model 2 (ion-induced emission) or 0 (absorption)
+    see = dict(SEE_OFF, **(electron_emission or {}))
+    i1, f5, f6, f10 = (lambda v: f"       {int(v):1d}"), (lambda v: f"       {v:5.3f}"), (lambda v: f"      {v:6.3f}"), \
+        (lambda v: f"  {v:10.3f}")
     mat = [
-        "------dd.ddd- dielectric constant", f"      {1.0:6.3f}",
-        "=======d===== elastic electron reflection model", f"       {0:1d}",
-        "-------d----- elastic electron reflection type", f"       {0:1d}",
+        "------dd.ddd- dielectric constant", f6(1.0),
+        "=======d===== elastic electron reflection model", i1(see["elastic_model"]),
+        "-------d----- elastic electron reflection type", i1(see["elastic_type"]),
         "------------- elastic reflection, model 1",
-        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
-        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
-        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- coefficient", f5(see["elastic_yield"]),
+        "--dddddd.ddd- E_min [eV]", f10(see["elastic_emin_ev"]),
+        "--dddddd.ddd- E_max [eV]", f10(see["elastic_emax_ev"]),
         "------------- elastic reflection, model 2",
-        "--dddddd.ddd- threshold [eV]", f"  {0.0:10.3f}",
-        "--dddddd.ddd- energy of the maximum [eV]", f"  {0.0:10.3f}",
-        "-------d.ddd- maximum", f"       {0.0:5.3f}",
-        "--dddddd.ddd- decay scale [eV]", f"  {0.0:10.3f}",
-        "-------d.ddd- high-energy fraction", f"       {0.0:5.3f}",
-        "=======d===== inelastic electron reflection model", f"       {0:1d}",
+        "--dddddd.ddd- threshold [eV]", f10(see["elastic_e0_ev"]),
+        "--dddddd.ddd- energy of the maximum [eV]", f10(see["elastic_emax_coef_ev"]),
+        "-------d.ddd- maximum", f5(see["elastic_max"]),
+        "--dddddd.ddd- decay scale [eV]", f10(see["elastic_de_ev"]),
+        "-------d.ddd- high-energy fraction", f5(see["elastic_frac_classic"]),
+        "=======d===== inelastic electron reflection model", i1(see["inelastic_model"]),
         "------------- inelastic reflection, model 1",
-        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
-        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
-        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- coefficient", f5(see["inelastic_yield"]),
+        "--dddddd.ddd- E_min [eV]", f10(see["inelastic_emin_ev"]),
+        "--dddddd.ddd- E_max [eV]", f10(see["inelastic_emax_ev"]),
         "------------- inelastic reflection, model 2",
-        "-------d.ddd- fraction", f"       {0.0:5.3f}",
-        "=======d===== true secondary emission model", f"       {0:1d}",
-        "--dddddd.ddd- temperature [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- fraction", f5(see["inelastic_frac_classic"]),
+        "=======d===== true secondary emission model", i1(see["true_model"]),
+        "--dddddd.ddd- temperature [eV]", f10(see["true_t_ev"]),
         "------------- true secondary emission, model 1",
-        "-------d.ddd- coefficient", f"       {0.0:5.3f}",
-        "--dddddd.ddd- E_min [eV]", f"  {0.0:10.3f}",
-        "--dddddd.ddd- E_max [eV]", f"  {0.0:10.3f}",
+        "-------d.ddd- coefficient", f5(see["true_yield"]),
+        "--dddddd.ddd- E_min [eV]", f10(see["true_emin_ev"]),
+        "--dddddd.ddd- E_max [eV]", f10(see["true_emax_ev"]),
         "------------- true secondary emission, model 2",
-        "--dddddd.ddd- threshold [eV]", f"  {0.0:10.3f}",
-        "--dddddd.ddd- energy of the maximum [eV]", f"  {0.0:10.3f}",
-        "------dd.ddd- maximum", f"      {0.0:6.3f}",
-        "-------d.ddd- smoothness", f"       {0.0:5.3f}",
+        "--dddddd.ddd- threshold [eV]", f10(see["classic_e0_ev"]),
+        "--dddddd.ddd- energy of the maximum [eV]", f10(see["classic_emax_ev"]),
+        "------dd.ddd- maximum", f6(see["classic_max"]),
+        "-------d.ddd- smoothness", f5(see["classic_k_smooth"]),
         "=======d===== ION-MATERIAL INTERACTION MODEL (0 absorb, 1 reflect, 2 ion-induced electron emission)",
         f"       {1 if ion_reflection else (2 if iee else 0):1d}",
     ]

@@ -117,6 +117,7 @@ struct edp_deck {
     // ion-induced electron emission of the four walls per ion species: yield, E_min [eV], E_max [eV], T [eV]
     double ii_ee[4][EDP_MAX_ION_SPECIES][4] = {};
     int32_t ion_model[4] = {};   // ion-material interaction model of each wall's material
+    edp_see_params see[4] = {};  // electron-induced emission of each wall's material
 };
 
 namespace {
@@ -295,6 +296,30 @@ int read_deck(const std::string& dir, edp_deck* d)
         if (mat == "      ") continue;
         Lines mf(dir + "/init_material_" + mat + ".dat");
         if (!mf.ok) continue;
+        {
+            // lines 3-56, in the order of pic2d_Materials.f90:84-149 (one header line before each value)
+            Lines sf(dir + "/init_material_" + mat + ".dat");
+            edp_see_params& s = d->see[w];
+            long long m1 = 0, rt = 0, m2 = 0, m3 = 0;
+            auto I = [&](long long* v) { return sf.next(L) && sf.next(L) && fint(L, 7, 1, v); };
+            auto R = [&](size_t skip, size_t width, double* v) { return sf.next(L) && sf.next(L) && freal(L, skip, width, v); };
+            auto H = [&]() { return sf.next(L); };
+            double eps = 0;
+            bool ok = R(6, 6, &eps) && I(&m1) && I(&rt) && H() && R(7, 5, &s.elastic_yield) &&
+                      R(2, 10, &s.elastic_emin_ev) && R(2, 10, &s.elastic_emax_ev) && H() && R(2, 10, &s.elastic_e0_ev) &&
+                      R(2, 10, &s.elastic_emax_coef_ev) && R(7, 5, &s.elastic_max) && R(2, 10, &s.elastic_de_ev) &&
+                      R(7, 5, &s.elastic_frac_classic) && I(&m2) && H() && R(7, 5, &s.inelastic_yield) &&
+                      R(2, 10, &s.inelastic_emin_ev) && R(2, 10, &s.inelastic_emax_ev) && H() &&
+                      R(7, 5, &s.inelastic_frac_classic) && I(&m3) && R(2, 10, &s.true_t_ev) && H() &&
+                      R(7, 5, &s.true_yield) && R(2, 10, &s.true_emin_ev) && R(2, 10, &s.true_emax_ev) && H() &&
+                      R(2, 10, &s.classic_e0_ev) && R(2, 10, &s.classic_emax_ev) && R(6, 6, &s.classic_max) &&
+                      R(7, 5, &s.classic_k_smooth);
+            if (!ok) return EDP_ERR_IO;
+            s.elastic_model = (int32_t)m1;
+            s.elastic_type = (int32_t)rt;
+            s.inelastic_model = (int32_t)m2;
+            s.true_model = (int32_t)m3;
+        }
         bool found = false;
         while (mf.next(L))
             if (L.find("ION-MATERIAL INTERACTION MODEL") != std::string::npos) {
@@ -530,6 +555,14 @@ int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model)
 {
     if (!d || !model || wall < 0 || wall > 3) return EDP_ERR_ARG;
     *model = d->ion_model[wall];
+    return EDP_OK;
+}
+
+int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled)
+{
+    if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    *out = d->see[wall];
+    if (enabled) *enabled = (out->elastic_model + out->inelastic_model + out->true_model) > 0;
     return EDP_OK;
 }
 

@@ -128,6 +128,23 @@ typedef struct edp_tables {
     const double* maxwell_v;
 } edp_tables;
 
+/* Electron-induced electron emission of one wall material (init_material_<NAME>.dat lines 3-56, read by
+ * PREPARE_WALL_MATERIALS, pic2d_Materials.f90:84-149); energies and temperature in eV as in the file. Models:
+ * 0 off, 1 constant coefficient between E_min and E_max, 2 the energy- and angle-dependent forms of Coeff_SEE_*
+ * (pic2d_SEEmission.f90:1054-1208). */
+typedef struct edp_see_params {
+    int32_t elastic_model, elastic_type;        /* Emitted_model(1); Elast_refl_type 0 specular, 1 random */
+    int32_t inelastic_model, true_model;        /* Emitted_model(2), Emitted_model(3) */
+    double elastic_yield, elastic_emin_ev, elastic_emax_ev;                         /* elastic, model 1 */
+    double elastic_e0_ev, elastic_emax_coef_ev, elastic_max, elastic_de_ev;        /* elastic, model 2 */
+    double elastic_frac_classic;                /* Frac_elast_highenergy */
+    double inelastic_yield, inelastic_emin_ev, inelastic_emax_ev;                   /* inelastic, model 1 */
+    double inelastic_frac_classic;              /* Frac_inelastic (model 2) */
+    double true_t_ev;                           /* T_see_true_eV */
+    double true_yield, true_emin_ev, true_emax_ev;                                  /* true secondaries, model 1 */
+    double classic_e0_ev, classic_emax_ev, classic_max, classic_k_smooth;          /* model 2 and the classic form */
+} edp_see_params;
+
 /* Counters of one step (COLLECT_PARTICLE_BOUNDARY_HITS, collision counters, particle totals). */
 typedef struct edp_counters {
     int64_t n_particles[1 + EDP_MAX_ION_SPECIES];           /* live particles */
@@ -200,6 +217,14 @@ int edp_set_ion_emission(edp_ctx* ctx, int32_t wall, int32_t ion_species, double
  * inside the wall with the normal velocity reversed, through the ion add list at the end of the step. Reflection
  * takes precedence over emission on the same wall. on = 0 restores absorption. */
 int edp_set_ion_reflection(edp_ctx* ctx, int32_t wall, int32_t on);
+/* Electron-induced electron emission of a domain wall (0 below, 1 above, 2 left, 3 right):
+ * PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION (pic2d_SEEmission.f90:4-151) for every electron the wall absorbs
+ * (PROCESS_ELECTRON_COLL_WITH_BOUNDARY_*, pic2d_ElectronWallCollisions.f90:3-287): elastic reflection, inelastic
+ * backscattering or true secondaries. The emitted electrons join at the end of the step and are counted with
+ * edp_query_emission. params = NULL, or all three models 0, switches the wall off. Returns EDP_ERR_ARG when a
+ * model number is outside 0-2. A wall whose elastic and inelastic coefficients add up to more than 1 at some
+ * impact sets the model error (EDP_ERR_STATE from edp_query_counters), where the reference stops. */
+int edp_set_electron_emission(edp_ctx* ctx, int32_t wall, const edp_see_params* params);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
  * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
 int edp_advance_electrons(edp_ctx* ctx);
@@ -328,6 +353,8 @@ int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_
 int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out);
 /* ion-material interaction model of wall's material (0 absorption, 1 specular reflection, 2 ion-induced emission) */
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
+/* electron-induced emission parameters of wall's material; *enabled = 1 when any of the three models is on */
+int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled);
 int edp_deck_free(edp_deck* d);
 
 /* ---- snapshot files (host side of CREATE_SNAPSHOT, pic2d_Snapshots.f90:303-1202), one cluster ---------------- */

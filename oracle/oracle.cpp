@@ -574,6 +574,138 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
     return n;
 }
 
+// Coeff_SEE_Classic pic2d_SEEmission.f90:1171-1208 (k is a REAL variable: 0.62 in single precision)
+static double see_classic(const oracle_see_t* w, double energy, double theta)
+{
+    if (!(energy > w->cl_e0)) return 0.0;
+    double energy_max_theta = w->cl_emax * (1.0 + 0.318309886 * w->cl_k * theta * theta);
+    double v = (energy - w->cl_e0) / (energy_max_theta - w->cl_e0);
+    double coeff_max_theta = w->cl_max * (1.0 + 0.159154943 * w->cl_k * theta * theta);
+    float k = v < 1.0 ? 0.62f : 0.25f;
+    return coeff_max_theta * std::pow(v * std::exp(1.0 - v), (double)k);
+}
+
+// Coeff_SEE_Elastic :1054-1099, Coeff_SEE_Inelastic :1103-1134, Coeff_SEE_True :1139-1167
+static double see_elastic(const oracle_see_t* w, double e, double th)
+{
+    switch (w->m_el) {
+    case 1: return (e > w->el_emin && e <= w->el_emax) ? w->el_yield : 0.0;
+    case 2:
+        if (e >= w->el_emaxc)
+            return w->el_max * std::exp(-(e - w->el_emaxc) / w->el_de) * (e - w->el_emaxc + w->el_de) / w->el_de +
+                   w->el_frac * see_classic(w, e, th);
+        if (e > w->el_e0)
+            return w->el_max * std::exp(-(e - w->el_emaxc) / (w->el_emaxc - w->el_e0)) * (e - w->el_e0) /
+                       (w->el_emaxc - w->el_e0) +
+                   w->el_frac * see_classic(w, e, th);
+        return 0.0;
+    default: return 0.0;
+    }
+}
+static double see_inelastic(const oracle_see_t* w, double e, double th)
+{
+    if (w->m_in == 1) return (e > w->in_emin && e <= w->in_emax) ? w->in_yield : 0.0;
+    if (w->m_in == 2) return w->in_frac * see_classic(w, e, th);
+    return 0.0;
+}
+static double see_true(const oracle_see_t* w, double e, double th)
+{
+    if (w->m_tr == 1) return (e > w->tr_emin && e <= w->tr_emax) ? w->tr_yield : 0.0;
+    if (w->m_tr != 2) return 0.0;
+    double c = see_classic(w, e, th) * (1.0 - w->el_frac - w->in_frac);
+    return c < 0.0 ? 0.0 : c;
+}
+
+int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
+                   uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap)
+{
+    const uint32_t stream = 0x53450000u;
+    x = std::min(std::max(x, 0.0), xmax);
+    y = std::min(std::max(y, 0.0), ymax);
+    double energy_inc = vx * vx + vy * vy + vz * vz;
+    if (energy_inc <= w->lowest) return 0;
+    double v = std::sqrt(energy_inc), theta_inc = 0.0;
+    if (v != 0.0) theta_inc = std::acos(std::min(1.0, std::fabs(wall >= 2 ? vx : vy) / v));
+    double ce = see_elastic(w, energy_inc, theta_inc), ci = see_inelastic(w, energy_inc, theta_inc);
+    if (ce + ci > 1.0) return -1;
+    double ct = see_true(w, energy_inc, theta_inc), ctot = ce + ci + ct;
+    if (ctot == 0.0) return 0;
+    uint32_t b0[4];
+    philox_block(id, seed, step, stream, 0u, b0);
+    double R = uniform(b0[0]);
+    int32_t n = 0;
+    auto put = [&](double nx, double ny, double a, double b, double c) {
+        if (n < cap) {
+            double* r = out + 5 * n;
+            r[0] = nx; r[1] = ny; r[2] = a; r[3] = b; r[4] = c;
+        }
+        ++n;
+    };
+    // the position and the direction of a scattered electron leaving the wall (the domain-wall branches)
+    auto scatter = [&](double speed, double theta, double fi) {
+        double c = speed * std::cos(theta), s1 = speed * std::sin(theta) * std::sin(fi),
+               s2 = speed * std::sin(theta) * std::cos(fi);
+        if (wall == 2) put(1.0e-6, y, c, s1, s2);
+        else if (wall == 1) put(x, ymax - 1.0e-6, s1, -c, s2);
+        else if (wall == 3) put(xmax - 1.0e-6, y, -c, s1, s2);
+        else put(x, 1.0e-6, s1, c, s2);
+    };
+    if (R <= ce) {   // INJECT_ELASTIC_REFLECTED_ELECTRON :155-557
+        if (!w->refl_random) {
+            if (wall == 2) put(1.0e-6, y, -vx, vy, vz);
+            else if (wall == 1) put(x, ymax - 1.0e-6, vx, -vy, vz);
+            else if (wall == 3) put(xmax - 1.0e-6, y, -vx, vy, vz);
+            else put(x, 1.0e-6, vx, -vy, vz);
+        } else {
+            scatter(v, std::asin(std::min(uniform(b0[1]), 1.0)), 6.283185307179 * uniform(b0[2]));
+        }
+        return n;
+    }
+    if (R > ce && R <= ce + ci) {   // INJECT_INELASTIC_BACKSCATTERED_ELECTRON :561-790
+        double th = std::asin(std::min(uniform(b0[1]), 1.0)), fi = 6.283185307179 * uniform(b0[2]);
+        scatter(v * std::sqrt(uniform(b0[3])), th, fi);
+        return n;
+    }
+    if (ct <= 0.0) return 0;
+    if (w->m_tr == 1) energy_inc = std::max(0.0, energy_inc - w->tr_emin);
+    else if (w->m_tr == 2) energy_inc = std::max(0.0, energy_inc - w->cl_e0);
+    uint32_t block = 1;
+    auto inject = [&]() {   // INJECT_TRUE_SECONDARY_ELECTRON :794-1050
+        if (energy_inc <= 0.0) return;
+        uint32_t wb[4];
+        philox_block(id, seed, step, stream, block++, wb);
+        double un = maxwell_inj_sample(w->maxwell_inj, uniform(wb[0]));
+        double t1 = oracle_maxwell_sample(w->maxwell_v, uniform(wb[1]));
+        double t2 = oracle_maxwell_sample(w->maxwell_v, uniform(wb[2]));
+        double xn, yn, nv[3];
+        if (wall == 2) { xn = 1.0e-6; yn = y; nv[0] = un; nv[1] = t1; nv[2] = t2; }
+        else if (wall == 1) { xn = x; yn = ymax - 1.0e-6; nv[0] = t1; nv[1] = -un; nv[2] = t2; }
+        else if (wall == 3) { xn = xmax - 1.0e-6; yn = y; nv[0] = -un; nv[1] = t1; nv[2] = t2; }
+        else { xn = x; yn = 1.0e-6; nv[0] = t1; nv[1] = un; nv[2] = t2; }
+        for (double& c : nv) c *= w->fconv;
+        double energy_new = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+        if (energy_new > energy_inc) {
+            double alpha = std::sqrt(energy_inc / energy_new);
+            for (double& c : nv) c *= alpha;
+            energy_inc = 0.0;
+        } else {
+            energy_inc -= energy_new;
+        }
+        put(xn, yn, nv[0], nv[1], nv[2]);
+    };
+    if (ctot <= 1.0) {
+        if (R > ce + ci && R <= ctot) inject();
+        return n;
+    }
+    ct = ct / (1.0 - (ce + ci));
+    while (ct >= 1.0) {
+        inject();
+        ct -= 1.0;
+    }
+    if (uniform(b0[3]) < ct) inject();
+    return n;
+}
+
 // INJECT_REFLECTED_ION pic2d_IonEmissions.f90:374-430 (m > 0, the domain walls)
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,
                         double* out)

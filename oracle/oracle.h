@@ -109,6 +109,27 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
                             double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
                             double* out, int32_t cap);
 
+/* electron-induced emission of one domain wall, in code units (PREPARE_WALL_MATERIALS, pic2d_Materials.f90:84-244) */
+typedef struct {
+    int32_t m_el, m_in, m_tr, refl_random;
+    double el_yield, el_emin, el_emax, el_e0, el_emaxc, el_max, el_de, el_frac;
+    double in_yield, in_emin, in_emax, in_frac;
+    double tr_yield, tr_emin, tr_emax;
+    double cl_e0, cl_emax, cl_max, cl_k;
+    double lowest, fconv;
+    const double* maxwell_v;     /* v[0..9000] */
+    const double* maxwell_inj;   /* v_inj[0..4500] */
+} oracle_see_t;
+/* PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION (pic2d_SEEmission.f90:4-151) with INJECT_ELASTIC_REFLECTED_ELECTRON,
+ * INJECT_INELASTIC_BACKSCATTERED_ELECTRON, INJECT_TRUE_SECONDARY_ELECTRON and the Coeff_SEE_* functions for an
+ * electron absorbed by `wall` at (x, y) (clamped along the wall here) with velocity v: rows {x, y, vx, vy, vz} of the
+ * emitted electrons (room for cap), returns their number or -1 when elastic + inelastic coefficients exceed 1.
+ * Variates: Philox4x32-10, key {id, seed_lo}, counter {step, 0x53450000, block, seed_hi}: block 0 words 0-3 = the
+ * process choice R, the two angle variates, the backscattered speed variate or the fractional true yield; block
+ * 1 + e = true secondary e (normal speed, two tangential components). */
+int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
+                   uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap);
+
 /* INJECT_REFLECTED_ION (pic2d_IonEmissions.f90:374-492) for a domain wall: the ion returns 1e-6 inside the wall
  * (coordinate along the wall clamped into the domain) with its normal velocity reversed; out = {x, y, vx, vy, vz} */
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,

@@ -79,6 +79,14 @@ class Emit(C.Structure):
                 ("maxwell_v", _D), ("maxwell_inj", _D)]
 
 
+class See(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("m_el", "m_in", "m_tr", "refl_random")] + \
+        [(n, C.c_double) for n in ("el_yield", "el_emin", "el_emax", "el_e0", "el_emaxc", "el_max", "el_de", "el_frac",
+                                   "in_yield", "in_emin", "in_emax", "in_frac", "tr_yield", "tr_emin", "tr_emax",
+                                   "cl_e0", "cl_emax", "cl_max", "cl_k", "lowest", "fconv")] + \
+        [("maxwell_v", _D), ("maxwell_inj", _D)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -99,6 +107,8 @@ def lib():
                                      C.c_int32], C.c_int32),
             "oracle_vdf": ([C.POINTER(Parts), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
                             _I32, _I32], C.c_int64),
+            "oracle_see": ([C.POINTER(See), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                            C.c_uint32, C.c_uint64, C.c_uint32, C.c_double, C.c_double, _D, C.c_int32], C.c_int32),
             "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _D], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
@@ -251,6 +261,42 @@ def vdf(parts, nbox, xmax, ymax, fvc, n_max_vel_s, n_vbins, two_d=False):
     i32 = lambda a: a.ctypes.data_as(_I32) if a is not None else None
     sk = lib().oracle_vdf(C.byref(parts.s), nbox[0], nbox[1], xmax, ymax, fvc, vmin, i32(h1), i32(h2))
     return h1, h2, sk
+
+
+class ElectronEmission:
+    """Electron-induced emission of one wall (oracle_see) from a dict of the material-file parameters in eV (the
+    fields of edp_see_params), converted to code units as PREPARE_WALL_MATERIALS does (pic2d_Materials.f90:195-244)
+    with energy_factor_ev."""
+
+    def __init__(self, prm, energy_factor_ev):
+        ef = energy_factor_ev
+        self.v, self.vi = maxwell_tables()
+        s = See()
+        s.m_el, s.m_in, s.m_tr = prm["elastic_model"], prm["inelastic_model"], prm["true_model"]
+        s.refl_random = 1 if prm["elastic_type"] else 0
+        s.el_yield, s.el_emin, s.el_emax = prm["elastic_yield"], prm["elastic_emin_ev"] / ef, prm["elastic_emax_ev"] / ef
+        s.el_e0, s.el_emaxc = prm["elastic_e0_ev"] / ef, prm["elastic_emax_coef_ev"] / ef
+        s.el_max, s.el_de, s.el_frac = prm["elastic_max"], prm["elastic_de_ev"] / ef, prm["elastic_frac_classic"]
+        s.in_yield, s.in_emin = prm["inelastic_yield"], prm["inelastic_emin_ev"] / ef
+        s.in_emax, s.in_frac = prm["inelastic_emax_ev"] / ef, prm["inelastic_frac_classic"]
+        s.tr_yield, s.tr_emin, s.tr_emax = prm["true_yield"], prm["true_emin_ev"] / ef, prm["true_emax_ev"] / ef
+        s.cl_e0, s.cl_emax = prm["classic_e0_ev"] / ef, prm["classic_emax_ev"] / ef
+        s.cl_max, s.cl_k = prm["classic_max"], prm["classic_k_smooth"]
+        s.fconv = np.sqrt(prm["true_t_ev"] / ef)
+        lo = 1.0e6 / ef
+        lo = min(lo, {1: s.el_emin, 2: s.el_e0}.get(s.m_el, lo))
+        lo = min(lo, {1: s.in_emin, 2: s.cl_e0}.get(s.m_in, lo))
+        lo = min(lo, {1: s.tr_emin, 2: s.cl_e0}.get(s.m_tr, lo))
+        s.lowest = lo
+        s.maxwell_v, s.maxwell_inj = dp(self.v), dp(self.vi)
+        self.s = s
+
+    def emit(self, wall, x, y, vx, vy, vz, ident, seed, step, xmax, ymax, cap=64):
+        out = np.zeros((cap, 5))
+        n = lib().oracle_see(C.byref(self.s), int(wall), x, y, vx, vy, vz, int(ident), seed, step, xmax, ymax,
+                             dp(out), cap)
+        assert n <= cap
+        return out[:max(n, 0)], n
 
 
 def ion_reflect(wall, x, y, vx, vy, vz, xmax, ymax):
