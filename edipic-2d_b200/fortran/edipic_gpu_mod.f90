@@ -161,6 +161,13 @@ module edipic_gpu
        type(c_ptr), value :: ctx
        integer(c_int64_t), value :: t_cntr
      end function edp_set_step
+     ! electron-induced emission of a wall: see = edp_see_params filled from the material file (eV)
+     integer(c_int) function edp_set_electron_emission(ctx, wall, see) bind(C, name="edp_set_electron_emission")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: wall
+       type(c_ptr), value :: see              ! c_loc of an interoperable copy of edp_see_params, or c_null_ptr
+     end function edp_set_electron_emission
      ! ion-material model 1 (specular reflection) of a wall
      integer(c_int) function edp_set_ion_reflection(ctx, wall, on) bind(C, name="edp_set_ion_reflection")
        import :: c_ptr, c_int, c_int32_t
