@@ -1048,6 +1048,39 @@ int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp
     return EDP_OK;
 }
 
+int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t model, double t_normal_ev,
+                           double t_parallel_ev, double beam_energy_ev)
+{
+    if (!c || wall < 0 || wall > 3 || !(n_per_step >= 0.0) || n_per_step > 1.0e9 || model < 0 || model > 1 ||
+        !(t_normal_ev >= 0.0) || !(t_parallel_ev >= 0.0))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection");
+    if (c->p.periodic_x && wall >= 2 && n_per_step > 0.0)
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection: a periodic domain has walls below and above only");
+    if (model == 1 && n_per_step > 0.0 && !(beam_energy_ev > 1.5 * t_normal_ev))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection: beam energy spread above the beam energy / 1.5");
+    TRY(wall_state(c));
+    // PREPARE_SETUP_VALUES, pic2d_Setup.f90:103-126: sqrt(T / T_e) / N_max_vel = sqrt(T / energy_factor_eV)
+    const double ef = c->tab.energy_factor_eV;
+    edp_inject_dev& in = c->inject;
+    in.maxwell_v = c->maxwell_v;
+    in.rmax = c->tab.maxwell_rmax;
+    in.maxwell_inj = c->maxwell_inj;
+    in.rmax_inj = c->emit_h->rmax_inj;
+    in.n[wall] = n_per_step;
+    in.model[wall] = model;
+    in.fp[wall] = std::sqrt(t_parallel_ev / ef);
+    if (model == 0) {
+        in.fn[wall] = std::sqrt(t_normal_ev / ef);
+        in.vb[wall] = 0.0;
+    } else {
+        in.fn[wall] = n_per_step > 0.0 ? std::sqrt(0.25 * t_normal_ev * t_normal_ev / (beam_energy_ev * ef)) : 0.0;
+        in.vb[wall] = std::sqrt(std::max(beam_energy_ev, 0.0) / ef);
+    }
+    c->inject_on = 0;
+    for (int w = 0; w < 4; ++w) c->inject_on |= in.n[w] > 0.0;
+    return EDP_OK;
+}
+
 int edp_set_ion_reflection(edp_ctx* c, int32_t wall, int32_t on)
 {
     if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
@@ -1134,7 +1167,9 @@ int edp_end_ion_cycle(edp_ctx* c)
     if (!c) return EDP_ERR_ARG;
     const bool ion_step = (c->n_sub_phase + 1) == c->p.n_subcycles;
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
-    if (ion_step || c->see_on) {
+    // PERFORM_ELECTRON_EMISSION_SETUP (pic2d_MainProgram.f90:353)
+    if (c->inject_on) TRY(edp_launch_wall_injection(c));
+    if (ion_step || c->see_on || c->inject_on) {
         // collisions run only on ion steps, so only then, or when walls emit electrons, can the add lists hold
         // anything (PROCESS_ADDED_ELECTRONS runs every step, pic2d_MainProgram.f90:363)
         TRY(edp_launch_append_born(c));

@@ -91,6 +91,17 @@ struct edp_warmstart;   // learned warm start of the CG solve (warmstart.cu)
 struct edp_emit_dev;    // ion-induced electron emission parameters (below)
 struct edp_see_dev;     // electron-induced electron emission parameters (below)
 
+// constant electron emission of the four domain walls (PERFORM_ELECTRON_EMISSION_SETUP), code units
+struct edp_inject_dev {
+    double n[4];           // N_electron_constant_emit, macroparticles per step
+    int model[4];          // 0 thermal, 1 beam
+    double fn[4], fp[4];   // factor_convert_vinj_normal/parallel_constant_emit
+    double vb[4];          // v_ebeam_constant_emit
+    const double* maxwell_v;
+    const double* maxwell_inj;
+    int rmax, rmax_inj;
+};
+
 // one level of the multigrid preconditioner: (nx+1) x (ny+1) nodes, x fastest, spacing 2^level
 #define EDP_MG_MAX_LEVELS 16
 struct edp_mg_level {
@@ -175,6 +186,8 @@ struct edp_ctx {
     edp_see_dev* see_dev = nullptr;   // electron-induced electron emission (device copy of see_h)
     edp_see_dev* see_h = nullptr;
     int see_on = 0;                   // electron wall hits are recorded
+    edp_inject_dev inject{};          // constant electron emission (by value into the kernel)
+    int inject_on = 0;
     double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
     int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     int32_t last_cg_iters = 0;
@@ -263,6 +276,8 @@ __host__ __device__ inline double edp_u01(uint32_t x) { return ((double)x + 0.5)
 #define EDP_STREAM_INIT(sp) (2u + ((uint32_t)(sp) << 8))
 #define EDP_STREAM_EMIT(s) (0x45450000u + (uint32_t)(s))   // ion-induced electron emission, ion species s
 #define EDP_STREAM_SEE 0x53450000u                          // electron-induced electron emission
+#define EDP_STREAM_INJECT 0x43450000u                       // constant electron emission of the walls
+#define EDP_INJECT_KEY 0xE1000000u                          // Philox key word 0 of wall w's injection: KEY + w
 
 // --------------------------------------------------------------------------- collision tables (device)
 struct edp_mcc_dev {
@@ -516,6 +531,7 @@ edp_rcx_dev edp_make_rcx_dev(const edp_ctx* c, int s);
 int edp_launch_push(edp_ctx* c, int species, bool ion_step, bool fuse);
 int edp_launch_ion_emission(edp_ctx* c);
 int edp_launch_electron_emission(edp_ctx* c);
+int edp_launch_wall_injection(edp_ctx* c);
 int edp_launch_collide_en(edp_ctx* c);
 int edp_launch_collide_rcx(edp_ctx* c);
 int edp_launch_append_born(edp_ctx* c);

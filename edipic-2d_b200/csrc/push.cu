@@ -1034,6 +1034,59 @@ int edp_launch_electron_emission(edp_ctx* c)
     return EDP_OK;
 }
 
+// PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001) for one cluster over the domain: wall blockIdx.y emits
+// INT(n) electrons and one more with probability n - INT(n) (:627-690). Variates: Philox4x32-10, key {EDP_INJECT_KEY
+// + wall, seed_lo}, counter {step, EDP_STREAM_INJECT, block, seed_hi}; block 0 word 0 for the fraction, block 1 + e for
+// electron e: word 0 its place along the wall, word 1 the normal speed, words 2 and 3 the tangential components (the
+// one in the wall's plane of the domain, then z).
+__global__ void __launch_bounds__(256) wall_injection_kernel(edp_inject_dev in, edp_born born_e,
+                                                             edp_dev_counters* dc, edp_kparams kp, uint32_t step)
+{
+    const int wall = blockIdx.y;
+    const double n = in.n[wall];
+    if (n <= 0.0) return;
+    const uint32_t key = EDP_INJECT_KEY + (uint32_t)wall;
+    int count = (int)n;
+    uint32_t w0[4];
+    edp_philox(step, EDP_STREAM_INJECT, 0u, kp.seed_hi, key, kp.seed_lo, w0);
+    if (edp_u01(w0[0]) < n - (double)count) ++count;
+    const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        uint32_t w[4];
+        edp_philox(step, EDP_STREAM_INJECT, 1u + (uint32_t)e, kp.seed_hi, key, kp.seed_lo, w);
+        double vn;
+        if (in.model[wall] == 0) {
+            vn = edp_maxwell_inj(in.maxwell_inj, in.rmax_inj, edp_u01(w[1])) * in.fn[wall];
+        } else {
+            vn = fmax(0.0, in.vb[wall] + edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[1])) * in.fn[wall]);
+        }
+        const double t1 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[2])) * in.fp[wall];
+        const double t2 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[3])) * in.fp[wall];
+        const double r = edp_u01(w[0]);
+        double x, y, v[3];
+        switch (wall) {
+        case 0: x = fmin(fmax(r * xmax, 0.0), xmax); y = 1.0e-6; v[0] = t1; v[1] = vn; v[2] = t2; break;
+        case 1: x = fmin(fmax(r * xmax, 0.0), xmax); y = ymax - 1.0e-6; v[0] = t1; v[1] = -vn; v[2] = t2; break;
+        case 2: x = 1.0e-6; y = fmin(fmax(r * ymax, 0.0), ymax); v[0] = vn; v[1] = t1; v[2] = t2; break;
+        default: x = xmax - 1.0e-6; y = fmin(fmax(r * ymax, 0.0), ymax); v[0] = -vn; v[1] = t1; v[2] = t2; break;
+        }
+        record_born(born_e, &dc->born_e_count, &dc->error_flags, x, y, v);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&dc->e_emit[wall], (unsigned long long)count);
+}
+
+int edp_launch_wall_injection(edp_ctx* c)
+{
+    double nmax = 0.0;
+    for (int w = 0; w < 4; ++w) nmax = std::max(nmax, c->inject.n[w]);
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(((int64_t)nmax + 256) / 256, 148));
+    ++c->launches;
+    wall_injection_kernel<<<dim3((unsigned)blocks, 4), 256, 0, c->stream>>>(c->inject, c->born_e, c->dc, c->kp,
+                                                                           (uint32_t)c->t_cntr);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
 int edp_launch_ion_emission(edp_ctx* c)
 {
     ++c->launches;

@@ -68,6 +68,7 @@ class Deck:
         self.ion_emission = {}
         self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission
         self.electron_emission = {}           # {wall: SeeParams} of the walls whose material emits electrons
+        self.wall_injection = {}              # {wall: (N per step, model, T_normal, T_parallel, W_beam)}
         buf = (C.c_double * 4)()
         model = C.c_int32()
         for wall in range(4):
@@ -76,6 +77,9 @@ class Deck:
             see, on = _abi.SeeParams(), C.c_int32()
             if self.lib.edp_deck_electron_emission(self.handle, wall, C.byref(see), C.byref(on)) == 0 and on.value:
                 self.electron_emission[wall] = see
+            inj = (C.c_double * 5)()
+            if self.lib.edp_deck_wall_injection(self.handle, wall, inj) == 0 and inj[0] > 0.0:
+                self.wall_injection[wall] = (inj[0], int(inj[1]), inj[2], inj[3], inj[4])
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(wall, s)] = tuple(buf)
@@ -127,6 +131,8 @@ class Simulation:
                 self.set_ion_reflection(wall, True)
         for wall, see in self.deck.electron_emission.items():
             self.set_electron_emission(wall, see)
+        for wall, (n, model, tn, tp, wb) in self.deck.wall_injection.items():
+            self.set_wall_injection(wall, n, model, tn, tp, wb)
 
     # ------------------------------------------------------------------------------------ plumbing
     def _check(self, rc, where):
@@ -266,6 +272,13 @@ class Simulation:
             params = _abi.SeeParams(**kw)
         self._check(self.lib.edp_set_electron_emission(self.ctx, wall, C.byref(params) if params is not None else None),
                     "edp_set_electron_emission")
+
+    def set_wall_injection(self, wall, n_per_step, model=0, t_normal_ev=0.0, t_parallel_ev=0.0, beam_energy_ev=0.0):
+        """Constant electron emission from a wall every step (PERFORM_ELECTRON_EMISSION_SETUP, pic2d_Setup.f90:599):
+        model 0 thermal, 1 beam."""
+        self._check(self.lib.edp_set_wall_injection(self.ctx, wall, float(n_per_step), int(model), float(t_normal_ev),
+                                                    float(t_parallel_ev), float(beam_energy_ev)),
+                    "edp_set_wall_injection")
 
     def emission_counts(self):
         """Electrons emitted by each object (walls 0-3, then inner objects; ion and electron impacts), cumulative:

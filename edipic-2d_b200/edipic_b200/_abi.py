@@ -112,6 +112,7 @@ SIGNATURES = {
     "edp_query_emission": [_CTX, _I64],
     "edp_set_ion_reflection": [_CTX, C.c_int32, C.c_int32],
     "edp_set_electron_emission": [_CTX, C.c_int32, P(SeeParams)],
+    "edp_set_wall_injection": [_CTX, C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double],
     "edp_advance_electrons": [_CTX],
     "edp_advance_ions": [_CTX],
     "edp_collide_en": [_CTX, _I64],
@@ -155,6 +156,7 @@ SIGNATURES = {
     "edp_deck_ion_emission": [C.c_void_p, C.c_int32, C.c_int32, _D],
     "edp_deck_ion_wall_model": [C.c_void_p, C.c_int32, _I32],
     "edp_deck_electron_emission": [C.c_void_p, C.c_int32, P(SeeParams), _I32],
+    "edp_deck_wall_injection": [C.c_void_p, C.c_int32, _D],
     "edp_deck_free": [C.c_void_p],
     "edp_write_snapshot_2d": [C.c_char_p, P(C.c_float), C.c_int32, C.c_int32, C.c_double],
     "edp_write_vdf1d": [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,

@@ -65,11 +65,13 @@ def _segments():
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
-               ion_emission=None, ion_reflection=False, electron_emission=None):
+               ion_emission=None, ion_reflection=False, electron_emission=None, wall_injection=None):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
     reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
-    and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default."""
+    and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default.
+    wall_injection: {wall (0 below, 1 above, 2 left, 3 right): (electrons per step, model, T_normal, T_parallel,
+    beam energy [eV])}, the constant electron emission of init_bo_NN.dat."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -154,18 +156,18 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         "-------d------- ions sense Z-electric field", f"       {0:1d}",
     ])
 
-    def bo(n, phi, amp=0.0, mhz=0.0):
+    def bo(n, phi, amp=0.0, mhz=0.0, inj=(0.0, 0, 0.0, 0.0, 0.0)):
         w(f"init_bo_{n:02d}.dat", [
             "------AAAAAA--- material", "      METAL1",
             "---ddddd.ddd--- constant potential [V]", f"   {phi:9.3f}",
             "---ddddd.ddd--- amplitude of oscillations [V]", f"   {amp:9.3f}",
             "---ddddd.ddd--- frequency [MHz]", f"   {mhz:9.3f}",
             "---ddddd.ddd--- phase [deg]", f"   {0.0:9.3f}",
-            "---ddddd.ddd--- electrons injected per step", f"   {0.0:9.3f}",
-            "-------d------- emission model", f"       {0:1d}",
-            "----dddd.ddd--- emitted temperature normal [eV]", f"    {0.0:8.3f}",
-            "----dddd.ddd--- emitted temperature parallel [eV]", f"    {0.0:8.3f}",
-            "----dddd.ddd--- beam energy [eV]", f"    {0.0:8.3f}",
+            "---ddddd.ddd--- electrons injected per step", f"   {inj[0]:9.3f}",
+            "-------d------- emission model", f"       {int(inj[1]):1d}",
+            "----dddd.ddd--- emitted temperature normal [eV]", f"    {inj[2]:8.3f}",
+            "----dddd.ddd--- emitted temperature parallel [eV]", f"    {inj[3]:8.3f}",
+            "----dddd.ddd--- beam energy [eV]", f"    {inj[4]:8.3f}",
             "-------d------- save collided ions", f"       {0:1d}",
             "-------d------- save collided electrons", f"       {0:1d}",
         ])
@@ -229,7 +231,8 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
             amp, mhz = (0.0, 0.0)
             if k == 1 and cfg.get("top_rf"):
                 amp, mhz = cfg["top_rf"]
-            bo(k + 1, wp.get(k + 1, 0.0), amp, mhz)
+            wall = (2, 1, 3, 0)[k]   # objects: left, above, right, below
+            bo(k + 1, wp.get(k + 1, 0.0), amp, mhz, (wall_injection or {}).get(wall, (0.0, 0, 0.0, 0.0, 0.0)))
     for q, (_a, _b, _c, _d, phi) in enumerate(inner_list):
         bo(len(objs) + q + 1, phi)
 

@@ -118,6 +118,7 @@ struct edp_deck {
     double ii_ee[4][EDP_MAX_ION_SPECIES][4] = {};
     int32_t ion_model[4] = {};   // ion-material interaction model of each wall's material
     edp_see_params see[4] = {};  // electron-induced emission of each wall's material
+    double inject[4][5] = {};    // constant electron emission of each wall: N per step, model, T_n, T_p, W_beam [eV]
 };
 
 namespace {
@@ -282,6 +283,25 @@ int read_deck(const std::string& dir, edp_deck* d)
         if (side_obj[s] >= 0 &&
             !read_bo(side_obj[s], &p.wall_phi_const[s], &p.wall_phi_var[s], &p.wall_omega[s], &p.wall_phase[s]))
             return EDP_ERR_IO;
+    // ---- constant electron emission of the walls (init_bo_NN.dat lines 11-20, PREPARE_SETUP_VALUES
+    // pic2d_Setup.f90:86-95): macroparticles per step (3x,f9.3), model (7x,i1), normal and parallel temperatures and
+    // the beam energy in eV (4x,f8.3)
+    for (int w = 0; w < 4; ++w) {
+        if (side_obj[w] < 0) continue;
+        char name[32];
+        snprintf(name, sizeof(name), "/init_bo_%02d.dat", side_obj[w] + 1);
+        Lines bf(dir + name);
+        if (!bf.ok) continue;
+        for (int k = 0; k < 10; ++k)
+            if (!bf.next(L)) return EDP_ERR_IO;
+        long long model = 0;
+        double* q = d->inject[w];
+        bool ok = bf.next(L) && bf.next(L) && freal(L, 3, 9, &q[0]) && bf.next(L) && bf.next(L) &&
+                  fint(L, 7, 1, &model) && bf.next(L) && bf.next(L) && freal(L, 4, 8, &q[2]) && bf.next(L) &&
+                  bf.next(L) && freal(L, 4, 8, &q[3]) && bf.next(L) && bf.next(L) && freal(L, 4, 8, &q[4]);
+        if (!ok) return EDP_ERR_IO;
+        q[1] = (double)model;
+    }
     // ---- wall materials (material name: init_bo_NN.dat line 2, (6x,A6), pic2d_Setup.f90:77; properties
     // init_material_<NAME>.dat, PREPARE_WALL_MATERIALS pic2d_Materials.f90:1-200). Only the ion-material interaction
     // model is used: 2 = ion-induced electron emission with, per ion species, a constant coefficient between
@@ -563,6 +583,13 @@ int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* 
     if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
     *out = d->see[wall];
     if (enabled) *enabled = (out->elastic_model + out->inelastic_model + out->true_model) > 0;
+    return EDP_OK;
+}
+
+int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out)
+{
+    if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    for (int k = 0; k < 5; ++k) out[k] = d->inject[wall][k];
     return EDP_OK;
 }
 

@@ -225,6 +225,14 @@ int edp_set_ion_reflection(edp_ctx* ctx, int32_t wall, int32_t on);
  * model number is outside 0-2. A wall whose elastic and inelastic coefficients add up to more than 1 at some
  * impact sets the model error (EDP_ERR_STATE from edp_query_counters), where the reference stops. */
 int edp_set_electron_emission(edp_ctx* ctx, int32_t wall, const edp_see_params* params);
+/* Constant electron emission from a domain wall, PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001), run by
+ * edp_end_ion_cycle every step (pic2d_MainProgram.f90:353): n_per_step macroparticles (the fraction as a
+ * probability) uniformly along the wall, 1e-6 inside it; model 0 thermal (normal speed from the flux-weighted
+ * half-Maxwellian of temperature t_normal_ev), model 1 a beam of energy beam_energy_ev with energy spread t_normal_ev
+ * (beam_energy_ev > 1.5 t_normal_ev, else EDP_ERR_ARG, pic2d_Setup.f90:107-121); tangential components Maxwellian of
+ * t_parallel_ev. n_per_step = 0 switches the wall off. */
+int edp_set_wall_injection(edp_ctx* ctx, int32_t wall, double n_per_step, int32_t model, double t_normal_ev,
+                           double t_parallel_ev, double beam_energy_ev);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
  * when fuse_collisions and this is an ion step, with PERFORM_ELECTRON_NEUTRAL_COLLISIONS */
 int edp_advance_electrons(edp_ctx* ctx);
@@ -353,6 +361,9 @@ int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_
 int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out);
 /* ion-material interaction model of wall's material (0 absorption, 1 specular reflection, 2 ion-induced emission) */
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
+/* constant electron emission of wall (init_bo_NN.dat, pic2d_Setup.f90:86-95): out = {N_electron_constant_emit,
+ * model_constant_emit, T_normal [eV], T_parallel [eV], beam energy [eV]} */
+int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out);
 /* electron-induced emission parameters of wall's material; *enabled = 1 when any of the three models is on */
 int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled);
 int edp_deck_free(edp_deck* d);

@@ -706,6 +706,36 @@ int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, doub
     return n;
 }
 
+// PERFORM_ELECTRON_EMISSION_SETUP pic2d_Setup.f90:618-1001: one local part per wall covering the whole wall
+// (corners of a single cluster), so the count is N_electron_constant_emit and the place spans the wall
+int32_t oracle_wall_injection(double n, int32_t model, double fn, double fp, double vb, int32_t wall, uint32_t step,
+                              uint64_t seed, double xmax, double ymax, const double* maxwell_v,
+                              const double* maxwell_inj, double* out, int32_t cap)
+{
+    const uint32_t key = 0xE1000000u + (uint32_t)wall, stream = 0x43450000u;
+    if (n <= 0.0) return 0;
+    int32_t count = (int32_t)n;
+    uint32_t w0[4];
+    philox_block(key, seed, step, stream, 0u, w0);
+    if (uniform(w0[0]) < n - (double)count) ++count;
+    for (int32_t e = 0; e < count && e < cap; ++e) {
+        uint32_t w[4];
+        philox_block(key, seed, step, stream, 1u + (uint32_t)e, w);
+        double vn = model == 0 ? maxwell_inj_sample(maxwell_inj, uniform(w[1])) * fn
+                               : std::max(0.0, vb + oracle_maxwell_sample(maxwell_v, uniform(w[1])) * fn);
+        double t1 = oracle_maxwell_sample(maxwell_v, uniform(w[2])) * fp;
+        double t2 = oracle_maxwell_sample(maxwell_v, uniform(w[3])) * fp;
+        double r = uniform(w[0]);
+        double* o = out + 5 * e;
+        if (wall == 0) { o[0] = std::min(std::max(r * xmax, 0.0), xmax); o[1] = 1.0e-6; o[2] = t1; o[3] = vn; }
+        else if (wall == 1) { o[0] = std::min(std::max(r * xmax, 0.0), xmax); o[1] = ymax - 1.0e-6; o[2] = t1; o[3] = -vn; }
+        else if (wall == 2) { o[0] = 1.0e-6; o[1] = std::min(std::max(r * ymax, 0.0), ymax); o[2] = vn; o[3] = t1; }
+        else { o[0] = xmax - 1.0e-6; o[1] = std::min(std::max(r * ymax, 0.0), ymax); o[2] = -vn; o[3] = t1; }
+        o[4] = t2;
+    }
+    return count;
+}
+
 // INJECT_REFLECTED_ION pic2d_IonEmissions.f90:374-430 (m > 0, the domain walls)
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,
                         double* out)

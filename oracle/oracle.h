@@ -130,6 +130,16 @@ typedef struct {
 int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
                    uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap);
 
+/* PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001) of one domain wall for one cluster over
+ * [0, xmax] x [0, ymax]: INT(n) electrons plus one with probability n - INT(n), uniform along the wall, 1e-6 inside;
+ * model 0 normal speed GetInjMaxwellVelocity * fn, model 1 MAX(0, vb + GetMaxwellVelocity * fn); tangential
+ * GetMaxwellVelocity * fp. Variates: Philox4x32-10, key {0xE1000000 + wall, seed_lo}, counter {step, 0x43450000,
+ * block, seed_hi}; block 0 word 0 the fraction; block 1 + e words 0-3: place, normal, tangential (in-plane), z.
+ * Rows {x, y, vx, vy, vz}; returns the count. */
+int32_t oracle_wall_injection(double n, int32_t model, double fn, double fp, double vb, int32_t wall, uint32_t step,
+                              uint64_t seed, double xmax, double ymax, const double* maxwell_v,
+                              const double* maxwell_inj, double* out, int32_t cap);
+
 /* INJECT_REFLECTED_ION (pic2d_IonEmissions.f90:374-492) for a domain wall: the ion returns 1e-6 inside the wall
  * (coordinate along the wall clamped into the domain) with its normal velocity reversed; out = {x, y, vx, vy, vz} */
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,

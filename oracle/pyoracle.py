@@ -109,6 +109,9 @@ def lib():
                             _I32, _I32], C.c_int64),
             "oracle_see": ([C.POINTER(See), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                             C.c_uint32, C.c_uint64, C.c_uint32, C.c_double, C.c_double, _D, C.c_int32], C.c_int32),
+            "oracle_wall_injection": ([C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                       C.c_uint32, C.c_uint64, C.c_double, C.c_double, _D, _D, _D, C.c_int32],
+                                      C.c_int32),
             "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _D], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
@@ -297,6 +300,22 @@ class ElectronEmission:
                              dp(out), cap)
         assert n <= cap
         return out[:max(n, 0)], n
+
+
+def wall_injection(wall, n, model, t_normal_ev, t_parallel_ev, beam_ev, energy_factor_ev, step, seed, xmax, ymax):
+    """oracle_wall_injection with the temperatures converted as PREPARE_SETUP_VALUES does (pic2d_Setup.f90:103-126):
+    rows {x, y, vx, vy, vz}."""
+    ef = energy_factor_ev
+    fp = np.sqrt(t_parallel_ev / ef)
+    if model == 0:
+        fn, vb = np.sqrt(t_normal_ev / ef), 0.0
+    else:
+        fn, vb = np.sqrt(0.25 * t_normal_ev ** 2 / (beam_ev * ef)), np.sqrt(beam_ev / ef)
+    v, vi = maxwell_tables()
+    cap = int(n) + 2
+    out = np.zeros((cap, 5))
+    m = lib().oracle_wall_injection(n, model, fn, fp, vb, wall, step, seed, xmax, ymax, dp(v), dp(vi), dp(out), cap)
+    return out[:m]
 
 
 def ion_reflect(wall, x, y, vx, vy, vz, xmax, ymax):
