@@ -168,6 +168,14 @@ module edipic_gpu
        integer(c_int32_t), value :: wall
        type(c_ptr), value :: see              ! c_loc of an interoperable copy of edp_see_params, or c_null_ptr
      end function edp_set_electron_emission
+     ! PERFORM_ELECTRON_EMISSION_SETUP of a wall (init_bo_NN.dat lines 11-20)
+     integer(c_int) function edp_set_wall_injection(ctx, wall, n_per_step, model, t_normal_ev, t_parallel_ev, &
+          beam_energy_ev) bind(C, name="edp_set_wall_injection")
+       import :: c_ptr, c_int, c_int32_t, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: wall, model
+       real(c_double), value :: n_per_step, t_normal_ev, t_parallel_ev, beam_energy_ev
+     end function edp_set_wall_injection
      ! ion-material model 1 (specular reflection) of a wall
      integer(c_int) function edp_set_ion_reflection(ctx, wall, on) bind(C, name="edp_set_ion_reflection")
        import :: c_ptr, c_int, c_int32_t
