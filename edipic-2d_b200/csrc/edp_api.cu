@@ -98,6 +98,24 @@ void rotation(double ax, double ay, double az, double* K)
     K[8] = (1.0 - th + 2.0 * az2) * inv;
 }
 
+// the wall-hit list with room for cap records (any previous list is released: it holds nothing between pushes)
+static int alloc_hits(edp_ctx* c, int64_t cap)
+{
+    edp_hits& h = c->hits;
+    for (void* q : {(void*)h.x, (void*)h.y, (void*)h.vx, (void*)h.vy, (void*)h.vz, (void*)h.id, (void*)h.ws})
+        if (q) cudaFree(q);
+    h = edp_hits();
+    h.cap = cap;
+    TRY(dalloc(c, &h.x, cap));
+    TRY(dalloc(c, &h.y, cap));
+    TRY(dalloc(c, &h.vx, cap));
+    TRY(dalloc(c, &h.vy, cap));
+    TRY(dalloc(c, &h.vz, cap));
+    TRY(dalloc(c, &h.id, cap));
+    TRY(dalloc(c, &h.ws, cap));
+    return EDP_OK;
+}
+
 int alloc_species(edp_ctx* c, int sp, int64_t n)
 {
     if (c->cap[sp] > 0) {
@@ -135,6 +153,7 @@ int alloc_species(edp_ctx* c, int sp, int64_t n)
         // add lists for ionisation products: a small fraction of the electron capacity
         int64_t bc = std::max<int64_t>(65536, cap / 64);
         c->born_cap = bc;
+        if (c->hits.x && c->hits.cap < bc) TRY(alloc_hits(c, bc));   // as large as the electron add list
         {
             edp_born& e = c->born_e;
             e.cap = bc;
@@ -514,6 +533,10 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
     if (p->n_ion_species < 1 || p->n_ion_species > EDP_MAX_ION_SPECIES) return EDP_ERR_ARG;
     if (p->n_subcycles < 1 || (p->n_subcycles % 2) == 0) return EDP_ERR_ARG;
     if (p->n_of_particles_cell < 1 || p->n_inner < 0 || p->n_inner > EDP_MAX_INNER) return EDP_ERR_ARG;
+    for (int n = 0; n < p->n_inner; ++n) {
+        if (!(p->inner_eps[n] >= 0.0) || !std::isfinite(p->inner_eps[n])) return EDP_ERR_ARG;
+        if (p->inner_eps[n] > 0.0 && p->solver != EDP_SOLVER_CG) return EDP_ERR_ARG;   // dielectrics: CG only
+    }
     if (p->solver == EDP_SOLVER_FFTX) {
         if (!p->periodic_x || (p->ncx & (p->ncx - 1)) != 0 || p->ncx > 4096) return EDP_ERR_ARG;
     } else if (p->solver == EDP_SOLVER_CG) {
@@ -547,6 +570,7 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
         kp.jbottom[n] = p->inner_jbottom[n];
         kp.iright[n] = p->inner_iright[n];
         kp.jtop[n] = p->inner_jtop[n];
+        if (p->inner_eps[n] > 0.0) kp.diel_mask |= 1 << n;
     }
     kp.nsub = p->n_subcycles;
     kp.seed_lo = (uint32_t)p->seed;
@@ -622,6 +646,10 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
     }
     if ((r = edp_fields_prepare(c))) return fail(r);
     if (p->solver == EDP_SOLVER_CG && (r = edp_mg_setup(c))) return fail(r);
+    if (kp.diel_mask) {
+        if ((r = edp_dielectrics_setup(c))) return fail(r);
+        if ((r = alloc_hits(c, 65536))) return fail(r);   // grows with the electron add list
+    }
     for (int s = 0; s < 4; ++s) c->phi_wall[s] = p->wall_phi_const[s] + p->wall_phi_var[s] * std::sin(p->wall_phase[s]);
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDP_ERR_CUDA);
     *out = c;
@@ -663,6 +691,7 @@ int edp_destroy(edp_ctx* c)
     delete c->emit_h;
     delete c->see_h;
     F(c->see_dev);
+    F(c->epsx); F(c->epsy); F(c->surf);
     F(c->hits.x); F(c->hits.y); F(c->hits.vx); F(c->hits.vy); F(c->hits.vz); F(c->hits.id); F(c->hits.ws);
     F(c->dc); F(c->dev_small); F(c->mcc_dev); F(c->born_dev); F(c->sel_list); F(c->sel_count);
     if (c->hc) cudaFreeHost(c->hc);
@@ -934,15 +963,7 @@ static int wall_state(edp_ctx* c)
         TRY(dalloc(c, &c->maxwell_inj, rmax_inj + 1));
         EDP_CUDA(c, cudaMemcpy(c->maxwell_inj, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
         TRY(dalloc(c, &c->emit_dev, 1));
-        edp_hits& h = c->hits;
-        h.cap = std::max<int64_t>(65536, c->born_cap);   // the electron add list's size, once allocated
-        TRY(dalloc(c, &h.x, h.cap));
-        TRY(dalloc(c, &h.y, h.cap));
-        TRY(dalloc(c, &h.vx, h.cap));
-        TRY(dalloc(c, &h.vy, h.cap));
-        TRY(dalloc(c, &h.vz, h.cap));
-        TRY(dalloc(c, &h.id, h.cap));
-        TRY(dalloc(c, &h.ws, h.cap));
+        if (!c->hits.x) TRY(alloc_hits(c, std::max<int64_t>(65536, c->born_cap)));   // the electron add list's size
         c->emit_h = new edp_emit_dev();
         memset(c->emit_h, 0, sizeof(edp_emit_dev));
         c->emit_h->maxwell_v = c->maxwell_v;
@@ -1113,7 +1134,7 @@ int edp_advance_electrons(edp_ctx* c)
     reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
     TRY(zero_density(c, 0));
     TRY(edp_launch_push(c, 0, ion_step, fuse));
-    if (c->see_on) TRY(edp_launch_electron_emission(c));
+    if (c->see_on || c->kp.diel_mask) TRY(edp_launch_electron_emission(c));
     return finish_sync(c);
 }
 
@@ -1128,7 +1149,7 @@ int edp_advance_ions(edp_ctx* c)
         TRY(zero_density(c, 1 + s));
         TRY(edp_launch_push(c, 1 + s, true, fuse));
     }
-    if (c->emit_on) TRY(edp_launch_ion_emission(c));
+    if (c->emit_on || c->kp.diel_mask) TRY(edp_launch_ion_emission(c));
     return finish_sync(c);
 }
 
@@ -1269,6 +1290,18 @@ int edp_query_emission(edp_ctx* c, int64_t* out)
     return EDP_OK;
 }
 
+// the outline surface charge between its fixed-point accumulators (2^32 units per charge) and FP64 node values
+__global__ void surf_to_double_kernel(const unsigned long long* s, double* d, int64_t n)
+{
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        d[q] = (double)(long long)s[q] * EDP_FIX_INV;
+}
+__global__ void double_to_surf_kernel(const double* d, unsigned long long* s, int64_t n)
+{
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        s[q] = (unsigned long long)__double2ll_rn(d[q] * EDP_FIX_ONE);
+}
+
 int edp_get_field(edp_ctx* c, int which, double* out)
 {
     if (!c || !out) return EDP_ERR_ARG;
@@ -1285,6 +1318,10 @@ int edp_get_field(edp_ctx* c, int which, double* out)
     case EDP_FIELD_ACC_EY: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, mixed, c->accy, c->acc2, 1, ref, w); break;
     case EDP_FIELD_PHI: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, c->phi, nullptr, 0, ref, w); break;
     case EDP_FIELD_RHO_TOTAL: expand_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->kp, 0, c->rho_total, nullptr, 0, ref, w); break;
+    case EDP_FIELD_SURFACE_CHARGE:   // dielectrics exist on walled domains only, where the two layouts agree
+        if (c->surf) surf_to_double_kernel<<<grid_of(nref), 256, 0, c->stream>>>(c->surf, ref, nref);
+        else cudaMemsetAsync(ref, 0, nref * sizeof(double), c->stream);
+        break;
     default: cudaFree(ref); return edp_fail(c, EDP_ERR_ARG, "edp_get_field: unknown field");
     }
     EDP_CUDA(c, cudaGetLastError());
@@ -1312,6 +1349,13 @@ int edp_set_field(edp_ctx* c, int which, const double* in)
     case EDP_FIELD_ACC_EY: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, mixed, ref, w, c->accy, c->acc2, 1); break;
     case EDP_FIELD_PHI: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, 0, ref, w, c->phi, nullptr, 0); break;
     case EDP_FIELD_RHO_TOTAL: contract_kernel<<<grid_of(nn), 256, 0, c->stream>>>(c->kp, 0, ref, w, c->rho_total, nullptr, 0); break;
+    case EDP_FIELD_SURFACE_CHARGE:
+        if (!c->surf) {
+            cudaFree(ref);
+            return edp_fail(c, EDP_ERR_STATE, "edp_set_field: no dielectric inner objects");
+        }
+        double_to_surf_kernel<<<grid_of(nn), 256, 0, c->stream>>>(ref, c->surf, nn);
+        break;
     default: cudaFree(ref); return edp_fail(c, EDP_ERR_ARG, "edp_set_field: unknown field");
     }
     EDP_CUDA(c, cudaGetLastError());

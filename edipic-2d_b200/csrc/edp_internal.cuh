@@ -124,6 +124,7 @@ struct edp_kparams {
     int32_t ileft[EDP_MAX_INNER], jbottom[EDP_MAX_INNER], iright[EDP_MAX_INNER], jtop[EDP_MAX_INNER];
     int32_t nsub;
     uint32_t seed_lo, seed_hi;
+    int32_t diel_mask;                        // bit n: inner object n is a dielectric
 };
 
 struct edp_ctx {
@@ -186,6 +187,8 @@ struct edp_ctx {
     edp_see_dev* see_dev = nullptr;   // electron-induced electron emission (device copy of see_h)
     edp_see_dev* see_h = nullptr;
     int see_on = 0;                   // electron wall hits are recorded
+    double *epsx = nullptr, *epsy = nullptr;   // face permittivities (dielectric inner objects), node-indexed
+    unsigned long long* surf = nullptr;        // surface charge of the dielectric outlines per node, 2^32 units
     edp_inject_dev inject{};          // constant electron emission (by value into the kernel)
     int inject_on = 0;
     double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
@@ -557,6 +560,7 @@ int edp_launch_download(edp_ctx* c, int species, int64_t cap, int64_t* n_out, do
 int edp_launch_moments(edp_ctx* c, int species, double out[7]);
 int edp_launch_mcc_choose(edp_ctx* c, int64_t n, const double* E, const double* r, int32_t* out);
 int edp_fields_prepare(edp_ctx* c);   // one-time FFT/CG tables
+int edp_dielectrics_setup(edp_ctx* c); // face permittivities and the surface-charge grid (dielectric inner objects)
 int edp_launch_deposit(edp_ctx* c, int species);   // CIC deposit of the whole array without a push
 
 // ------------------------------------------------------------------------------ ion-induced electron emission
@@ -812,4 +816,93 @@ __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, d
     }
     if (edp_u01(b0[3]) < ct) inject();
     return n;
+}
+
+// ------------------------------------------------------------------------------------- dielectric inner objects
+// CHECK_INTERSECTION_WITH_VERTICAL_SEGMENT (pic2d_ElectronWallCollisions.f90:746-779) of the trajectory (xo, yo) ->
+// (x, y) with the segment x = xs, ys0 <= y <= ys1: true and the crossing's y when they cross
+__device__ inline bool edp_cross_vertical(double xo, double yo, double x, double y, double xs, double ys0, double ys1,
+                                          double& yc)
+{
+    if (fmax(xo, x) < xs || fmin(xo, x) > xs || fmax(yo, y) < ys0 || fmin(yo, y) > ys1 || xo == x) return false;
+    yc = yo + (y - yo) * (xs - xo) / (x - xo);
+    if (!isfinite(yc) || yc < ys0 || yc > ys1 || yc < fmin(y, yo) || yc > fmax(y, yo)) return false;
+    return true;
+}
+
+// The trajectory's first crossing of an inner object's outline (FIND_CLOSEST_INTERSECTION_WITH_OBJECT, :649-742,
+// over all inner objects as TRY_ELECTRON_COLL_WITH_INNER_OBJECT :470-557 / TRY_ION_COLL_WITH_INNER_OBJECT,
+// pic2d_IonWallCollisions.f90:391-480; segments 1 left, 2 top, 3 right, 4 bottom; ties keep the earlier one), and
+// the charge q of the absorbed particle given to the two outline nodes next to the crossing when that object is a
+// dielectric (DO_ELECTRON_COLL_WITH_INNER_OBJECT :561-645 / DO_ION_COLL_WITH_INNER_OBJECT): the node fractions
+// are the fractional part of the crossing coordinate, as there. surf holds the charge per node in units of 2^-32.
+// Returns the object index, or -1 when no crossing is found.
+__device__ inline int edp_inner_hit(const edp_kparams& kp, unsigned long long* surf, double X, double Y, double vx,
+                                    double vy, double xmul, double q)
+{
+    const double xo = X - vx * xmul, yo = Y - vy * xmul;
+    int best = -1, bm = 0;
+    double bx = 0.0, by = 0.0, bd = 0.0;
+    for (int n = 0; n < kp.n_inner; ++n) {
+        const double il = kp.ileft[n], ir = kp.iright[n], jb = kp.jbottom[n], jt = kp.jtop[n];
+        for (int m = 1; m <= 4; ++m) {
+            double xc, yc;
+            bool ok;
+            if (m == 1 || m == 3) {
+                xc = m == 1 ? il : ir;
+                ok = edp_cross_vertical(xo, yo, X, Y, xc, jb, jt, yc);
+            } else {   // a horizontal segment is the vertical case with x and y exchanged
+                yc = m == 2 ? jt : jb;
+                ok = edp_cross_vertical(yo, xo, Y, X, yc, il, ir, xc);
+            }
+            if (!ok) continue;
+            const double d = (xc - xo) * (xc - xo) + (yc - yo) * (yc - yo);
+            if (best >= 0 && d >= bd) continue;
+            best = n;
+            bm = m;
+            bx = xc;
+            by = yc;
+            bd = d;
+        }
+    }
+    if (best < 0 || !((kp.diel_mask >> best) & 1)) return best;
+    const int il = kp.ileft[best], ir = kp.iright[best], jb = kp.jbottom[best], jt = kp.jtop[best];
+    const int64_t w = kp.nxg;
+    int64_t na, nb;   // the outline nodes i and i+1 of the reference's numbering
+    double fa;        // fraction of the charge at node i
+    switch (bm) {
+    case 1: {   // left side, coll_direction_flag 3
+        const int k = min((int)(by - jb), jt - jb - 1);
+        na = (int64_t)(jb + k) * w + il;
+        nb = na + w;
+        fa = 1.0 - (by - (double)(int)by);
+        break;
+    }
+    case 2: {   // top side, flag 4
+        const int k = min((int)(bx - il), ir - il - 1);
+        na = (int64_t)jt * w + il + k;
+        nb = na + 1;
+        fa = 1.0 - (bx - (double)(int)bx);
+        break;
+    }
+    case 3: {   // right side from the top, flag 1
+        const int k = min((int)(jt - by), jt - jb - 1);
+        na = (int64_t)(jt - k) * w + ir;
+        nb = na - w;
+        fa = by - (double)(int)by;
+        break;
+    }
+    default: {   // bottom side from the right, flag 2; past the last node the outline closes at (ileft, jbottom)
+        const int k = min((int)(ir - bx), ir - il - 1);
+        na = (int64_t)jb * w + ir - k;
+        nb = na - 1;
+        fa = bx - (double)(int)bx;
+        break;
+    }
+    }
+    const long long qa = __double2ll_rn(fa * EDP_FIX_ONE);
+    const long long qb = 4294967296LL - qa;
+    atomicAdd(&surf[na], (unsigned long long)__double2ll_rn(q * (double)qa));
+    atomicAdd(&surf[nb], (unsigned long long)__double2ll_rn(q * (double)qb));
+    return best;
 }

@@ -18,7 +18,8 @@
 namespace {
 
 __global__ void density_kernel(edp_kparams kp, int precision, int nion, const unsigned long long* const* rho_fix,
-                               const double* const* rho_d, const double* qs, double factor_rho, double* out)
+                               const double* const* rho_d, const double* qs, double factor_rho,
+                               const unsigned long long* surf, double* out)
 {
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
@@ -38,7 +39,10 @@ __global__ void density_kernel(edp_kparams kp, int precision, int nion, const un
             bool ex = (i == 0 || i == kp.ncx), ey = (j == 0 || j == kp.ncy);
             f = (ex && ey) ? 4.0 : ((ex || ey) ? 2.0 : 1.0);
         }
-        out[q] = factor_rho * ((ri * f) - (re * f));
+        double v = (ri * f) - (re * f);
+        // the surface charge of the dielectric outlines, subtracted from rho_e (pic2d_ElectronDynamics.f90:1903-1909)
+        if (surf) v += (double)(long long)surf[q] * EDP_FIX_INV;
+        out[q] = factor_rho * v;
     }
 }
 
@@ -230,13 +234,16 @@ struct CgGeom {
     edp_kparams kp;
     double wall[4];
     double inner[EDP_MAX_INNER];
+    const double *epsx, *epsy;   // face permittivities, or null (vacuum everywhere)
 };
 
+// 1 for a Dirichlet node (walls and metal inner objects, value in *val); the nodes of dielectric objects are unknowns
 __device__ __forceinline__ int cg_node_kind(const CgGeom& g, int i, int j, double* val)
 {
     const edp_kparams& kp = g.kp;
     for (int n = 0; n < kp.n_inner; ++n)
-        if (i >= kp.ileft[n] && i <= kp.iright[n] && j >= kp.jbottom[n] && j <= kp.jtop[n]) {
+        if (!((kp.diel_mask >> n) & 1) && i >= kp.ileft[n] && i <= kp.iright[n] && j >= kp.jbottom[n] &&
+            j <= kp.jtop[n]) {
             *val = g.inner[n];
             return 1;
         }
@@ -265,10 +272,12 @@ __global__ void cg_setup(CgGeom g, const double* __restrict__ rho, int warm, con
             continue;
         }
         double s = rho[q], d;
-        if (cg_node_kind(g, i - 1, j, &d)) s += d;
-        if (cg_node_kind(g, i + 1, j, &d)) s += d;
-        if (cg_node_kind(g, i, j - 1, &d)) s += d;
-        if (cg_node_kind(g, i, j + 1, &d)) s += d;
+        const int64_t w = kp.nxg;
+        const bool e = g.epsx != nullptr;
+        if (cg_node_kind(g, i - 1, j, &d)) s += (e ? g.epsx[q] : 1.0) * d;
+        if (cg_node_kind(g, i + 1, j, &d)) s += (e ? g.epsx[q + 1] : 1.0) * d;
+        if (cg_node_kind(g, i, j - 1, &d)) s += (e ? g.epsy[q] : 1.0) * d;
+        if (cg_node_kind(g, i, j + 1, &d)) s += (e ? g.epsy[q + w] : 1.0) * d;
         b[q] = s;
         phi[q] = (warm == EDP_WARM_ZERO) ? 0.0 : x0[q];
         acc += s * s;
@@ -277,10 +286,22 @@ __global__ void cg_setup(CgGeom g, const double* __restrict__ rho, int warm, con
     if (threadIdx.x == 0) atomicAdd(&scal[0], acc);
 }
 
-__device__ __forceinline__ double apply_A(const edp_kparams& kp, const int8_t* kind, const double* v, int64_t q)
+// the operator of SolverInitialization (pic2d_PETSc_Solver.F90:311-..., sign reversed): sum over the four faces of
+// eps_face (v_q - v_neighbour), Dirichlet neighbours moved to the right-hand side; eps = 1 without dielectrics
+__device__ __forceinline__ double apply_A(const edp_kparams& kp, const int8_t* kind, const double* v, int64_t q,
+                                          const double* ex, const double* ey)
 {
-    double s = 4.0 * v[q];
     const int64_t w = kp.nxg;
+    if (ex) {
+        const double cw = ex[q], ce = ex[q + 1], cs = ey[q], cn = ey[q + w];
+        double s = (cw + ce + cs + cn) * v[q];
+        if (!kind[q - 1]) s -= cw * v[q - 1];
+        if (!kind[q + 1]) s -= ce * v[q + 1];
+        if (!kind[q - w]) s -= cs * v[q - w];
+        if (!kind[q + w]) s -= cn * v[q + w];
+        return s;
+    }
+    double s = 4.0 * v[q];
     if (!kind[q - 1]) s -= v[q - 1];
     if (!kind[q + 1]) s -= v[q + 1];
     if (!kind[q - w]) s -= v[q - w];
@@ -290,7 +311,7 @@ __device__ __forceinline__ double apply_A(const edp_kparams& kp, const int8_t* k
 
 // r = b - A x, p = r, rr accumulated
 __global__ void cg_residual(edp_kparams kp, const int8_t* kind, const double* x, const double* b, double* r, double* p,
-                            double* rr)
+                            double* rr, const double* ex, const double* ey)
 {
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     double acc = 0.0;
@@ -300,7 +321,7 @@ __global__ void cg_residual(edp_kparams kp, const int8_t* kind, const double* x,
             p[q] = 0.0;
             continue;
         }
-        double v = b[q] - apply_A(kp, kind, x, q);
+        double v = b[q] - apply_A(kp, kind, x, q, ex, ey);
         r[q] = v;
         p[q] = v;
         acc += v * v;
@@ -309,7 +330,8 @@ __global__ void cg_residual(edp_kparams kp, const int8_t* kind, const double* x,
     if (threadIdx.x == 0) atomicAdd(rr, acc);
 }
 
-__global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, double* Ap, double* pAp)
+__global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, double* Ap, double* pAp, const double* ex,
+                        const double* ey)
 {
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     double acc = 0.0;
@@ -318,7 +340,7 @@ __global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, dou
             Ap[q] = 0.0;
             continue;
         }
-        double v = apply_A(kp, kind, p, q);
+        double v = apply_A(kp, kind, p, q, ex, ey);
         Ap[q] = v;
         acc += p[q] * v;
     }
@@ -403,6 +425,69 @@ int edp_fields_prepare(edp_ctx* c)
     return EDP_OK;
 }
 
+// SET_EPS_ISHIFTED / SET_EPS_JSHIFTED (pic2d_PETSc_Solver.F90:1724-2045): the permittivity of the face between nodes
+// (i-1, j) and (i, j) (xface) or (i, j-1) and (i, j). A face inside a dielectric takes its eps; a face on the outline
+// of one or two dielectrics averages them with vacuum, or with each other; a face inside a metal object, or on the
+// outline of two, is 0; a face on one metal outline takes the dielectric average or 1.
+static double face_eps(const edp_params& p, int i, int j, bool xface)
+{
+    auto covers = [&](int n) {
+        if (xface)
+            return i - 1 >= p.inner_ileft[n] && i - 1 <= p.inner_iright[n] && j >= p.inner_jbottom[n] &&
+                   j <= p.inner_jtop[n] && i <= p.inner_iright[n];
+        return i >= p.inner_ileft[n] && i <= p.inner_iright[n] && j - 1 >= p.inner_jbottom[n] &&
+               j - 1 <= p.inner_jtop[n] && j <= p.inner_jtop[n];
+    };
+    auto on_outline = [&](int n) {
+        return xface ? (j == p.inner_jtop[n] || j == p.inner_jbottom[n])
+                     : (i == p.inner_ileft[n] || i == p.inner_iright[n]);
+    };
+    double eps = 0.0;
+    int count = 0;
+    bool inside = false;
+    for (int n = 0; n < p.n_inner; ++n) {
+        if (!(p.inner_eps[n] > 0.0) || !covers(n)) continue;
+        if (on_outline(n)) {
+            ++count;
+            eps += p.inner_eps[n];
+        } else {
+            inside = true;
+            eps = p.inner_eps[n];
+            count = 1;
+            break;
+        }
+    }
+    bool on_metal = false;
+    for (int n = 0; n < p.n_inner; ++n) {
+        if (p.inner_eps[n] > 0.0 || !covers(n)) continue;
+        if (!on_outline(n) || on_metal) return 0.0;
+        on_metal = true;
+    }
+    if (on_metal) return count == 0 ? 1.0 : eps / count;
+    if (count == 0) return 1.0;
+    if (count == 1) return inside ? eps : (1.0 + eps) / 2.0;
+    return eps / (double)count;   // two outlines meet (three cannot on non-overlapping rectangles)
+}
+
+int edp_dielectrics_setup(edp_ctx* c)
+{
+    const edp_kparams& kp = c->kp;
+    const int64_t nn = (int64_t)kp.nxg * kp.nyg;
+    std::vector<double> ex(nn, 1.0), ey(nn, 1.0);
+    for (int j = 0; j <= c->p.ncy; ++j)
+        for (int i = 0; i < kp.nxg; ++i) {
+            if (i >= 1) ex[(int64_t)j * kp.nxg + i] = face_eps(c->p, i, j, true);
+            if (j >= 1) ey[(int64_t)j * kp.nxg + i] = face_eps(c->p, i, j, false);
+        }
+    EDP_CUDA(c, cudaMalloc(&c->epsx, nn * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&c->epsy, nn * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&c->surf, nn * sizeof(unsigned long long)));
+    EDP_CUDA(c, cudaMemcpy(c->epsx, ex.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    EDP_CUDA(c, cudaMemcpy(c->epsy, ey.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    EDP_CUDA(c, cudaMemset(c->surf, 0, nn * sizeof(unsigned long long)));
+    return EDP_OK;
+}
+
 int edp_launch_density(edp_ctx* c)
 {
     struct Ptrs {
@@ -420,7 +505,8 @@ int edp_launch_density(edp_ctx* c)
     EDP_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
     ++c->launches;
     density_kernel<<<grid_nodes(c->kp), 256, 0, c->stream>>>(c->kp, c->p.precision, c->p.n_ion_species, d->f, d->d,
-                                                             d->qs, 1.0 / c->p.n_of_particles_cell, c->rho_total);
+                                                             d->qs, 1.0 / c->p.n_of_particles_cell, c->surf,
+                                                             c->rho_total);
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
 }
@@ -462,6 +548,8 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     g.kp = kp;
     for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
     for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    g.epsx = c->epsx;
+    g.epsy = c->epsy;
     // scalars: [0] |b|^2, [1] r.r before iteration 0; iteration k keeps r.z at 2+4k, p.Ap at 3+4k and the
     // residual norm^2 after it at 4(k+1)
     double* scal = nullptr;
@@ -470,6 +558,8 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
     auto rr_at = [&](int k) { return k == 0 ? scal + 1 : scal + 4 * k; };
     const unsigned gr = grid_nodes(kp);
+    // the network was trained on the vacuum operator: with dielectric objects the previous potential starts the solve
+    if (warm == EDP_WARM_LEARNED && kp.diel_mask) warm = EDP_WARM_PREVIOUS;
     const bool learned = warm == EDP_WARM_LEARNED;
     if (learned && !c->ws) {
         cudaFreeAsync(scal, c->stream);
@@ -478,7 +568,8 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     ++c->launches;
     cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
     ++c->launches;
-    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
+    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1],
+                                           c->epsx, c->epsy);
     if (learned) {
         int e = edp_warmstart_forward(c, &scal[1]);
         if (e == EDP_OK) e = edp_warmstart_residual(c);
@@ -528,7 +619,7 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
                 }
             }
             ++c->launches;
-            cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp);
+            cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp, c->epsx, c->epsy);
             ++c->launches;
             cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r,
                                                  rr_at(k + 1));
@@ -564,13 +655,16 @@ extern "C" int edp_warmstart_predict(edp_ctx* c, double* guess_out, double* res_
     g.kp = kp;
     for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
     for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    g.epsx = c->epsx;
+    g.epsy = c->epsy;
     double* scal = nullptr;
     EDP_CUDA(c, cudaMallocAsync(&scal, 2 * sizeof(double), c->stream));
     EDP_CUDA(c, cudaMemsetAsync(scal, 0, 2 * sizeof(double), c->stream));
     const unsigned gr = grid_nodes(kp);
     c->launches += 2;
     cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, EDP_WARM_PREVIOUS, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
-    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1]);
+    cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1],
+                                           c->epsx, c->epsy);
     TRY(edp_warmstart_forward(c, &scal[1]));
     TRY(edp_warmstart_residual(c));
     double h[2];

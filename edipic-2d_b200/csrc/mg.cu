@@ -260,7 +260,7 @@ int edp_mg_setup(edp_ctx* c)
                 const int i = I << l, j = J << l;
                 int8_t k = (i == 0 || j == 0 || i == p.ncx || j == p.ncy) ? 1 : 0;
                 for (int o = 0; o < p.n_inner; ++o)
-                    if (i >= p.inner_ileft[o] && i <= p.inner_iright[o] && j >= p.inner_jbottom[o] && j <= p.inner_jtop[o])
+                    if (!(p.inner_eps[o] > 0.0) && i >= p.inner_ileft[o] && i <= p.inner_iright[o] && j >= p.inner_jbottom[o] && j <= p.inner_jtop[o])
                         k = 1;
                 h[(size_t)J * w + I] = k;
             }

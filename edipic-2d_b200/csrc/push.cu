@@ -218,6 +218,9 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
                   (nj > kp.jbottom[n] || (nj == kp.jbottom[n] && ny > 0.0f)) && nj < kp.jtop[n];
         if (in) {
             atomicAdd(&s.cnt[4 + n], 1ull);
+            if ((kp.diel_mask >> n) & 1)   // its outline takes the charge: the crossing is found after the push
+                record_hit(a.hits, a.dc, 4 + n, ION ? a.species - 1 : 0, (double)ni + (double)nx,
+                           (double)nj + (double)ny, vx, vy, vz, id);
             return false;
         }
     }
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             a.P.x[k] = -1.0e30;
             atomicAdd(&cnt[obj], 1ull);
             atomicAdd(&cnt[17], 1ull);
-            if (a.emit_on && obj < 4)
+            if ((a.emit_on && obj < 4) || (obj >= 4 && ((kp.diel_mask >> (obj - 4)) & 1)))
                 record_hit(a.hits, a.dc, obj, a.is_ion ? a.species - 1 : 0, X, Y, vx, vy, vz, a.P.id[k]);
             continue;
         }
@@ -976,13 +979,23 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
 // pic2d_IonWallCollisions.f90:3-303, which first clamps the coordinate along the wall into the domain): a reflecting
 // wall returns the ion specularly, 1e-6 inside the wall, through the ion add list (INJECT_REFLECTED_ION,
 // pic2d_IonEmissions.f90:374-492); otherwise PROCESS_ION_INDUCED_ELECTRON_EMISSION.
+struct IonCharges {
+    double qs[EDP_MAX_ION_SPECIES];
+};
+
 __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp_emit_dev* em, edp_born_dev* born,
-                                                           edp_dev_counters* dc, edp_kparams kp, uint32_t step)
+                                                           edp_dev_counters* dc, edp_kparams kp, uint32_t step,
+                                                           unsigned long long* surf, IonCharges qs)
 {
     const int64_t n = min((int64_t)dc->hit_count, h.cap);
     const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int ws = h.ws[k], wall = ws & 255, s = ws >> 8;
+        if (wall >= 4) {   // a dielectric inner object: charge Qs on its outline (ions move V N_subcycles per step)
+            edp_inner_hit(kp, surf, h.x[k], h.y[k], h.vx[k], h.vy[k], (double)kp.nsub, qs.qs[s]);
+            continue;
+        }
+        if (!em) continue;
         const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
         if (em->reflect[wall]) {
             double v[3] = {h.vx[k], h.vy[k], h.vz[k]};
@@ -1008,12 +1021,18 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
 // PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION for every electron wall hit of this step (the coordinate along the wall
 // clamped into the domain first, pic2d_ElectronWallCollisions.f90:21, :93, :165, :237)
 __global__ void __launch_bounds__(256) electron_emission_kernel(edp_hits h, const edp_see_dev* sd, edp_born born_e,
-                                                                edp_dev_counters* dc, edp_kparams kp, uint32_t step)
+                                                                edp_dev_counters* dc, edp_kparams kp, uint32_t step,
+                                                                unsigned long long* surf)
 {
     const int64_t n = min((int64_t)dc->hit_count, h.cap);
     const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int wall = h.ws[k] & 255;
+        if (wall >= 4) {   // a dielectric inner object: its outline gets the electron's charge
+            edp_inner_hit(kp, surf, h.x[k], h.y[k], h.vx[k], h.vy[k], 1.0, -1.0);
+            continue;
+        }
+        if (!sd) continue;
         const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
         const int m = edp_see_electrons(sd, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
                                         kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
@@ -1027,8 +1046,8 @@ __global__ void __launch_bounds__(256) electron_emission_kernel(edp_hits h, cons
 int edp_launch_electron_emission(edp_ctx* c)
 {
     ++c->launches;
-    electron_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->see_dev, c->born_e, c->dc, c->kp,
-                                                           (uint32_t)c->t_cntr);
+    electron_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->see_on ? c->see_dev : nullptr, c->born_e,
+                                                           c->dc, c->kp, (uint32_t)c->t_cntr, c->surf);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));
     return EDP_OK;
@@ -1090,8 +1109,10 @@ int edp_launch_wall_injection(edp_ctx* c)
 int edp_launch_ion_emission(edp_ctx* c)
 {
     ++c->launches;
-    ion_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->emit_dev, c->born_dev, c->dc, c->kp,
-                                                      (uint32_t)c->t_cntr);
+    IonCharges qs;
+    for (int s = 0; s < EDP_MAX_ION_SPECIES; ++s) qs.qs[s] = (double)c->p.ion_charge[s];
+    ion_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->emit_on ? c->emit_dev : nullptr, c->born_dev,
+                                                      c->dc, c->kp, (uint32_t)c->t_cntr, c->surf, qs);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));
     return EDP_OK;

@@ -11,14 +11,15 @@ import numpy as np
 
 from . import _abi
 from ._abi import SeeParams  # noqa: F401
-from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL, IONS,
+from ._abi import (ELECTRONS, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_EX, FIELD_EY, FIELD_PHI, FIELD_RHO_TOTAL,
+                   FIELD_SURFACE_CHARGE, IONS,
                    PREC_FP64, PREC_MIXED, PRECOND_MG, PRECOND_NONE, SOLVER_CG, SOLVER_FFTX, WARM_LEARNED, WARM_PREVIOUS,
                    WARM_USER, WARM_ZERO, Counters,
                    Params, Tables)
 
 __all__ = ["Simulation", "EdpError", "read_deck", "library", "Params", "Tables", "Counters", "ELECTRONS", "IONS",
            "PREC_MIXED", "PREC_FP64", "SOLVER_FFTX", "SOLVER_CG", "FIELD_EX", "FIELD_EY", "FIELD_ACC_EX",
-           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER", "WARM_LEARNED",
+           "FIELD_ACC_EY", "FIELD_PHI", "FIELD_RHO_TOTAL", "FIELD_SURFACE_CHARGE", "WARM_ZERO", "WARM_PREVIOUS", "WARM_USER", "WARM_LEARNED",
            "PRECOND_NONE", "PRECOND_MG"]
 
 _lib = None

@@ -12,14 +12,14 @@ MAX_COLPROC = 8
 MAX_SEG = 32
 MAX_SPECIES = 1 + MAX_ION
 N_HIT = 4 + MAX_INNER
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_BOUNDS, ERR_NOT_CONVERGED, ERR_TIMEOUT, ERR_STATE, ERR_IO = \
     0, -1, -2, -3, -4, -5, -6, -7, -8
 PREC_MIXED, PREC_FP64 = 0, 1
 SOLVER_FFTX, SOLVER_CG = 0, 1
 ELECTRONS, IONS = 0, 1
-FIELD_EX, FIELD_EY, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_PHI, FIELD_RHO_TOTAL = range(6)
+FIELD_EX, FIELD_EY, FIELD_ACC_EX, FIELD_ACC_EY, FIELD_PHI, FIELD_RHO_TOTAL, FIELD_SURFACE_CHARGE = range(7)
 WARM_ZERO, WARM_PREVIOUS, WARM_USER = 0, 1, 2
 PRECOND_NONE, PRECOND_MG = 0, 1
 WARM_LEARNED = 3
@@ -47,6 +47,7 @@ class Params(C.Structure):
         ("inner_phi", C.c_double * MAX_INNER),
         ("seed", C.c_uint64), ("precision", C.c_int32), ("solver", C.c_int32), ("sort_every", C.c_int32),
         ("fuse_collisions", C.c_int32), ("capacity", C.c_int64 * MAX_SPECIES),
+        ("inner_eps", C.c_double * MAX_INNER),
     ]
 
 

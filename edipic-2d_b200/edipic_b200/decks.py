@@ -99,7 +99,8 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         objs = [(2, [(0, 0, 0, gmj)]), (1, [(0, gmj, gmi, gmj)]), (2, [(gmi, 0, gmi, gmj)]), (1, [(0, 0, gmi, 0)])]
     else:
         objs = [(1, [(0, 0, 0, gmj)]), (1, [(0, gmj, gmi, gmj)]), (1, [(gmi, 0, gmi, gmj)]), (1, [(0, 0, gmi, 0)])]
-    inner_list = [inner] if inner else []
+    # inner objects: (ileft, jbottom, iright, jtop, phi) for a metal one, (..., phi, eps) for a dielectric one
+    inner_list = ([inner] if isinstance(inner, tuple) else list(inner)) if inner else []
     cf = [
         "---dddd.ddddddd----- scale electron temperature [eV]", f"   {T_SCALE_EV:12.7f}",
         "---+d.dddddddE+dd--- scale electron density [m^-3]", f"   {N_SCALE_M3:14.7E}",
@@ -118,8 +119,9 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         cf += [f"===dd===dd=== object type, number of segments // #{k + 1}", f"   {ty:2d}   {len(segs):2d}",
                "---dddddd---dddddd---dddddd---dddddd--- segment start X/Y end X/Y"]
         cf += [f"   {a:6d}   {b:6d}   {c:6d}   {d:6d}" for (a, b, c, d) in segs]
-    for (il, jb, ir, jt, _phi) in inner_list:
-        cf += ["===dd=== object type", f"   {1:2d}",
+    for obj in inner_list:
+        il, jb, ir, jt = obj[:4]
+        cf += ["===dd=== object type", f"   {4 if len(obj) > 5 else 1:2d}",
                "---dddddd---dddddd---dddddd---dddddd--- left bottom X/Y, right top X/Y",
                f"   {il:6d}   {jb:6d}   {ir:6d}   {jt:6d}"]
     w("init_configuration.dat", cf)
@@ -156,9 +158,9 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         "-------d------- ions sense Z-electric field", f"       {0:1d}",
     ])
 
-    def bo(n, phi, amp=0.0, mhz=0.0, inj=(0.0, 0, 0.0, 0.0, 0.0)):
+    def bo(n, phi, amp=0.0, mhz=0.0, inj=(0.0, 0, 0.0, 0.0, 0.0), material="METAL1"):
         w(f"init_bo_{n:02d}.dat", [
-            "------AAAAAA--- material", "      METAL1",
+            "------AAAAAA--- material", f"      {material}",
             "---ddddd.ddd--- constant potential [V]", f"   {phi:9.3f}",
             "---ddddd.ddd--- amplitude of oscillations [V]", f"   {amp:9.3f}",
             "---ddddd.ddd--- frequency [MHz]", f"   {mhz:9.3f}",
@@ -225,6 +227,7 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
                 "--dddddd.ddd- temperature of emitted electrons [eV]", f"  {t:10.3f}",
             ]
     w("init_material_METAL1.dat", mat)
+    mat_rest = mat[2:]
     wp = wall_potentials or {}
     for k, (ty, _s) in enumerate(objs):
         if ty == 1:
@@ -233,8 +236,13 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
                 amp, mhz = cfg["top_rf"]
             wall = (2, 1, 3, 0)[k]   # objects: left, above, right, below
             bo(k + 1, wp.get(k + 1, 0.0), amp, mhz, (wall_injection or {}).get(wall, (0.0, 0, 0.0, 0.0, 0.0)))
-    for q, (_a, _b, _c, _d, phi) in enumerate(inner_list):
-        bo(len(objs) + q + 1, phi)
+    for q, obj in enumerate(inner_list):
+        if len(obj) > 5:   # dielectric: its own material, whose first value is the permittivity
+            mname = f"DIEL{q:02d}"
+            w(f"init_material_{mname}.dat", ["------dd.ddd- dielectric constant", f"      {obj[5]:6.3f}"] + mat_rest)
+            bo(len(objs) + q + 1, obj[4], material=mname)
+        else:
+            bo(len(objs) + q + 1, obj[4])
 
     if not collisions:
         w("init_neutrals.dat", ["----------dd--- number of neutral species", f"          {0:2d}"])

@@ -10,7 +10,7 @@ module edipic_gpu
   use, intrinsic :: iso_c_binding
   implicit none
 
-  integer(c_int), parameter :: EDP_ABI_VERSION = 1
+  integer(c_int), parameter :: EDP_ABI_VERSION = 2
   integer(c_int), parameter :: EDP_MAX_ION_SPECIES = 4, EDP_MAX_INNER = 4, EDP_MAX_COLPROC = 8, EDP_MAX_SEGMENTS = 32
   integer(c_int), parameter :: EDP_PREC_MIXED = 0, EDP_PREC_FP64 = 1, EDP_SOLVER_FFTX = 0, EDP_SOLVER_CG = 1
   integer(c_int), parameter :: EDP_ELECTRONS = 0, EDP_IONS = 1
@@ -32,6 +32,7 @@ module edipic_gpu
      integer(c_int64_t) :: seed
      integer(c_int32_t) :: precision, solver, sort_every, fuse_collisions
      integer(c_int64_t) :: capacity(1 + EDP_MAX_ION_SPECIES)
+     real(c_double) :: inner_eps(EDP_MAX_INNER)      ! 0 metal, > 0 dielectric permittivity
   end type edp_params
 
   type, bind(C) :: edp_tables

@@ -366,7 +366,22 @@ int read_deck(const std::string& dir, edp_deck* d)
     if (nio > EDP_MAX_INNER) return EDP_ERR_IO;
     p.n_inner = (int32_t)nio;
     for (int n = 0; n < nio; ++n) {
-        if (otype[nbo + n] != 1) return EDP_ERR_IO;
+        // METAL_WALL = 1 or DIELECTRIC = 4 (pic2d_Modules.f90:143-147); a dielectric's permittivity is the first
+        // value of its material file, (6x,f6.3) (pic2d_Materials.f90:81-82)
+        if (otype[nbo + n] != 1 && otype[nbo + n] != 4) return EDP_ERR_IO;
+        p.inner_eps[n] = 0.0;
+        if (otype[nbo + n] == 4) {
+            if (p.periodic_x) return EDP_ERR_IO;   // dielectrics: CG solver (walled domain) only
+            char name[32];
+            snprintf(name, sizeof(name), "/init_bo_%02d.dat", (int)(nbo + n + 1));
+            Lines bf(dir + name);
+            if (!bf.ok || !bf.next(L) || !bf.next(L)) return EDP_ERR_IO;
+            const std::string mat = (L + "      ").substr(6, 6);
+            Lines mf(dir + "/init_material_" + mat + ".dat");
+            double eps = 0.0;
+            if (!mf.ok || !mf.next(L) || !mf.next(L) || !freal(L, 6, 6, &eps) || !(eps > 0.0)) return EDP_ERR_IO;
+            p.inner_eps[n] = eps;
+        }
         p.inner_ileft[n] = inner[n].is;
         p.inner_jbottom[n] = inner[n].js;
         p.inner_iright[n] = inner[n].ie;

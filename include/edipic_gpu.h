@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define EDP_ABI_VERSION 1
+#define EDP_ABI_VERSION 2
 
 enum edp_status {
     EDP_OK = 0,
@@ -49,7 +49,9 @@ enum edp_solver { EDP_SOLVER_FFTX = 0, EDP_SOLVER_CG = 1 };
 enum edp_species { EDP_ELECTRONS = 0, EDP_IONS = 1 /* ion species s is EDP_IONS + s */ };
 enum edp_field {
     EDP_FIELD_EX = 0, EDP_FIELD_EY = 1, EDP_FIELD_ACC_EX = 2, EDP_FIELD_ACC_EY = 3,
-    EDP_FIELD_PHI = 4, EDP_FIELD_RHO_TOTAL = 5
+    EDP_FIELD_PHI = 4, EDP_FIELD_RHO_TOTAL = 5,
+    EDP_FIELD_SURFACE_CHARGE = 6   /* charge on the outlines of the dielectric inner objects per node, in macroparticle
+                                      charges (whole_object%surface_charge); zero without dielectrics */
 };
 /* initial guess of edp_field_cg. LEARNED: the previous potential plus the update the loaded network
  * (edp_warmstart_load) predicts from its residual against the new density; the previous potential is kept
@@ -95,6 +97,11 @@ typedef struct edp_params {
     int32_t sort_every;             /* cell sort period in steps (mixed precision), 0 = never */
     int32_t fuse_collisions;        /* 1: MCC/RCX run in the push epilogue (same variates as the separate pass) */
     int64_t capacity[1 + EDP_MAX_ION_SPECIES];      /* particle slots per species (0 = automatic) */
+    /* inner object k: 0 = METAL_WALL (potential inner_phi[k]); > 0 = DIELECTRIC with that permittivity (eps_diel of
+       its material): its nodes are unknowns of the CG solve with the face permittivities of SET_EPS_ISHIFTED /
+       SET_EPS_JSHIFTED (pic2d_PETSc_Solver.F90:1724-2045) and the particles it absorbs charge its outline
+       (DO_ELECTRON_COLL_WITH_INNER_OBJECT, pic2d_ElectronWallCollisions.f90:561-645). CG solver only. */
+    double inner_eps[EDP_MAX_INNER];
 } edp_params;
 
 /* Collision and sampling tables, as built on the host by INITIATE_ELECTRON_NEUTRAL_COLLISIONS

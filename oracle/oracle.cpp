@@ -736,6 +736,101 @@ int32_t oracle_wall_injection(double n, int32_t model, double fn, double fp, dou
     return count;
 }
 
+// CHECK_INTERSECTION_WITH_VERTICAL_SEGMENT / _HORIZONTAL_SEGMENT pic2d_ElectronWallCollisions.f90:746-812
+static bool cross_vertical(double xorg, double yorg, double x, double y, double xseg, double ymin, double ymax,
+                           double* ycross)
+{
+    if (std::max(xorg, x) < xseg || std::min(xorg, x) > xseg) return false;
+    if (std::max(yorg, y) < ymin || std::min(yorg, y) > ymax) return false;
+    if (xorg == x) return false;
+    double yc = yorg + (y - yorg) * (xseg - xorg) / (x - xorg);
+    if (!std::isfinite(yc) || yc < ymin || yc > ymax || yc < std::min(y, yorg) || yc > std::max(y, yorg)) return false;
+    *ycross = yc;
+    return true;
+}
+static bool cross_horizontal(double xorg, double yorg, double x, double y, double yseg, double xmin, double xmax,
+                             double* xcross)
+{
+    if (std::max(yorg, y) < yseg || std::min(yorg, y) > yseg) return false;
+    if (std::max(xorg, x) < xmin || std::min(xorg, x) > xmax) return false;
+    if (yorg == y) return false;
+    double xc = xorg + (x - xorg) * (yseg - yorg) / (y - yorg);
+    if (!std::isfinite(xc) || xc < xmin || xc > xmax || xc < std::min(x, xorg) || xc > std::max(x, xorg)) return false;
+    *xcross = xc;
+    return true;
+}
+
+int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double x, double y, double vx, double vy,
+                         double xmul, double q, double* surf)
+{
+    const double xorg = x - vx * xmul, yorg = y - vy * xmul;
+    int n_do = -1, mcross = -1;
+    double xcross = 0.0, ycross = 0.0, distorg = 0.0;
+    for (int n = 0; n < g->n_inner; ++n)
+        for (int m = 1; m <= 4; ++m) {   // FIND_CLOSEST_INTERSECTION_WITH_OBJECT :649-742, segments as :277-300
+            double xc = 0.0, yc = 0.0;
+            bool ok;
+            if (m == 1 || m == 3) {
+                xc = m == 1 ? g->ileft[n] : g->iright[n];
+                ok = cross_vertical(xorg, yorg, x, y, xc, g->jbottom[n], g->jtop[n], &yc);
+            } else {
+                yc = m == 2 ? g->jtop[n] : g->jbottom[n];
+                ok = cross_horizontal(xorg, yorg, x, y, yc, g->ileft[n], g->iright[n], &xc);
+            }
+            if (!ok) continue;
+            double d = (xc - xorg) * (xc - xorg) + (yc - yorg) * (yc - yorg);
+            if (mcross != -1 && d >= distorg) continue;
+            n_do = n;
+            mcross = m;
+            xcross = xc;
+            ycross = yc;
+            distorg = d;
+        }
+    if (n_do < 0 || !(inner_eps[n_do] > 0.0)) return n_do;
+    // the outline numbering of DO_ELECTRON_COLL_WITH_INNER_OBJECT :582-640: position 1 = (ileft, jbottom), up the
+    // left side, along the top, down the right side, back along the bottom
+    const int il = g->ileft[n_do], ir = g->iright[n_do], jb = g->jbottom[n_do], jt = g->jtop[n_do];
+    const int i_left_top = jt - jb + 1, i_right_top = i_left_top + ir - il, i_right_bottom = i_right_top + jt - jb;
+    const int i_left_bottom_bis = i_right_bottom + ir - il - 1;
+    auto pos_node = [&](int pos) -> int64_t {
+        if (pos <= i_left_top) return node(g, il, jb + pos - 1);
+        if (pos <= i_right_top) return node(g, il + pos - i_left_top, jt);
+        if (pos <= i_right_bottom) return node(g, ir, jt - (pos - i_right_top));
+        return node(g, ir - (pos - i_right_bottom), jb);
+    };
+    int i = 0, ip1 = 0;
+    double dqi = 0.0, dqip1 = 0.0;
+    switch (mcross) {
+    case 1:   // coll_direction_flag 3
+        i = std::min((int)(ycross - jb) + 1, i_left_top - 1);
+        dqip1 = ycross - (int)ycross;
+        dqi = 1.0 - dqip1;
+        ip1 = i + 1;
+        break;
+    case 2:   // flag 4
+        i = std::min((int)(xcross - il) + i_left_top, i_right_top - 1);
+        dqip1 = xcross - (int)xcross;
+        dqi = 1.0 - dqip1;
+        ip1 = i + 1;
+        break;
+    case 3:   // flag 1
+        i = std::min((int)(jt - ycross) + i_right_top, i_right_bottom - 1);
+        dqi = ycross - (int)ycross;
+        dqip1 = 1.0 - dqi;
+        ip1 = i + 1;
+        break;
+    default:  // flag 2
+        i = std::min((int)(ir - xcross) + i_right_bottom, i_left_bottom_bis);
+        dqi = xcross - (int)xcross;
+        dqip1 = 1.0 - dqi;
+        ip1 = (i == i_left_bottom_bis) ? 1 : i + 1;
+        break;
+    }
+    surf[pos_node(i)] += q * dqi;
+    surf[pos_node(ip1)] += q * dqip1;
+    return n_do;
+}
+
 // INJECT_REFLECTED_ION pic2d_IonEmissions.f90:374-430 (m > 0, the domain walls)
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,
                         double* out)
@@ -1217,16 +1312,82 @@ static int node_kind(const oracle_geom_t* g, int i, int j, int* inner)
     return 0;
 }
 
+// SET_EPS_ISHIFTED (x face between nodes (i-1, j) and (i, j)) / SET_EPS_JSHIFTED (y face between (i, j-1) and
+// (i, j)), pic2d_PETSc_Solver.F90:1724-2045, for the inner objects of g (eps[n] > 0 dielectric, 0 metal)
+static double set_eps_face(const oracle_geom_t* g, const double* eps_of, int i, int j, bool xface)
+{
+    double eps = 0.0;
+    int count = 0;
+    bool inside_dielectric = false, on_metal_surface = false;
+    for (int pass = 0; pass < 2; ++pass)   // pass 0: dielectric objects, pass 1: metal objects
+        for (int n = 0; n < g->n_inner; ++n) {
+            const bool metal = !(eps_of[n] > 0.0);
+            if (metal != (pass == 1)) continue;
+            const int il = g->ileft[n], ir = g->iright[n], jb = g->jbottom[n], jt = g->jtop[n];
+            bool covered, outline;
+            if (xface) {
+                covered = !(i - 1 < il || i - 1 > ir || j < jb || j > jt || i > ir);
+                outline = j == jt || j == jb;
+            } else {
+                covered = !(i < il || i > ir || j - 1 < jb || j - 1 > jt || j > jt);
+                outline = i == il || i == ir;
+            }
+            if (!covered) continue;
+            if (pass == 0) {
+                if (outline) {
+                    ++count;
+                    eps += eps_of[n];
+                } else {
+                    inside_dielectric = true;
+                    eps = eps_of[n];
+                    count = 1;
+                    break;
+                }
+            } else {
+                if (!outline || on_metal_surface) return 0.0;
+                on_metal_surface = true;
+            }
+        }
+    if (on_metal_surface) return count == 0 ? 1.0 : eps / count;
+    if (count == 0) return 1.0;
+    if (count == 1) return inside_dielectric ? eps : (1.0 + eps) / 2.0;
+    return eps / (double)count;
+}
+
+static int32_t cg_general(const oracle_geom_t* g, const double* rho, const double* wall_phi, const double* inner_phi,
+                          const double* inner_eps, double rtol, int32_t max_it, double* phi, double* relres_out);
+
 int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho, const double* wall_phi, const double* inner_phi,
                         double rtol, int32_t max_it, double* phi, double* relres_out)
+{
+    return cg_general(g, rho, wall_phi, inner_phi, nullptr, rtol, max_it, phi, relres_out);
+}
+
+int32_t oracle_cg_solve_eps(const oracle_geom_t* g, const double* rho, const double* wall_phi, const double* inner_phi,
+                            const double* inner_eps, double rtol, int32_t max_it, double* phi, double* relres_out)
+{
+    return cg_general(g, rho, wall_phi, inner_phi, inner_eps, rtol, max_it, phi, relres_out);
+}
+
+static int32_t cg_general(const oracle_geom_t* g, const double* rho, const double* wall_phi, const double* inner_phi,
+                          const double* inner_eps, double rtol, int32_t max_it, double* phi, double* relres_out)
 {
     const int nx = oracle_nx_nodes(g), J = g->ncy;
     const int64_t nn = (int64_t)nx * (J + 1);
     std::vector<int8_t> kind(nn);
+    // face permittivities of the operator: ex at node (i, j) = face to (i-1, j); ey = face to (i, j-1)
+    std::vector<double> ex(nn, 1.0), ey(nn, 1.0);
+    if (inner_eps)
+        for (int j = 0; j <= J; ++j)
+            for (int i = 0; i < nx; ++i) {
+                if (i >= 1) ex[node(g, i, j)] = set_eps_face(g, inner_eps, i, j, true);
+                if (j >= 1) ey[node(g, i, j)] = set_eps_face(g, inner_eps, i, j, false);
+            }
     for (int j = 0; j <= J; ++j)
         for (int i = 0; i < nx; ++i) {
             int w = 0;
             int k = node_kind(g, i, j, &w);
+            if (k == 2 && inner_eps && inner_eps[w] > 0.0) k = 0;   // dielectric nodes are unknowns
             kind[node(g, i, j)] = (int8_t)k;
             if (k == 1) phi[node(g, i, j)] = wall_phi[-1 - w];
             if (k == 2) phi[node(g, i, j)] = inner_phi[w];
@@ -1234,6 +1395,15 @@ int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho, const double*
     // A = -(5-point Laplacian) on unknown nodes, b = rho + Dirichlet neighbours
     std::vector<double> b(nn, 0.0), x(nn, 0.0), r(nn, 0.0), p(nn, 0.0), Ap(nn, 0.0);
     const int di[4] = {-1, 1, 0, 0}, dj[4] = {0, 0, -1, 1};
+    // the face towards neighbour d of node q
+    auto face = [&](int64_t q, int d) {
+        switch (d) {
+        case 0: return ex[q];
+        case 1: return ex[q + 1];
+        case 2: return ey[q];
+        default: return ey[q + nx];
+        }
+    };
     for (int j = 1; j < J; ++j)
         for (int i = 1; i < nx - 1; ++i) {
             int64_t q = node(g, i, j);
@@ -1241,7 +1411,7 @@ int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho, const double*
             double s = rho[q];
             for (int d = 0; d < 4; ++d) {
                 int64_t q2 = node(g, i + di[d], j + dj[d]);
-                if (kind[q2]) s += phi[q2];
+                if (kind[q2]) s += face(q, d) * phi[q2];
             }
             b[q] = s;
             x[q] = phi[q];
@@ -1251,10 +1421,11 @@ int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho, const double*
             for (int i = 1; i < nx - 1; ++i) {
                 int64_t q = node(g, i, j);
                 if (kind[q]) continue;
-                double s = 4.0 * in[q];
+                double s = 0.0;
                 for (int d = 0; d < 4; ++d) {
                     int64_t q2 = node(g, i + di[d], j + dj[d]);
-                    if (!kind[q2]) s -= in[q2];
+                    s += face(q, d) * in[q];
+                    if (!kind[q2]) s -= face(q, d) * in[q2];
                 }
                 out[q] = s;
             }

@@ -235,6 +235,19 @@ void oracle_efield(const oracle_geom_t* g, const double* phi, double factor2, do
 int32_t oracle_cg_solve(const oracle_geom_t* g, const double* rho_total, const double* wall_phi /*4*/,
                         const double* inner_phi, double rtol, int32_t max_it, double* phi, double* relres_out);
 
+/* the CG solve with dielectric inner objects: inner_eps[n] > 0 makes object n a dielectric of that permittivity
+ * (its nodes unknowns, the faces weighted as SET_EPS_ISHIFTED/JSHIFTED, pic2d_PETSc_Solver.F90:1724-2045) */
+int32_t oracle_cg_solve_eps(const oracle_geom_t* g, const double* rho_total, const double* wall_phi,
+                            const double* inner_phi, const double* inner_eps, double rtol, int32_t max_it, double* phi,
+                            double* relres_out);
+/* TRY_ELECTRON_COLL_WITH_INNER_OBJECT / TRY_ION_COLL_WITH_INNER_OBJECT and DO_*_COLL_WITH_INNER_OBJECT
+ * (pic2d_ElectronWallCollisions.f90:470-742, pic2d_IonWallCollisions.f90:391-560): the first crossing of the
+ * trajectory (x - vx*xmul, y - vy*xmul) -> (x, y) with an inner object's outline, and the charge q (-1 electrons,
+ * Qs ions) split over the two outline nodes next to it when that object is a dielectric (inner_eps > 0), added to
+ * surf on the node grid. Returns the object, -1 when the trajectory crosses none. */
+int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double x, double y, double vx, double vy,
+                         double xmul, double q, double* surf);
+
 /* ---------------------------------------------------------------- whole cycle (CPU baseline) */
 typedef struct {
     oracle_geom_t geom;

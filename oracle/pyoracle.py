@@ -112,6 +112,9 @@ def lib():
             "oracle_wall_injection": ([C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
                                        C.c_uint32, C.c_uint64, C.c_double, C.c_double, _D, _D, _D, C.c_int32],
                                       C.c_int32),
+            "oracle_cg_solve_eps": ([C.POINTER(Geom), _D, _D, _D, _D, C.c_double, C.c_int32, _D, _D], C.c_int32),
+            "oracle_inner_hit": ([C.POINTER(Geom), _D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, _D], C.c_int32),
             "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _D], None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
@@ -364,6 +367,23 @@ def cg_solve(g, rho_total, wall_phi, inner_phi, rtol=1e-12, max_it=100000, phi0=
                                dp(np.asarray(list(inner_phi) + [0.0] * 4, dtype=np.float64)), rtol, max_it, dp(phi),
                                C.byref(rel))
     return phi, it, rel.value
+
+
+def cg_solve_eps(g, rho_total, wall_phi, inner_phi, inner_eps, rtol=1e-12, max_it=100000, phi0=None):
+    """oracle_cg_solve_eps: the CG solve with dielectric inner objects (inner_eps[n] > 0)."""
+    phi = np.zeros(nodes_shape(g)) if phi0 is None else np.array(phi0, dtype=np.float64)
+    rel = C.c_double()
+    pad = lambda v: dp(np.asarray(list(v) + [0.0] * (4 - len(v)), dtype=np.float64))
+    it = lib().oracle_cg_solve_eps(C.byref(g), dp(np.ascontiguousarray(rho_total)),
+                                   dp(np.asarray(wall_phi, dtype=np.float64)), pad(inner_phi), pad(inner_eps), rtol,
+                                   max_it, dp(phi), C.byref(rel))
+    return phi, it, rel.value
+
+
+def inner_hit(g, inner_eps, x, y, vx, vy, xmul, q, surf):
+    """oracle_inner_hit: adds the outline charge of one absorbed particle to surf (node grid); returns the object."""
+    e = np.asarray(list(inner_eps) + [0.0] * (4 - len(inner_eps)), dtype=np.float64)
+    return lib().oracle_inner_hit(C.byref(g), dp(e), x, y, vx, vy, xmul, q, dp(surf))
 
 
 # ------------------------------------------------------------------------------ collision tables
