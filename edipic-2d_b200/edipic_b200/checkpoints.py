@@ -14,9 +14,9 @@ max_N_ions(s), N_ions(s) per species and last len_surf_charge. Values are in the
 
 The device keeps no WELL19937a stream (its variates are Philox keyed by particle id and step), so a checkpoint written
 here carries either the RNG states of the checkpoint the run was loaded from, or per-rank states seeded as
-well_random_seed (pic2d_RandomNumberInterface.f90:39-57) does. Surface charges (dielectrics) and object potentials
-(external circuits) are outside the device path: a checkpoint that has any is rejected on loading, and written
-checkpoints have none.
+well_random_seed (pic2d_RandomNumberInterface.f90:39-57) does. The surface charges of dielectric inner objects are
+rank 0's REAL(8) block, each object's outline in the order of its boundary nodes (pic2d_Checkpoints.f90:806-812);
+dielectric walls and object potentials (external circuits) are outside the device path and rejected on loading.
 """
 import os
 
@@ -201,6 +201,19 @@ def write_mpiio(path, ranks):
 
 
 # ------------------------------------------------------------------------------------------------- Simulation side
+def outline_nodes(il, jb, ir, jt):
+    """(i, j) of an inner object's boundary nodes 1..N_boundary_nodes: up the left side from (ileft, jbottom), along
+    the top, down the right side, back along the bottom (Get_Surface_Charge_Inner_Object,
+    pic2d_PETSc_Solver.F90:1645-1720)."""
+    nodes = [(il, j) for j in range(jb, jt + 1)] + [(i, jt) for i in range(il + 1, ir + 1)]
+    nodes += [(ir, j) for j in range(jt - 1, jb - 1, -1)] + [(i, jb) for i in range(ir - 1, il, -1)]
+    return nodes
+
+
+def _dielectrics(p):
+    return [(p.inner_ileft[n], p.inner_jbottom[n], p.inner_iright[n], p.inner_jtop[n]) for n in range(p.n_inner)
+            if p.inner_eps[n] > 0.0]
+
 def _records(d):
     a = np.zeros(len(d["x"]), REC)
     for f in REC.names:
@@ -220,8 +233,20 @@ def load_checkpoint(sim, t_cntr, root="."):
     ranks = read_mpiio(path, n_spec) if os.path.exists(path) else read_posix(root, t_cntr, n_spec)
     if any(rk.t_cntr != t_cntr for rk in ranks):
         raise ValueError("checkpoint T_cntr does not match its file name")
-    if any(len(rk.surf) for rk in ranks):
-        raise ValueError("checkpoint holds surface charges or object potentials (dielectrics, external circuit)")
+    diel = _dielectrics(sim.params)
+    want = sum(len(outline_nodes(*o)) for o in diel)
+    if any(len(rk.surf) for rk in ranks[1:]) or len(ranks[0].surf) != want:
+        raise ValueError("checkpoint surface charges do not match the dielectric inner objects (dielectric walls or "
+                         "object potentials are not supported)")
+    if diel:
+        from . import FIELD_SURFACE_CHARGE
+        grid = np.zeros((sim.ny_ref, sim.nx_ref))
+        k = 0
+        for o in diel:
+            for (i, j) in outline_nodes(*o):
+                grid[j, i] = ranks[0].surf[k]
+                k += 1
+        sim.set_field(FIELD_SURFACE_CHARGE, grid)
     ncx = sim.params.ncx
     for k in range(n_spec + 1):
         a = np.concatenate([rk.electrons if k == 0 else rk.ions[k - 1] for rk in ranks])
@@ -264,8 +289,14 @@ def save_checkpoint(sim, root=".", nprocs=1, fmt="posix", carry=None, seed=1):
         for s in range(n_spec):
             h[636 + 2 * s + 1] = len(share[1 + s])
             h[636 + 2 * s] = max(int(h[636 + 2 * s]), len(share[1 + s]))
-        h[-1] = 0
-        ranks.append(Rank(h, np.zeros(0), share[0], share[1:]))
+        surf = np.zeros(0)
+        diel = _dielectrics(p)
+        if r == 0 and diel:
+            from . import FIELD_SURFACE_CHARGE
+            grid = sim.field(FIELD_SURFACE_CHARGE)
+            surf = np.array([grid[j, i] for o in diel for (i, j) in outline_nodes(*o)])
+        h[-1] = len(surf)
+        ranks.append(Rank(h, surf, share[0], share[1:]))
     if fmt == "posix":
         return write_posix(root, t, ranks)
     return [write_mpiio(mpiio_path(root, t), ranks)]

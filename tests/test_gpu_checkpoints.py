@@ -57,3 +57,29 @@ def test_checkpoint_restart(tmp_path, precision, geometry, fmt, nprocs):
             # in the uninterrupted run and from zero after the restart (a checkpoint holds no potential), so the
             # fields agree to the CG tolerance
             assert np.abs(ra - rb).max() < (1e-9 if geometry == "periodic" else 1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt,nprocs", [("posix", 2), ("mpiio", 3)])
+def test_checkpoint_dielectric_surface_charge(tmp_path, fmt, nprocs):
+    """The outline charge of a dielectric inner object travels in rank 0's surface-charge block, in the order of the
+    object's boundary nodes."""
+    from edipic_b200 import FIELD_SURFACE_CHARGE
+    diel = (30, 12, 40, 26, 0.0, 3.0)
+    d = small_deck(tmp_path / "deck", "walled", inner=[diel], collisions=False)
+    root = str(tmp_path / "run")
+    os.makedirs(root)
+    with Simulation(d, precision=PREC_MIXED, sort_every=0) as a:
+        x, y, vx, vy, vz = random_particles(a, 5000, seed=9)
+        a.upload_particles(ELECTRONS, x, y, vx, vy, vz)
+        a.upload_particles(IONS, x, y, 0.01 * vx, 0.01 * vy, 0.01 * vz)
+        surf = np.zeros((a.ny_ref, a.nx_ref))
+        for (i, j) in checkpoints.outline_nodes(*diel[:4]):
+            surf[j, i] = 0.25 * i - 0.5 * j
+        a.set_field(FIELD_SURFACE_CHARGE, surf)
+        a.set_step(5)
+        checkpoints.save_checkpoint(a, root, nprocs=nprocs, fmt=fmt)
+    with Simulation(d, precision=PREC_MIXED, sort_every=0) as b:
+        ranks = checkpoints.load_checkpoint(b, 5, root)
+        assert len(ranks[0].surf) == 2 * (10 + 14) and all(len(r.surf) == 0 for r in ranks[1:])
+        assert np.abs(b.field(FIELD_SURFACE_CHARGE) - surf).max() < 1e-9
