@@ -1,0 +1,99 @@
+"""Long-run statistical comparison of the mixed-precision device cycle with the plain FP64 device cycle on the
+RF-driven periodic configuration (the cfg4 physics: top electrode at 200 V and 13.56 MHz, bottom grounded, e-Ar MCC,
+Ar+-Ar charge exchange, ion-induced electron emission of yield 0.1 at both walls), over several seeds. Each run
+samples, after a burn-in, the electron energy distribution (EEDF), the electron and ion density profiles across the
+gap (COLLECT_*_MOMENTS averaged along x), the electron f(v_x) of CALCULATE_ELECTRON_VDF and the ion flux to each wall.
+`compare` turns the per-seed samples of the two precisions into z-scores: the difference of the means over seeds
+divided by its standard error.
+
+    python -m edipic_b200.longrun --seeds 8 --steps 3000 --cells 128 128 --ppc 100 --out longrun.json
+"""
+import argparse
+import json
+import os
+import tempfile
+
+import numpy as np
+
+from . import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation, decks
+
+EEDF_EDGES_EV = np.concatenate([[0.0], np.geomspace(0.05, 100.0, 40)])
+
+
+def run(precision, seed, steps, cells=(64, 64), ppc=64, burn_in=None, sample_every=20, workdir=None):
+    """One run of `steps` steps; returns the time-averaged samples of the second half (or after burn_in)."""
+    burn_in = steps // 2 if burn_in is None else burn_in
+    tmp = tempfile.mkdtemp(dir=workdir)
+    d = decks.write_deck(os.path.join(tmp, "deck"), "cfg4", ncx=cells[0], ncy=cells[1], ppc=ppc, steps=steps)
+    with Simulation(d, precision=precision, sort_every=20 if precision == PREC_MIXED else 0, seed=seed) as sim:
+        ef = sim.deck.tables.energy_factor_eV
+        sim.distribute_particles(ppc)
+        eedf = np.zeros(len(EEDF_EDGES_EV) - 1)
+        ne = np.zeros(sim.ny_ref)
+        ni = np.zeros(sim.ny_ref)
+        fvx = None
+        n_samples = 0
+        hits0 = None
+        for t in range(steps):
+            sim.step(1)
+            if t + 1 == burn_in:
+                c = sim.counters()
+                hits0 = np.array(c.ion_hits[:2], dtype=np.float64)
+            if t + 1 > burn_in and (t + 1 - burn_in) % sample_every == 0:
+                el = sim.download_particles(ELECTRONS)
+                e = (el["vx"] ** 2 + el["vy"] ** 2 + el["vz"] ** 2) * ef
+                h, _ = np.histogram(e, bins=EEDF_EDGES_EV)
+                eedf += h / max(len(e), 1)
+                ne += sim.collect_moments(ELECTRONS)[0].mean(axis=1)
+                ni += sim.collect_moments(IONS)[0].mean(axis=1)
+                v1, _, _ = sim.calculate_vdf(ELECTRONS, (1, 1), 4, 10)
+                f = v1[0, 0].astype(np.float64)
+                fvx = f / f.sum() if fvx is None else fvx + f / f.sum()
+                n_samples += 1
+        c = sim.counters()
+        flux = (np.array(c.ion_hits[:2], dtype=np.float64) - hits0) / (steps - burn_in)
+    return dict(eedf=(eedf / n_samples).tolist(), ne=(ne / n_samples).tolist(), ni=(ni / n_samples).tolist(),
+                fvx=(fvx / n_samples).tolist(), ion_flux=flux.tolist(), samples=n_samples)
+
+
+def zscores(a, b, floor=0.0):
+    """|mean_a - mean_b| / sqrt(se_a^2 + se_b^2) per component for per-seed samples a, b [seeds, n]; components
+    whose means are both below floor are dropped."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    ma, mb = a.mean(0), b.mean(0)
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    keep = (np.maximum(ma, mb) > floor) & (se > 0)
+    return (ma - mb)[keep] / se[keep]
+
+
+def compare(mixed, fp64):
+    """z-scores of every quantity between the two lists of run() results."""
+    out = {}
+    for k, floor in (("eedf", 1e-3), ("ne", 0.0), ("ni", 0.0), ("fvx", 1e-3), ("ion_flux", 0.0)):
+        z = zscores([r[k] for r in mixed], [r[k] for r in fp64], floor)
+        out[k] = dict(n=int(z.size), max_abs_z=float(np.abs(z).max()) if z.size else 0.0,
+                      mean_z2=float((z ** 2).mean()) if z.size else 0.0)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--seeds", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--cells", type=int, nargs=2, default=(128, 128))
+    ap.add_argument("--ppc", type=int, default=100)
+    ap.add_argument("--out", default="longrun.json")
+    args = ap.parse_args()
+    res = {}
+    for prec, name in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
+        res[name] = [run(prec, 1000 + s, args.steps, tuple(args.cells), args.ppc) for s in range(args.seeds)]
+    summary = dict(config=dict(seeds=args.seeds, steps=args.steps, cells=list(args.cells), ppc=args.ppc),
+                   z=compare(res["mixed"], res["fp64"]),
+                   ion_flux=dict(mixed=np.mean([r["ion_flux"] for r in res["mixed"]], 0).tolist(),
+                                 fp64=np.mean([r["ion_flux"] for r in res["fp64"]], 0).tolist()))
+    json.dump(dict(summary=summary, runs=res), open(args.out, "w"))
+    print(json.dumps(summary))
+
+
+if __name__ == "__main__":
+    main()
