@@ -196,7 +196,8 @@ int finish_sync(edp_ctx* c)
 // -------------------------------------------------------------------------------- utility kernels
 __global__ void upload_kernel(edp_kparams kp, int precision, int64_t n, int64_t base, const double* x, const double* y,
                               const double* vx, const double* vy, const double* vz, const int32_t* tag,
-                              const uint32_t* id, edp_species_mixed m, edp_species_fp64 d, unsigned int* eflag)
+                              const uint32_t* id, edp_species_mixed m, edp_species_fp64 d, unsigned int* eflag,
+                              uint64_t id_base)
 {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         double X = x[k], Y = y[k];
@@ -209,7 +210,7 @@ __global__ void upload_kernel(edp_kparams kp, int precision, int64_t n, int64_t 
         }
         if (bad) atomicOr(eflag, EDP_EFLAG_BOUNDS);
         int64_t slot = base + k;
-        uint32_t pid = id ? id[k] : (uint32_t)(base + k);
+        uint32_t pid = id ? id[k] : (uint32_t)(id_base + (uint64_t)k);
         int32_t t = tag ? tag[k] : 0;
         if (precision == EDP_PREC_MIXED) {
             int i = (int)X, j = (int)Y;
@@ -481,6 +482,7 @@ int ref_width(const edp_ctx* c) { return c->kp.periodic ? c->p.ncx + 2 : c->p.nc
 int zero_density(edp_ctx* c, int sp)
 {
     const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    c->dirty |= 1u << sp;
     if (c->p.precision == EDP_PREC_MIXED)
         EDP_CUDA(c, cudaMemsetAsync(c->rho_fix[sp], 0, nn * sizeof(unsigned long long), c->stream));
     else
@@ -751,9 +753,10 @@ int edp_upload_particles(edp_ctx* c, int sp, int64_t n, const double* x, const d
     if (n)
         upload_kernel<<<grid_of(n), 256, 0, c->stream>>>(c->kp, c->p.precision, n, 0, dbuf, dbuf + nn, dbuf + 2 * nn,
                                                          dbuf + 3 * nn, dbuf + 4 * nn, tag ? tbuf : nullptr,
-                                                         id ? ibuf : nullptr, c->pm[sp], c->pd[sp], &c->dc->error_flags);
+                                                         id ? ibuf : nullptr, c->pm[sp], c->pd[sp], &c->dc->error_flags,
+                                                         c->id_base);
     EDP_CUDA(c, cudaGetLastError());
-    unsigned long long ns = (unsigned long long)n, nid = (unsigned long long)n;
+    unsigned long long ns = (unsigned long long)n, nid = (unsigned long long)(c->id_base + n);
     if (id && n) {
         std::vector<uint32_t> h(id, id + n);
         nid = (unsigned long long)*std::max_element(h.begin(), h.end()) + 1ull;
@@ -781,7 +784,7 @@ int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv,
     if (copy_pos && (n != c->host_slots[0] || c->sorted_end[0] != 0))
         return edp_fail(c, EDP_ERR_STATE, "ions copy electron positions: same per_cell, before the electron sort");
     TRY(alloc_species(c, sp, n));
-    const int64_t base_id = 0;
+    const int64_t base_id = (int64_t)c->id_base;
     ++c->launches;
     distribute_kernel<<<grid_of(n, 148 * 64), 256, 0, c->stream>>>(
         c->kp, c->p.precision, sp, per_cell, fconv, zero_vz, copy_pos, c->maxwell_v, c->tab.maxwell_rmax, base_id,
@@ -789,7 +792,8 @@ int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv,
     EDP_CUDA(c, cudaGetLastError());
     unsigned long long ns = (unsigned long long)n;
     EDP_CUDA(c, cudaMemcpyAsync(&c->dc->n_slots[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
-    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->next_id[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
+    const unsigned long long nid = (unsigned long long)(base_id + n);
+    EDP_CUDA(c, cudaMemcpyAsync(&c->dc->next_id[sp], &nid, sizeof(nid), cudaMemcpyHostToDevice, c->stream));
     c->host_slots[sp] = n;
     // the electron array is sorted only after the ions copied its positions
     if (sp == 0 && copy_pos == 0) {
@@ -1218,6 +1222,33 @@ int edp_end_ion_cycle(edp_ctx* c)
         c->steps_since_sort = 0;
     }
     return finish_sync(c);
+}
+
+int edp_set_id_base(edp_ctx* c, uint64_t base)
+{
+    if (!c || base >= (1ull << 32)) return edp_fail(c, EDP_ERR_ARG, "edp_set_id_base");
+    c->id_base = base;
+    return EDP_OK;
+}
+
+int edp_reduce_list(edp_ctx* c, int32_t max, void** ptr, int64_t* count, int32_t* is_int64, int32_t* n_out)
+{
+    if (!c || !ptr || !count || !is_int64 || !n_out || max < 0) return edp_fail(c, EDP_ERR_ARG, "edp_reduce_list");
+    if (c->kp.diel_mask) return edp_fail(c, EDP_ERR_STATE, "edp_reduce_list: dielectric objects on one rank only");
+    const int64_t nn = (int64_t)c->kp.nxg * c->kp.nyg;
+    const bool mixed = c->p.precision == EDP_PREC_MIXED;
+    int32_t n = 0;
+    for (int s = 0; s < c->nspec; ++s) {
+        if (!((c->dirty >> s) & 1) || !c->uploaded[s]) continue;
+        if (n == max) return edp_fail(c, EDP_ERR_ARG, "edp_reduce_list: max too small");
+        ptr[n] = mixed ? (void*)c->rho_fix[s] : (void*)c->rho_d[s];
+        count[n] = nn;
+        is_int64[n] = mixed ? 1 : 0;
+        ++n;
+    }
+    c->dirty = 0;
+    *n_out = n;
+    return EDP_OK;
 }
 
 int edp_set_step(edp_ctx* c, int64_t t_cntr)

@@ -141,6 +141,8 @@ struct edp_ctx {
     int64_t host_slots[EDP_MAX_SPECIES] = {0};   // host-side upper bound of n_slots
     int64_t sorted_end[EDP_MAX_SPECIES] = {0};   // slots [0, sorted_end) are tile-sorted
     int64_t steps_since_sort = 0;
+    uint64_t id_base = 0;             // first id of the particles this context creates (distribution, upload)
+    uint32_t dirty = 0;               // bit s: species s's density was deposited since the last edp_reduce_list
     int uploaded[EDP_MAX_SPECIES] = {0};
 
     // particles

@@ -159,6 +159,22 @@ class Simulation:
         except Exception:
             pass
 
+    def stream(self):
+        """The cudaStream_t (as an integer) on which the context runs its work."""
+        ptr = C.c_void_p()
+        self._check(self.lib.edp_get_stream(self.ctx, C.byref(ptr)), "edp_get_stream")
+        return ptr.value or 0
+
+    def set_id_base(self, base):
+        """First id of the particles the context creates from now on (disjoint ranges for ranks of a cluster)."""
+        self._check(self.lib.edp_set_id_base(self.ctx, int(base)), "edp_set_id_base")
+
+    def reduce_list(self):
+        """[(device pointer, count, is_int64)] of the densities deposited since the last call (edp_reduce_list)."""
+        ptrs, counts, ints, n = (C.c_void_p * 8)(), (C.c_int64 * 8)(), (C.c_int32 * 8)(), C.c_int32()
+        self._check(self.lib.edp_reduce_list(self.ctx, 8, ptrs, counts, ints, C.byref(n)), "edp_reduce_list")
+        return [(ptrs[k], counts[k], bool(ints[k])) for k in range(n.value)]
+
     def synchronize(self):
         self._check(self.lib.edp_synchronize(self.ctx), "edp_synchronize")
 

@@ -121,6 +121,8 @@ SIGNATURES = {
     "edp_end_ion_cycle": [_CTX],
     "edp_step": [_CTX, C.c_int32],
     "edp_set_step": [_CTX, C.c_int64],
+    "edp_set_id_base": [_CTX, C.c_uint64],
+    "edp_reduce_list": [_CTX, C.c_int32, P(C.c_void_p), _I64, _I32, _I32],
     "edp_query_counters": [_CTX, P(Counters)],
     "edp_get_field": [_CTX, C.c_int, _D],
     "edp_set_field": [_CTX, C.c_int, _D],

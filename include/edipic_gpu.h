@@ -260,6 +260,17 @@ int edp_end_ion_cycle(edp_ctx* ctx);
  * where checkpoints are taken (:103-108). The step counter keys the device's random streams and the wall
  * potentials. */
 int edp_set_step(edp_ctx* ctx, int64_t t_cntr);
+/* Several ranks (one GPU each) sharing one cluster's particles, as the reference's processes of a cluster do: each
+ * context holds the whole grid and its own share of the particles. After each step (after edp_end_ion_cycle) and
+ * after the initial distribution or upload, the caller sums, in place and over the ranks, the accumulators this
+ * call lists (the cluster reduce of c_rho, GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1641 and
+ * GATHER_ION_CHARGE_DENSITY): the densities deposited since the previous call, device buffers of count[k] int64
+ * (mixed precision, fixed point, so the sum is exact and order-independent) or FP64 values. The sum must be ordered
+ * on the context's stream (edp_get_stream). Every rank then solves the same field. Not with dielectric objects. */
+int edp_reduce_list(edp_ctx* ctx, int32_t max, void** ptr, int64_t* count, int32_t* is_int64, int32_t* n_out);
+/* ids of the particles the context creates from now on (distribution, upload without ids) start at base
+ * (< 2^32); ranks sharing a cluster take disjoint ranges so that their random streams differ */
+int edp_set_id_base(edp_ctx* ctx, uint64_t base);
 /* One or more whole steps of pic2d_MainProgram.f90:151-309 in order (convenience for drivers). */
 int edp_step(edp_ctx* ctx, int32_t nsteps);
 
