@@ -13,7 +13,10 @@ a Fortran host uses, with the per-step host reads of the collision counters.
 
 --impl reference times the CPU restatement of the reference routines (the oracle: the reference's Fortran
 cannot be built in this image) on the host cores, on a bounded sample of the same workload.
-Multi-GPU (torchrun): independent replicas, one per GPU (weak scaling), device time max over ranks.
+Multi-GPU (torchrun): the ranks share one cluster's particles (each GPU pushes args.ppc electrons and ions per cell
+over the whole grid, so the particles per cell grow with N: weak scaling); the int64 fixed-point densities are summed
+over the ranks with an NCCL all-reduce after every step and every rank solves the same field. Device time is the max
+over ranks.
 """
 import argparse
 import ctypes as C
@@ -34,7 +37,8 @@ BYTES_PER_PARTICLE_STEP = {"mixed": 52, "fp64": 84}
 
 
 def workload_desc(args):
-    return (f"{args.config}: {args.cells_x}x{args.cells_y} cells, {args.ppc} e- + {args.ppc} Ar+ per cell, "
+    per = " per GPU" if getattr(args, "world", 1) > 1 else ""
+    return (f"{args.config}: {args.cells_x}x{args.cells_y} cells, {args.ppc} e- + {args.ppc} Ar+ per cell{per}, "
             f"{'B 10 mT at 30 deg, ' if args.config == 'cfg1' else ''}e-Ar MCC + Ar+-Ar RCX, FFT_X, "
             f"{args.precision} precision, sort every {args.sort_every}")
 
@@ -314,13 +318,17 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     else:
         torch.cuda.set_device(0)
-    from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation, decks
+    args.world = world
+    from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation, cluster, decks
     tmp = tempfile.mkdtemp(prefix=f"edp_bench_{rank}_")
-    d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc, seed=rank)
+    # the deck's particles per cell (the density normalisation) count all ranks' particles
+    d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc * world)
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
-    sim = Simulation(d, precision=prec, sort_every=args.sort_every, fuse_collisions=True, seed=1000 + rank)
+    sim = Simulation(d, precision=prec, sort_every=args.sort_every, fuse_collisions=True, seed=1000)
     lib, ctx = sim.lib, sim.ctx
+    share = cluster.ClusterShare(sim, rank, world)   # disjoint ids; density sums over the ranks
     sim.distribute_particles(args.ppc)
+    share.reduce()
     sptr = C.c_void_p()
     lib.edp_get_stream(ctx, C.byref(sptr))
     stream = torch.cuda.ExternalStream(sptr.value)
@@ -341,6 +349,7 @@ def run_ours(args):
         chk(lib.edp_collide_en(ctx, None), "en")
         chk(lib.edp_collide_rcx(ctx, None), "rcx")
         chk(lib.edp_end_ion_cycle(ctx), "end")
+        share.reduce()
         sim.counters_cache_t = t + 1
 
     for _ in range(args.warmup):
@@ -401,6 +410,7 @@ def run_ours(args):
         chk(lib.edp_collide_en(ctx, cnt_buf), "en")
         chk(lib.edp_collide_rcx(ctx, C.byref(rcx_buf)), "rcx")
         chk(lib.edp_end_ion_cycle(ctx), "end")
+        share.reduce()
         sim.counters_cache_t = t + 1
     ee.record(stream)
     ee.synchronize()
@@ -437,7 +447,9 @@ def run_ours(args):
             "dtype": "f32 particles / i64 fixed-point density / f64 field" if args.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": workload_desc(args), "cells": [args.cells_x, args.cells_y],
-                       "particles_per_gpu": int(per_gpu_particles), "parallelism": f"replicas x{world}",
+                       "particles_per_gpu": int(per_gpu_particles),
+                       "parallelism": (f"one cluster over {world} GPUs: particles split, densities summed by NCCL "
+                                       "all-reduce, field replicated" if world > 1 else "1 GPU"),
                        "l2": "particle arrays (>10 GB) exceed L2 each step"},
             "poisson_ms_per_step": 1e3 * t_field / args.steps,
             "push_ms_per_step": 1e3 * t_push / args.steps,
