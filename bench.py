@@ -4,7 +4,7 @@
 Workload (default): the 1024x1024-cell periodic-x plasma with 200 electrons and 200 Ar+ per cell
 (419,430,400 particles), B = 10 mT at 30 degrees in plane, e-Ar (elastic, excitation, ionisation) and Ar+-Ar
 charge exchange, N_subcycles = 1, mixed precision (int32 cell + FP32 offsets/velocities, int64 fixed-point
-deposit), tile sort every 20 steps. Synthetic deck and initial plasma (no dataset is involved).
+deposit), tile sort every 80 steps. Synthetic deck and initial plasma (no dataset is involved).
 
 One step = one pass of MainProg's cycle (pic2d_MainProgram.f90:151-309): density, FFT_X solve and E, electron
 push+deposit+MCC, ion push+deposit+RCX, appends. value = (electrons + ions) * steps / device time of the timed
@@ -249,7 +249,7 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
     for name, pc, warm in runs:
         with tempfile.TemporaryDirectory() as tmp:
             d = decks.write_deck(tmp, "cfg2")
-            with Simulation(d, sort_every=20, fuse_collisions=True, seed=2000) as sim:
+            with Simulation(d, sort_every=80, fuse_collisions=True, seed=2000) as sim:
                 sim.set_cg_preconditioner(pc)
                 if theta is not None:
                     sim.load_warm_start(theta)
@@ -497,7 +497,7 @@ def main():
     ap.add_argument("--cells", type=int, nargs=2, default=None, metavar=("NX", "NY"))
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--sort-every", type=int, default=20)
+    ap.add_argument("--sort-every", type=int, default=80)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the FP64-cycle and Poisson legs")
     args = ap.parse_args()
