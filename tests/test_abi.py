@@ -49,3 +49,23 @@ def test_init_rejects_bad_arguments_without_gpu():
     ctx = C.c_void_p()
     assert lib.edp_init(C.byref(p), C.byref(t), C.byref(ctx)) == _abi.ERR_ARG   # wrong ABI version
     assert lib.edp_destroy(None) == 0
+
+
+def test_init_limits_without_gpu(tmp_path):
+    """edp_init checks its arguments before it looks for a device: an FFT_X grid beyond 4096 columns or not a power
+    of two, a negative permittivity, and a dielectric object with the FFT_X solver are refused."""
+    from edipic_b200 import decks, read_deck
+    d = read_deck(decks.write_deck(str(tmp_path), "cfg0", ncx=64, ncy=32, ppc=4))
+    lib = _abi.load()
+    ctx = C.c_void_p()
+    p = _abi.Params.from_buffer_copy(d.params)
+    assert lib.edp_init(C.byref(p), C.byref(d.tables), C.byref(ctx)) == _abi.ERR_CUDA   # valid: fails on no device
+    for change in ({"ncx": 8192}, {"ncx": 96}, {"n_inner": 1, "eps": -1.0}, {"n_inner": 1, "eps": 2.0}):
+        p = _abi.Params.from_buffer_copy(d.params)
+        if "ncx" in change:
+            p.ncx = change["ncx"]
+        if "n_inner" in change:
+            p.n_inner = 1
+            p.inner_ileft[0], p.inner_jbottom[0], p.inner_iright[0], p.inner_jtop[0] = 10, 10, 20, 20
+            p.inner_eps[0] = change["eps"]
+        assert lib.edp_init(C.byref(p), C.byref(d.tables), C.byref(ctx)) == _abi.ERR_ARG, change
