@@ -11,7 +11,7 @@
 
 #define EDP_MAX_SPECIES (1 + EDP_MAX_ION_SPECIES)
 
-// tile geometry of the mixed-precision push: particles are cell-sorted tile by tile; a CTA stages the
+// tile geometry of the mixed-precision push: particles are sorted tile by tile; a CTA stages the
 // field and accumulates the density of its tile plus a halo of HALO cells in shared memory.
 #define EDP_TILE 16
 #define EDP_HALO 2

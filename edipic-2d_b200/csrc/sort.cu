@@ -1,8 +1,13 @@
-// Cell sort of the mixed-precision particle arrays (no reference analogue: EDIPIC-2D keeps particles in
-// arrival order). Counting sort on a tile-major cell key, so that every EDP_TILE x EDP_TILE tile is one
-// contiguous slot range and, inside it, particles of one cell are adjacent. Dead slots are dropped, which
-// is also the compaction of particles removed at walls since the last sort. Each tile's range is padded with
-// dead slots to a multiple of EDP_ITEMS, so the push reads and writes every tile in whole 128-bit groups.
+// Tile sort of the mixed-precision particle arrays (no reference analogue: EDIPIC-2D keeps particles in
+// arrival order). Counting sort on a key of (tile, (source slot / 32) mod 256), so that every EDP_TILE x EDP_TILE
+// tile is one contiguous slot range. Inside a tile the 256 sub-buckets interleave runs of 32 source slots: a run
+// (one scatter warp) stays contiguous, so its stores and its counter atomic stay coalesced, while the 128
+// consecutive particles of one push warp come from four runs 8192 source slots apart. Long runs of one cell (the
+// initial distribution fills the slots cell by cell) are thereby spread over the tile, and the lanes of a push
+// warp do not pile their shared-memory deposits onto one node; a plain cell order made the push 9 % slower on
+// 1024^2 cells at 200 particles per cell. Dead slots are dropped, which is also the compaction of particles
+// removed at walls since the last sort. Each tile's range is padded with dead slots to a multiple of EDP_ITEMS, so
+// the push reads and writes every tile in whole 128-bit groups.
 #include <algorithm>
 #include <vector>
 
@@ -10,10 +15,10 @@
 
 namespace {
 
-__device__ __forceinline__ uint32_t tile_key(int cell, int ntx)
+__device__ __forceinline__ uint32_t tile_key(int cell, int64_t k, int ntx)
 {
     int i = cell & 0xFFFF, j = cell >> 16;
-    return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)(((j & 15) << 4) | (i & 15));
+    return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)((k >> 5) & 255);
 }
 
 __global__ void hist_kernel(const int32_t* __restrict__ cell, const unsigned long long* n_slots, int ntx,
@@ -24,13 +29,13 @@ __global__ void hist_kernel(const int32_t* __restrict__ cell, const unsigned lon
     for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x; k0 < n; k0 += (int64_t)gridDim.x * blockDim.x) {
         int64_t k = k0 + threadIdx.x;
         int c = k < n ? cell[k] : -1;
-        uint32_t key = c >= 0 ? tile_key(c, ntx) : 0xFFFFFFFFu;
+        uint32_t key = c >= 0 ? tile_key(c, k, ntx) : 0xFFFFFFFFu;
         unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
         if (key != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&count[key], (uint32_t)__popc(peers));
     }
 }
 
-// exclusive scan of the 256 cell counts of one tile (one CTA per tile); tile_total[t] = live particles in it
+// exclusive scan of the 256 sub-bucket counts of one tile (one CTA per tile); tile_total[t] = live particles in it
 __global__ void tile_scan_kernel(const uint32_t* __restrict__ count, unsigned long long* __restrict__ local,
                                  unsigned long long* __restrict__ tile_total)
 {
@@ -107,7 +112,7 @@ __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, con
     for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x; k0 < n; k0 += (int64_t)gridDim.x * blockDim.x) {
         int64_t k = k0 + threadIdx.x;
         int c = k < n ? src.cell[k] : -1;
-        uint32_t key = c >= 0 ? tile_key(c, ntx) : 0xFFFFFFFFu;
+        uint32_t key = c >= 0 ? tile_key(c, k, ntx) : 0xFFFFFFFFu;
         unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
         int leader = __ffs(peers) - 1;
         unsigned long long base = 0;
