@@ -617,7 +617,8 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
     cudaMemset(c->rho_total, 0, nn * sizeof(double));
     if (p->solver == EDP_SOLVER_CG) {
         if ((r = dalloc(c, &c->cg_b, nn)) || (r = dalloc(c, &c->cg_r, nn)) || (r = dalloc(c, &c->cg_p, nn)) ||
-            (r = dalloc(c, &c->cg_Ap, nn)) || (r = dalloc(c, &c->cg_z, nn)) || (r = dalloc(c, &c->cg_kind, nn)))
+            (r = dalloc(c, &c->cg_Ap, nn)) || (r = dalloc(c, &c->cg_z, nn)) || (r = dalloc(c, &c->cg_kind, nn)) ||
+            (r = dalloc(c, &c->cg_sc, EDP_CG_SCALARS)))
             return fail(r);
     }
     // sort workspace
@@ -686,7 +687,10 @@ int edp_destroy(edp_ctx* c)
     F(c->sort_count); F(c->sort_offset); F(c->scan_tmp);
     F(c->E2); F(c->acc2); F(c->Ex); F(c->Ey); F(c->accx); F(c->accy);
     F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
-    F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind);
+    F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind); F(c->cg_sc);
+    for (auto& row : c->cg_exec)
+        for (auto& g : row)
+            if (g) cudaGraphExecDestroy(g);
     edp_mg_free(c);
     edp_warmstart_free(c);
     F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v); F(c->maxwell_inj); F(c->emit_dev);

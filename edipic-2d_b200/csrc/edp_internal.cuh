@@ -18,6 +18,12 @@
 #define EDP_WIN_CELLS (EDP_TILE + 2 * EDP_HALO)
 #define EDP_WIN_NODES (EDP_WIN_CELLS + 1)
 #define EDP_CHUNK 8192          // particles per CTA work item inside one tile
+// CG runs in blocks of iterations (the host reads the residual norms back once per block); a block keeps its
+// scalars (r.z, p.Ap, r.r after each iteration) in one of two areas, the previous block's in the other
+#define EDP_CG_CHECK_MG 2
+#define EDP_CG_CHECK_PLAIN 8
+#define EDP_CG_AREA (4 * EDP_CG_CHECK_PLAIN + 4)
+#define EDP_CG_SCALARS (2 + 2 * EDP_CG_AREA)
 #define EDP_PUSH_THREADS 256
 #define EDP_ITEMS 4             // particles per thread per iteration (128-bit loads)
 
@@ -177,6 +183,9 @@ struct edp_ctx {
     // CG workspace
     double *cg_b = nullptr, *cg_r = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_z = nullptr;
     int8_t* cg_kind = nullptr;        // 0 unknown, 1 Dirichlet
+    double* cg_sc = nullptr;          // CG scalars: |b|^2, r.r before iteration 0, two areas of block scalars
+    cudaGraphExec_t cg_exec[2][3] = {};   // [multigrid][first block, odd block, even block]: captured iterations
+    int64_t cg_exec_launches[2][3] = {};  // kernels in each captured block
     int32_t precond = 1;              // edp_precond
     int32_t mg_nlev = 0, mg_lc = 0;   // multigrid levels; levels >= mg_lc run inside one CTA
     edp_mg_level mg[EDP_MG_MAX_LEVELS];

@@ -540,6 +540,48 @@ int edp_launch_efield(edp_ctx* c)
     return EDP_OK;
 }
 
+// Iterations k0 .. k0+n-1 of (preconditioned) CG, launched on the context's stream with no host synchronisation,
+// so that a whole block can be captured as a graph. Block b = k0 / check accumulates its scalars in area b & 1 (zeroed
+// first): r.z of iteration j of the block at 4j, p.Ap at 4j+1, r.r after it at 4j+2. Values of the previous block
+// are read from the other area, which this block does not touch; r.r before iteration 0 is scalar [1].
+static int cg_block(edp_ctx* c, const CgGeom& g, bool mg, int k0, int n, int check)
+{
+    const edp_kparams& kp = g.kp;
+    const unsigned gr = grid_nodes(kp);
+    double* S = c->cg_sc;
+    double* A = S + 2 + ((k0 / check) & 1) * EDP_CG_AREA;
+    double* P = S + 2 + (((k0 / check) + 1) & 1) * EDP_CG_AREA;
+    EDP_CUDA(c, cudaMemsetAsync(A, 0, 4 * check * sizeof(double), c->stream));
+    // r.r after iteration m (m >= 0) of the solve, for m in this block or the previous one
+    auto rr_after = [&](int m) { return m >= k0 ? A + 4 * (m - k0) + 2 : P + 4 * (m - (k0 - check)) + 2; };
+    auto rr_before = [&](int k) { return k == 0 ? S + 1 : rr_after(k - 1); };
+    for (int j = 0; j < n; ++j) {
+        const int k = k0 + j;
+        double* rz = A + 4 * j;
+        double* pAp = A + 4 * j + 1;
+        if (mg) {
+            TRY(edp_mg_apply(c, c->cg_r, c->cg_z));
+            ++c->launches;
+            pcg_dot<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_r, c->cg_z, rz);
+            const double* rz_prev = k == 0 ? nullptr : (j ? A + 4 * (j - 1) : P + 4 * (check - 1));
+            ++c->launches;
+            pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rz_prev, c->cg_z, c->cg_p);
+        } else {
+            rz = rr_before(k);
+            if (k) {
+                ++c->launches;
+                pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rr_before(k - 1), c->cg_r, c->cg_p);
+            }
+        }
+        ++c->launches;
+        cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp, g.epsx, g.epsy);
+        ++c->launches;
+        cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r, A + 4 * j + 2);
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
 int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
 {
     const edp_kparams& kp = c->kp;
@@ -550,33 +592,22 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
     g.epsx = c->epsx;
     g.epsy = c->epsy;
-    // scalars: [0] |b|^2, [1] r.r before iteration 0; iteration k keeps r.z at 2+4k, p.Ap at 3+4k and the
-    // residual norm^2 after it at 4(k+1)
-    double* scal = nullptr;
-    const int nscal = 4 * (max_it + 2);
-    EDP_CUDA(c, cudaMallocAsync(&scal, nscal * sizeof(double), c->stream));
-    EDP_CUDA(c, cudaMemsetAsync(scal, 0, nscal * sizeof(double), c->stream));
-    auto rr_at = [&](int k) { return k == 0 ? scal + 1 : scal + 4 * k; };
+    // scalars: [0] |b|^2, [1] r.r before iteration 0, then the two block areas (cg_block)
+    double* scal = c->cg_sc;
+    EDP_CUDA(c, cudaMemsetAsync(scal, 0, 2 * sizeof(double), c->stream));
     const unsigned gr = grid_nodes(kp);
     // the network was trained on the vacuum operator: with dielectric objects the previous potential starts the solve
     if (warm == EDP_WARM_LEARNED && kp.diel_mask) warm = EDP_WARM_PREVIOUS;
     const bool learned = warm == EDP_WARM_LEARNED;
-    if (learned && !c->ws) {
-        cudaFreeAsync(scal, c->stream);
-        return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
-    }
+    if (learned && !c->ws) return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
     ++c->launches;
     cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
     ++c->launches;
     cg_residual<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->phi, c->cg_b, c->cg_r, c->cg_p, &scal[1],
                                            c->epsx, c->epsy);
     if (learned) {
-        int e = edp_warmstart_forward(c, &scal[1]);
-        if (e == EDP_OK) e = edp_warmstart_residual(c);
-        if (e != EDP_OK) {
-            cudaFreeAsync(scal, c->stream);
-            return e;
-        }
+        TRY(edp_warmstart_forward(c, &scal[1]));
+        TRY(edp_warmstart_residual(c));
     }
     double h[3] = {0.0, 0.0, 0.0};
     EDP_CUDA(c, cudaMemcpyAsync(h, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -593,47 +624,44 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     }
     c->last_cg_relres0 = rel;
     int it = 0, done_at = rel <= rtol ? 0 : -1;
-    const int check = mg ? 2 : 8;
-    std::vector<double> blk(4 * check + 4);
+    const int check = mg ? EDP_CG_CHECK_MG : EDP_CG_CHECK_PLAIN;
+    std::vector<double> blk(4 * check);
     while (done_at < 0 && it < max_it) {
-        const int stop = std::min(max_it, it + check);
-        for (int k = it; k < stop; ++k) {
-            double* rz = scal + 2 + 4 * k;
-            double* pAp = scal + 3 + 4 * k;
-            if (mg) {
-                const int e = edp_mg_apply(c, c->cg_r, c->cg_z);
+        const int n = std::min(max_it - it, check);
+        double* area = scal + 2 + ((it / check) & 1) * EDP_CG_AREA;
+        if (n == check) {   // a whole block: replayed from its captured graph
+            const int which = it == 0 ? 0 : 1 + ((it / check) & 1);
+            cudaGraphExec_t& ex = c->cg_exec[mg][which];
+            if (!ex) {
+                const int64_t l0 = c->launches;
+                EDP_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                const int e = cg_block(c, g, mg, it, check, check);
+                cudaGraph_t graph = nullptr;
+                const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
                 if (e != EDP_OK) {
-                    cudaFreeAsync(scal, c->stream);
+                    if (graph) cudaGraphDestroy(graph);
                     return e;
                 }
-                ++c->launches;
-                pcg_dot<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_r, c->cg_z, rz);
-                ++c->launches;
-                pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, k ? scal + 2 + 4 * (k - 1) : nullptr,
-                                                         c->cg_z, c->cg_p);
-            } else {
-                rz = rr_at(k);
-                if (k) {
-                    ++c->launches;
-                    pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rr_at(k - 1), c->cg_r, c->cg_p);
-                }
+                EDP_CUDA(c, ce);
+                const cudaError_t ie = cudaGraphInstantiate(&ex, graph, 0);
+                cudaGraphDestroy(graph);
+                EDP_CUDA(c, ie);
+                c->cg_exec_launches[mg][which] = c->launches - l0;
+                c->launches = l0;
             }
-            ++c->launches;
-            cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp, c->epsx, c->epsy);
-            ++c->launches;
-            cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r,
-                                                 rr_at(k + 1));
+            EDP_CUDA(c, cudaGraphLaunch(ex, c->stream));
+            c->launches += c->cg_exec_launches[mg][which];
+        } else {
+            TRY(cg_block(c, g, mg, it, n, check));
         }
-        // residual norms after iterations it+1 .. stop; the iteration count is the first that met rtol
-        const int n = 4 * (stop - it) - 3;
-        EDP_CUDA(c, cudaMemcpyAsync(blk.data(), rr_at(it + 1), n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        // residual norms after iterations it+1 .. it+n; the iteration count is the first that met rtol
+        EDP_CUDA(c, cudaMemcpyAsync(blk.data(), area, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         EDP_CUDA(c, cudaStreamSynchronize(c->stream));
-        for (int k = it + 1; k <= stop && done_at < 0; ++k)
-            if (std::sqrt(blk[4 * (k - it - 1)]) / bn <= rtol) done_at = k;
-        rel = std::sqrt(blk[4 * (stop - it - 1)]) / bn;   // the solution carries the whole block
-        it = stop;
+        for (int j = 0; j < n && done_at < 0; ++j)
+            if (std::sqrt(blk[4 * j + 2]) / bn <= rtol) done_at = it + j + 1;
+        rel = std::sqrt(blk[4 * (n - 1) + 2]) / bn;   // the solution carries the whole block
+        it += n;
     }
-    EDP_CUDA(c, cudaFreeAsync(scal, c->stream));
     EDP_CUDA(c, cudaGetLastError());
     const int reported = done_at >= 0 ? done_at : it;
     c->last_cg_iters = reported;
