@@ -92,8 +92,10 @@ __global__ void fftx_forward(edp_kparams kp, const double* __restrict__ rho, dou
 // SOLVE_POISSON_FFTX_LINSYSY :690-756 for metal walls (a_eq(0) = a_eq(J) = 0). The forward sweep
 //   rr(j) = (-y(j) - rr(j-1)) a(j),  j = 1..J-1,  rr(0) = y(0)
 // and the back substitution phi(j) = rr(j) - a(j) phi(j+1), phi(J) = y(J), are first-order affine recurrences.
-// One warp solves one mode: lane l composes the maps of its segment of rows, a shuffle scan over the lanes gives
-// each segment its incoming value, and the lane re-sweeps its rows. Same recurrence, reassociated.
+// The interior rows of a mode are cut into kTmSegs segments. A thread composes the maps of its segment, the
+// compositions are scanned over the segments (shuffles inside a warp, shared memory across the warps), and the
+// thread re-sweeps its rows from its incoming value. Same recurrence, reassociated. A warp holds 8 consecutive
+// modes x 4 segments (lane = 8 segment + mode), so every row is read and written as 128 contiguous bytes.
 struct Aff {   // x -> c + b x, complex c, real b
     double cx, cy, b;
 };
@@ -103,62 +105,83 @@ __device__ __forceinline__ Aff aff_after(const Aff& late, const Aff& early)   //
     return Aff{late.cx + late.b * early.cx, late.cy + late.b * early.cy, late.b * early.b};
 }
 
-__device__ __forceinline__ Aff shfl_aff(const Aff& a, int src, bool up, int off)
+__device__ __forceinline__ Aff shfl_aff(const Aff& a, bool up, int off)
 {
     Aff r;
     r.cx = up ? __shfl_up_sync(0xFFFFFFFFu, a.cx, off) : __shfl_down_sync(0xFFFFFFFFu, a.cx, off);
     r.cy = up ? __shfl_up_sync(0xFFFFFFFFu, a.cy, off) : __shfl_down_sync(0xFFFFFFFFu, a.cy, off);
     r.b = up ? __shfl_up_sync(0xFFFFFFFFu, a.b, off) : __shfl_down_sync(0xFFFFFFFFu, a.b, off);
-    (void)src;
     return r;
 }
 
-__global__ void fftx_thomas(int J, int nm, const double* __restrict__ aeq, double2* __restrict__ spec)
+constexpr int kTmModes = 8, kTmWarps = 16, kTmSegs = 4 * kTmWarps;
+
+__global__ void __launch_bounds__(32 * kTmWarps) fftx_thomas(int J, int nm, const double* __restrict__ aeq,
+                                                             double2* __restrict__ spec)
 {
-    const int m = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (m >= nm) return;   // whole warps
-    const int n = J - 1, per = (n + 31) / 32;
-    const int j0 = 1 + lane * per, j1 = min(j0 + per, J);   // interior rows [j0, j1) of this lane
-    // ---- forward sweep: compose rr(j) = -a y(j) + (-a) rr(j-1) over the segment
+    __shared__ Aff part[kTmWarps][kTmModes];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ml = lane & 7, sw = lane >> 3;
+    const int m = blockIdx.x * kTmModes + ml;
+    const bool active = m < nm;
+    const int mm = active ? m : nm - 1;   // lanes past the last mode shadow it without storing
+    const int seg = 4 * w + sw;
+    const int per = (J - 1 + kTmSegs - 1) / kTmSegs;
+    const int j0 = 1 + seg * per, j1 = min(j0 + per, J);   // interior rows [j0, j1) of this segment
+    // ---- forward sweep
     Aff f{0.0, 0.0, 1.0};
+#pragma unroll 4
     for (int j = j0; j < j1; ++j) {
-        const double a = aeq[(int64_t)j * nm + m];
-        const double2 y = spec[(int64_t)j * nm + m];
+        const double a = aeq[(int64_t)j * nm + mm];
+        const double2 y = spec[(int64_t)j * nm + mm];
         f = aff_after(Aff{-a * y.x, -a * y.y, -a}, f);
     }
-    for (int off = 1; off < 32; off <<= 1) {   // inclusive scan, lane l = segments 0..l
-        Aff p = shfl_aff(f, lane - off, true, off);
+    for (int off = 8; off < 32; off <<= 1) {   // inclusive over the warp's segments, earliest first
+        Aff p = shfl_aff(f, true, off);
         if (lane >= off) f = aff_after(f, p);
     }
-    const double2 rr0 = spec[m];   // transformed wall row
-    Aff ex = shfl_aff(f, lane - 1, true, 1);
-    double2 prev = lane == 0 ? rr0 : make_double2(ex.cx + ex.b * rr0.x, ex.cy + ex.b * rr0.y);
+    if (sw == 3) part[w][ml] = f;
+    __syncthreads();
+    Aff inc{0.0, 0.0, 1.0};
+    for (int q = 0; q < w; ++q) inc = aff_after(part[q][ml], inc);
+    Aff ex = shfl_aff(f, true, 8);
+    if (sw > 0) inc = aff_after(ex, inc);
+    const double2 rr0 = spec[mm];   // transformed wall row
+    double2 prev = make_double2(inc.cx + inc.b * rr0.x, inc.cy + inc.b * rr0.y);
+#pragma unroll 4
     for (int j = j0; j < j1; ++j) {
-        const double a = aeq[(int64_t)j * nm + m];
-        const double2 y = spec[(int64_t)j * nm + m];
+        const double a = aeq[(int64_t)j * nm + mm];
+        const double2 y = spec[(int64_t)j * nm + mm];
         prev = make_double2((-y.x - prev.x) * a, (-y.y - prev.y) * a);
-        spec[(int64_t)j * nm + m] = prev;
+        if (active) spec[(int64_t)j * nm + mm] = prev;
     }
-    // ---- back substitution: phi(j) = rr(j) + (-a(j)) phi(j+1), segments composed from the top
+    // ---- back substitution, segments composed from the top
     Aff g{0.0, 0.0, 1.0};
+#pragma unroll 4
     for (int j = j1 - 1; j >= j0; --j) {
-        const double a = aeq[(int64_t)j * nm + m];
-        const double2 r = spec[(int64_t)j * nm + m];
+        const double a = aeq[(int64_t)j * nm + mm];
+        const double2 r = spec[(int64_t)j * nm + mm];
         g = aff_after(Aff{r.x, r.y, -a}, g);
     }
-    for (int off = 1; off < 32; off <<= 1) {   // inclusive scan from lane 31 down: lane l = segments l..31
-        Aff p = shfl_aff(g, lane + off, false, off);
+    for (int off = 8; off < 32; off <<= 1) {   // inclusive over the warp's segments, latest first
+        Aff p = shfl_aff(g, false, off);
         if (lane + off < 32) g = aff_after(g, p);
     }
-    const double2 phiJ = spec[(int64_t)J * nm + m];
-    Aff ey = shfl_aff(g, lane + 1, false, 1);
-    double2 next = lane == 31 ? phiJ : make_double2(ey.cx + ey.b * phiJ.x, ey.cy + ey.b * phiJ.y);
+    __syncthreads();   // every thread has read the forward totals
+    if (sw == 0) part[w][ml] = g;
+    __syncthreads();
+    Aff inb{0.0, 0.0, 1.0};
+    for (int q = kTmWarps - 1; q > w; --q) inb = aff_after(part[q][ml], inb);
+    Aff ey = shfl_aff(g, false, 8);
+    if (sw < 3) inb = aff_after(ey, inb);
+    const double2 phiJ = spec[(int64_t)J * nm + mm];
+    double2 next = make_double2(inb.cx + inb.b * phiJ.x, inb.cy + inb.b * phiJ.y);
+#pragma unroll 4
     for (int j = j1 - 1; j >= j0; --j) {
-        const double a = aeq[(int64_t)j * nm + m];
-        const double2 r = spec[(int64_t)j * nm + m];
+        const double a = aeq[(int64_t)j * nm + mm];
+        const double2 r = spec[(int64_t)j * nm + mm];
         next = make_double2(r.x - a * next.x, r.y - a * next.y);
-        spec[(int64_t)j * nm + m] = next;
+        if (active) spec[(int64_t)j * nm + mm] = next;
     }
     // row 0 keeps rr(0) = phi(0) since a_eq(0) = 0
 }
@@ -517,12 +540,12 @@ int edp_launch_fftx(edp_ctx* c)
     int logn = 0;
     while ((1 << logn) < N) ++logn;
     size_t smem = (size_t)N * sizeof(double2);
-    int thr = std::min(512, std::max(32, N / 2));
+    int thr = std::min(128, std::max(32, N / 2));   // 8 rows of 1024 in flight per SM: one wave at 1025 rows
     ++c->launches;
     fftx_forward<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->rho_total, c->phi_wall[0], c->phi_wall[1], c->twiddle,
                                                      logn, c->nm, c->spec);
     ++c->launches;
-    fftx_thomas<<<(c->nm + 7) / 8, 256, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);   // a warp per mode
+    fftx_thomas<<<(c->nm + kTmModes - 1) / kTmModes, 32 * kTmWarps, 0, c->stream>>>(c->p.ncy, c->nm, c->aeq, c->spec);
     ++c->launches;
     fftx_inverse<<<c->kp.nyg, thr, smem, c->stream>>>(c->kp, c->spec, c->twiddle, logn, c->nm, c->phi);
     EDP_CUDA(c, cudaGetLastError());
