@@ -687,7 +687,7 @@ int edp_destroy(edp_ctx* c)
     F(c->sort_count); F(c->sort_offset); F(c->scan_tmp);
     F(c->E2); F(c->acc2); F(c->Ex); F(c->Ey); F(c->accx); F(c->accy);
     F(c->rho_total); F(c->phi); F(c->phi_prev); F(c->spec); F(c->aeq); F(c->twiddle);
-    F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind); F(c->cg_sc);
+    F(c->cg_b); F(c->cg_r); F(c->cg_p); F(c->cg_Ap); F(c->cg_z); F(c->cg_kind); F(c->cg_sc); F(c->strip_cnt);
     for (auto& row : c->cg_exec)
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
@@ -761,9 +761,10 @@ int edp_upload_particles(edp_ctx* c, int sp, int64_t n, const double* x, const d
                                                          c->id_base);
     EDP_CUDA(c, cudaGetLastError());
     unsigned long long ns = (unsigned long long)n, nid = (unsigned long long)(c->id_base + n);
-    if (id && n) {
+    if (id && n) {   // new particles continue after the uploaded ids, inside this context's range (edp_set_id_base)
         std::vector<uint32_t> h(id, id + n);
-        nid = (unsigned long long)*std::max_element(h.begin(), h.end()) + 1ull;
+        nid = std::max<unsigned long long>((unsigned long long)*std::max_element(h.begin(), h.end()) + 1ull,
+                                           (unsigned long long)c->id_base);
     }
     EDP_CUDA(c, cudaMemcpyAsync(&c->dc->n_slots[sp], &ns, sizeof(ns), cudaMemcpyHostToDevice, c->stream));
     EDP_CUDA(c, cudaMemcpyAsync(&c->dc->next_id[sp], &nid, sizeof(nid), cudaMemcpyHostToDevice, c->stream));
@@ -998,6 +999,7 @@ static int upload_wall_state(edp_ctx* c)
 int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double yield, double emin_ev, double emax_ev,
                          double t_emit_ev)
 {
+    if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
     if (!c || wall < 0 || wall > 3 || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
         !(emax_ev > emin_ev) || !(t_emit_ev >= 0.0))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_emission");
@@ -1016,6 +1018,7 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
 
 int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp)
 {
+    if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
     if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission");
     if (sp && (sp->elastic_model < 0 || sp->elastic_model > 2 || sp->inelastic_model < 0 || sp->inelastic_model > 2 ||
                sp->true_model < 0 || sp->true_model > 2))
@@ -1080,6 +1083,7 @@ int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp
 int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t model, double t_normal_ev,
                            double t_parallel_ev, double beam_energy_ev)
 {
+    if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
     if (!c || wall < 0 || wall > 3 || !(n_per_step >= 0.0) || n_per_step > 1.0e9 || model < 0 || model > 1 ||
         !(t_normal_ev >= 0.0) || !(t_parallel_ev >= 0.0))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection");
@@ -1112,6 +1116,7 @@ int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t 
 
 int edp_set_ion_reflection(edp_ctx* c, int32_t wall, int32_t on)
 {
+    if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
     if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
     TRY(wall_state(c));
     c->emit_h->reflect[wall] = on ? 1 : 0;

@@ -131,6 +131,7 @@ struct edp_kparams {
     int32_t nsub;
     uint32_t seed_lo, seed_hi;
     int32_t diel_mask;                        // bit n: inner object n is a dielectric
+    int32_t strip;                            // > 0: one x strip of a periodic domain with this many ghost columns
 };
 
 struct edp_ctx {
@@ -186,6 +187,7 @@ struct edp_ctx {
     double* cg_sc = nullptr;          // CG scalars: |b|^2, r.r before iteration 0, two areas of block scalars
     cudaGraphExec_t cg_exec[2][3] = {};   // [multigrid][first block, odd block, even block]: captured iterations
     int64_t cg_exec_launches[2][3] = {};  // kernels in each captured block
+    unsigned long long* strip_cnt = nullptr;   // left / right record counts of edp_strip_take
     int32_t precond = 1;              // edp_precond
     int32_t mg_nlev = 0, mg_lc = 0;   // multigrid levels; levels >= mg_lc run inside one CTA
     edp_mg_level mg[EDP_MG_MAX_LEVELS];

@@ -240,7 +240,16 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         bool outx = ni < 0 || ni > kp.ncx || (ni == kp.ncx && nx > 0.0f);
         bool outy = nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f);
         if (outx || outy) {
-            int obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
+            int obj;
+            if (kp.strip) {   // the y walls of the periodic domain; leaving the strip and its ghost columns is an error
+                if (!outy) {
+                    atomicOr(&a.dc->error_flags, EDP_EFLAG_BOUNDS);
+                    return false;
+                }
+                obj = nj < 0 ? 0 : 1;
+            } else {
+                obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
+            }
             atomicAdd(&s.cnt[obj], 1ull);
             if (a.emit_on)
                 record_hit(a.hits, a.dc, obj, ION ? a.species - 1 : 0, (double)ni + (double)nx,

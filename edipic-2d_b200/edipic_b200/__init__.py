@@ -104,11 +104,20 @@ def read_deck(directory):
 class Simulation:
     """One device context. Method names follow the reference subroutines they replace."""
 
-    def __init__(self, deck, precision=PREC_MIXED, sort_every=None, fuse_collisions=True, capacity=None, seed=None):
+    def __init__(self, deck, precision=PREC_MIXED, sort_every=None, fuse_collisions=True, capacity=None, seed=None,
+                 strip=None):
+        """strip = (own columns, ghost columns): one x strip of the deck's periodic domain (edp_set_strip), a
+        walled-x context of own + 2 ghost columns whose field comes from a context of the whole grid."""
         self.lib = library()
         self.deck = deck if isinstance(deck, Deck) else Deck(deck)
         p = Params.from_buffer_copy(self.deck.params)
         p.precision = precision
+        if strip is not None:
+            if not p.periodic_x:
+                raise ValueError("strips split a periodic-x domain")
+            p.ncx = int(strip[0]) + 2 * int(strip[1])
+            p.periodic_x = 0
+            p.solver = SOLVER_CG
         if sort_every is not None:
             p.sort_every = sort_every
         p.fuse_collisions = 1 if fuse_collisions else 0
@@ -122,6 +131,8 @@ class Simulation:
         rc = self.lib.edp_init(C.byref(p), C.byref(self.deck.tables), C.byref(self.ctx))
         if rc != 0:
             raise EdpError(rc, "edp_init")
+        if strip is not None:
+            self._check(self.lib.edp_set_strip(self.ctx, int(strip[1])), "edp_set_strip")
         self.periodic = bool(p.periodic_x)
         self.nx_ref = p.ncx + 2 if self.periodic else p.ncx + 1
         self.ny_ref = p.ncy + 1
@@ -174,6 +185,14 @@ class Simulation:
         ptrs, counts, ints, n = (C.c_void_p * 8)(), (C.c_int64 * 8)(), (C.c_int32 * 8)(), C.c_int32()
         self._check(self.lib.edp_reduce_list(self.ctx, 8, ptrs, counts, ints, C.byref(n)), "edp_reduce_list")
         return [(ptrs[k], counts[k], bool(ints[k])) for k in range(n.value)]
+
+    def device_buffer(self, which, species=0):
+        """(device pointer, element count) of the fixed-point density of `species` (which 0), the field (1) or the
+        accumulated field (2), internal node layout (edp_device_buffer)."""
+        ptr, n = C.c_void_p(), C.c_int64()
+        self._check(self.lib.edp_device_buffer(self.ctx, int(which), int(species), C.byref(ptr), C.byref(n)),
+                    "edp_device_buffer")
+        return ptr.value, n.value
 
     def synchronize(self):
         self._check(self.lib.edp_synchronize(self.ctx), "edp_synchronize")

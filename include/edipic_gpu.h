@@ -269,8 +269,43 @@ int edp_set_step(edp_ctx* ctx, int64_t t_cntr);
  * on the context's stream (edp_get_stream). Every rank then solves the same field. Not with dielectric objects. */
 int edp_reduce_list(edp_ctx* ctx, int32_t max, void** ptr, int64_t* count, int32_t* is_int64, int32_t* n_out);
 /* ids of the particles the context creates from now on (distribution, upload without ids) start at base
- * (< 2^32); ranks sharing a cluster take disjoint ranges so that their random streams differ */
+ * (< 2^32); ranks sharing a cluster take disjoint ranges so that their random streams differ. After an upload
+ * with ids, particles born later continue after the largest uploaded id, and never below base. */
 int edp_set_id_base(edp_ctx* ctx, uint64_t base);
+/* ---- x strips of a periodic domain (the reference's clusters along x, pic2d_ParticleExchange.f90:3-1762;
+ * density halo sums GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1645-1800) ---------------------
+ * A strip context covers its own columns plus `ghost` columns on each side: it is set up walled in x (CG
+ * solver, never used) with ncx = own + 2 ghost, mixed precision, no inner objects and no wall emission, then
+ * marked with edp_set_strip before any particle is uploaded. Its local column c is global column
+ * x_first + c (periodic), x_first = first own column - ghost. Particles moving out of the strip and its ghost
+ * columns in one step are an error (EDP_ERR_BOUNDS at the next check); the y walls count their hits as objects
+ * 0 (below) and 1 (above), as the periodic domain does. Per step, for each species: zero the global density
+ * of a context holding the whole periodic grid (edp_device_buffer), edp_strip_add_density from every strip (sum
+ * over ranks), edp_field_fftx on the whole grid, edp_strip_set_field into every strip, the strip's own
+ * advance / collide / end_ion_cycle calls, then edp_strip_take and edp_strip_put to move the particles that
+ * ended the step in ghost columns to the neighbour owning them. Their charge was deposited by the sender. */
+int edp_set_strip(edp_ctx* ctx, int32_t ghost);
+/* Takes the particles of species `species` in the left (local columns < ghost) and right (>= ncx - ghost)
+ * ghost columns out of the strip into caller device buffers of records of 8 doubles (x, y in local cells, vx,
+ * vy, vz, id, tag, 0): left[cap_left * 8], right[cap_right * 8]; n_left / n_right receive the counts.
+ * EDP_ERR_CAPACITY when a buffer is too small (the particles past it are lost). Synchronises. */
+int edp_strip_take(edp_ctx* ctx, int32_t species, double* left, int64_t cap_left, double* right, int64_t cap_right,
+                   int64_t* n_left, int64_t* n_right);
+/* Appends n records (device buffer, edp_strip_take's layout) with x shifted by x_shift cells, keeping their ids
+ * and tags and depositing nothing. */
+int edp_strip_put(edp_ctx* ctx, int32_t species, const double* records, int64_t n, double x_shift);
+/* Adds the strip's fixed-point density of one species into global_dev[(ncy + 1) * nx_global] (the node layout
+ * of a periodic context, column c at (x_first + c) mod nx_global), on the strip's stream. */
+int edp_strip_add_density(edp_ctx* ctx, int32_t species, uint64_t* global_dev, int32_t nx_global, int32_t x_first);
+/* Copies the strip's columns of a whole-grid field (float2 (Ex, Ey) per node, layout as above) and of its
+ * accumulated field for the ions into the strip. */
+int edp_strip_set_field(edp_ctx* ctx, const void* e_global_dev, const void* acc_global_dev, int32_t nx_global,
+                        int32_t x_first);
+/* Device pointer and element count of a context's arrays: which = 0 the fixed-point density of `species`
+ * (uint64 per node), 1 the field (float2 per node), 2 the accumulated field of the ions (float2); mixed
+ * precision, internal node layout (periodic: ncx columns). */
+int edp_device_buffer(edp_ctx* ctx, int32_t which, int32_t species, void** ptr, int64_t* count);
+
 /* One or more whole steps of pic2d_MainProgram.f90:151-309 in order (convenience for drivers). */
 int edp_step(edp_ctx* ctx, int32_t nsteps);
 
