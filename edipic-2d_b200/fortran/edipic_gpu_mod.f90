@@ -206,6 +206,47 @@ module edipic_gpu
        integer(c_int), value :: species
        real(c_float), intent(out) :: out(*)
      end function edp_collect_moments
+     ! x strips of a periodic domain (one cluster per strip along x, pic2d_ParticleExchange.f90); the record and
+     ! density buffers are device memory the host allocates (cudaMalloc through its CUDA Fortran or C layer)
+     integer(c_int) function edp_set_strip(ctx, ghost) bind(C, name="edp_set_strip")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: ghost
+     end function edp_set_strip
+     integer(c_int) function edp_strip_take(ctx, species, left, cap_left, right, cap_right, n_left, n_right) &
+          bind(C, name="edp_strip_take")
+       import :: c_ptr, c_int, c_int32_t, c_int64_t
+       type(c_ptr), value :: ctx, left, right
+       integer(c_int32_t), value :: species
+       integer(c_int64_t), value :: cap_left, cap_right
+       integer(c_int64_t), intent(out) :: n_left, n_right
+     end function edp_strip_take
+     integer(c_int) function edp_strip_put(ctx, species, records, n, x_shift) bind(C, name="edp_strip_put")
+       import :: c_ptr, c_int, c_int32_t, c_int64_t, c_double
+       type(c_ptr), value :: ctx, records
+       integer(c_int32_t), value :: species
+       integer(c_int64_t), value :: n
+       real(c_double), value :: x_shift
+     end function edp_strip_put
+     integer(c_int) function edp_strip_add_density(ctx, species, global_dev, nx_global, x_first) &
+          bind(C, name="edp_strip_add_density")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx, global_dev
+       integer(c_int32_t), value :: species, nx_global, x_first
+     end function edp_strip_add_density
+     integer(c_int) function edp_strip_set_field(ctx, e_global, acc_global, nx_global, x_first) &
+          bind(C, name="edp_strip_set_field")
+       import :: c_ptr, c_int, c_int32_t
+       type(c_ptr), value :: ctx, e_global, acc_global
+       integer(c_int32_t), value :: nx_global, x_first
+     end function edp_strip_set_field
+     integer(c_int) function edp_device_buffer(ctx, which, species, ptr, count) bind(C, name="edp_device_buffer")
+       import :: c_ptr, c_int, c_int32_t, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: which, species
+       type(c_ptr), intent(out) :: ptr
+       integer(c_int64_t), intent(out) :: count
+     end function edp_device_buffer
      integer(c_int) function edp_query_counters(ctx, c) bind(C, name="edp_query_counters")
        import :: c_ptr, c_int, edp_counters
        type(c_ptr), value :: ctx
