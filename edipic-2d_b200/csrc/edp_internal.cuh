@@ -192,6 +192,9 @@ struct edp_ctx {
     int32_t mg_nlev = 0, mg_lc = 0;   // multigrid levels; levels >= mg_lc run inside one CTA
     edp_mg_level mg[EDP_MG_MAX_LEVELS];
     size_t mg_smem = 0;               // shared memory of the coarse-level kernel
+    double* mg_cinv = nullptr;        // inverse of the coarsest level's operator (mg_cn x mg_cn), or null
+    int32_t* mg_cidx = nullptr;       // node index of each coarsest-level unknown
+    int32_t mg_cn = 0;
     edp_warmstart* ws = nullptr;      // network of the learned warm start, once loaded
     edp_emit_dev* emit_dev = nullptr; // ion-induced electron emission (device copy of emit_h)
     edp_emit_dev* emit_h = nullptr;   // host copy

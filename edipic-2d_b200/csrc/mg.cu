@@ -22,6 +22,7 @@ constexpr int kNu = 2;                 // RB sweeps before and after the coarse 
 constexpr int kCoarsestSweeps = 24;    // RB sweep pairs on the coarsest level
 constexpr int kCtaNodes = 4225;        // levels with at most this many nodes (65 x 65) run in the coarse CTA
 constexpr int kCoarseThreads = 1024;
+constexpr int kDirectMax = 256;        // the coarsest level is solved exactly (dense inverse) up to this many unknowns
 
 struct Lev {
     double* u;
@@ -127,6 +128,9 @@ struct CoarseArgs {
     const int8_t* mask[EDP_MG_MAX_LEVELS];
     const double* f_in;                   // right-hand side of the top level here
     double* u_out;                        // its correction
+    const double* cinv;                   // inverse of the coarsest level's operator on its cn unknowns, or null
+    const int32_t* cidx;                  // node of each unknown
+    int cn;
 };
 
 // The bottom of the V-cycle in one CTA: every level lives in shared memory, phases are separated by barriers.
@@ -170,17 +174,32 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) mg_coarse_kernel(CoarseArgs
         restrict_to(L[l], const_cast<double*>(L[l + 1].f), L[l + 1].mask, a.nx[l + 1], a.ny[l + 1], t, T);
         __syncthreads();
     }
-    for (int s = 0; s < kCoarsestSweeps; ++s) {
-        half_sweep(L[last], 0, s == 0, t, T);
+    if (a.cinv) {   // exact: u = A^-1 f on the unknowns, one warp per row
+        const int64_t n = (int64_t)(a.nx[last] + 1) * (a.ny[last] + 1);
+        for (int64_t q = t; q < n; q += T) L[last].u[q] = 0.0;
         __syncthreads();
-        half_sweep(L[last], 1, false, t, T);
+        const int lane = t & 31;
+        for (int r = t >> 5; r < a.cn; r += T >> 5) {
+            const double* row = a.cinv + (int64_t)r * a.cn;
+            double acc = 0.0;
+            for (int k = lane; k < a.cn; k += 32) acc += row[k] * L[last].f[a.cidx[k]];
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+            if (lane == 0) L[last].u[a.cidx[r]] = acc;
+        }
         __syncthreads();
-    }
-    for (int s = 0; s < kCoarsestSweeps; ++s) {
-        half_sweep(L[last], 1, false, t, T);
-        __syncthreads();
-        half_sweep(L[last], 0, false, t, T);
-        __syncthreads();
+    } else {
+        for (int s = 0; s < kCoarsestSweeps; ++s) {
+            half_sweep(L[last], 0, s == 0, t, T);
+            __syncthreads();
+            half_sweep(L[last], 1, false, t, T);
+            __syncthreads();
+        }
+        for (int s = 0; s < kCoarsestSweeps; ++s) {
+            half_sweep(L[last], 1, false, t, T);
+            __syncthreads();
+            half_sweep(L[last], 0, false, t, T);
+            __syncthreads();
+        }
     }
     for (int l = last - 1; l >= 0; --l) {
         prolong_add(L[l], L[l + 1].u, a.nx[l + 1], t, T);
@@ -217,6 +236,64 @@ Lev lev_of(const edp_ctx* c, int l, double* u, const double* f)
 }
 
 }  // namespace
+
+// The coarsest level's operator (4 u - neighbours) / h^2 on its unknown nodes, inverted once on the host (Gauss-Jordan
+// with partial pivoting, FP64): the V-cycle then solves that level exactly, which keeps it symmetric.
+static int coarsest_inverse(edp_ctx* c, const std::vector<int8_t>& mask, int nx, int ny, double h2)
+{
+    const int w = nx + 1;
+    std::vector<int32_t> idx, pos(mask.size(), -1);
+    for (size_t q = 0; q < mask.size(); ++q)
+        if (!mask[q]) {
+            pos[q] = (int32_t)idx.size();
+            idx.push_back((int32_t)q);
+        }
+    const int n = (int)idx.size();
+    if (n == 0 || n > kDirectMax) return EDP_OK;
+    std::vector<double> a((size_t)n * n, 0.0), inv((size_t)n * n, 0.0);
+    for (int r = 0; r < n; ++r) {
+        const int q = idx[r], i = q % w, j = q / w;
+        a[(size_t)r * n + r] = 4.0 / h2;
+        const int nb[4][2] = {{i - 1, j}, {i + 1, j}, {i, j - 1}, {i, j + 1}};
+        for (const auto& e : nb) {
+            if (e[0] < 0 || e[0] > nx || e[1] < 0 || e[1] > ny) continue;
+            const int k = pos[(size_t)e[1] * w + e[0]];
+            if (k >= 0) a[(size_t)r * n + k] = -1.0 / h2;
+        }
+        inv[(size_t)r * n + r] = 1.0;
+    }
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < n; ++r)
+            if (std::fabs(a[(size_t)r * n + col]) > std::fabs(a[(size_t)piv * n + col])) piv = r;
+        if (a[(size_t)piv * n + col] == 0.0) return EDP_OK;   // singular: keep the sweeps
+        if (piv != col)
+            for (int k = 0; k < n; ++k) {
+                std::swap(a[(size_t)piv * n + k], a[(size_t)col * n + k]);
+                std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]);
+            }
+        const double d = 1.0 / a[(size_t)col * n + col];
+        for (int k = 0; k < n; ++k) {
+            a[(size_t)col * n + k] *= d;
+            inv[(size_t)col * n + k] *= d;
+        }
+        for (int r = 0; r < n; ++r) {
+            if (r == col) continue;
+            const double f = a[(size_t)r * n + col];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; ++k) {
+                a[(size_t)r * n + k] -= f * a[(size_t)col * n + k];
+                inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k];
+            }
+        }
+    }
+    EDP_CUDA(c, cudaMalloc(&c->mg_cinv, (size_t)n * n * sizeof(double)));
+    EDP_CUDA(c, cudaMalloc(&c->mg_cidx, (size_t)n * sizeof(int32_t)));
+    EDP_CUDA(c, cudaMemcpy(c->mg_cinv, inv.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice));
+    EDP_CUDA(c, cudaMemcpy(c->mg_cidx, idx.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    c->mg_cn = n;
+    return EDP_OK;
+}
 
 int edp_mg_setup(edp_ctx* c)
 {
@@ -270,6 +347,7 @@ int edp_mg_setup(edp_ctx* c)
             EDP_CUDA(c, cudaMalloc(&m.u, n * sizeof(double)));
             EDP_CUDA(c, cudaMalloc(&m.f, n * sizeof(double)));
         }
+        if (l == nl - 1) TRY(coarsest_inverse(c, h, m.nx, m.ny, (double)(1 << l) * (double)(1 << l)));
     }
     return EDP_OK;
 }
@@ -285,6 +363,11 @@ void edp_mg_free(edp_ctx* c)
         c->mg[l] = edp_mg_level();
     }
     c->mg_nlev = 0;
+    cudaFree(c->mg_cinv);
+    cudaFree(c->mg_cidx);
+    c->mg_cinv = nullptr;
+    c->mg_cidx = nullptr;
+    c->mg_cn = 0;
 }
 
 int edp_mg_apply(edp_ctx* c, const double* r, double* z)
@@ -315,6 +398,9 @@ int edp_mg_apply(edp_ctx* c, const double* r, double* z)
     }
     a.f_in = f_of(lc);
     a.u_out = u_of(lc);
+    a.cinv = c->mg_cinv;
+    a.cidx = c->mg_cidx;
+    a.cn = c->mg_cn;
     ++c->launches;
     mg_coarse_kernel<<<1, kCoarseThreads, c->mg_smem, c->stream>>>(a);
     for (int l = lc - 1; l >= 0; --l) {
