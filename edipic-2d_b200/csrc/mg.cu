@@ -105,20 +105,68 @@ __device__ __forceinline__ void prolong_add(const Lev& F, const double* uc, int 
     }
 }
 
-__global__ void mg_sweep_kernel(Lev L, int color, int first)
+// The 2 kNu half-sweeps of one smoothing pass of a level in one launch (temporal blocking): a CTA stages a tile of
+// kTx x kTy nodes with a halo of kHalo = 2 kNu nodes, runs the half-sweeps on a region that loses one node on every
+// side per half-sweep, and writes back the tile. Every update reads the values the sequence of whole-grid
+// half-sweeps would, in the same order, so the result is the same to the bit. zero_start: the pass starts from a
+// zero correction (pre-smoothing). uc: the coarse correction, prolonged and added while the tile is staged
+// (post-smoothing, prolong_add's interpolation).
+constexpr int kTx = 32, kTy = 16, kHalo = 2 * kNu;
+constexpr int kSw = kTx + 2 * kHalo, kSh = kTy + 2 * kHalo;
+
+__global__ void __launch_bounds__(256) mg_smooth_kernel(Lev L, int first_color, int zero_start, const double* uc,
+                                                        int nxc)
 {
-    half_sweep(L, color, first != 0, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+    __shared__ double su[kSh][kSw];
+    __shared__ double sf[kSh][kSw];
+    __shared__ int8_t sm[kSh][kSw];
+    const int w = L.nx + 1, wc = nxc + 1;
+    const int x0 = blockIdx.x * kTx - kHalo, y0 = blockIdx.y * kTy - kHalo;
+    for (int k = threadIdx.x; k < kSw * kSh; k += blockDim.x) {
+        const int lx = k % kSw, ly = k / kSw, i = x0 + lx, j = y0 + ly;
+        double u = 0.0, f = 0.0;
+        int8_t m = 1;   // outside the grid: never updated, never read by an unknown node (walls are Dirichlet)
+        if (i >= 0 && i <= L.nx && j >= 0 && j <= L.ny) {
+            const int64_t q = (int64_t)j * w + i;
+            m = L.mask[q];
+            f = L.f[q];
+            if (!zero_start) u = L.u[q];
+            if (uc && !m) {
+                const int I = i >> 1, J = j >> 1;
+                const int64_t Q = (int64_t)J * wc + I;
+                double e;
+                if (!(i & 1) && !(j & 1)) e = uc[Q];
+                else if (!(j & 1)) e = 0.5 * (uc[Q] + uc[Q + 1]);
+                else if (!(i & 1)) e = 0.5 * (uc[Q] + uc[Q + wc]);
+                else e = 0.25 * (uc[Q] + uc[Q + 1] + uc[Q + wc] + uc[Q + wc + 1]);
+                u += e;
+            }
+        }
+        su[ly][lx] = u;
+        sf[ly][lx] = f;
+        sm[ly][lx] = m;
+    }
+    __syncthreads();
+    for (int h = 0; h < kHalo; ++h) {
+        const int color = first_color ^ (h & 1);
+        const int lo = h + 1, nxr = kSw - 2 * lo, nyr = kSh - 2 * lo;
+        for (int k = threadIdx.x; k < nxr * nyr; k += blockDim.x) {
+            const int lx = lo + k % nxr, ly = lo + k / nxr;
+            if (sm[ly][lx] || (((x0 + lx) + (y0 + ly)) & 1) != color) continue;
+            su[ly][lx] = 0.25 * (L.h2 * sf[ly][lx] + su[ly][lx - 1] + su[ly][lx + 1] + su[ly - 1][lx] + su[ly + 1][lx]);
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < kTx * kTy; k += blockDim.x) {
+        const int lx = kHalo + k % kTx, ly = kHalo + k / kTx, i = x0 + lx, j = y0 + ly;
+        if (i <= L.nx && j <= L.ny) L.u[(int64_t)j * w + i] = su[ly][lx];
+    }
 }
 
 __global__ void mg_restrict_kernel(Lev F, double* fc, const int8_t* maskc, int nxc, int nyc)
 {
     restrict_to(F, fc, maskc, nxc, nyc, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
                 (int64_t)gridDim.x * blockDim.x);
-}
-
-__global__ void mg_prolong_kernel(Lev F, const double* uc, int nxc)
-{
-    prolong_add(F, uc, nxc, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 struct CoarseArgs {
@@ -375,14 +423,11 @@ int edp_mg_apply(edp_ctx* c, const double* r, double* z)
     const int nl = c->mg_nlev, lc = c->mg_lc;
     auto u_of = [&](int l) { return l == 0 ? z : c->mg[l].u; };
     auto f_of = [&](int l) { return l == 0 ? r : (const double*)c->mg[l].f; };
+    auto tiles = [](const Lev& L) { return dim3((unsigned)((L.nx + kTx) / kTx), (unsigned)((L.ny + kTy) / kTy)); };
     for (int l = 0; l < lc; ++l) {
         Lev L = lev_of(c, l, u_of(l), f_of(l));
-        const unsigned g = grid_of_nodes(L.nx, L.ny);
-        for (int s = 0; s < kNu; ++s) {
-            c->launches += 2;
-            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 0, s == 0);
-            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 1, 0);
-        }
+        ++c->launches;   // pre-smoothing from a zero correction: red, black, red, black
+        mg_smooth_kernel<<<tiles(L), 256, 0, c->stream>>>(L, 0, 1, nullptr, 0);
         ++c->launches;
         mg_restrict_kernel<<<grid_of_nodes(c->mg[l + 1].nx, c->mg[l + 1].ny), 256, 0, c->stream>>>(
             L, c->mg[l + 1].f, c->mg[l + 1].mask, c->mg[l + 1].nx, c->mg[l + 1].ny);
@@ -405,14 +450,8 @@ int edp_mg_apply(edp_ctx* c, const double* r, double* z)
     mg_coarse_kernel<<<1, kCoarseThreads, c->mg_smem, c->stream>>>(a);
     for (int l = lc - 1; l >= 0; --l) {
         Lev L = lev_of(c, l, u_of(l), f_of(l));
-        const unsigned g = grid_of_nodes(L.nx, L.ny);
-        ++c->launches;
-        mg_prolong_kernel<<<g, 256, 0, c->stream>>>(L, c->mg[l + 1].u, c->mg[l + 1].nx);
-        for (int s = 0; s < kNu; ++s) {
-            c->launches += 2;
-            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 1, 0);
-            mg_sweep_kernel<<<g, 256, 0, c->stream>>>(L, 0, 0);
-        }
+        ++c->launches;   // prolongation, then post-smoothing: black, red, black, red
+        mg_smooth_kernel<<<tiles(L), 256, 0, c->stream>>>(L, 1, 0, c->mg[l + 1].u, c->mg[l + 1].nx);
     }
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
