@@ -224,7 +224,7 @@ def network_leg():
     return out
 
 
-def poisson_leg(args, stream_of, warmup=10, steps=30):
+def poisson_leg(args, stream_of, warmup=10, steps=30, only=None):
     """Poisson ms/step on the inner-object geometry (512 x 512 cells, metal walls at 0 V, a 64 x 32-cell metal
     rectangle at -100 V centred at (256, 128), 100 e- + 100 Ar+ per cell, the full collision set): each step of the
     cycle solves with CG to a 1e-8 relative residual from the previous step's potential. Timed by CUDA events
@@ -246,6 +246,8 @@ def poisson_leg(args, stream_of, warmup=10, steps=30):
         runs += [("learned_mg", PRECOND_MG, WARM_LEARNED), ("learned_nopc", PRECOND_NONE, WARM_LEARNED)]
     elif "learned" not in out:
         out["learned"] = {"unavailable": "no trained weights (edipic_b200.train_warmstart writes them)"}
+    if only:
+        runs = [r for r in runs if r[0] in only]
     for name, pc, warm in runs:
         with tempfile.TemporaryDirectory() as tmp:
             d = decks.write_deck(tmp, "cfg2")
@@ -500,6 +502,10 @@ def main():
     ap.add_argument("--sort-every", type=int, default=80)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the FP64-cycle and Poisson legs")
+    ap.add_argument("--poisson-only", nargs="*", default=None, metavar="RUN",
+                    help="only the Poisson leg (cfg2 geometry), optionally only the named runs "
+                         "(plain_mg, plain_nopc, learned_mg, learned_nopc)")
+    ap.add_argument("--poisson-steps", type=int, default=30)
     args = ap.parse_args()
     from edipic_b200 import decks
     cfg = decks.CONFIGS[args.config]
@@ -507,7 +513,16 @@ def main():
     args.ppc = args.ppc or cfg["ppc"]
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.poisson_only is not None:
+        import torch
+
+        def stream_of(s):
+            ptr = C.c_void_p()
+            s.lib.edp_get_stream(s.ctx, C.byref(ptr))
+            return torch.cuda.ExternalStream(ptr.value)
+        print(json.dumps({"poisson": poisson_leg(args, stream_of, warmup=max(args.warmup, 3), steps=args.poisson_steps,
+                                                 only=args.poisson_only or None)}))
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
