@@ -7,6 +7,9 @@
 #include <cstring>
 #include <vector>
 
+#include <map>
+#include <mutex>
+
 #include "edp_internal.cuh"
 
 int edp_fail(edp_ctx* c, int code, const std::string& msg)
@@ -509,6 +512,19 @@ int after_particles_changed(edp_ctx* c, int sp)
 }
 
 }  // namespace
+
+int edp_raise_smem_limit(edp_ctx* c, const void* kernel, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<const void*, size_t> limit;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limit[kernel];
+    if (bytes <= cur) return EDP_OK;
+    EDP_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+    return EDP_OK;
+}
+
 
 int edp_launch_deposit(edp_ctx* c, int sp)
 {

@@ -131,7 +131,10 @@ struct edp_kparams {
     int32_t nsub;
     uint32_t seed_lo, seed_hi;
     int32_t diel_mask;                        // bit n: inner object n is a dielectric
-    int32_t strip;                            // > 0: one x strip of a periodic domain with this many ghost columns
+    int32_t strip;                            // 1: one x strip of a domain (edp_set_strip)
+    int32_t strip_gl, strip_gr;               // ghost columns on its left / right; 0: that side is the domain's wall
+    int32_t strip_x0, strip_ncx;              // global column of local column 0, columns of the whole domain
+    int32_t strip_periodic;                   // the whole domain is periodic in x
 };
 
 struct edp_ctx {
@@ -531,6 +534,9 @@ __device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, u
 
 // --------------------------------------------------------------------------------- host helpers
 int edp_fail(edp_ctx* c, int code, const std::string& msg);
+// Raises a kernel's dynamic shared memory limit to at least `bytes`. The limit belongs to the kernel for the whole
+// process, so a context that needs less never lowers what another context set.
+int edp_raise_smem_limit(edp_ctx* c, const void* kernel, size_t bytes);
 int edp_cuda_check(edp_ctx* c, cudaError_t e, const char* what);
 #define EDP_CUDA(ctx, call)                                            \
     do {                                                               \

@@ -442,8 +442,8 @@ int edp_fields_prepare(edp_ctx* c)
     EDP_CUDA(c, cudaMemcpy(c->aeq, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice));
     size_t smem = (size_t)N * sizeof(double2);
     if (smem > 48 * 1024) {
-        EDP_CUDA(c, cudaFuncSetAttribute(fftx_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        EDP_CUDA(c, cudaFuncSetAttribute(fftx_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        TRY(edp_raise_smem_limit(c, (const void*)fftx_forward, smem));
+        TRY(edp_raise_smem_limit(c, (const void*)fftx_inverse, smem));
     }
     return EDP_OK;
 }

@@ -373,7 +373,7 @@ int edp_mg_setup(edp_ctx* c)
         return EDP_OK;
     }
     c->mg_smem = smem;
-    EDP_CUDA(c, cudaFuncSetAttribute(mg_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TRY(edp_raise_smem_limit(c, (const void*)mg_coarse_kernel, smem));
     // Dirichlet masks: walls, and the metal inner objects, of the finest node at (2^l I, 2^l J)
     for (int l = 0; l < nl; ++l) {
         edp_mg_level& m = c->mg[l];

@@ -241,12 +241,17 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         bool outy = nj < 0 || nj > kp.ncy || (nj == kp.ncy && ny > 0.0f);
         if (outx || outy) {
             int obj;
-            if (kp.strip) {   // the y walls of the periodic domain; leaving the strip and its ghost columns is an error
-                if (!outy) {
+            if (kp.strip) {
+                // the walls of the whole domain, in its coordinates; leaving the strip and its ghost columns through a
+                // side that is not a wall of the domain is an error
+                const bool wall_x = outx && ((ni < 0 && kp.strip_gl == 0) || (ni >= 0 && kp.strip_gr == 0));
+                if (!outy && !wall_x) {
                     atomicOr(&a.dc->error_flags, EDP_EFLAG_BOUNDS);
                     return false;
                 }
-                obj = nj < 0 ? 0 : 1;
+                if (kp.strip_periodic) obj = nj < 0 ? 0 : 1;
+                else obj = wall_object((double)(ni + kp.strip_x0) + (double)nx, (double)nj + (double)ny,
+                                       (double)kp.strip_ncx, (double)kp.ncy);
             } else {
                 obj = wall_object((double)ni + (double)nx, (double)nj + (double)ny, (double)kp.ncx, (double)kp.ncy);
             }

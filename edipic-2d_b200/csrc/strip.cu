@@ -2,9 +2,10 @@
 // pic2d_ParticleExchange.f90:3-1762 moves the particles between neighbouring clusters, and GATHER_*_CHARGE_DENSITY
 // pic2d_ElectronDynamics.f90:1645-1800 sums the densities of the nodes the clusters share).
 //
-// A strip context holds its own columns plus `ghost` columns on each side. Its particles are pushed against the
-// field copied from a context that solves the whole periodic grid, and deposit into the strip's nodes, ghost nodes
-// included; the strips' densities are summed into the whole grid before the next solve. After a step, particles in
+// A strip context holds its own columns plus ghost columns on the sides that face another strip (a side on the
+// domain's wall has none). Its particles are pushed against the field copied from a context that solves the whole
+// grid, and deposit into the strip's nodes, ghost nodes included; the strips' densities are summed into the whole
+// grid before the next solve. After a step, particles in
 // the ghost columns belong to a neighbour: edp_strip_take lifts them out as records, the caller moves the records,
 // and edp_strip_put appends them to the neighbour without depositing (the sender already did). Positions keep
 // their FP32 in-cell offsets and ids, so a run over strips does the arithmetic of the one-context run.
@@ -25,12 +26,11 @@ __global__ void strip_take_kernel(edp_kparams kp, edp_species_mixed P, const uns
                                   unsigned long long* n_live, unsigned int* eflag)
 {
     const int64_t n = (int64_t)*n_slots;
-    const int g = kp.strip;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int c = P.cell[k];
         if (c < 0) continue;
         const int i = c & 0xFFFF;
-        const int side = i < g ? 0 : (i >= kp.ncx - g ? 1 : -1);
+        const int side = i < kp.strip_gl ? 0 : (i >= kp.ncx - kp.strip_gr ? 1 : -1);
         if (side < 0) continue;
         const unsigned long long pos = atomicAdd(&cnt[side], 1ull);
         if ((int64_t)pos < (side ? cap_r : cap_l)) {
@@ -142,17 +142,25 @@ int check_flags(edp_ctx* c)
 
 }  // namespace
 
-int edp_set_strip(edp_ctx* c, int32_t ghost)
+int edp_set_strip(edp_ctx* c, int32_t ghost_left, int32_t ghost_right, int32_t x_first, int32_t ncx_global,
+                  int32_t periodic)
 {
-    if (!c || ghost < 1) return edp_fail(c, EDP_ERR_ARG, "edp_set_strip: ghost columns >= 1");
-    if (c->kp.periodic || c->p.precision != EDP_PREC_MIXED || c->p.n_inner != 0 || c->p.ncx <= 2 * ghost)
-        return edp_fail(c, EDP_ERR_STATE, "a strip is a walled-x, mixed-precision context without inner objects, "
-                                          "wider than its two ghost margins");
+    if (!c || ghost_left < 0 || ghost_right < 0 || ncx_global < 2 || (periodic && (!ghost_left || !ghost_right)) ||
+        (!periodic && (x_first < 0 || x_first + c->p.ncx > ncx_global)))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_strip: ghost columns, position in the domain");
+    if (c->kp.periodic || c->p.precision != EDP_PREC_MIXED || c->kp.diel_mask || c->p.ncx <= ghost_left + ghost_right)
+        return edp_fail(c, EDP_ERR_STATE, "a strip is a walled-x, mixed-precision context without dielectric objects, "
+                                          "wider than its ghost margins");
     if (c->emit_on || c->see_on || c->inject_on) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
     for (int s = 0; s < c->nspec; ++s)
         if (c->uploaded[s]) return edp_fail(c, EDP_ERR_STATE, "edp_set_strip before the particles are uploaded");
     if (!c->strip_cnt) EDP_CUDA(c, cudaMalloc(&c->strip_cnt, 2 * sizeof(unsigned long long)));
-    c->kp.strip = ghost;
+    c->kp.strip = 1;
+    c->kp.strip_gl = ghost_left;
+    c->kp.strip_gr = ghost_right;
+    c->kp.strip_x0 = x_first;
+    c->kp.strip_ncx = ncx_global;
+    c->kp.strip_periodic = periodic ? 1 : 0;
     return EDP_OK;
 }
 

@@ -157,7 +157,7 @@ extern "C" int edp_calculate_vdf(edp_ctx* c, int species, int32_t n_max_vel, int
     a.h2 = vdf2d ? buf + n1 : nullptr;
     a.skipped = reinterpret_cast<unsigned long long*>(buf + n1 + n2 + ((n1 + n2) & 1));
     if (smem > 48 * 1024)
-        EDP_CUDA(c, cudaFuncSetAttribute(vdf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        TRY(edp_raise_smem_limit(c, (const void*)vdf_kernel, smem));
     // about 64 particles per thread, so that the private copies are flushed rarely
     const int64_t slots = c->host_slots[species];
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((slots + 256 * 64 - 1) / (256 * 64), 148 * 4));

@@ -106,18 +106,23 @@ class Simulation:
 
     def __init__(self, deck, precision=PREC_MIXED, sort_every=None, fuse_collisions=True, capacity=None, seed=None,
                  strip=None):
-        """strip = (own columns, ghost columns): one x strip of the deck's periodic domain (edp_set_strip), a
-        walled-x context of own + 2 ghost columns whose field comes from a context of the whole grid."""
+        """strip = (own columns, ghost columns on the left, on the right, global column of local column 0): one x
+        strip of the deck's domain (edp_set_strip), a walled-x context of own + ghost columns whose field comes
+        from a context of the whole grid. Its inner objects are the deck's, in its columns."""
         self.lib = library()
         self.deck = deck if isinstance(deck, Deck) else Deck(deck)
         p = Params.from_buffer_copy(self.deck.params)
         p.precision = precision
+        strip_frame = None
         if strip is not None:
-            if not p.periodic_x:
-                raise ValueError("strips split a periodic-x domain")
-            p.ncx = int(strip[0]) + 2 * int(strip[1])
+            own, gl, gr, x_first = (int(v) for v in strip)
+            strip_frame = (gl, gr, x_first, p.ncx, p.periodic_x)
+            p.ncx = own + gl + gr
             p.periodic_x = 0
             p.solver = SOLVER_CG
+            for n in range(p.n_inner):   # strip columns; an object past the strip is clipped one column beyond it
+                p.inner_ileft[n] = min(max(p.inner_ileft[n] - x_first, -1), p.ncx + 1)
+                p.inner_iright[n] = min(max(p.inner_iright[n] - x_first, -1), p.ncx + 1)
         if sort_every is not None:
             p.sort_every = sort_every
         p.fuse_collisions = 1 if fuse_collisions else 0
@@ -131,8 +136,8 @@ class Simulation:
         rc = self.lib.edp_init(C.byref(p), C.byref(self.deck.tables), C.byref(self.ctx))
         if rc != 0:
             raise EdpError(rc, "edp_init")
-        if strip is not None:
-            self._check(self.lib.edp_set_strip(self.ctx, int(strip[1])), "edp_set_strip")
+        if strip_frame is not None:
+            self._check(self.lib.edp_set_strip(self.ctx, *strip_frame), "edp_set_strip")
         self.periodic = bool(p.periodic_x)
         self.nx_ref = p.ncx + 2 if self.periodic else p.ncx + 1
         self.ny_ref = p.ncy + 1

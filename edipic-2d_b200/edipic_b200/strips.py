@@ -1,12 +1,14 @@
-"""One periodic-x domain cut into x strips, as the reference cuts the domain into clusters along x
+"""One domain cut into x strips, as the reference cuts the domain into clusters along x
 (pic2d_ParticleExchange.f90:3-1762 moves the particles between neighbouring clusters, GATHER_*_CHARGE_DENSITY
 pic2d_ElectronDynamics.f90:1645-1800 sums the densities of the nodes they share, and the field of the whole domain
 reaches every cluster).
 
-A strip is a context of its own columns plus `ghost` columns on each side (edp_set_strip). Next to the strips runs
-a context of the whole grid that only solves the field. A step, in the order of pic2d_MainProgram.f90:151-309:
+A strip is a context of its own columns plus `ghost` columns on each side that faces another strip (edp_set_strip;
+a side on the domain's wall has none). Next to the strips runs a context of the whole grid that only solves the
+field. A step, in the order of pic2d_MainProgram.f90:151-309:
 1. every strip adds its fixed-point densities into the whole grid's density (summed over the ranks: int64, exact);
-2. the whole grid solves the field (FFT_X), and every strip copies its columns of E and of the ions' accumulated E;
+2. the whole grid solves the field (FFT_X, or CG with the multigrid preconditioner for walled domains), and every
+   strip copies its columns of E and of the ions' accumulated E;
 3. every strip pushes, collides and ends the step;
 4. the particles that ended the step in ghost columns move to the neighbour owning them, as records of 8 doubles
    (the counts first, then the records). Their charge stays where the sender deposited it.
@@ -20,7 +22,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import PREC_MIXED, Simulation
+from . import PREC_MIXED, WARM_PREVIOUS, Simulation
 from .cluster import ID_SPACE, _Buffer
 
 REC = 8   # doubles per record: x, y (local cells), vx, vy, vz, id, tag, 0
@@ -39,13 +41,31 @@ def partition(ncx, n_strips):
     return out
 
 
-def split_particles(x, ncx, parts, ghost):
-    """For global positions x (periodic, [0, ncx)): the strip owning each particle and its local x."""
+def frames(parts, ghost, periodic):
+    """(ghost columns on the left, on the right, global column of local column 0) of each strip: no ghost columns
+    on a side that is the wall of a walled domain."""
+    n = len(parts)
+    out = []
+    for r, (x0, _) in enumerate(parts):
+        gl = ghost if periodic or r > 0 else 0
+        gr = ghost if periodic or r < n - 1 else 0
+        out.append((gl, gr, x0 - gl))
+    return out
+
+
+def split_particles(x, parts, x_firsts):
+    """For global positions x: the strip owning each particle and its local x."""
     x = np.asarray(x, dtype=np.float64)
     starts = np.array([p[0] for p in parts])
     owner = np.searchsorted(starts, np.floor(x), side="right") - 1
-    local = x - (starts[owner] - ghost)
+    local = x - np.asarray(x_firsts)[owner]
     return owner, local
+
+
+def shift(x_first_from, x_first_to, wrap, ncx):
+    """x shift of a record from one strip's columns to another's; wrap = +1 / -1 when it crosses the periodic
+    boundary to the right / left."""
+    return float(x_first_from - x_first_to - wrap * ncx)
 
 
 class Strip:
@@ -56,17 +76,18 @@ class Strip:
                  fuse_collisions=True, id_base=None):
         self.field = field if field is not None else Simulation(deck, PREC_MIXED, sort_every=0, seed=seed)
         p = self.field.params
-        if not p.periodic_x:
-            raise ValueError("strips split a periodic-x domain")
         self.ncx, self.ncy = p.ncx, p.ncy
+        self.periodic = bool(p.periodic_x)
+        self.nx_global = p.ncx if self.periodic else p.ncx + 1   # node columns of the whole grid's arrays
         self.parts = partition(p.ncx, n_strips)
+        self.frames = frames(self.parts, int(ghost), self.periodic)
         self.n_strips, self.index, self.ghost = n_strips, index, int(ghost)
         self.x0, self.own = self.parts[index]
         if self.own <= self.ghost:
             raise ValueError("each strip needs more own columns than ghost columns")
-        self.x_first = self.x0 - self.ghost
+        gl, gr, self.x_first = self.frames[index]
         self.sim = Simulation(deck, PREC_MIXED, sort_every=sort_every, seed=seed, capacity=capacity,
-                              fuse_collisions=fuse_collisions, strip=(self.own, self.ghost))
+                              fuse_collisions=fuse_collisions, strip=(self.own, gl, gr, self.x_first))
         if id_base is not None:
             self.sim.set_id_base(id_base)
         self.nspec = 1 + p.n_ion_species
@@ -76,7 +97,7 @@ class Strip:
     # ----------------------------------------------------------------------------- particles
     def load(self, species, x, y, vx, vy, vz, ids, tags=None):
         """Uploads the particles of `species` (global positions) that this strip owns."""
-        owner, local = split_particles(x, self.ncx, self.parts, self.ghost)
+        owner, local = split_particles(x, self.parts, [f[2] for f in self.frames])
         m = owner == self.index
         self.sim.upload_particles(species, local[m], np.asarray(y)[m], np.asarray(vx)[m], np.asarray(vy)[m],
                                   np.asarray(vz)[m], ids=np.asarray(ids, dtype=np.uint32)[m],
@@ -85,26 +106,30 @@ class Strip:
     def download(self, species):
         """The strip's particles of `species` with global x in [0, ncx)."""
         d = self.sim.download_particles(species)
-        d["x"] = np.mod(d["x"] + self.x_first, self.ncx)
+        d["x"] = d["x"] + self.x_first
+        if self.periodic:
+            d["x"] = np.mod(d["x"], self.ncx)
         return d
 
     def shifts(self):
         """x shifts of the records sent to the left and to the right neighbour (their local columns)."""
-        left_own = self.parts[(self.index - 1) % self.n_strips][1]
-        return float(left_own), float(-self.own)
+        r, n = self.index, self.n_strips
+        lo, hi = (r - 1) % n, (r + 1) % n
+        return (shift(self.x_first, self.frames[lo][2], -1 if r == 0 else 0, self.ncx),
+                shift(self.x_first, self.frames[hi][2], 1 if r == n - 1 else 0, self.ncx))
 
     # ----------------------------------------------------------------------------- one step
     def add_density(self):
         """Adds the strip's densities into the whole grid's (edp_strip_add_density), on the strip's stream."""
         for s in range(self.nspec):
             ptr, _ = self.field.device_buffer(0, s)
-            self.sim._check(self.lib.edp_strip_add_density(self.sim.ctx, s, C.c_void_p(ptr), self.ncx, self.x_first),
-                            "edp_strip_add_density")
+            self.sim._check(self.lib.edp_strip_add_density(self.sim.ctx, s, C.c_void_p(ptr), self.nx_global,
+                                                           self.x_first), "edp_strip_add_density")
 
     def set_field(self):
         e, _ = self.field.device_buffer(1)
         a, _ = self.field.device_buffer(2)
-        self.sim._check(self.lib.edp_strip_set_field(self.sim.ctx, C.c_void_p(e), C.c_void_p(a), self.ncx,
+        self.sim._check(self.lib.edp_strip_set_field(self.sim.ctx, C.c_void_p(e), C.c_void_p(a), self.nx_global,
                                                      self.x_first), "edp_strip_set_field")
 
     def advance(self):
@@ -152,6 +177,18 @@ class Strip:
         self.sim.close()
 
 
+def _solve_field(field, t):
+    """UPDATE_WALL_POTENTIALS and the field of the whole grid, as edp_step solves it."""
+    f = field
+    f._check(f.lib.edp_update_wall_potentials(f.ctx, t), "edp_update_wall_potentials")
+    if f.periodic:
+        f.solve_poisson_fftx_linsysy()
+    else:
+        it = C.c_int32()
+        f._check(f.lib.edp_field_cg(f.ctx, 1e-8, 100000, WARM_PREVIOUS, C.byref(it)), "edp_field_cg")
+    f.synchronize()
+
+
 def _zero_field_density(field, nspec):
     import torch
     for s in range(nspec):
@@ -187,9 +224,7 @@ class LocalStrips:
             for s in self.strips:
                 s.add_density()
                 s.sim.synchronize()
-            f._check(f.lib.edp_update_wall_potentials(f.ctx, self.t), "edp_update_wall_potentials")
-            f.solve_poisson_fftx_linsysy()
-            f.synchronize()
+            _solve_field(f, self.t)
             for s in self.strips:
                 s.set_field()
                 s.advance()
@@ -255,9 +290,7 @@ class StripRank:
                     ptr, cnt = f.device_buffer(0, sp)
                     dist.all_reduce(torch.as_tensor(_Buffer(ptr, cnt, True, True), device="cuda"), group=self.group)
                 torch.cuda.synchronize()
-            f._check(f.lib.edp_update_wall_potentials(f.ctx, self.t), "edp_update_wall_potentials")
-            f.solve_poisson_fftx_linsysy()
-            f.synchronize()
+            _solve_field(f, self.t)
             s.set_field()
             s.advance()
             f._check(f.lib.edp_end_ion_cycle(f.ctx), "edp_end_ion_cycle")
@@ -280,10 +313,12 @@ class StripRank:
             if dist.get_backend(self.group) == "gloo":   # gloo moves host tensors point to point
                 left, right = left.cpu(), right.cpu()
             from_left, from_right = exchange_records(left, right, self.rank, self.world, self.group)
-            # what comes from the left neighbour was its right ghost: its shift is minus its own width
-            own_left = self.strip.parts[(self.rank - 1) % self.world][1]
-            self.strip.put(sp, from_left.to("cuda"), float(-own_left))
-            self.strip.put(sp, from_right.to("cuda"), float(self.strip.own))
+            # what comes from a neighbour was its ghost column on this side: shift from its columns into ours
+            st, r, n = self.strip, self.rank, self.world
+            lo, hi = (r - 1) % n, (r + 1) % n
+            self.strip.put(sp, from_left.to("cuda"), shift(st.frames[lo][2], st.x_first, 1 if r == 0 else 0, st.ncx))
+            self.strip.put(sp, from_right.to("cuda"), shift(st.frames[hi][2], st.x_first, -1 if r == n - 1 else 0,
+                                                            st.ncx))
             torch.cuda.synchronize()
 
     def close(self):

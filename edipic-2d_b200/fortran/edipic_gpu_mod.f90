@@ -208,10 +208,11 @@ module edipic_gpu
      end function edp_collect_moments
      ! x strips of a periodic domain (one cluster per strip along x, pic2d_ParticleExchange.f90); the record and
      ! density buffers are device memory the host allocates (cudaMalloc through its CUDA Fortran or C layer)
-     integer(c_int) function edp_set_strip(ctx, ghost) bind(C, name="edp_set_strip")
+     integer(c_int) function edp_set_strip(ctx, ghost_left, ghost_right, x_first, ncx_global, periodic) &
+          bind(C, name="edp_set_strip")
        import :: c_ptr, c_int, c_int32_t
        type(c_ptr), value :: ctx
-       integer(c_int32_t), value :: ghost
+       integer(c_int32_t), value :: ghost_left, ghost_right, x_first, ncx_global, periodic
      end function edp_set_strip
      integer(c_int) function edp_strip_take(ctx, species, left, cap_left, right, cap_right, n_left, n_right) &
           bind(C, name="edp_strip_take")

@@ -272,21 +272,24 @@ int edp_reduce_list(edp_ctx* ctx, int32_t max, void** ptr, int64_t* count, int32
  * (< 2^32); ranks sharing a cluster take disjoint ranges so that their random streams differ. After an upload
  * with ids, particles born later continue after the largest uploaded id, and never below base. */
 int edp_set_id_base(edp_ctx* ctx, uint64_t base);
-/* ---- x strips of a periodic domain (the reference's clusters along x, pic2d_ParticleExchange.f90:3-1762;
- * density halo sums GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1645-1800) ---------------------
- * A strip context covers its own columns plus `ghost` columns on each side: it is set up walled in x (CG
- * solver, never used) with ncx = own + 2 ghost, mixed precision, no inner objects and no wall emission, then
- * marked with edp_set_strip before any particle is uploaded. Its local column c is global column
- * x_first + c (periodic), x_first = first own column - ghost. Particles moving out of the strip and its ghost
- * columns in one step are an error (EDP_ERR_BOUNDS at the next check); the y walls count their hits as objects
- * 0 (below) and 1 (above), as the periodic domain does. Per step, for each species: zero the global density
- * of a context holding the whole periodic grid (edp_device_buffer), edp_strip_add_density from every strip (sum
- * over ranks), edp_field_fftx on the whole grid, edp_strip_set_field into every strip, the strip's own
- * advance / collide / end_ion_cycle calls, then edp_strip_take and edp_strip_put to move the particles that
- * ended the step in ghost columns to the neighbour owning them. Their charge was deposited by the sender. */
-int edp_set_strip(edp_ctx* ctx, int32_t ghost);
-/* Takes the particles of species `species` in the left (local columns < ghost) and right (>= ncx - ghost)
- * ghost columns out of the strip into caller device buffers of records of 8 doubles (x, y in local cells, vx,
+/* ---- x strips of a domain (the reference's clusters along x, pic2d_ParticleExchange.f90:3-1762; density sums
+ * of the shared nodes GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1645-1800) ----------------------
+ * A strip context covers its own columns plus ghost columns on each side that faces another strip (none on a side
+ * that is the domain's wall; in a periodic domain every side faces a strip). It is set up walled in x (CG solver,
+ * never used) with ncx = own + ghost_left + ghost_right, mixed precision, metal inner objects only (in its own
+ * columns: shifted by -x_first) and no wall emission, then marked with edp_set_strip before any particle is
+ * uploaded. Its local column c is global column x_first + c (modulo ncx_global when periodic). Particles that leave
+ * the strip and its ghost columns through a side that is not the domain's wall in one step are an error
+ * (EDP_ERR_BOUNDS at the next check); walls count their hits as the whole domain does. Per step, for each species:
+ * zero the density of a context holding the whole grid (edp_device_buffer), edp_strip_add_density from every strip
+ * (sum over ranks), the field solve on the whole grid (edp_field_fftx or edp_field_cg), edp_strip_set_field into
+ * every strip, the strip's own advance / collide / end_ion_cycle calls, then edp_strip_take and edp_strip_put to
+ * move the particles that ended the step in ghost columns to the neighbour owning them. Their charge was deposited
+ * by the sender. */
+int edp_set_strip(edp_ctx* ctx, int32_t ghost_left, int32_t ghost_right, int32_t x_first, int32_t ncx_global,
+                  int32_t periodic);
+/* Takes the particles of species `species` in the left (local columns < ghost_left) and right
+ * (>= ncx - ghost_right) ghost columns out of the strip into caller device buffers of records of 8 doubles (x, y in local cells, vx,
  * vy, vz, id, tag, 0): left[cap_left * 8], right[cap_right * 8]; n_left / n_right receive the counts.
  * EDP_ERR_CAPACITY when a buffer is too small (the particles past it are lost). Synchronises. */
 int edp_strip_take(edp_ctx* ctx, int32_t species, double* left, int64_t cap_left, double* right, int64_t cap_right,
@@ -294,8 +297,9 @@ int edp_strip_take(edp_ctx* ctx, int32_t species, double* left, int64_t cap_left
 /* Appends n records (device buffer, edp_strip_take's layout) with x shifted by x_shift cells, keeping their ids
  * and tags and depositing nothing. */
 int edp_strip_put(edp_ctx* ctx, int32_t species, const double* records, int64_t n, double x_shift);
-/* Adds the strip's fixed-point density of one species into global_dev[(ncy + 1) * nx_global] (the node layout
- * of a periodic context, column c at (x_first + c) mod nx_global), on the strip's stream. */
+/* Adds the strip's fixed-point density of one species into global_dev[(ncy + 1) * nx_global] (the internal node
+ * layout of the whole-grid context: nx_global = ncx periodic, ncx + 1 walled; column c at (x_first + c) mod
+ * nx_global), on the strip's stream. */
 int edp_strip_add_density(edp_ctx* ctx, int32_t species, uint64_t* global_dev, int32_t nx_global, int32_t x_first);
 /* Copies the strip's columns of a whole-grid field (float2 (Ex, Ey) per node, layout as above) and of its
  * accumulated field for the ions into the strip. */

@@ -1,4 +1,4 @@
-"""A periodic domain cut into x strips against one context holding the whole domain. The strips push their own
+"""A domain cut into x strips against one context holding the whole domain. The strips push their own
 particles against their columns of the whole grid's field, deposit into their own and ghost nodes, sum the densities
 into the whole grid and hand the particles that end a step in ghost columns to the neighbour owning them. Without
 ionisation (whose new ids depend on the order of creation) the union of the strips' particles, the potential and the
@@ -32,7 +32,7 @@ def _plasma(sim, n=30000):
     return e, i, ids, tags
 
 
-def _reference(deck, sort_every, steps):
+def _reference(deck, sort_every, steps, n_hits=2):
     from edipic_b200 import ELECTRONS, FIELD_PHI, IONS, Simulation
     with Simulation(deck, sort_every=sort_every, fuse_collisions=True) as sim:
         e, i, ids, tags = _plasma(sim)
@@ -41,7 +41,7 @@ def _reference(deck, sort_every, steps):
         sim.step(steps)
         c = sim.counters()
         return ((e, i, ids, tags), [sim.download_particles(s) for s in (ELECTRONS, IONS)], sim.field(FIELD_PHI),
-                list(c.electron_hits[:2]), list(c.ion_hits[:2]))
+                list(c.electron_hits[:n_hits]), list(c.ion_hits[:n_hits]))
 
 
 @pytest.mark.gpu
@@ -67,6 +67,36 @@ def test_strips_equal_one_context(tmp_path, n_strips, sort_every):
     assert np.array_equal(phi, phi_ref)
     assert c["electron_hits"][:2] == eh and c["ion_hits"][:2] == ih
     assert sum(eh) > 0 and min(moved) > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_strips", [2, 3])
+def test_walled_strips_equal_one_context(tmp_path, n_strips):
+    """The walled domain with the metal rectangle at -100 V across the strip boundary, the field by multigrid PCG on
+    the whole grid: the end strips have the domain's walls instead of ghost columns, and the rectangle absorbs in
+    every strip it reaches. Same particles and wall hits as one context."""
+    from edipic_b200 import ELECTRONS, FIELD_PHI, IONS
+    from edipic_b200.strips import LocalStrips
+    deck = small_deck(tmp_path, "walled", collisions=False, wall_potentials={2: 5.0, 4: -3.0})
+    (e, i, ids, tags), ref, phi_ref, eh, ih = _reference(deck, 4, STEPS, n_hits=8)
+    with LocalStrips(deck, n_strips, ghost=4, sort_every=4) as ls:
+        assert [s.frames[s.index][:2] for s in ls.strips][0][0] == 0   # the left wall takes no ghost columns
+        ls.load(ELECTRONS, *e, ids=ids, tags=tags)
+        ls.load(IONS, *i, ids=ids, tags=tags)
+        ls.step(STEPS)
+        got = [ls.download(s) for s in (ELECTRONS, IONS)]
+        phi = ls.field.field(FIELD_PHI)
+        c = ls.counters()
+    # CG sums its dot products with atomics in an order that varies from run to run, so the potential of two runs
+    # agrees to rounding, not to the bit; the FP32 field and the particles almost always do
+    for s in range(2):
+        a, ia, ta = _rows(got[s])
+        b, ib, tb = _rows(ref[s])
+        assert np.array_equal(ia, ib) and np.array_equal(ta, tb)
+        assert np.abs(a - b).max() < 1e-6
+    assert np.abs(phi - phi_ref).max() <= 1e-10 * np.abs(phi_ref).max()
+    assert c["electron_hits"] == eh and c["ion_hits"] == ih
+    assert eh[2] > 0 and eh[3] > 0 and eh[4] > 0   # left and right walls and the rectangle took electrons
 
 
 @pytest.mark.gpu
@@ -100,10 +130,10 @@ def test_strip_api_refusals(tmp_path):
     deck = small_deck(tmp_path, "periodic", collisions=False)
     with Simulation(deck) as sim:   # the whole periodic domain is not a strip
         with pytest.raises(EdpError):
-            sim._check(sim.lib.edp_set_strip(sim.ctx, 4), "edp_set_strip")
+            sim._check(sim.lib.edp_set_strip(sim.ctx, 4, 4, -4, 64, 1), "edp_set_strip")
         nl, nr = C.c_int64(), C.c_int64()
         assert sim.lib.edp_strip_take(sim.ctx, 0, None, 0, None, 0, C.byref(nl), C.byref(nr)) == -7
-    with Simulation(deck, strip=(32, 4)) as st:
+    with Simulation(deck, strip=(32, 4, 4, -4)) as st:
         assert st.params.ncx == 40 and not st.periodic
         with pytest.raises(EdpError):   # no wall emission on a strip
             st.set_ion_emission(0, 1, 0.1, 0.0, 100.0, 2.0)
@@ -111,7 +141,7 @@ def test_strip_api_refusals(tmp_path):
         assert st.lib.edp_strip_put(st.ctx, 0, C.c_void_p(rec.data_ptr()), 1, 0.0) == -7   # before the upload
         x = np.array([10.5])
         st.upload_particles(ELECTRONS, x, x, 0 * x, 0 * x, 0 * x)
-        assert st.lib.edp_set_strip(st.ctx, 4) == -7   # after the upload
+        assert st.lib.edp_set_strip(st.ctx, 4, 4, -4, 64, 1) == -7   # after the upload
 
 
 def _rank_worker(rank, world, port, deck, out):

@@ -10,7 +10,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from edipic_b200.strips import REC, exchange_records, partition, split_particles
+from edipic_b200.strips import REC, exchange_records, frames, partition, shift, split_particles
 
 
 def test_partition_covers_the_columns():
@@ -23,33 +23,42 @@ def test_partition_covers_the_columns():
         partition(4, 5)
 
 
-def test_owner_and_local_position():
+@pytest.mark.parametrize("periodic", [True, False])
+def test_owner_and_local_position(periodic):
     ncx, ghost = 64, 4
     parts = partition(ncx, 3)   # 22, 21, 21
-    x = np.array([0.0, 21.999, 22.0, 42.5, 43.0, 63.75])
-    owner, local = split_particles(x, ncx, parts, ghost)
-    assert list(owner) == [0, 0, 1, 1, 2, 2]
+    fr = frames(parts, ghost, periodic)
+    if not periodic:   # the walls of the domain take no ghost columns
+        assert fr[0][0] == 0 and fr[2][1] == 0 and fr[1] == (ghost, ghost, 22 - ghost)
+    x = np.array([0.0, 21.999, 22.0, 42.5, 43.0, 63.75] + ([] if periodic else [64.0]))
+    owner, local = split_particles(x, parts, [f[2] for f in fr])
+    assert list(owner) == [0, 0, 1, 1, 2, 2] + ([] if periodic else [2])
     for o, xl, xg in zip(owner, local, x):
         x0, own = parts[o]
-        assert ghost <= xl < ghost + own and xl == xg - (x0 - ghost)
+        gl = fr[o][0]
+        assert gl <= xl <= gl + own and xl == xg - fr[o][2]
 
 
+@pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("n", [1, 2, 3, 5])
-def test_shifts_carry_ghost_particles_to_the_owner(n):
+def test_shifts_carry_ghost_particles_to_the_owner(n, periodic):
     """A particle in a ghost column of strip r, shifted as it is sent, lands in its neighbour's own columns at the
-    same global (periodic) position."""
+    same global position."""
     ncx, ghost = 60, 3
     parts = partition(ncx, n)
+    fr = frames(parts, ghost, periodic)
     for r, (x0, own) in enumerate(parts):
-        left_own = parts[(r - 1) % n][1]
-        for xl, side in ((0.25, "left"), (ghost - 0.5, "left"), (ghost + own + 0.5, "right"),
-                         (own + 2 * ghost - 0.25, "right")):
-            xg = (x0 - ghost + xl) % ncx
+        gl, gr, xf = fr[r]
+        cases = [(0.25, "left"), (gl - 0.5, "left")] if gl else []
+        cases += [(gl + own + 0.5, "right"), (gl + own + gr - 0.25, "right")] if gr else []
+        for xl, side in cases:
+            xg = (xf + xl) % ncx
             q = (r - 1) % n if side == "left" else (r + 1) % n
-            x_new = xl + (left_own if side == "left" else -own)
+            wrap = (-1 if r == 0 else 0) if side == "left" else (1 if r == n - 1 else 0)
+            x_new = xl + shift(xf, fr[q][2], wrap, ncx)
             qx0, qown = parts[q]
-            assert ghost <= x_new < ghost + qown
-            assert abs((qx0 - ghost + x_new) % ncx - xg) < 1e-12
+            assert fr[q][0] <= x_new < fr[q][0] + qown
+            assert abs((fr[q][2] + x_new) % ncx - xg) < 1e-12
 
 
 def _exchange_worker(rank, world, port, out):
