@@ -755,6 +755,8 @@ int edp_upload_particles(edp_ctx* c, int sp, int64_t n, const double* x, const d
 {
     if (!c || sp < 0 || sp >= c->nspec || n < 0 || (n > 0 && (!x || !y || !vx || !vy || !vz)))
         return edp_fail(c, EDP_ERR_ARG, "edp_upload_particles: bad arguments");
+    if (!id && c->id_base + (uint64_t)n > c->id_end)
+        return edp_fail(c, EDP_ERR_CAPACITY, "edp_upload_particles: more particles than ids left in the context's range");
     TRY(alloc_species(c, sp, n));
     // staging copies of the host columns
     double* dbuf = nullptr;
@@ -802,6 +804,8 @@ int edp_distribute_particles(edp_ctx* c, int sp, int32_t per_cell, double fconv,
     if (!c || sp < 0 || sp >= c->nspec || per_cell < 1) return edp_fail(c, EDP_ERR_ARG, "edp_distribute_particles");
     if (copy_pos && (sp == 0 || !c->uploaded[0])) return edp_fail(c, EDP_ERR_STATE, "electrons must be distributed first");
     const int64_t n = (int64_t)per_cell * c->p.ncx * c->p.ncy;
+    if (c->id_base + (uint64_t)n > c->id_end)
+        return edp_fail(c, EDP_ERR_CAPACITY, "edp_distribute_particles: more particles than ids left in the context's range");
     if (copy_pos && (n != c->host_slots[0] || c->sorted_end[0] != 0))
         return edp_fail(c, EDP_ERR_STATE, "ions copy electron positions: same per_cell, before the electron sort");
     TRY(alloc_species(c, sp, n));
@@ -1249,11 +1253,18 @@ int edp_end_ion_cycle(edp_ctx* c)
     return finish_sync(c);
 }
 
+int edp_set_id_range(edp_ctx* c, uint64_t base, uint64_t end)
+{
+    if (!c || base >= end || end > (1ull << 32)) return edp_fail(c, EDP_ERR_ARG, "edp_set_id_range");
+    c->id_base = base;
+    c->id_end = end;
+    return EDP_OK;
+}
+
 int edp_set_id_base(edp_ctx* c, uint64_t base)
 {
     if (!c || base >= (1ull << 32)) return edp_fail(c, EDP_ERR_ARG, "edp_set_id_base");
-    c->id_base = base;
-    return EDP_OK;
+    return edp_set_id_range(c, base, 1ull << 32);
 }
 
 int edp_reduce_list(edp_ctx* c, int32_t max, void** ptr, int64_t* count, int32_t* is_int64, int32_t* n_out)
@@ -1332,6 +1343,8 @@ int edp_query_counters(edp_ctx* c, edp_counters* out)
     if (c->hc->error_flags & EDP_EFLAG_PENDING) return edp_fail(c, EDP_ERR_CAPACITY, "add-list capacity exceeded");
     if (c->hc->error_flags & EDP_EFLAG_BOUNDS) return edp_fail(c, EDP_ERR_BOUNDS, "particle outside the domain");
     if (c->hc->error_flags & EDP_EFLAG_TIMEOUT) return edp_fail(c, EDP_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (c->hc->error_flags & EDP_EFLAG_IDS)
+        return edp_fail(c, EDP_ERR_CAPACITY, "particle id range used up: born particles were not appended");
     if (c->hc->error_flags & EDP_EFLAG_SEE_MODEL)
         return edp_fail(c, EDP_ERR_STATE, "elastic + inelastic emission coefficients above 1 (secondary emission model)");
     return EDP_OK;

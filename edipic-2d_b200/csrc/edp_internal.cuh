@@ -37,6 +37,7 @@
 #define EDP_EFLAG_PENDING 4
 #define EDP_EFLAG_TIMEOUT 8   // a bounded device-side wait gave up
 #define EDP_EFLAG_SEE_MODEL 16   // elastic + inelastic emission coefficients above 1 at some electron impact
+#define EDP_EFLAG_IDS 32         // a born particle found the context's id range used up (not appended)
 
 struct edp_chunk {      // one CTA work item of the sorted push
     int64_t start, end; // slot range
@@ -152,6 +153,7 @@ struct edp_ctx {
     int64_t sorted_end[EDP_MAX_SPECIES] = {0};   // slots [0, sorted_end) are tile-sorted
     int64_t steps_since_sort = 0;
     uint64_t id_base = 0;             // first id of the particles this context creates (distribution, upload)
+    uint64_t id_end = 1ull << 32;     // one past the last id of the context's range (edp_set_id_range)
     uint32_t dirty = 0;               // bit s: species s's density was deposited since the last edp_reduce_list
     int uploaded[EDP_MAX_SPECIES] = {0};
 

@@ -27,7 +27,8 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[EDP_NOALLOC_MAX_DEVICES] = {nullptr};
 
 // host-side set-up, once per device with that device current: the array's name is only a host-side stand-in,
-// the kernels need the device address
+// the kernels need the device address. The address is kept for the life of the process; cudaDeviceReset would
+// make it stale, which the header tells callers.
 int scratch_address(void** out)
 {
     int dev = 0;
@@ -157,6 +158,9 @@ extern "C" int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* 
                                         double phi_top, double* phi_dev, void* stream)
 {
     if (ncx < 4 || ncy < 2 || (ncx & (ncx - 1)) != 0 || ncx > 4096 || !rho_dev || !phi_dev) return EDP_ERR_ARG;
+    // an error left pending by the caller's earlier work is reported here, before anything is queued, and stays
+    // pending; the status returned at the end then belongs to this call's own launches
+    if (cudaPeekAtLastError() != cudaSuccess) return EDP_ERR_CUDA;
     const int nm = ncx / 2 + 1;
     // workspace sections, each starting on a 256-byte boundary (double2 accesses need 16-byte alignment)
     auto align256 = [](size_t b) { return (b + 255) & ~(size_t)255; };

@@ -794,6 +794,7 @@ struct AppendArgs {
     unsigned long long* n_slots;
     unsigned long long* n_live;
     unsigned long long* next_id;
+    unsigned long long id_end;   // one past the context's last id
     unsigned long long* rho_fix;
     double* rho_d;
     edp_dev_counters* dc;
@@ -811,7 +812,12 @@ __global__ void append_kernel(AppendArgs a)
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nread; k += (int64_t)gridDim.x * blockDim.x) {
         double X = a.src.x[k], Y = a.src.y[k];
         double vx = a.src.vx[k], vy = a.src.vy[k], vz = a.src.vz[k];
-        uint32_t id = (uint32_t)atomicAdd(a.next_id, 1ull);
+        const unsigned long long id_l = atomicAdd(a.next_id, 1ull);
+        if (id_l >= a.id_end) {   // the range is used up: an id of another rank's range would repeat its streams
+            atomicOr(&a.dc->error_flags, EDP_EFLAG_IDS);
+            continue;
+        }
+        const uint32_t id = (uint32_t)id_l;
         unsigned long long slot = atomicAdd(a.n_slots, 1ull);
         if ((int64_t)slot >= a.cap) {
             atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
@@ -1194,6 +1200,7 @@ static AppendArgs append_args(edp_ctx* c, int sp)
     a.n_slots = &c->dc->n_slots[sp];
     a.n_live = &c->dc->n_live[sp];
     a.next_id = &c->dc->next_id[sp];
+    a.id_end = (unsigned long long)c->id_end;
     a.rho_fix = c->rho_fix[sp];
     a.rho_d = c->rho_d[sp];
     a.dc = c->dc;

@@ -21,9 +21,11 @@ __device__ __forceinline__ int pos_mod(int a, int n)
     return r < 0 ? r + n : r;
 }
 
+// A particle leaves the strip only when its record was written: one past a full buffer stays in its ghost column,
+// is still counted in cnt, and a later call with a larger buffer takes it.
 __global__ void strip_take_kernel(edp_kparams kp, edp_species_mixed P, const unsigned long long* n_slots,
                                   double* left, int64_t cap_l, double* right, int64_t cap_r, unsigned long long* cnt,
-                                  unsigned long long* n_live, unsigned int* eflag)
+                                  unsigned long long* n_live)
 {
     const int64_t n = (int64_t)*n_slots;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -43,11 +45,9 @@ __global__ void strip_take_kernel(edp_kparams kp, edp_species_mixed P, const uns
             r[5] = (double)P.id[k];
             r[6] = (double)P.tag[k];
             r[7] = 0.0;
-        } else {
-            atomicOr(eflag, EDP_EFLAG_CAPACITY);
+            P.cell[k] = -1;
+            atomicAdd(n_live, (unsigned long long)(-1LL));
         }
-        P.cell[k] = -1;
-        atomicAdd(n_live, (unsigned long long)(-1LL));
     }
 }
 
@@ -176,15 +176,19 @@ int edp_strip_take(edp_ctx* c, int32_t sp, double* left, int64_t cap_left, doubl
     EDP_CUDA(c, cudaMemsetAsync(c->strip_cnt, 0, 2 * sizeof(unsigned long long), c->stream));
     ++c->launches;
     strip_take_kernel<<<grid_for_n(c->host_slots[sp]), 256, 0, c->stream>>>(
-        c->kp, c->pm[sp], &c->dc->n_slots[sp], left, cap_left, right, cap_right, c->strip_cnt, &c->dc->n_live[sp],
-        &c->dc->error_flags);
+        c->kp, c->pm[sp], &c->dc->n_slots[sp], left, cap_left, right, cap_right, c->strip_cnt, &c->dc->n_live[sp]);
     EDP_CUDA(c, cudaGetLastError());
     unsigned long long h[2];
     EDP_CUDA(c, cudaMemcpyAsync(h, c->strip_cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
     *n_left = (int64_t)h[0];
     *n_right = (int64_t)h[1];
-    return check_flags(c);
+    int r = check_flags(c);
+    if (r != EDP_OK) return r;
+    // not a device error flag: the context stays usable, and the particles past the buffers are still in the strip
+    if ((int64_t)h[0] > cap_left || (int64_t)h[1] > cap_right)
+        return edp_fail(c, EDP_ERR_CAPACITY, "edp_strip_take: record buffer smaller than the ghost-column count");
+    return EDP_OK;
 }
 
 int edp_strip_put(edp_ctx* c, int32_t sp, const double* rec, int64_t n, double x_shift)

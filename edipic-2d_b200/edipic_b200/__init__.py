@@ -181,9 +181,13 @@ class Simulation:
         self._check(self.lib.edp_get_stream(self.ctx, C.byref(ptr)), "edp_get_stream")
         return ptr.value or 0
 
-    def set_id_base(self, base):
-        """First id of the particles the context creates from now on (disjoint ranges for ranks of a cluster)."""
-        self._check(self.lib.edp_set_id_base(self.ctx, int(base)), "edp_set_id_base")
+    def set_id_base(self, base, end=None):
+        """First id of the particles the context creates from now on, and one past its last (disjoint ranges for
+        ranks of a cluster; born particles past the end are refused, edp_set_id_range)."""
+        if end is None:
+            self._check(self.lib.edp_set_id_base(self.ctx, int(base)), "edp_set_id_base")
+        else:
+            self._check(self.lib.edp_set_id_range(self.ctx, int(base), int(end)), "edp_set_id_range")
 
     def reduce_list(self):
         """[(device pointer, count, is_int64)] of the densities deposited since the last call (edp_reduce_list)."""

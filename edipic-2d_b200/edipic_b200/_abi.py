@@ -122,6 +122,7 @@ SIGNATURES = {
     "edp_step": [_CTX, C.c_int32],
     "edp_set_step": [_CTX, C.c_int64],
     "edp_set_id_base": [_CTX, C.c_uint64],
+    "edp_set_id_range": [_CTX, C.c_uint64, C.c_uint64],
     "edp_reduce_list": [_CTX, C.c_int32, P(C.c_void_p), _I64, _I32, _I32],
     "edp_set_strip": [_CTX, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
     "edp_strip_take": [_CTX, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, _I64, _I64],

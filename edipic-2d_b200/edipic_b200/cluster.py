@@ -58,7 +58,7 @@ class ClusterShare:
     def __init__(self, sim, rank, world, group=None, blocking=False, device=True):
         self.sim, self.rank, self.world, self.group, self.blocking = sim, rank, world, group, blocking
         self.device = device
-        sim.set_id_base(rank * (ID_SPACE // world))
+        sim.set_id_base(rank * (ID_SPACE // world), (rank + 1) * (ID_SPACE // world))
 
     def reduce(self):
         """GATHER_*_CHARGE_DENSITY's cluster reduce: call after the distribution or upload and after every step."""

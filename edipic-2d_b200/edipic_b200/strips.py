@@ -89,7 +89,7 @@ class Strip:
         self.sim = Simulation(deck, PREC_MIXED, sort_every=sort_every, seed=seed, capacity=capacity,
                               fuse_collisions=fuse_collisions, strip=(self.own, gl, gr, self.x_first))
         if id_base is not None:
-            self.sim.set_id_base(id_base)
+            self.sim.set_id_base(*id_base) if isinstance(id_base, tuple) else self.sim.set_id_base(id_base)
         self.nspec = 1 + p.n_ion_species
         self.lib = self.sim.lib
         self._bufs = {}
@@ -158,9 +158,18 @@ class Strip:
         cap = live * 2 * (self.ghost + 1) // self.own + 65536
         left, right = self._buffer(species, 0, cap), self._buffer(species, 1, cap)
         nl, nr = C.c_int64(), C.c_int64()
-        self.sim._check(self.lib.edp_strip_take(self.sim.ctx, species, C.c_void_p(left.data_ptr()), left.shape[0],
-                                                C.c_void_p(right.data_ptr()), right.shape[0], C.byref(nl),
-                                                C.byref(nr)), "edp_strip_take")
+        rc = self.lib.edp_strip_take(self.sim.ctx, species, C.c_void_p(left.data_ptr()), left.shape[0],
+                                     C.c_void_p(right.data_ptr()), right.shape[0], C.byref(nl), C.byref(nr))
+        if rc == -3 and (nl.value > left.shape[0] or nr.value > right.shape[0]):
+            # the particles past the buffers stayed in the strip: keep the records taken, take the rest
+            got_l, got_r = left[:min(nl.value, left.shape[0])].clone(), right[:min(nr.value, right.shape[0])].clone()
+            more_l, more_r = self._buffer(species, 0, nl.value), self._buffer(species, 1, nr.value)
+            rc = self.lib.edp_strip_take(self.sim.ctx, species, C.c_void_p(more_l.data_ptr()), more_l.shape[0],
+                                         C.c_void_p(more_r.data_ptr()), more_r.shape[0], C.byref(nl), C.byref(nr))
+            self.sim._check(rc, "edp_strip_take")
+            import torch
+            return torch.cat([got_l, more_l[:nl.value]]), torch.cat([got_r, more_r[:nr.value]])
+        self.sim._check(rc, "edp_strip_take")
         return left[:nl.value], right[:nr.value]
 
     def put(self, species, records, shift):
@@ -202,7 +211,8 @@ class LocalStrips:
     def __init__(self, deck, n_strips, ghost=4, sort_every=None, seed=None, capacity=None, fuse_collisions=True):
         self.field = Simulation(deck, PREC_MIXED, sort_every=0, seed=seed)
         self.strips = [Strip(deck, n_strips, r, ghost, self.field, sort_every, seed, capacity, fuse_collisions,
-                             id_base=r * (ID_SPACE // n_strips)) for r in range(n_strips)]
+                             id_base=(r * (ID_SPACE // n_strips), (r + 1) * (ID_SPACE // n_strips)))
+                       for r in range(n_strips)]
         self.nspec = self.strips[0].nspec
         self.t = 0
 
@@ -270,7 +280,7 @@ class StripRank:
                  fuse_collisions=True):
         self.rank, self.world, self.group = rank, world, group
         self.strip = Strip(deck, world, rank, ghost, None, sort_every, seed, capacity, fuse_collisions,
-                           id_base=rank * (ID_SPACE // world))
+                           id_base=(rank * (ID_SPACE // world), (rank + 1) * (ID_SPACE // world)))
         self.field = self.strip.field
         self.nspec = self.strip.nspec
         self.t = 0

@@ -206,6 +206,12 @@ module edipic_gpu
        integer(c_int), value :: species
        real(c_float), intent(out) :: out(*)
      end function edp_collect_moments
+     ! ids of the particles this context creates stay in [base, end): ranks of one cluster take disjoint ranges
+     integer(c_int) function edp_set_id_range(ctx, base, end) bind(C, name="edp_set_id_range")
+       import :: c_ptr, c_int, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), value :: base, end
+     end function edp_set_id_range
      ! x strips of a periodic domain (one cluster per strip along x, pic2d_ParticleExchange.f90); the record and
      ! density buffers are device memory the host allocates (cudaMalloc through its CUDA Fortran or C layer)
      integer(c_int) function edp_set_strip(ctx, ghost_left, ghost_right, x_first, ncx_global, periodic) &

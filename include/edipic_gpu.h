@@ -272,6 +272,11 @@ int edp_reduce_list(edp_ctx* ctx, int32_t max, void** ptr, int64_t* count, int32
  * (< 2^32); ranks sharing a cluster take disjoint ranges so that their random streams differ. After an upload
  * with ids, particles born later continue after the largest uploaded id, and never below base. */
 int edp_set_id_base(edp_ctx* ctx, uint64_t base);
+/* The same with the end of the range: ids stay in [base, end), end <= 2^32 (edp_set_id_base takes end = 2^32).
+ * Distribution and uploads without ids that need more ids than the range holds return EDP_ERR_CAPACITY. A particle
+ * born after the range is used up is not appended (its id would belong to another rank and repeat that particle's
+ * random streams); the next edp_query_counters returns EDP_ERR_CAPACITY. */
+int edp_set_id_range(edp_ctx* ctx, uint64_t base, uint64_t end);
 /* ---- x strips of a domain (the reference's clusters along x, pic2d_ParticleExchange.f90:3-1762; density sums
  * of the shared nodes GATHER_ELECTRON_CHARGE_DENSITY pic2d_ElectronDynamics.f90:1645-1800) ----------------------
  * A strip context covers its own columns plus ghost columns on each side that faces another strip (none on a side
@@ -291,7 +296,10 @@ int edp_set_strip(edp_ctx* ctx, int32_t ghost_left, int32_t ghost_right, int32_t
 /* Takes the particles of species `species` in the left (local columns < ghost_left) and right
  * (>= ncx - ghost_right) ghost columns out of the strip into caller device buffers of records of 8 doubles (x, y in local cells, vx,
  * vy, vz, id, tag, 0): left[cap_left * 8], right[cap_right * 8]; n_left / n_right receive the counts.
- * EDP_ERR_CAPACITY when a buffer is too small (the particles past it are lost). Synchronises. */
+ * When a side holds more particles than its buffer, the call returns EDP_ERR_CAPACITY: the first cap records of
+ * that side are written and those particles leave the strip, the others stay in their ghost columns, and n_left /
+ * n_right receive the whole counts found. The context stays usable; a caller moves the records it got and calls
+ * again with buffers of at least the remaining count. Synchronises. */
 int edp_strip_take(edp_ctx* ctx, int32_t species, double* left, int64_t cap_left, double* right, int64_t cap_right,
                    int64_t* n_left, int64_t* n_right);
 /* Appends n records (device buffer, edp_strip_take's layout) with x shifted by x_shift cells, keeping their ids
@@ -348,13 +356,16 @@ int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const doubl
  * are device buffers of the caller in the periodic reference layout, (ncx+2) x (ncy+1) FP64 nodes x fastest,
  * rho_dev holding factor_rho*(rho_i - rho_e); phi_bottom/phi_top are the normalised wall potentials; stream is
  * a cudaStream_t (NULL = default stream). The workspace is a file-scope device array of
- * EDP_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps until exit; (ncy+1)*(ncx/2+1)*24 +
- * ncx*8 bytes plus up to 512 bytes of section alignment must fit in it, else EDP_ERR_CAPACITY (1024 x 1023
- * cells fit). The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current; make it before any stream capture. All calls share
- * the array, so calls that overlap on the GPU race: order them on one stream. Work is queued on the stream and
- * the call returns without synchronising. */
-#define EDP_NOALLOC_SCRATCH_BYTES (8u << 20)
+ * EDP_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading this library keeps until exit; (ncy+1)*(ncx/2+1)*24 +
+ * ncx*8 bytes plus up to 512 bytes of section alignment must fit in it, else EDP_ERR_CAPACITY. The largest grids
+ * that fit: 512 x 2718, 1024 x 1360 (so the 1024 x 1024 grid fits, and 1024 x 1361 does not), 2048 x 680,
+ * 4096 x 339 cells. The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current and keeps it; make that call before any stream capture, and do not call this entry point
+ * on a device after cudaDeviceReset (the kept address would be stale). All calls share the array, so calls that
+ * overlap on the GPU race: order them on one stream. If a CUDA error from earlier work is pending on the calling
+ * thread, the call returns EDP_ERR_CUDA before it queues anything and leaves that error pending. Work is queued on
+ * the stream and the call returns without synchronising. */
+#define EDP_NOALLOC_SCRATCH_BYTES (16u << 20)
 int edp_poisson_fftx_noalloc(int32_t ncx, int32_t ncy, const double* rho_dev, double phi_bottom, double phi_top,
                              double* phi_dev, void* stream);
 

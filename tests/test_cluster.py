@@ -1,6 +1,6 @@
 """The host side of a cluster shared by several ranks (edipic_b200.cluster), as world-size-2 gloo process groups on
 the CPU: the listed int64 and FP64 buffers are summed in place over the ranks (exactly for int64), and each rank's id
-range is disjoint. Runs without a GPU."""
+range is disjoint and ends where the next rank's begins. Runs without a GPU."""
 import os
 import socket
 
@@ -19,8 +19,8 @@ class FakeSim:
         self.rho_i = np.linspace(0.0, 1.0, 7) * (rank + 1)
         self.base = None
 
-    def set_id_base(self, base):
-        self.base = base
+    def set_id_base(self, base, end=None):
+        self.base = (base, end)
 
     def reduce_list(self):
         return [(self.rho_e.ctypes.data, self.rho_e.size, True), (self.rho_i.ctypes.data, self.rho_i.size, False)]
@@ -49,4 +49,4 @@ def test_cluster_reduce_on_gloo():
     want_e = 2 * (np.arange(12, dtype=np.int64) * (1 << 33)) + 1
     assert np.array_equal(e0, want_e) and np.array_equal(e1, want_e)
     assert np.allclose(i0, np.linspace(0.0, 1.0, 7) * 3) and np.array_equal(i0, i1)
-    assert (b0, b1) == (0, 1 << 31)
+    assert (b0, b1) == ((0, 1 << 31), (1 << 31, 1 << 32))
