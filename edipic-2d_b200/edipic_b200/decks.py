@@ -65,13 +65,15 @@ def _segments():
 
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
-               ion_emission=None, ion_reflection=False, electron_emission=None, wall_injection=None):
+               ion_emission=None, ion_reflection=False, electron_emission=None, wall_injection=None, ez=0.0,
+               ions_sense_b=False, ions_sense_ez=False):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
     reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
     and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default.
     wall_injection: {wall (0 below, 1 above, 2 left, 3 right): (electrons per step, model, T_normal, T_parallel,
-    beam energy [eV])}, the constant electron emission of init_bo_NN.dat."""
+    beam energy [eV])}, the constant electron emission of init_bo_NN.dat. ez: uniform Z electric field [V/cm];
+    ions_sense_b / ions_sense_ez: the ions feel the magnetic / Z electric field (init_extfields.dat flags)."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -153,9 +155,9 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         "---ddddd.ddd--- BZ at y=Lsys [Gauss]", f"   {0.0:9.3f}",
         "---ddddd.ddd--- decay length below y_Bmax [cm]", f"   {1.0:9.3f}",
         "---ddddd.ddd--- decay length above y_Bmax [cm]", f"   {1.0:9.3f}",
-        "---ddddd.ddd--- Z-electric field [V/cm]", f"   {0.0:9.3f}",
-        "-------d------- ions sense magnetic field", f"       {0:1d}",
-        "-------d------- ions sense Z-electric field", f"       {0:1d}",
+        "---ddddd.ddd--- Z-electric field [V/cm]", f"   {ez:9.3f}",
+        "-------d------- ions sense magnetic field", f"       {int(bool(ions_sense_b)):1d}",
+        "-------d------- ions sense Z-electric field", f"       {int(bool(ions_sense_ez)):1d}",
     ])
 
     def bo(n, phi, amp=0.0, mhz=0.0, inj=(0.0, 0, 0.0, 0.0, 0.0), material="METAL1"):

@@ -202,14 +202,14 @@ int read_deck(const std::string& dir, edp_deck* d)
     p.n_of_particles_cell = (int32_t)nppc;
     // ---- scales (:719-723, :893-900)
     const double vte = std::sqrt(2.0 * Te * E_CL / M_E_KG);
-    const double wp = std::sqrt(Np * E_CL * E_CL / (EPS0 * M_E_KG));
+    const double wp = std::sqrt(Np * (E_CL * E_CL) / (EPS0 * M_E_KG));   // N e**2 / (eps0 m)
     const double ld = vte / wp;
     p.delta_x_m = ld / ncd;
     p.delta_t_s = p.delta_x_m / (nmv * vte);
     p.v_scale_ms = nmv * vte;
     p.e_scale_vm = M_E_KG * p.v_scale_ms / (E_CL * p.delta_t_s);
     p.b_scale_t = M_E_KG / (E_CL * p.delta_t_s);
-    p.f_scale_v = E_CL * Np * p.delta_x_m * p.delta_x_m / EPS0;
+    p.f_scale_v = E_CL * Np * (p.delta_x_m * p.delta_x_m) / EPS0;   // e N dx**2 / eps0, in the reference's order
     d->t_e = Te;
     d->n_plasma = Np;
     d->n_max_vel = (int32_t)nmv;
@@ -413,7 +413,7 @@ int read_deck(const std::string& dir, edp_deck* d)
         t.maxwell_rmax = R;
         t.maxwell_v = d->maxwell.data();
     }
-    t.energy_factor_eV = 0.5 * M_E_KG * p.v_scale_ms * p.v_scale_ms / E_CL;
+    t.energy_factor_eV = 0.5 * M_E_KG * (p.v_scale_ms * p.v_scale_ms) / E_CL;
     // ---- neutrals (pic2d_enCollisionsGeneralProc.f90:63-200)
     Lines nf(dir + "/init_neutrals.dat");
     if (!nf.ok) return EDP_OK;   // no neutrals: collisions off
@@ -539,7 +539,7 @@ int read_deck(const std::string& dir, edp_deck* d)
             t.rcx_vfactor[k] = std::sqrt(tgas * KB_JK / (Te * E_CL * p.ion_mass_me[k])) / (double)nmv;
             double tg_eV = tgas * KB_JK / E_CL;
             double l = 1.0 - alpha * std::log(std::fmax(1.5 * tg_eV, 0.001));
-            double sth = sig * l * l;
+            double sth = sig * (l * l);
             double vmean = std::sqrt(2.54647908947033 * tg_eV * E_CL / (p.ion_mass_me[k] * M_E_KG));
             t.rcx_probab_thermal[k] = ngas * sth * vmean * p.delta_t_s * p.n_subcycles;
         }

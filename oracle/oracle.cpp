@@ -1549,20 +1549,33 @@ int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* 
     double* phi = work + 3 * nn;
     double* ex = work + 4 * nn;
     double* ey = work + 5 * nn;
-    int64_t processed = e->n + ion->n;
-    // GATHER_ION_CHARGE_DENSITY / GATHER_ELECTRON_CHARGE_DENSITY (MainProgram:151-157)
-    deposit_threads(g, ion, c->ion_charge, rho_i, c->nthreads);
-    oracle_fold_and_wall_scale(g, rho_i);
+    double* acc_ex = work + 7 * nn;
+    double* acc_ey = work + 8 * nn;
+    const int32_t nsub = c->i_sp.nsub > 0 ? c->i_sp.nsub : 1;
+    const bool ion_step = c->n_sub_phase + 1 == nsub;
+    int64_t processed = e->n + (ion_step ? ion->n : 0);
+    // GATHER_ION_CHARGE_DENSITY when n_sub == 0 / GATHER_ELECTRON_CHARGE_DENSITY (MainProgram:151-157)
+    if (c->n_sub_phase == 0) {
+        deposit_threads(g, ion, c->ion_charge, rho_i, c->nthreads);
+        oracle_fold_and_wall_scale(g, rho_i);
+        std::fill(acc_ex, acc_ex + nn, 0.0);   // acc_E starts the ion cycle at zero
+        std::fill(acc_ey, acc_ey + nn, 0.0);
+    }
     deposit_threads(g, e, 1.0, rho_e, c->nthreads);
     oracle_fold_and_wall_scale(g, rho_e);
     for (int64_t q = 0; q < nn; ++q) rho[q] = c->factor_rho * (rho_i[q] - rho_e[q]);
-    // SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:182-191); acc_E == E for N_sub = 1
+    // SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY (:182-191), acc_E += E
     oracle_fftx_solve(g, rho, c->phi_bottom, c->phi_top, phi);
-    oracle_efield(g, phi, c->factor2_E, c->factor1_E, ex, ey, nullptr, nullptr);
+    oracle_efield(g, phi, c->factor2_E, c->factor1_E, ex, ey, acc_ex, acc_ey);
     // ADVANCE_ELECTRONS_PLUS (:210)
     push_threads(g, &c->e_sp, ex, ey, e, counters + 8, c->nthreads);
-    // ADVANCE_IONS_PLUS (:231)
-    push_threads(g, &c->i_sp, ex, ey, ion, counters + 8, c->nthreads);
+    if (!ion_step) {
+        c->n_sub_phase++;
+        c->mcc_ctx.step++;
+        return processed;
+    }
+    // ADVANCE_IONS_PLUS on the accumulated field (:231)
+    push_threads(g, &c->i_sp, acc_ex, acc_ey, ion, counters + 8, c->nthreads);
     // PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:275), PERFORM_RESONANT_CHARGE_EXCHANGE (:287)
     c->born_e.n = 0;
     c->born_i.n = 0;
@@ -1577,6 +1590,10 @@ int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* 
         double v[3] = {c->born_e.vx[k], c->born_e.vy[k], c->born_e.vz[k]};
         append(e, cap_e, c->born_e.x[k], c->born_e.y[k], v, c->next_id_e++);
     }
+    // CLEAR_ACCUMULATED_FIELDS (:303); n_sub = 0
+    std::fill(acc_ex, acc_ex + nn, 0.0);
+    std::fill(acc_ey, acc_ey + nn, 0.0);
+    c->n_sub_phase = 0;
     c->mcc_ctx.step++;
     return processed;
 }

@@ -266,13 +266,17 @@ typedef struct {
     oracle_parts_t born_e, born_i;
     int64_t cap_born;
     uint32_t next_id_e, next_id_i;  /* id of the next particle that joins (max id + 1 at the start) */
+    int32_t n_sub_phase;            /* n_sub of MainProg: electron steps since the last ion step (0 at the start) */
 } oracle_cycle_t;
 
-/* one electron+ion step with N_subcycles == 1 in the order of pic2d_MainProgram.f90:151-363:
- * gather densities, FFT_X solve, E, push electrons, push ions, MCC, RCX, append born ions, append born electrons.
- * Particle arrays must have room for the appended particles (cap). Returns particles processed. */
+/* one electron step in the order of pic2d_MainProgram.f90:151-363. The ion density is gathered only when
+ * n_sub == 0 (:151), the electron density every step; FFT_X solve; E, with acc_E += E (CALCULATE_ELECTRIC_FIELD_*);
+ * electron push. On the ion step (n_sub + 1 == N_subcycles, :196) the ions are pushed on acc_E with QM2sNsub and
+ * X += V N_subcycles (ADVANCE_IONS, pic2d_IonDynamics.f90:86-155), then MCC, RCX, the born ions and electrons
+ * join, acc_E is cleared (CLEAR_ACCUMULATED_FIELDS) and n_sub returns to 0. Particle arrays must have room for the
+ * appended particles (cap). work[9 * node grid] keeps rho_i and acc_E between calls. Returns particles pushed. */
 int64_t oracle_cycle_step(oracle_cycle_t* c, oracle_parts_t* e, oracle_parts_t* i, int64_t cap_e, int64_t cap_i,
-                          double* work /* 7 * node grid */, int64_t* counters /* [16] */);
+                          double* work /* 9 * node grid */, int64_t* counters /* [16] */);
 
 #ifdef __cplusplus
 }

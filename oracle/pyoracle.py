@@ -4,6 +4,7 @@ INITIATE_ELECTRON_NEUTRAL_COLLISIONS (pic2d_enCollisionsGeneralProc.f90:63-200) 
 deck reader. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module.
 """
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -67,7 +68,7 @@ class Cycle(C.Structure):
                 ("phi_bottom", C.c_double), ("phi_top", C.c_double), ("mcc", C.POINTER(MccTable)),
                 ("mcc_ctx", MccCtx), ("rcx", Rcx), ("rcx_on", C.c_int32), ("nthreads", C.c_int32),
                 ("born_e", Parts), ("born_i", Parts), ("cap_born", C.c_int64),
-                ("next_id_e", C.c_uint32), ("next_id_i", C.c_uint32)]
+                ("next_id_e", C.c_uint32), ("next_id_i", C.c_uint32), ("n_sub_phase", C.c_int32)]
 
 
 _lib = None
@@ -460,13 +461,230 @@ class MccTables:
                         dtype=np.int32)
 
 
+# ------------------------------------------------------------------------------------ deck reading
+# The oracle reads the init_*.dat decks itself, with the edit descriptors of the reference's READ statements, and
+# derives the normalisation and collision constants with the reference's formulas; nothing here comes from the
+# product's deck reader. Physical constants of pic2d_Modules.f90:161-168.
+E_CL, M_E_KG, EPS0_FM, AMU_KG, KB_JK, PI = 1.602189e-19, 9.109534e-31, 8.854188e-12, 1.660565e-27, 1.38064852e-23, \
+    3.141592653589793
+
+
+def fortran_field(line, skip, width, kind, decimals=0):
+    """One fixed-width field of a formatted Fortran READ: columns [skip, skip+width); blanks are ignored, an empty
+    field reads as zero, and a real field written without a decimal point carries `decimals` implied digits."""
+    f = line[skip:skip + width].replace(" ", "").replace("\t", "")
+    if kind == "i":
+        return int(f) if f else 0
+    if not f:
+        return 0.0
+    f = f.replace("d", "e").replace("D", "e")
+    mant = f.split("e")[0].split("E")[0]
+    v = float(f)
+    if "." not in mant and decimals:
+        v /= 10.0 ** decimals
+    return v
+
+
+class _Lines:
+    def __init__(self, path):
+        self.v = [ln.rstrip("\r") for ln in open(path).read().splitlines()]
+        self.k = 0
+
+    def next(self):
+        self.k += 1
+        return self.v[self.k - 1]
+
+    def value(self, skip, width, kind, decimals=0):
+        """a header line, then the value line (the deck layout of READ (9,'(A1)') buf; READ (9, fmt) value)"""
+        self.next()
+        return fortran_field(self.next(), skip, width, kind, decimals)
+
+
+def read_deck(directory):
+    """INITIATE_PARAMETERS (pic2d_CurProblemValues.f90), PREPARE_EXTERNAL_FIELDS (pic2d_ExternalFields.f90:36-145),
+    the boundary-object files of PREPARE_SETUP_VALUES (pic2d_Setup.f90:60-100), SET_ION_SPECIES (:1505-1507) and
+    the ion-neutral set-up (pic2d_inCollisionsGeneralProc.f90:3-90, pic2d_inCollisionsSpecificProc.f90:4-44) for
+    the deck subset the oracle's cycle covers: one cluster, metal or periodic boundary objects, rectangular inner
+    objects, uniform external fields, one neutral species. Returns a dict of module values."""
+    path = lambda fn: os.path.join(directory, fn)
+    d = {}
+    # SET_PHYSICAL_CONSTANTS (:3-55): eps_0 from init_physconstants.dat when it holds a positive value
+    eps0 = EPS0_FM
+    if os.path.exists(path("init_physconstants.dat")):
+        try:
+            v = float(open(path("init_physconstants.dat")).read().splitlines()[1].split()[0].replace("d", "e"))
+            if v > 0.0:
+                eps0 = v
+        except (IndexError, ValueError):
+            pass
+    d["eps_0_Fm"] = eps0
+    # init_configuration.dat (:157-330)
+    cf = _Lines(path("init_configuration.dat"))
+    T_e_eV = cf.value(3, 12, "f", 7)
+    N_plasma_m3 = cf.value(3, 14, "e", 7)
+    N_of_cells_debye = cf.value(3, 3, "i")
+    N_max_vel = cf.value(3, 3, "i")
+    N_blocks_x = cf.value(3, 3, "i")
+    N_blocks_y = cf.value(3, 3, "i")
+    N_grid_block_x = cf.value(3, 3, "i")
+    N_grid_block_y = cf.value(3, 3, "i")
+    N_of_particles_cell = cf.value(2, 4, "i")
+    cf.value(5, 1, "i")
+    cf.value(5, 1, "i")
+    cf.next()
+    ln = cf.next()
+    n_bo, n_io = fortran_field(ln, 3, 3, "i"), fortran_field(ln, 9, 3, "i")
+    gmi = N_blocks_x * N_grid_block_x + 1   # global_maximal_i/j (:913-914)
+    gmj = N_blocks_y * N_grid_block_y + 1
+    objs = []
+    for _n in range(n_bo):
+        cf.next()
+        ln = cf.next()
+        ty, ns = fortran_field(ln, 3, 2, "i"), fortran_field(ln, 8, 2, "i")
+        cf.next()
+        segs = []
+        for _m in range(ns):
+            ln = cf.next()
+            segs.append(tuple(fortran_field(ln, c, 6, "i") for c in (3, 12, 21, 30)))
+        objs.append((ty, segs))
+    inner = []
+    for _n in range(n_io):
+        cf.next()
+        ty = fortran_field(cf.next(), 3, 2, "i")
+        cf.next()
+        ln = cf.next()
+        inner.append((ty,) + tuple(fortran_field(ln, c, 6, "i") for c in (3, 12, 21, 30)))
+    periodic = any(abs(ty) == 2 for ty, _s in objs)   # PERIODIC_PIPELINE_X (:399-415)
+    side = {}   # 0 below, 1 above, 2 left, 3 right -> boundary object number (1-based)
+    for n, (ty, segs) in enumerate(objs):
+        for (i0, j0, i1, j1) in segs:
+            if j0 == j1 == 0:
+                s_ = 0
+            elif j0 == j1 == gmj:
+                s_ = 1
+            elif i0 == i1 == 0:
+                s_ = 2
+            elif i0 == i1 == gmi:
+                s_ = 3
+            else:
+                continue
+            if ty == 1:
+                side[s_] = n + 1
+    d.update(ncx=gmi - 1 if periodic else gmi, ncy=gmj, periodic=periodic, N_of_particles_cell=N_of_particles_cell,
+             N_max_vel=N_max_vel, T_e_eV=T_e_eV, N_plasma_m3=N_plasma_m3,
+             inner=[(il, jb, ir, jt) for (_t, il, jb, ir, jt) in inner], inner_type=[t for (t, *_r) in inner])
+    # scales (:719-723, :893-900)
+    v_Te_ms = math.sqrt(2.0 * T_e_eV * E_CL / M_E_KG)
+    W_plasma_s1 = math.sqrt(N_plasma_m3 * (E_CL * E_CL) / (eps0 * M_E_KG))
+    L_debye_m = v_Te_ms / W_plasma_s1
+    delta_x_m = L_debye_m / N_of_cells_debye
+    delta_t_s = delta_x_m / (N_max_vel * v_Te_ms)
+    V_scale_ms = N_max_vel * v_Te_ms
+    E_scale_Vm = M_E_KG * V_scale_ms / (E_CL * delta_t_s)
+    B_scale_T = M_E_KG / (E_CL * delta_t_s)
+    F_scale_V = E_CL * N_plasma_m3 * (delta_x_m * delta_x_m) / eps0
+    energy_factor_eV = 0.5 * M_E_KG * (V_scale_ms * V_scale_ms) / E_CL
+    d.update(delta_x_m=delta_x_m, delta_t_s=delta_t_s, V_scale_ms=V_scale_ms, E_scale_Vm=E_scale_Vm,
+             B_scale_T=B_scale_T, F_scale_V=F_scale_V, energy_factor_eV=energy_factor_eV,
+             factor_rho=1.0 / N_of_particles_cell,
+             factor2_E=F_scale_V / (E_scale_Vm * 2.0 * delta_x_m), factor1_E=F_scale_V / (E_scale_Vm * delta_x_m))
+    # init_simcontrol.dat (:830-845)
+    sc = _Lines(path("init_simcontrol.dat"))
+    t_sim_ns = sc.value(3, 11, "f", 3)
+    d["N_subcycles"] = sc.value(8, 2, "i")
+    d["Max_T_cntr"] = int(t_sim_ns / (1.0e9 * delta_t_s))
+    # init_particles.dat (:1005-1031); SET_ION_SPECIES (:1505-1507)
+    pf = _Lines(path("init_particles.dat"))
+    d["init_Te_eV"] = pf.value(3, 8, "f", 3)
+    d["init_Ne_m3"] = pf.value(3, 10, "e", 3)
+    n_spec = pf.value(6, 1, "i")
+    pf.next()
+    ions = []
+    for _s in range(n_spec):
+        ln = pf.next()
+        m_amu, q = fortran_field(ln, 3, 5, "f", 1), fortran_field(ln, 11, 2, "i")
+        ti = fortran_field(ln, 16, 8, "f", 3)
+        Ms = (AMU_KG * m_amu) / M_E_KG
+        ions.append(dict(M_i_amu=m_amu, Qs=q, init_Ti_eV=ti, Ms=Ms, QM2s=0.5 * q / Ms,
+                         QM2sNsub=d["N_subcycles"] * (0.5 * q / Ms)))
+    d["ions"] = ions
+    d["seed"] = pf.value(3, 9, "i")
+    # init_extfields.dat (pic2d_ExternalFields.f90:36-145)
+    bx = by = bz = ez = 0.0
+    sense_b = sense_ez = False
+    if os.path.exists(path("init_extfields.dat")):
+        ef = _Lines(path("init_extfields.dat"))
+        bx = ef.value(3, 9, "f", 3)
+        by = ef.value(3, 9, "f", 3)
+        ef.next()
+        ef.value(3, 9, "f", 3)          # y_Bmax
+        ef.value(3, 9, "f", 3)          # Bz_0
+        bz_max = ef.value(3, 9, "f", 3)
+        ef.value(3, 9, "f", 3)          # Bz_Lsys
+        ef.value(3, 9, "f", 3)
+        ef.value(3, 9, "f", 3)
+        ez = ef.value(3, 9, "f", 3)
+        sense_b = ef.value(7, 1, "i") == 1
+        sense_ez = ef.value(7, 1, "i") == 1
+        bx, by, bz = bx * 1.0e-4 / B_scale_T, by * 1.0e-4 / B_scale_T, bz_max * 1.0e-4 / B_scale_T   # Bz_ext = Bz_max
+        ez = ez * 100.0 / E_scale_Vm
+    d.update(Bx_ext=bx, By_ext=by, Bz_ext=bz, Ez_ext=ez, ions_sense_magnetic_field=sense_b, ions_sense_Ez=sense_ez)
+
+    # init_bo_NN.dat (pic2d_Setup.f90:60-100), normalised as pic2d_CurProblemValues.f90:1218-1221
+    def bo(n):
+        fn = path(f"init_bo_{n:02d}.dat")
+        if not os.path.exists(fn):
+            return dict(material="", phi_const=0.0, phi_var=0.0, omega=0.0, phase=0.0)
+        b = _Lines(fn)
+        b.next()
+        mat = b.next()[6:12]
+        c0, var, om, ph = (b.value(3, 9, "f", 3) for _ in range(4))
+        return dict(material=mat, phi_const=c0 / F_scale_V, phi_var=var / F_scale_V, omega=om * 2.0e6 * PI * delta_t_s,
+                    phase=ph * PI / 180.0)
+    d["walls"] = {s_: bo(n) for s_, n in side.items()}
+    d["inner_objects"] = [bo(n_bo + k + 1) for k in range(n_io)]
+    # neutrals and collisions
+    if os.path.exists(path("init_neutrals.dat")):
+        nl = open(path("init_neutrals.dat")).read().splitlines()
+        n_neutral = fortran_field(nl[1], 10, 2, "i")
+    else:
+        n_neutral = 0
+    d["neutral"] = None
+    d["rcx"] = None
+    if n_neutral >= 1:
+        neu = read_neutral_deck(directory)
+        d["neutral"] = neu
+        # ion_velocity_factor of the ions an ionisation produces (pic2d_enCollisionsGeneralProc.f90:224)
+        d["ion_velocity_factor"] = [
+            math.sqrt(neu["t_k"] * KB_JK / (T_e_eV * E_CL)) / (N_max_vel * math.sqrt(ions[c["isp"] - 1]["Ms"]))
+            if 1 <= c["isp"] <= n_spec else 0.0 for c in neu["cs"]]
+        rf = path(f"init_neutral_{neu['name']}_rcx_param.dat")
+        if os.path.exists(rf):
+            toks = open(rf).read().splitlines()[1].replace(",", " ").split()
+            s_, sig, alpha = int(toks[0]), float(toks[1].replace("d", "e")), float(toks[2].replace("d", "e"))
+            if 1 <= s_ <= n_spec:
+                Ms = ions[s_ - 1]["Ms"]
+                tg_ev = neu["t_k"] * KB_JK / E_CL
+                lf = 1.0 - alpha * math.log(max(1.5 * tg_ev, 0.001))
+                sig_th = sig * (lf * lf)                                                 # sigma_rcx_m2 (:35-44)
+                vmean = math.sqrt(2.54647908947033 * tg_ev * E_CL / (Ms * M_E_KG))
+                d["rcx"] = dict(
+                    species=s_, sigma_1eV=sig, alpha=alpha,
+                    vfactor=math.sqrt(neu["t_k"] * KB_JK / (T_e_eV * E_CL * Ms)) / N_max_vel,        # :83
+                    probab_thermal=neu["n_m3"] * sig_th * vmean * delta_t_s * d["N_subcycles"],     # :4-31
+                    prob_factor=neu["n_m3"] * delta_t_s * d["N_subcycles"],                         # :103
+                    factor_eV=Ms * energy_factor_eV)                                                # :102
+    return d
+
+
 # --------------------------------------------------------------------------------- whole cycle
 class OracleCycle:
-    """The oracle's cycle (oracle_cycle_step: MainProg order with N_subcycles = 1) set up from a deck and the
-    product-independent tables above. Particles are given as FP64 columns; capacity for appended particles."""
+    """The oracle's cycle (oracle_cycle_step: MainProg order, N_subcycles from the deck) set up from the deck by the
+    oracle's own reader (read_deck above) and its own tables. Particles are given as FP64 columns; capacity for
+    appended particles. Wall potentials follow UPDATE_WALL_POTENTIALS each step (wall_potential)."""
 
-    def __init__(self, deck_dir, params, tables, electrons, ions, seed, nthreads=1, cap_factor=1.3):
-        p, t = params, tables
+    def __init__(self, deck_dir, electrons, ions, seed, nthreads=1, cap_factor=1.3):
+        dk = self.deck = read_deck(deck_dir)
         n_e, n_i = len(electrons[0]), len(ions[0])
         self.pe = ParticleSet(*electrons[:5], ids=electrons[5] if len(electrons) > 5 else None,
                               cap=int(n_e * cap_factor) + 1024)
@@ -474,39 +692,57 @@ class OracleCycle:
         nb = max(n_e // 4, 4096)
         mk = lambda: ParticleSet(*(np.zeros(0),) * 5, cap=nb)
         self.be, self.bi = mk(), mk()
-        self.neu = read_neutral_deck(deck_dir)
-        self.mcc = MccTables(self.neu, p.n_subcycles, p.delta_t_s)
+        nsub = dk["N_subcycles"]
         self.mv, _ = maxwell_tables()
-        inner = [(p.inner_ileft[k], p.inner_jbottom[k], p.inner_iright[k], p.inner_jtop[k]) for k in range(p.n_inner)]
-        g = geom(p.ncx, p.ncy, p.periodic_x, inner)
+        g = geom(dk["ncx"], dk["ncy"], dk["periodic"], dk["inner"])
+        ion = dk["ions"][0]
         c = Cycle()
         c.geom = g
-        c.e_sp = Species(p.bx, p.by, p.bz, p.ez, 0, 0.0, p.n_subcycles, 0, 0)
-        c.i_sp = Species(p.bx, p.by, p.bz, p.ez, 1, 0.5 * p.ion_charge[0] / p.ion_mass_me[0], p.n_subcycles,
-                         p.ions_sense_b, p.ions_sense_ez)
-        c.factor_rho = 1.0 / p.n_of_particles_cell
-        c.ion_charge = float(p.ion_charge[0])
-        c.factor2_E = p.f_scale_v / (p.e_scale_vm * 2.0 * p.delta_x_m)
-        c.factor1_E = p.f_scale_v / (p.e_scale_vm * p.delta_x_m)
-        c.phi_bottom, c.phi_top = p.wall_phi_const[0], p.wall_phi_const[1]
-        c.mcc = C.pointer(self.mcc.t)
-        c.mcc_ctx = MccCtx(seed, 0, t.energy_factor_eV, self.neu["mass"], t.ion_velocity_factor[2], dp(self.mv))
-        c.rcx = Rcx(t.rcx_prob_factor, p.v_scale_ms, p.ion_mass_me[0] * t.energy_factor_eV, t.rcx_sigma_1eV,
-                    t.rcx_alpha, t.rcx_probab_thermal[0], t.rcx_vfactor[0])
-        c.rcx_on = int(t.rcx_on[0])
+        c.e_sp = Species(dk["Bx_ext"], dk["By_ext"], dk["Bz_ext"], dk["Ez_ext"], 0, 0.0, nsub, 0, 0)
+        c.i_sp = Species(dk["Bx_ext"], dk["By_ext"], dk["Bz_ext"], dk["Ez_ext"], 1, ion["QM2s"], nsub,
+                         int(dk["ions_sense_magnetic_field"]), int(dk["ions_sense_Ez"]))
+        c.factor_rho = dk["factor_rho"]
+        c.ion_charge = float(ion["Qs"])
+        c.factor2_E, c.factor1_E = dk["factor2_E"], dk["factor1_E"]
+        self.mcc = None
+        neu = dk["neutral"]
+        if neu is not None and neu["cs"]:
+            self.mcc = MccTables(neu, nsub, dk["delta_t_s"])
+            c.mcc = C.pointer(self.mcc.t)
+            ivf = max(dk["ion_velocity_factor"])
+            c.mcc_ctx = MccCtx(seed, 0, dk["energy_factor_eV"], neu["mass"], ivf, dp(self.mv))
+        else:
+            c.mcc_ctx = MccCtx(seed, 0, dk["energy_factor_eV"], 0.0, 0.0, dp(self.mv))
+        r = dk["rcx"]
+        if r is not None:
+            c.rcx = Rcx(r["prob_factor"], dk["V_scale_ms"], r["factor_eV"], r["sigma_1eV"], r["alpha"],
+                        r["probab_thermal"], r["vfactor"])
+            c.rcx_on = 1
         c.nthreads = nthreads
         c.born_e, c.born_i, c.cap_born = self.be.s, self.bi.s, nb
         c.next_id_e = int(self.pe.id[:n_e].max()) + 1 if n_e else 0
         c.next_id_i = int(self.pi.id[:n_i].max()) + 1 if n_i else 0
+        c.n_sub_phase = 0
         self.c = c
+        self.t_cntr = 0
         ny, nx = nodes_shape(g)
-        self.work = np.zeros(7 * nx * ny)
+        self.work = np.zeros(9 * nx * ny)
         self.counters = np.zeros(16, dtype=np.int64)
 
     def step(self, n=1):
         processed = 0
         for _ in range(n):
+            w = self.deck["walls"]
+            self.c.phi_bottom = wall_potential(w[0], self.t_cntr) if 0 in w else 0.0
+            self.c.phi_top = wall_potential(w[1], self.t_cntr) if 1 in w else 0.0
             processed += lib().oracle_cycle_step(C.byref(self.c), C.byref(self.pe.s), C.byref(self.pi.s),
                                                  len(self.pe.cols["x"]), len(self.pi.cols["x"]), dp(self.work),
                                                  self.counters.ctypes.data_as(_I64))
+            self.t_cntr += 1
         return processed
+
+
+def wall_potential(obj, t_cntr):
+    """UPDATE_WALL_POTENTIALS (pic2d_WallPotentials.f90:1-56) for a metal object without a waveform or amplitude
+    profile: phi_const + phi_var sin(omega T_cntr + phase) (Harmonic_Oscillation, :58-93)."""
+    return obj["phi_const"] + obj["phi_var"] * np.sin(obj["omega"] * t_cntr + obj["phase"])

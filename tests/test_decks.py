@@ -133,3 +133,40 @@ def test_wall_material_ion_reflection(tmp_path):
     assert d.ion_emission == {}
     d = read_deck(decks.write_deck(str(tmp_path / "e"), "cfg4", ncx=64, ncy=32, ppc=4))
     assert d.ion_wall_model == [2, 2, 0, 0]
+
+
+def test_oracle_reads_the_deck_independently(deck):
+    """The oracle's own reading of the decks (pyoracle.read_deck: the reference's READ edit descriptors and its
+    normalisation formulas, pic2d_CurProblemValues.f90:157-1255, pic2d_ExternalFields.f90:36-145,
+    pic2d_inCollisionsGeneralProc.f90:3-90) gives every constant the device cycle uses, bit for bit equal to the
+    product's edp_deck_read. The whole-cycle parity tests build the oracle's cycle from this reading only."""
+    _name, d, dk = deck
+    p, t = dk.params, dk.tables
+    o = pyoracle.read_deck(d)
+    assert (o["ncx"], o["ncy"], int(o["periodic"])) == (p.ncx, p.ncy, p.periodic_x)
+    assert o["N_of_particles_cell"] == p.n_of_particles_cell and o["N_subcycles"] == p.n_subcycles
+    assert o["seed"] == p.seed
+    for a, b in (("delta_t_s", "delta_t_s"), ("delta_x_m", "delta_x_m"), ("V_scale_ms", "v_scale_ms"),
+                 ("E_scale_Vm", "e_scale_vm"), ("B_scale_T", "b_scale_t"), ("F_scale_V", "f_scale_v"),
+                 ("Bx_ext", "bx"), ("By_ext", "by"), ("Bz_ext", "bz"), ("Ez_ext", "ez")):
+        assert o[a] == getattr(p, b), a
+    assert int(o["ions_sense_magnetic_field"]) == p.ions_sense_b and int(o["ions_sense_Ez"]) == p.ions_sense_ez
+    assert o["energy_factor_eV"] == t.energy_factor_eV
+    ion = o["ions"][0]
+    assert ion["Ms"] == p.ion_mass_me[0] and ion["Qs"] == p.ion_charge[0]
+    for side, w in o["walls"].items():
+        assert (w["phi_const"], w["phi_var"], w["omega"], w["phase"]) == (
+            p.wall_phi_const[side], p.wall_phi_var[side], p.wall_omega[side], p.wall_phase[side]), side
+    assert len(o["inner"]) == p.n_inner
+    for k, (il, jb, ir, jt) in enumerate(o["inner"]):
+        assert (il, jb, ir, jt) == (p.inner_ileft[k], p.inner_jbottom[k], p.inner_iright[k], p.inner_jtop[k])
+        b = o["inner_objects"][k]
+        assert b["phi_const"] + b["phi_var"] * math.sin(b["phase"]) == p.inner_phi[k]
+    assert o["ion_velocity_factor"] == [t.ion_velocity_factor[q] for q in range(t.n_act)]
+    r = o["rcx"]
+    assert t.rcx_on[0] == 1 and r["species"] == 1
+    assert (r["prob_factor"], r["sigma_1eV"], r["alpha"], r["probab_thermal"], r["vfactor"]) == (
+        t.rcx_prob_factor, t.rcx_sigma_1eV, t.rcx_alpha, t.rcx_probab_thermal[0], t.rcx_vfactor[0])
+    # E from phi (CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY, pic2d_ElectricFieldCalc_FFT_X.f90:1350-1351)
+    assert o["factor2_E"] == p.f_scale_v / (p.e_scale_vm * 2.0 * p.delta_x_m)
+    assert o["factor_rho"] == 1.0 / p.n_of_particles_cell

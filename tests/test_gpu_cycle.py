@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from edipic_b200 import ELECTRONS, IONS, PREC_FP64, PREC_MIXED, Simulation
+from edipic_b200 import ELECTRONS, FIELD_ACC_EX, FIELD_PHI, IONS, PREC_FP64, PREC_MIXED, Simulation
 from gpu_common import match_by_id, oracle_geom, periodic_dx, random_particles, small_deck
 
 
@@ -42,10 +42,10 @@ def test_fp64_cycle_matches_oracle_cycle(tmp_path):
     own ids."""
     d = small_deck(tmp_path, "periodic", ncx=32, ncy=32, n_gas=5.0e22)
     with Simulation(d, precision=PREC_FP64, seed=3) as sim:
-        p, t = sim.params, sim.deck.tables
+        p = sim.params
         e, ivs = _plasma(sim, PREC_FP64, n_per_cell=24)
         n = e[0].size
-        oc = pyoracle.OracleCycle(d, p, t, e, (e[0], e[1], ivs[0], ivs[1], ivs[2]), seed=3)
+        oc = pyoracle.OracleCycle(d, e, (e[0], e[1], ivs[0], ivs[1], ivs[2]), seed=3)
         for step in (1, 2):
             sim.step(1)
             oc.step(1)
@@ -122,3 +122,111 @@ def test_fused_collisions_equal_separate_passes(tmp_path, precision):
     ia, ib = match_by_id(a, b)
     for k in ("vx", "vy", "vz"):
         assert np.abs(a[k][ia] - b[k][ib]).max() < 1e-6
+
+
+def _oracle_phi(oc, sim):
+    """the oracle's potential of its last step on the product's reference node layout"""
+    ny, nx = pyoracle.nodes_shape(oc.c.geom)
+    nn = nx * ny
+    phi = oc.work[3 * nn:4 * nn].reshape(ny, nx)
+    out = np.zeros((sim.ny_ref, sim.nx_ref))
+    w = min(nx, sim.nx_ref)
+    out[:, :w] = phi[:, :w]
+    if sim.periodic:
+        p = sim.params
+        out[:, p.ncx] = out[:, 0]
+        out[:, p.ncx + 1] = out[:, 1]
+    return out
+
+
+def _oracle_acc(oc, sim):
+    ny, nx = pyoracle.nodes_shape(oc.c.geom)
+    nn = nx * ny
+    return oc.work[7 * nn:8 * nn].reshape(ny, nx)
+
+
+@pytest.mark.gpu
+def test_mixed_cycle_matches_oracle_cycle_over_12_steps(tmp_path):
+    """Twelve whole steps of the mixed-precision cycle (int32 cell + FP32 offsets and velocities, FP32 E, int64
+    fixed-point densities, FP64 FFT_X) in the magnetised cfg1 field against the FP64 oracle's cycle, both started
+    from the same FP32-snapped particles, collisions off, with a re-sort every 4 steps. The oracle reads the deck
+    itself (its constants are not the product's). Stated bounds after 12 steps: positions 2e-5 cell, velocities
+    2e-5 of max|v|, potential 1e-5 of max|phi|; identical particle counts and wall hits."""
+    d = small_deck(tmp_path, "periodic", ncx=48, ncy=40, collisions=False, rcx=False, bx=86.6, by=50.0,
+                   wall_potentials={2: 15.0, 4: -5.0})
+    with Simulation(d, precision=PREC_MIXED, sort_every=4, seed=5) as sim:
+        p = sim.params
+        e, ivs = _plasma(sim, PREC_MIXED, n_per_cell=16, seed=31)
+        oc = pyoracle.OracleCycle(d, e, (e[0], e[1], ivs[0], ivs[1], ivs[2]), seed=5)
+        sim.step(12)
+        oc.step(12)
+        c = sim.counters()
+        assert c.n_particles[0] == oc.pe.n and c.n_particles[1] == oc.pi.n
+        assert list(c.electron_hits[:4]) == list(oc.counters[8:12])
+        for got, ref in ((sim.download_particles(ELECTRONS), oc.pe.arrays()),
+                         (sim.download_particles(IONS), oc.pi.arrays())):
+            ia, ib = match_by_id(got, ref)
+            dx = np.abs(periodic_dx(got["x"][ia] - ref["x"][ib], p.ncx)).max()
+            dy = np.abs(got["y"][ia] - ref["y"][ib]).max()
+            assert dx < 2e-5 and dy < 2e-5, (dx, dy)
+            vmax = max(np.abs(ref[k]).max() for k in ("vx", "vy", "vz"))
+            dv = max(np.abs(got[k][ia] - ref[k][ib]).max() for k in ("vx", "vy", "vz"))
+            assert dv < 2e-5 * vmax, (dv, vmax)
+        phi = sim.field(FIELD_PHI)
+        ref_phi = _oracle_phi(oc, sim)
+        assert np.abs(phi - ref_phi).max() < 1e-5 * np.abs(ref_phi).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_subcycled_ions_match_oracle_cycle(tmp_path, precision):
+    """N_subcycles = 3 (ADVANCE_IONS on acc_E with QM2sNsub and X += V N_subcycles, pic2d_IonDynamics.f90:86-155;
+    MCC and RCX only on ion steps, pic2d_MainProgram.f90:196-303; CLEAR_ACCUMULATED_FIELDS after them), with the
+    ions feeling B and Ez. Against the oracle's subcycled cycle: acc_E after the first two electron steps, acc_E
+    cleared after the ion step, and every particle after 3 and 6 steps. FP64 to 1e-9; mixed (FP32 storage, no
+    collisions) to 2e-5."""
+    fp64 = precision == PREC_FP64
+    d = small_deck(tmp_path, "periodic", ncx=32, ncy=32, n_subcycles=3, collisions=fp64, rcx=fp64, n_gas=5.0e22,
+                   bx=86.6, by=50.0, ez=200.0, ions_sense_b=True, ions_sense_ez=True)
+    tol = 1e-9 if fp64 else 2e-5
+    with Simulation(d, precision=precision, sort_every=0, seed=9) as sim:
+        p = sim.params
+        assert p.n_subcycles == 3 and p.ions_sense_b == 1 and p.ions_sense_ez == 1
+        n = p.ncx * p.ncy * 20
+        e = random_particles(sim, n, seed=41, precision=precision, fast_fraction=0.01)
+        ivs = np.random.default_rng(42).normal(0, 0.01, (3, n))   # ions fast enough that 3 steps move them visibly
+        if not fp64:
+            ivs = ivs.astype(np.float32).astype(np.float64)
+        sim.upload_particles(ELECTRONS, *e, ids=np.arange(n, dtype=np.uint32))
+        sim.upload_particles(IONS, e[0], e[1], ivs[0], ivs[1], ivs[2], ids=np.arange(n, dtype=np.uint32))
+        oc = pyoracle.OracleCycle(d, e, (e[0], e[1], ivs[0], ivs[1], ivs[2]), seed=9)
+        ions0 = sim.download_particles(IONS)
+        sim.step(2)
+        oc.step(2)
+        # two electron steps: acc_E holds E of both, the ions have not moved
+        acc = sim.field(FIELD_ACC_EX)
+        ref_acc = _oracle_acc(oc, sim)
+        w = ref_acc.shape[1]
+        assert np.abs(acc[:, :w] - ref_acc).max() <= (1e-12 if fp64 else 1e-6) * np.abs(ref_acc).max()
+        ions2 = sim.download_particles(IONS)
+        ia, ib = match_by_id(ions2, ions0)
+        assert np.array_equal(ions2["x"][ia], ions0["x"][ib])
+        for step in (3, 6):
+            sim.step(1 if step == 3 else 3)
+            oc.step(1 if step == 3 else 3)
+            if step == 3:
+                assert np.abs(sim.field(FIELD_ACC_EX)).max() == 0.0   # CLEAR_ACCUMULATED_FIELDS
+                c = sim.counters()
+                if fp64:
+                    assert list(c.en_collisions[:3]) == list(oc.counters[:3]) and min(c.en_collisions[:3]) > 0
+                    assert c.rcx_collisions[0] == oc.counters[4] > 0
+            for got, ref in ((sim.download_particles(ELECTRONS), oc.pe.arrays()),
+                             (sim.download_particles(IONS), oc.pi.arrays())):
+                a, _ = _split(got, n)
+                b, _ = _split(ref, n)
+                ia, ib = match_by_id(a, b)
+                assert np.abs(periodic_dx(a["x"][ia] - b["x"][ib], p.ncx)).max() < tol, step
+                assert np.abs(a["y"][ia] - b["y"][ib]).max() < tol, step
+                vmax = max(np.abs(b[k]).max() for k in ("vx", "vy", "vz"))
+                for k in ("vx", "vy", "vz"):
+                    assert np.abs(a[k][ia] - b[k][ib]).max() < tol * max(1.0, vmax), (step, k)
