@@ -4,7 +4,9 @@
 Workload (default): the 1024x1024-cell periodic-x plasma with 200 electrons and 200 Ar+ per cell
 (419,430,400 particles), B = 10 mT at 30 degrees in plane, e-Ar (elastic, excitation, ionisation) and Ar+-Ar
 charge exchange, N_subcycles = 1, mixed precision (int32 cell + FP32 offsets/velocities, int64 fixed-point
-deposit), tile sort every 80 steps. Synthetic deck and initial plasma (no dataset is involved).
+deposit), tile sort every 20 steps (the configuration's period; the timed window holds whole sort periods, and a
+partial one is charged its share of a separately timed sort). Synthetic deck and initial plasma (no dataset is
+involved).
 
 One step = one pass of MainProg's cycle (pic2d_MainProgram.f90:151-309): density, FFT_X solve and E, electron
 push+deposit+MCC, ion push+deposit+RCX, appends. value = (electrons + ions) * steps / device time of the timed
@@ -12,7 +14,8 @@ steps (CUDA events on the library's stream). e2e = the same steps driven through
 a Fortran host uses, with the per-step host reads of the collision counters.
 
 --impl reference times the CPU restatement of the reference routines (the oracle: the reference's Fortran
-cannot be built in this image) on the host cores, on a bounded sample of the same workload.
+cannot be built in this image) on the host cores, on a bounded sample of the same workload (its physics and
+particles per cell on a 256 x 128-cell grid), without loading the device library.
 Multi-GPU (torchrun): the ranks share one cluster's particles (each GPU pushes args.ppc electrons and ions per cell
 over the whole grid, so the particles per cell grow with N: weak scaling); the int64 fixed-point densities are summed
 over the ranks with an NCCL all-reduce after every step and every rank solves the same field. Device time is the max
@@ -102,26 +105,39 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(args, deck_dir, seconds=15.0):
-    """The oracle's cycle (FP64, OpenMP on all host threads) on a bounded sample of the workload: the same
-    physics and particles per cell on a smaller periodic grid, stepped for about `seconds`."""
+def _decks_module():
+    """The synthetic-deck writer (edipic_b200/decks.py, which writes plain text files), loaded from its file so that
+    the CPU legs import nothing else of the device package and never load libedipic_b200.so."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "edipic_decks", os.path.join(ROOT, "edipic-2d_b200", "edipic_b200", "decks.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def _oracle_cycle_rate(config, ncx, ncy, ppc, threads, seconds, seed=1):
+    """particle-steps/s of the oracle's cycle (FP64; OpenMP on `threads` threads) on a deck of the given
+    configuration and grid, with the plasma of its init_particles.dat (uniform positions, Maxwellian electrons at
+    init_Te and ions at init_Ti, DISTRIBUTE_PARTICLES), stepped for about `seconds` after one untimed step. The deck
+    is read by the oracle's own reader."""
     import numpy as np
 
     import pyoracle
-    from edipic_b200 import decks, read_deck
-    ncx, ncy = 128, 64
+    decks = _decks_module()
     with tempfile.TemporaryDirectory() as tmp:
-        d = decks.write_deck(tmp, args.config, ncx=ncx, ncy=ncy, ppc=args.ppc)
-        dk = read_deck(d)
-        p, t = dk.params, dk.tables
-        rng = np.random.default_rng(0)
-        n = ncx * ncy * args.ppc
+        d = decks.write_deck(tmp, config, ncx=ncx, ncy=ncy, ppc=ppc)
+        dk = pyoracle.read_deck(d)
+        rng = np.random.default_rng(seed)
+        n = ncx * ncy * ppc
         x = rng.uniform(0, ncx, n)
         y = rng.uniform(0, ncy, n)
-        ve = rng.normal(0, np.sqrt(2.0 / dk.t_e_ev / 2.0) / dk.n_max_vel, (3, n))
-        vi = rng.normal(0, np.sqrt(0.03 / dk.t_e_ev / 2.0 / p.ion_mass_me[0]) / dk.n_max_vel, (3, n))
-        threads = os.cpu_count() or 1
-        oc = pyoracle.OracleCycle(d, p, t, (x, y, ve[0], ve[1], ve[2]), (x, y, vi[0], vi[1], vi[2]), seed=1,
+        # factor_convert = sqrt(T / T_scale) / N_max_vel per component of exp(-u^2) (pic2d_CurProblemValues.f90:3127)
+        fe = np.sqrt(dk["init_Te_eV"] / dk["T_e_eV"]) / dk["N_max_vel"]
+        fi = np.sqrt(dk["ions"][0]["init_Ti_eV"] / (dk["T_e_eV"] * dk["ions"][0]["Ms"])) / dk["N_max_vel"]
+        ve = rng.normal(0, fe / np.sqrt(2.0), (3, n))
+        vi = rng.normal(0, fi / np.sqrt(2.0), (3, n))
+        oc = pyoracle.OracleCycle(d, (x, y, ve[0], ve[1], ve[2]), (x, y, vi[0], vi[1], vi[2]), seed=seed,
                                   nthreads=threads)
         oc.step(1)
         done, steps, t0 = 0, 0, time.perf_counter()
@@ -131,9 +147,49 @@ def cpu_baseline(args, deck_dir, seconds=15.0):
             el = time.perf_counter() - t0
             if el > seconds or steps >= 5000:
                 break
-    return {"value": done / el, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{ncx}x{ncy} cells x {args.ppc}+{args.ppc} per cell ({2 * n} particles), {steps} steps, "
-                      f"{el:.1f} s, FP64 oracle cycle incl. FFT_X"}
+    return done / el, steps, el, 2 * n
+
+
+def host_cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(args, seconds=12.0):
+    """The oracle's cycle (the FP64 restatement of the reference routines) on the host cores: the line's
+    workload per particle (its configuration's physics and particles per cell, the grid sampled to 256 x 128 cells)
+    on all host threads and on one thread, plus the reference's own CPU-runnable case (cfg0: 128 x 128 cells,
+    64 + 64 per cell, FFT_X) on all threads. Each leg steps for about `seconds`."""
+    threads = os.cpu_count() or 1
+    sx, sy = min(args.cells_x, 256), min(args.cells_y, 128)
+    v_all, st_all, el_all, n_all = _oracle_cycle_rate(args.config, sx, sy, args.ppc, threads, seconds)
+    v_one, st_one, el_one, _ = _oracle_cycle_rate(args.config, sx, sy, args.ppc, 1, seconds)
+    v_c0, st_c0, el_c0, n_c0 = _oracle_cycle_rate("cfg0", 128, 128, 64, threads, seconds)
+    return {"value": v_all, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "cpu_model": host_cpu_model(),
+            "sample": f"{args.config} physics on {sx}x{sy} cells x {args.ppc}+{args.ppc} per cell ({n_all} "
+                      f"particles), {st_all} steps in {el_all:.1f} s on {threads} threads; FP64 oracle cycle incl. "
+                      f"FFT_X (the reference's Fortran/MPI/PETSc cannot be built in this image)",
+            "one_thread": {"value": v_one, "steps": st_one, "seconds": el_one},
+            "cfg0_all_threads": {"value": v_c0, "steps": st_c0, "seconds": el_c0,
+                                 "sample": f"cfg0: 128x128 cells x 64+64 per cell ({n_c0} particles), FFT_X"}}
+
+
+def line_config(args, world=1, per_gpu_particles=None):
+    """The `config` object of the JSON line, the same for both arms."""
+    c = {"workload": workload_desc(args), "cells": [args.cells_x, args.cells_y],
+         "particles_per_gpu": int(per_gpu_particles if per_gpu_particles is not None
+                                  else 2 * args.cells_x * args.cells_y * args.ppc),
+         "parallelism": (f"one cluster over {world} GPUs: particles split, densities summed by NCCL all-reduce, "
+                         "field replicated" if world > 1 else "1 GPU"),
+         "l2": "particle arrays (>10 GB) exceed L2 each step",
+         "sort": f"tile sort every {args.sort_every} steps, amortised in ms_per_step"}
+    return c
 
 
 def fp64_cycle_leg(args, stream_of):
@@ -289,18 +345,16 @@ def poisson_leg(args, stream_of, warmup=10, steps=30, only=None):
 
 
 def run_reference(args):
+    """The reference arm: the reference's routines for the path on the host CPU. The reference's Fortran cannot be
+    built in this image, so its CPU restatement (the oracle) runs, on all host threads, on the line's workload per
+    particle (the grid sampled: cpu_baseline). Only rank 0 works; nothing of the device library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from edipic_b200 import decks
-    with tempfile.TemporaryDirectory() as tmp:
-        d = decks.write_deck(tmp, args.config, ncx=args.cells_x, ncy=args.cells_y, ppc=args.ppc)
-        cb = cpu_baseline(args, d, seconds=30.0)
+    cb = cpu_baseline(args, seconds=20.0)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(args), "reference_arm": "CPU restatement of the reference routines "
-                       "(the reference's Fortran/MPI/PETSc cannot be built in this image)"},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": line_config(args),
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
                                          "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -356,6 +410,21 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         step_plain()
+    # the timed window starts right after a sort, so that it holds steps // sort_every sorts; a window that is not
+    # a whole number of sort periods is charged the rest of the period's sort by the separately timed sort below
+    sort_s = 0.0
+    if args.sort_every > 0 and prec == PREC_MIXED:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ts0 = time.perf_counter()
+        chk(lib.edp_sort_particles(ctx), "sort")
+        torch.cuda.synchronize()
+        sort_s = time.perf_counter() - ts0
+        if dist:
+            tt = torch.tensor([sort_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            sort_s = tt.item()
     c0 = sim.counters()
     n0 = c0.n_particles[0] + c0.n_particles[1]
     launches0 = c0.kernel_launches
@@ -389,6 +458,9 @@ def run_ours(args):
     else:
         nsum = float(n0 + n1)
     particle_steps = 0.5 * nsum * args.steps
+    sorts_in_window = args.steps // args.sort_every if (args.sort_every > 0 and prec == PREC_MIXED) else 0
+    sort_charge = (args.steps / args.sort_every - sorts_in_window) * sort_s if sorts_in_window or sort_s else 0.0
+    t_total += sort_charge
     value = particle_steps / t_total
 
     # end to end: the drop-in call order of a Fortran host (pic2d_MainProgram.f90:151-309) with its per-step reads
@@ -448,11 +520,11 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 particles / i64 fixed-point density / f64 field" if args.precision == "mixed" else "f64",
             "data": "synthetic",
-            "config": {"workload": workload_desc(args), "cells": [args.cells_x, args.cells_y],
-                       "particles_per_gpu": int(per_gpu_particles),
-                       "parallelism": (f"one cluster over {world} GPUs: particles split, densities summed by NCCL "
-                                       "all-reduce, field replicated" if world > 1 else "1 GPU"),
-                       "l2": "particle arrays (>10 GB) exceed L2 each step"},
+            "config": line_config(args, world, per_gpu_particles),
+            "sort": {"every": args.sort_every, "sorts_in_window": sorts_in_window, "sort_ms": 1e3 * sort_s,
+                     "charged_ms": 1e3 * sort_charge,
+                     "how": "window starts right after a sort and holds steps // every sorts; the rest of a partial "
+                            "period is charged from a separately timed sort"},
             "poisson_ms_per_step": 1e3 * t_field / args.steps,
             "push_ms_per_step": 1e3 * t_push / args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -482,7 +554,7 @@ def run_ours(args):
                                               "2 x pixels x 9 x c_in x c_out FLOPs, peak bf16 "
                                               + line["network"]["peak_kind"]}
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(args, d)
+            line["cpu_baseline"] = cpu_baseline(args)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -499,7 +571,8 @@ def main():
     ap.add_argument("--cells", type=int, nargs=2, default=None, metavar=("NX", "NY"))
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--sort-every", type=int, default=80)
+    ap.add_argument("--sort-every", type=int, default=None,
+                    help="tile sort period in steps (default: the configuration's, 20 for cfg1)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the FP64-cycle and Poisson legs")
     ap.add_argument("--poisson-only", nargs="*", default=None, metavar="RUN",
@@ -507,10 +580,11 @@ def main():
                          "(plain_mg, plain_nopc, learned_mg, learned_nopc)")
     ap.add_argument("--poisson-steps", type=int, default=30)
     args = ap.parse_args()
-    from edipic_b200 import decks
-    cfg = decks.CONFIGS[args.config]
+    cfg = _decks_module().CONFIGS[args.config]
     args.cells_x, args.cells_y = args.cells if args.cells else (cfg["ncx"], cfg["ncy"])
     args.ppc = args.ppc or cfg["ppc"]
+    if args.sort_every is None:
+        args.sort_every = cfg.get("sort_every", 20)
     if args.warmup < 3:
         args.warmup = 3
     if args.poisson_only is not None:

@@ -743,6 +743,15 @@ int edp_get_stream(edp_ctx* c, void** out)
     return EDP_OK;
 }
 
+int edp_sort_particles(edp_ctx* c)
+{
+    if (!c) return EDP_ERR_ARG;
+    for (int s = 0; s < c->nspec; ++s)
+        if (c->uploaded[s]) TRY(edp_launch_sort(c, s));
+    c->steps_since_sort = 0;
+    return finish_sync(c);
+}
+
 int edp_synchronize(edp_ctx* c)
 {
     if (!c) return EDP_ERR_ARG;

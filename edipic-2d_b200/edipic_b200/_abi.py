@@ -101,6 +101,7 @@ SIGNATURES = {
     "edp_set_sync": [_CTX, C.c_int],
     "edp_synchronize": [_CTX],
     "edp_get_stream": [_CTX, P(C.c_void_p)],
+    "edp_sort_particles": [_CTX],
     "edp_upload_particles": [_CTX, C.c_int, C.c_int64, _D, _D, _D, _D, _D, _I32, _U32],
     "edp_download_particles": [_CTX, C.c_int, C.c_int64, _I64, _D, _D, _D, _D, _D, _I32, _U32],
     "edp_distribute_particles": [_CTX, C.c_int, C.c_int32, C.c_double, C.c_int32, C.c_int32],

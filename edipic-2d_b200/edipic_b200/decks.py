@@ -24,7 +24,7 @@ E_ION_EV = 15.76
 CONFIGS = {
     # name: (ncx, ncy, periodic, ppc, n_init, dt_s, steps, B_gauss (Bx, By), inner object, top RF (V, MHz))
     "cfg0": dict(ncx=128, ncy=128, periodic=True, ppc=64, n_init=1.0e16, dt=5e-12, steps=1000, bx=0.0, by=0.0),
-    "cfg1": dict(ncx=1024, ncy=1024, periodic=True, ppc=200, n_init=1.0e16, dt=5e-12, steps=200,
+    "cfg1": dict(ncx=1024, ncy=1024, periodic=True, ppc=200, n_init=1.0e16, dt=5e-12, steps=200, sort_every=20,
                  bx=100.0 * math.cos(math.radians(30.0)), by=100.0 * math.sin(math.radians(30.0))),
     "cfg2": dict(ncx=512, ncy=512, periodic=False, ppc=100, n_init=1.0e16, dt=5e-12, steps=2000, bx=0.0, by=0.0,
                  inner=(224, 112, 288, 144, -100.0)),

@@ -206,6 +206,11 @@ module edipic_gpu
        integer(c_int), value :: species
        real(c_float), intent(out) :: out(*)
      end function edp_collect_moments
+     ! re-sort the particles by tile now (restarts the sort period); results do not depend on it
+     integer(c_int) function edp_sort_particles(ctx) bind(C, name="edp_sort_particles")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+     end function edp_sort_particles
      ! ids of the particles this context creates stay in [base, end): ranks of one cluster take disjoint ranges
      integer(c_int) function edp_set_id_range(ctx, base, end) bind(C, name="edp_set_id_range")
        import :: c_ptr, c_int, c_int64_t

@@ -178,6 +178,10 @@ int edp_set_sync(edp_ctx* ctx, int sync);
 int edp_synchronize(edp_ctx* ctx);
 /* the context's CUDA stream (a cudaStream_t), e.g. to record timing events on it */
 int edp_get_stream(edp_ctx* ctx, void** stream_out);
+/* No counterpart in the reference (it keeps particles in arrival order). Re-sorts every species' particles by tile
+ * now (mixed precision; a no-op for FP64) and restarts the sort period counted by the cycle (sort_every). Results
+ * do not depend on when sorts happen; this only moves the cost. Synchronises. */
+int edp_sort_particles(edp_ctx* ctx);
 
 /* ---- particles ----------------------------------------------------------------------------------- */
 /* after DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325) or a checkpoint read: the host's
