@@ -669,7 +669,18 @@ int edp_init(const edp_params* p, const edp_tables* t, edp_ctx** out)
         if ((r = edp_dielectrics_setup(c))) return fail(r);
         if ((r = alloc_hits(c, 65536))) return fail(r);   // grows with the electron add list
     }
-    for (int s = 0; s < 4; ++s) c->phi_wall[s] = p->wall_phi_const[s] + p->wall_phi_var[s] * std::sin(p->wall_phase[s]);
+    for (int s = 0; s < 4; ++s) {
+        EdpPotentialProfile& q = c->pot[s];
+        q.phi_const = p->wall_phi_const[s];
+        q.phi_var = p->wall_phi_var[s];
+        q.omega = p->wall_omega[s];
+        q.phase = q.phase_adjusted = p->wall_phase[s];
+        c->phi_wall[s] = q.value(0);
+    }
+    for (int n = 0; n < EDP_MAX_INNER; ++n) {   // constant until edp_set_potential_profile gives a time dependence
+        c->pot[4 + n].phi_const = p->inner_phi[n];
+        c->phi_inner[n] = p->inner_phi[n];
+    }
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(EDP_ERR_CUDA);
     *out = c;
     return EDP_OK;
@@ -946,9 +957,39 @@ int edp_gather_charge_density(edp_ctx* c, int sp, double* rho_out)
 
 int edp_update_wall_potentials(edp_ctx* c, int64_t t)
 {
-    if (!c) return EDP_ERR_ARG;
-    for (int s = 0; s < 4; ++s)
-        c->phi_wall[s] = c->p.wall_phi_const[s] + c->p.wall_phi_var[s] * std::sin(c->p.wall_omega[s] * (double)t + c->p.wall_phase[s]);
+    if (!c || t < 0 || t > INT32_MAX) return EDP_ERR_ARG;
+    for (int s = 0; s < 4; ++s) c->phi_wall[s] = c->pot[s].value((int32_t)t);
+    for (int n = 0; n < c->p.n_inner; ++n)
+        if (c->p.inner_eps[n] == 0.0) c->phi_inner[n] = c->pot[4 + n].value((int32_t)t);   // metal objects only
+    return EDP_OK;
+}
+
+int edp_set_potential_profile(edp_ctx* c, int32_t object, const double* harmonic, int32_t n_wf, const int32_t* wf_t,
+                              const float* wf_phi, int32_t n_ap, const int32_t* ap_t, const float* ap_factor)
+{
+    if (!c || object < 0 || object >= 4 + EDP_MAX_INNER || !harmonic || n_wf < 0 || n_ap < 0 || n_wf == 1 ||
+        n_ap == 1 || (n_wf && (!wf_t || !wf_phi)) || (n_ap && (!ap_t || !ap_factor)))
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_potential_profile");
+    for (int32_t k = 0; k + 1 < n_wf; ++k)
+        if (!(wf_t[k + 1] > wf_t[k]) || wf_t[0] != 0) return edp_fail(c, EDP_ERR_ARG, "waveform times must rise from 0");
+    for (int32_t k = 0; k + 1 < n_ap; ++k)
+        if (!(ap_t[k + 1] > ap_t[k]) || ap_t[0] != 0)
+            return edp_fail(c, EDP_ERR_ARG, "amplitude-profile times must rise from 0");
+    EdpPotentialProfile& q = c->pot[object];
+    q.phi_const = harmonic[0];
+    q.phi_var = harmonic[1];
+    q.omega = harmonic[2];
+    q.phase = harmonic[3];
+    q.wf_t.assign(wf_t, wf_t + n_wf);
+    q.wf_phi.assign(wf_phi, wf_phi + n_wf);
+    q.ap_t.assign(ap_t, ap_t + n_ap);
+    q.ap_factor.assign(ap_factor, ap_factor + n_ap);
+    q.adjust_phase((int32_t)c->t_cntr);
+    // the potential of the current step, as UPDATE_WALL_POTENTIALS at set-up
+    EdpPotentialProfile q0 = q;
+    const double v = q0.value((int32_t)c->t_cntr);
+    if (object < 4) c->phi_wall[object] = v;
+    else c->phi_inner[object - 4] = v;
     return EDP_OK;
 }
 
@@ -1302,6 +1343,7 @@ int edp_set_step(edp_ctx* c, int64_t t_cntr)
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
     c->t_cntr = t_cntr;
     c->n_sub_phase = 0;
+    for (auto& q : c->pot) q.adjust_phase((int32_t)t_cntr);   // ADJUST_HARMONIC_OSCILLATIONS_PHASE (MainProgram:94)
     return EDP_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/edipic_gpu.h"
+#include "../host/potentials.h"
 
 #define EDP_MAX_SPECIES (1 + EDP_MAX_ION_SPECIES)
 
@@ -237,6 +238,8 @@ struct edp_ctx {
     double K[EDP_MAX_SPECIES][9];
     void* dev_small = nullptr;        // 4 KB device block for kernel pointer tables
     double phi_wall[4];               // current wall potentials (normalised)
+    double phi_inner[EDP_MAX_INNER];  // current potentials of the metal inner objects (normalised)
+    EdpPotentialProfile pot[4 + EDP_MAX_INNER];   // their time dependence (walls by side, then inner objects)
     int64_t launches = 0;             // kernels launched (reported by edp_query_counters)
 };
 

@@ -612,7 +612,7 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     CgGeom g;
     g.kp = kp;
     for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
-    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->phi_inner[n];
     g.epsx = c->epsx;
     g.epsy = c->epsy;
     // scalars: [0] |b|^2, [1] r.r before iteration 0, then the two block areas (cg_block)
@@ -705,7 +705,7 @@ extern "C" int edp_warmstart_predict(edp_ctx* c, double* guess_out, double* res_
     CgGeom g;
     g.kp = kp;
     for (int s = 0; s < 4; ++s) g.wall[s] = c->phi_wall[s];
-    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->p.inner_phi[n];
+    for (int n = 0; n < EDP_MAX_INNER; ++n) g.inner[n] = c->phi_inner[n];
     g.epsx = c->epsx;
     g.epsy = c->epsy;
     double* scal = nullptr;

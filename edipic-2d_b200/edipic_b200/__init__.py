@@ -84,6 +84,36 @@ class Deck:
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(wall, s)] = tuple(buf)
+        # time dependence of the metal objects' potentials (walls 0..3, inner objects 4 + n): those with a waveform,
+        # an amplitude profile, or an oscillating inner object (walls' harmonic fields are in params already)
+        self.potential_profiles = {}
+        for obj in range(4 + _abi.MAX_INNER):
+            prof = self.potential_profile(obj)
+            if prof[1] is not None or prof[2] is not None or (obj >= 4 and prof[0][1] != 0.0):
+                self.potential_profiles[obj] = prof
+
+    def potential_profile(self, obj):
+        """(harmonic {phi_const, phi_var, omega, phase}, (wf_T_cntr, wf_phi) or None, (ap_T_cntr, ap_factor) or None)
+        of metal object obj as the deck sets it up (edp_deck_potential_profile)."""
+        harm = np.zeros(4)
+        nw, na = C.c_int32(), C.c_int32()
+        self.lib.edp_deck_potential_profile(self.handle, obj, _dp(harm), C.byref(nw), None, None, C.byref(na), None,
+                                            None)
+        wt, wv = np.zeros(nw.value, dtype=np.int32), np.zeros(nw.value, dtype=np.float32)
+        at, av = np.zeros(na.value, dtype=np.int32), np.zeros(na.value, dtype=np.float32)
+        i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        f32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self.lib.edp_deck_potential_profile(self.handle, obj, _dp(harm), C.byref(nw), i32(wt), f32(wv), C.byref(na),
+                                            i32(at), f32(av))
+        return harm, ((wt, wv) if nw.value else None), ((at, av) if na.value else None)
+
+    def potential_series(self, obj, t0, n):
+        """UPDATE_WALL_POTENTIALS of metal object obj for steps t0 .. t0 + n - 1 (no device needed)."""
+        out = np.zeros(int(n))
+        rc = self.lib.edp_deck_potential_series(self.handle, obj, int(t0), int(n), _dp(out))
+        if rc != 0:
+            raise EdpError(rc, "edp_deck_potential_series")
+        return out
 
     def close(self):
         if self.handle:
@@ -150,6 +180,9 @@ class Simulation:
             self.set_electron_emission(wall, see)
         for wall, (n, model, tn, tp, wb) in self.deck.wall_injection.items():
             self.set_wall_injection(wall, n, model, tn, tp, wb)
+        for obj, (harm, wf, ap) in self.deck.potential_profiles.items():
+            if obj < 4 or obj - 4 < p.n_inner:
+                self.set_potential_profile(obj, harm, wf, ap)
 
     # ------------------------------------------------------------------------------------ plumbing
     def _check(self, rc, where):
@@ -263,6 +296,19 @@ class Simulation:
 
     def update_wall_potentials(self, t_cntr):
         self._check(self.lib.edp_update_wall_potentials(self.ctx, int(t_cntr)), "edp_update_wall_potentials")
+
+    def set_potential_profile(self, obj, harmonic, waveform=None, amplitude=None):
+        """Time dependence of metal object obj's potential (edp_set_potential_profile): harmonic {phi_const, phi_var,
+        omega, phase}; waveform / amplitude: (T_cntr array, value array) or None."""
+        h = np.ascontiguousarray(harmonic, dtype=np.float64)
+        wt, wv = (np.ascontiguousarray(waveform[0], dtype=np.int32), np.ascontiguousarray(waveform[1], dtype=np.float32)) \
+            if waveform is not None else (np.zeros(0, np.int32), np.zeros(0, np.float32))
+        at, av = (np.ascontiguousarray(amplitude[0], dtype=np.int32), np.ascontiguousarray(amplitude[1], dtype=np.float32)) \
+            if amplitude is not None else (np.zeros(0, np.int32), np.zeros(0, np.float32))
+        i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        f32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(self.lib.edp_set_potential_profile(self.ctx, int(obj), _dp(h), wt.size, i32(wt), f32(wv), at.size,
+                                                       i32(at), f32(av)), "edp_set_potential_profile")
 
     def solve_poisson_fftx_linsysy(self, want_phi=False):
         """SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY."""

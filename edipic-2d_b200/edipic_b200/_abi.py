@@ -107,6 +107,8 @@ SIGNATURES = {
     "edp_distribute_particles": [_CTX, C.c_int, C.c_int32, C.c_double, C.c_int32, C.c_int32],
     "edp_gather_charge_density": [_CTX, C.c_int, _D],
     "edp_update_wall_potentials": [_CTX, C.c_int64],
+    "edp_set_potential_profile": [_CTX, C.c_int32, _D, C.c_int32, P(C.c_int32), P(C.c_float), C.c_int32,
+                                  P(C.c_int32), P(C.c_float)],
     "edp_field_fftx": [_CTX, _D],
     "edp_field_cg": [_CTX, C.c_double, C.c_int32, C.c_int32, _I32],
     "edp_set_cg_preconditioner": [_CTX, C.c_int32],
@@ -168,6 +170,9 @@ SIGNATURES = {
     "edp_deck_ion_wall_model": [C.c_void_p, C.c_int32, _I32],
     "edp_deck_electron_emission": [C.c_void_p, C.c_int32, P(SeeParams), _I32],
     "edp_deck_wall_injection": [C.c_void_p, C.c_int32, _D],
+    "edp_deck_potential_profile": [C.c_void_p, C.c_int32, _D, P(C.c_int32), P(C.c_int32), P(C.c_float),
+                                   P(C.c_int32), P(C.c_int32), P(C.c_float)],
+    "edp_deck_potential_series": [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, _D],
     "edp_deck_free": [C.c_void_p],
     "edp_write_snapshot_2d": [C.c_char_p, P(C.c_float), C.c_int32, C.c_int32, C.c_double],
     "edp_write_vdf1d": [C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32,

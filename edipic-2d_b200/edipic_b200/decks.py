@@ -66,14 +66,18 @@ def _segments():
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
                ion_emission=None, ion_reflection=False, electron_emission=None, wall_injection=None, ez=0.0,
-               ions_sense_b=False, ions_sense_ez=False):
+               ions_sense_b=False, ions_sense_ez=False, oscillations=None, waveforms=None, amplitude_profiles=None):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
     reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
     and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default.
     wall_injection: {wall (0 below, 1 above, 2 left, 3 right): (electrons per step, model, T_normal, T_parallel,
     beam energy [eV])}, the constant electron emission of init_bo_NN.dat. ez: uniform Z electric field [V/cm];
-    ions_sense_b / ions_sense_ez: the ions feel the magnetic / Z electric field (init_extfields.dat flags)."""
+    ions_sense_b / ions_sense_ez: the ions feel the magnetic / Z electric field (init_extfields.dat flags).
+    Time dependence of metal objects, keyed by the reference's object number (1-based: the four boundary objects,
+    then the inner objects): oscillations {n: (amplitude [V], frequency [MHz], phase [deg])} in init_bo_NN.dat;
+    waveforms {n: (amplitude [V], frequency [Hz], [(fraction of the period, value), ...])} written as
+    init_bo_NN_waveform.dat; amplitude_profiles {n: [(time [ns], factor), ...]} as init_bo_NN_amplitude_profile.dat."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -160,13 +164,18 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
         "-------d------- ions sense Z-electric field", f"       {int(bool(ions_sense_ez)):1d}",
     ])
 
+    osc = oscillations or {}
+
     def bo(n, phi, amp=0.0, mhz=0.0, inj=(0.0, 0, 0.0, 0.0, 0.0), material="METAL1"):
+        phase = 0.0
+        if n in osc:
+            amp, mhz, phase = osc[n]
         w(f"init_bo_{n:02d}.dat", [
             "------AAAAAA--- material", f"      {material}",
             "---ddddd.ddd--- constant potential [V]", f"   {phi:9.3f}",
             "---ddddd.ddd--- amplitude of oscillations [V]", f"   {amp:9.3f}",
             "---ddddd.ddd--- frequency [MHz]", f"   {mhz:9.3f}",
-            "---ddddd.ddd--- phase [deg]", f"   {0.0:9.3f}",
+            "---ddddd.ddd--- phase [deg]", f"   {phase:9.3f}",
             "---ddddd.ddd--- electrons injected per step", f"   {inj[0]:9.3f}",
             "-------d------- emission model", f"       {int(inj[1]):1d}",
             "----dddd.ddd--- emitted temperature normal [eV]", f"    {inj[2]:8.3f}",
@@ -245,6 +254,13 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
             bo(len(objs) + q + 1, obj[4], material=mname)
         else:
             bo(len(objs) + q + 1, obj[4])
+    for n, (amp_v, nu_hz, pts) in (waveforms or {}).items():
+        w(f"init_bo_{n:02d}_waveform.dat", [f"  {amp_v}  potential amplitude [V]", f"  {nu_hz:.6e}   frequency [Hz]",
+                                             "# time as a fraction of the period, value",
+                                             "# (values are multiplied by the amplitude)"]
+          + [f"  {a}   {b}" for a, b in pts])
+    for n, pts in (amplitude_profiles or {}).items():
+        w(f"init_bo_{n:02d}_amplitude_profile.dat", ["time [ns], amplitude factor"] + [f"  {a}   {b}" for a, b in pts])
 
     if not collisions:
         w("init_neutrals.dat", ["----------dd--- number of neutral species", f"          {0:2d}"])

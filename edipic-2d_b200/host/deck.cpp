@@ -6,6 +6,7 @@
 // walls (type 1) or periodic pipes (type 2) on the four sides, metal rectangular inner objects, uniform external
 // B and Ez, one neutral species with e-n processes of types 10/11/20/30 and resonant charge exchange.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -16,10 +17,11 @@
 #include <vector>
 
 #include "../../include/edipic_gpu.h"
+#include "potentials.h"
 
 namespace {
 
-const double E_CL = 1.602189e-19, M_E_KG = 9.109534e-31, EPS0 = 8.854188e-12, AMU_KG = 1.660565e-27,
+const double E_CL = 1.602189e-19, M_E_KG = 9.109534e-31, TRUE_EPS0 = 8.854188e-12, AMU_KG = 1.660565e-27,
              KB_JK = 1.38064852e-23, PI = 3.141592653589793;
 
 struct Lines {
@@ -119,6 +121,8 @@ struct edp_deck {
     int32_t ion_model[4] = {};   // ion-material interaction model of each wall's material
     edp_see_params see[4] = {};  // electron-induced emission of each wall's material
     double inject[4][5] = {};    // constant electron emission of each wall: N per step, model, T_n, T_p, W_beam [eV]
+    // potentials of the metal objects over time (walls 0 below, 1 above, 2 left, 3 right; inner objects 4 + n)
+    EdpPotentialProfile pot[4 + EDP_MAX_INNER];
 };
 
 namespace {
@@ -132,6 +136,18 @@ int read_deck(const std::string& dir, edp_deck* d)
     p.abi_version = EDP_ABI_VERSION;
     std::string L;
     // ---- init_configuration.dat (pic2d_CurProblemValues.f90:157-330)
+    // SET_PHYSICAL_CONSTANTS (pic2d_CurProblemValues.f90:3-55): eps_0 from init_physconstants.dat when it holds a
+    // positive value on its second line, else the true value
+    double EPS0 = TRUE_EPS0;
+    {
+        Lines pc(dir + "/init_physconstants.dat");
+        std::string l1, l2;
+        if (pc.ok && pc.next(l1) && pc.next(l2)) {
+            bool ok = false;
+            const double v = edp_potentials_detail::first_number(l2, &ok);   // READ (9, *) temp
+            if (ok && v > 0.0) EPS0 = v;
+        }
+    }
     Lines cf(dir + "/init_configuration.dat");
     if (!cf.ok) return EDP_ERR_IO;
     double Te, Np;
@@ -279,10 +295,26 @@ int read_deck(const std::string& dir, edp_deck* d)
         *ph = *ph * PI / 180.0;
         return g3;
     };
+    // the optional waveform and amplitude-profile files of a metal object (PREPARE_WAVEFORMS,
+    // PREPARE_OSCILLATIONS_AMPLITUDE_PROFILE, pic2d_Setup.f90:150-412), named by the object's number
+    auto read_profiles = [&](int n, EdpPotentialProfile* q) {
+        char name[64];
+        snprintf(name, sizeof(name), "/init_bo_%02d_waveform.dat", n + 1);
+        edp_read_waveform(dir + name, p.delta_t_s, p.f_scale_v, q);
+        snprintf(name, sizeof(name), "/init_bo_%02d_amplitude_profile.dat", n + 1);
+        edp_read_amplitude_profile(dir + name, p.delta_t_s, q);
+    };
     for (int s = 0; s < 4; ++s)
-        if (side_obj[s] >= 0 &&
-            !read_bo(side_obj[s], &p.wall_phi_const[s], &p.wall_phi_var[s], &p.wall_omega[s], &p.wall_phase[s]))
-            return EDP_ERR_IO;
+        if (side_obj[s] >= 0) {
+            if (!read_bo(side_obj[s], &p.wall_phi_const[s], &p.wall_phi_var[s], &p.wall_omega[s], &p.wall_phase[s]))
+                return EDP_ERR_IO;
+            EdpPotentialProfile& q = d->pot[s];
+            q.phi_const = p.wall_phi_const[s];
+            q.phi_var = p.wall_phi_var[s];
+            q.omega = p.wall_omega[s];
+            q.phase = q.phase_adjusted = p.wall_phase[s];
+            read_profiles(side_obj[s], &q);
+        }
     // ---- constant electron emission of the walls (init_bo_NN.dat lines 11-20, PREPARE_SETUP_VALUES
     // pic2d_Setup.f90:86-95): macroparticles per step (3x,f9.3), model (7x,i1), normal and parallel temperatures and
     // the beam energy in eV (4x,f8.3)
@@ -388,7 +420,14 @@ int read_deck(const std::string& dir, edp_deck* d)
         p.inner_jtop[n] = inner[n].je;
         double c0, var, om, ph;
         if (!read_bo(nbo + n, &c0, &var, &om, &ph)) return EDP_ERR_IO;
-        p.inner_phi[n] = c0 + var * std::sin(ph);
+        EdpPotentialProfile& q = d->pot[4 + n];
+        q.phi_const = c0;
+        q.phi_var = var;
+        q.omega = om;
+        q.phase = q.phase_adjusted = ph;
+        if (otype[nbo + n] == 1) read_profiles(nbo + n, &q);   // METAL_WALL only
+        EdpPotentialProfile q0 = q;
+        p.inner_phi[n] = q0.value(0);   // UPDATE_WALL_POTENTIALS(0) at set-up (pic2d_CurProblemValues.f90:1226)
     }
     p.precision = EDP_PREC_MIXED;
     p.solver = p.periodic_x ? EDP_SOLVER_FFTX : EDP_SOLVER_CG;
@@ -605,6 +644,40 @@ int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out)
 {
     if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
     for (int k = 0; k < 5; ++k) out[k] = d->inject[wall][k];
+    return EDP_OK;
+}
+
+int edp_deck_potential_profile(const edp_deck* d, int32_t object, double* harmonic, int32_t* n_wf, int32_t* wf_t,
+                               float* wf_phi, int32_t* n_ap, int32_t* ap_t, float* ap_factor)
+{
+    if (!d || object < 0 || object >= 4 + EDP_MAX_INNER || !n_wf || !n_ap) return EDP_ERR_ARG;
+    const EdpPotentialProfile& q = d->pot[object];
+    if (harmonic) {
+        harmonic[0] = q.phi_const;
+        harmonic[1] = q.phi_var;
+        harmonic[2] = q.omega;
+        harmonic[3] = q.phase;
+    }
+    *n_wf = (int32_t)q.wf_t.size();
+    *n_ap = (int32_t)q.ap_t.size();
+    for (size_t k = 0; k < q.wf_t.size(); ++k) {
+        if (wf_t) wf_t[k] = q.wf_t[k];
+        if (wf_phi) wf_phi[k] = q.wf_phi[k];
+    }
+    for (size_t k = 0; k < q.ap_t.size(); ++k) {
+        if (ap_t) ap_t[k] = q.ap_t[k];
+        if (ap_factor) ap_factor[k] = q.ap_factor[k];
+    }
+    return EDP_OK;
+}
+
+int edp_deck_potential_series(const edp_deck* d, int32_t object, int64_t t0, int64_t n, double* out)
+{
+    if (!d || object < 0 || object >= 4 + EDP_MAX_INNER || t0 < 0 || n < 0 || t0 + n > INT32_MAX || (n && !out))
+        return EDP_ERR_ARG;
+    EdpPotentialProfile q = d->pot[object];
+    q.adjust_phase((int32_t)t0);
+    for (int64_t k = 0; k < n; ++k) out[k] = q.value((int32_t)(t0 + k));
     return EDP_OK;
 }
 

@@ -204,8 +204,19 @@ int edp_distribute_particles(edp_ctx* ctx, int species, int32_t per_cell, double
  * converts the accumulated fixed-point density to FP64 with the periodic fold and wall factors and,
  * when rho_out != NULL, copies it to the host (species EDP_ELECTRONS: c_rho; EDP_IONS: c_rho_i, Qs-weighted). */
 int edp_gather_charge_density(edp_ctx* ctx, int species, double* rho_out);
-/* UPDATE_WALL_POTENTIALS (pic2d_WallPotentials.f90:1-56) for step T_cntr */
+/* UPDATE_WALL_POTENTIALS (pic2d_WallPotentials.f90:1-165) for step T_cntr: every metal wall and metal inner object
+ * takes phi_const + (Harmonic_Oscillation + Custom_Waveform) * Amplitude_Profile. Call it for consecutive steps:
+ * with an amplitude profile the oscillation's phase is re-anchored at each profile period start. */
 int edp_update_wall_potentials(edp_ctx* ctx, int64_t t_cntr);
+/* The time dependence of one metal object's potential, as PREPARE_WAVEFORMS and
+ * PREPARE_OSCILLATIONS_AMPLITUDE_PROFILE leave it in whole_object (pic2d_Setup.f90:150-412): object 0..3 are the
+ * walls (below, above, left, right), 4 + n inner object n. harmonic = {phi_const, phi_var, omega [rad/step],
+ * phase [rad]}, normalised; the waveform's n_wf points (wf_T_cntr, wf_phi normalised, REAL) and the amplitude
+ * profile's n_ap points (ap_T_cntr, ap_factor, REAL), each 0 for none, times rising from 0 (the last is the
+ * period). Without this call walls follow edp_params' harmonic fields and inner objects keep inner_phi. */
+int edp_set_potential_profile(edp_ctx* ctx, int32_t object, const double* harmonic, int32_t n_wf,
+                              const int32_t* wf_t_cntr, const float* wf_phi, int32_t n_ap, const int32_t* ap_t_cntr,
+                              const float* ap_factor);
 /* SOLVE_POISSON_FFTX_LINSYSY + CALCULATE_ELECTRIC_FIELD_FFTX_LINSYSY
  * (pic2d_ElectricFieldCalc_FFT_X.f90:3-1547): phi_out may be NULL */
 int edp_field_fftx(edp_ctx* ctx, double* phi_out);
@@ -438,6 +449,13 @@ int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
 int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out);
 /* electron-induced emission parameters of wall's material; *enabled = 1 when any of the three models is on */
 int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled);
+/* the time dependence of metal object `object` (0..3 walls, 4 + n inner objects) as the deck sets it up,
+ * in edp_set_potential_profile's layout: counts always, arrays when not NULL (call once for the counts) */
+int edp_deck_potential_profile(const edp_deck* d, int32_t object, double* harmonic, int32_t* n_wf, int32_t* wf_t_cntr,
+                               float* wf_phi, int32_t* n_ap, int32_t* ap_t_cntr, float* ap_factor);
+/* UPDATE_WALL_POTENTIALS of that object for steps t0 .. t0 + n - 1 of a run started (or continued, with
+ * ADJUST_HARMONIC_OSCILLATIONS_PHASE) at t0, without a device: out[n] */
+int edp_deck_potential_series(const edp_deck* d, int32_t object, int64_t t0, int64_t n, double* out);
 int edp_deck_free(edp_deck* d);
 
 /* ---- snapshot files (host side of CREATE_SNAPSHOT, pic2d_Snapshots.f90:303-1202), one cluster ---------------- */

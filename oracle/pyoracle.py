@@ -634,13 +634,13 @@ def read_deck(directory):
     def bo(n):
         fn = path(f"init_bo_{n:02d}.dat")
         if not os.path.exists(fn):
-            return dict(material="", phi_const=0.0, phi_var=0.0, omega=0.0, phase=0.0)
+            return dict(material="", phi_const=0.0, phi_var=0.0, omega=0.0, phase=0.0, number=n)
         b = _Lines(fn)
         b.next()
         mat = b.next()[6:12]
         c0, var, om, ph = (b.value(3, 9, "f", 3) for _ in range(4))
         return dict(material=mat, phi_const=c0 / F_scale_V, phi_var=var / F_scale_V, omega=om * 2.0e6 * PI * delta_t_s,
-                    phase=ph * PI / 180.0)
+                    phase=ph * PI / 180.0, number=n)
     d["walls"] = {s_: bo(n) for s_, n in side.items()}
     d["inner_objects"] = [bo(n_bo + k + 1) for k in range(n_io)]
     # neutrals and collisions
@@ -681,7 +681,7 @@ def read_deck(directory):
 class OracleCycle:
     """The oracle's cycle (oracle_cycle_step: MainProg order, N_subcycles from the deck) set up from the deck by the
     oracle's own reader (read_deck above) and its own tables. Particles are given as FP64 columns; capacity for
-    appended particles. Wall potentials follow UPDATE_WALL_POTENTIALS each step (wall_potential)."""
+    appended particles. Wall potentials follow UPDATE_WALL_POTENTIALS each step (WallProfile)."""
 
     def __init__(self, deck_dir, electrons, ions, seed, nthreads=1, cap_factor=1.3):
         dk = self.deck = read_deck(deck_dir)
@@ -725,6 +725,7 @@ class OracleCycle:
         c.n_sub_phase = 0
         self.c = c
         self.t_cntr = 0
+        self.walls = wall_profiles(deck_dir, dk)
         ny, nx = nodes_shape(g)
         self.work = np.zeros(9 * nx * ny)
         self.counters = np.zeros(16, dtype=np.int64)
@@ -732,9 +733,9 @@ class OracleCycle:
     def step(self, n=1):
         processed = 0
         for _ in range(n):
-            w = self.deck["walls"]
-            self.c.phi_bottom = wall_potential(w[0], self.t_cntr) if 0 in w else 0.0
-            self.c.phi_top = wall_potential(w[1], self.t_cntr) if 1 in w else 0.0
+            w = self.walls
+            self.c.phi_bottom = w[0].value(self.t_cntr) if 0 in w else 0.0
+            self.c.phi_top = w[1].value(self.t_cntr) if 1 in w else 0.0
             processed += lib().oracle_cycle_step(C.byref(self.c), C.byref(self.pe.s), C.byref(self.pi.s),
                                                  len(self.pe.cols["x"]), len(self.pi.cols["x"]), dp(self.work),
                                                  self.counters.ctypes.data_as(_I64))
@@ -742,7 +743,134 @@ class OracleCycle:
         return processed
 
 
-def wall_potential(obj, t_cntr):
-    """UPDATE_WALL_POTENTIALS (pic2d_WallPotentials.f90:1-56) for a metal object without a waveform or amplitude
-    profile: phi_const + phi_var sin(omega T_cntr + phase) (Harmonic_Oscillation, :58-93)."""
-    return obj["phi_const"] + obj["phi_var"] * np.sin(obj["omega"] * t_cntr + obj["phase"])
+class WallProfile:
+    """UPDATE_WALL_POTENTIALS for one metal object (pic2d_WallPotentials.f90:1-165): Harmonic_Oscillation (with the
+    phase re-anchored at each amplitude-profile period), Custom_Waveform and Amplitude_Profile, with the waveform
+    values, amplitude factors and interpolation weight in single precision as the reference's REAL variables; the two
+    optional files read as PREPARE_WAVEFORMS and PREPARE_OSCILLATIONS_AMPLITUDE_PROFILE read them
+    (pic2d_Setup.f90:150-412)."""
+
+    def __init__(self, obj, directory=None, number=None, delta_t_s=None, f_scale_v=None):
+        self.phi_const, self.phi_var = obj["phi_const"], obj["phi_var"]
+        self.omega, self.phase = obj["omega"], obj["phase"]
+        self.phase_adjusted = self.phase
+        self.wf_t, self.wf_phi, self.ap_t, self.ap_factor = [], [], [], []
+        if directory is not None:
+            self._read_waveform(os.path.join(directory, f"init_bo_{number:02d}_waveform.dat"), delta_t_s, f_scale_v)
+            self._read_amplitude(os.path.join(directory, f"init_bo_{number:02d}_amplitude_profile.dat"), delta_t_s)
+
+    @staticmethod
+    def _pairs(lines):
+        out = []
+        for ln in lines:
+            tok = ln.replace(",", " ").split()
+            if not tok:
+                continue
+            if len(tok) < 2:
+                break
+            try:
+                a, b = float(tok[0].replace("d", "e")), float(tok[1].replace("d", "e"))
+            except ValueError:
+                break
+            out.append((tok[0].replace("d", "e"), tok[1].replace("d", "e")))
+        return out
+
+    def _read_waveform(self, path, dt, fsc):
+        if not os.path.exists(path):
+            return
+        L = open(path).read().splitlines()
+        pts = self._pairs(L[4:])
+        n = len(pts)
+        if n <= 1:
+            return
+        phi_v, nu = float(L[0].split()[0].replace("d", "e")), float(L[1].split()[0].replace("d", "e"))
+        if phi_v == 0.0:
+            return
+        period = int(1.0 / (nu * dt))
+        if period < n - 1:
+            return
+        t = [int(np.float32(a) * np.float32(period)) for a, _b in pts]          # REAL * INTEGER
+        v = [np.float32((phi_v / fsc) * float(np.float32(b))) for _a, b in pts]
+        t[0], t[-1] = 0, period
+        for i in range(1, n - 1):
+            t[i] = max(t[i], t[i - 1] + 1)
+        if t[-1] > t[-2]:
+            self.wf_t, self.wf_phi = t, v
+
+    def _read_amplitude(self, path, dt):
+        if not os.path.exists(path):
+            return
+        pts = self._pairs(open(path).read().splitlines()[1:])
+        n = len(pts)
+        if n <= 1:
+            return
+        t = [int(float(np.float32(a)) * 1.0e-9 / dt) for a, _b in pts]
+        f = [np.float32(b) for _a, b in pts]
+        t[0] = 0
+        for i in range(1, n - 1):
+            t[i] = max(t[i], t[i - 1] + 1)
+        if self.wf_t:
+            wp = self.wf_t[-1]
+            for i in range(n - 1):
+                if f[i] == 0.0 and f[i + 1] != 0.0:
+                    d = t[i + 1] - t[i]
+                    t[i] = wp * (t[i] // wp)
+                    t[i + 1] = t[i] + d
+            for i in range(1, n):
+                if f[i - 1] != 0.0 and f[i] == 0.0:
+                    d = t[i] - t[i - 1]
+                    t[i] = wp * (t[i] // wp)
+                    t[i - 1] = t[i] - d
+            t[-1] = wp * (t[-1] // wp)
+        if all(t[i + 1] > t[i] for i in range(n - 1)):
+            self.ap_t, self.ap_factor = t, f
+
+    @staticmethod
+    def _interp(tt, vv, t):
+        per = tt[-1]
+        my = t - (t // per) * per
+        for i in range(len(tt) - 1):
+            if tt[i] <= my <= tt[i + 1]:
+                ai = np.float32((tt[i + 1] - my) / (tt[i + 1] - tt[i]))
+                return float(np.float32(vv[i] * ai)) + float(vv[i + 1]) * (1.0 - float(ai))
+        return None
+
+    def adjust_phase(self, start_t):
+        """ADJUST_HARMONIC_OSCILLATIONS_PHASE (pic2d_WallPotentials.f90:180-206) for a run continued at start_t"""
+        if start_t == 0 or not self.ap_t:
+            return
+        per = self.ap_t[-1]
+        my = (start_t // per) * per
+        n_periods = int((self.omega * my) / (2.0 * PI))
+        self.phase_adjusted = n_periods * 2.0 * PI + self.phase - self.omega * my
+
+    def value(self, t):
+        if self.ap_t:
+            per = self.ap_t[-1]
+            if t == (t // per) * per:
+                n_periods = int((self.omega * t) / (2.0 * PI))
+                self.phase_adjusted = n_periods * 2.0 * PI + self.phase - self.omega * t
+            harm = self.phi_var * math.sin(self.omega * t + self.phase_adjusted)
+        else:
+            harm = self.phi_var * math.sin(self.omega * t + self.phase)
+        wf = 0.0
+        if self.wf_t:
+            r = self._interp(self.wf_t, self.wf_phi, t)
+            wf = 0.0 if r is None else r
+        amp = 1.0
+        if self.ap_t:
+            r = self._interp(self.ap_t, self.ap_factor, t)
+            amp = 1.0 if r is None else r
+        return self.phi_const + (harm + wf) * amp
+
+
+def wall_profiles(deck_dir, dk=None):
+    """{object (0..3 walls by side, 4 + n inner objects): WallProfile} of the deck's metal objects."""
+    dk = dk or read_deck(deck_dir)
+    out = {}
+    for side, w in dk["walls"].items():
+        out[side] = WallProfile(w, deck_dir, w["number"], dk["delta_t_s"], dk["F_scale_V"])
+    for k, w in enumerate(dk["inner_objects"]):
+        if dk["inner_type"][k] == 1:
+            out[4 + k] = WallProfile(w, deck_dir, w["number"], dk["delta_t_s"], dk["F_scale_V"])
+    return out

@@ -95,3 +95,39 @@ def test_multigrid_pcg(tmp_path, ncx, ncy, inner):
     assert its[PRECOND_MG] * 4 < its[PRECOND_NONE]
     if ncx == 256:
         assert its[PRECOND_MG] <= 20
+
+
+@pytest.mark.gpu
+def test_time_dependent_potentials_reach_the_field_solve(tmp_path):
+    """UPDATE_WALL_POTENTIALS with a pulsed custom waveform on the top wall (FFT_X) and a harmonically oscillating
+    metal inner object (CG): after edp_update_wall_potentials(T) for consecutive T, the solved potential on the wall
+    row and on the object's nodes equals the oracle's restatement of the potential at T."""
+    d = small_deck(tmp_path / "p", "periodic", ncx=64, ncy=48, wall_potentials={2: 12.0},
+                   oscillations={2: (30.0, 731.0, 15.0)},
+                   waveforms={2: (50.0, 1.0e9, [(0.0, -1.0), (0.49, -0.5), (0.51, 1.0), (1.0, 0.5)])},
+                   amplitude_profiles={2: [(0.0, 1.0), (5.0, 1.0), (5.0, 0.0), (19.5, 0.0)]})
+    prof = pyoracle.wall_profiles(d)
+    with Simulation(d, sort_every=0) as sim:
+        _load_plasma(sim, PREC_MIXED)
+        checked = 0
+        for t in range(0, 4200):
+            sim.update_wall_potentials(t)
+            want = prof[1].value(t)
+            prof[0].value(t)
+            if t % 97 == 0 or t in (998, 999, 1000, 1001, 3799, 3800, 3801):
+                phi = sim.solve_poisson_fftx_linsysy(want_phi=True)
+                assert abs(phi[-1, 7] - want) <= 1e-12 * max(1.0, abs(want)), t
+                checked += 1
+        assert checked > 40
+    dw = small_deck(tmp_path / "w", "walled", ncx=64, ncy=64, inner=(20, 24, 36, 32, -40.0),
+                    oscillations={5: (25.0, 1000.0, 45.0)})
+    prof = pyoracle.wall_profiles(dw)
+    with Simulation(dw, sort_every=0) as sim:
+        _load_plasma(sim, PREC_MIXED)
+        for t in range(0, 60):
+            sim.update_wall_potentials(t)
+            want = prof[4].value(t)
+            if t % 7 == 0:
+                sim.solve_potential_with_cg(rtol=1e-10, max_it=5000)
+                phi = sim.field(FIELD_PHI)
+                assert np.abs(phi[24:33, 20:37] - want).max() <= 1e-12 * max(1.0, abs(want)), t
