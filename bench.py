@@ -382,6 +382,8 @@ def run_ours(args):
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
     sim = Simulation(d, precision=prec, sort_every=args.sort_every, fuse_collisions=True, seed=1000)
     lib, ctx = sim.lib, sim.ctx
+    if args.push_kernel is not None:
+        sim._check(lib.edp_set_push_kernel(ctx, args.push_kernel), "edp_set_push_kernel")
     share = cluster.ClusterShare(sim, rank, world)   # disjoint ids; density sums over the ranks
     sim.distribute_particles(args.ppc)
     share.reduce()
@@ -579,6 +581,9 @@ def main():
                     help="only the Poisson leg (cfg2 geometry), optionally only the named runs "
                          "(plain_mg, plain_nopc, learned_mg, learned_nopc)")
     ap.add_argument("--poisson-steps", type=int, default=30)
+    ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2],
+                    help="mixed push over the sorted chunks (edp_set_push_kernel): 0 per-chunk CTAs, 1 streaming "
+                         "(bulk copies, 4 particles per thread), 2 streaming (2 per thread, 3 stages)")
     args = ap.parse_args()
     cfg = _decks_module().CONFIGS[args.config]
     args.cells_x, args.cells_y = args.cells if args.cells else (cfg["ncx"], cfg["ncy"])

@@ -241,6 +241,9 @@ struct edp_ctx {
     double phi_inner[EDP_MAX_INNER];  // current potentials of the metal inner objects (normalised)
     EdpPotentialProfile pot[4 + EDP_MAX_INNER];   // their time dependence (walls by side, then inner objects)
     int64_t launches = 0;             // kernels launched (reported by edp_query_counters)
+    // mixed push over the sorted chunks: 0 one CTA per chunk with the threads' own loads; 1 persistent CTAs with
+    // bulk-copy staging, 4 particles per thread, 2 stages; 2 the same with 2 particles per thread, 3 stages
+    int32_t push_kernel = 1;
 };
 
 // ------------------------------------------------------------------------------------------ Philox

@@ -477,6 +477,283 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArg
     }
 }
 
+// ------------------------------------------------------------------------ streaming push (bulk-copy staging)
+// The same push over the sorted chunks, with the particle columns brought into shared memory by the bulk-copy
+// engine instead of by the threads' own loads. A persistent CTA walks its chunks (blockIdx.x, + gridDim.x, ...) in
+// sub-chunks of SUB particles; thread 0 keeps NST sub-chunks in flight (one cp.async.bulk per column, completion
+// counted on the stage's mbarrier), so HBM streams the next sub-chunks, across chunk boundaries and through the
+// window flushes, while the warps compute. The threads read their IPT particles from shared memory and write the
+// results straight to global memory. Every wait is bounded: a wait that gives up raises EDP_EFLAG_TIMEOUT, and the
+// CTA waits (bounded) for its copies in flight before it returns.
+__device__ __forceinline__ uint32_t push_smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool push_mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long it = 0; it < (1LL << 22); ++it) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P;\n\t}\n"
+                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+struct StreamCursor {
+    int64_t chunk, off, end;   // chunk index; first slot of the sub-chunk; end of the chunk
+};
+
+template <int SUB>
+__device__ __forceinline__ void cursor_first(const PushArgs& a, StreamCursor& c)
+{
+    c.chunk = blockIdx.x;
+    if (c.chunk < a.n_chunks) {
+        const edp_chunk ch = a.chunks[c.chunk];
+        c.off = ch.start;
+        c.end = ch.end;
+    }
+}
+
+template <int SUB>
+__device__ __forceinline__ void cursor_next(const PushArgs& a, StreamCursor& c)
+{
+    c.off += SUB;
+    if (c.off < c.end) return;
+    c.chunk += gridDim.x;
+    if (c.chunk < a.n_chunks) {
+        const edp_chunk ch = a.chunks[c.chunk];
+        c.off = ch.start;
+        c.end = ch.end;
+    }
+}
+
+// columns of a stage: cell, ox, oy, vx, vy, vz, id
+#define EDP_STREAM_COLS 7
+
+template <int SUB>
+__device__ __forceinline__ void stream_issue(const PushArgs& a, const StreamCursor& c, uint32_t stage_base,
+                                             uint32_t bar, int ncols)
+{
+    const int64_t n = min((int64_t)SUB, c.end - c.off);   // a multiple of EDP_ITEMS: 16-byte sizes and addresses
+    const uint32_t bytes = (uint32_t)(n * 4);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes * ncols)
+                 : "memory");
+    const void* src[EDP_STREAM_COLS] = {a.P.cell + c.off, a.P.ox + c.off, a.P.oy + c.off, a.P.vx + c.off,
+                                        a.P.vy + c.off, a.P.vz + c.off, a.P.id + c.off};
+    for (int k = 0; k < ncols; ++k)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                     ::"r"(stage_base + (uint32_t)(k * SUB * 4)), "l"(src[k]), "r"(bytes), "r"(bar)
+                     : "memory");
+}
+
+template <bool PER>
+__device__ __forceinline__ void window_load(const PushArgs& a, Smem& s, int wx0, int wy0)
+{
+    const edp_kparams& kp = a.kp;
+    for (int t = threadIdx.x; t < EDP_WIN_NODES * EDP_WIN_NODES; t += blockDim.x) {
+        int lx = t % EDP_WIN_NODES, ly = t / EDP_WIN_NODES;
+        int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
+        bool ok = gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg;
+        s.E[t] = ok ? __ldg(&a.E[(int64_t)gy * kp.nxg + gx]) : make_float2(0.f, 0.f);
+        s.hi[t] = 0;
+        s.lo[t] = 0u;
+    }
+}
+
+__device__ __forceinline__ void window_flush(const PushArgs& a, Smem& s, int wx0, int wy0)
+{
+    const edp_kparams& kp = a.kp;
+    for (int t = threadIdx.x; t < EDP_WIN_NODES * EDP_WIN_NODES; t += blockDim.x) {
+        long long v = (long long)s.hi[t] * 65536LL + (long long)s.lo[t];
+        if (v == 0) continue;
+        int lx = t % EDP_WIN_NODES, ly = t / EDP_WIN_NODES;
+        int gx = wrapx(wx0 + lx, kp), gy = wy0 + ly;
+        if (gx >= 0 && gx < kp.nxg && gy >= 0 && gy < kp.nyg)
+            atomicAdd(&a.rho[(int64_t)gy * kp.nxg + gx], (unsigned long long)v);
+        else atomicOr(&a.dc->error_flags, EDP_EFLAG_BOUNDS);
+    }
+}
+
+template <bool ION, bool PER, bool ROT, int IPT, int NST>
+__global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 3 : 4) push_stream_kernel(PushArgs a)
+{
+    constexpr int SUB = EDP_PUSH_THREADS * IPT;
+    constexpr int STAGE_BYTES = EDP_STREAM_COLS * SUB * 4;
+    extern __shared__ __align__(128) unsigned char stage_mem[];
+    __shared__ Smem s;
+    __shared__ __align__(8) uint64_t full[NST];
+    int fail = 0;
+    const int tid = threadIdx.x;
+    const int ncols = (a.do_coll || a.emit_on) ? EDP_STREAM_COLS : EDP_STREAM_COLS - 1;
+    const uint32_t stage0 = push_smem_u32(stage_mem);
+    if (tid < 32) s.cnt[tid] = 0ull;
+    if (tid == 0) {
+        s.nsel = 0u;
+        for (int k = 0; k < NST; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(push_smem_u32(&full[k])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    // producer: thread 0 fills every stage first
+    StreamCursor prod;
+    int64_t issued = 0;
+    if (tid == 0) {
+        cursor_first<SUB>(a, prod);
+        for (int k = 0; k < NST && prod.chunk < a.n_chunks; ++k) {
+            stream_issue<SUB>(a, prod, stage0 + (uint32_t)(k * STAGE_BYTES), push_smem_u32(&full[k]), ncols);
+            ++issued;
+            cursor_next<SUB>(a, prod);
+        }
+    }
+    StreamCursor cur;
+    cursor_first<SUB>(a, cur);
+    int64_t win = -1, consumed = 0;
+    int wx0 = 0, wy0 = 0;
+    int st = 0;
+    uint32_t ph = 0;
+    for (; cur.chunk < a.n_chunks; cursor_next<SUB>(a, cur)) {
+        if (cur.chunk != win) {   // a new chunk: flush the previous window, stage the new field window
+            if (win >= 0) {
+                __syncthreads();
+                window_flush(a, s, wx0, wy0);
+                __syncthreads();
+            }
+            const edp_chunk ch = a.chunks[cur.chunk];
+            wx0 = ch.wx0;
+            wy0 = ch.wy0;
+            window_load<PER>(a, s, wx0, wy0);
+            win = cur.chunk;
+        }
+        const bool landed = push_mbar_wait(push_smem_u32(&full[st]), ph);
+        // the stage has landed; every thread is done with the previous stage and the window; the same verdict
+        // reaches every thread
+        if (__syncthreads_or(landed ? 0 : 1)) {
+            fail = 1;
+            break;
+        }
+        // refill the stage the previous sub-chunk used
+        if (tid == 0 && consumed > 0 && prod.chunk < a.n_chunks) {
+            const int ps = (st + NST - 1) % NST;
+            stream_issue<SUB>(a, prod, stage0 + (uint32_t)(ps * STAGE_BYTES), push_smem_u32(&full[ps]), ncols);
+            ++issued;
+            cursor_next<SUB>(a, prod);
+        }
+        const int64_t base = cur.off + (int64_t)tid * IPT;
+        if (base < cur.end) {
+            const unsigned char* sb = stage_mem + st * STAGE_BYTES;
+            int c[IPT];
+            float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
+            uint32_t id[IPT];
+            const bool with_id = ncols == EDP_STREAM_COLS;
+            if constexpr (IPT == 4) {
+                const int4 c4 = reinterpret_cast<const int4*>(sb)[tid];
+                const float4 ox4 = reinterpret_cast<const float4*>(sb + 1 * SUB * 4)[tid];
+                const float4 oy4 = reinterpret_cast<const float4*>(sb + 2 * SUB * 4)[tid];
+                const float4 vx4 = reinterpret_cast<const float4*>(sb + 3 * SUB * 4)[tid];
+                const float4 vy4 = reinterpret_cast<const float4*>(sb + 4 * SUB * 4)[tid];
+                const float4 vz4 = reinterpret_cast<const float4*>(sb + 5 * SUB * 4)[tid];
+                const uint4 id4 = with_id ? reinterpret_cast<const uint4*>(sb + 6 * SUB * 4)[tid] : make_uint4(0, 0, 0, 0);
+                c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
+                ox[0] = ox4.x; ox[1] = ox4.y; ox[2] = ox4.z; ox[3] = ox4.w;
+                oy[0] = oy4.x; oy[1] = oy4.y; oy[2] = oy4.z; oy[3] = oy4.w;
+                vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
+                vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
+                vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
+                id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
+            } else {
+                const int2 c2 = reinterpret_cast<const int2*>(sb)[tid];
+                const float2 ox2 = reinterpret_cast<const float2*>(sb + 1 * SUB * 4)[tid];
+                const float2 oy2 = reinterpret_cast<const float2*>(sb + 2 * SUB * 4)[tid];
+                const float2 vx2 = reinterpret_cast<const float2*>(sb + 3 * SUB * 4)[tid];
+                const float2 vy2 = reinterpret_cast<const float2*>(sb + 4 * SUB * 4)[tid];
+                const float2 vz2 = reinterpret_cast<const float2*>(sb + 5 * SUB * 4)[tid];
+                const uint2 id2 = with_id ? reinterpret_cast<const uint2*>(sb + 6 * SUB * 4)[tid] : make_uint2(0, 0);
+                c[0] = c2.x; c[1] = c2.y;
+                ox[0] = ox2.x; ox[1] = ox2.y;
+                oy[0] = oy2.x; oy[1] = oy2.y;
+                vx[0] = vx2.x; vx[1] = vx2.y;
+                vy[0] = vy2.x; vy[1] = vy2.y;
+                vz[0] = vz2.x; vz[1] = vz2.y;
+                id[0] = id2.x; id[1] = id2.y;
+            }
+            DepAcc acc;
+            acc.b = -1;
+#pragma unroll
+            for (int e = 0; e < IPT; ++e) {
+                if (c[e] < 0) continue;
+                if (!push_one<ION, PER, ROT>(a, s, true, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                                             (uint32_t)(base + e))) {
+                    c[e] = -1;
+                    atomicAdd(&s.cnt[17], 1ull);
+                }
+            }
+            dep_flush(s, acc);
+            if constexpr (IPT == 4) {
+                const int64_t g = base / 4;
+                __stcs(reinterpret_cast<int4*>(a.P.cell) + g, make_int4(c[0], c[1], c[2], c[3]));
+                __stcs(reinterpret_cast<float4*>(a.P.ox) + g, make_float4(ox[0], ox[1], ox[2], ox[3]));
+                __stcs(reinterpret_cast<float4*>(a.P.oy) + g, make_float4(oy[0], oy[1], oy[2], oy[3]));
+                __stcs(reinterpret_cast<float4*>(a.P.vx) + g, make_float4(vx[0], vx[1], vx[2], vx[3]));
+                __stcs(reinterpret_cast<float4*>(a.P.vy) + g, make_float4(vy[0], vy[1], vy[2], vy[3]));
+                __stcs(reinterpret_cast<float4*>(a.P.vz) + g, make_float4(vz[0], vz[1], vz[2], vz[3]));
+            } else {
+                const int64_t g = base / 2;
+                __stcs(reinterpret_cast<int2*>(a.P.cell) + g, make_int2(c[0], c[1]));
+                __stcs(reinterpret_cast<float2*>(a.P.ox) + g, make_float2(ox[0], ox[1]));
+                __stcs(reinterpret_cast<float2*>(a.P.oy) + g, make_float2(oy[0], oy[1]));
+                __stcs(reinterpret_cast<float2*>(a.P.vx) + g, make_float2(vx[0], vx[1]));
+                __stcs(reinterpret_cast<float2*>(a.P.vy) + g, make_float2(vy[0], vy[1]));
+                __stcs(reinterpret_cast<float2*>(a.P.vz) + g, make_float2(vz[0], vz[1]));
+            }
+        }
+        ++consumed;
+        if (++st == NST) {
+            st = 0;
+            ph ^= 1u;
+        }
+    }
+    __syncthreads();
+    if (fail) {
+        // a wait gave up: wait (bounded) for the copies still in flight into this CTA's stages, then leave
+        if (tid == 0) {
+            atomicOr(&a.dc->error_flags, EDP_EFLAG_TIMEOUT);
+            for (int64_t k = consumed; k < issued; ++k)
+                push_mbar_wait(push_smem_u32(&full[k % NST]), (uint32_t)((k / NST) & 1));
+        }
+        return;
+    }
+    if (win >= 0) window_flush(a, s, wx0, wy0);
+    if (!ION) {
+        __shared__ unsigned long long sel_base;
+        const unsigned nsel = min(s.nsel, (unsigned)EDP_SEL_SMEM);
+        if (tid == 0 && nsel) sel_base = atomicAdd(a.sel_count, (unsigned long long)nsel);
+        __syncthreads();
+        for (unsigned q = tid; q < nsel; q += blockDim.x) {
+            unsigned long long g = sel_base + q;
+            if ((int64_t)g < a.sel_cap) a.sel_list[g] = s.sel[q];
+            else atomicOr(&a.dc->error_flags, EDP_EFLAG_PENDING);
+        }
+    }
+    if (tid < 32) {
+        unsigned long long v = s.cnt[tid];
+        if (v) {
+            int k = tid;
+            if (k < 8) atomicAdd(ION ? &a.dc->i_hits[k] : &a.dc->e_hits[k], v);
+            else if (k < 16) {
+                atomicAdd(&a.dc->en_coll[k - 8], v);
+                atomicAdd(&a.dc->en_coll_step[k - 8], v);
+            } else if (k == 16) {
+                atomicAdd(&a.dc->rcx[a.species - 1], v);
+                atomicAdd(&a.dc->rcx_step[a.species - 1], v);
+            } else if (k == 17) {
+                atomicAdd(&a.dc->n_live[a.species], (unsigned long long)(-(long long)v));
+            }
+        }
+    }
+}
+
 struct SelArgs {
     edp_kparams kp;
     edp_species_mixed P;
@@ -879,6 +1156,53 @@ void fill_rot(const edp_ctx* c, int species, float* Kf, double* Kd)
 }  // namespace
 
 // ------------------------------------------------------------------------------------------- launch
+template <bool ION, bool PER, bool ROT, int IPT, int NST>
+static int launch_stream_variant(edp_ctx* c, const PushArgs& a)
+{
+    auto k = push_stream_kernel<ION, PER, ROT, IPT, NST>;
+    const size_t smem = (size_t)NST * EDP_STREAM_COLS * EDP_PUSH_THREADS * IPT * 4;
+    TRY(edp_raise_smem_limit(c, (const void*)k, smem));
+    static int per_sm[2][2][2] = {};   // resident CTAs per SM of this instantiation, found once per process
+    static int n_sm = 0;
+    int& r = per_sm[ION][PER][ROT];
+    if (!r) {
+        EDP_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k, EDP_PUSH_THREADS, smem));
+        if (r < 1) r = 1;
+    }
+    if (!n_sm) EDP_CUDA(c, cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, c->device));
+    const int64_t grid = std::min<int64_t>(a.n_chunks, (int64_t)n_sm * r);
+    k<<<(unsigned)grid, EDP_PUSH_THREADS, smem, c->stream>>>(a);
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
+template <int IPT, int NST>
+static int launch_stream_kind(edp_ctx* c, int variant, const PushArgs& a)
+{
+    switch (variant) {
+    case 0: return launch_stream_variant<false, false, false, IPT, NST>(c, a);
+    case 1: return launch_stream_variant<false, false, true, IPT, NST>(c, a);
+    case 2: return launch_stream_variant<false, true, false, IPT, NST>(c, a);
+    case 3: return launch_stream_variant<false, true, true, IPT, NST>(c, a);
+    case 4: return launch_stream_variant<true, false, false, IPT, NST>(c, a);
+    case 5: return launch_stream_variant<true, false, true, IPT, NST>(c, a);
+    case 6: return launch_stream_variant<true, true, false, IPT, NST>(c, a);
+    default: return launch_stream_variant<true, true, true, IPT, NST>(c, a);
+    }
+}
+
+static int launch_stream_push(edp_ctx* c, int variant, int kind, const PushArgs& a)
+{
+    return kind == 2 ? launch_stream_kind<2, 3>(c, variant, a) : launch_stream_kind<4, 2>(c, variant, a);
+}
+
+int edp_set_push_kernel(edp_ctx* c, int32_t kind)
+{
+    if (!c || kind < 0 || kind > 2) return edp_fail(c, EDP_ERR_ARG, "edp_set_push_kernel");
+    c->push_kernel = kind;
+    return EDP_OK;
+}
+
 int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
 {
     const edp_params& p = c->p;
@@ -929,11 +1253,18 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         int64_t per_cta = (int64_t)EDP_PUSH_THREADS * EDP_ITEMS * 8;
         a.tail_ctas = (tail + per_cta - 1) / per_cta;
         if (a.tail_ctas < 1) a.tail_ctas = 1;
-        int64_t grid = a.n_chunks + a.tail_ctas;
         ++c->launches;
-        const unsigned gr = (unsigned)grid;
         const int variant = (is_ion ? 4 : 0) | (c->kp.periodic ? 2 : 0) | (use_rot ? 1 : 0);
-        switch (variant) {
+        bool classic = true;
+        if (c->push_kernel != 0 && a.n_chunks > 0) {
+            // the sorted chunks by the streaming kernel, the unsorted tail (if any) by the per-chunk kernel
+            TRY(launch_stream_push(c, variant, c->push_kernel, a));
+            a.n_chunks = 0;
+            classic = tail > 0;
+            if (classic) ++c->launches;
+        }
+        const unsigned gr = (unsigned)(a.n_chunks + a.tail_ctas);
+        if (classic) switch (variant) {
         case 0: push_mixed_kernel<false, false, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
         case 1: push_mixed_kernel<false, false, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
         case 2: push_mixed_kernel<false, true, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
