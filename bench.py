@@ -581,9 +581,10 @@ def main():
                     help="only the Poisson leg (cfg2 geometry), optionally only the named runs "
                          "(plain_mg, plain_nopc, learned_mg, learned_nopc)")
     ap.add_argument("--poisson-steps", type=int, default=30)
-    ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2],
+    ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2, 3],
                     help="mixed push over the sorted chunks (edp_set_push_kernel): 0 per-chunk CTAs, 1 streaming "
-                         "(bulk copies, 4 particles per thread), 2 streaming (2 per thread, 3 stages)")
+                         "(bulk copies, 4 particles per thread), 2 streaming (2 per thread, 3 stages), 3 per-chunk "
+                         "CTAs with 2 particles per thread")
     args = ap.parse_args()
     cfg = _decks_module().CONFIGS[args.config]
     args.cells_x, args.cells_y = args.cells if args.cells else (cfg["ncx"], cfg["ncy"])

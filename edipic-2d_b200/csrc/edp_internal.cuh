@@ -242,8 +242,9 @@ struct edp_ctx {
     EdpPotentialProfile pot[4 + EDP_MAX_INNER];   // their time dependence (walls by side, then inner objects)
     int64_t launches = 0;             // kernels launched (reported by edp_query_counters)
     // mixed push over the sorted chunks: 0 one CTA per chunk with the threads' own loads; 1 persistent CTAs with
-    // bulk-copy staging, 4 particles per thread, 2 stages; 2 the same with 2 particles per thread, 3 stages
-    int32_t push_kernel = 1;
+    // bulk-copy staging, 4 particles per thread, 2 stages; 2 the same with 2 particles per thread, 3 stages; 3 as 0
+    // with 2 particles per thread
+    int32_t push_kernel = 0;
 };
 
 // ------------------------------------------------------------------------------------------ Philox

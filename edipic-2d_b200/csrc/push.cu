@@ -154,6 +154,15 @@ __device__ __forceinline__ int win_dx(int d, const edp_kparams& kp)
     return PER ? (d & (kp.ncx - 1)) : d;
 }
 
+// round-to-nearest-even of 0 <= x <= 2^51 to an integer with one FP64 add: x + 1.5 * 2^52 has a unit in the last
+// place of 1, so the sum is rounded to an integer and its low mantissa bits hold it (the classic magic-number
+// conversion); equal to __double2ll_rn(x) on that range, on the FP64 pipe instead of the conversion unit
+__device__ __forceinline__ long long fix_round(double x)
+{
+    const double magic = 6755399441055744.0;   // 1.5 * 2^52
+    return __double_as_longlong(__dadd_rn(x, magic)) - __double_as_longlong(magic);
+}
+
 // One particle. Returns false when it was absorbed (the caller stores cell = -1).
 // ION: ion species (acc_E, RCX) instead of electrons (E, MCC selection); PER: periodic x; ROT: Boris rotation.
 template <bool ION, bool PER, bool ROT>
@@ -270,11 +279,11 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     // ---- deposit (:1597-1639): exact FP64 weights of the FP32 offsets, rounded to 2^-32; the fourth weight
     // takes the remainder so that every particle deposits exactly 2^32 units
     // (the 2^32 scaling is exact, so folding it into one factor rounds the same way)
-    const double dx = (double)nx, dy = (double)ny, mxd = 1.0 - dx;
-    const double A = (1.0 - dy) * EDP_FIX_ONE, B = dy * EDP_FIX_ONE;
-    const long long q00 = __double2ll_rn(mxd * A);
-    const long long q10 = __double2ll_rn(dx * A);
-    const long long q01 = __double2ll_rn(mxd * B);
+    const double dx = (double)nx, dy = (double)ny, mxd = __dsub_rn(1.0, dx);
+    const double A = __dmul_rn(__dsub_rn(1.0, dy), EDP_FIX_ONE), B = __dmul_rn(dy, EDP_FIX_ONE);
+    const long long q00 = fix_round(__dmul_rn(mxd, A));
+    const long long q10 = fix_round(__dmul_rn(dx, A));
+    const long long q01 = fix_round(__dmul_rn(mxd, B));
     const long long q11 = 4294967296LL - q00 - q10 - q01;
     const int dlx = win_dx<PER>(ni - wx0, kp), dly = nj - wy0;
     if (windowed && (unsigned)dlx < EDP_WIN_CELLS && (unsigned)dly < EDP_WIN_CELLS) {
@@ -318,40 +327,54 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     return true;
 }
 
-// four consecutive slots [4g, 4g+4). WIN: a sorted chunk, always whole groups (tiles are padded to multiples of
-// EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted to [lo, hi).
-template <bool ION, bool PER, bool ROT, bool WIN>
+// vector access to IPT consecutive 32-bit values (IPT = 4: 128-bit, 2: 64-bit), streaming (not kept in L1/L2)
+template <int IPT>
+__device__ __forceinline__ void vload(const void* p, int64_t g, uint32_t* v)
+{
+    if constexpr (IPT == 4) {
+        const uint4 x = __ldcs(reinterpret_cast<const uint4*>(p) + g);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+        const uint2 x = __ldcs(reinterpret_cast<const uint2*>(p) + g);
+        v[0] = x.x; v[1] = x.y;
+    }
+}
+template <int IPT>
+__device__ __forceinline__ void vstore(void* p, int64_t g, const uint32_t* v)
+{
+    if constexpr (IPT == 4) __stcs(reinterpret_cast<uint4*>(p) + g, make_uint4(v[0], v[1], v[2], v[3]));
+    else __stcs(reinterpret_cast<uint2*>(p) + g, make_uint2(v[0], v[1]));
+}
+
+// IPT consecutive slots [IPT g, IPT g + IPT). WIN: a sorted chunk, always whole groups (tiles are padded to
+// multiples of EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted
+// to [lo, hi).
+template <bool ION, bool PER, bool ROT, bool WIN, int IPT>
 __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
                                            int64_t hi)
 {
-    const int64_t base = g * EDP_ITEMS;
-    const bool full = WIN || (base >= lo && base + EDP_ITEMS <= hi);
+    const int64_t base = g * IPT;
+    const bool full = WIN || (base >= lo && base + IPT <= hi);
     const bool windowed = WIN;
-    int c[4];
-    float ox[4], oy[4], vx[4], vy[4], vz[4];
-    uint32_t id[4];
+    int c[IPT];
+    float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
+    uint32_t id[IPT];
     if (full) {
-        int4 c4 = __ldcs(reinterpret_cast<const int4*>(a.P.cell) + g);
-        float4 ox4 = __ldcs(reinterpret_cast<const float4*>(a.P.ox) + g);
-        float4 oy4 = __ldcs(reinterpret_cast<const float4*>(a.P.oy) + g);
-        float4 vx4 = __ldcs(reinterpret_cast<const float4*>(a.P.vx) + g);
-        float4 vy4 = __ldcs(reinterpret_cast<const float4*>(a.P.vy) + g);
-        float4 vz4 = __ldcs(reinterpret_cast<const float4*>(a.P.vz) + g);
-        c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
-        ox[0] = ox4.x; ox[1] = ox4.y; ox[2] = ox4.z; ox[3] = ox4.w;
-        oy[0] = oy4.x; oy[1] = oy4.y; oy[2] = oy4.z; oy[3] = oy4.w;
-        vx[0] = vx4.x; vx[1] = vx4.y; vx[2] = vx4.z; vx[3] = vx4.w;
-        vy[0] = vy4.x; vy[1] = vy4.y; vy[2] = vy4.z; vy[3] = vy4.w;
-        vz[0] = vz4.x; vz[1] = vz4.y; vz[2] = vz4.z; vz[3] = vz4.w;
+        vload<IPT>(a.P.cell, g, reinterpret_cast<uint32_t*>(c));
+        vload<IPT>(a.P.ox, g, reinterpret_cast<uint32_t*>(ox));
+        vload<IPT>(a.P.oy, g, reinterpret_cast<uint32_t*>(oy));
+        vload<IPT>(a.P.vx, g, reinterpret_cast<uint32_t*>(vx));
+        vload<IPT>(a.P.vy, g, reinterpret_cast<uint32_t*>(vy));
+        vload<IPT>(a.P.vz, g, reinterpret_cast<uint32_t*>(vz));
         if (a.do_coll || a.emit_on) {
-            uint4 id4 = __ldcs(reinterpret_cast<const uint4*>(a.P.id) + g);
-            id[0] = id4.x; id[1] = id4.y; id[2] = id4.z; id[3] = id4.w;
+            vload<IPT>(a.P.id, g, id);
         } else {
-            id[0] = id[1] = id[2] = id[3] = 0u;
+#pragma unroll
+            for (int e = 0; e < IPT; ++e) id[e] = 0u;
         }
     } else {
 #pragma unroll
-        for (int e = 0; e < EDP_ITEMS; ++e) {
+        for (int e = 0; e < IPT; ++e) {
             int64_t k = base + e;
             bool ok = k >= lo && k < hi;
             c[e] = ok ? a.P.cell[k] : -1;
@@ -366,7 +389,7 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
-    for (int e = 0; e < EDP_ITEMS; ++e) {
+    for (int e = 0; e < IPT; ++e) {
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
                                      (uint32_t)(base + e))) {
@@ -376,15 +399,15 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
     }
     dep_flush(s, acc);
     if (full) {
-        __stcs(reinterpret_cast<int4*>(a.P.cell) + g, make_int4(c[0], c[1], c[2], c[3]));
-        __stcs(reinterpret_cast<float4*>(a.P.ox) + g, make_float4(ox[0], ox[1], ox[2], ox[3]));
-        __stcs(reinterpret_cast<float4*>(a.P.oy) + g, make_float4(oy[0], oy[1], oy[2], oy[3]));
-        __stcs(reinterpret_cast<float4*>(a.P.vx) + g, make_float4(vx[0], vx[1], vx[2], vx[3]));
-        __stcs(reinterpret_cast<float4*>(a.P.vy) + g, make_float4(vy[0], vy[1], vy[2], vy[3]));
-        __stcs(reinterpret_cast<float4*>(a.P.vz) + g, make_float4(vz[0], vz[1], vz[2], vz[3]));
+        vstore<IPT>(a.P.cell, g, reinterpret_cast<const uint32_t*>(c));
+        vstore<IPT>(a.P.ox, g, reinterpret_cast<const uint32_t*>(ox));
+        vstore<IPT>(a.P.oy, g, reinterpret_cast<const uint32_t*>(oy));
+        vstore<IPT>(a.P.vx, g, reinterpret_cast<const uint32_t*>(vx));
+        vstore<IPT>(a.P.vy, g, reinterpret_cast<const uint32_t*>(vy));
+        vstore<IPT>(a.P.vz, g, reinterpret_cast<const uint32_t*>(vz));
     } else {
 #pragma unroll
-        for (int e = 0; e < EDP_ITEMS; ++e) {
+        for (int e = 0; e < IPT; ++e) {
             int64_t k = base + e;
             if (k < lo || k >= hi) continue;
             a.P.cell[k] = c[e];
@@ -398,8 +421,9 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
     }
 }
 
-template <bool ION, bool PER, bool ROT>
-__global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArgs a)   // 64 registers, no spills
+// IPT particles per thread: 4 (128-bit accesses, 4 CTAs of 256 per SM) or 2 (64-bit, 5 CTAs per SM)
+template <bool ION, bool PER, bool ROT, int IPT>
+__global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed_kernel(PushArgs a)
 {
     __shared__ Smem s;
     const edp_kparams& kp = a.kp;
@@ -428,13 +452,13 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, 4) push_mixed_kernel(PushArg
     }
     __syncthreads();
     if (windowed) {
-        for (int64_t g = lo / EDP_ITEMS + threadIdx.x; g * EDP_ITEMS < hi; g += blockDim.x)
-            push_group<ION, PER, ROT, true>(a, s, wx0, wy0, g, lo, hi);
+        for (int64_t g = lo / IPT + threadIdx.x; g * IPT < hi; g += blockDim.x)
+            push_group<ION, PER, ROT, true, IPT>(a, s, wx0, wy0, g, lo, hi);
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
-        int64_t g0 = lo / EDP_ITEMS;
-        for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * EDP_ITEMS < hi; g += a.tail_ctas * blockDim.x)
-            push_group<ION, PER, ROT, false>(a, s, 0, 0, g, lo, hi);
+        int64_t g0 = lo / IPT;
+        for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * IPT < hi; g += a.tail_ctas * blockDim.x)
+            push_group<ION, PER, ROT, false, IPT>(a, s, 0, 0, g, lo, hi);
     }
     __syncthreads();
     if (windowed) {
@@ -1196,9 +1220,26 @@ static int launch_stream_push(edp_ctx* c, int variant, int kind, const PushArgs&
     return kind == 2 ? launch_stream_kind<2, 3>(c, variant, a) : launch_stream_kind<4, 2>(c, variant, a);
 }
 
+template <int IPT>
+static int launch_classic_push(edp_ctx* c, int variant, unsigned gr, const PushArgs& a)
+{
+    switch (variant) {
+    case 0: push_mixed_kernel<false, false, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 1: push_mixed_kernel<false, false, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 2: push_mixed_kernel<false, true, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 3: push_mixed_kernel<false, true, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 4: push_mixed_kernel<true, false, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 5: push_mixed_kernel<true, false, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 6: push_mixed_kernel<true, true, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    default: push_mixed_kernel<true, true, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    }
+    EDP_CUDA(c, cudaGetLastError());
+    return EDP_OK;
+}
+
 int edp_set_push_kernel(edp_ctx* c, int32_t kind)
 {
-    if (!c || kind < 0 || kind > 2) return edp_fail(c, EDP_ERR_ARG, "edp_set_push_kernel");
+    if (!c || kind < 0 || kind > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_push_kernel");
     c->push_kernel = kind;
     return EDP_OK;
 }
@@ -1256,7 +1297,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         ++c->launches;
         const int variant = (is_ion ? 4 : 0) | (c->kp.periodic ? 2 : 0) | (use_rot ? 1 : 0);
         bool classic = true;
-        if (c->push_kernel != 0 && a.n_chunks > 0) {
+        if ((c->push_kernel == 1 || c->push_kernel == 2) && a.n_chunks > 0) {
             // the sorted chunks by the streaming kernel, the unsorted tail (if any) by the per-chunk kernel
             TRY(launch_stream_push(c, variant, c->push_kernel, a));
             a.n_chunks = 0;
@@ -1264,15 +1305,9 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
             if (classic) ++c->launches;
         }
         const unsigned gr = (unsigned)(a.n_chunks + a.tail_ctas);
-        if (classic) switch (variant) {
-        case 0: push_mixed_kernel<false, false, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 1: push_mixed_kernel<false, false, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 2: push_mixed_kernel<false, true, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 3: push_mixed_kernel<false, true, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 4: push_mixed_kernel<true, false, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 5: push_mixed_kernel<true, false, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        case 6: push_mixed_kernel<true, true, false><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-        default: push_mixed_kernel<true, true, true><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+        if (classic) {
+            if (c->push_kernel == 3) TRY(launch_classic_push<2>(c, variant, gr, a));
+            else TRY(launch_classic_push<4>(c, variant, gr, a));
         }
         if (do_mcc) {
             SelArgs b;
