@@ -1296,11 +1296,24 @@ int edp_end_ion_cycle(edp_ctx* c)
     c->steps_since_sort++;
     if (c->p.precision == EDP_PREC_MIXED && c->p.sort_every > 0 && c->steps_since_sort >= c->p.sort_every &&
         c->n_sub_phase == 0) {
-        for (int s = 0; s < c->nspec; ++s)
-            if (c->uploaded[s]) TRY(edp_launch_sort(c, s));
+        for (int s = 0; s < c->nspec; ++s) {
+            if (!c->uploaded[s]) continue;
+            if (c->fused_sort) c->sort_due[s] = 1;   // done by the species' next push
+            else TRY(edp_launch_sort(c, s));
+        }
         c->steps_since_sort = 0;
     }
     return finish_sync(c);
+}
+
+int edp_set_sort_in_push(edp_ctx* c, int32_t on)
+{
+    if (!c) return EDP_ERR_ARG;
+    c->fused_sort = on ? 1 : 0;
+    if (!on)
+        for (int s = 0; s < c->nspec; ++s)
+            if (c->sort_due[s]) TRY(edp_launch_sort(c, s));
+    return EDP_OK;
 }
 
 int edp_set_id_range(edp_ctx* c, uint64_t base, uint64_t end)

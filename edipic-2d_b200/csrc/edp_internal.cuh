@@ -72,6 +72,14 @@ struct edp_species_mixed {
     int32_t* tag = nullptr;
 };
 
+// sort key of a mixed-precision particle in slot k: its 16 x 16-cell tile, then (k / 32) mod 256, so that runs of 32
+// source slots stay together and runs interleave inside a tile (see sort.cu)
+__device__ __forceinline__ uint32_t edp_tile_key(int cell, int64_t k, int ntx)
+{
+    int i = cell & 0xFFFF, j = cell >> 16;
+    return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)((k >> 5) & 255);
+}
+
 struct edp_species_fp64 {
     double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;  // x < -1e29: dead
     uint32_t* id = nullptr;
@@ -153,6 +161,8 @@ struct edp_ctx {
     int64_t host_slots[EDP_MAX_SPECIES] = {0};   // host-side upper bound of n_slots
     int64_t sorted_end[EDP_MAX_SPECIES] = {0};   // slots [0, sorted_end) are tile-sorted
     int64_t steps_since_sort = 0;
+    int sort_due[EDP_MAX_SPECIES] = {0};   // the next push of the species sorts it (fused_sort)
+    int32_t fused_sort = 1;                // periodic sorts inside the push (1) or as a separate pass (0)
     uint64_t id_base = 0;             // first id of the particles this context creates (distribution, upload)
     uint64_t id_end = 1ull << 32;     // one past the last id of the context's range (edp_set_id_range)
     uint32_t dirty = 0;               // bit s: species s's density was deposited since the last edp_reduce_list
@@ -570,6 +580,11 @@ int edp_launch_collide_en(edp_ctx* c);
 int edp_launch_collide_rcx(edp_ctx* c);
 int edp_launch_append_born(edp_ctx* c);
 int edp_launch_sort(edp_ctx* c, int species);
+// the sort done by the next push of a species (edp_end_ion_cycle marks it due): the histogram and scans of the
+// pre-push keys (edp_sort_prepare), the push writing every particle to its sorted slot in the other arrays, then
+// edp_sort_finish (slot count, swap, chunk list)
+int edp_sort_prepare(edp_ctx* c, int species, unsigned long long** cursor);
+int edp_sort_finish(edp_ctx* c, int species);
 int edp_launch_density(edp_ctx* c);
 int edp_launch_fftx(edp_ctx* c);
 int edp_launch_efield(edp_ctx* c);

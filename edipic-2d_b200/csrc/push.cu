@@ -36,6 +36,11 @@ struct PushArgs {
     int64_t sel_cap;
     edp_hits hits;                 // wall-hit list of ion-induced electron emission
     int emit_on;
+    // sort inside the push: every particle goes to slot cursor[key of its pre-push cell and source slot]++ of D
+    edp_species_mixed D;
+    unsigned long long* cursor;
+    int ntx;
+    int64_t cap;
 };
 
 __device__ __forceinline__ int wrapx(int lx, const edp_kparams& kp)
@@ -168,7 +173,7 @@ __device__ __forceinline__ long long fix_round(double x)
 template <bool ION, bool PER, bool ROT>
 __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, DepAcc& acc,
                                          int& cell, float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id,
-                                         uint32_t slot)
+                                         bool& selected)
 {
     const edp_kparams& kp = a.kp;
     int i = cell & 0xFFFF, j = cell >> 16;
@@ -313,7 +318,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     // ---- collisions in the epilogue, with the variates of the separate passes
     if (!ION && a.do_coll) {
         double r;
-        if (edp_mcc_select(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, r)) select_slot(a, s, slot);
+        selected = edp_mcc_select(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, r);
     }
     if (ION && a.do_coll) {
         double dvx = vx, dvy = vy, dvz = vz;
@@ -349,16 +354,18 @@ __device__ __forceinline__ void vstore(void* p, int64_t g, const uint32_t* v)
 // IPT consecutive slots [IPT g, IPT g + IPT). WIN: a sorted chunk, always whole groups (tiles are padded to
 // multiples of EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted
 // to [lo, hi).
-template <bool ION, bool PER, bool ROT, bool WIN, int IPT>
+template <bool ION, bool PER, bool ROT, bool WIN, int IPT, bool SCAT>
 __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
                                            int64_t hi)
 {
+    const unsigned mask = __activemask();
     const int64_t base = g * IPT;
     const bool full = WIN || (base >= lo && base + IPT <= hi);
     const bool windowed = WIN;
-    int c[IPT];
+    int c[IPT], cpre[IPT], tag[IPT] = {};
     float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
     uint32_t id[IPT];
+    bool sel[IPT];
     if (full) {
         vload<IPT>(a.P.cell, g, reinterpret_cast<uint32_t*>(c));
         vload<IPT>(a.P.ox, g, reinterpret_cast<uint32_t*>(ox));
@@ -366,12 +373,13 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
         vload<IPT>(a.P.vx, g, reinterpret_cast<uint32_t*>(vx));
         vload<IPT>(a.P.vy, g, reinterpret_cast<uint32_t*>(vy));
         vload<IPT>(a.P.vz, g, reinterpret_cast<uint32_t*>(vz));
-        if (a.do_coll || a.emit_on) {
+        if (a.do_coll || a.emit_on || SCAT) {
             vload<IPT>(a.P.id, g, id);
         } else {
 #pragma unroll
             for (int e = 0; e < IPT; ++e) id[e] = 0u;
         }
+        if constexpr (SCAT) vload<IPT>(a.P.tag, g, reinterpret_cast<uint32_t*>(tag));
     } else {
 #pragma unroll
         for (int e = 0; e < IPT; ++e) {
@@ -384,20 +392,58 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
             vy[e] = ok ? a.P.vy[k] : 0.f;
             vz[e] = ok ? a.P.vz[k] : 0.f;
             id[e] = ok ? a.P.id[k] : 0u;
+            if constexpr (SCAT) tag[e] = ok ? a.P.tag[k] : 0;
         }
     }
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
     for (int e = 0; e < IPT; ++e) {
+        cpre[e] = c[e];
+        sel[e] = false;
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                     (uint32_t)(base + e))) {
+                                     sel[e])) {
             c[e] = -1;
+            sel[e] = false;
             atomicAdd(&s.cnt[17], 1ull);
         }
     }
     dep_flush(s, acc);
+    if constexpr (SCAT) {
+        // each live source slot takes the next slot of its key's run in D (warp-aggregated cursor updates); a
+        // particle absorbed now leaves a dead slot there, compacted by the next sort
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int e = 0; e < IPT; ++e) {
+            const uint32_t key = cpre[e] >= 0 ? edp_tile_key(cpre[e], base + e, a.ntx) : 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(mask, key);
+            const int leader = __ffs(peers) - 1;
+            unsigned long long b0 = 0;
+            if (key != 0xFFFFFFFFu && lane == leader) b0 = atomicAdd(&a.cursor[key], (unsigned long long)__popc(peers));
+            b0 = __shfl_sync(mask, b0, leader);
+            if (key == 0xFFFFFFFFu) continue;
+            const unsigned long long pos = b0 + __popc(peers & ((1u << lane) - 1u));
+            if ((int64_t)pos >= a.cap) {
+                atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
+                continue;
+            }
+            a.D.cell[pos] = c[e];
+            if (c[e] < 0) continue;
+            a.D.ox[pos] = ox[e];
+            a.D.oy[pos] = oy[e];
+            a.D.vx[pos] = vx[e];
+            a.D.vy[pos] = vy[e];
+            a.D.vz[pos] = vz[e];
+            a.D.id[pos] = id[e];
+            a.D.tag[pos] = tag[e];
+            if (sel[e]) select_slot(a, s, (uint32_t)pos);
+        }
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < IPT; ++e)
+        if (sel[e]) select_slot(a, s, (uint32_t)(base + e));
     if (full) {
         vstore<IPT>(a.P.cell, g, reinterpret_cast<const uint32_t*>(c));
         vstore<IPT>(a.P.ox, g, reinterpret_cast<const uint32_t*>(ox));
@@ -421,8 +467,9 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
     }
 }
 
-// IPT particles per thread: 4 (128-bit accesses, 4 CTAs of 256 per SM) or 2 (64-bit, 5 CTAs per SM)
-template <bool ION, bool PER, bool ROT, int IPT>
+// IPT particles per thread: 4 (128-bit accesses, 4 CTAs of 256 per SM) or 2 (64-bit, 5 CTAs per SM). SCAT: the
+// push of a sort step, writing every particle to its sorted slot of a.D
+template <bool ION, bool PER, bool ROT, int IPT, bool SCAT>
 __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed_kernel(PushArgs a)
 {
     __shared__ Smem s;
@@ -453,12 +500,12 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed
     __syncthreads();
     if (windowed) {
         for (int64_t g = lo / IPT + threadIdx.x; g * IPT < hi; g += blockDim.x)
-            push_group<ION, PER, ROT, true, IPT>(a, s, wx0, wy0, g, lo, hi);
+            push_group<ION, PER, ROT, true, IPT, SCAT>(a, s, wx0, wy0, g, lo, hi);
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
         int64_t g0 = lo / IPT;
         for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * IPT < hi; g += a.tail_ctas * blockDim.x)
-            push_group<ION, PER, ROT, false, IPT>(a, s, 0, 0, g, lo, hi);
+            push_group<ION, PER, ROT, false, IPT, SCAT>(a, s, 0, 0, g, lo, hi);
     }
     __syncthreads();
     if (windowed) {
@@ -707,10 +754,13 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 3 : 4) push_strea
 #pragma unroll
             for (int e = 0; e < IPT; ++e) {
                 if (c[e] < 0) continue;
+                bool sel = false;
                 if (!push_one<ION, PER, ROT>(a, s, true, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                             (uint32_t)(base + e))) {
+                                             sel)) {
                     c[e] = -1;
                     atomicAdd(&s.cnt[17], 1ull);
+                } else if (sel) {
+                    select_slot(a, s, (uint32_t)(base + e));
                 }
             }
             dep_flush(s, acc);
@@ -1220,18 +1270,18 @@ static int launch_stream_push(edp_ctx* c, int variant, int kind, const PushArgs&
     return kind == 2 ? launch_stream_kind<2, 3>(c, variant, a) : launch_stream_kind<4, 2>(c, variant, a);
 }
 
-template <int IPT>
+template <int IPT, bool SCAT>
 static int launch_classic_push(edp_ctx* c, int variant, unsigned gr, const PushArgs& a)
 {
     switch (variant) {
-    case 0: push_mixed_kernel<false, false, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 1: push_mixed_kernel<false, false, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 2: push_mixed_kernel<false, true, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 3: push_mixed_kernel<false, true, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 4: push_mixed_kernel<true, false, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 5: push_mixed_kernel<true, false, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 6: push_mixed_kernel<true, true, false, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    default: push_mixed_kernel<true, true, true, IPT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 0: push_mixed_kernel<false, false, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 1: push_mixed_kernel<false, false, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 2: push_mixed_kernel<false, true, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 3: push_mixed_kernel<false, true, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 4: push_mixed_kernel<true, false, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 5: push_mixed_kernel<true, false, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 6: push_mixed_kernel<true, true, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    default: push_mixed_kernel<true, true, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
     }
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
@@ -1294,10 +1344,21 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         int64_t per_cta = (int64_t)EDP_PUSH_THREADS * EDP_ITEMS * 8;
         a.tail_ctas = (tail + per_cta - 1) / per_cta;
         if (a.tail_ctas < 1) a.tail_ctas = 1;
+        // a sort due for this species happens in this push: the particles go to their sorted slots in the other
+        // arrays (the keys are those of the cells before the push, so a particle ends within a cell of its tile)
+        const bool fused = c->sort_due[sp] != 0;
+        if (fused) {
+            unsigned long long* cur = nullptr;
+            TRY(edp_sort_prepare(c, sp, &cur));
+            a.D = c->pm_alt[sp];
+            a.cursor = cur;
+            a.ntx = c->ntx;
+            a.cap = c->cap[sp];
+        }
         ++c->launches;
         const int variant = (is_ion ? 4 : 0) | (c->kp.periodic ? 2 : 0) | (use_rot ? 1 : 0);
         bool classic = true;
-        if ((c->push_kernel == 1 || c->push_kernel == 2) && a.n_chunks > 0) {
+        if ((c->push_kernel == 1 || c->push_kernel == 2) && a.n_chunks > 0 && !fused) {
             // the sorted chunks by the streaming kernel, the unsorted tail (if any) by the per-chunk kernel
             TRY(launch_stream_push(c, variant, c->push_kernel, a));
             a.n_chunks = 0;
@@ -1306,9 +1367,11 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         }
         const unsigned gr = (unsigned)(a.n_chunks + a.tail_ctas);
         if (classic) {
-            if (c->push_kernel == 3) TRY(launch_classic_push<2>(c, variant, gr, a));
-            else TRY(launch_classic_push<4>(c, variant, gr, a));
+            if (fused) TRY((launch_classic_push<4, true>(c, variant, gr, a)));
+            else if (c->push_kernel == 3) TRY((launch_classic_push<2, false>(c, variant, gr, a)));
+            else TRY((launch_classic_push<4, false>(c, variant, gr, a)));
         }
+        if (fused) TRY(edp_sort_finish(c, sp));   // the sorted arrays are the species' arrays from here on
         if (do_mcc) {
             SelArgs b;
             memset(&b, 0, sizeof(b));

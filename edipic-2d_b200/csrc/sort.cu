@@ -15,11 +15,7 @@
 
 namespace {
 
-__device__ __forceinline__ uint32_t tile_key(int cell, int64_t k, int ntx)
-{
-    int i = cell & 0xFFFF, j = cell >> 16;
-    return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)((k >> 5) & 255);
-}
+__device__ __forceinline__ uint32_t tile_key(int cell, int64_t k, int ntx) { return edp_tile_key(cell, k, ntx); }
 
 __global__ void hist_kernel(const int32_t* __restrict__ cell, const unsigned long long* n_slots, int ntx,
                             uint32_t* __restrict__ count)
@@ -94,18 +90,22 @@ __global__ void tiles_scan_kernel(const unsigned long long* __restrict__ tile_to
 // scatter cursors = tile base + offset inside the tile; padding slots at each tile's end marked dead
 __global__ void cursor_kernel(const unsigned long long* __restrict__ local, const unsigned long long* __restrict__ tile_base,
                               const unsigned long long* __restrict__ tile_total, int64_t ntiles,
-                              unsigned long long* __restrict__ cursor, int32_t* __restrict__ dst_cell)
+                              unsigned long long* __restrict__ cursor, int32_t* __restrict__ dst_cell, int64_t cap,
+                              unsigned int* eflag)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < ntiles * 256) cursor[k] = tile_base[k >> 8] + local[k];
     if (k < ntiles) {
         const unsigned long long e = tile_base[k] + tile_total[k];
-        for (unsigned long long q = e; q < tile_base[k + 1]; ++q) dst_cell[q] = -1;
+        for (unsigned long long q = e; q < tile_base[k + 1]; ++q) {
+            if ((int64_t)q < cap) dst_cell[q] = -1;
+            else atomicOr(eflag, EDP_EFLAG_CAPACITY);
+        }
     }
 }
 
 __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, const unsigned long long* n_slots,
-                               int ntx, unsigned long long* __restrict__ cursor)
+                               int ntx, unsigned long long* __restrict__ cursor, int64_t cap, unsigned int* eflag)
 {
     const int64_t n = (int64_t)*n_slots;
     const int lane = threadIdx.x & 31;
@@ -120,6 +120,10 @@ __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, con
         base = __shfl_sync(0xFFFFFFFFu, base, leader);
         if (key == 0xFFFFFFFFu) continue;
         unsigned long long pos = base + __popc(peers & ((1u << lane) - 1u));
+        if ((int64_t)pos >= cap) {   // the padded total exceeds the capacity: reported, nothing written
+            atomicOr(eflag, EDP_EFLAG_CAPACITY);
+            continue;
+        }
         dst.cell[pos] = c;
         dst.ox[pos] = src.ox[k];
         dst.oy[pos] = src.oy[k];
@@ -135,19 +139,19 @@ __global__ void set_slots(unsigned long long* n_slots, unsigned long long* n_liv
                           const unsigned long long* live)
 {
     *n_slots = *total;
-    *n_live = *live;
+    if (n_live) *n_live = *live;
 }
 
 }  // namespace
 
-int edp_launch_sort(edp_ctx* c, int sp)
+// histogram of the keys of the current particles, the scans, the cursors of the other arrays and their padding
+// slots (marked dead); the scratch layout is tile_total[ntiles] | tile_base[ntiles+1] | cursor[nkeys] | live[1]
+int edp_sort_prepare(edp_ctx* c, int sp, unsigned long long** cursor_out)
 {
-    if (c->p.precision != EDP_PREC_MIXED) return EDP_OK;
     const int64_t ntiles = (int64_t)c->ntx * c->nty;
     const int64_t nkeys = ntiles * 256;
     const int64_t nslots = std::max<int64_t>(c->host_slots[sp], 1);
     unsigned grid = (unsigned)std::min<int64_t>((nslots + 255) / 256, 148 * 16);
-    // scratch layout: tile_total[ntiles] | tile_base[ntiles+1] | cursor[nkeys] | live[1]
     unsigned long long* tile_total = c->scan_tmp;
     unsigned long long* tile_base = tile_total + ntiles;
     unsigned long long* cursor = tile_base + ntiles + 1;
@@ -162,11 +166,25 @@ int edp_launch_sort(edp_ctx* c, int sp)
     tiles_scan_kernel<<<1, 1024, 0, c->stream>>>(tile_total, ntiles, tile_base, live);
     ++c->launches;
     cursor_kernel<<<(unsigned)((nkeys + 255) / 256), 256, 0, c->stream>>>(c->sort_offset, tile_base, tile_total,
-                                                                           ntiles, cursor, c->pm_alt[sp].cell);
+                                                                           ntiles, cursor, c->pm_alt[sp].cell,
+                                                                           c->cap[sp], &c->dc->error_flags);
+    EDP_CUDA(c, cudaGetLastError());
+    *cursor_out = cursor;
+    return EDP_OK;
+}
+
+// after the particles were written to their sorted slots in pm_alt: slot count (and, for the separate pass, the live
+// count), swap, and the chunk list of the new order (one synchronisation)
+static int sort_finish(edp_ctx* c, int sp, bool set_live)
+{
+    const int64_t ntiles = (int64_t)c->ntx * c->nty;
+    const int64_t nkeys = ntiles * 256;
+    unsigned long long* tile_total = c->scan_tmp;
+    unsigned long long* tile_base = tile_total + ntiles;
+    unsigned long long* live = tile_base + ntiles + 1 + nkeys;
     ++c->launches;
-    scatter_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp], c->pm_alt[sp], &c->dc->n_slots[sp], c->ntx, cursor);
-    ++c->launches;
-    set_slots<<<1, 1, 0, c->stream>>>(&c->dc->n_slots[sp], &c->dc->n_live[sp], tile_base + ntiles, live);
+    set_slots<<<1, 1, 0, c->stream>>>(&c->dc->n_slots[sp], set_live ? &c->dc->n_live[sp] : nullptr,
+                                      tile_base + ntiles, live);
     EDP_CUDA(c, cudaGetLastError());
     std::swap(c->pm[sp], c->pm_alt[sp]);
     std::vector<unsigned long long> h(ntiles + 1);
@@ -201,5 +219,22 @@ int edp_launch_sort(edp_ctx* c, int sp)
     c->n_chunks[sp] = (int64_t)ch.size();
     c->sorted_end[sp] = (int64_t)h[ntiles];
     c->host_slots[sp] = (int64_t)h[ntiles];
+    c->sort_due[sp] = 0;
     return EDP_OK;
+}
+
+int edp_sort_finish(edp_ctx* c, int sp) { return sort_finish(c, sp, false); }
+
+int edp_launch_sort(edp_ctx* c, int sp)
+{
+    if (c->p.precision != EDP_PREC_MIXED) return EDP_OK;
+    const int64_t nslots = std::max<int64_t>(c->host_slots[sp], 1);
+    unsigned grid = (unsigned)std::min<int64_t>((nslots + 255) / 256, 148 * 16);
+    unsigned long long* cursor = nullptr;
+    TRY(edp_sort_prepare(c, sp, &cursor));
+    ++c->launches;
+    scatter_kernel<<<grid, 256, 0, c->stream>>>(c->pm[sp], c->pm_alt[sp], &c->dc->n_slots[sp], c->ntx, cursor,
+                                                c->cap[sp], &c->dc->error_flags);
+    EDP_CUDA(c, cudaGetLastError());
+    return sort_finish(c, sp, true);
 }

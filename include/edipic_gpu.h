@@ -188,6 +188,10 @@ int edp_sort_particles(edp_ctx* ctx);
  * thread and 3 stages; 3 as 0 with 2 particles per thread (more resident warps). All give the same results; only
  * the speed differs. */
 int edp_set_push_kernel(edp_ctx* ctx, int32_t kind);
+/* No counterpart in the reference. on = 1 (default): a periodic sort (every sort_every steps) is done by each
+ * species' next push, which writes the pushed particles straight to their sorted slots (keys of their cells before
+ * the push); on = 0: a separate pass at the end of the step. Same results. */
+int edp_set_sort_in_push(edp_ctx* ctx, int32_t on);
 
 /* ---- particles ----------------------------------------------------------------------------------- */
 /* after DISTRIBUTE_PARTICLES (pic2d_CurProblemValues.f90:3127-3325) or a checkpoint read: the host's

@@ -96,6 +96,36 @@ def test_sorting_does_not_change_the_state(tmp_path):
 
 
 @pytest.mark.gpu
+def test_sort_in_the_push_equals_the_separate_sort(tmp_path):
+    """A periodic sort done by the next push (each particle written straight to its sorted slot, keyed by its cell
+    before the push) and the separate sort pass at the end of the step give bit-identical particles, densities and
+    wall hits over 14 steps with a sort every 3, with the unsorted tail of appended particles (ion-induced emission)
+    and with particles absorbed in the sorting push."""
+    d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, collisions=False, rcx=True, bx=86.6, by=50.0,
+                   ion_emission=(0.5, 0.0, 10000.0, 2.0))
+    out = []
+    for fused in (0, 1):
+        with Simulation(d, precision=PREC_MIXED, sort_every=3, seed=17) as sim:
+            sim._check(sim.lib.edp_set_sort_in_push(sim.ctx, fused), "edp_set_sort_in_push")
+            n = 64 * 48 * 20
+            e = random_particles(sim, n, seed=61, fast_fraction=0.05)
+            ivs = np.random.default_rng(62).normal(0, 0.02, (3, n)).astype(np.float32).astype(np.float64)
+            sim.upload_particles(ELECTRONS, *e, ids=np.arange(n, dtype=np.uint32))
+            sim.upload_particles(IONS, e[0], e[1], ivs[0], ivs[1], ivs[2], ids=np.arange(n, dtype=np.uint32))
+            sim.step(14)
+            c = sim.counters()
+            out.append((_rows(sim.download_particles(ELECTRONS)), sim.download_particles(IONS),
+                        sim.gather_electron_charge_density(), sim.gather_ion_charge_density(),
+                        list(c.electron_hits), list(c.ion_hits), c.rcx_collisions[0], list(c.n_particles[:2])))
+    (a, b) = out
+    assert a[4:] == b[4:] and sum(a[5][:2]) > 100
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+    ia, ib = match_by_id(a[1], b[1])
+    for k in ("x", "y", "vx", "vy", "vz"):
+        assert np.array_equal(a[1][k][ia], b[1][k][ib]), k
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
 def test_fused_collisions_equal_separate_passes(tmp_path, precision):
     d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, n_gas=1.0e23)
