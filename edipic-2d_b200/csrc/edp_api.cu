@@ -1057,9 +1057,12 @@ static int upload_wall_state(edp_ctx* c)
 {
     const edp_emit_dev& h = *c->emit_h;
     c->emit_on = 0;
-    for (int w = 0; w < 4; ++w) {
-        c->emit_on |= h.reflect[w];
-        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) c->emit_on |= h.on[w][q];
+    c->kp.ion_inner_mask = 0;
+    for (int w = 0; w < EDP_N_HIT_COUNTERS; ++w) {
+        int any = h.reflect[w];
+        for (int q = 0; q < EDP_MAX_ION_SPECIES; ++q) any |= h.on[w][q];
+        c->emit_on |= any;
+        if (w >= 4 && any) c->kp.ion_inner_mask |= 1 << (w - 4);
     }
     EDP_CUDA(c, cudaMemcpyAsync(c->emit_dev, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1070,7 +1073,7 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
                          double t_emit_ev)
 {
     if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
-    if (!c || wall < 0 || wall > 3 || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
+    if (!c || wall < 0 || wall >= 4 + c->p.n_inner || ion_species < 1 || ion_species >= c->nspec || !(yield >= 0.0) ||
         !(emax_ev > emin_ev) || !(t_emit_ev >= 0.0))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_emission");
     TRY(wall_state(c));
@@ -1187,7 +1190,7 @@ int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t 
 int edp_set_ion_reflection(edp_ctx* c, int32_t wall, int32_t on)
 {
     if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
-    if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
+    if (!c || wall < 0 || wall >= 4 + c->p.n_inner) return edp_fail(c, EDP_ERR_ARG, "edp_set_ion_reflection");
     TRY(wall_state(c));
     c->emit_h->reflect[wall] = on ? 1 : 0;
     return upload_wall_state(c);

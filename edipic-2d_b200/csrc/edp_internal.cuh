@@ -141,6 +141,7 @@ struct edp_kparams {
     int32_t nsub;
     uint32_t seed_lo, seed_hi;
     int32_t diel_mask;                        // bit n: inner object n is a dielectric
+    int32_t ion_inner_mask;                   // bit n: inner object n emits electrons under ion impact or reflects ions
     int32_t strip;                            // 1: one x strip of a domain (edp_set_strip)
     int32_t strip_gl, strip_gr;               // ghost columns on its left / right; 0: that side is the domain's wall
     int32_t strip_x0, strip_ncx;              // global column of local column 0, columns of the whole domain
@@ -616,11 +617,12 @@ int edp_launch_deposit(edp_ctx* c, int species);   // CIC deposit of the whole a
 // (an ion's energy is Ms v^2, an electron's v^2), and the velocity factor sqrt(T_emit / energy_factor_eV) of the
 // emitted electrons (= sqrt(T_emit / T_e) / N_max_vel, :188).
 struct edp_emit_dev {
-    int reflect[4];            // ion-material model 1: the wall reflects every ion specularly
-    int on[4][EDP_MAX_ION_SPECIES];
-    double yield[4][EDP_MAX_ION_SPECIES];
-    double emin[4][EDP_MAX_ION_SPECIES], emax[4][EDP_MAX_ION_SPECIES];
-    double fconv[4][EDP_MAX_ION_SPECIES];
+    // per object: the four domain walls (0 below, 1 above, 2 left, 3 right), then inner object n at 4 + n
+    int reflect[EDP_N_HIT_COUNTERS];   // ion-material model 1: the object reflects every ion specularly
+    int on[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES];
+    double yield[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES];
+    double emin[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES], emax[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES];
+    double fconv[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES];
     double ms[EDP_MAX_ION_SPECIES];
     const double* maxwell_v;   // GetMaxwellVelocity table, rmax + 1 values
     const double* maxwell_inj; // GetInjMaxwellVelocity table, rmax_inj + 1 values
@@ -641,19 +643,33 @@ __device__ inline double edp_maxwell_inj(const double* v, int rmax, double u)
 // for the domain walls): 1e-6 inside the wall, normal speed from the injection table (variate w0), tangential
 // components from the Maxwell table (w1, w2) in x, y, z order, all times f, then scaled down to the energy left
 // (`energy`, which the electron's energy reduces). Returns false, emitting nothing, when no energy is left.
+// The emitting surface: its outward normal (0 +y, 1 -y, 2 +x, 3 -x: the domain wall below, above, left, right, or an
+// inner object's top, bottom, right, left side) and its coordinate along that normal
+struct edp_face {
+    int dir;
+    double at;
+};
+__device__ __forceinline__ edp_face edp_wall_face(int wall, double xmax, double ymax)
+{
+    edp_face f;
+    f.dir = wall;
+    f.at = wall == 0 ? 0.0 : wall == 1 ? ymax : wall == 2 ? 0.0 : xmax;
+    return f;
+}
+
 __device__ inline bool edp_emit_thermal(const double* maxwell_v, int rmax, const double* maxwell_inj, int rmax_inj,
-                                        int wall, double x, double y, double xmax, double ymax, double f,
-                                        double& energy, const uint32_t w[4], double& nx, double& ny, double v[3])
+                                        edp_face face, double x, double y, double f, double& energy,
+                                        const uint32_t w[4], double& nx, double& ny, double v[3])
 {
     if (energy <= 0.0) return false;
     const double un = edp_maxwell_inj(maxwell_inj, rmax_inj, edp_u01(w[0]));
     const double t1 = edp_maxwell(maxwell_v, rmax, edp_u01(w[1]));
     const double t2 = edp_maxwell(maxwell_v, rmax, edp_u01(w[2]));
-    switch (wall) {
-    case 0: nx = x; ny = 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2; break;            // below (dirflag 4)
-    case 1: nx = x; ny = ymax - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2; break;    // above (dirflag 2)
-    case 2: nx = 1.0e-6; ny = y; v[0] = un; v[1] = t1; v[2] = t2; break;            // left (dirflag 1)
-    default: nx = xmax - 1.0e-6; ny = y; v[0] = -un; v[1] = t1; v[2] = t2; break;   // right (dirflag 3)
+    switch (face.dir) {
+    case 0: nx = x; ny = face.at + 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2; break;    // normal +y (dirflag 4)
+    case 1: nx = x; ny = face.at - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2; break;   // normal -y (dirflag 2)
+    case 2: nx = face.at + 1.0e-6; ny = y; v[0] = un; v[1] = t1; v[2] = t2; break;    // normal +x (dirflag 1)
+    default: nx = face.at - 1.0e-6; ny = y; v[0] = -un; v[1] = t1; v[2] = t2; break;  // normal -x (dirflag 3)
     }
     v[0] *= f;
     v[1] *= f;
@@ -680,7 +696,7 @@ __device__ inline bool edp_emit_thermal(const double* maxwell_v, int rmax, const
 template <class Out>
 __device__ __noinline__ int edp_emit_electrons(const edp_emit_dev* em, int s, int wall, double x, double y,
                                                double vx, double vy, double vz, uint32_t id, uint32_t step,
-                                               uint32_t seed_lo, uint32_t seed_hi, double xmax, double ymax, Out out)
+                                               uint32_t seed_lo, uint32_t seed_hi, edp_face face, Out out)
 {
     if (!em->on[wall][s]) return 0;
     double energy = em->ms[s] * (vx * vx + vy * vy + vz * vz);
@@ -695,8 +711,8 @@ __device__ __noinline__ int edp_emit_electrons(const edp_emit_dev* em, int s, in
         if (energy <= 0.0) return;
         edp_philox(step, EDP_STREAM_EMIT(s), 1u + (uint32_t)e, seed_hi, id, seed_lo, w);
         double nx, ny, v[3];
-        if (!edp_emit_thermal(em->maxwell_v, em->rmax, em->maxwell_inj, em->rmax_inj, wall, x, y, xmax, ymax, f,
-                              energy, w, nx, ny, v))
+        if (!edp_emit_thermal(em->maxwell_v, em->rmax, em->maxwell_inj, em->rmax_inj, face, x, y, f, energy, w, nx,
+                              ny, v))
             return;
         ++e;
         out(nx, ny, v);
@@ -844,8 +860,8 @@ __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, d
         uint32_t wb[4];
         if (energy <= 0.0) return;
         edp_philox(step, EDP_STREAM_SEE, 1u + (uint32_t)k, seed_hi, id, seed_lo, wb);
-        if (!edp_emit_thermal(sd->maxwell_v, sd->rmax, sd->maxwell_inj, sd->rmax_inj, wall, x, y, xmax, ymax, w.fconv,
-                              energy, wb, nx, ny, nv))
+        if (!edp_emit_thermal(sd->maxwell_v, sd->rmax, sd->maxwell_inj, sd->rmax_inj, edp_wall_face(wall, xmax, ymax),
+                              x, y, w.fconv, energy, wb, nx, ny, nv))
             return;
         ++k;
         out(nx, ny, nv);
@@ -878,17 +894,16 @@ __device__ inline bool edp_cross_vertical(double xo, double yo, double x, double
 
 // The trajectory's first crossing of an inner object's outline (FIND_CLOSEST_INTERSECTION_WITH_OBJECT, :649-742,
 // over all inner objects as TRY_ELECTRON_COLL_WITH_INNER_OBJECT :470-557 / TRY_ION_COLL_WITH_INNER_OBJECT,
-// pic2d_IonWallCollisions.f90:391-480; segments 1 left, 2 top, 3 right, 4 bottom; ties keep the earlier one), and
-// the charge q of the absorbed particle given to the two outline nodes next to the crossing when that object is a
-// dielectric (DO_ELECTRON_COLL_WITH_INNER_OBJECT :561-645 / DO_ION_COLL_WITH_INNER_OBJECT): the node fractions
-// are the fractional part of the crossing coordinate, as there. surf holds the charge per node in units of 2^-32.
-// Returns the object index, or -1 when no crossing is found.
-__device__ inline int edp_inner_hit(const edp_kparams& kp, unsigned long long* surf, double X, double Y, double vx,
-                                    double vy, double xmul, double q)
+// pic2d_IonWallCollisions.f90:391-480; segments 1 left, 2 top, 3 right, 4 bottom; ties keep the earlier one). Returns
+// the object index and the segment m and crossing (bx, by), or -1 when no crossing is found.
+__device__ inline int edp_inner_cross(const edp_kparams& kp, double X, double Y, double vx, double vy, double xmul,
+                                      int& bm, double& bx, double& by)
 {
     const double xo = X - vx * xmul, yo = Y - vy * xmul;
-    int best = -1, bm = 0;
-    double bx = 0.0, by = 0.0, bd = 0.0;
+    int best = -1;
+    double bd = 0.0;
+    bm = 0;
+    bx = by = 0.0;
     for (int n = 0; n < kp.n_inner; ++n) {
         const double il = kp.ileft[n], ir = kp.iright[n], jb = kp.jbottom[n], jt = kp.jtop[n];
         for (int m = 1; m <= 4; ++m) {
@@ -911,8 +926,17 @@ __device__ inline int edp_inner_hit(const edp_kparams& kp, unsigned long long* s
             bd = d;
         }
     }
-    if (best < 0 || !((kp.diel_mask >> best) & 1)) return best;
-    const int il = kp.ileft[best], ir = kp.iright[best], jb = kp.jbottom[best], jt = kp.jtop[best];
+    return best;
+}
+
+// The charge q given to the two outline nodes of dielectric object `obj` next to the crossing (bx, by) on segment m
+// (DO_ELECTRON_COLL_WITH_INNER_OBJECT :561-645 / DO_ION_COLL_WITH_INNER_OBJECT; an electron emitted there gives
+// +1 with the same split, INJECT_ION_IMPACT_EXTRACTED_ELECTRON pic2d_IonEmissions.f90:232-330): the node fractions
+// are the fractional part of the crossing coordinate, as there. surf holds the charge per node in units of 2^-32.
+__device__ inline void edp_inner_charge(const edp_kparams& kp, unsigned long long* surf, int obj, int bm, double bx,
+                                        double by, double q)
+{
+    const int il = kp.ileft[obj], ir = kp.iright[obj], jb = kp.jbottom[obj], jt = kp.jtop[obj];
     const int64_t w = kp.nxg;
     int64_t na, nb;   // the outline nodes i and i+1 of the reference's numbering
     double fa;        // fraction of the charge at node i
@@ -950,5 +974,28 @@ __device__ inline int edp_inner_hit(const edp_kparams& kp, unsigned long long* s
     const long long qb = 4294967296LL - qa;
     atomicAdd(&surf[na], (unsigned long long)__double2ll_rn(q * (double)qa));
     atomicAdd(&surf[nb], (unsigned long long)__double2ll_rn(q * (double)qb));
+}
+
+// The emitting face of inner object `obj` at segment m: outward normal and the side's coordinate
+__device__ __forceinline__ edp_face edp_inner_face(const edp_kparams& kp, int obj, int bm)
+{
+    edp_face f;
+    switch (bm) {
+    case 1: f.dir = 3; f.at = (double)kp.ileft[obj]; break;     // left side: normal -x (dirflag 3)
+    case 2: f.dir = 0; f.at = (double)kp.jtop[obj]; break;      // top side: normal +y (dirflag 4)
+    case 3: f.dir = 2; f.at = (double)kp.iright[obj]; break;    // right side: normal +x (dirflag 1)
+    default: f.dir = 1; f.at = (double)kp.jbottom[obj]; break;  // bottom side: normal -y (dirflag 2)
+    }
+    return f;
+}
+
+// crossing plus the charge of a dielectric object; returns the object or -1
+__device__ inline int edp_inner_hit(const edp_kparams& kp, unsigned long long* surf, double X, double Y, double vx,
+                                    double vy, double xmul, double q)
+{
+    int bm;
+    double bx, by;
+    const int best = edp_inner_cross(kp, X, Y, vx, vy, xmul, bm, bx, by);
+    if (best >= 0 && ((kp.diel_mask >> best) & 1)) edp_inner_charge(kp, surf, best, bm, bx, by, q);
     return best;
 }

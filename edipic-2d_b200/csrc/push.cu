@@ -232,7 +232,9 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
                   (nj > kp.jbottom[n] || (nj == kp.jbottom[n] && ny > 0.0f)) && nj < kp.jtop[n];
         if (in) {
             atomicAdd(&s.cnt[4 + n], 1ull);
-            if ((kp.diel_mask >> n) & 1)   // its outline takes the charge: the crossing is found after the push
+            // the crossing is found after the push: a dielectric's outline takes the charge, an ion-emitting or
+            // ion-reflecting object answers the ion
+            if (((kp.diel_mask | (ION ? kp.ion_inner_mask : 0)) >> n) & 1)
                 record_hit(a.hits, a.dc, 4 + n, ION ? a.species - 1 : 0, (double)ni + (double)nx,
                            (double)nj + (double)ny, vx, vy, vz, id);
             return false;
@@ -965,7 +967,8 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             a.P.x[k] = -1.0e30;
             atomicAdd(&cnt[obj], 1ull);
             atomicAdd(&cnt[17], 1ull);
-            if ((a.emit_on && obj < 4) || (obj >= 4 && ((kp.diel_mask >> (obj - 4)) & 1)))
+            if ((a.emit_on && obj < 4) ||
+                (obj >= 4 && (((kp.diel_mask | (a.is_ion ? kp.ion_inner_mask : 0)) >> (obj - 4)) & 1)))
                 record_hit(a.hits, a.dc, obj, a.is_ion ? a.species - 1 : 0, X, Y, vx, vy, vz, a.P.id[k]);
             continue;
         }
@@ -1440,8 +1443,41 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
     const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int ws = h.ws[k], wall = ws & 255, s = ws >> 8;
-        if (wall >= 4) {   // a dielectric inner object: charge Qs on its outline (ions move V N_subcycles per step)
-            edp_inner_hit(kp, surf, h.x[k], h.y[k], h.vx[k], h.vy[k], (double)kp.nsub, qs.qs[s]);
+        if (wall >= 4) {
+            // an inner object (DO_ION_COLL_WITH_INNER_OBJECT, pic2d_IonWallCollisions.f90:484-575): the side the
+            // trajectory crossed first (ions move V N_subcycles per step); a reflecting object returns the ion; a
+            // dielectric takes the charge Qs; an emitting one emits from the crossing point, and a dielectric takes
+            // +1 per emitted electron there
+            int bm;
+            double bx, by;
+            const int obj = edp_inner_cross(kp, h.x[k], h.y[k], h.vx[k], h.vy[k], (double)kp.nsub, bm, bx, by);
+            if (obj < 0) continue;
+            const int o = 4 + obj;
+            const edp_face face = edp_inner_face(kp, obj, bm);
+            const bool diel = (kp.diel_mask >> obj) & 1;
+            if (em && em->reflect[o]) {   // INJECT_REFLECTED_ION, pic2d_IonEmissions.f90:374-492 (m = -1)
+                double v[3] = {h.vx[k], h.vy[k], h.vz[k]};
+                double nx = bx, ny = by;
+                switch (face.dir) {
+                case 0: ny = face.at + 1.0e-6; v[1] = -v[1]; break;
+                case 1: ny = face.at - 1.0e-6; v[1] = -v[1]; break;
+                case 2: nx = face.at + 1.0e-6; v[0] = -v[0]; break;
+                default: nx = face.at - 1.0e-6; v[0] = -v[0]; break;
+                }
+                record_born(born->born_i[s], &dc->born_i_count[s], &dc->error_flags, nx, ny, v);
+                continue;
+            }
+            if (diel) edp_inner_charge(kp, surf, obj, bm, bx, by, qs.qs[s]);
+            if (!em) continue;
+            const edp_born born_e = born->born_e;
+            const int m = edp_emit_electrons(em, s, o, bx, by, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
+                                             kp.seed_hi, face, [&](double nx, double ny, const double* v) {
+                                                 record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
+                                             });
+            if (m) {
+                atomicAdd(&dc->e_emit[o], (unsigned long long)m);
+                if (diel) edp_inner_charge(kp, surf, obj, bm, bx, by, (double)m);
+            }
             continue;
         }
         if (!em) continue;
@@ -1460,7 +1496,8 @@ __global__ void __launch_bounds__(256) ion_emission_kernel(edp_hits h, const edp
         }
         const edp_born born_e = born->born_e;
         const int m = edp_emit_electrons(em, s, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
-                                         kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
+                                         kp.seed_hi, edp_wall_face(wall, xmax, ymax),
+                                         [&](double nx, double ny, const double* v) {
                                              record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
                                          });
         if (m) atomicAdd(&dc->e_emit[wall], (unsigned long long)m);

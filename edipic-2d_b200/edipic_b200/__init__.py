@@ -67,7 +67,7 @@ class Deck:
         self.n_max_vel, self.n_plasma_m3, self.max_t_cntr = nmv.value, npl.value, maxt.value
         # ion-induced electron emission of the walls' materials: {(wall, ion species): (yield, E_min, E_max, T)}
         self.ion_emission = {}
-        self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission
+        self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission; walls, then inner objects
         self.electron_emission = {}           # {wall: SeeParams} of the walls whose material emits electrons
         self.wall_injection = {}              # {wall: (N per step, model, T_normal, T_parallel, W_beam)}
         buf = (C.c_double * 4)()
@@ -84,6 +84,15 @@ class Deck:
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, wall, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(wall, s)] = tuple(buf)
+        # the inner objects' materials (objects 4 + n): ion reflection and ion-induced emission
+        for obj in range(4, 4 + self.params.n_inner):
+            if self.lib.edp_deck_ion_wall_model(self.handle, obj, C.byref(model)) == 0 and model.value:
+                self.ion_wall_model.append(model.value)
+            else:
+                self.ion_wall_model.append(0)
+            for s in range(1, self.params.n_ion_species + 1):
+                if self.lib.edp_deck_ion_emission(self.handle, obj, s, buf) == 0 and buf[0] > 0.0:
+                    self.ion_emission[(obj, s)] = tuple(buf)
         # time dependence of the metal objects' potentials (walls 0..3, inner objects 4 + n): those with a waveform,
         # an amplitude profile, or an oscillating inner object (walls' harmonic fields are in params already)
         self.potential_profiles = {}

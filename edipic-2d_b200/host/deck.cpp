@@ -117,9 +117,10 @@ struct edp_deck {
     int32_t n_max_vel = 0;
     int64_t max_t_cntr = 0;
     // ion-induced electron emission of the four walls per ion species: yield, E_min [eV], E_max [eV], T [eV]
-    double ii_ee[4][EDP_MAX_ION_SPECIES][4] = {};
-    int32_t ion_model[4] = {};   // ion-material interaction model of each wall's material
-    edp_see_params see[4] = {};  // electron-induced emission of each wall's material
+    // per object: the walls 0 below, 1 above, 2 left, 3 right, then inner object n at 4 + n
+    double ii_ee[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES][4] = {};
+    int32_t ion_model[EDP_N_HIT_COUNTERS] = {};   // ion-material interaction model of the object's material
+    edp_see_params see[EDP_N_HIT_COUNTERS] = {};  // electron-induced emission of the object's material
     double inject[4][5] = {};    // constant electron emission of each wall: N per step, model, T_n, T_p, W_beam [eV]
     // potentials of the metal objects over time (walls 0 below, 1 above, 2 left, 3 right; inner objects 4 + n)
     EdpPotentialProfile pot[4 + EDP_MAX_INNER];
@@ -338,10 +339,11 @@ int read_deck(const std::string& dir, edp_deck* d)
     // init_material_<NAME>.dat, PREPARE_WALL_MATERIALS pic2d_Materials.f90:1-200). Only the ion-material interaction
     // model is used: 2 = ion-induced electron emission with, per ion species, a constant coefficient between
     // E_min and E_max and the temperature of the emitted electrons. A missing file means default materials.
-    for (int w = 0; w < 4; ++w) {
-        if (side_obj[w] < 0) continue;
+    for (int w = 0; w < 4 + std::min<int>((int)nio, EDP_MAX_INNER); ++w) {
+        const int bo = w < 4 ? side_obj[w] : (int)nbo + (w - 4);   // the walls, then the inner objects
+        if (bo < 0) continue;
         char name[32];
-        snprintf(name, sizeof(name), "/init_bo_%02d.dat", side_obj[w] + 1);
+        snprintf(name, sizeof(name), "/init_bo_%02d.dat", bo + 1);
         Lines bf(dir + name);
         if (!bf.ok || !bf.next(L) || !bf.next(L)) continue;
         const std::string mat = (L + "      ").substr(6, 6);   // the six characters of the A6 field
@@ -620,14 +622,15 @@ int edp_deck_initial_plasma(const edp_deck* d, double* te, double* ne, double* t
 
 int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out)
 {
-    if (!d || !out || wall < 0 || wall > 3 || ion_species < 1 || ion_species > EDP_MAX_ION_SPECIES) return EDP_ERR_ARG;
+    if (!d || !out || wall < 0 || wall >= EDP_N_HIT_COUNTERS || ion_species < 1 || ion_species > EDP_MAX_ION_SPECIES)
+        return EDP_ERR_ARG;
     for (int k = 0; k < 4; ++k) out[k] = d->ii_ee[wall][ion_species - 1][k];
     return EDP_OK;
 }
 
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model)
 {
-    if (!d || !model || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    if (!d || !model || wall < 0 || wall >= EDP_N_HIT_COUNTERS) return EDP_ERR_ARG;
     *model = d->ion_model[wall];
     return EDP_OK;
 }

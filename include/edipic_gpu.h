@@ -241,13 +241,17 @@ int edp_set_cg_preconditioner(edp_ctx* ctx, int32_t kind);
  * PROCESS_ION_INDUCED_ELECTRON_EMISSION, pic2d_IonEmissions.f90:1-348): ions of ion_species (1-based) absorbed by
  * wall (0 below, 1 above, 2 left, 3 right) with energy in (emin_ev, emax_ev) emit on average `yield` electrons with
  * temperature t_emit_ev, within the ion's energy. The emitted electrons join the electron arrays at the end of the
- * step (edp_end_ion_cycle) and are counted per wall (edp_query_emission). yield 0 switches the wall off. */
+ * step (edp_end_ion_cycle) and are counted per wall (edp_query_emission). yield 0 switches the wall off. wall 4 + n
+ * is inner object n (DO_ION_COLL_WITH_INNER_OBJECT, pic2d_IonWallCollisions.f90:484-575): the electrons leave the
+ * side the ion's trajectory crossed first, 1e-6 outside it at the crossing point, and a dielectric object takes +1
+ * per emitted electron there besides the ion's charge. */
 int edp_set_ion_emission(edp_ctx* ctx, int32_t wall, int32_t ion_species, double yield, double emin_ev,
                          double emax_ev, double t_emit_ev);
 /* Ion-material model 1 (pic2d_Materials.f90:159-161): wall (0 below, 1 above, 2 left, 3 right) reflects every ion
  * specularly (INJECT_REFLECTED_ION, pic2d_IonEmissions.f90:374-492). The hit is counted, and the ion returns 1e-6
  * inside the wall with the normal velocity reversed, through the ion add list at the end of the step. Reflection
- * takes precedence over emission on the same wall. on = 0 restores absorption. */
+ * takes precedence over emission on the same wall. on = 0 restores absorption. wall 4 + n is inner object n: the
+ * ion returns 1e-6 outside the side it crossed first. */
 int edp_set_ion_reflection(edp_ctx* ctx, int32_t wall, int32_t on);
 /* Electron-induced electron emission of a domain wall (0 below, 1 above, 2 left, 3 right):
  * PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION (pic2d_SEEmission.f90:4-151) for every electron the wall absorbs
@@ -448,11 +452,12 @@ int edp_deck_read(const char* dir, edp_deck** out, edp_params* p, edp_tables* t)
 /* initial plasma of init_particles.dat: init_Te_eV, init_Ne_m3, init_Ti_eV(s), T_e_eV, N_max_vel ... */
 int edp_deck_initial_plasma(const edp_deck* d, double* init_te_ev, double* init_ne_m3, double* init_ti_ev,
                             double* t_e_ev, int32_t* n_max_vel, double* n_plasma_m3, int64_t* max_t_cntr);
-/* ion-induced electron emission of wall (0 below, 1 above, 2 left, 3 right) for ion_species (1-based), from the
- * wall's init_material_<NAME>.dat: out = {yield, E_min [eV], E_max [eV], T_emit [eV]}, all 0 when the wall's
- * material has no emission (pic2d_Materials.f90:150-188) */
+/* ion-induced electron emission of wall (0 below, 1 above, 2 left, 3 right; 4 + n inner object n) for ion_species
+ * (1-based), from the object's init_material_<NAME>.dat: out = {yield, E_min [eV], E_max [eV], T_emit [eV]}, all 0
+ * when the material has no emission (pic2d_Materials.f90:150-188) */
 int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, double* out);
-/* ion-material interaction model of wall's material (0 absorption, 1 specular reflection, 2 ion-induced emission) */
+/* ion-material interaction model of the object's material (0 absorption, 1 specular reflection, 2 ion-induced
+ * emission); objects as above */
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
 /* constant electron emission of wall (init_bo_NN.dat, pic2d_Setup.f90:86-95): out = {N_electron_constant_emit,
  * model_constant_emit, T_normal [eV], T_parallel [eV], beam energy [eV]} */

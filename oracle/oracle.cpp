@@ -174,6 +174,7 @@ void oracle_push_hits(const oracle_geom_t* g, const oracle_species_t* sp, const 
             if (X <= (double)g->ileft[n] || X >= (double)g->iright[n]) continue;
             if (Y <= (double)g->jbottom[n] || Y >= (double)g->jtop[n]) continue;
             hits[4 + n]++;
+            record(4 + n, X, Y, k);
             hit_inner = true;
             break;
         }
@@ -514,13 +515,15 @@ static double maxwell_inj_sample(const double* v, double u)
 // INJECT_ION_IMPACT_EXTRACTED_ELECTRON :91-348 for the domain walls (m > 0): position 1e-6 inside the wall,
 // normal component from the injection distribution, tangential ones Maxwellian, all times the conversion factor,
 // scaled down to the ion's remaining energy when above it.
-int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, double y, double vx, double vy,
-                            double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
-                            double* out, int32_t cap)
+// INJECT_ION_IMPACT_EXTRACTED_ELECTRON's placement by the struck surface: dirflag 1 (normal +x), 2 (-y), 3 (-x),
+// 4 (+y) at coordinate `at` (the domain wall's, or the inner object's side: xmax + 1e-6, ymin - 1e-6, xmin - 1e-6,
+// ymax + 1e-6 for m = -1, pic2d_IonEmissions.f90:232-330)
+int32_t oracle_ion_emission_face(const oracle_emit_t* em, int32_t obj, int32_t dirflag, double at, double x, double y,
+                                 double vx, double vy, double vz, uint32_t id, uint64_t seed, uint32_t step,
+                                 double* out, int32_t cap)
 {
-    if (!em->on[wall]) return 0;
-    x = std::min(std::max(x, 0.0), xmax);
-    y = std::min(std::max(y, 0.0), ymax);
+    if (!em->on[obj]) return 0;
+    const int wall = obj;
     double energy_inc = em->ms * (vx * vx + vy * vy + vz * vz);
     if (energy_inc <= em->emin[wall]) return 0;
     if (energy_inc >= em->emax[wall]) return 0;
@@ -538,14 +541,14 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
         double t1 = oracle_maxwell_sample(em->maxwell_v, uniform(w[1]));
         double t2 = oracle_maxwell_sample(em->maxwell_v, uniform(w[2]));
         double xn, yn, v[3];
-        if (wall == 2) {        // left, dirflag 1
-            xn = 1.0e-6; yn = y; v[0] = un; v[1] = t1; v[2] = t2;
-        } else if (wall == 3) { // right, dirflag 3
-            xn = xmax - 1.0e-6; yn = y; v[0] = -un; v[1] = t1; v[2] = t2;
-        } else if (wall == 0) { // below, dirflag 4
-            xn = x; yn = 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2;
-        } else {                // above, dirflag 2
-            xn = x; yn = ymax - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2;
+        if (dirflag == 1) {
+            xn = at + 1.0e-6; yn = y; v[0] = un; v[1] = t1; v[2] = t2;
+        } else if (dirflag == 3) {
+            xn = at - 1.0e-6; yn = y; v[0] = -un; v[1] = t1; v[2] = t2;
+        } else if (dirflag == 4) {
+            xn = x; yn = at + 1.0e-6; v[0] = t1; v[1] = un; v[2] = t2;
+        } else {
+            xn = x; yn = at - 1.0e-6; v[0] = t1; v[1] = -un; v[2] = t2;
         }
         const double f = em->fconv[wall];
         for (double& c : v) c *= f;
@@ -572,6 +575,19 @@ int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, dou
     philox_block(id, seed, step, stream, 0u, w0);
     if (uniform(w0[0]) < coef_total) inject();
     return n;
+}
+
+int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, double y, double vx, double vy,
+                            double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
+                            double* out, int32_t cap)
+{
+    if (!em->on[wall]) return 0;
+    x = std::min(std::max(x, 0.0), xmax);
+    y = std::min(std::max(y, 0.0), ymax);
+    // domain walls: left dirflag 1 at 0, right 3 at xmax, below 4 at 0, above 2 at ymax
+    const int32_t dirflag = wall == 2 ? 1 : wall == 3 ? 3 : wall == 0 ? 4 : 2;
+    const double at = wall == 3 ? xmax : wall == 1 ? ymax : 0.0;
+    return oracle_ion_emission_face(em, wall, dirflag, at, x, y, vx, vy, vz, id, seed, step, out, cap);
 }
 
 // Coeff_SEE_Classic pic2d_SEEmission.f90:1171-1208 (k is a REAL variable: 0.62 in single precision)
@@ -760,8 +776,8 @@ static bool cross_horizontal(double xorg, double yorg, double x, double y, doubl
     return true;
 }
 
-int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double x, double y, double vx, double vy,
-                         double xmul, double q, double* surf)
+int32_t oracle_inner_cross(const oracle_geom_t* g, double x, double y, double vx, double vy, double xmul,
+                           int32_t* m_out, double* xc_out, double* yc_out)
 {
     const double xorg = x - vx * xmul, yorg = y - vy * xmul;
     int n_do = -1, mcross = -1;
@@ -786,7 +802,15 @@ int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double
             ycross = yc;
             distorg = d;
         }
-    if (n_do < 0 || !(inner_eps[n_do] > 0.0)) return n_do;
+    *m_out = mcross;
+    *xc_out = xcross;
+    *yc_out = ycross;
+    return n_do;
+}
+
+void oracle_inner_charge(const oracle_geom_t* g, int32_t n_do, int32_t mcross, double xcross, double ycross, double q,
+                         double* surf)
+{
     // the outline numbering of DO_ELECTRON_COLL_WITH_INNER_OBJECT :582-640: position 1 = (ileft, jbottom), up the
     // left side, along the top, down the right side, back along the bottom
     const int il = g->ileft[n_do], ir = g->iright[n_do], jb = g->jbottom[n_do], jt = g->jtop[n_do];
@@ -828,7 +852,16 @@ int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double
     }
     surf[pos_node(i)] += q * dqi;
     surf[pos_node(ip1)] += q * dqip1;
-    return n_do;
+}
+
+int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double x, double y, double vx, double vy,
+                         double xmul, double q, double* surf)
+{
+    int32_t m = -1;
+    double xc = 0.0, yc = 0.0;
+    const int32_t n = oracle_inner_cross(g, x, y, vx, vy, xmul, &m, &xc, &yc);
+    if (n >= 0 && inner_eps[n] > 0.0) oracle_inner_charge(g, n, m, xc, yc, q, surf);
+    return n;
 }
 
 // INJECT_REFLECTED_ION pic2d_IonEmissions.f90:374-430 (m > 0, the domain walls)

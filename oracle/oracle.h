@@ -91,8 +91,8 @@ double oracle_maxwell_sample(const double* v, double u);
 /* one ion species at the four domain walls (0 below, 1 above, 2 left, 3 right), in code units
  * (pic2d_Materials.f90:165-188): yield between emin and emax (energies Ms v^2), fconv = sqrt(T_emit/T_e)/N_max_vel */
 typedef struct {
-    int32_t on[4];
-    double yield[4], emin[4], emax[4], fconv[4];
+    int32_t on[8];   /* the walls 0 below, 1 above, 2 left, 3 right, then inner object n at 4 + n */
+    double yield[8], emin[8], emax[8], fconv[8];
     double ms;
     uint32_t species;            /* 0-based ion species */
     const double* maxwell_v;     /* v[0..9000] */
@@ -108,6 +108,11 @@ typedef struct {
 int32_t oracle_ion_emission(const oracle_emit_t* em, int32_t wall, double x, double y, double vx, double vy,
                             double vz, uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax,
                             double* out, int32_t cap);
+/* the same for object `obj` (0..7) emitting from a surface given by INJECT_ION_IMPACT_EXTRACTED_ELECTRON's dirflag
+ * (1 normal +x, 2 -y, 3 -x, 4 +y) at coordinate `at`, from the point (x, y) on it (no clamping) */
+int32_t oracle_ion_emission_face(const oracle_emit_t* em, int32_t obj, int32_t dirflag, double at, double x, double y,
+                                 double vx, double vy, double vz, uint32_t id, uint64_t seed, uint32_t step,
+                                 double* out, int32_t cap);
 
 /* electron-induced emission of one domain wall, in code units (PREPARE_WALL_MATERIALS, pic2d_Materials.f90:84-244) */
 typedef struct {
@@ -247,6 +252,12 @@ int32_t oracle_cg_solve_eps(const oracle_geom_t* g, const double* rho_total, con
  * surf on the node grid. Returns the object, -1 when the trajectory crosses none. */
 int32_t oracle_inner_hit(const oracle_geom_t* g, const double* inner_eps, double x, double y, double vx, double vy,
                          double xmul, double q, double* surf);
+/* its two parts: the crossing (object returned; segment m 1 left, 2 top, 3 right, 4 bottom; crossing point) and the
+ * charge q on the outline nodes next to a crossing */
+int32_t oracle_inner_cross(const oracle_geom_t* g, double x, double y, double vx, double vy, double xmul,
+                           int32_t* m_out, double* xc_out, double* yc_out);
+void oracle_inner_charge(const oracle_geom_t* g, int32_t n_do, int32_t mcross, double xcross, double ycross, double q,
+                         double* surf);
 
 /* ---------------------------------------------------------------- whole cycle (CPU baseline) */
 typedef struct {

@@ -75,8 +75,8 @@ _lib = None
 
 
 class Emit(C.Structure):
-    _fields_ = [("on", C.c_int32 * 4), ("yld", C.c_double * 4), ("emin", C.c_double * 4),
-                ("emax", C.c_double * 4), ("fconv", C.c_double * 4), ("ms", C.c_double), ("species", C.c_uint32),
+    _fields_ = [("on", C.c_int32 * 8), ("yld", C.c_double * 8), ("emin", C.c_double * 8),
+                ("emax", C.c_double * 8), ("fconv", C.c_double * 8), ("ms", C.c_double), ("species", C.c_uint32),
                 ("maxwell_v", _D), ("maxwell_inj", _D)]
 
 
@@ -118,6 +118,13 @@ def lib():
                                   C.c_double, _D], C.c_int32),
             "oracle_ion_reflect": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _D], None),
+            "oracle_ion_emission_face": ([C.POINTER(Emit), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, _D,
+                                          C.c_int32], C.c_int32),
+            "oracle_inner_cross": ([C.POINTER(Geom), C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    _I32, _D, _D], C.c_int32),
+            "oracle_inner_charge": ([C.POINTER(Geom), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _D],
+                                    None),
             "oracle_deposit": ([C.POINTER(Geom), C.POINTER(Parts), C.c_double, _D], None),
             "oracle_fold_and_wall_scale": ([C.POINTER(Geom), _D], None),
             "oracle_collect_moments": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _D], None),
@@ -256,6 +263,58 @@ class IonEmission:
                                       ymax, dp(out), cap)
         assert n <= cap
         return out[:n]
+
+    def emit_face(self, obj, dirflag, at, x, y, vx, vy, vz, ident, seed, step, cap=64):
+        out = np.zeros((cap, 5))
+        n = lib().oracle_ion_emission_face(C.byref(self.s), int(obj), int(dirflag), at, x, y, vx, vy, vz, int(ident),
+                                           seed, step, dp(out), cap)
+        assert n <= cap
+        return out[:n]
+
+
+# the sides of an inner object (segments 1 left, 2 top, 3 right, 4 bottom) as INJECT_* dirflags and their coordinate
+def inner_face(g, n, m):
+    return {1: (3, g.ileft[n]), 2: (4, g.jtop[n]), 3: (1, g.iright[n]), 4: (2, g.jbottom[n])}[m]
+
+
+def inner_cross(g, x, y, vx, vy, xmul):
+    """(object or -1, segment, x, y) of the trajectory's first crossing of an inner object's outline"""
+    m, xc, yc = C.c_int32(), C.c_double(), C.c_double()
+    n = lib().oracle_inner_cross(C.byref(g), x, y, vx, vy, xmul, C.byref(m), C.byref(xc), C.byref(yc))
+    return n, m.value, xc.value, yc.value
+
+
+def inner_charge(g, n, m, xc, yc, q, surf):
+    lib().oracle_inner_charge(C.byref(g), int(n), int(m), xc, yc, q, dp(surf))
+
+
+def inner_ion_impact(g, em, reflect, dielectric, q, row, seed, step, xmul, surf):
+    """DO_ION_COLL_WITH_INNER_OBJECT (pic2d_IonWallCollisions.f90:484-575) for one absorbed ion (a push_hits row of
+    object 4 + n): (emitted electrons, reflected ion row or None). A reflecting object returns the ion 1e-6 outside
+    the side crossed first, its normal velocity reversed (INJECT_REFLECTED_ION, pic2d_IonEmissions.f90:374-492); a
+    dielectric takes the charge q, and +1 per emitted electron, at the crossing (surf updated)."""
+    _obj, x, y, vx, vy, vz, ident = row
+    n, m, xc, yc = inner_cross(g, x, y, vx, vy, xmul)
+    if n < 0:
+        return np.zeros((0, 5)), None
+    dirflag, at = inner_face(g, n, m)
+    if reflect.get(4 + n):
+        nx, ny, v = xc, yc, [vx, vy, vz]
+        if dirflag == 1:
+            nx, v[0] = at + 1e-6, -vx
+        elif dirflag == 3:
+            nx, v[0] = at - 1e-6, -vx
+        elif dirflag == 4:
+            ny, v[1] = at + 1e-6, -vy
+        else:
+            ny, v[1] = at - 1e-6, -vy
+        return np.zeros((0, 5)), np.array([nx, ny] + v)
+    if dielectric.get(n):
+        inner_charge(g, n, m, xc, yc, q, surf)
+    out = em.emit_face(4 + n, dirflag, at, xc, yc, vx, vy, vz, int(ident), seed, step)
+    if dielectric.get(n) and len(out):
+        inner_charge(g, n, m, xc, yc, float(len(out)), surf)
+    return out, None
 
 
 def vdf(parts, nbox, xmax, ymax, fvc, n_max_vel_s, n_vbins, two_d=False):

@@ -107,7 +107,8 @@ def test_wall_material_ion_emission(tmp_path):
     assert d.ion_emission == {(0, 1): (0.1, 0.0, 10000.0, 2.0), (1, 1): (0.1, 0.0, 10000.0, 2.0)}
     d = read_deck(decks.write_deck(str(tmp_path / "b"), "cfg2", ncx=64, ncy=32, ppc=4,
                                    ion_emission=(1.25, 5.0, 500.0, 1.5)))
-    assert d.ion_emission == {(w, 1): (1.25, 5.0, 500.0, 1.5) for w in range(4)}
+    # the four walls and the inner object (object 4) share the material METAL1
+    assert d.ion_emission == {(w, 1): (1.25, 5.0, 500.0, 1.5) for w in range(5)}
     d = read_deck(decks.write_deck(str(tmp_path / "c"), "cfg0", ncx=64, ncy=32, ppc=4))
     assert d.ion_emission == {}
 
@@ -129,7 +130,7 @@ def test_reference_ion_emission_deck():
 
 def test_wall_material_ion_reflection(tmp_path):
     d = read_deck(decks.write_deck(str(tmp_path / "r"), "cfg2", ncx=64, ncy=32, ppc=4, ion_reflection=True))
-    assert d.ion_wall_model == [1, 1, 1, 1]
+    assert d.ion_wall_model == [1, 1, 1, 1, 1]   # the walls, then the inner object
     assert d.ion_emission == {}
     d = read_deck(decks.write_deck(str(tmp_path / "e"), "cfg4", ncx=64, ncy=32, ppc=4))
     assert d.ion_wall_model == [2, 2, 0, 0]
