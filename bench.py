@@ -431,6 +431,7 @@ def run_ours(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             sort_s = tt.item()
         step_plain()
+    c0 = sim.counters()
     n0 = c0.n_particles[0] + c0.n_particles[1]
     launches0 = c0.kernel_launches
     if dist:

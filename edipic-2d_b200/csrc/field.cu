@@ -13,6 +13,8 @@
 #include <cmath>
 #include <vector>
 
+#include <chrono>
+
 #include "edp_internal.cuh"
 
 namespace {
@@ -621,8 +623,18 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     const unsigned gr = grid_nodes(kp);
     // the network was trained on the vacuum operator: with dielectric objects the previous potential starts the solve
     if (warm == EDP_WARM_LEARNED && kp.diel_mask) warm = EDP_WARM_PREVIOUS;
-    const bool learned = warm == EDP_WARM_LEARNED;
-    if (learned && !c->ws) return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
+    const bool asked = warm == EDP_WARM_LEARNED;
+    if (asked && !c->ws) return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
+    // the network runs unless the solves it started were slower on average than those from the previous potential
+    // (then only every 64th call re-tries it); the first call runs it, the second measures the previous start
+    bool learned = false;
+    if (asked) {
+        const int64_t k = c->ws_calls++;
+        if (c->ws_t_net < 0.0) learned = true;
+        else if (c->ws_t_prev < 0.0) learned = false;
+        else learned = c->ws_t_net < c->ws_t_prev || k % 64 == 0;
+    }
+    const auto t_start = std::chrono::steady_clock::now();
     ++c->launches;
     cg_setup<<<gr, 256, 0, c->stream>>>(g, c->rho_total, warm, c->phi, c->cg_kind, c->phi, c->cg_b, scal);
     ++c->launches;
@@ -690,6 +702,11 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     c->last_cg_iters = reported;
     c->last_cg_relres = rel;
     if (iters) *iters = reported;
+    if (asked) {   // the solve's wall time (it ends synchronised) into the running average of its start
+        const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+        double& avg = learned ? c->ws_t_net : c->ws_t_prev;
+        avg = avg < 0.0 ? t : 0.75 * avg + 0.25 * t;
+    }
     return done_at >= 0 ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
 }
 

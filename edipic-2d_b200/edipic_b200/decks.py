@@ -66,7 +66,8 @@ def _segments():
 def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None, seed=0, n_subcycles=1,
                collisions=True, rcx=True, bx=None, by=None, inner=None, wall_potentials=None, n_gas=3.2e21,
                ion_emission=None, ion_reflection=False, electron_emission=None, wall_injection=None, ez=0.0,
-               ions_sense_b=False, ions_sense_ez=False, oscillations=None, waveforms=None, amplitude_profiles=None):
+               ions_sense_b=False, ions_sense_ez=False, oscillations=None, waveforms=None, amplitude_profiles=None,
+               en_collisions=True):
     """ion_emission: (yield, E_min [eV], E_max [eV], T_emit [eV]) of ion-induced electron emission at every wall
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
     reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
@@ -77,7 +78,8 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
     Time dependence of metal objects, keyed by the reference's object number (1-based: the four boundary objects,
     then the inner objects): oscillations {n: (amplitude [V], frequency [MHz], phase [deg])} in init_bo_NN.dat;
     waveforms {n: (amplitude [V], frequency [Hz], [(fraction of the period, value), ...])} written as
-    init_bo_NN_waveform.dat; amplitude_profiles {n: [(time [ns], factor), ...]} as init_bo_NN_amplitude_profile.dat."""
+    init_bo_NN_waveform.dat; amplitude_profiles {n: [(time [ns], factor), ...]} as init_bo_NN_amplitude_profile.dat.
+    en_collisions=False keeps the neutral gas (for charge exchange) with its electron-neutral processes deactivated."""
     cfg = dict(CONFIGS[name])
     ncx = ncx or cfg["ncx"]
     ncy = ncy or cfg["ncy"]
@@ -277,7 +279,7 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
           f"        {3:2d}"]
     for k, ty in enumerate((10, 20, 30)):
         nl += [f"---dd--d--dd--d- collision #{k + 1} :: type / activated / ion species / save",
-               f"   {ty:2d}  {1:1d}  {(1 if ty == 30 else 0):2d}  {0:1d}"]
+               f"   {ty:2d}  {int(bool(en_collisions)):1d}  {(1 if ty == 30 else 0):2d}  {0:1d}"]
     nl += ["--------dd--- number of energy segments", f"        {len(segs):2d}",
            "--ddddd.ddd------------- minimal energy [eV]", f"  {e0:9.3f}"]
     for k, (up, st) in enumerate(segs):

@@ -55,7 +55,9 @@ enum edp_field {
 };
 /* initial guess of edp_field_cg. LEARNED: the previous potential plus the update the loaded network
  * (edp_warmstart_load) predicts from its residual against the new density; the previous potential is kept
- * whenever the prediction's residual is not smaller. */
+ * whenever the prediction's residual is not smaller. The network is also judged by wall time: once the solves it
+ * started were slower on average than solves from the previous potential, it runs only on every 64th LEARNED call
+ * (to re-measure), and the previous potential starts the others. */
 enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2, EDP_WARM_LEARNED = 3 };
 /* preconditioner of edp_field_cg: NONE is Jacobi, which is plain CG here because the operator's diagonal is
  * constant; MG (the default) is one symmetric geometric-multigrid V-cycle per iteration */

@@ -101,7 +101,7 @@ def test_sort_in_the_push_equals_the_separate_sort(tmp_path):
     before the push) and the separate sort pass at the end of the step give bit-identical particles, densities and
     wall hits over 14 steps with a sort every 3, with the unsorted tail of appended particles (ion-induced emission)
     and with particles absorbed in the sorting push."""
-    d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, collisions=False, rcx=True, bx=86.6, by=50.0,
+    d = small_deck(tmp_path, "periodic", ncx=64, ncy=48, en_collisions=False, rcx=True, bx=86.6, by=50.0,
                    ion_emission=(0.5, 0.0, 10000.0, 2.0))
     out = []
     for fused in (0, 1):
@@ -273,7 +273,7 @@ def test_push_kernels_give_identical_states(tmp_path, ion_emission):
     atomic appends, which no kernel fixes, so electrons are compared as sets of rows; their physics does not depend
     on the ids without electron-neutral collisions."""
     kw = dict(ion_emission=(0.5, 0.0, 10000.0, 2.0)) if ion_emission else {}
-    d = small_deck(tmp_path, "periodic", ncx=128, ncy=64, collisions=False, rcx=True, bx=86.6, by=50.0, **kw)
+    d = small_deck(tmp_path, "periodic", ncx=128, ncy=64, en_collisions=False, rcx=True, bx=86.6, by=50.0, **kw)
     out = []
     for kind in (0, 1, 2, 3):
         with Simulation(d, precision=PREC_MIXED, sort_every=5, seed=13) as sim:
