@@ -344,6 +344,67 @@ def poisson_leg(args, stream_of, warmup=10, steps=30, only=None):
     return out
 
 
+def warm_start_ceiling(args, stream_of, warmup=12, samples=3):
+    """How close a warm start must be to cut CG work: on the cfg2 geometry (512 x 512 cells, metal rectangle at
+    -100 V, 100 + 100 per cell) after `warmup` steps of the cycle, for `samples` later steps, the converged potential
+    phi* (relative residual 1e-13) and the previous one give starts phi_prev + (1 - eps) (phi* - phi_prev) of known
+    accuracy eps; CG iterations to 1e-8 from each, plain and multigrid-preconditioned. eps = 1 is the plain previous
+    start. With trained weights, the network's guess is placed on the same scale (its eps = |guess - phi*| /
+    |phi* - phi_prev| in the RMS over the nodes)."""
+    import numpy as np
+
+    from edipic_b200 import FIELD_PHI, PRECOND_MG, PRECOND_NONE, WARM_PREVIOUS, WARM_USER, Simulation, decks, warmstart
+    eps_list = [1.0, 0.3, 0.1, 0.03, 0.01, 3e-3, 1e-3, 3e-4, 1e-4]
+    out = {"workload": "cfg2 geometry, starts phi_prev + (1 - eps)(phi* - phi_prev), CG to 1e-8", "eps": eps_list}
+    theta = None
+    wpath = os.path.join(ROOT, "edipic-2d_b200", "weights", "warmstart_cfg3.npz")
+    if os.path.exists(wpath):
+        try:
+            theta = warmstart.load_blob(wpath)
+        except ValueError:
+            theta = None
+    iters = {"plain": [[] for _ in eps_list], "mg": [[] for _ in eps_list]}
+    net_eps = []
+    with tempfile.TemporaryDirectory() as tmp:
+        d = decks.write_deck(tmp, "cfg2")
+        with Simulation(d, sort_every=20, fuse_collisions=True, seed=2100) as sim:
+            if theta is not None:
+                sim.load_warm_start(theta)
+            sim.distribute_particles(100)
+            for k in range(warmup + samples):
+                sim.update_wall_potentials(k)
+                if k >= warmup:
+                    phi_prev = sim.field(FIELD_PHI)
+                    guess = sim.predict_warm_start()[0] if theta is not None else None
+                    sim.set_cg_preconditioner(PRECOND_MG)
+                    sim.solve_potential_with_cg(rtol=1e-13, max_it=200000, warm_start=WARM_PREVIOUS)
+                    phi_star = sim.field(FIELD_PHI)
+                    dphi = phi_star - phi_prev
+                    if guess is not None:
+                        net_eps.append(float(np.sqrt(np.mean((guess - phi_star) ** 2) / np.mean(dphi ** 2))))
+                    for name, pc in (("plain", PRECOND_NONE), ("mg", PRECOND_MG)):
+                        sim.set_cg_preconditioner(pc)
+                        for q, eps in enumerate(eps_list):
+                            sim.set_field(FIELD_PHI, phi_prev + (1.0 - eps) * dphi)
+                            iters[name][q].append(sim.solve_potential_with_cg(rtol=1e-8, max_it=200000,
+                                                                              warm_start=WARM_USER))
+                    sim.set_cg_preconditioner(PRECOND_MG)
+                    sim.set_field(FIELD_PHI, phi_star)
+                else:
+                    sim.solve_potential_with_cg(rtol=1e-8, max_it=200000, warm_start=WARM_PREVIOUS)
+                sim.advance_electrons()
+                sim.advance_ions()
+                sim.perform_electron_neutral_collisions()
+                sim.perform_resonant_charge_exchange()
+                sim.end_ion_cycle()
+    for name in ("plain", "mg"):
+        mean = [float(np.mean(v)) for v in iters[name]]
+        out[name] = {"cg_iterations": mean, "ratio_to_previous_start": [mean[0] / max(m, 1e-9) for m in mean]}
+    if net_eps:
+        out["network_eps"] = float(np.mean(net_eps))
+    return out
+
+
 def run_reference(args):
     """The reference arm: the reference's routines for the path on the host CPU. The reference's Fortran cannot be
     built in this image, so its CPU restatement (the oracle) runs, on all host threads, on the line's workload per
@@ -555,6 +616,7 @@ def run_ours(args):
             line["fp64_gpu_cycle"] = fp64_cycle_leg(args, stream_of)
             line["fp64_gpu_cycle"]["mixed_over_fp64"] = value / line["fp64_gpu_cycle"]["value"]
             line["poisson"] = poisson_leg(args, stream_of)
+            line["warm_start_ceiling"] = warm_start_ceiling(args, stream_of)
             line["network"] = network_leg()
             line["roofline_conv"] = {"bound": "tensor", "achieved": line["network"]["batch4"]["conv_tflops"],
                                      "peak": line["network"]["peak_tflops"], "unit": "TFLOP/s",
@@ -588,6 +650,7 @@ def main():
                     help="only the Poisson leg (cfg2 geometry), optionally only the named runs "
                          "(plain_mg, plain_nopc, learned_mg, learned_nopc)")
     ap.add_argument("--poisson-steps", type=int, default=30)
+    ap.add_argument("--warm-ceiling", action="store_true", help="only the warm-start accuracy leg (cfg2 geometry)")
     ap.add_argument("--sort-pass", action="store_true",
                     help="periodic sorts as a separate pass instead of inside the next push")
     ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2, 3],
@@ -611,6 +674,8 @@ def main():
             return torch.cuda.ExternalStream(ptr.value)
         print(json.dumps({"poisson": poisson_leg(args, stream_of, warmup=max(args.warmup, 3), steps=args.poisson_steps,
                                                  only=args.poisson_only or None)}))
+    elif args.warm_ceiling:
+        print(json.dumps({"warm_start_ceiling": warm_start_ceiling(args, None)}))
     elif args.impl == "reference":
         run_reference(args)
     else:

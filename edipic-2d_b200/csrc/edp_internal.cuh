@@ -230,7 +230,7 @@ struct edp_ctx {
     // (negative: none yet), and the learned-start calls so far: the network runs while it pays, and is re-tried on
     // every 64th call once it does not
     double ws_t_net = -1.0, ws_t_prev = -1.0;
-    int64_t ws_calls = 0;
+    int64_t ws_calls = 0, ws_runs = 0;
     int32_t last_cg_iters = 0;
     double last_cg_relres = 0.0;
     double last_cg_relres0 = 0.0;     // relative residual of the initial guess

@@ -626,13 +626,16 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     const bool asked = warm == EDP_WARM_LEARNED;
     if (asked && !c->ws) return edp_fail(c, EDP_ERR_STATE, "no warm-start network loaded");
     // the network runs unless the solves it started were slower on average than those from the previous potential
-    // (then only every 64th call re-tries it); the first call runs it, the second measures the previous start
+    // (then only every 64th call re-tries it); the first call (which may also capture the CG graphs) is not timed,
+    // the second times the network's start and the third the previous potential's
     bool learned = false;
+    int64_t k_call = -1;
     if (asked) {
-        const int64_t k = c->ws_calls++;
-        if (c->ws_t_net < 0.0) learned = true;
-        else if (c->ws_t_prev < 0.0) learned = false;
-        else learned = c->ws_t_net < c->ws_t_prev || k % 64 == 0;
+        k_call = c->ws_calls++;
+        if (k_call < 2) learned = true;
+        else if (k_call == 2) learned = false;
+        else learned = c->ws_t_net < c->ws_t_prev || k_call % 64 == 0;
+        if (learned) ++c->ws_runs;
     }
     const auto t_start = std::chrono::steady_clock::now();
     ++c->launches;
@@ -702,12 +705,22 @@ int edp_launch_cg(edp_ctx* c, double rtol, int max_it, int warm, int* iters)
     c->last_cg_iters = reported;
     c->last_cg_relres = rel;
     if (iters) *iters = reported;
-    if (asked) {   // the solve's wall time (it ends synchronised) into the running average of its start
+    if (asked && k_call > 0) {   // the solve's wall time (it ends synchronised) into the running average of its start
         const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
         double& avg = learned ? c->ws_t_net : c->ws_t_prev;
         avg = avg < 0.0 ? t : 0.75 * avg + 0.25 * t;
     }
     return done_at >= 0 ? EDP_OK : edp_fail(c, EDP_ERR_NOT_CONVERGED, "CG did not converge within max_it");
+}
+
+extern "C" int edp_warmstart_timing(edp_ctx* c, double* out)
+{
+    if (!c || !out) return EDP_ERR_ARG;
+    out[0] = c->ws_t_net;
+    out[1] = c->ws_t_prev;
+    out[2] = (double)c->ws_calls;
+    out[3] = (double)c->ws_runs;
+    return EDP_OK;
 }
 
 // The network's guess for the current density without solving: guess_out (node layout) and the residual norms of

@@ -55,9 +55,10 @@ enum edp_field {
 };
 /* initial guess of edp_field_cg. LEARNED: the previous potential plus the update the loaded network
  * (edp_warmstart_load) predicts from its residual against the new density; the previous potential is kept
- * whenever the prediction's residual is not smaller. The network is also judged by wall time: once the solves it
- * started were slower on average than solves from the previous potential, it runs only on every 64th LEARNED call
- * (to re-measure), and the previous potential starts the others. */
+ * whenever the prediction's residual is not smaller. The network is also judged by wall time: after the first
+ * three LEARNED calls (the network, the network timed, the previous potential timed), the network runs while the
+ * solves it started are faster on average than those from the previous potential, else only on every 64th call (to
+ * re-measure), and the previous potential starts the others. */
 enum edp_warm_start { EDP_WARM_ZERO = 0, EDP_WARM_PREVIOUS = 1, EDP_WARM_USER = 2, EDP_WARM_LEARNED = 3 };
 /* preconditioner of edp_field_cg: NONE is Jacobi, which is plain CG here because the operator's diagonal is
  * constant; MG (the default) is one symmetric geometric-multigrid V-cycle per iteration */
@@ -416,6 +417,9 @@ int edp_warmstart_load(edp_ctx* ctx, const float* blob, int64_t n_floats);
 /* the network's forward pass on the current residual: fills guess_out (reference node layout) with
  * phi_prev + predicted update; the residual norms of phi_prev and of the guess go to res_out[0..1] */
 int edp_warmstart_predict(edp_ctx* ctx, double* guess_out, double* res_out);
+/* the wall-time judge of EDP_WARM_LEARNED: out[4] = {average seconds of the solves the network started (negative:
+ * none yet), of those the previous potential started, LEARNED calls, calls on which the network ran} */
+int edp_warmstart_timing(edp_ctx* ctx, double* out);
 
 /* Kernels of the network, on caller-owned device memory and a caller stream (cudaStream_t), for training.
  * Activations are NHWC BF16, c1, c2 and c_out multiples of 32 (c2 may be 0: one input tensor). */
