@@ -13,6 +13,7 @@
 // One CTA keeps private copies of the histograms in shared memory when they fit (the 1D ones always do at the
 // reference's sizes) and adds them to the global counts once; otherwise it adds each count to global memory.
 #include <algorithm>
+#include <vector>
 
 #include "edp_internal.cuh"
 
@@ -171,5 +172,84 @@ extern "C" int edp_calculate_vdf(edp_ctx* c, int species, int32_t n_max_vel, int
     EDP_CUDA(c, cudaFreeAsync(buf, c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
     if (skipped) *skipped = (int64_t)sk;
+    return EDP_OK;
+}
+
+// ------------------------------------------------------------------------------------------ energy distribution
+// Counts of the particles of one species by kinetic energy in eV (the electron energy distribution of the long-run
+// comparison, the EEDF, without downloading the particles): E = (vx^2 + vy^2 + vz^2) * energy_factor_eV (* Ms for
+// ions, PERFORM_RESONANT_CHARGE_EXCHANGE's factor_eV), in the bins [edges[k], edges[k+1]); energies outside
+// [edges[0], edges[n_bins]) are not counted. Private shared-memory histograms per CTA, one global add per bin.
+namespace {
+
+constexpr int kMaxEnergyBins = 256;
+
+__global__ void __launch_bounds__(256) energy_hist_kernel(int precision, edp_species_mixed m, edp_species_fp64 d,
+                                                          const unsigned long long* n_slots, double factor,
+                                                          const double* edges, int n_bins,
+                                                          unsigned long long* counts)
+{
+    __shared__ double e[kMaxEnergyBins + 1];
+    __shared__ unsigned h[kMaxEnergyBins];
+    for (int k = threadIdx.x; k <= n_bins; k += blockDim.x) e[k] = edges[k];
+    for (int k = threadIdx.x; k < n_bins; k += blockDim.x) h[k] = 0u;
+    __syncthreads();
+    const int64_t n = (int64_t)*n_slots;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double vx, vy, vz;
+        if (precision == EDP_PREC_MIXED) {
+            if (m.cell[k] < 0) continue;
+            vx = m.vx[k];
+            vy = m.vy[k];
+            vz = m.vz[k];
+        } else {
+            if (d.x[k] < -1.0e29) continue;
+            vx = d.vx[k];
+            vy = d.vy[k];
+            vz = d.vz[k];
+        }
+        const double en = (vx * vx + vy * vy + vz * vz) * factor;
+        if (!(en >= e[0] && en < e[n_bins])) continue;
+        int lo = 0, hi = n_bins;   // e[lo] <= en < e[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (en >= e[mid]) lo = mid;
+            else hi = mid;
+        }
+        atomicAdd(&h[lo], 1u);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n_bins; k += blockDim.x)
+        if (h[k]) atomicAdd(&counts[k], (unsigned long long)h[k]);
+}
+
+}  // namespace
+
+extern "C" int edp_energy_histogram(edp_ctx* c, int species, int32_t n_bins, const double* edges_ev, int64_t* counts)
+{
+    if (!c || species < 0 || species >= c->nspec || n_bins < 1 || n_bins > kMaxEnergyBins || !edges_ev || !counts)
+        return edp_fail(c, EDP_ERR_ARG, "edp_energy_histogram");
+    for (int k = 0; k < n_bins; ++k)
+        if (!(edges_ev[k + 1] > edges_ev[k])) return edp_fail(c, EDP_ERR_ARG, "edp_energy_histogram: edges must rise");
+    if (!c->uploaded[species]) return edp_fail(c, EDP_ERR_STATE, "species not uploaded");
+    double factor = c->tab.energy_factor_eV;
+    if (species > 0) factor *= c->p.ion_mass_me[species - 1];
+    double* dev_edges = nullptr;
+    unsigned long long* dev_counts = nullptr;
+    EDP_CUDA(c, cudaMallocAsync(&dev_edges, (n_bins + 1) * sizeof(double), c->stream));
+    EDP_CUDA(c, cudaMallocAsync(&dev_counts, n_bins * sizeof(unsigned long long), c->stream));
+    EDP_CUDA(c, cudaMemcpyAsync(dev_edges, edges_ev, (n_bins + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    EDP_CUDA(c, cudaMemsetAsync(dev_counts, 0, n_bins * sizeof(unsigned long long), c->stream));
+    ++c->launches;
+    energy_hist_kernel<<<148 * 8, 256, 0, c->stream>>>(c->p.precision, c->pm[species], c->pd[species],
+                                                      &c->dc->n_slots[species], factor, dev_edges, n_bins, dev_counts);
+    EDP_CUDA(c, cudaGetLastError());
+    std::vector<unsigned long long> h(n_bins);
+    EDP_CUDA(c, cudaMemcpyAsync(h.data(), dev_counts, n_bins * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                c->stream));
+    EDP_CUDA(c, cudaFreeAsync(dev_edges, c->stream));
+    EDP_CUDA(c, cudaFreeAsync(dev_counts, c->stream));
+    EDP_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < n_bins; ++k) counts[k] = (int64_t)h[k];
     return EDP_OK;
 }

@@ -426,6 +426,14 @@ class Simulation:
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.ny_ref, self.nx_ref)
         self._check(self.lib.edp_set_field(self.ctx, which, _dp(a)), "edp_set_field")
 
+    def energy_histogram(self, species, edges_ev):
+        """Counts of the species' particles by kinetic energy in eV between the given edges (edp_energy_histogram)."""
+        e = np.ascontiguousarray(edges_ev, dtype=np.float64)
+        out = np.zeros(e.size - 1, dtype=np.int64)
+        self._check(self.lib.edp_energy_histogram(self.ctx, species, out.size, _dp(e),
+                                                  out.ctypes.data_as(C.POINTER(C.c_int64))), "edp_energy_histogram")
+        return out
+
     def moments(self, species):
         out = np.zeros(7)
         self._check(self.lib.edp_moments(self.ctx, species, _dp(out)), "edp_moments")

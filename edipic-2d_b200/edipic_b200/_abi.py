@@ -103,6 +103,7 @@ SIGNATURES = {
     "edp_get_stream": [_CTX, P(C.c_void_p)],
     "edp_sort_particles": [_CTX],
     "edp_warmstart_timing": [_CTX, _D],
+    "edp_energy_histogram": [_CTX, C.c_int, C.c_int32, _D, P(C.c_int64)],
     "edp_set_push_kernel": [_CTX, C.c_int32],
     "edp_set_sort_in_push": [_CTX, C.c_int32],
     "edp_upload_particles": [_CTX, C.c_int, C.c_int64, _D, _D, _D, _D, _D, _I32, _U32],

@@ -3,10 +3,12 @@ RF-driven periodic configuration (the cfg4 physics: top electrode at 200 V and 1
 Ar+-Ar charge exchange, ion-induced electron emission of yield 0.1 at both walls), over several seeds. Each run
 samples, after a burn-in, the electron energy distribution (EEDF), the electron and ion density profiles across the
 gap (COLLECT_*_MOMENTS averaged along x), the electron f(v_x) of CALCULATE_ELECTRON_VDF and the ion flux to each wall.
-`compare` turns the per-seed samples of the two precisions into z-scores: the difference of the means over seeds
-divided by its standard error.
+Two analyses of the per-seed samples: `compare_paired` for runs of the two precisions started from the same seed
+(the same initial plasma and random streams): the per-seed differences, their mean over seeds divided by its standard
+error, and the smallest bias the test could detect (3 standard errors, relative to the quantity); `compare` (Welch)
+for independent seeds.
 
-    python -m edipic_b200.longrun --seeds 8 --steps 3000 --cells 128 128 --ppc 100 --out longrun.json
+    python -m edipic_b200.longrun --seeds 8 --steps 12000 --cells 2048 512 --ppc 100 --out longrun.json
 """
 import argparse
 import json
@@ -26,7 +28,6 @@ def run(precision, seed, steps, cells=(64, 64), ppc=64, burn_in=None, sample_eve
     tmp = tempfile.mkdtemp(dir=workdir)
     d = decks.write_deck(os.path.join(tmp, "deck"), "cfg4", ncx=cells[0], ncy=cells[1], ppc=ppc, steps=steps)
     with Simulation(d, precision=precision, sort_every=20 if precision == PREC_MIXED else 0, seed=seed) as sim:
-        ef = sim.deck.tables.energy_factor_eV
         sim.distribute_particles(ppc)
         eedf = np.zeros(len(EEDF_EDGES_EV) - 1)
         ne = np.zeros(sim.ny_ref)
@@ -40,10 +41,10 @@ def run(precision, seed, steps, cells=(64, 64), ppc=64, burn_in=None, sample_eve
                 c = sim.counters()
                 hits0 = np.array(c.ion_hits[:2], dtype=np.float64)
             if t + 1 > burn_in and (t + 1 - burn_in) % sample_every == 0:
-                el = sim.download_particles(ELECTRONS)
-                e = (el["vx"] ** 2 + el["vy"] ** 2 + el["vz"] ** 2) * ef
-                h, _ = np.histogram(e, bins=EEDF_EDGES_EV)
-                eedf += h / max(len(e), 1)
+                # the EEDF on the device (edp_energy_histogram), normalised by all electrons
+                h = sim.energy_histogram(ELECTRONS, EEDF_EDGES_EV).astype(np.float64)
+                n_e = max(int(sim.counters().n_particles[0]), 1)
+                eedf += h / n_e
                 ne += sim.collect_moments(ELECTRONS)[0].mean(axis=1)
                 ni += sim.collect_moments(IONS)[0].mean(axis=1)
                 v1, _, _ = sim.calculate_vdf(ELECTRONS, (1, 1), 4, 10)
@@ -66,13 +67,38 @@ def zscores(a, b, floor=0.0):
     return (ma - mb)[keep] / se[keep]
 
 
+QUANTITIES = (("eedf", 1e-3), ("ne", 0.0), ("ni", 0.0), ("fvx", 1e-3), ("ion_flux", 0.0))
+
+
 def compare(mixed, fp64):
-    """z-scores of every quantity between the two lists of run() results."""
+    """Welch z-scores of every quantity between the two lists of run() results (independent seeds)."""
     out = {}
-    for k, floor in (("eedf", 1e-3), ("ne", 0.0), ("ni", 0.0), ("fvx", 1e-3), ("ion_flux", 0.0)):
+    for k, floor in QUANTITIES:
         z = zscores([r[k] for r in mixed], [r[k] for r in fp64], floor)
         out[k] = dict(n=int(z.size), max_abs_z=float(np.abs(z).max()) if z.size else 0.0,
                       mean_z2=float((z ** 2).mean()) if z.size else 0.0)
+    return out
+
+
+def compare_paired(mixed, fp64):
+    """Paired analysis of runs with the same seeds (mixed[s] and fp64[s] from the same initial plasma): per component
+    the per-seed differences d_s, z = mean(d) / (sd(d) / sqrt(seeds)); and the bias the test could detect, 3 sd(d) /
+    sqrt(seeds) relative to the component's mean, as its median over the components (the largest, the smallest)."""
+    out = {}
+    for k, floor in QUANTITIES:
+        a = np.asarray([r[k] for r in mixed], dtype=np.float64)
+        b = np.asarray([r[k] for r in fp64], dtype=np.float64)
+        d = a - b
+        m = 0.5 * (a.mean(0) + b.mean(0))
+        se = d.std(0, ddof=1) / np.sqrt(len(d))
+        keep = (np.abs(m) > floor) & (se > 0)
+        z = d.mean(0)[keep] / se[keep]
+        detect = 3.0 * se[keep] / np.abs(m[keep])
+        out[k] = dict(n=int(z.size), max_abs_z=float(np.abs(z).max()) if z.size else 0.0,
+                      mean_z2=float((z ** 2).mean()) if z.size else 0.0,
+                      detectable_bias_median=float(np.median(detect)) if z.size else 0.0,
+                      detectable_bias_max=float(detect.max()) if z.size else 0.0,
+                      detectable_bias_min=float(detect.min()) if z.size else 0.0)
     return out
 
 
@@ -82,13 +108,19 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--cells", type=int, nargs=2, default=(128, 128))
     ap.add_argument("--ppc", type=int, default=100)
+    ap.add_argument("--burn-in", type=int, default=None)
+    ap.add_argument("--sample-every", type=int, default=20)
     ap.add_argument("--out", default="longrun.json")
     args = ap.parse_args()
     res = {}
     for prec, name in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
-        res[name] = [run(prec, 1000 + s, args.steps, tuple(args.cells), args.ppc) for s in range(args.seeds)]
-    summary = dict(config=dict(seeds=args.seeds, steps=args.steps, cells=list(args.cells), ppc=args.ppc),
-                   z=compare(res["mixed"], res["fp64"]),
+        res[name] = [run(prec, 1000 + s, args.steps, tuple(args.cells), args.ppc, burn_in=args.burn_in,
+                         sample_every=args.sample_every) for s in range(args.seeds)]
+    summary = dict(config=dict(seeds=args.seeds, steps=args.steps, cells=list(args.cells), ppc=args.ppc,
+                               burn_in=args.burn_in or args.steps // 2, sample_every=args.sample_every,
+                               samples=res["mixed"][0]["samples"]),
+                   paired=compare_paired(res["mixed"], res["fp64"]),
+                   welch=compare(res["mixed"], res["fp64"]),
                    ion_flux=dict(mixed=np.mean([r["ion_flux"] for r in res["mixed"]], 0).tolist(),
                                  fp64=np.mean([r["ion_flux"] for r in res["fp64"]], 0).tolist()))
     json.dump(dict(summary=summary, runs=res), open(args.out, "w"))

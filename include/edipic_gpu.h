@@ -377,6 +377,10 @@ int edp_collect_moments(edp_ctx* ctx, int species, float* out);
  * number of particles outside the bins (may be NULL). */
 int edp_calculate_vdf(edp_ctx* ctx, int species, int32_t n_max_vel, int32_t nbox_x, int32_t nbox_y,
                       int32_t n_max_vel_s, int32_t n_vbins, int32_t* vdf1d, int32_t* vdf2d, int64_t* skipped);
+/* No counterpart in the reference (its EEDF comes from the snapshot VDFs of downloaded particles). Counts of the
+ * species' particles by kinetic energy in eV, E = |v|^2 energy_factor_eV (times Ms for ions), in the bins
+ * [edges_ev[k], edges_ev[k+1]), k < n_bins <= 256; energies outside the edges are not counted. Synchronises. */
+int edp_energy_histogram(edp_ctx* ctx, int species, int32_t n_bins, const double* edges_ev, int64_t* counts);
 /* kind selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS (:447-485) evaluated on the device for given
  * (energy, r) pairs: kind_out[k] = indx_coll (n_act+1 = null collision) */
 int edp_mcc_choose(edp_ctx* ctx, int64_t n, const double* energy_eV, const double* r, int32_t* kind_out);

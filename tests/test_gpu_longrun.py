@@ -1,11 +1,13 @@
 """Long-run statistics of the mixed-precision cycle against the plain FP64 device cycle on the RF-driven periodic
-configuration (cfg4 physics, reduced to 64 x 64 cells, 64 particles per cell and 400 steps), over 8 seeds: the EEDF,
-the electron and ion density profiles, the electron f(v_x) and the ion flux to each wall agree within their
-statistical errors (Welch z-scores of the differences of the means over seeds)."""
+configuration (cfg4 physics, reduced to 64 x 64 cells, 64 particles per cell and 400 steps), over 8 seeds: the EEDF
+(device energy histogram), the electron and ion density profiles, the electron f(v_x) and the ion flux to each wall
+agree within their statistical errors. Both precisions start from the same seed, so the per-seed differences are
+tested (paired z-scores); the test also states the smallest relative bias it could detect."""
+import numpy as np
 import pytest
 
-from edipic_b200 import PREC_FP64, PREC_MIXED
-from edipic_b200.longrun import compare, run
+from edipic_b200 import ELECTRONS, PREC_FP64, PREC_MIXED, Simulation, decks
+from edipic_b200.longrun import compare_paired, run
 
 
 @pytest.mark.gpu
@@ -13,9 +15,30 @@ def test_mixed_matches_fp64_statistically(tmp_path):
     kw = dict(steps=400, cells=(64, 64), ppc=64, burn_in=200, sample_every=20, workdir=str(tmp_path))
     mixed = [run(PREC_MIXED, 1000 + s, **kw) for s in range(8)]
     fp64 = [run(PREC_FP64, 1000 + s, **kw) for s in range(8)]
-    z = compare(mixed, fp64)
+    z = compare_paired(mixed, fp64)
     for k, v in z.items():
         assert v["n"] > 0, k
         assert v["max_abs_z"] < 6.0, (k, v)
-        assert v["mean_z2"] < 2.0, (k, v)
+        assert v["mean_z2"] < 2.5, (k, v)
+    # the pairing makes the comparison sensitive: biases of a few percent of the EEDF or the density would show
+    assert z["eedf"]["detectable_bias_median"] < 0.05 and z["ne"]["detectable_bias_median"] < 0.05, z
     assert min(r["ion_flux"][0] + r["ion_flux"][1] for r in mixed) > 0
+
+
+@pytest.mark.gpu
+def test_energy_histogram_matches_downloaded_particles(tmp_path):
+    """edp_energy_histogram against numpy on the downloaded electrons and ions (mixed and FP64)."""
+    d = decks.write_deck(str(tmp_path), "cfg4", ncx=64, ncy=32, ppc=16)
+    edges = np.concatenate([[0.0], np.geomspace(0.05, 100.0, 40)])
+    for prec in (PREC_MIXED, PREC_FP64):
+        with Simulation(d, precision=prec, seed=3) as sim:
+            sim.distribute_particles(16)
+            sim.step(3)
+            ef = sim.deck.tables.energy_factor_eV
+            for sp, f in ((ELECTRONS, ef), (1, ef * sim.params.ion_mass_me[0])):
+                got = sim.energy_histogram(sp, edges)
+                p = sim.download_particles(sp)
+                e = (p["vx"] ** 2 + p["vy"] ** 2 + p["vz"] ** 2) * f
+                want, _ = np.histogram(e[(e >= edges[0]) & (e < edges[-1])], bins=edges)
+                # a particle exactly on an edge may fall on either side by the last bit of the energy
+                assert np.abs(got - want).sum() <= 2 and got.sum() > 0.5 * len(e), (prec, sp)
