@@ -1092,7 +1092,7 @@ int edp_set_ion_emission(edp_ctx* c, int32_t wall, int32_t ion_species, double y
 int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp)
 {
     if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
-    if (!c || wall < 0 || wall > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission");
+    if (!c || wall < 0 || wall >= 4 + c->p.n_inner) return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission");
     if (sp && (sp->elastic_model < 0 || sp->elastic_model > 2 || sp->inelastic_model < 0 || sp->inelastic_model > 2 ||
                sp->true_model < 0 || sp->true_model > 2))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_electron_emission: model outside 0-2");
@@ -1146,8 +1146,11 @@ int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp
         if (w.m_tr == 2) lo = std::min(lo, w.cl_e0);
         w.lowest = lo;
     }
-    c->see_on = 0;
+    c->see_on = 0;   // the domain walls; inner objects by bit
     for (int q = 0; q < 4; ++q) c->see_on |= c->see_h->w[q].on;
+    c->kp.see_inner_mask = 0;
+    for (int n = 0; n < EDP_MAX_INNER; ++n)
+        if (c->see_h->w[4 + n].on) c->kp.see_inner_mask |= 1 << n;
     EDP_CUDA(c, cudaMemcpyAsync(c->see_dev, c->see_h, sizeof(edp_see_dev), cudaMemcpyHostToDevice, c->stream));
     EDP_CUDA(c, cudaStreamSynchronize(c->stream));
     return EDP_OK;
@@ -1220,7 +1223,7 @@ int edp_advance_electrons(edp_ctx* c)
     reset_step_counters_kernel<<<1, 1, 0, c->stream>>>(c->dc);
     TRY(zero_density(c, 0));
     TRY(edp_launch_push(c, 0, ion_step, fuse));
-    if (c->see_on || c->kp.diel_mask) TRY(edp_launch_electron_emission(c));
+    if (c->see_on || c->kp.diel_mask || c->kp.see_inner_mask) TRY(edp_launch_electron_emission(c));
     return finish_sync(c);
 }
 

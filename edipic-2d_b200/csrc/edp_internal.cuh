@@ -142,6 +142,7 @@ struct edp_kparams {
     uint32_t seed_lo, seed_hi;
     int32_t diel_mask;                        // bit n: inner object n is a dielectric
     int32_t ion_inner_mask;                   // bit n: inner object n emits electrons under ion impact or reflects ions
+    int32_t see_inner_mask;                   // bit n: inner object n emits electrons under electron impact
     int32_t strip;                            // 1: one x strip of a domain (edp_set_strip)
     int32_t strip_gl, strip_gr;               // ghost columns on its left / right; 0: that side is the domain's wall
     int32_t strip_x0, strip_ncx;              // global column of local column 0, columns of the whole domain
@@ -746,7 +747,7 @@ struct edp_see_wall {
     double fconv;    // factor_convert_seetrue_vinj = sqrt(T_see / T_e) / N_max_vel
 };
 struct edp_see_dev {
-    edp_see_wall w[4];
+    edp_see_wall w[EDP_N_HIT_COUNTERS];   // the domain walls, then inner object n at 4 + n
     const double* maxwell_v;
     const double* maxwell_inj;
     int rmax, rmax_inj;
@@ -789,17 +790,18 @@ __device__ inline double edp_see_true(const edp_see_wall& w, double e, double th
     return fmax(0.0, edp_see_classic(w, e, theta) * (1.0 - w.el_frac - w.in_frac));
 }
 
-// A reflected or backscattered electron of speed `speed` leaving wall `wall` at angle theta from the normal and
-// azimuth fi (INJECT_ELASTIC_REFLECTED_ELECTRON / INJECT_INELASTIC_BACKSCATTERED_ELECTRON for the domain walls)
-__device__ inline void edp_see_scatter(int wall, double x, double y, double xmax, double ymax, double speed,
-                                       double theta, double fi, double& nx, double& ny, double v[3])
+// A reflected or backscattered electron of speed `speed` leaving the surface `face` at angle theta from the normal
+// and azimuth fi (INJECT_ELASTIC_REFLECTED_ELECTRON / INJECT_INELASTIC_BACKSCATTERED_ELECTRON; a domain wall, or an
+// inner object's side with m = -1, 1e-6 outside it)
+__device__ inline void edp_see_scatter(edp_face face, double x, double y, double speed, double theta, double fi,
+                                       double& nx, double& ny, double v[3])
 {
     const double c = speed * cos(theta), s1 = speed * sin(theta) * sin(fi), s2 = speed * sin(theta) * cos(fi);
-    switch (wall) {
-    case 0: nx = x; ny = 1.0e-6; v[0] = s1; v[1] = c; v[2] = s2; break;
-    case 1: nx = x; ny = ymax - 1.0e-6; v[0] = s1; v[1] = -c; v[2] = s2; break;
-    case 2: nx = 1.0e-6; ny = y; v[0] = c; v[1] = s1; v[2] = s2; break;
-    default: nx = xmax - 1.0e-6; ny = y; v[0] = -c; v[1] = s1; v[2] = s2; break;
+    switch (face.dir) {
+    case 0: nx = x; ny = face.at + 1.0e-6; v[0] = s1; v[1] = c; v[2] = s2; break;
+    case 1: nx = x; ny = face.at - 1.0e-6; v[0] = s1; v[1] = -c; v[2] = s2; break;
+    case 2: nx = face.at + 1.0e-6; ny = y; v[0] = c; v[1] = s1; v[2] = s2; break;
+    default: nx = face.at - 1.0e-6; ny = y; v[0] = -c; v[1] = s1; v[2] = s2; break;
     }
 }
 
@@ -812,7 +814,7 @@ __device__ inline void edp_see_scatter(int wall, double x, double y, double xmax
 template <class Out>
 __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, double x, double y, double vx,
                                               double vy, double vz, uint32_t id, uint32_t step, uint32_t seed_lo,
-                                              uint32_t seed_hi, double xmax, double ymax, Out out)
+                                              uint32_t seed_hi, edp_face face, Out out)
 {
     const edp_see_wall& w = sd->w[wall];
     if (!w.on) return 0;
@@ -820,7 +822,7 @@ __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, d
     if (e <= w.lowest) return 0;
     const double v = sqrt(e);
     double theta = 0.0;
-    if (v != 0.0) theta = acos(fmin(1.0, fabs(wall >= 2 ? vx : vy) / v));
+    if (v != 0.0) theta = acos(fmin(1.0, fabs(face.dir >= 2 ? vx : vy) / v));
     const double ce = edp_see_elastic(w, e, theta), ci = edp_see_inelastic(w, e, theta);
     if (ce + ci > 1.0) return -1;
     double ct = edp_see_true(w, e, theta);
@@ -837,22 +839,22 @@ __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, d
             nv[0] = vx;
             nv[1] = vy;
             nv[2] = vz;
-            switch (wall) {
-            case 0: ny = 1.0e-6; nv[1] = -vy; break;
-            case 1: ny = ymax - 1.0e-6; nv[1] = -vy; break;
-            case 2: nx = 1.0e-6; nv[0] = -vx; break;
-            default: nx = xmax - 1.0e-6; nv[0] = -vx; break;
+            switch (face.dir) {
+            case 0: ny = face.at + 1.0e-6; nv[1] = -vy; break;
+            case 1: ny = face.at - 1.0e-6; nv[1] = -vy; break;
+            case 2: nx = face.at + 1.0e-6; nv[0] = -vx; break;
+            default: nx = face.at - 1.0e-6; nv[0] = -vx; break;
             }
         } else {
-            edp_see_scatter(wall, x, y, xmax, ymax, v, asin(fmin(edp_u01(b0[1]), 1.0)),
-                            6.283185307179 * edp_u01(b0[2]), nx, ny, nv);
+            edp_see_scatter(face, x, y, v, asin(fmin(edp_u01(b0[1]), 1.0)), 6.283185307179 * edp_u01(b0[2]), nx, ny,
+                            nv);
         }
         out(nx, ny, nv);
         return 1;
     }
     if (R > ce && R <= ce + ci) {   // INJECT_INELASTIC_BACKSCATTERED_ELECTRON :561-790
         const double th = asin(fmin(edp_u01(b0[1]), 1.0)), fi = 6.283185307179 * edp_u01(b0[2]);
-        edp_see_scatter(wall, x, y, xmax, ymax, v * sqrt(edp_u01(b0[3])), th, fi, nx, ny, nv);
+        edp_see_scatter(face, x, y, v * sqrt(edp_u01(b0[3])), th, fi, nx, ny, nv);
         out(nx, ny, nv);
         return 1;
     }
@@ -865,8 +867,8 @@ __device__ __noinline__ int edp_see_electrons(const edp_see_dev* sd, int wall, d
         uint32_t wb[4];
         if (energy <= 0.0) return;
         edp_philox(step, EDP_STREAM_SEE, 1u + (uint32_t)k, seed_hi, id, seed_lo, wb);
-        if (!edp_emit_thermal(sd->maxwell_v, sd->rmax, sd->maxwell_inj, sd->rmax_inj, edp_wall_face(wall, xmax, ymax),
-                              x, y, w.fconv, energy, wb, nx, ny, nv))
+        if (!edp_emit_thermal(sd->maxwell_v, sd->rmax, sd->maxwell_inj, sd->rmax_inj, face, x, y, w.fconv, energy, wb,
+                              nx, ny, nv))
             return;
         ++k;
         out(nx, ny, nv);

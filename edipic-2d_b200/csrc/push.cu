@@ -36,6 +36,7 @@ struct PushArgs {
     int64_t sel_cap;
     edp_hits hits;                 // wall-hit list of ion-induced electron emission
     int emit_on;
+    int need_id;                   // the ids are read: collisions, or hits recorded for emission
     // sort inside the push: every particle goes to slot cursor[key of its pre-push cell and source slot]++ of D
     edp_species_mixed D;
     unsigned long long* cursor;
@@ -234,7 +235,7 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
             atomicAdd(&s.cnt[4 + n], 1ull);
             // the crossing is found after the push: a dielectric's outline takes the charge, an ion-emitting or
             // ion-reflecting object answers the ion
-            if (((kp.diel_mask | (ION ? kp.ion_inner_mask : 0)) >> n) & 1)
+            if (((kp.diel_mask | (ION ? kp.ion_inner_mask : kp.see_inner_mask)) >> n) & 1)
                 record_hit(a.hits, a.dc, 4 + n, ION ? a.species - 1 : 0, (double)ni + (double)nx,
                            (double)nj + (double)ny, vx, vy, vz, id);
             return false;
@@ -356,15 +357,14 @@ __device__ __forceinline__ void vstore(void* p, int64_t g, const uint32_t* v)
 // IPT consecutive slots [IPT g, IPT g + IPT). WIN: a sorted chunk, always whole groups (tiles are padded to
 // multiples of EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted
 // to [lo, hi).
-template <bool ION, bool PER, bool ROT, bool WIN, int IPT, bool SCAT>
+template <bool ION, bool PER, bool ROT, bool WIN, int IPT>
 __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
                                            int64_t hi)
 {
-    const unsigned mask = __activemask();
     const int64_t base = g * IPT;
     const bool full = WIN || (base >= lo && base + IPT <= hi);
     const bool windowed = WIN;
-    int c[IPT], cpre[IPT], tag[IPT] = {};
+    int c[IPT];
     float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
     uint32_t id[IPT];
     bool sel[IPT];
@@ -375,13 +375,12 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
         vload<IPT>(a.P.vx, g, reinterpret_cast<uint32_t*>(vx));
         vload<IPT>(a.P.vy, g, reinterpret_cast<uint32_t*>(vy));
         vload<IPT>(a.P.vz, g, reinterpret_cast<uint32_t*>(vz));
-        if (a.do_coll || a.emit_on || SCAT) {
+        if (a.need_id) {
             vload<IPT>(a.P.id, g, id);
         } else {
 #pragma unroll
             for (int e = 0; e < IPT; ++e) id[e] = 0u;
         }
-        if constexpr (SCAT) vload<IPT>(a.P.tag, g, reinterpret_cast<uint32_t*>(tag));
     } else {
 #pragma unroll
         for (int e = 0; e < IPT; ++e) {
@@ -394,14 +393,12 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
             vy[e] = ok ? a.P.vy[k] : 0.f;
             vz[e] = ok ? a.P.vz[k] : 0.f;
             id[e] = ok ? a.P.id[k] : 0u;
-            if constexpr (SCAT) tag[e] = ok ? a.P.tag[k] : 0;
         }
     }
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
     for (int e = 0; e < IPT; ++e) {
-        cpre[e] = c[e];
         sel[e] = false;
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
@@ -412,37 +409,6 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
         }
     }
     dep_flush(s, acc);
-    if constexpr (SCAT) {
-        // each live source slot takes the next slot of its key's run in D (warp-aggregated cursor updates); a
-        // particle absorbed now leaves a dead slot there, compacted by the next sort
-        const int lane = threadIdx.x & 31;
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) {
-            const uint32_t key = cpre[e] >= 0 ? edp_tile_key(cpre[e], base + e, a.ntx) : 0xFFFFFFFFu;
-            const unsigned peers = __match_any_sync(mask, key);
-            const int leader = __ffs(peers) - 1;
-            unsigned long long b0 = 0;
-            if (key != 0xFFFFFFFFu && lane == leader) b0 = atomicAdd(&a.cursor[key], (unsigned long long)__popc(peers));
-            b0 = __shfl_sync(mask, b0, leader);
-            if (key == 0xFFFFFFFFu) continue;
-            const unsigned long long pos = b0 + __popc(peers & ((1u << lane) - 1u));
-            if ((int64_t)pos >= a.cap) {
-                atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
-                continue;
-            }
-            a.D.cell[pos] = c[e];
-            if (c[e] < 0) continue;
-            a.D.ox[pos] = ox[e];
-            a.D.oy[pos] = oy[e];
-            a.D.vx[pos] = vx[e];
-            a.D.vy[pos] = vy[e];
-            a.D.vz[pos] = vz[e];
-            a.D.id[pos] = id[e];
-            a.D.tag[pos] = tag[e];
-            if (sel[e]) select_slot(a, s, (uint32_t)pos);
-        }
-        return;
-    }
 #pragma unroll
     for (int e = 0; e < IPT; ++e)
         if (sel[e]) select_slot(a, s, (uint32_t)(base + e));
@@ -466,6 +432,76 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
             a.P.vy[k] = vy[e];
             a.P.vz[k] = vz[e];
         }
+    }
+}
+
+// The push of a sort step over a block of 128 slots [b, b + 128) taken by one warp, lane l holding slots
+// b + 32 e + l (e < 4): the loads are coalesced per element, and the 32 lanes of an element are 32 consecutive source
+// slots, which share their sort key run, so each particle's write to its sorted slot in a.D (the cursor of the key of
+// its cell before the push and its source slot) is a coalesced 128-byte run per column. A particle absorbed now
+// leaves a dead slot, compacted by the next sort. Called warp-uniformly (every lane, every block).
+template <bool ION, bool PER, bool ROT, bool WIN>
+__device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t b,
+                                                   int64_t lo, int64_t hi)
+{
+    const int lane = threadIdx.x & 31;
+    int c[4], cpre[4], tag[4];
+    float ox[4], oy[4], vx[4], vy[4], vz[4];
+    uint32_t id[4];
+    bool sel[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int64_t k = b + 32 * e + lane;
+        const bool ok = k >= lo && k < hi;
+        c[e] = ok ? __ldcs(a.P.cell + k) : -1;
+        ox[e] = ok ? __ldcs(a.P.ox + k) : 0.f;
+        oy[e] = ok ? __ldcs(a.P.oy + k) : 0.f;
+        vx[e] = ok ? __ldcs(a.P.vx + k) : 0.f;
+        vy[e] = ok ? __ldcs(a.P.vy + k) : 0.f;
+        vz[e] = ok ? __ldcs(a.P.vz + k) : 0.f;
+        id[e] = ok ? __ldcs(a.P.id + k) : 0u;
+        tag[e] = ok ? __ldcs(a.P.tag + k) : 0;
+    }
+    DepAcc acc;
+    acc.b = -1;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        cpre[e] = c[e];
+        sel[e] = false;
+        if (c[e] < 0) continue;
+        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                                     sel[e])) {
+            c[e] = -1;
+            sel[e] = false;
+            atomicAdd(&s.cnt[17], 1ull);
+        }
+    }
+    dep_flush(s, acc);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const uint32_t key = cpre[e] >= 0 ? edp_tile_key(cpre[e], b + 32 * e + lane, a.ntx) : 0xFFFFFFFFu;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+        const int leader = __ffs(peers) - 1;
+        unsigned long long b0 = 0;
+        if (key != 0xFFFFFFFFu && lane == leader) b0 = atomicAdd(&a.cursor[key], (unsigned long long)__popc(peers));
+        b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
+        if (key == 0xFFFFFFFFu) continue;
+        const unsigned long long pos = b0 + __popc(peers & ((1u << lane) - 1u));
+        if ((int64_t)pos >= a.cap) {
+            atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
+            continue;
+        }
+        __stcs(a.D.cell + pos, c[e]);
+        if (c[e] < 0) continue;
+        __stcs(a.D.ox + pos, ox[e]);
+        __stcs(a.D.oy + pos, oy[e]);
+        __stcs(a.D.vx + pos, vx[e]);
+        __stcs(a.D.vy + pos, vy[e]);
+        __stcs(a.D.vz + pos, vz[e]);
+        __stcs(a.D.id + pos, id[e]);
+        __stcs(a.D.tag + pos, tag[e]);
+        if (sel[e]) select_slot(a, s, (uint32_t)pos);
     }
 }
 
@@ -500,14 +536,25 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed
         hi = (int64_t)*a.n_slots;
     }
     __syncthreads();
-    if (windowed) {
+    if constexpr (SCAT) {
+        const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        const int64_t b0 = lo & ~(int64_t)127;   // blocks aligned to 128 slots: a lane's key run is its 32-slot group
+        if (windowed) {
+            for (int64_t b = b0 + 128 * warp; b < hi; b += 128 * nw)
+                push_block_scatter<ION, PER, ROT, true>(a, s, wx0, wy0, b, lo, hi);
+        } else {
+            const int64_t t = blockIdx.x - a.n_chunks;
+            for (int64_t b = b0 + 128 * (t * nw + warp); b < hi; b += 128 * nw * a.tail_ctas)
+                push_block_scatter<ION, PER, ROT, false>(a, s, 0, 0, b, lo, hi);
+        }
+    } else if (windowed) {
         for (int64_t g = lo / IPT + threadIdx.x; g * IPT < hi; g += blockDim.x)
-            push_group<ION, PER, ROT, true, IPT, SCAT>(a, s, wx0, wy0, g, lo, hi);
+            push_group<ION, PER, ROT, true, IPT>(a, s, wx0, wy0, g, lo, hi);
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
         int64_t g0 = lo / IPT;
         for (int64_t g = g0 + t * blockDim.x + threadIdx.x; g * IPT < hi; g += a.tail_ctas * blockDim.x)
-            push_group<ION, PER, ROT, false, IPT, SCAT>(a, s, 0, 0, g, lo, hi);
+            push_group<ION, PER, ROT, false, IPT>(a, s, 0, 0, g, lo, hi);
     }
     __syncthreads();
     if (windowed) {
@@ -660,7 +707,7 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 3 : 4) push_strea
     __shared__ __align__(8) uint64_t full[NST];
     int fail = 0;
     const int tid = threadIdx.x;
-    const int ncols = (a.do_coll || a.emit_on) ? EDP_STREAM_COLS : EDP_STREAM_COLS - 1;
+    const int ncols = a.need_id ? EDP_STREAM_COLS : EDP_STREAM_COLS - 1;
     const uint32_t stage0 = push_smem_u32(stage_mem);
     if (tid < 32) s.cnt[tid] = 0ull;
     if (tid == 0) {
@@ -968,7 +1015,8 @@ __global__ void __launch_bounds__(256) push_fp64_kernel(PushArgs64 a)
             atomicAdd(&cnt[obj], 1ull);
             atomicAdd(&cnt[17], 1ull);
             if ((a.emit_on && obj < 4) ||
-                (obj >= 4 && (((kp.diel_mask | (a.is_ion ? kp.ion_inner_mask : 0)) >> (obj - 4)) & 1)))
+                (obj >= 4 &&
+                 (((kp.diel_mask | (a.is_ion ? kp.ion_inner_mask : kp.see_inner_mask)) >> (obj - 4)) & 1)))
                 record_hit(a.hits, a.dc, obj, a.is_ion ? a.species - 1 : 0, X, Y, vx, vy, vz, a.P.id[k]);
             continue;
         }
@@ -1341,6 +1389,7 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.sel_cap = c->sel_cap;
         a.hits = c->hits;
         a.emit_on = is_ion ? c->emit_on : c->see_on;
+        a.need_id = a.do_coll || a.emit_on || (is_ion ? c->kp.ion_inner_mask : c->kp.see_inner_mask) != 0;
         if (do_mcc) EDP_CUDA(c, cudaMemsetAsync(c->sel_count, 0, sizeof(unsigned long long), c->stream));
         int64_t tail = c->host_slots[sp] - c->sorted_end[sp];
         if (tail < 0) tail = 0;
@@ -1514,14 +1563,37 @@ __global__ void __launch_bounds__(256) electron_emission_kernel(edp_hits h, cons
     const double xmax = (double)kp.ncx, ymax = (double)kp.ncy;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const int wall = h.ws[k] & 255;
-        if (wall >= 4) {   // a dielectric inner object: its outline gets the electron's charge
-            edp_inner_hit(kp, surf, h.x[k], h.y[k], h.vx[k], h.vy[k], 1.0, -1.0);
+        if (wall >= 4) {
+            // an inner object (DO_ELECTRON_COLL_WITH_INNER_OBJECT, pic2d_ElectronWallCollisions.f90:561-645): the side
+            // the trajectory crossed first; a dielectric's outline takes the electron's charge there, an emitting
+            // object emits from the crossing (PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION with m = -1), and a dielectric
+            // takes +1 per electron leaving it
+            int bm;
+            double bx, by;
+            const int obj = edp_inner_cross(kp, h.x[k], h.y[k], h.vx[k], h.vy[k], 1.0, bm, bx, by);
+            if (obj < 0) continue;
+            const bool diel = (kp.diel_mask >> obj) & 1;
+            if (diel) edp_inner_charge(kp, surf, obj, bm, bx, by, -1.0);
+            if (!sd) continue;
+            const int o = 4 + obj;
+            const int m = edp_see_electrons(sd, o, bx, by, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
+                                            kp.seed_hi, edp_inner_face(kp, obj, bm),
+                                            [&](double nx, double ny, const double* v) {
+                                                record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
+                                            });
+            if (m < 0) {
+                atomicOr(&dc->error_flags, EDP_EFLAG_SEE_MODEL);
+            } else if (m) {
+                atomicAdd(&dc->e_emit[o], (unsigned long long)m);
+                if (diel) edp_inner_charge(kp, surf, obj, bm, bx, by, (double)m);
+            }
             continue;
         }
         if (!sd) continue;
         const double x = fmin(fmax(h.x[k], 0.0), xmax), y = fmin(fmax(h.y[k], 0.0), ymax);
         const int m = edp_see_electrons(sd, wall, x, y, h.vx[k], h.vy[k], h.vz[k], h.id[k], step, kp.seed_lo,
-                                        kp.seed_hi, xmax, ymax, [&](double nx, double ny, const double* v) {
+                                        kp.seed_hi, edp_wall_face(wall, xmax, ymax),
+                                        [&](double nx, double ny, const double* v) {
                                             record_born(born_e, &dc->born_e_count, &dc->error_flags, nx, ny, v);
                                         });
         if (m < 0) atomicOr(&dc->error_flags, EDP_EFLAG_SEE_MODEL);
@@ -1532,7 +1604,8 @@ __global__ void __launch_bounds__(256) electron_emission_kernel(edp_hits h, cons
 int edp_launch_electron_emission(edp_ctx* c)
 {
     ++c->launches;
-    electron_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, c->see_on ? c->see_dev : nullptr, c->born_e,
+    const bool any_see = c->see_on || c->kp.see_inner_mask;
+    electron_emission_kernel<<<148 * 2, 256, 0, c->stream>>>(c->hits, any_see ? c->see_dev : nullptr, c->born_e,
                                                            c->dc, c->kp, (uint32_t)c->t_cntr, c->surf);
     EDP_CUDA(c, cudaGetLastError());
     EDP_CUDA(c, cudaMemsetAsync(&c->dc->hit_count, 0, sizeof(unsigned long long), c->stream));

@@ -90,6 +90,9 @@ class Deck:
                 self.ion_wall_model.append(model.value)
             else:
                 self.ion_wall_model.append(0)
+            see, on = _abi.SeeParams(), C.c_int32()
+            if self.lib.edp_deck_electron_emission(self.handle, obj, C.byref(see), C.byref(on)) == 0 and on.value:
+                self.electron_emission[obj] = see
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, obj, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(obj, s)] = tuple(buf)

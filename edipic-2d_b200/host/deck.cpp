@@ -637,7 +637,7 @@ int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model)
 
 int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled)
 {
-    if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    if (!d || !out || wall < 0 || wall >= EDP_N_HIT_COUNTERS) return EDP_ERR_ARG;
     *out = d->see[wall];
     if (enabled) *enabled = (out->elastic_model + out->inelastic_model + out->true_model) > 0;
     return EDP_OK;

@@ -260,7 +260,10 @@ int edp_set_ion_reflection(edp_ctx* ctx, int32_t wall, int32_t on);
  * PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION (pic2d_SEEmission.f90:4-151) for every electron the wall absorbs
  * (PROCESS_ELECTRON_COLL_WITH_BOUNDARY_*, pic2d_ElectronWallCollisions.f90:3-287): elastic reflection, inelastic
  * backscattering or true secondaries. The emitted electrons join at the end of the step and are counted with
- * edp_query_emission. params = NULL, or all three models 0, switches the wall off. Returns EDP_ERR_ARG when a
+ * edp_query_emission. wall 4 + n is inner object n (DO_ELECTRON_COLL_WITH_INNER_OBJECT,
+ * pic2d_ElectronWallCollisions.f90:561-645): the electrons leave the side crossed first, 1e-6 outside it at the
+ * crossing, and a dielectric object takes +1 per electron leaving it besides the absorbed electron's -1.
+ * params = NULL, or all three models 0, switches the wall off. Returns EDP_ERR_ARG when a
  * model number is outside 0-2. A wall whose elastic and inelastic coefficients add up to more than 1 at some
  * impact sets the model error (EDP_ERR_STATE from edp_query_counters), where the reference stops. */
 int edp_set_electron_emission(edp_ctx* ctx, int32_t wall, const edp_see_params* params);
@@ -472,7 +475,8 @@ int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
 /* constant electron emission of wall (init_bo_NN.dat, pic2d_Setup.f90:86-95): out = {N_electron_constant_emit,
  * model_constant_emit, T_normal [eV], T_parallel [eV], beam energy [eV]} */
 int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out);
-/* electron-induced emission parameters of wall's material; *enabled = 1 when any of the three models is on */
+/* electron-induced emission parameters of the object's material (walls 0-3, inner objects 4 + n); *enabled = 1 when any
+ * of the three models is on */
 int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* out, int32_t* enabled);
 /* the time dependence of metal object `object` (0..3 walls, 4 + n inner objects) as the deck sets it up,
  * in edp_set_potential_profile's layout: counts always, arrays when not NULL (call once for the counts) */

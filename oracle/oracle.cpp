@@ -632,16 +632,17 @@ static double see_true(const oracle_see_t* w, double e, double th)
     return c < 0.0 ? 0.0 : c;
 }
 
-int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
-                   uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap)
+// the electron leaves the surface given by dirflag (1 normal +x, 2 -y, 3 -x, 4 +y) at coordinate `at`, 1e-6 outside
+// it: a domain wall (m > 0) or an inner object's side (m = -1, pic2d_SEEmission.f90:388-544)
+int32_t oracle_see_face(const oracle_see_t* w, int32_t dirflag, double at, double x, double y, double vx, double vy,
+                        double vz, uint32_t id, uint64_t seed, uint32_t step, double* out, int32_t cap)
 {
     const uint32_t stream = 0x53450000u;
-    x = std::min(std::max(x, 0.0), xmax);
-    y = std::min(std::max(y, 0.0), ymax);
+    const bool xnormal = dirflag == 1 || dirflag == 3;
     double energy_inc = vx * vx + vy * vy + vz * vz;
     if (energy_inc <= w->lowest) return 0;
     double v = std::sqrt(energy_inc), theta_inc = 0.0;
-    if (v != 0.0) theta_inc = std::acos(std::min(1.0, std::fabs(wall >= 2 ? vx : vy) / v));
+    if (v != 0.0) theta_inc = std::acos(std::min(1.0, std::fabs(xnormal ? vx : vy) / v));
     double ce = see_elastic(w, energy_inc, theta_inc), ci = see_inelastic(w, energy_inc, theta_inc);
     if (ce + ci > 1.0) return -1;
     double ct = see_true(w, energy_inc, theta_inc), ctot = ce + ci + ct;
@@ -661,17 +662,17 @@ int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, doub
     auto scatter = [&](double speed, double theta, double fi) {
         double c = speed * std::cos(theta), s1 = speed * std::sin(theta) * std::sin(fi),
                s2 = speed * std::sin(theta) * std::cos(fi);
-        if (wall == 2) put(1.0e-6, y, c, s1, s2);
-        else if (wall == 1) put(x, ymax - 1.0e-6, s1, -c, s2);
-        else if (wall == 3) put(xmax - 1.0e-6, y, -c, s1, s2);
-        else put(x, 1.0e-6, s1, c, s2);
+        if (dirflag == 1) put(at + 1.0e-6, y, c, s1, s2);
+        else if (dirflag == 2) put(x, at - 1.0e-6, s1, -c, s2);
+        else if (dirflag == 3) put(at - 1.0e-6, y, -c, s1, s2);
+        else put(x, at + 1.0e-6, s1, c, s2);
     };
     if (R <= ce) {   // INJECT_ELASTIC_REFLECTED_ELECTRON :155-557
         if (!w->refl_random) {
-            if (wall == 2) put(1.0e-6, y, -vx, vy, vz);
-            else if (wall == 1) put(x, ymax - 1.0e-6, vx, -vy, vz);
-            else if (wall == 3) put(xmax - 1.0e-6, y, -vx, vy, vz);
-            else put(x, 1.0e-6, vx, -vy, vz);
+            if (dirflag == 1) put(at + 1.0e-6, y, -vx, vy, vz);
+            else if (dirflag == 2) put(x, at - 1.0e-6, vx, -vy, vz);
+            else if (dirflag == 3) put(at - 1.0e-6, y, -vx, vy, vz);
+            else put(x, at + 1.0e-6, vx, -vy, vz);
         } else {
             scatter(v, std::asin(std::min(uniform(b0[1]), 1.0)), 6.283185307179 * uniform(b0[2]));
         }
@@ -694,10 +695,10 @@ int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, doub
         double t1 = oracle_maxwell_sample(w->maxwell_v, uniform(wb[1]));
         double t2 = oracle_maxwell_sample(w->maxwell_v, uniform(wb[2]));
         double xn, yn, nv[3];
-        if (wall == 2) { xn = 1.0e-6; yn = y; nv[0] = un; nv[1] = t1; nv[2] = t2; }
-        else if (wall == 1) { xn = x; yn = ymax - 1.0e-6; nv[0] = t1; nv[1] = -un; nv[2] = t2; }
-        else if (wall == 3) { xn = xmax - 1.0e-6; yn = y; nv[0] = -un; nv[1] = t1; nv[2] = t2; }
-        else { xn = x; yn = 1.0e-6; nv[0] = t1; nv[1] = un; nv[2] = t2; }
+        if (dirflag == 1) { xn = at + 1.0e-6; yn = y; nv[0] = un; nv[1] = t1; nv[2] = t2; }
+        else if (dirflag == 2) { xn = x; yn = at - 1.0e-6; nv[0] = t1; nv[1] = -un; nv[2] = t2; }
+        else if (dirflag == 3) { xn = at - 1.0e-6; yn = y; nv[0] = -un; nv[1] = t1; nv[2] = t2; }
+        else { xn = x; yn = at + 1.0e-6; nv[0] = t1; nv[1] = un; nv[2] = t2; }
         for (double& c : nv) c *= w->fconv;
         double energy_new = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
         if (energy_new > energy_inc) {
@@ -720,6 +721,16 @@ int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, doub
     }
     if (uniform(b0[3]) < ct) inject();
     return n;
+}
+
+int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
+                   uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap)
+{
+    x = std::min(std::max(x, 0.0), xmax);
+    y = std::min(std::max(y, 0.0), ymax);
+    const int32_t dirflag = wall == 2 ? 1 : wall == 3 ? 3 : wall == 0 ? 4 : 2;
+    const double at = wall == 3 ? xmax : wall == 1 ? ymax : 0.0;
+    return oracle_see_face(w, dirflag, at, x, y, vx, vy, vz, id, seed, step, out, cap);
 }
 
 // PERFORM_ELECTRON_EMISSION_SETUP pic2d_Setup.f90:618-1001: one local part per wall covering the whole wall

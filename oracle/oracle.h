@@ -134,6 +134,9 @@ typedef struct {
  * 1 + e = true secondary e (normal speed, two tangential components). */
 int32_t oracle_see(const oracle_see_t* w, int32_t wall, double x, double y, double vx, double vy, double vz,
                    uint32_t id, uint64_t seed, uint32_t step, double xmax, double ymax, double* out, int32_t cap);
+/* the same from the surface given by dirflag (1 normal +x, 2 -y, 3 -x, 4 +y) at coordinate `at` (no clamping) */
+int32_t oracle_see_face(const oracle_see_t* w, int32_t dirflag, double at, double x, double y, double vx, double vy,
+                        double vz, uint32_t id, uint64_t seed, uint32_t step, double* out, int32_t cap);
 
 /* PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001) of one domain wall for one cluster over
  * [0, xmax] x [0, ymax]: INT(n) electrons plus one with probability n - INT(n), uniform along the wall, 1e-6 inside;

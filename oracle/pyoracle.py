@@ -121,6 +121,8 @@ def lib():
             "oracle_ion_emission_face": ([C.POINTER(Emit), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, _D,
                                           C.c_int32], C.c_int32),
+            "oracle_see_face": ([C.POINTER(See), C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_uint32, C.c_uint64, C.c_uint32, _D, C.c_int32], C.c_int32),
             "oracle_inner_cross": ([C.POINTER(Geom), C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                     _I32, _D, _D], C.c_int32),
             "oracle_inner_charge": ([C.POINTER(Geom), C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _D],
@@ -288,6 +290,25 @@ def inner_charge(g, n, m, xc, yc, q, surf):
     lib().oracle_inner_charge(C.byref(g), int(n), int(m), xc, yc, q, dp(surf))
 
 
+def inner_electron_impact(g, see, dielectric, row, seed, step, surf):
+    """DO_ELECTRON_COLL_WITH_INNER_OBJECT (pic2d_ElectronWallCollisions.f90:561-645) for one absorbed electron (a
+    push_hits row of object 4 + n): the electrons the object's material emits from the side crossed first
+    (ElectronEmission by object in `see`), with a dielectric's outline taking -1 and +1 per emitted electron."""
+    _obj, x, y, vx, vy, vz, ident = row
+    n, m, xc, yc = inner_cross(g, x, y, vx, vy, 1.0)
+    if n < 0:
+        return np.zeros((0, 5))
+    if dielectric.get(n):
+        inner_charge(g, n, m, xc, yc, -1.0, surf)
+    if 4 + n not in see:
+        return np.zeros((0, 5))
+    dirflag, at = inner_face(g, n, m)
+    out, k = see[4 + n].emit_face(dirflag, at, xc, yc, vx, vy, vz, int(ident), seed, step)
+    if dielectric.get(n) and k > 0:
+        inner_charge(g, n, m, xc, yc, float(k), surf)
+    return out
+
+
 def inner_ion_impact(g, em, reflect, dielectric, q, row, seed, step, xmul, surf):
     """DO_ION_COLL_WITH_INNER_OBJECT (pic2d_IonWallCollisions.f90:484-575) for one absorbed ion (a push_hits row of
     object 4 + n): (emitted electrons, reflected ion row or None). A reflecting object returns the ion 1e-6 outside
@@ -361,6 +382,13 @@ class ElectronEmission:
         out = np.zeros((cap, 5))
         n = lib().oracle_see(C.byref(self.s), int(wall), x, y, vx, vy, vz, int(ident), seed, step, xmax, ymax,
                              dp(out), cap)
+        assert n <= cap
+        return out[:max(n, 0)], n
+
+    def emit_face(self, dirflag, at, x, y, vx, vy, vz, ident, seed, step, cap=64):
+        out = np.zeros((cap, 5))
+        n = lib().oracle_see_face(C.byref(self.s), int(dirflag), at, x, y, vx, vy, vz, int(ident), seed, step,
+                                  dp(out), cap)
         assert n <= cap
         return out[:max(n, 0)], n
 

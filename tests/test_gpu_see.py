@@ -103,3 +103,66 @@ def test_electron_emission_matches_oracle(tmp_path, precision, sort_every, geome
     vs = np.abs(ref[:, 2:]).max()
     tol = 2e-6 if precision == PREC_MIXED else 1e-12
     assert pair_rows(ref, got, np.array([1.0, 1.0, vs, vs, vs])) <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_electron_emission_at_inner_objects_matches_oracle(tmp_path, precision):
+    """DO_ELECTRON_COLL_WITH_INNER_OBJECT (pic2d_ElectronWallCollisions.f90:561-645) with electron-induced emission
+    from a metal and a dielectric inner object (the two example materials above, keyed 4 + n): electrons launched
+    into both objects from all four sides with 3 to 700 eV, one electron push without field; the electrons each object
+    emits leave the side crossed first, at the crossing (PROCESS_ELECTRON_INDUCED_ELECTRON_EMISSION with the object's
+    face); the dielectric's outline takes -1 per absorbed electron and +1 per emitted one. Counts per object exact,
+    rows paired with the oracle's, outline charge as the dielectric tests."""
+    from test_gpu_dielectric import particles_into
+    from test_gpu_emission import DIEL, METAL
+
+    from edipic_b200 import FIELD_SURFACE_CHARGE
+
+    d = small_deck(tmp_path, "walled", ncx=64, ncy=48, inner=[METAL, DIEL], collisions=False)
+    mats = {4: WALLS[0], 5: WALLS[1]}
+    with Simulation(d, precision=precision, sort_every=0, fuse_collisions=False) as sim:
+        p = sim.params
+        ef = sim.deck.tables.energy_factor_eV
+        for o, prm in mats.items():
+            sim.set_electron_emission(o, **prm)
+        xa = particles_into(sim, METAL, 6000, 21, 0.7, precision)
+        xb = particles_into(sim, DIEL, 6000, 22, 0.7, precision)
+        x, y, vx, vy, vz = (np.concatenate([a, b]) for a, b in zip(xa, xb))
+        ids = np.arange(x.size, dtype=np.uint32) * 5 + 3
+        sim.upload_particles(ELECTRONS, x, y, vx, vy, vz, ids=ids)
+        step = sim.counters().step
+        sim.advance_electrons()
+        c = sim.counters()
+        emitted = sim.emission_counts()
+        surf_got = sim.field(FIELD_SURFACE_CHARGE)
+        sim.end_ion_cycle()
+        el = sim.download_particles(ELECTRONS)
+    new = ~np.isin(el["id"], ids)
+    got = np.stack([el[k][new] for k in ("x", "y", "vx", "vy", "vz")], axis=1)
+
+    g = oracle_geom(sim)
+    sp = pyoracle.Species(p.bx, p.by, p.bz, p.ez, 0, 0.0, p.n_subcycles, p.ions_sense_b, p.ions_sense_ez)
+    ps = pyoracle.ParticleSet(x, y, vx, vy, vz, ids=ids)
+    zero = np.zeros((sim.ny_ref, sim.nx_ref))
+    hits, rows = pyoracle.push_hits(g, sp, zero, zero, ps)
+    see = {o: pyoracle.ElectronEmission(prm, ef) for o, prm in mats.items()}
+    surf = np.zeros(pyoracle.nodes_shape(g))
+    ref, per_obj = [], np.zeros(8, np.int64)
+    for r in rows:
+        if int(r[0]) < 4:
+            continue
+        out = pyoracle.inner_electron_impact(g, see, {1: True}, r, p.seed, step, surf)
+        per_obj[int(r[0])] += len(out)
+        ref.append(out)
+    ref = np.concatenate(ref) if ref else np.zeros((0, 5))
+    assert np.array_equal(np.array(c.electron_hits[:8]), hits), (list(c.electron_hits[:8]), hits)
+    assert hits[4] > 3000 and hits[5] > 3000
+    assert np.array_equal(emitted, per_obj), (emitted, per_obj)
+    assert per_obj[4] > 300 and per_obj[5] > 300
+    assert got.shape == ref.shape
+    vs = np.abs(ref[:, 2:]).max()
+    tol = 2e-6 if precision == PREC_MIXED else 1e-12
+    assert pair_rows(ref, got, np.array([1.0, 1.0, vs, vs, vs])) <= tol
+    stol = 5e-4 if precision == PREC_MIXED else 1e-8
+    assert np.abs(surf_got - surf).max() < stol, np.abs(surf_got - surf).max()
