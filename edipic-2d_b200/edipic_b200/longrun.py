@@ -14,6 +14,7 @@ import argparse
 import json
 import os
 import tempfile
+import time
 
 import numpy as np
 
@@ -112,18 +113,25 @@ def main():
     ap.add_argument("--sample-every", type=int, default=20)
     ap.add_argument("--out", default="longrun.json")
     args = ap.parse_args()
-    res = {}
-    for prec, name in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
-        res[name] = [run(prec, 1000 + s, args.steps, tuple(args.cells), args.ppc, burn_in=args.burn_in,
-                         sample_every=args.sample_every) for s in range(args.seeds)]
-    summary = dict(config=dict(seeds=args.seeds, steps=args.steps, cells=list(args.cells), ppc=args.ppc,
-                               burn_in=args.burn_in or args.steps // 2, sample_every=args.sample_every,
-                               samples=res["mixed"][0]["samples"]),
-                   paired=compare_paired(res["mixed"], res["fp64"]),
-                   welch=compare(res["mixed"], res["fp64"]),
-                   ion_flux=dict(mixed=np.mean([r["ion_flux"] for r in res["mixed"]], 0).tolist(),
-                                 fp64=np.mean([r["ion_flux"] for r in res["fp64"]], 0).tolist()))
-    json.dump(dict(summary=summary, runs=res), open(args.out, "w"))
+    res = {"mixed": [], "fp64": [], "seconds": []}
+    summary = None
+    # seed by seed, both precisions, so that an interrupted run still leaves complete pairs in the output file
+    for s in range(args.seeds):
+        for prec, name in ((PREC_MIXED, "mixed"), (PREC_FP64, "fp64")):
+            t0 = time.perf_counter()
+            res[name].append(run(prec, 1000 + s, args.steps, tuple(args.cells), args.ppc, burn_in=args.burn_in,
+                                 sample_every=args.sample_every))
+            res["seconds"].append([name, s, time.perf_counter() - t0])
+        summary = dict(config=dict(seeds=s + 1, steps=args.steps, cells=list(args.cells), ppc=args.ppc,
+                                   burn_in=args.burn_in or args.steps // 2, sample_every=args.sample_every,
+                                   samples=res["mixed"][0]["samples"]),
+                       ion_flux=dict(mixed=np.mean([r["ion_flux"] for r in res["mixed"]], 0).tolist(),
+                                     fp64=np.mean([r["ion_flux"] for r in res["fp64"]], 0).tolist()))
+        if s >= 1:
+            summary["paired"] = compare_paired(res["mixed"], res["fp64"])
+            summary["welch"] = compare(res["mixed"], res["fp64"])
+        with open(args.out, "w") as f:
+            json.dump(dict(summary=summary, runs=res), f)
     print(json.dumps(summary))
 
 
