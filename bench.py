@@ -653,10 +653,11 @@ def main():
     ap.add_argument("--warm-ceiling", action="store_true", help="only the warm-start accuracy leg (cfg2 geometry)")
     ap.add_argument("--sort-pass", action="store_true",
                     help="periodic sorts as a separate pass instead of inside the next push")
-    ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2, 3],
+    ap.add_argument("--push-kernel", type=int, default=None, choices=[0, 1, 2, 3, 4],
                     help="mixed push over the sorted chunks (edp_set_push_kernel): 0 per-chunk CTAs, 1 streaming "
                          "(bulk copies, 4 particles per thread), 2 streaming (2 per thread, 3 stages), 3 per-chunk "
-                         "CTAs with 2 particles per thread")
+                         "CTAs with 2 particles per thread, 4 per-chunk CTAs with each thread's next group copied "
+                         "ahead by cp.async")
     args = ap.parse_args()
     cfg = _decks_module().CONFIGS[args.config]
     args.cells_x, args.cells_y = args.cells if args.cells else (cfg["ncx"], cfg["ncy"])

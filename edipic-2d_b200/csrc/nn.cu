@@ -249,6 +249,242 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
 }
 
+// ------------------------------------------------------------------------------------------ persistent halo forward
+// The same convolution as a persistent, warp-specialised kernel for the layers with many pixels and few channels.
+// A tile is an 8 x 16-pixel patch (M = 128 rows of the implicit GEMM, row r = pixel (r % 8, r / 8)). Its input is
+// brought in ONCE as a 10 x 18-pixel halo and serves all nine taps: the halo of a 32-channel chunk lies in shared
+// memory as four planes of 8 channels, plane s holding pixel q at byte 16 q (the canonical K-major layout without
+// swizzle: core matrices of 8 pixels x 16 bytes), so the A operand of tap (dx, dy) is the same planes read from
+// pixel 10 dy + dx on: stride between 8-row groups (SBO) = one halo row = 160 bytes, between the two 8-channel
+// halves of a K step (LBO) = one plane. The planes are padded so that the 16-byte writes of eight lanes (two pixels
+// x four planes) hit all 32 banks. The weights of the whole layer stay in shared memory (loaded once by TMA, 64-byte
+// swizzle, one (32, c_out) box per tap and chunk).
+// Roles: warps 0-1 copy halos with cp.async (16-byte pieces of the NHWC rows, zero-filled off the image) into a ring
+// of stages, each copy signalling the stage's full barrier when it lands (cp.async.mbarrier.arrive.noinc); warp 2,
+// lane 0, loads the weights and issues the MMAs (tcgen05.mma, accumulator in one of two tensor-memory buffers,
+// committed to the stage's empty barrier and, after the tile's last chunk, to the buffer's full barrier); warps
+// 3-6 (one per quarter of the tensor-memory lanes) read the accumulator back (tcgen05.ld), add the bias, apply ReLU
+// and store BF16, then release the buffer.
+// Tiles are taken round-robin by the persistent CTAs, so the next tile's copies and MMAs overlap this tile's
+// epilogue. Every wait is bounded; a wait that gives up sets the error word and stops every role.
+constexpr int kHaloThreads = 224;
+constexpr int kHaloStages = 4;
+constexpr int kHaloPlane = 2912;                      // 182 pixel slots of 16 bytes (180 used)
+constexpr int kHaloStage = 4 * kHaloPlane;            // one 32-channel chunk
+constexpr int kHaloMaxWeights = 112 * 1024;           // largest resident weight set (9 x c_in x c_out x 2 bytes)
+
+struct HaloArgs {
+    const bf16* x1;
+    const bf16* x2;
+    int c1, c2, nimg, h, w, cout, relu, tiles_x, tiles_y;
+    int64_t n_tiles;
+    const float* bias;
+    bf16* y;
+    int* err;
+};
+
+__device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity, volatile int* fail)
+{
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P;\n\t}\n"
+                     : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+        if ((it & 1023) == 1023 && *fail) return false;
+    }
+    *fail = 1;
+    return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kHaloThreads, 1)
+    conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, HaloArgs a)
+{
+    constexpr uint32_t TMEM_COLS = BN <= 32 ? 64 : BN <= 64 ? 128 : 256;   // two accumulators
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+    // A: no swizzle, LBO = one plane (K direction), SBO = one halo row of 10 pixels (M direction)
+    constexpr uint64_t DESC_A = ((uint64_t)(160 >> 4) << 32) | ((uint64_t)(kHaloPlane >> 4) << 16) | ((uint64_t)1 << 46);
+    // B: 64-byte swizzle, 8-row atoms of 64 bytes (SBO = 512 bytes), LBO unused
+    constexpr uint64_t DESC_B = ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61) |
+                                ((uint64_t)1 << 16);
+    constexpr int B_CHUNK = BN * 64;   // bytes of one (tap, chunk) weight box
+    extern __shared__ unsigned char dsm[];
+    __shared__ __align__(8) uint64_t full[kHaloStages], empty[kHaloStages], acc_full[2], acc_empty[2], wbar, done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = a.c1 + a.c2, n_chunks = cin / 32;
+    const uint32_t wbase = (smem_u32(dsm) + 1023u) & ~1023u;
+    const uint32_t hbase = wbase + (uint32_t)(9 * n_chunks * B_CHUNK);
+
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int s = 0; s < kHaloStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(64));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+        }
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&acc_full[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(smem_u32(&acc_empty[b])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&wbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&done_bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    const int64_t stride = gridDim.x;
+
+    if (warp < 2) {
+        // ---------------- halo producer: 64 threads, 16-byte pieces, 4 per pixel and chunk
+        const int pt = tid;   // 0..63
+        int64_t it = 0;
+        for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride) {
+            const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
+            const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
+            const int gx0 = tx * 8 - 1, gy0 = ty * 16 - 1;
+            for (int cc = 0; cc < n_chunks; ++cc, ++it) {
+                const int s = (int)(it % kHaloStages);
+                if (it >= kHaloStages &&
+                    !mbar_wait_or_fail(smem_u32(&empty[s]), (uint32_t)(((it / kHaloStages) - 1) & 1), &fail_sh))
+                    break;
+                const int c0 = cc * 32;
+                const bf16* src = c0 < a.c1 ? a.x1 : a.x2;
+                const int cs = c0 < a.c1 ? a.c1 : a.c2, co = c0 < a.c1 ? c0 : c0 - a.c1;
+                const uint32_t st = hbase + (uint32_t)(s * kHaloStage);
+                for (int q = pt; q < 180 * 4; q += 64) {
+                    const int px = q >> 2, pl = q & 3;
+                    const int hx = px % 10, hy = px / 10;
+                    const int gx = gx0 + hx, gy = gy0 + hy;
+                    const bool ok = gx >= 0 && gx < a.w && gy >= 0 && gy < a.h;
+                    const bf16* g = ok ? src + (((int64_t)img * a.h + gy) * a.w + gx) * cs + co + 8 * pl : src;
+                    cp_async16(st + (uint32_t)(pl * kHaloPlane + px * 16), g, ok);
+                }
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[s]))
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    } else if (warp == 2) {
+        // ---------------- weights once, then the MMAs (lane 0)
+        if (lane == 0) {
+            const uint32_t wb = smem_u32(&wbar);
+            const uint32_t bytes = (uint32_t)(9 * n_chunks * B_CHUNK);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(wb), "r"(bytes) : "memory");
+            for (int k = 0; k < 9 * n_chunks; ++k)
+                asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                             ::"r"(wbase + (uint32_t)(k * B_CHUNK)), "l"(&mw), "r"(k * 32), "r"(0), "r"(wb) : "memory");
+            bool ok = mbar_wait_or_fail(wb, 0u, &fail_sh);
+            int64_t it = 0, tl = 0;
+            for (int64_t t = blockIdx.x; ok && t < a.n_tiles && !fail_sh; t += stride, ++tl) {
+                const int buf = (int)(tl & 1);
+                if (tl >= 2 && !mbar_wait_or_fail(smem_u32(&acc_empty[buf]), (uint32_t)(((tl >> 1) - 1) & 1), &fail_sh))
+                    break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(buf * BN);
+                for (int cc = 0; cc < n_chunks; ++cc, ++it) {
+                    const int s = (int)(it % kHaloStages);
+                    if (!mbar_wait_or_fail(smem_u32(&full[s]), (uint32_t)((it / kHaloStages) & 1), &fail_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    // the halo was written by the generic proxy (cp.async); the MMAs read it through the async one
+                    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t As = hbase + (uint32_t)(s * kHaloStage);
+                    for (int tap = 0; tap < 9; ++tap) {
+                        const uint32_t a0 = As + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
+                        const uint32_t b0 = wbase + (uint32_t)((tap * n_chunks + cc) * B_CHUNK);
+                        for (int ks = 0; ks < 2; ++ks) {
+                            const uint64_t da = DESC_A | (uint64_t)(((a0 + (uint32_t)(2 * ks * kHaloPlane)) >> 4) & 0x3FFFu);
+                            const uint64_t db = DESC_B | (uint64_t)(((b0 + 32u * ks) >> 4) & 0x3FFFu);
+                            const uint32_t accum = (cc > 0 || tap > 0 || ks > 0) ? 1u : 0u;
+                            asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                                         ::"r"(acc), "l"(da), "l"(db), "r"(IDESC), "r"(accum));
+                        }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                                 ::"r"(smem_u32(&empty[s])) : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                             ::"r"(smem_u32(&acc_full[buf])) : "memory");
+            }
+            // every MMA issued has finished before the accumulators are released
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         ::"r"(smem_u32(&done_bar)) : "memory");
+            mbar_wait_or_fail(smem_u32(&done_bar), 0u, &fail_sh);
+        }
+        __syncwarp();
+    }
+    if (warp >= 3) {
+        // ---------------- epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31; lane 0 waits for the
+        // warp, so that the whole warp takes the same path through the .sync.aligned loads
+        const int q = warp & 3;
+        const int r = q * 32 + lane;
+        int64_t tl = 0;
+        for (int64_t t = blockIdx.x; t < a.n_tiles; t += stride, ++tl) {
+            const int buf = (int)(tl & 1);
+            int go = 0;
+            if (lane == 0) go = !fail_sh && mbar_wait_or_fail(smem_u32(&acc_full[buf]), (uint32_t)((tl >> 1) & 1), &fail_sh);
+            if (!__shfl_sync(0xFFFFFFFFu, go, 0)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
+            const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
+            const int px = tx * 8 + (r & 7), py = ty * 16 + (r >> 3);
+            const bool inside = px < a.w && py < a.h;
+            const int64_t p = ((int64_t)img * a.h + py) * a.w + px;
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t v[16];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                             " [%16];\n"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                               "=r"(v[14]), "=r"(v[15])
+                             : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN + c0)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (inside) {
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        float v0 = __uint_as_float(v[2 * k]) + (a.bias ? __ldg(a.bias + c0 + 2 * k) : 0.0f);
+                        float v1 = __uint_as_float(v[2 * k + 1]) + (a.bias ? __ldg(a.bias + c0 + 2 * k + 1) : 0.0f);
+                        if (a.relu) {
+                            v0 = fmaxf(v0, 0.0f);
+                            v1 = fmaxf(v1, 0.0f);
+                        }
+                        __nv_bfloat162 h2 = __floats2bfloat162_rn(v0, v1);
+                        pk[k] = *reinterpret_cast<uint32_t*>(&h2);
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(a.y + p * a.cout + c0);
+                    dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (fail_sh && tid == 0) atomicExch(a.err, 1);
+    if (warp == 2) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -346,6 +582,64 @@ int launch_tma_cout(const ConvArgs& a, int* err, cudaStream_t s)
     case 384: return launch_tma<192, CW>(a, err, s);
     default: return EDP_ERR_ARG;
     }
+}
+
+// the persistent halo kernel for c_out = BN: all 9 x c_in x BN weights resident, as many CTAs per SM as shared memory
+// and the two accumulators per CTA in tensor memory (512 columns per SM) allow, one per SM at least
+template <int BN>
+int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
+{
+    const int n_chunks = (c.c1 + c.c2) / 32;
+    const int smem = 1024 + 9 * n_chunks * BN * 64 + kHaloStages * kHaloStage;
+    static int configured[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
+    if (configured[dev] < smem) {
+        if (cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+            return EDP_ERR_CUDA;
+        configured[dev] = smem;
+    }
+    CUtensorMap mw;
+    if (!map_wt(&mw, c.wt, 9 * (c.c1 + c.c2), c.cout, 32, BN)) return EDP_ERR_CUDA;
+    HaloArgs a;
+    a.x1 = c.x1;
+    a.x2 = c.x2;
+    a.c1 = c.c1;
+    a.c2 = c.c2;
+    a.nimg = c.nimg;
+    a.h = c.h;
+    a.w = c.w;
+    a.cout = c.cout;
+    a.relu = c.relu;
+    a.tiles_x = (c.w + 7) / 8;
+    a.tiles_y = (c.h + 15) / 16;
+    a.n_tiles = (int64_t)a.tiles_x * a.tiles_y * c.nimg;
+    a.bias = c.bias;
+    a.y = c.y;
+    a.err = err;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_fwd_halo_kernel<BN>, kHaloThreads, smem) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return EDP_ERR_CUDA;
+    const int tmem_cols = BN <= 32 ? 64 : BN <= 64 ? 128 : 256;
+    if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t grid = a.n_tiles < (int64_t)sms * per_sm ? a.n_tiles : (int64_t)sms * per_sm;
+    conv3x3_fwd_halo_kernel<BN><<<(unsigned)grid, kHaloThreads, smem, s>>>(mw, a);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+// 0: the halo kernel where it applies (c_out 32, 64 or 128, the weights fit in shared memory, at least two tiles
+// per SM), else the tile kernel; 1: always the tile kernel; 2: always the halo kernel (refused where it does not apply)
+int g_conv_mode = 0;
+
+bool halo_applies(const ConvArgs& c)
+{
+    const int64_t tiles = (int64_t)((c.w + 7) / 8) * ((c.h + 15) / 16) * c.nimg;
+    return (c.cout == 32 || c.cout == 64 || c.cout == 128) && 9LL * (c.c1 + c.c2) * c.cout * 2 <= kHaloMaxWeights &&
+           tiles >= 2 * 148;
 }
 
 // wt_t[c][8 - tap][n] = wt[n][tap][c]: the weights of the data gradient
@@ -474,6 +768,221 @@ __global__ void __launch_bounds__((BM / 32) * (BN / 16) * 32) conv3x3_wgrad_kern
                 const int ci = ci0 + wn * 16 + j * 8 + 2 * t + (q & 1);
                 atomicAdd(&a.dw[((int64_t)co * 9 + tap) * cin + ci], acc[i][j][q]);
             }
+}
+
+// ------------------------------------------------------------------------------------------ weight gradient on tcgen05
+// dw[n][tap][c] += sum_p dz[p][n] x[p + off(tap)][c] as one GEMM per tap with M = output channels (a chunk of M = 64
+// or 128 of them), N = a 32-channel chunk of the input, K = pixels. The pixels come in 8 x 16 patches as in the
+// halo forward kernel: the patch of dz lies in shared memory as planes of 8 output channels (pixel q at byte 16 q),
+// which is the canonical MN-major layout without swizzle for A (8-channel groups one plane apart = SBO, 8-pixel groups
+// 128 bytes apart = LBO); the 10 x 18 halo of x lies as four planes of 8 input channels, and the B operand of tap
+// (dx, dy) is the same planes read from pixel 10 dy + dx on (MN-major: channel groups one plane apart = SBO, 8-pixel
+// groups = patch rows one halo row apart = LBO of 160 bytes). One patch and one halo serve all nine taps, whose
+// accumulators (9 x 32 FP32 columns) stay in tensor memory for the CTA's whole pixel range. Pixels are split over
+// the CTAs (patches taken round-robin); at the end each CTA adds its partial sums to dw with vector FP32 reductions.
+// Roles as in the halo forward kernel: warps 0-1 copy (cp.async, zero-filled off the image), warp 2 lane 0 issues
+// the MMAs, warps 3-6 read the accumulators back. With M = 64 the accumulator rows 16 q .. 16 q + 15 sit in lanes
+// 32 q .. 32 q + 15 of tensor memory; output channels past c_out read zero planes.
+constexpr int kWgStages = 3;
+constexpr int kDzPlane = 2064;   // 129 pixel slots of 16 bytes (128 used)
+
+struct WgradTcArgs {
+    const bf16* x1;
+    const bf16* x2;
+    int c1, c2;
+    const bf16* dz;
+    int cout, nimg, h, w, tiles_x, tiles_y;
+    int64_t n_tiles;
+    float* dw;
+    int* err;
+};
+
+template <int M>
+__global__ void __launch_bounds__(kHaloThreads, 1) conv3x3_wgrad_tc_kernel(WgradTcArgs a)
+{
+    constexpr int NP = M / 8;                                   // dz planes
+    constexpr int STAGE = NP * kDzPlane + kHaloStage;
+    constexpr uint32_t TMEM_COLS = 512;                         // 9 taps x 32 columns
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((32u >> 3) << 17) |
+                               ((uint32_t)(M >> 4) << 24);
+    constexpr uint64_t DESC_A = ((uint64_t)(kDzPlane >> 4) << 32) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)1 << 46);
+    constexpr uint64_t DESC_B = ((uint64_t)(kHaloPlane >> 4) << 32) | ((uint64_t)(160 >> 4) << 16) | ((uint64_t)1 << 46);
+    extern __shared__ unsigned char dsm[];
+    __shared__ __align__(8) uint64_t full[kWgStages], empty[kWgStages], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c0 = blockIdx.y * 32;                              // input channels of this CTA
+    const int m0 = blockIdx.z * M;                               // output channels of this CTA
+    const int mvalid = a.cout - m0 < M ? a.cout - m0 : M;
+    const uint32_t base = (smem_u32(dsm) + 127u) & ~127u;
+    unsigned char* gbase = dsm + (base - smem_u32(dsm));
+
+    // planes past c_out stay zero in every stage
+    for (int st = 0; st < kWgStages; ++st)
+        for (int b = (mvalid / 8) * kDzPlane + tid * 16; b < NP * kDzPlane; b += kHaloThreads * 16)
+            *reinterpret_cast<uint4*>(gbase + st * STAGE + b) = make_uint4(0u, 0u, 0u, 0u);
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int st = 0; st < kWgStages; ++st) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[st])), "r"(64));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[st])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&done_bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    const int64_t stride = gridDim.x;
+    bool any = false;   // this CTA has at least one patch (every role sees the same)
+    if (blockIdx.x < a.n_tiles) any = true;
+
+    if (warp < 2) {
+        // ---------------- producer: dz patch planes and the x halo of each patch
+        const int pt = tid;
+        const bf16* xs = c0 < a.c1 ? a.x1 : a.x2;
+        const int xcs = c0 < a.c1 ? a.c1 : a.c2, xco = c0 < a.c1 ? c0 : c0 - a.c1;
+        const int nzp = mvalid / 8;
+        int64_t it = 0;
+        for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride, ++it) {
+            const int s = (int)(it % kWgStages);
+            if (it >= kWgStages &&
+                !mbar_wait_or_fail(smem_u32(&empty[s]), (uint32_t)(((it / kWgStages) - 1) & 1), &fail_sh))
+                break;
+            const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
+            const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
+            const uint32_t st = base + (uint32_t)(s * STAGE);
+            for (int q = pt; q < 128 * nzp; q += 64) {
+                const int px = q / nzp, pl = q - px * nzp;
+                const int gx = tx * 8 + (px & 7), gy = ty * 16 + (px >> 3);
+                const bool ok = gx < a.w && gy < a.h;
+                const bf16* g = ok ? a.dz + (((int64_t)img * a.h + gy) * a.w + gx) * a.cout + m0 + 8 * pl : a.dz;
+                cp_async16(st + (uint32_t)(pl * kDzPlane + px * 16), g, ok);
+            }
+            const uint32_t hs = st + (uint32_t)(NP * kDzPlane);
+            for (int q = pt; q < 180 * 4; q += 64) {
+                const int px = q >> 2, pl = q & 3;
+                const int gx = tx * 8 - 1 + px % 10, gy = ty * 16 - 1 + px / 10;
+                const bool ok = gx >= 0 && gx < a.w && gy >= 0 && gy < a.h;
+                const bf16* g = ok ? xs + (((int64_t)img * a.h + gy) * a.w + gx) * xcs + xco + 8 * pl : xs;
+                cp_async16(hs + (uint32_t)(pl * kHaloPlane + px * 16), g, ok);
+            }
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[s])) : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    } else if (warp == 2) {
+        if (lane == 0) {
+            int64_t it = 0;
+            for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride, ++it) {
+                const int s = (int)(it % kWgStages);
+                if (!mbar_wait_or_fail(smem_u32(&full[s]), (uint32_t)((it / kWgStages) & 1), &fail_sh)) break;
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t As = base + (uint32_t)(s * STAGE), Hs = As + (uint32_t)(NP * kDzPlane);
+                for (int tap = 0; tap < 9; ++tap) {
+                    const uint32_t b0 = Hs + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
+                    for (int ks = 0; ks < 8; ++ks) {
+                        const uint64_t da = DESC_A | (uint64_t)(((As + (uint32_t)(256 * ks)) >> 4) & 0x3FFFu);
+                        const uint64_t db = DESC_B | (uint64_t)(((b0 + (uint32_t)(320 * ks)) >> 4) & 0x3FFFu);
+                        const uint32_t accum = (it > 0 || ks > 0) ? 1u : 0u;
+                        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                                     ::"r"(tmem + (uint32_t)(tap * 32)), "l"(da), "l"(db), "r"(IDESC), "r"(accum));
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                             ::"r"(smem_u32(&empty[s])) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         ::"r"(smem_u32(&done_bar)) : "memory");
+            mbar_wait_or_fail(smem_u32(&done_bar), 0u, &fail_sh);
+        }
+        __syncwarp();
+    }
+    __syncthreads();   // the producer and the MMAs are done (or gave up)
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp >= 3 && any && !fail_sh) {
+        const int q = warp & 3;
+        const int r = M == 128 ? q * 32 + lane : q * 16 + lane;   // accumulator row of this lane
+        const bool valid = (M == 128 || lane < 16) && r < mvalid;
+        for (int tap = 0; tap < 9; ++tap) {
+            for (int h = 0; h < 2; ++h) {
+                uint32_t v[16];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                             " [%16];\n"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                               "=r"(v[14]), "=r"(v[15])
+                             : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tap * 32 + 16 * h)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (valid) {
+                    float* d = a.dw + ((int64_t)(m0 + r) * 9 + tap) * (a.c1 + a.c2) + c0 + 16 * h;
+#pragma unroll
+                    for (int k = 0; k < 16; k += 4)
+                        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n"
+                                     ::"l"(d + k), "f"(__uint_as_float(v[k])), "f"(__uint_as_float(v[k + 1])),
+                                       "f"(__uint_as_float(v[k + 2])), "f"(__uint_as_float(v[k + 3]))
+                                     : "memory");
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (fail_sh && tid == 0) atomicExch(a.err, 1);
+    if (warp == 2) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// 0 (default) and 2: the weight gradient on tcgen05; 1: the mma.sync kernel
+int g_wgrad_mode = 0;
+
+// one CTA per SM (its 9 x 32 accumulator columns take 512 of tensor memory), the patches split over the CTAs of each
+// (input chunk, output chunk) pair
+template <int M>
+int launch_wgrad_tc(const WgradArgs& w, int* err, cudaStream_t s)
+{
+    constexpr int SMEM = 128 + kWgStages * ((M / 8) * kDzPlane + kHaloStage);
+    static bool configured[64] = {false};
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
+            cudaSuccess)
+            return EDP_ERR_CUDA;
+        configured[dev] = true;
+    }
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return EDP_ERR_CUDA;
+    WgradTcArgs a;
+    a.x1 = w.x;
+    a.x2 = w.x2;
+    a.c1 = w.c1;
+    a.c2 = w.c2;
+    a.dz = w.dz;
+    a.cout = w.cout;
+    a.nimg = w.nimg;
+    a.h = w.h;
+    a.w = w.w;
+    a.tiles_x = (w.w + 7) / 8;
+    a.tiles_y = (w.h + 15) / 16;
+    a.n_tiles = (int64_t)a.tiles_x * a.tiles_y * w.nimg;
+    a.dw = w.dw;
+    a.err = err;
+    const int n_c = (w.c1 + w.c2) / 32, n_m = (w.cout + M - 1) / M;
+    int64_t split = (sms + (int64_t)n_c * n_m - 1) / ((int64_t)n_c * n_m);
+    if (split > a.n_tiles) split = a.n_tiles;
+    if (split < 1) split = 1;
+    conv3x3_wgrad_tc_kernel<M><<<dim3((unsigned)split, (unsigned)n_c, (unsigned)n_m), kHaloThreads, SMEM, s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
 // db[n] += sum_p dz[p][n]
@@ -725,9 +1234,35 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
     cudaStream_t s = (cudaStream_t)stream;
     int* err = tc_error_word();
     if (!err) return EDP_ERR_CUDA;
+    const bool halo = g_conv_mode == 2 || (g_conv_mode == 0 && halo_applies(a));
+    if (halo) {
+        if (9LL * (c1 + c2) * cout * 2 > kHaloMaxWeights) return EDP_ERR_ARG;
+        switch (cout) {
+        case 32: return launch_halo<32>(a, err, s);
+        case 64: return launch_halo<64>(a, err, s);
+        case 128: return launch_halo<128>(a, err, s);
+        default: return EDP_ERR_ARG;
+        }
+    }
     // 64-channel chunks when neither c_in nor the concatenation split breaks them, else 32
     if (c1 % 64 == 0 && c2 % 64 == 0) return launch_tma_cout<64>(a, err, s);
     return launch_tma_cout<32>(a, err, s);
+}
+
+/* which weight-gradient kernel edp_nn_conv3x3_wgrad uses: 0 (default) or 2 tcgen05, 1 mma.sync */
+int edp_nn_wgrad_select(int32_t mode)
+{
+    if (mode < 0 || mode > 2) return EDP_ERR_ARG;
+    g_wgrad_mode = mode;
+    return EDP_OK;
+}
+
+/* which forward kernel edp_nn_conv3x3_fwd uses: 0 automatic, 1 the tile kernel, 2 the persistent halo kernel */
+int edp_nn_conv_select(int32_t mode)
+{
+    if (mode < 0 || mode > 2) return EDP_ERR_ARG;
+    g_conv_mode = mode;
+    return EDP_OK;
 }
 
 /* bounded-wait error word of the tcgen05 kernels: nonzero once a wait gave up; reading clears it */
@@ -769,6 +1304,19 @@ int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int
     a.dw = dw;
     const int64_t P = (int64_t)nimg * h * w;
     const int cin = c1 + c2;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (g_wgrad_mode != 1) {
+        int* err = tc_error_word();
+        if (!err) return EDP_ERR_CUDA;
+        const int rc = cout % 128 == 0 ? launch_wgrad_tc<128>(a, err, s) : launch_wgrad_tc<64>(a, err, s);
+        if (rc != EDP_OK) return rc;
+        if (db) {
+            const int lanes = 1024 / cout;
+            bias_grad_kernel<<<grid_for(P, 1024), lanes * cout, lanes * cout * sizeof(float), s>>>((const bf16*)dz, P,
+                                                                                                cout, db);
+        }
+        return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+    }
     const int bm = cout % 64 == 0 ? 64 : 32;
     // the input-channel tile must not straddle the two concatenated tensors
     const int bn = (cin % 64 == 0 && c1 % 64 == 0) ? 64 : 32;
@@ -779,7 +1327,6 @@ int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int
     per = (per + kWK - 1) / kWK * kWK;
     a.pix_per_cta = per;
     dim3 grid((unsigned)((P + per - 1) / per), (unsigned)tiles);
-    cudaStream_t s = (cudaStream_t)stream;
     if (bm == 64 && bn == 64) conv3x3_wgrad_kernel<64, 64><<<grid, 256, 0, s>>>(a);
     else if (bm == 64) conv3x3_wgrad_kernel<64, 32><<<grid, 128, 0, s>>>(a);
     else if (bn == 64) conv3x3_wgrad_kernel<32, 64><<<grid, 128, 0, s>>>(a);

@@ -354,54 +354,22 @@ __device__ __forceinline__ void vstore(void* p, int64_t g, const uint32_t* v)
     else __stcs(reinterpret_cast<uint2*>(p) + g, make_uint2(v[0], v[1]));
 }
 
-// IPT consecutive slots [IPT g, IPT g + IPT). WIN: a sorted chunk, always whole groups (tiles are padded to
-// multiples of EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted
-// to [lo, hi).
+// The push, deposit and stores of IPT consecutive slots [IPT g, IPT g + IPT) whose columns are in registers; `full`:
+// the whole group lies in [lo, hi) (vector stores), else only the slots inside are stored.
 template <bool ION, bool PER, bool ROT, bool WIN, int IPT>
-__device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
-                                           int64_t hi)
+__device__ __forceinline__ void push_group_body(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
+                                                int64_t hi, bool full, int* c, float* ox, float* oy, float* vx,
+                                                float* vy, float* vz, const uint32_t* id)
 {
     const int64_t base = g * IPT;
-    const bool full = WIN || (base >= lo && base + IPT <= hi);
-    const bool windowed = WIN;
-    int c[IPT];
-    float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
-    uint32_t id[IPT];
     bool sel[IPT];
-    if (full) {
-        vload<IPT>(a.P.cell, g, reinterpret_cast<uint32_t*>(c));
-        vload<IPT>(a.P.ox, g, reinterpret_cast<uint32_t*>(ox));
-        vload<IPT>(a.P.oy, g, reinterpret_cast<uint32_t*>(oy));
-        vload<IPT>(a.P.vx, g, reinterpret_cast<uint32_t*>(vx));
-        vload<IPT>(a.P.vy, g, reinterpret_cast<uint32_t*>(vy));
-        vload<IPT>(a.P.vz, g, reinterpret_cast<uint32_t*>(vz));
-        if (a.need_id) {
-            vload<IPT>(a.P.id, g, id);
-        } else {
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) id[e] = 0u;
-        }
-    } else {
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) {
-            int64_t k = base + e;
-            bool ok = k >= lo && k < hi;
-            c[e] = ok ? a.P.cell[k] : -1;
-            ox[e] = ok ? a.P.ox[k] : 0.f;
-            oy[e] = ok ? a.P.oy[k] : 0.f;
-            vx[e] = ok ? a.P.vx[k] : 0.f;
-            vy[e] = ok ? a.P.vy[k] : 0.f;
-            vz[e] = ok ? a.P.vz[k] : 0.f;
-            id[e] = ok ? a.P.id[k] : 0u;
-        }
-    }
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
     for (int e = 0; e < IPT; ++e) {
         sel[e] = false;
         if (c[e] < 0) continue;
-        if (!push_one<ION, PER, ROT>(a, s, windowed, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
                                      sel[e])) {
             c[e] = -1;
             sel[e] = false;
@@ -432,6 +400,96 @@ __device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, 
             a.P.vy[k] = vy[e];
             a.P.vz[k] = vz[e];
         }
+    }
+}
+
+// IPT consecutive slots [IPT g, IPT g + IPT). WIN: a sorted chunk, always whole groups (tiles are padded to
+// multiples of EDP_ITEMS), gathered and deposited through the shared window. Otherwise the unsorted tail, restricted
+// to [lo, hi).
+template <bool ION, bool PER, bool ROT, bool WIN, int IPT>
+__device__ __forceinline__ void push_group(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t g, int64_t lo,
+                                           int64_t hi)
+{
+    const int64_t base = g * IPT;
+    const bool full = WIN || (base >= lo && base + IPT <= hi);
+    int c[IPT];
+    float ox[IPT], oy[IPT], vx[IPT], vy[IPT], vz[IPT];
+    uint32_t id[IPT];
+    if (full) {
+        vload<IPT>(a.P.cell, g, reinterpret_cast<uint32_t*>(c));
+        vload<IPT>(a.P.ox, g, reinterpret_cast<uint32_t*>(ox));
+        vload<IPT>(a.P.oy, g, reinterpret_cast<uint32_t*>(oy));
+        vload<IPT>(a.P.vx, g, reinterpret_cast<uint32_t*>(vx));
+        vload<IPT>(a.P.vy, g, reinterpret_cast<uint32_t*>(vy));
+        vload<IPT>(a.P.vz, g, reinterpret_cast<uint32_t*>(vz));
+        if (a.need_id) {
+            vload<IPT>(a.P.id, g, id);
+        } else {
+#pragma unroll
+            for (int e = 0; e < IPT; ++e) id[e] = 0u;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < IPT; ++e) {
+            int64_t k = base + e;
+            bool ok = k >= lo && k < hi;
+            c[e] = ok ? a.P.cell[k] : -1;
+            ox[e] = ok ? a.P.ox[k] : 0.f;
+            oy[e] = ok ? a.P.oy[k] : 0.f;
+            vx[e] = ok ? a.P.vx[k] : 0.f;
+            vy[e] = ok ? a.P.vy[k] : 0.f;
+            vz[e] = ok ? a.P.vz[k] : 0.f;
+            id[e] = ok ? a.P.id[k] : 0u;
+        }
+    }
+    push_group_body<ION, PER, ROT, WIN, IPT>(a, s, wx0, wy0, g, lo, hi, full, c, ox, oy, vx, vy, vz, id);
+}
+
+// 16-byte copy global -> shared that bypasses L1 (cp.async.cg)
+__device__ __forceinline__ void pf_copy16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+
+// The sorted chunk of one CTA with 4 particles per thread, each thread's next group copied ahead into shared memory
+// by cp.async while it pushes the current one, so that every warp has its next loads in flight during its
+// arithmetic. A thread reads back only the 16-byte pieces it copied itself: no barrier, only its own wait.
+template <bool ION, bool PER, bool ROT>
+__device__ __forceinline__ void push_chunk_prefetch(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t lo,
+                                                    int64_t hi)
+{
+    __shared__ __align__(16) uint4 pf[7][EDP_PUSH_THREADS];
+    const int ncol = a.need_id ? 7 : 6;
+    const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(&pf[0][threadIdx.x]);
+    const void* col[7] = {a.P.cell, a.P.ox, a.P.oy, a.P.vx, a.P.vy, a.P.vz, a.P.id};
+    auto issue = [&](int64_t g) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            if (k < ncol) pf_copy16(d0 + (uint32_t)(k * EDP_PUSH_THREADS * 16), reinterpret_cast<const uint4*>(col[k]) + g);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    int64_t g = lo / 4 + threadIdx.x;
+    if (g * 4 < hi) issue(g);
+    for (; g * 4 < hi; g += blockDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        int c[4];
+        float ox[4], oy[4], vx[4], vy[4], vz[4];
+        uint32_t id[4] = {0u, 0u, 0u, 0u};
+        const uint4 v0 = pf[0][threadIdx.x], v1 = pf[1][threadIdx.x], v2 = pf[2][threadIdx.x];
+        const uint4 v3 = pf[3][threadIdx.x], v4 = pf[4][threadIdx.x], v5 = pf[5][threadIdx.x];
+        if (ncol == 7) {
+            const uint4 v6 = pf[6][threadIdx.x];
+            id[0] = v6.x; id[1] = v6.y; id[2] = v6.z; id[3] = v6.w;
+        }
+        c[0] = (int)v0.x; c[1] = (int)v0.y; c[2] = (int)v0.z; c[3] = (int)v0.w;
+        ox[0] = __uint_as_float(v1.x); ox[1] = __uint_as_float(v1.y); ox[2] = __uint_as_float(v1.z); ox[3] = __uint_as_float(v1.w);
+        oy[0] = __uint_as_float(v2.x); oy[1] = __uint_as_float(v2.y); oy[2] = __uint_as_float(v2.z); oy[3] = __uint_as_float(v2.w);
+        vx[0] = __uint_as_float(v3.x); vx[1] = __uint_as_float(v3.y); vx[2] = __uint_as_float(v3.z); vx[3] = __uint_as_float(v3.w);
+        vy[0] = __uint_as_float(v4.x); vy[1] = __uint_as_float(v4.y); vy[2] = __uint_as_float(v4.z); vy[3] = __uint_as_float(v4.w);
+        vz[0] = __uint_as_float(v5.x); vz[1] = __uint_as_float(v5.y); vz[2] = __uint_as_float(v5.z); vz[3] = __uint_as_float(v5.w);
+        const int64_t gn = g + blockDim.x;
+        if (gn * 4 < hi) issue(gn);   // the pieces just read are in registers; the copies may overwrite them
+        push_group_body<ION, PER, ROT, true, 4>(a, s, wx0, wy0, g, lo, hi, true, c, ox, oy, vx, vy, vz, id);
     }
 }
 
@@ -507,7 +565,7 @@ __device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, i
 
 // IPT particles per thread: 4 (128-bit accesses, 4 CTAs of 256 per SM) or 2 (64-bit, 5 CTAs per SM). SCAT: the
 // push of a sort step, writing every particle to its sorted slot of a.D
-template <bool ION, bool PER, bool ROT, int IPT, bool SCAT>
+template <bool ION, bool PER, bool ROT, int IPT, bool SCAT, bool PF>
 __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed_kernel(PushArgs a)
 {
     __shared__ Smem s;
@@ -548,8 +606,12 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 4 : 5) push_mixed
                 push_block_scatter<ION, PER, ROT, false>(a, s, 0, 0, b, lo, hi);
         }
     } else if (windowed) {
-        for (int64_t g = lo / IPT + threadIdx.x; g * IPT < hi; g += blockDim.x)
-            push_group<ION, PER, ROT, true, IPT>(a, s, wx0, wy0, g, lo, hi);
+        if constexpr (PF) {
+            push_chunk_prefetch<ION, PER, ROT>(a, s, wx0, wy0, lo, hi);
+        } else {
+            for (int64_t g = lo / IPT + threadIdx.x; g * IPT < hi; g += blockDim.x)
+                push_group<ION, PER, ROT, true, IPT>(a, s, wx0, wy0, g, lo, hi);
+        }
     } else {
         int64_t t = blockIdx.x - a.n_chunks;
         int64_t g0 = lo / IPT;
@@ -1321,18 +1383,18 @@ static int launch_stream_push(edp_ctx* c, int variant, int kind, const PushArgs&
     return kind == 2 ? launch_stream_kind<2, 3>(c, variant, a) : launch_stream_kind<4, 2>(c, variant, a);
 }
 
-template <int IPT, bool SCAT>
+template <int IPT, bool SCAT, bool PF>
 static int launch_classic_push(edp_ctx* c, int variant, unsigned gr, const PushArgs& a)
 {
     switch (variant) {
-    case 0: push_mixed_kernel<false, false, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 1: push_mixed_kernel<false, false, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 2: push_mixed_kernel<false, true, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 3: push_mixed_kernel<false, true, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 4: push_mixed_kernel<true, false, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 5: push_mixed_kernel<true, false, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    case 6: push_mixed_kernel<true, true, false, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
-    default: push_mixed_kernel<true, true, true, IPT, SCAT><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 0: push_mixed_kernel<false, false, false, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 1: push_mixed_kernel<false, false, true, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 2: push_mixed_kernel<false, true, false, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 3: push_mixed_kernel<false, true, true, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 4: push_mixed_kernel<true, false, false, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 5: push_mixed_kernel<true, false, true, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    case 6: push_mixed_kernel<true, true, false, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
+    default: push_mixed_kernel<true, true, true, IPT, SCAT, PF><<<gr, EDP_PUSH_THREADS, 0, c->stream>>>(a); break;
     }
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
@@ -1340,7 +1402,7 @@ static int launch_classic_push(edp_ctx* c, int variant, unsigned gr, const PushA
 
 int edp_set_push_kernel(edp_ctx* c, int32_t kind)
 {
-    if (!c || kind < 0 || kind > 3) return edp_fail(c, EDP_ERR_ARG, "edp_set_push_kernel");
+    if (!c || kind < 0 || kind > 4) return edp_fail(c, EDP_ERR_ARG, "edp_set_push_kernel");
     c->push_kernel = kind;
     return EDP_OK;
 }
@@ -1419,9 +1481,10 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         }
         const unsigned gr = (unsigned)(a.n_chunks + a.tail_ctas);
         if (classic) {
-            if (fused) TRY((launch_classic_push<4, true>(c, variant, gr, a)));
-            else if (c->push_kernel == 3) TRY((launch_classic_push<2, false>(c, variant, gr, a)));
-            else TRY((launch_classic_push<4, false>(c, variant, gr, a)));
+            if (fused) TRY((launch_classic_push<4, true, false>(c, variant, gr, a)));
+            else if (c->push_kernel == 3) TRY((launch_classic_push<2, false, false>(c, variant, gr, a)));
+            else if (c->push_kernel == 4) TRY((launch_classic_push<4, false, true>(c, variant, gr, a)));
+            else TRY((launch_classic_push<4, false, false>(c, variant, gr, a)));
         }
         if (fused) TRY(edp_sort_finish(c, sp));   // the sorted arrays are the species' arrays from here on
         if (do_mcc) {

@@ -152,6 +152,8 @@ SIGNATURES = {
                            C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
     "edp_nn_flip_transpose": [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
     "edp_nn_error": [_I32],
+    "edp_nn_conv_select": [C.c_int32],
+    "edp_nn_wgrad_select": [C.c_int32],
     "edp_nn_conv3x3_wgrad": [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
                              C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],
     "edp_nn_pool": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p],

@@ -188,8 +188,9 @@ int edp_sort_particles(edp_ctx* ctx);
 /* No counterpart in the reference. Kernel of the mixed-precision push over the sorted particles: 0 one CTA per
  * sorted chunk, the threads load their particles (default); 1 persistent CTAs whose particle columns are streamed
  * into shared memory by bulk copies, 4 particles per thread, 2 stages in flight; 2 the same with 2 particles per
- * thread and 3 stages; 3 as 0 with 2 particles per thread (more resident warps). All give the same results; only
- * the speed differs. */
+ * thread and 3 stages; 3 as 0 with 2 particles per thread (more resident warps); 4 as 0 with each thread's next 4
+ * particles copied into shared memory by cp.async while it pushes the current ones. All give the same results;
+ * only the speed differs. */
 int edp_set_push_kernel(edp_ctx* ctx, int32_t kind);
 /* No counterpart in the reference. on = 1 (default): a periodic sort (every sort_every steps) is done by each
  * species' next push, which writes the pushed particles straight to their sorted slots (keys of their cells before
@@ -435,8 +436,16 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
 int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream);
 /* nonzero in *out when a bounded wait of the tensor-core convolution gave up since the last call (then cleared) */
 int edp_nn_error(int32_t* out);
+/* the forward kernel edp_nn_conv3x3_fwd uses (process-wide): 0 automatic (the persistent halo kernel for c_out of
+ * 32, 64 or 128 when the layer's weights fit in shared memory, 9 c_in c_out 2 <= 112 KiB, and it has at least 296
+ * patches of 8 x 16 pixels; else the tile kernel), 1 the tile kernel, 2 the halo kernel (EDP_ERR_ARG where it does
+ * not apply). No counterpart in the reference. */
+int edp_nn_conv_select(int32_t mode);
 int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
                          const void* dz, int32_t cout, float* dw, float* db, void* stream);
+/* the weight-gradient kernel edp_nn_conv3x3_wgrad uses (process-wide): 0 or 2 tcgen05 (default), 1 mma.sync.
+ * No counterpart in the reference. */
+int edp_nn_wgrad_select(int32_t mode);
 /* f x f average pooling (h, w: input size) and nearest f x upsampling (h, w: output size), f = 2 or 4 */
 int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream);
 int edp_nn_pool_bwd(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* dy, void* dx,

@@ -265,8 +265,8 @@ def test_subcycled_ions_match_oracle_cycle(tmp_path, precision):
 @pytest.mark.gpu
 @pytest.mark.parametrize("ion_emission", [False, True])
 def test_push_kernels_give_identical_states(tmp_path, ion_emission):
-    """The four kernels of the mixed push over the sorted chunks (one CTA per chunk with the threads' own loads, 4 or 2
-    particles per thread; the persistent streaming kernels whose particle columns arrive by bulk copies, 4 particles
+    """The five kernels of the mixed push over the sorted chunks (one CTA per chunk with the threads' own loads, 4 or 2
+    particles per thread, or 4 with each thread's next group copied ahead by cp.async; the persistent streaming kernels whose particle columns arrive by bulk copies, 4 particles
     per thread in 2 stages or 2 in 3 stages) give bit-identical particles, densities, wall hits and charge-exchange counts over 12 steps of the
     magnetised cycle with RCX (the id column in the stages) and, in the second case, ion-induced emission whose
     electrons join after the last sort (the unsorted tail). Particles born on the device take ids in the order of
@@ -275,7 +275,7 @@ def test_push_kernels_give_identical_states(tmp_path, ion_emission):
     kw = dict(ion_emission=(0.5, 0.0, 10000.0, 2.0)) if ion_emission else {}
     d = small_deck(tmp_path, "periodic", ncx=128, ncy=64, en_collisions=False, rcx=True, bx=86.6, by=50.0, **kw)
     out = []
-    for kind in (0, 1, 2, 3):
+    for kind in (0, 1, 2, 3, 4):
         with Simulation(d, precision=PREC_MIXED, sort_every=5, seed=13) as sim:
             sim._check(sim.lib.edp_set_push_kernel(sim.ctx, kind), "edp_set_push_kernel")
             n = 128 * 64 * 24

@@ -79,6 +79,81 @@ def test_conv_kernels_match_oracle(c1, c2, cout, n, h, w):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (64, 0, 64), (32, 0, 128)])
+@pytest.mark.parametrize("n,h,w", [(1, 23, 13), (2, 40, 36), (3, 150, 97)])
+def test_halo_conv_matches_oracle(c1, c2, cout, n, h, w):
+    """The persistent halo kernel (edp_nn_conv_select(2): 8 x 16-pixel patches, one 10 x 18 halo per 32-channel
+    chunk for all nine taps, resident weights, two tensor-memory accumulators) against the oracle, on images that do
+    not fill their last patch, concatenated inputs, and more patches than CTAs (each CTA takes several); then the
+    automatic choice gives the same output as the tile kernel within the BF16 rounding of both."""
+    lib = library()
+    rng = np.random.default_rng(7 * c1 + c2 + cout + h)
+    x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
+    x2 = O.bf16(rng.normal(0, 1, (n, h, w, c2))) if c2 else None
+    cin = c1 + c2
+    wt = O.bf16(rng.normal(0, 1.0 / np.sqrt(9 * cin), (cout, 9, cin)))
+    b = rng.normal(0, 0.1, cout).astype(np.float32).astype(np.float64)
+    xin = x1 if c2 == 0 else np.concatenate([x1, x2], axis=-1)
+    tx1, tx2, tw, tb = _bf(x1), (_bf(x2) if c2 else None), _bf(wt), _f32(b)
+    y = torch.full((n, h, w, cout), 7.0, device="cuda", dtype=torch.bfloat16)
+    try:
+        assert lib.edp_nn_conv_select(2) == 0
+        for relu in (0, 1):
+            assert lib.edp_nn_conv3x3_fwd(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tw), _p(tb), cout, relu, _p(y),
+                                          _stream()) == 0
+            ref = O.conv_fwd(xin, wt, b, relu=bool(relu))
+            assert _rel(_np(y), ref) < 8e-3   # BF16 output rounding
+        flag = C.c_int32(-1)
+        assert lib.edp_nn_error(C.byref(flag)) == 0 and flag.value == 0
+        y1 = torch.empty_like(y)
+        assert lib.edp_nn_conv_select(1) == 0
+        assert lib.edp_nn_conv3x3_fwd(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tw), _p(tb), cout, 1, _p(y1),
+                                      _stream()) == 0
+        assert _rel(_np(y1), _np(y)) < 8e-3
+    finally:
+        lib.edp_nn_conv_select(0)
+    # a layer whose weights do not fit is refused when the halo kernel is forced
+    assert lib.edp_nn_conv_select(2) == 0
+    try:
+        big = torch.empty((256, 9, 256), device="cuda", dtype=torch.bfloat16)
+        assert lib.edp_nn_conv3x3_fwd(n, h, w, _p(tx1), 256, None, 0, _p(big), None, 128, 0, _p(y), _stream()) != 0
+    finally:
+        lib.edp_nn_conv_select(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (128, 64, 128), (64, 0, 96)])
+@pytest.mark.parametrize("n,h,w", [(1, 9, 9), (3, 150, 97)])
+def test_wgrad_kernels_match_oracle(c1, c2, cout, n, h, w):
+    """The weight gradient on tcgen05 (edp_nn_wgrad_select(0): 8 x 16-pixel patches as the K dimension, the nine
+    taps' accumulators in tensor memory, M = 64 output channels with zero rows past c_out, or 128) and on mma.sync
+    (select 1) against the oracle, accumulated onto a nonzero dw, with more patches than CTAs."""
+    lib = library()
+    rng = np.random.default_rng(5 * c1 + c2 + cout + h)
+    x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
+    x2 = O.bf16(rng.normal(0, 1, (n, h, w, c2))) if c2 else None
+    cin = c1 + c2
+    xin = x1 if c2 == 0 else np.concatenate([x1, x2], axis=-1)
+    dz = O.bf16(rng.normal(0, 1, (n, h, w, cout)))
+    tx1, tx2, tdz = _bf(x1), (_bf(x2) if c2 else None), _bf(dz)
+    w0 = rng.normal(0, 1, (cout, 9, cin)).astype(np.float32)
+    rw, rb = O.conv_wgrad(xin, dz)
+    try:
+        for mode in (0, 1):
+            assert lib.edp_nn_wgrad_select(mode) == 0
+            dw = _f32(w0)
+            db = torch.zeros(cout, device="cuda", dtype=torch.float32)
+            assert lib.edp_nn_conv3x3_wgrad(n, h, w, _p(tx1), c1, _p(tx2), c2, _p(tdz), cout, _p(dw), _p(db),
+                                            _stream()) == 0
+            assert _rel(_np(dw) - w0, rw) < 1e-5, mode
+            assert _rel(_np(db), rb) < 1e-5
+    finally:
+        lib.edp_nn_wgrad_select(0)
+    flag = C.c_int32(-1)
+    assert lib.edp_nn_error(C.byref(flag)) == 0 and flag.value == 0
+
+
+@pytest.mark.gpu
 def test_glue_kernels_match_oracle():
     lib = library()
     rng = np.random.default_rng(5)
