@@ -720,7 +720,7 @@ int edp_destroy(edp_ctx* c)
             if (g) cudaGraphExecDestroy(g);
     edp_mg_free(c);
     edp_warmstart_free(c);
-    F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v); F(c->maxwell_inj); F(c->emit_dev);
+    F(c->mcc_prob); F(c->mcc_energy); F(c->maxwell_v); F(c->maxwell_inj); F(c->emit_dev); F(c->inject_cells);
     delete c->emit_h;
     delete c->see_h;
     F(c->see_dev);
@@ -1156,15 +1156,83 @@ int edp_set_electron_emission(edp_ctx* c, int32_t wall, const edp_see_params* sp
     return EDP_OK;
 }
 
+// Covered cells of the sides of inner object n (pic2d_CurProblemValues.f90:603-683): a cell of a side is covered when
+// a domain wall's segment lies on it or another inner object touches or overlaps it. Side m = 1 left, 2 top, 3 right,
+// 4 bottom; cells along the side from its start (jbottom or ileft). The domain walls are the segments j = 0 and
+// j = ncy for all i, and, on a walled domain, i = 0 and i = ncx for all j.
+static std::vector<char> inner_side_covered(const edp_ctx* c, int n, int m)
+{
+    const edp_kparams& k = c->kp;
+    const bool vertical = m == 1 || m == 3;
+    const int at = m == 1 ? k.ileft[n] : m == 3 ? k.iright[n] : m == 2 ? k.jtop[n] : k.jbottom[n];
+    const int a0 = vertical ? k.jbottom[n] : k.ileft[n], a1 = vertical ? k.jtop[n] : k.iright[n];
+    std::vector<char> cov(std::max(0, a1 - a0), 0);
+    for (int q = a0; q < a1; ++q) {
+        bool c1 = false;
+        if (vertical) c1 = !c->p.periodic_x && (at == 0 || at == k.ncx) && q >= 0 && q < k.ncy;
+        else c1 = (at == 0 || at == k.ncy);
+        for (int o = 0; o < k.n_inner && !c1; ++o) {
+            if (o == n) continue;
+            if (vertical) c1 = at >= k.ileft[o] && at <= k.iright[o] && q >= k.jbottom[o] && q < k.jtop[o];
+            else c1 = at >= k.jbottom[o] && at <= k.jtop[o] && q >= k.ileft[o] && q < k.iright[o];
+        }
+        cov[q - a0] = c1;
+    }
+    return cov;
+}
+
+// The emitting sides of inner object n for N macroparticles per step (PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS,
+// pic2d_Setup.f90:1005-1591, one cluster over the domain): a side inside the domain emits
+// REAL(N) * REAL(open) / REAL(L) per step, `open` its cells not covered inside [cross_min, cross_max), L the open
+// cells of all four sides; the open cells are listed for the placement.
+static int inner_injection_sides(edp_ctx* c, int n, double n_emit, std::vector<int>* cells)
+{
+    const edp_kparams& k = c->kp;
+    edp_inject_dev& in = c->inject;
+    const int xmax_idx = c->p.periodic_x ? k.ncx + 1 : k.ncx;   // c_indx_x_max of the one cluster
+    const int ymax_idx = k.ncy;
+    std::vector<char> cov[4];
+    int L = 0;
+    for (int m = 1; m <= 4; ++m) {
+        cov[m - 1] = inner_side_covered(c, n, m);
+        for (char v : cov[m - 1]) L += !v;
+    }
+    for (int m = 1; m <= 4; ++m) {
+        const int s = 4 * n + (m - 1);
+        in.side_n[s] = 0.0;
+        in.side_open[s] = 0;
+        const bool vertical = m == 1 || m == 3;
+        const int at = m == 1 ? k.ileft[n] : m == 3 ? k.iright[n] : m == 2 ? k.jtop[n] : k.jbottom[n];
+        const int a0 = vertical ? k.jbottom[n] : k.ileft[n], a1 = vertical ? k.jtop[n] : k.iright[n];
+        const int lim = vertical ? xmax_idx : ymax_idx;       // the side must lie strictly inside the cluster
+        const int alim = vertical ? ymax_idx : xmax_idx;
+        if (!(n_emit > 0.0) || L == 0 || !(at > 0 && at < lim) || !(a0 < alim && a1 > 0)) continue;
+        const int cmin = std::max(a0, 0), cmax = std::min(a1, alim - 1);
+        in.side_off[s] = (int)cells->size();
+        for (int q = cmin; q < cmax; ++q)
+            if (!cov[m - 1][q - a0]) cells->push_back(q);
+        const int open = (int)cells->size() - in.side_off[s];
+        if (open == 0) continue;
+        in.side_open[s] = open;
+        in.side_cmin[s] = cmin;
+        in.side_cmax[s] = cmax;
+        in.side_at[s] = (m == 1 || m == 4) ? (double)at - 1.0e-6 : (double)at + 1.0e-6;
+        in.side_n[s] = (double)((float)n_emit * (float)open / (float)L);   // single precision, as the reference
+    }
+    return EDP_OK;
+}
+
 int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t model, double t_normal_ev,
                            double t_parallel_ev, double beam_energy_ev)
 {
     if (c && c->kp.strip) return edp_fail(c, EDP_ERR_STATE, "no wall emission on a strip");
-    if (!c || wall < 0 || wall > 3 || !(n_per_step >= 0.0) || n_per_step > 1.0e9 || model < 0 || model > 1 ||
-        !(t_normal_ev >= 0.0) || !(t_parallel_ev >= 0.0))
+    if (!c || wall < 0 || wall >= 4 + c->p.n_inner || !(n_per_step >= 0.0) || n_per_step > 1.0e9 || model < 0 ||
+        model > 1 || !(t_normal_ev >= 0.0) || !(t_parallel_ev >= 0.0))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection");
-    if (c->p.periodic_x && wall >= 2 && n_per_step > 0.0)
+    if (c->p.periodic_x && (wall == 2 || wall == 3) && n_per_step > 0.0)
         return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection: a periodic domain has walls below and above only");
+    if (wall >= 4 && c->p.inner_eps[wall - 4] > 0.0 && n_per_step > 0.0)
+        return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection: only metal inner objects emit");
     if (model == 1 && n_per_step > 0.0 && !(beam_energy_ev > 1.5 * t_normal_ev))
         return edp_fail(c, EDP_ERR_ARG, "edp_set_wall_injection: beam energy spread above the beam energy / 1.5");
     TRY(wall_state(c));
@@ -1185,8 +1253,18 @@ int edp_set_wall_injection(edp_ctx* c, int32_t wall, double n_per_step, int32_t 
         in.fn[wall] = n_per_step > 0.0 ? std::sqrt(0.25 * t_normal_ev * t_normal_ev / (beam_energy_ev * ef)) : 0.0;
         in.vb[wall] = std::sqrt(std::max(beam_energy_ev, 0.0) / ef);
     }
+    // the sides of all emitting inner objects, listed again
+    std::vector<int> cells;
+    for (int n = 0; n < c->p.n_inner; ++n) TRY(inner_injection_sides(c, n, in.n[4 + n], &cells));
+    if (cells.size() > EDP_INJECT_MAX_CELLS) return edp_fail(c, EDP_ERR_CAPACITY, "edp_set_wall_injection: sides");
+    if (!cells.empty()) {
+        if (!c->inject_cells) TRY(dalloc(c, &c->inject_cells, EDP_INJECT_MAX_CELLS));
+        EDP_CUDA(c, cudaMemcpy(c->inject_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    in.open_cells = c->inject_cells;
     c->inject_on = 0;
     for (int w = 0; w < 4; ++w) c->inject_on |= in.n[w] > 0.0;
+    for (int s = 0; s < EDP_INJECT_SIDES; ++s) c->inject_on |= in.side_n[s] > 0.0;
     return EDP_OK;
 }
 

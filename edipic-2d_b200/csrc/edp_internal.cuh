@@ -108,11 +108,21 @@ struct edp_emit_dev;    // ion-induced electron emission parameters (below)
 struct edp_see_dev;     // electron-induced electron emission parameters (below)
 
 // constant electron emission of the four domain walls (PERFORM_ELECTRON_EMISSION_SETUP), code units
+// sides of the inner objects that emit: side 4 n + (m - 1) of inner object n, m = 1 left, 2 top, 3 right, 4 bottom
+// (the segment numbers of PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS)
+#define EDP_INJECT_SIDES (4 * EDP_MAX_INNER)
+#define EDP_INJECT_MAX_CELLS 65536   // open cells over all sides
 struct edp_inject_dev {
-    double n[4];           // N_electron_constant_emit, macroparticles per step
-    int model[4];          // 0 thermal, 1 beam
-    double fn[4], fp[4];   // factor_convert_vinj_normal/parallel_constant_emit
-    double vb[4];          // v_ebeam_constant_emit
+    double n[EDP_N_HIT_COUNTERS];       // walls: N_electron_constant_emit, macroparticles per step
+    int model[EDP_N_HIT_COUNTERS];      // 0 thermal, 1 beam (walls, then inner objects)
+    double fn[EDP_N_HIT_COUNTERS], fp[EDP_N_HIT_COUNTERS];   // factor_convert_vinj_normal/parallel_constant_emit
+    double vb[EDP_N_HIT_COUNTERS];      // v_ebeam_constant_emit
+    double side_n[EDP_INJECT_SIDES];    // inner objects: macroparticles per step from the side (0: none)
+    double side_at[EDP_INJECT_SIDES];   // X (sides 1, 3) or Y (2, 4) of the emitted electrons, 1e-6 outside
+    int side_open[EDP_INJECT_SIDES];    // open (not covered) cells of the side in [cmin, cmax)
+    int side_off[EDP_INJECT_SIDES];     // their first entry in open_cells
+    int side_cmin[EDP_INJECT_SIDES], side_cmax[EDP_INJECT_SIDES];   // cross_j/i_min, cross_j/i_max
+    const int* open_cells;              // cell index along the side (j for sides 1, 3; i for 2, 4), by side
     const double* maxwell_v;
     const double* maxwell_inj;
     int rmax, rmax_inj;
@@ -226,6 +236,7 @@ struct edp_ctx {
     edp_inject_dev inject{};          // constant electron emission (by value into the kernel)
     int inject_on = 0;
     double* maxwell_inj = nullptr;    // GetInjMaxwellVelocity table on the device
+    int* inject_cells = nullptr;      // open cells of the emitting sides of inner objects (edp_inject_dev)
     int32_t last_ws_used = 0;         // the last CG solve started from the network's guess
     // wall time of learned-start solves (the network ran) and of previous-start ones, running averages in seconds
     // (negative: none yet), and the learned-start calls so far: the network runs while it pays, and is re-tried on
@@ -535,8 +546,21 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev* m, uint32_t id
 
 // PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:90-121) for one ion; true on exchange.
 // The test r <= sqrt(P^2 + P_th^2), P = n dt N_sub |v| V_scale sigma(E), is evaluated as r^2 <= P^2 + P_th^2.
+// the same with the decision word w0 (word 0 of Philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id)) drawn by the
+// caller, so that a thread can draw for several ions at once
+__device__ __forceinline__ bool edp_rcx_ion_drawn(const edp_rcx_dev& r, uint32_t w0, uint32_t id, uint32_t step,
+                                                  uint32_t species, uint32_t seed_lo, uint32_t seed_hi, double& vx,
+                                                  double& vy, double& vz);
 __device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, uint32_t step, uint32_t species,
                                             uint32_t seed_lo, uint32_t seed_hi, double& vx, double& vy, double& vz)
+{
+    uint32_t w[2];
+    edp_philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id, w);
+    return edp_rcx_ion_drawn(r, w[0], id, step, species, seed_lo, seed_hi, vx, vy, vz);
+}
+__device__ __forceinline__ bool edp_rcx_ion_drawn(const edp_rcx_dev& r, uint32_t w0, uint32_t id, uint32_t step,
+                                                  uint32_t species, uint32_t seed_lo, uint32_t seed_hi, double& vx,
+                                                  double& vy, double& vz)
 {
     double vsq = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
     double k2 = r.k2;
@@ -546,9 +570,7 @@ __device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, u
         k2 = __dmul_rn(k, k);
     }
     double p2 = __dadd_rn(__dmul_rn(k2, vsq), r.pth2);
-    uint32_t w[2];
-    edp_philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id, w);
-    double u = edp_u01(w[0]);
+    double u = edp_u01(w0);
     if (!(__dmul_rn(u, u) <= p2)) return false;
     uint32_t b[4];
     edp_philox(step, EDP_STREAM_RCX(species), 1u, seed_hi, id, seed_lo, b);

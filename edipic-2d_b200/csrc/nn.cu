@@ -16,6 +16,9 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <mutex>
+#include <vector>
+
 namespace {
 
 typedef __nv_bfloat16 bf16;
@@ -107,6 +110,7 @@ struct TmaArgs {
     const float* bias;
     bf16* y;
     int* err;
+    float* ws;   // split K (gridDim.z slices): FP32 partial sums [P][cout] added here, finished by conv_finish_kernel
 };
 
 template <int BN, int CW>
@@ -132,7 +136,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int x0 = tx * 16, y0 = ty * 8;
     const int n0 = blockIdx.y * BN;
     const int cin = ta.c1 + ta.c2;
-    const int KT = 9 * cin / CW;
+    // K slice of this CTA (the whole K range unless the layer is split over gridDim.z slices)
+    const int KT_all = 9 * cin / CW;
+    const int kbeg = (int)(((int64_t)blockIdx.z * KT_all) / gridDim.z);
+    const int KT = (int)(((int64_t)(blockIdx.z + 1) * KT_all) / gridDim.z) - kbeg;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         auto issue = [&](int kt) {
             const int s = kt % STAGES;
             const uint32_t As = base + s * STAGE, Bs = As + A_BYTES, fb = smem_u32(&full[s]);
-            const int k0 = kt * CW, tap = k0 / cin, ci = k0 - tap * cin;
+            const int k0 = (kbeg + kt) * CW, tap = k0 / cin, ci = k0 - tap * cin;
             const int xx = x0 + tap % 3 - 1, yy = y0 + tap / 3 - 1;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(STAGE) : "memory");
             const CUtensorMap* ma = ci < ta.c1 ? &mx1 : &mx2;
@@ -222,7 +229,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                            "=r"(v[14]), "=r"(v[15])
                          : "r"(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            if (inside) {
+            if (inside && ta.ws) {
+                float* d = ta.ws + p * ta.cout + n0 + c0;
+                for (int q = 0; q < 16; q += 4)
+                    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n"
+                                 ::"l"(d + q), "f"(__uint_as_float(v[q])), "f"(__uint_as_float(v[q + 1])),
+                                   "f"(__uint_as_float(v[q + 2])), "f"(__uint_as_float(v[q + 3]))
+                                 : "memory");
+            } else if (inside) {
                 uint32_t pk[8];
                 for (int q = 0; q < 8; ++q) {
                     const int n = n0 + c0 + 2 * q;
@@ -272,6 +286,8 @@ constexpr int kHaloStages = 4;
 constexpr int kHaloPlane = 2912;                      // 182 pixel slots of 16 bytes (180 used)
 constexpr int kHaloStage = 4 * kHaloPlane;            // one 32-channel chunk
 constexpr int kHaloMaxWeights = 112 * 1024;           // largest resident weight set (9 x c_in x c_out x 2 bytes)
+template <int BN>
+constexpr int kHaloAcc = BN == 32 ? 3 : BN == 64 ? 2 : 1;   // partial accumulators per tile
 
 struct HaloArgs {
     const bf16* x1;
@@ -301,7 +317,10 @@ template <int BN>
 __global__ void __launch_bounds__(kHaloThreads, 1)
     conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, HaloArgs a)
 {
-    constexpr uint32_t TMEM_COLS = BN <= 32 ? 64 : BN <= 64 ? 128 : 256;   // two accumulators
+    // NACC partial accumulators per tile (tap % NACC), summed in the epilogue: consecutive MMAs of the short (small N)
+    // chains go to independent accumulators; two tiles' sets of them (double buffering) in 256 columns
+    constexpr int NACC = kHaloAcc<BN>;
+    constexpr uint32_t TMEM_COLS = 256;
     constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
     // A: no swizzle, LBO = one plane (K direction), SBO = one halo row of 10 pixels (M direction)
     constexpr uint64_t DESC_A = ((uint64_t)(160 >> 4) << 32) | ((uint64_t)(kHaloPlane >> 4) << 16) | ((uint64_t)1 << 46);
@@ -389,7 +408,7 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
                 if (tl >= 2 && !mbar_wait_or_fail(smem_u32(&acc_empty[buf]), (uint32_t)(((tl >> 1) - 1) & 1), &fail_sh))
                     break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const uint32_t acc = tmem + (uint32_t)(buf * BN);
+                const uint32_t acc = tmem + (uint32_t)(buf * NACC * BN);
                 for (int cc = 0; cc < n_chunks; ++cc, ++it) {
                     const int s = (int)(it % kHaloStages);
                     if (!mbar_wait_or_fail(smem_u32(&full[s]), (uint32_t)((it / kHaloStages) & 1), &fail_sh)) {
@@ -400,16 +419,17 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
                     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                     const uint32_t As = hbase + (uint32_t)(s * kHaloStage);
-                    for (int tap = 0; tap < 9; ++tap) {
-                        const uint32_t a0 = As + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
-                        const uint32_t b0 = wbase + (uint32_t)((tap * n_chunks + cc) * B_CHUNK);
-                        for (int ks = 0; ks < 2; ++ks) {
+                    for (int ks = 0; ks < 2; ++ks) {
+                        for (int tap = 0; tap < 9; ++tap) {
+                            const uint32_t a0 = As + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
+                            const uint32_t b0 = wbase + (uint32_t)((tap * n_chunks + cc) * B_CHUNK);
                             const uint64_t da = DESC_A | (uint64_t)(((a0 + (uint32_t)(2 * ks * kHaloPlane)) >> 4) & 0x3FFFu);
                             const uint64_t db = DESC_B | (uint64_t)(((b0 + 32u * ks) >> 4) & 0x3FFFu);
-                            const uint32_t accum = (cc > 0 || tap > 0 || ks > 0) ? 1u : 0u;
+                            const uint32_t accum = (cc > 0 || ks > 0 || tap >= NACC) ? 1u : 0u;
                             asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                                          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-                                         ::"r"(acc), "l"(da), "l"(db), "r"(IDESC), "r"(accum));
+                                         ::"r"(acc + (uint32_t)((tap % NACC) * BN)), "l"(da), "l"(db), "r"(IDESC),
+                                           "r"(accum));
                         }
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
@@ -445,20 +465,28 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
             const int64_t p = ((int64_t)img * a.h + py) * a.w + px;
 #pragma unroll
             for (int c0 = 0; c0 < BN; c0 += 16) {
-                uint32_t v[16];
-                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
-                             " [%16];\n"
-                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                               "=r"(v[14]), "=r"(v[15])
-                             : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN + c0)));
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                float f[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) f[k] = 0.0f;
+#pragma unroll
+                for (int j = 0; j < NACC; ++j) {
+                    uint32_t v[16];
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                                 " [%16];\n"
+                                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                                   "=r"(v[14]), "=r"(v[15])
+                                 : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * NACC + j) * BN + c0)));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) f[k] += __uint_as_float(v[k]);
+                }
                 if (inside) {
                     uint32_t pk[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        float v0 = __uint_as_float(v[2 * k]) + (a.bias ? __ldg(a.bias + c0 + 2 * k) : 0.0f);
-                        float v1 = __uint_as_float(v[2 * k + 1]) + (a.bias ? __ldg(a.bias + c0 + 2 * k + 1) : 0.0f);
+                        float v0 = f[2 * k] + (a.bias ? __ldg(a.bias + c0 + 2 * k) : 0.0f);
+                        float v1 = f[2 * k + 1] + (a.bias ? __ldg(a.bias + c0 + 2 * k + 1) : 0.0f);
                         if (a.relu) {
                             v0 = fmaxf(v0, 0.0f);
                             v1 = fmaxf(v1, 0.0f);
@@ -483,6 +511,67 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
     }
+}
+
+// y = act(ws + bias) in BF16 for the split-K path, and ws back to zero for the next layer; 4 channels per thread
+__global__ void conv_finish_kernel(float* __restrict__ ws, int64_t n4, int cout, const float* __restrict__ bias,
+                                   int relu, bf16* __restrict__ y)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 v = reinterpret_cast<float4*>(ws)[i];
+        reinterpret_cast<float4*>(ws)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int n = (int)((4 * i) % cout);
+        if (bias) {
+            v.x += bias[n];
+            v.y += bias[n + 1];
+            v.z += bias[n + 2];
+            v.w += bias[n + 3];
+        }
+        if (relu) {
+            v.x = fmaxf(v.x, 0.f);
+            v.y = fmaxf(v.y, 0.f);
+            v.z = fmaxf(v.z, 0.f);
+            v.w = fmaxf(v.w, 0.f);
+        }
+        __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        reinterpret_cast<uint2*>(y)[i] = make_uint2(*reinterpret_cast<uint32_t*>(&a), *reinterpret_cast<uint32_t*>(&b));
+    }
+}
+
+// FP32 workspace of the split-K path, one per (device, stream), kept zeroed between layers (conv_finish_kernel
+// clears what it read). Grown on demand: the old buffer is freed after the stream has finished with it.
+float* splitk_workspace(cudaStream_t s, size_t bytes)
+{
+    struct Ws {
+        int dev;
+        cudaStream_t stream;
+        float* p;
+        size_t bytes;
+    };
+    static std::mutex mu;
+    static std::vector<Ws> all;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    Ws* w = nullptr;
+    for (auto& x : all)
+        if (x.dev == dev && x.stream == s) w = &x;
+    if (!w) {
+        all.push_back({dev, s, nullptr, 0});
+        w = &all.back();
+    }
+    if (w->bytes < bytes) {
+        if (w->p) {
+            if (cudaStreamSynchronize(s) != cudaSuccess) return nullptr;
+            cudaFree(w->p);
+            w->p = nullptr;
+            w->bytes = 0;
+        }
+        if (cudaMalloc(&w->p, bytes) != cudaSuccess) return nullptr;
+        if (cudaMemsetAsync(w->p, 0, bytes, s) != cudaSuccess) return nullptr;
+        w->bytes = bytes;
+    }
+    return w->p;
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -564,8 +653,30 @@ int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
     ta.bias = c.bias;
     ta.y = c.y;
     ta.err = err;
-    dim3 grid((unsigned)(ta.tiles_x * ta.tiles_y * c.nimg), c.cout / BN);
+    ta.ws = nullptr;
+    const int64_t ctas = (int64_t)ta.tiles_x * ta.tiles_y * c.nimg * (c.cout / BN);
+    // a layer with fewer than two CTAs per SM splits its K range (taps x channel chunks, at least two chunks per
+    // slice) over more CTAs, whose FP32 partial sums meet in a workspace
+    const int kt_all = 9 * (c.c1 + c.c2) / CW;
+    int ks = 1;
+    if (ctas < 2 * 148) {
+        ks = (int)((2 * 148 + ctas - 1) / ctas);
+        if (ks > kt_all / 2) ks = kt_all / 2;
+        if (ks < 1) ks = 1;
+    }
+    const int64_t P = (int64_t)c.nimg * c.h * c.w;
+    if (ks > 1) {
+        ta.ws = splitk_workspace(s, (size_t)P * c.cout * sizeof(float));
+        if (!ta.ws) return EDP_ERR_CUDA;
+    }
+    dim3 grid((unsigned)(ta.tiles_x * ta.tiles_y * c.nimg), c.cout / BN, (unsigned)ks);
     conv3x3_fwd_tma_kernel<BN, CW><<<grid, kTcThreads, SMEM, s>>>(m1, m2, mw, ta);
+    if (ks > 1) {
+        const int64_t n4 = P * c.cout / 4;
+        int64_t g = (n4 + 255) / 256;
+        if (g > 148 * 8) g = 148 * 8;
+        conv_finish_kernel<<<(unsigned)g, 256, 0, s>>>(ta.ws, n4, c.cout, c.bias, c.relu, c.y);
+    }
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
@@ -596,7 +707,9 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
     if (configured[dev] < smem) {
         if (cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess)
+                cudaSuccess ||
+            cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+                cudaSuccess)
             return EDP_ERR_CUDA;
         configured[dev] = smem;
     }
@@ -618,13 +731,13 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
     a.bias = c.bias;
     a.y = c.y;
     a.err = err;
-    int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_fwd_halo_kernel<BN>, kHaloThreads, smem) !=
-            cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    int sms = 0, smem_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
         return EDP_ERR_CUDA;
-    const int tmem_cols = BN <= 32 ? 64 : BN <= 64 ? 128 : 256;
-    if (per_sm > 512 / tmem_cols) per_sm = 512 / tmem_cols;
+    // CTAs per SM: shared memory (1 KiB per CTA reserved by the driver) and 256 tensor-memory columns per CTA
+    int per_sm = smem_sm / (smem + 1024);
+    if (per_sm > 2) per_sm = 2;
     if (per_sm < 1) per_sm = 1;
     const int64_t grid = a.n_tiles < (int64_t)sms * per_sm ? a.n_tiles : (int64_t)sms * per_sm;
     conv3x3_fwd_halo_kernel<BN><<<(unsigned)grid, kHaloThreads, smem, s>>>(mw, a);
@@ -886,10 +999,12 @@ __global__ void __launch_bounds__(kHaloThreads, 1) conv3x3_wgrad_tc_kernel(Wgrad
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t As = base + (uint32_t)(s * STAGE), Hs = As + (uint32_t)(NP * kDzPlane);
-                for (int tap = 0; tap < 9; ++tap) {
-                    const uint32_t b0 = Hs + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
-                    for (int ks = 0; ks < 8; ++ks) {
-                        const uint64_t da = DESC_A | (uint64_t)(((As + (uint32_t)(256 * ks)) >> 4) & 0x3FFFu);
+                // K steps outside, taps inside: consecutive MMAs go to the nine independent accumulators, so that
+                // none waits for the one before it
+                for (int ks = 0; ks < 8; ++ks) {
+                    const uint64_t da = DESC_A | (uint64_t)(((As + (uint32_t)(256 * ks)) >> 4) & 0x3FFFu);
+                    for (int tap = 0; tap < 9; ++tap) {
+                        const uint32_t b0 = Hs + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
                         const uint64_t db = DESC_B | (uint64_t)(((b0 + (uint32_t)(320 * ks)) >> 4) & 0x3FFFu);
                         const uint32_t accum = (it > 0 || ks > 0) ? 1u : 0u;
                         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"

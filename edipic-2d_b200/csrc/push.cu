@@ -171,10 +171,20 @@ __device__ __forceinline__ long long fix_round(double x)
 
 // One particle. Returns false when it was absorbed (the caller stores cell = -1).
 // ION: ion species (acc_E, RCX) instead of electrons (E, MCC selection); PER: periodic x; ROT: Boris rotation.
+// The collision decision word of one particle: word 0 of its Philox2x32 draw keyed by (id, step) for MCC selection
+// (electrons) or charge exchange (ions). Independent of the push, so a thread draws for all its particles at once.
+template <bool ION>
+__device__ __forceinline__ uint32_t push_draw(const PushArgs& a, uint32_t id)
+{
+    uint32_t w[2];
+    edp_philox2x32(a.step, a.kp.seed_lo ^ (ION ? EDP_SEL_RCX((uint32_t)(a.species - 1)) : EDP_SEL_MCC), id, w);
+    return w[0];
+}
+
 template <bool ION, bool PER, bool ROT>
 __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, DepAcc& acc,
                                          int& cell, float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id,
-                                         bool& selected)
+                                         uint32_t draw, bool& selected)
 {
     const edp_kparams& kp = a.kp;
     int i = cell & 0xFFFF, j = cell >> 16;
@@ -319,13 +329,11 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         atomicAdd(&a.rho[r1 + i1], (unsigned long long)q11);
     }
     // ---- collisions in the epilogue, with the variates of the separate passes
-    if (!ION && a.do_coll) {
-        double r;
-        selected = edp_mcc_select(a.mcc, id, a.step, kp.seed_lo, kp.seed_hi, r);
-    }
+    if (!ION && a.do_coll) selected = (unsigned long long)draw < a.mcc->pmax_x;   // as edp_mcc_select
     if (ION && a.do_coll) {
         double dvx = vx, dvy = vy, dvz = vz;
-        if (edp_rcx_ion(a.rcx, id, a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, dvx, dvy, dvz)) {
+        if (edp_rcx_ion_drawn(a.rcx, draw, id, a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, dvx, dvy,
+                              dvz)) {
             vx = (float)dvx;
             vy = (float)dvy;
             vz = (float)dvz;
@@ -363,13 +371,17 @@ __device__ __forceinline__ void push_group_body(const PushArgs& a, Smem& s, int 
 {
     const int64_t base = g * IPT;
     bool sel[IPT];
+    // the decision draws first, for all particles of the thread: independent Philox chains that overlap
+    uint32_t draw[IPT];
+#pragma unroll
+    for (int e = 0; e < IPT; ++e) draw[e] = a.do_coll ? push_draw<ION>(a, id[e]) : 0u;
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
     for (int e = 0; e < IPT; ++e) {
         sel[e] = false;
         if (c[e] < 0) continue;
-        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e], draw[e],
                                      sel[e])) {
             c[e] = -1;
             sel[e] = false;
@@ -528,7 +540,7 @@ __device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, i
         sel[e] = false;
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                     sel[e])) {
+                                     a.do_coll ? push_draw<ION>(a, id[e]) : 0u, sel[e])) {
             c[e] = -1;
             sel[e] = false;
             atomicAdd(&s.cnt[17], 1ull);
@@ -867,6 +879,7 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 3 : 4) push_strea
                 if (c[e] < 0) continue;
                 bool sel = false;
                 if (!push_one<ION, PER, ROT>(a, s, true, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                                             a.do_coll ? push_draw<ION>(a, id[e]) : 0u,
                                              sel)) {
                     c[e] = -1;
                     atomicAdd(&s.cnt[17], 1ull);
@@ -1675,18 +1688,21 @@ int edp_launch_electron_emission(edp_ctx* c)
     return EDP_OK;
 }
 
-// PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001) for one cluster over the domain: wall blockIdx.y emits
-// INT(n) electrons and one more with probability n - INT(n) (:627-690). Variates: Philox4x32-10, key {EDP_INJECT_KEY
-// + wall, seed_lo}, counter {step, EDP_STREAM_INJECT, block, seed_hi}; block 0 word 0 for the fraction, block 1 + e for
-// electron e: word 0 its place along the wall, word 1 the normal speed, words 2 and 3 the tangential components (the
-// one in the wall's plane of the domain, then z).
+// PERFORM_ELECTRON_EMISSION_SETUP (pic2d_Setup.f90:599-1001) for one cluster over the domain: wall blockIdx.y < 4
+// emits INT(n) electrons and one more with probability n - INT(n) (:627-690); PERFORM_ELECTRON_EMISSION_SETUP_INNER_
+// OBJECTS (:1005-1591): blockIdx.y = 4 + s for side s of an inner object, which emits INT(n_s) + Bernoulli electrons
+// spread uniformly over its open cells, 1e-6 outside the side, with the normal velocity pointing out. Variates:
+// Philox4x32-10, key {EDP_INJECT_KEY + blockIdx.y, seed_lo}, counter {step, EDP_STREAM_INJECT, block, seed_hi}; block
+// 0 word 0 for the fraction, block 1 + e for electron e: word 0 its place along the wall or side, word 1 the normal
+// speed, words 2 and 3 the tangential components (the one in the domain's plane, then z).
 __global__ void __launch_bounds__(256) wall_injection_kernel(edp_inject_dev in, edp_born born_e,
                                                              edp_dev_counters* dc, edp_kparams kp, uint32_t step)
 {
-    const int wall = blockIdx.y;
-    const double n = in.n[wall];
-    if (n <= 0.0) return;
-    const uint32_t key = EDP_INJECT_KEY + (uint32_t)wall;
+    const int y = blockIdx.y;
+    const int side = y - 4, obj = y < 4 ? y : 4 + side / 4, seg = side % 4 + 1;
+    const double n = y < 4 ? in.n[y] : in.side_n[side];
+    if (!(n > 0.0)) return;
+    const uint32_t key = EDP_INJECT_KEY + (uint32_t)y;
     int count = (int)n;
     uint32_t w0[4];
     edp_philox(step, EDP_STREAM_INJECT, 0u, kp.seed_hi, key, kp.seed_lo, w0);
@@ -1696,34 +1712,55 @@ __global__ void __launch_bounds__(256) wall_injection_kernel(edp_inject_dev in, 
         uint32_t w[4];
         edp_philox(step, EDP_STREAM_INJECT, 1u + (uint32_t)e, kp.seed_hi, key, kp.seed_lo, w);
         double vn;
-        if (in.model[wall] == 0) {
-            vn = edp_maxwell_inj(in.maxwell_inj, in.rmax_inj, edp_u01(w[1])) * in.fn[wall];
+        if (in.model[obj] == 0) {
+            vn = edp_maxwell_inj(in.maxwell_inj, in.rmax_inj, edp_u01(w[1])) * in.fn[obj];
         } else {
-            vn = fmax(0.0, in.vb[wall] + edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[1])) * in.fn[wall]);
+            vn = fmax(0.0, in.vb[obj] + edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[1])) * in.fn[obj]);
         }
-        const double t1 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[2])) * in.fp[wall];
-        const double t2 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[3])) * in.fp[wall];
+        const double t1 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[2])) * in.fp[obj];
+        const double t2 = edp_maxwell(in.maxwell_v, in.rmax, edp_u01(w[3])) * in.fp[obj];
         const double r = edp_u01(w[0]);
-        double x, y, v[3];
-        switch (wall) {
-        case 0: x = fmin(fmax(r * xmax, 0.0), xmax); y = 1.0e-6; v[0] = t1; v[1] = vn; v[2] = t2; break;
-        case 1: x = fmin(fmax(r * xmax, 0.0), xmax); y = ymax - 1.0e-6; v[0] = t1; v[1] = -vn; v[2] = t2; break;
-        case 2: x = 1.0e-6; y = fmin(fmax(r * ymax, 0.0), ymax); v[0] = vn; v[1] = t1; v[2] = t2; break;
-        default: x = xmax - 1.0e-6; y = fmin(fmax(r * ymax, 0.0), ymax); v[0] = -vn; v[1] = t1; v[2] = t2; break;
+        double x, yy, v[3];
+        if (y < 4) {
+            switch (y) {
+            case 0: x = fmin(fmax(r * xmax, 0.0), xmax); yy = 1.0e-6; v[0] = t1; v[1] = vn; v[2] = t2; break;
+            case 1: x = fmin(fmax(r * xmax, 0.0), xmax); yy = ymax - 1.0e-6; v[0] = t1; v[1] = -vn; v[2] = t2; break;
+            case 2: x = 1.0e-6; yy = fmin(fmax(r * ymax, 0.0), ymax); v[0] = vn; v[1] = t1; v[2] = t2; break;
+            default: x = xmax - 1.0e-6; yy = fmin(fmax(r * ymax, 0.0), ymax); v[0] = -vn; v[1] = t1; v[2] = t2; break;
+            }
+        } else {
+            // the place along the side: d = r (open - 1e-6) walks the open cells, a whole cell at a time
+            // (:1064-1078); d - k is exact, as the reference's k subtractions of 1 are
+            const int open = in.side_open[side];
+            double d = r * ((double)open - 1.0e-6);
+            int k = (int)d;
+            if (k > open - 1) k = open - 1;
+            d -= (double)k;
+            const double c0 = (double)in.open_cells[in.side_off[side] + k];
+            double t = fmax(c0, fmin(c0 + d, c0 + 1.0));
+            t = fmin(fmax(t, (double)in.side_cmin[side]), (double)in.side_cmax[side] - 1.0e-6);
+            const double at = in.side_at[side];
+            switch (seg) {
+            case 1: x = at; yy = t; v[0] = -vn; v[1] = t1; v[2] = t2; break;   // left: out along -x
+            case 3: x = at; yy = t; v[0] = vn; v[1] = t1; v[2] = t2; break;    // right
+            case 2: x = t; yy = at; v[0] = t1; v[1] = vn; v[2] = t2; break;    // top
+            default: x = t; yy = at; v[0] = t1; v[1] = -vn; v[2] = t2; break;  // bottom
+            }
         }
-        record_born(born_e, &dc->born_e_count, &dc->error_flags, x, y, v);
+        record_born(born_e, &dc->born_e_count, &dc->error_flags, x, yy, v);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&dc->e_emit[wall], (unsigned long long)count);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&dc->e_emit[obj], (unsigned long long)count);
 }
 
 int edp_launch_wall_injection(edp_ctx* c)
 {
     double nmax = 0.0;
     for (int w = 0; w < 4; ++w) nmax = std::max(nmax, c->inject.n[w]);
+    for (int s = 0; s < EDP_INJECT_SIDES; ++s) nmax = std::max(nmax, c->inject.side_n[s]);
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(((int64_t)nmax + 256) / 256, 148));
     ++c->launches;
-    wall_injection_kernel<<<dim3((unsigned)blocks, 4), 256, 0, c->stream>>>(c->inject, c->born_e, c->dc, c->kp,
-                                                                           (uint32_t)c->t_cntr);
+    wall_injection_kernel<<<dim3((unsigned)blocks, 4 + EDP_INJECT_SIDES), 256, 0, c->stream>>>(
+        c->inject, c->born_e, c->dc, c->kp, (uint32_t)c->t_cntr);
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;
 }

@@ -69,7 +69,7 @@ class Deck:
         self.ion_emission = {}
         self.ion_wall_model = [0, 0, 0, 0]   # 0 absorb, 1 reflect, 2 ion-induced emission; walls, then inner objects
         self.electron_emission = {}           # {wall: SeeParams} of the walls whose material emits electrons
-        self.wall_injection = {}              # {wall: (N per step, model, T_normal, T_parallel, W_beam)}
+        self.wall_injection = {}              # {object: (N per step, model, T_normal, T_parallel, W_beam)}
         buf = (C.c_double * 4)()
         model = C.c_int32()
         for wall in range(4):
@@ -93,6 +93,11 @@ class Deck:
             see, on = _abi.SeeParams(), C.c_int32()
             if self.lib.edp_deck_electron_emission(self.handle, obj, C.byref(see), C.byref(on)) == 0 and on.value:
                 self.electron_emission[obj] = see
+            # constant electron emission: metal inner objects only (PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS)
+            inj = (C.c_double * 5)()
+            if (self.params.inner_eps[obj - 4] == 0.0 and self.lib.edp_deck_wall_injection(self.handle, obj, inj) == 0
+                    and inj[0] > 0.0):
+                self.wall_injection[obj] = (inj[0], int(inj[1]), inj[2], inj[3], inj[4])
             for s in range(1, self.params.n_ion_species + 1):
                 if self.lib.edp_deck_ion_emission(self.handle, obj, s, buf) == 0 and buf[0] > 0.0:
                     self.ion_emission[(obj, s)] = tuple(buf)

@@ -72,8 +72,8 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
     (the wall material METAL1), False for none, None for the configuration's default. ion_reflection: the walls
     reflect all ions specularly instead (ion-material model 1). electron_emission: fields of edp_see_params (models
     and parameters of electron-induced emission, energies in eV) for the walls' material; all models off by default.
-    wall_injection: {wall (0 below, 1 above, 2 left, 3 right): (electrons per step, model, T_normal, T_parallel,
-    beam energy [eV])}, the constant electron emission of init_bo_NN.dat. ez: uniform Z electric field [V/cm];
+    wall_injection: {wall (0 below, 1 above, 2 left, 3 right; 4 + n metal inner object n): (electrons per step, model,
+    T_normal, T_parallel, beam energy [eV])}, the constant electron emission of init_bo_NN.dat. ez: uniform Z electric field [V/cm];
     ions_sense_b / ions_sense_ez: the ions feel the magnetic / Z electric field (init_extfields.dat flags).
     Time dependence of metal objects, keyed by the reference's object number (1-based: the four boundary objects,
     then the inner objects): oscillations {n: (amplitude [V], frequency [MHz], phase [deg])} in init_bo_NN.dat;
@@ -255,7 +255,7 @@ def write_deck(directory, name="cfg0", ncx=None, ncy=None, ppc=None, steps=None,
             w(f"init_material_{mname}.dat", ["------dd.ddd- dielectric constant", f"      {obj[5]:6.3f}"] + mat_rest)
             bo(len(objs) + q + 1, obj[4], material=mname)
         else:
-            bo(len(objs) + q + 1, obj[4])
+            bo(len(objs) + q + 1, obj[4], inj=(wall_injection or {}).get(4 + q, (0.0, 0, 0.0, 0.0, 0.0)))
     for n, (amp_v, nu_hz, pts) in (waveforms or {}).items():
         w(f"init_bo_{n:02d}_waveform.dat", [f"  {amp_v}  potential amplitude [V]", f"  {nu_hz:.6e}   frequency [Hz]",
                                              "# time as a fraction of the period, value",

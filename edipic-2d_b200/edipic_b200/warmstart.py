@@ -396,8 +396,11 @@ def time_layer(cin, cout, h, w, nimg, reps=10):
 
 
 if __name__ == "__main__":
-    # python -m edipic_b200.warmstart CIN COUT H W IMAGES: times one convolution layer
+    # python -m edipic_b200.warmstart CIN COUT H W IMAGES [KERNEL]: times one convolution layer; KERNEL selects the
+    # forward kernel as edp_nn_conv_select does (0 automatic, 1 tile, 2 persistent halo)
     import sys
     a = [int(v) for v in sys.argv[1:6]]
+    if len(sys.argv) > 6:
+        _check(library().edp_nn_conv_select(int(sys.argv[6])), "edp_nn_conv_select")
     us, tf = time_layer(*a)
     print(f"{a[0]}->{a[1]} {a[4]}x{a[2]}x{a[3]}: {us:.1f} us, {tf:.1f} TFLOP/s")

@@ -121,7 +121,8 @@ struct edp_deck {
     double ii_ee[EDP_N_HIT_COUNTERS][EDP_MAX_ION_SPECIES][4] = {};
     int32_t ion_model[EDP_N_HIT_COUNTERS] = {};   // ion-material interaction model of the object's material
     edp_see_params see[EDP_N_HIT_COUNTERS] = {};  // electron-induced emission of the object's material
-    double inject[4][5] = {};    // constant electron emission of each wall: N per step, model, T_n, T_p, W_beam [eV]
+    // constant electron emission of each metal wall and inner object: N per step, model, T_n, T_p, W_beam [eV]
+    double inject[EDP_N_HIT_COUNTERS][5] = {};
     // potentials of the metal objects over time (walls 0 below, 1 above, 2 left, 3 right; inner objects 4 + n)
     EdpPotentialProfile pot[4 + EDP_MAX_INNER];
 };
@@ -319,10 +320,11 @@ int read_deck(const std::string& dir, edp_deck* d)
     // ---- constant electron emission of the walls (init_bo_NN.dat lines 11-20, PREPARE_SETUP_VALUES
     // pic2d_Setup.f90:86-95): macroparticles per step (3x,f9.3), model (7x,i1), normal and parallel temperatures and
     // the beam energy in eV (4x,f8.3)
-    for (int w = 0; w < 4; ++w) {
-        if (side_obj[w] < 0) continue;
+    for (int w = 0; w < 4 + std::min<int>((int)nio, EDP_MAX_INNER); ++w) {
+        const int bo = w < 4 ? side_obj[w] : (int)nbo + (w - 4);   // the walls, then the inner objects
+        if (bo < 0) continue;
         char name[32];
-        snprintf(name, sizeof(name), "/init_bo_%02d.dat", side_obj[w] + 1);
+        snprintf(name, sizeof(name), "/init_bo_%02d.dat", bo + 1);
         Lines bf(dir + name);
         if (!bf.ok) continue;
         for (int k = 0; k < 10; ++k)
@@ -333,6 +335,7 @@ int read_deck(const std::string& dir, edp_deck* d)
                   fint(L, 7, 1, &model) && bf.next(L) && bf.next(L) && freal(L, 4, 8, &q[2]) && bf.next(L) &&
                   bf.next(L) && freal(L, 4, 8, &q[3]) && bf.next(L) && bf.next(L) && freal(L, 4, 8, &q[4]);
         if (!ok) return EDP_ERR_IO;
+        q[0] = (double)(float)q[0];   // N_electron_constant_emit is REAL
         q[1] = (double)model;
     }
     // ---- wall materials (material name: init_bo_NN.dat line 2, (6x,A6), pic2d_Setup.f90:77; properties
@@ -645,7 +648,7 @@ int edp_deck_electron_emission(const edp_deck* d, int32_t wall, edp_see_params* 
 
 int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out)
 {
-    if (!d || !out || wall < 0 || wall > 3) return EDP_ERR_ARG;
+    if (!d || !out || wall < 0 || wall >= EDP_N_HIT_COUNTERS) return EDP_ERR_ARG;
     for (int k = 0; k < 5; ++k) out[k] = d->inject[wall][k];
     return EDP_OK;
 }

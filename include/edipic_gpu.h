@@ -273,7 +273,11 @@ int edp_set_electron_emission(edp_ctx* ctx, int32_t wall, const edp_see_params* 
  * probability) uniformly along the wall, 1e-6 inside it; model 0 thermal (normal speed from the flux-weighted
  * half-Maxwellian of temperature t_normal_ev), model 1 a beam of energy beam_energy_ev with energy spread t_normal_ev
  * (beam_energy_ev > 1.5 t_normal_ev, else EDP_ERR_ARG, pic2d_Setup.f90:107-121); tangential components Maxwellian of
- * t_parallel_ev. n_per_step = 0 switches the wall off. */
+ * t_parallel_ev. n_per_step = 0 switches the wall off. wall = 4 + n: metal inner object n
+ * (PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS, pic2d_Setup.f90:1005-1591): each side strictly inside the domain
+ * emits REAL(n_per_step) * REAL(open) / REAL(L) per step from its open cells (not covered by a wall or another inner
+ * object; L = the open cells of all four sides), 1e-6 outside the side, the normal velocity pointing out; a
+ * dielectric object is refused. */
 int edp_set_wall_injection(edp_ctx* ctx, int32_t wall, double n_per_step, int32_t model, double t_normal_ev,
                            double t_parallel_ev, double beam_energy_ev);
 /* ADVANCE_ELECTRONS (pic2d_ElectronDynamics.f90:3-513), fused with the next step's electron deposit and,
@@ -481,8 +485,9 @@ int edp_deck_ion_emission(const edp_deck* d, int32_t wall, int32_t ion_species, 
 /* ion-material interaction model of the object's material (0 absorption, 1 specular reflection, 2 ion-induced
  * emission); objects as above */
 int edp_deck_ion_wall_model(const edp_deck* d, int32_t wall, int32_t* model);
-/* constant electron emission of wall (init_bo_NN.dat, pic2d_Setup.f90:86-95): out = {N_electron_constant_emit,
- * model_constant_emit, T_normal [eV], T_parallel [eV], beam energy [eV]} */
+/* constant electron emission of a wall (0-3) or inner object (4 + n) (init_bo_NN.dat, pic2d_Setup.f90:86-95):
+ * out = {N_electron_constant_emit (a REAL: rounded to single precision), model_constant_emit, T_normal [eV],
+ * T_parallel [eV], beam energy [eV]} */
 int edp_deck_wall_injection(const edp_deck* d, int32_t wall, double* out);
 /* electron-induced emission parameters of the object's material (walls 0-3, inner objects 4 + n); *enabled = 1 when any
  * of the three models is on */

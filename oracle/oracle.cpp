@@ -763,6 +763,114 @@ int32_t oracle_wall_injection(double n, int32_t model, double fn, double fp, dou
     return count;
 }
 
+// Covered cells of segment m of inner object n (pic2d_CurProblemValues.f90:603-683): the walls of the domain are the
+// boundary objects (horizontal segments j = 0 and j = ncy over all i; on a walled domain also the vertical segments
+// i = 0 and i = ncx over j in [0, ncy)), the other inner objects come second. Index: cell - segment start.
+static std::vector<bool> inner_segment_covered(const oracle_geom_t* g, int n, int m)
+{
+    const int il = g->ileft[n], ir = g->iright[n], jb = g->jbottom[n], jt = g->jtop[n];
+    std::vector<bool> cov;
+    if (m == 1 || m == 3) {
+        const int istart = m == 1 ? il : ir;
+        for (int j = jb; j < jt; ++j) {
+            bool c = false;
+            // boundary objects: vertical wall segments with the same i
+            if (!g->periodic && (istart == 0 || istart == g->ncx) && j >= 0 && j < g->ncy) c = true;
+            for (int o = 0; o < g->n_inner && !c; ++o) {
+                if (o == n) continue;
+                if (istart < g->ileft[o] || istart > g->iright[o]) continue;
+                if (j >= g->jbottom[o] && j < g->jtop[o]) c = true;
+            }
+            cov.push_back(c);
+        }
+    } else {
+        const int jstart = m == 2 ? jt : jb;
+        for (int i = il; i < ir; ++i) {
+            bool c = jstart == 0 || jstart == g->ncy;
+            for (int o = 0; o < g->n_inner && !c; ++o) {
+                if (o == n) continue;
+                if (jstart < g->jbottom[o] || jstart > g->jtop[o]) continue;
+                if (i >= g->ileft[o] && i < g->iright[o]) c = true;
+            }
+            cov.push_back(c);
+        }
+    }
+    return cov;
+}
+
+int32_t oracle_inner_injection(const oracle_geom_t* g, int32_t n, double n_emit, int32_t model, double fn, double fp,
+                               double vb, uint32_t step, uint64_t seed, const double* maxwell_v,
+                               const double* maxwell_inj, double* out, int32_t cap, int32_t* per_side)
+{
+    const uint32_t stream = 0x43450000u;
+    std::vector<bool> cov[5];
+    int32_t L = 0;
+    for (int m = 1; m <= 4; ++m) {
+        cov[m] = inner_segment_covered(g, n, m);
+        for (bool c : cov[m]) L += c ? 0 : 1;
+    }
+    // c_indx_x/y_min and _max of the one cluster: 0 and the last node's index
+    const int cxmin = 0, cxmax = g->periodic ? g->ncx + 1 : g->ncx, cymin = 0, cymax = g->ncy;
+    int32_t total = 0;
+    for (int m = 1; m <= 4; ++m) {
+        per_side[m - 1] = 0;
+        const bool vert = m == 1 || m == 3;
+        const int at = m == 1 ? g->ileft[n] : m == 3 ? g->iright[n] : m == 2 ? g->jtop[n] : g->jbottom[n];
+        const int a0 = vert ? g->jbottom[n] : g->ileft[n], a1 = vert ? g->jtop[n] : g->iright[n];
+        if (n_emit <= 0.0 || L == 0) continue;
+        if (vert) {
+            if (!(at > cxmin && at < cxmax)) continue;
+            if (!(a0 < cymax && a1 > cymin)) continue;
+        } else {
+            if (!(at > cymin && at < cymax)) continue;
+            if (!(a0 < cxmax && a1 > cxmin)) continue;
+        }
+        const int cmin = std::max(a0, vert ? cymin : cxmin), cmax = std::min(a1, (vert ? cymax : cxmax) - 1);
+        int count_open = 0;
+        for (int q = cmin; q < cmax; ++q)
+            if (!cov[m][q - a0]) ++count_open;
+        // REAL arithmetic: N_electron_constant_emit * REAL(count_open) / REAL(L)
+        const double add = (double)((float)n_emit * (float)count_open / (float)L);
+        if (count_open == 0) continue;
+        const uint32_t key = 0xE1000000u + 4u + 4u * (uint32_t)n + (uint32_t)(m - 1);
+        int32_t count = (int32_t)add;
+        uint32_t w0[4];
+        philox_block(key, seed, step, stream, 0u, w0);
+        if (uniform(w0[0]) < add - (double)count) ++count;
+        for (int32_t e = 0; e < count; ++e) {
+            uint32_t w[4];
+            philox_block(key, seed, step, stream, 1u + (uint32_t)e, w);
+            // the walk over the open cells, one subtraction of 1 per open cell (:1064-1078)
+            double d = uniform(w[0]) * ((double)count_open - 1.0e-6);
+            double t = 0.0;
+            for (int q = cmin; q < cmax; ++q) {
+                if (cov[m][q - a0]) continue;
+                if (d < 1.0) {
+                    t = std::max((double)q, std::min((double)q + d, (double)(q + 1)));
+                    break;
+                }
+                d -= 1.0;
+            }
+            t = std::min(std::max(t, (double)cmin), (double)cmax - 1.0e-6);
+            double vn = model == 0 ? maxwell_inj_sample(maxwell_inj, uniform(w[1])) * fn
+                                   : std::max(0.0, vb + oracle_maxwell_sample(maxwell_v, uniform(w[1])) * fn);
+            double t1 = oracle_maxwell_sample(maxwell_v, uniform(w[2])) * fp;
+            double t2 = oracle_maxwell_sample(maxwell_v, uniform(w[3])) * fp;
+            if (total < cap) {
+                double* o = out + 5 * total;
+                if (m == 1) { o[0] = (double)at - 1.0e-6; o[1] = t; o[2] = -vn; o[3] = t1; }
+                else if (m == 3) { o[0] = (double)at + 1.0e-6; o[1] = t; o[2] = vn; o[3] = t1; }
+                else if (m == 2) { o[0] = t; o[1] = (double)at + 1.0e-6; o[2] = t1; o[3] = vn; }
+                else { o[0] = t; o[1] = (double)at - 1.0e-6; o[2] = t1; o[3] = -vn; }
+                o[4] = t2;
+            }
+            ++total;
+        }
+        per_side[m - 1] = count;
+    }
+    return total;
+}
+
 // CHECK_INTERSECTION_WITH_VERTICAL_SEGMENT / _HORIZONTAL_SEGMENT pic2d_ElectronWallCollisions.f90:746-812
 static bool cross_vertical(double xorg, double yorg, double x, double y, double xseg, double ymin, double ymax,
                            double* ycross)

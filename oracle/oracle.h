@@ -148,6 +148,17 @@ int32_t oracle_wall_injection(double n, int32_t model, double fn, double fp, dou
                               uint64_t seed, double xmax, double ymax, const double* maxwell_v,
                               const double* maxwell_inj, double* out, int32_t cap);
 
+/* PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS (pic2d_Setup.f90:1005-1591) of metal inner object n for one cluster
+ * over the domain: each side strictly inside the cluster emits REAL(N) * REAL(open) / REAL(L) per step (integer
+ * part, then one more with that probability), open = its cells not covered by a wall or another inner object inside
+ * [cross_min, cross_max), L = the open cells of the four sides; places by the walk over the open cells, 1e-6
+ * outside the side, normal velocity out. Variates as oracle_wall_injection with key 0xE1000000 + 4 + 4 n + (m - 1)
+ * for side m (1 left, 2 top, 3 right, 4 bottom). Rows {x, y, vx, vy, vz} (at most cap); per_side[4] the counts;
+ * returns the total. */
+int32_t oracle_inner_injection(const oracle_geom_t* g, int32_t n, double n_emit, int32_t model, double fn, double fp,
+                               double vb, uint32_t step, uint64_t seed, const double* maxwell_v,
+                               const double* maxwell_inj, double* out, int32_t cap, int32_t* per_side);
+
 /* INJECT_REFLECTED_ION (pic2d_IonEmissions.f90:374-492) for a domain wall: the ion returns 1e-6 inside the wall
  * (coordinate along the wall clamped into the domain) with its normal velocity reversed; out = {x, y, vx, vy, vz} */
 void oracle_ion_reflect(int32_t wall, double x, double y, double vx, double vy, double vz, double xmax, double ymax,

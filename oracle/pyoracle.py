@@ -113,6 +113,8 @@ def lib():
             "oracle_wall_injection": ([C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32,
                                        C.c_uint32, C.c_uint64, C.c_double, C.c_double, _D, _D, _D, C.c_int32],
                                       C.c_int32),
+            "oracle_inner_injection": ([C.POINTER(Geom), C.c_int32, C.c_double, C.c_int32, C.c_double, C.c_double,
+                                        C.c_double, C.c_uint32, C.c_uint64, _D, _D, _D, C.c_int32, _I32], C.c_int32),
             "oracle_cg_solve_eps": ([C.POINTER(Geom), _D, _D, _D, _D, C.c_double, C.c_int32, _D, _D], C.c_int32),
             "oracle_inner_hit": ([C.POINTER(Geom), _D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                   C.c_double, _D], C.c_int32),
@@ -407,6 +409,25 @@ def wall_injection(wall, n, model, t_normal_ev, t_parallel_ev, beam_ev, energy_f
     out = np.zeros((cap, 5))
     m = lib().oracle_wall_injection(n, model, fn, fp, vb, wall, step, seed, xmax, ymax, dp(v), dp(vi), dp(out), cap)
     return out[:m]
+
+
+def inner_injection(g, n, n_per_step, model, t_normal_ev, t_parallel_ev, beam_ev, energy_factor_ev, step, seed):
+    """oracle_inner_injection for metal inner object n with the temperatures converted as for the walls: (rows
+    {x, y, vx, vy, vz}, counts of sides 1 left, 2 top, 3 right, 4 bottom)."""
+    ef = energy_factor_ev
+    fp = np.sqrt(t_parallel_ev / ef)
+    if model == 0:
+        fn, vb = np.sqrt(t_normal_ev / ef), 0.0
+    else:
+        fn, vb = np.sqrt(0.25 * t_normal_ev ** 2 / (beam_ev * ef)), np.sqrt(beam_ev / ef)
+    v, vi = maxwell_tables()
+    cap = 4 * int(n_per_step) + 8
+    out = np.zeros((cap, 5))
+    per = np.zeros(4, dtype=np.int32)
+    m = lib().oracle_inner_injection(C.byref(g), n, n_per_step, model, fn, fp, vb, step, seed, dp(v), dp(vi),
+                                     dp(out), cap, per.ctypes.data_as(_I32))
+    assert m <= cap
+    return out[:m], per
 
 
 def ion_reflect(wall, x, y, vx, vy, vz, xmax, ymax):

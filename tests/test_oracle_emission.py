@@ -66,3 +66,24 @@ def test_energy_budget():
         spent = (rows[:, 2:] ** 2).sum() * EF
         assert spent <= (e_ion - 10.0) * (1 + 1e-9)
         assert 1 <= len(rows) <= 3
+
+
+def test_inner_injection_places_electrons_on_open_cells():
+    """oracle_inner_injection (PERFORM_ELECTRON_EMISSION_SETUP_INNER_OBJECTS, pic2d_Setup.f90:1005-1591): an object
+    on the bottom wall emits nothing below; where another object covers part of a side, no electron starts there; the
+    per-side counts follow REAL(N) REAL(open) / REAL(L); every electron starts 1e-6 outside a side and moves out."""
+    g = pyoracle.geom(64, 48, False, [(20, 24, 36, 32), (36, 26, 44, 30), (50, 0, 56, 10)])
+    tot = np.zeros(4)
+    steps = 400
+    for t in range(steps):
+        rows, per = pyoracle.inner_injection(g, 0, 10.0, 0, 2.0, 1.0, 0.0, EF, t, 77)
+        tot += per
+        right = rows[np.isclose(rows[:, 0], 36 + 1e-6, atol=1e-9)]
+        # object 1 covers the cells 26..29 of object 0's right side
+        assert np.all((right[:, 1] < 26) | (right[:, 1] >= 30)) and np.all(right[:, 2] > 0)
+        left = rows[np.isclose(rows[:, 0], 20 - 1e-6, atol=1e-9)]
+        assert np.all(left[:, 2] < 0)
+    # L = 8 + 16 + 4 + 16 = 44 open cells (right side 8 - 4 covered): rates 8, 16, 4, 16 of 44 per 10 electrons
+    np.testing.assert_allclose(tot / steps, 10.0 * np.array([8, 16, 4, 16]) / 44, rtol=0.06)
+    _, per = pyoracle.inner_injection(g, 2, 10.0, 0, 2.0, 1.0, 0.0, EF, 3, 77)
+    assert per[3] == 0
