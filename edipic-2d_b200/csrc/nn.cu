@@ -110,7 +110,7 @@ struct TmaArgs {
     const float* bias;
     bf16* y;
     int* err;
-    float* ws;   // split K (gridDim.z slices): FP32 partial sums [P][cout] added here, finished by conv_finish_kernel
+    float* ws;   // split K (gridDim.z slices): FP32 partial sums [slice][P][cout], summed by conv_finish_kernel
 };
 
 template <int BN, int CW>
@@ -230,12 +230,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                          : "r"(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             if (inside && ta.ws) {
-                float* d = ta.ws + p * ta.cout + n0 + c0;
-                for (int q = 0; q < 16; q += 4)
-                    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n"
-                                 ::"l"(d + q), "f"(__uint_as_float(v[q])), "f"(__uint_as_float(v[q + 1])),
-                                   "f"(__uint_as_float(v[q + 2])), "f"(__uint_as_float(v[q + 3]))
-                                 : "memory");
+                const int64_t P = (int64_t)ta.nimg * ta.h * ta.w;
+                float4* d = reinterpret_cast<float4*>(ta.ws + ((int64_t)blockIdx.z * P + p) * ta.cout + n0 + c0);
+                for (int q = 0; q < 4; ++q)
+                    d[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                       __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
             } else if (inside) {
                 uint32_t pk[8];
                 for (int q = 0; q < 8; ++q) {
@@ -513,13 +512,20 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
     }
 }
 
-// y = act(ws + bias) in BF16 for the split-K path, and ws back to zero for the next layer; 4 channels per thread
-__global__ void conv_finish_kernel(float* __restrict__ ws, int64_t n4, int cout, const float* __restrict__ bias,
-                                   int relu, bf16* __restrict__ y)
+// y = act(sum of the ks partial sums + bias) in BF16 for the split-K path, the slices summed in order; 4 channels per
+// thread
+__global__ void conv_finish_kernel(const float* __restrict__ ws, int ks, int64_t n4, int cout,
+                                   const float* __restrict__ bias, int relu, bf16* __restrict__ y)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
-        float4 v = reinterpret_cast<float4*>(ws)[i];
-        reinterpret_cast<float4*>(ws)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 v = reinterpret_cast<const float4*>(ws)[i];
+        for (int z = 1; z < ks; ++z) {
+            const float4 u = reinterpret_cast<const float4*>(ws)[z * n4 + i];
+            v.x += u.x;
+            v.y += u.y;
+            v.z += u.z;
+            v.w += u.w;
+        }
         const int n = (int)((4 * i) % cout);
         if (bias) {
             v.x += bias[n];
@@ -538,8 +544,8 @@ __global__ void conv_finish_kernel(float* __restrict__ ws, int64_t n4, int cout,
     }
 }
 
-// FP32 workspace of the split-K path, one per (device, stream), kept zeroed between layers (conv_finish_kernel
-// clears what it read). Grown on demand: the old buffer is freed after the stream has finished with it.
+// FP32 workspace of the split-K path, one per (device, stream). Grown on demand: the old buffer is freed after the
+// stream has finished with it.
 float* splitk_workspace(cudaStream_t s, size_t bytes)
 {
     struct Ws {
@@ -568,7 +574,6 @@ float* splitk_workspace(cudaStream_t s, size_t bytes)
             w->bytes = 0;
         }
         if (cudaMalloc(&w->p, bytes) != cudaSuccess) return nullptr;
-        if (cudaMemsetAsync(w->p, 0, bytes, s) != cudaSuccess) return nullptr;
         w->bytes = bytes;
     }
     return w->p;
@@ -655,18 +660,18 @@ int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
     ta.err = err;
     ta.ws = nullptr;
     const int64_t ctas = (int64_t)ta.tiles_x * ta.tiles_y * c.nimg * (c.cout / BN);
-    // a layer with fewer than two CTAs per SM splits its K range (taps x channel chunks, at least two chunks per
-    // slice) over more CTAs, whose FP32 partial sums meet in a workspace
+    // a layer with fewer CTAs than SMs splits its K range (taps x channel chunks, at least two chunks per slice) over
+    // about one CTA per SM; the slices' FP32 partial sums go to a workspace and are added in order by the finish
     const int kt_all = 9 * (c.c1 + c.c2) / CW;
     int ks = 1;
-    if (ctas < 2 * 148) {
-        ks = (int)((2 * 148 + ctas - 1) / ctas);
+    if (ctas < 148) {
+        ks = (int)((148 + ctas - 1) / ctas);
         if (ks > kt_all / 2) ks = kt_all / 2;
         if (ks < 1) ks = 1;
     }
     const int64_t P = (int64_t)c.nimg * c.h * c.w;
     if (ks > 1) {
-        ta.ws = splitk_workspace(s, (size_t)P * c.cout * sizeof(float));
+        ta.ws = splitk_workspace(s, (size_t)ks * P * c.cout * sizeof(float));
         if (!ta.ws) return EDP_ERR_CUDA;
     }
     dim3 grid((unsigned)(ta.tiles_x * ta.tiles_y * c.nimg), c.cout / BN, (unsigned)ks);
@@ -675,7 +680,7 @@ int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
         const int64_t n4 = P * c.cout / 4;
         int64_t g = (n4 + 255) / 256;
         if (g > 148 * 8) g = 148 * 8;
-        conv_finish_kernel<<<(unsigned)g, 256, 0, s>>>(ta.ws, n4, c.cout, c.bias, c.relu, c.y);
+        conv_finish_kernel<<<(unsigned)g, 256, 0, s>>>(ta.ws, ks, n4, c.cout, c.bias, c.relu, c.y);
     }
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }

@@ -371,18 +371,14 @@ __device__ __forceinline__ void push_group_body(const PushArgs& a, Smem& s, int 
 {
     const int64_t base = g * IPT;
     bool sel[IPT];
-    // the decision draws first, for all particles of the thread: independent Philox chains that overlap
-    uint32_t draw[IPT];
-#pragma unroll
-    for (int e = 0; e < IPT; ++e) draw[e] = a.do_coll ? push_draw<ION>(a, id[e]) : 0u;
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
     for (int e = 0; e < IPT; ++e) {
         sel[e] = false;
         if (c[e] < 0) continue;
-        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e], draw[e],
-                                     sel[e])) {
+        if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
+                                     a.do_coll ? push_draw<ION>(a, id[e]) : 0u, sel[e])) {
             c[e] = -1;
             sel[e] = false;
             atomicAdd(&s.cnt[17], 1ull);

@@ -17,6 +17,10 @@ def test_mixed_matches_fp64_statistically(tmp_path):
     fp64 = [run(PREC_FP64, 1000 + s, **kw) for s in range(8)]
     z = compare_paired(mixed, fp64)
     for k, v in z.items():
+        if k == "ion_flux" and v["n"] == 0:
+            # few ions reach the walls in 200 steps: the two precisions may count exactly the same in every seed
+            assert all(a["ion_flux"] == b["ion_flux"] for a, b in zip(mixed, fp64))
+            continue
         assert v["n"] > 0, k
         assert v["max_abs_z"] < 6.0, (k, v)
         assert v["mean_z2"] < 2.5, (k, v)
