@@ -269,24 +269,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // memory as four planes of 8 channels, plane s holding pixel q at byte 16 q (the canonical K-major layout without
 // swizzle: core matrices of 8 pixels x 16 bytes), so the A operand of tap (dx, dy) is the same planes read from
 // pixel 10 dy + dx on: stride between 8-row groups (SBO) = one halo row = 160 bytes, between the two 8-channel
-// halves of a K step (LBO) = one plane. The planes are padded so that the 16-byte writes of eight lanes (two pixels
-// x four planes) hit all 32 banks. The weights of the whole layer stay in shared memory (loaded once by TMA, 64-byte
+// halves of a K step (LBO) = one plane (planes 128-byte aligned for the TMA copies; in the weight gradient, whose
+// halo is copied by cp.async, padded instead so that the 16-byte writes of eight lanes, two pixels x four planes,
+// hit all 32 banks). The weights of the whole layer stay in shared memory (loaded once by TMA, 64-byte
 // swizzle, one (32, c_out) box per tap and chunk).
-// Roles: warps 0-1 copy halos with cp.async (16-byte pieces of the NHWC rows, zero-filled off the image) into a ring
-// of stages, each copy signalling the stage's full barrier when it lands (cp.async.mbarrier.arrive.noinc); warp 2,
-// lane 0, loads the weights and issues the MMAs (tcgen05.mma, accumulator in one of two tensor-memory buffers,
-// committed to the stage's empty barrier and, after the tile's last chunk, to the buffer's full barrier); warps
-// 3-6 (one per quarter of the tensor-memory lanes) read the accumulator back (tcgen05.ld), add the bias, apply ReLU
-// and store BF16, then release the buffer.
+// Roles: warp 0, lane 0, copies each halo by TMA, one (8 channels, 10, 18) box per plane, zero-filled off the image,
+// into a ring of stages (expect-tx on the stage's full barrier); warp 1, lane 0, loads the weights and issues the
+// MMAs (tcgen05.mma, accumulators in one of two tensor-memory buffers, committed to the stage's empty barrier and,
+// after the tile's last chunk, to the buffer's full barrier); warps 2-5 (one per quarter of the tensor-memory lanes)
+// read the accumulators back (tcgen05.ld), add them and the bias, apply ReLU and store BF16, then release the buffer.
 // Tiles are taken round-robin by the persistent CTAs, so the next tile's copies and MMAs overlap this tile's
 // epilogue. Every wait is bounded; a wait that gives up sets the error word and stops every role.
-constexpr int kHaloThreads = 224;
+constexpr int kHaloThreads = 224;     // weight gradient: 2 copy warps, 1 MMA warp, 4 epilogue warps
+constexpr int kHaloMmaWarp = 1;       // forward halo kernel: the TMA warp, the MMA warp, 4 epilogue warps
+constexpr int kHaloFwdThreads = 192;
 constexpr int kHaloStages = 4;
-constexpr int kHaloPlane = 2912;                      // 182 pixel slots of 16 bytes (180 used)
+constexpr int kHaloBoxBytes = 180 * 16;               // one plane of the halo: 10 x 18 pixels x 8 channels
+constexpr int kHaloPlane = 2944;                      // plane stride: 184 pixel slots, 128-byte aligned (TMA)
 constexpr int kHaloStage = 4 * kHaloPlane;            // one 32-channel chunk
+constexpr int kWgPlane = 2912;                        // weight gradient (cp.async): 182 slots, bank-spread writes
+constexpr int kWgHaloStage = 4 * kWgPlane;
 constexpr int kHaloMaxWeights = 112 * 1024;           // largest resident weight set (9 x c_in x c_out x 2 bytes)
 template <int BN>
-constexpr int kHaloAcc = BN == 32 ? 3 : BN == 64 ? 2 : 1;   // partial accumulators per tile
+constexpr int kHaloAcc = BN == 128 ? 1 : 2;   // partial accumulators per tile
+template <int BN>
+constexpr int kHaloTmemCols = 2 * kHaloAcc<BN> * BN <= 128 ? 128 : 256;   // two tiles' accumulators
 
 struct HaloArgs {
     const bf16* x1;
@@ -313,13 +320,14 @@ __device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity,
 }
 
 template <int BN>
-__global__ void __launch_bounds__(kHaloThreads, 1)
-    conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, HaloArgs a)
+__global__ void __launch_bounds__(kHaloFwdThreads, 1)
+    conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap mx1,
+                            const __grid_constant__ CUtensorMap mx2, HaloArgs a)
 {
     // NACC partial accumulators per tile (tap % NACC), summed in the epilogue: consecutive MMAs of the short (small N)
-    // chains go to independent accumulators; two tiles' sets of them (double buffering) in 256 columns
+    // chains go to independent accumulators; two tiles' sets of them (double buffering)
     constexpr int NACC = kHaloAcc<BN>;
-    constexpr uint32_t TMEM_COLS = 256;
+    constexpr uint32_t TMEM_COLS = kHaloTmemCols<BN>;
     constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
     // A: no swizzle, LBO = one plane (K direction), SBO = one halo row of 10 pixels (M direction)
     constexpr uint64_t DESC_A = ((uint64_t)(160 >> 4) << 32) | ((uint64_t)(kHaloPlane >> 4) << 16) | ((uint64_t)1 << 46);
@@ -331,12 +339,14 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
     __shared__ __align__(8) uint64_t full[kHaloStages], empty[kHaloStages], acc_full[2], acc_empty[2], wbar, done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int fail_sh;
+    __shared__ float bias_sh[BN];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cin = a.c1 + a.c2, n_chunks = cin / 32;
     const uint32_t wbase = (smem_u32(dsm) + 1023u) & ~1023u;
     const uint32_t hbase = wbase + (uint32_t)(9 * n_chunks * B_CHUNK);
 
-    if (warp == 2) {
+    for (int i = tid; i < BN; i += blockDim.x) bias_sh[i] = a.bias ? a.bias[i] : 0.0f;
+    if (warp == kHaloMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
@@ -344,7 +354,7 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
     if (tid == 0) {
         fail_sh = 0;
         for (int s = 0; s < kHaloStages; ++s) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(64));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[s])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
         }
         for (int b = 0; b < 2; ++b) {
@@ -361,37 +371,42 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
     const uint32_t tmem = tmem_base_sh;
     const int64_t stride = gridDim.x;
 
-    if (warp < 2) {
-        // ---------------- halo producer: 64 threads, 16-byte pieces, 4 per pixel and chunk
-        const int pt = tid;   // 0..63
-        int64_t it = 0;
-        for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride) {
-            const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
-            const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
-            const int gx0 = tx * 8 - 1, gy0 = ty * 16 - 1;
-            for (int cc = 0; cc < n_chunks; ++cc, ++it) {
-                const int s = (int)(it % kHaloStages);
-                if (it >= kHaloStages &&
-                    !mbar_wait_or_fail(smem_u32(&empty[s]), (uint32_t)(((it / kHaloStages) - 1) & 1), &fail_sh))
-                    break;
-                const int c0 = cc * 32;
-                const bf16* src = c0 < a.c1 ? a.x1 : a.x2;
-                const int cs = c0 < a.c1 ? a.c1 : a.c2, co = c0 < a.c1 ? c0 : c0 - a.c1;
-                const uint32_t st = hbase + (uint32_t)(s * kHaloStage);
-                for (int q = pt; q < 180 * 4; q += 64) {
-                    const int px = q >> 2, pl = q & 3;
-                    const int hx = px % 10, hy = px / 10;
-                    const int gx = gx0 + hx, gy = gy0 + hy;
-                    const bool ok = gx >= 0 && gx < a.w && gy >= 0 && gy < a.h;
-                    const bf16* g = ok ? src + (((int64_t)img * a.h + gy) * a.w + gx) * cs + co + 8 * pl : src;
-                    cp_async16(st + (uint32_t)(pl * kHaloPlane + px * 16), g, ok);
+    if (warp == 0) {
+        // ---------------- halo producer (lane 0): four TMA boxes of (8 channels, 10 x, 18 y) per 32-channel chunk,
+        // one per plane, zero-filled where the halo leaves the image
+        if (lane == 0) {
+            int64_t it = 0;
+            for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride) {
+                const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
+                const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
+                const int gx0 = tx * 8 - 1, gy0 = ty * 16 - 1;
+                bool ok = true;
+                for (int cc = 0; cc < n_chunks; ++cc, ++it) {
+                    const int s = (int)(it % kHaloStages);
+                    if (it >= kHaloStages &&
+                        !mbar_wait_or_fail(smem_u32(&empty[s]), (uint32_t)(((it / kHaloStages) - 1) & 1), &fail_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    const int c0 = cc * 32;
+                    const CUtensorMap* m = c0 < a.c1 ? &mx1 : &mx2;
+                    const int co = c0 < a.c1 ? c0 : c0 - a.c1;
+                    const uint32_t st = hbase + (uint32_t)(s * kHaloStage), fb = smem_u32(&full[s]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                                 "r"(4 * kHaloBoxBytes) : "memory");
+                    for (int pl = 0; pl < 4; ++pl)
+                        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                                     ::"r"(st + (uint32_t)(pl * kHaloPlane)), "l"(m), "r"(co + 8 * pl), "r"(gx0), "r"(gy0),
+                                       "r"(img), "r"(fb) : "memory");
                 }
-                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[s]))
-                             : "memory");
+                if (!ok) break;
             }
+            // copies still in flight (their stages not consumed after a failure) land before the CTA leaves
+            for (int64_t q = it > kHaloStages ? it - kHaloStages : 0; q < it; ++q)
+                mbar_wait(smem_u32(&full[q % kHaloStages]), (uint32_t)((q / kHaloStages) & 1));
         }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-    } else if (warp == 2) {
+        __syncwarp();
+    } else if (warp == kHaloMmaWarp) {
         // ---------------- weights once, then the MMAs (lane 0)
         if (lane == 0) {
             const uint32_t wb = smem_u32(&wbar);
@@ -414,8 +429,6 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
                         ok = false;
                         break;
                     }
-                    // the halo was written by the generic proxy (cp.async); the MMAs read it through the async one
-                    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                     const uint32_t As = hbase + (uint32_t)(s * kHaloStage);
                     for (int ks = 0; ks < 2; ++ks) {
@@ -445,7 +458,7 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
         }
         __syncwarp();
     }
-    if (warp >= 3) {
+    if (warp > kHaloMmaWarp) {
         // ---------------- epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31; lane 0 waits for the
         // warp, so that the whole warp takes the same path through the .sync.aligned loads
         const int q = warp & 3;
@@ -484,8 +497,8 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
                     uint32_t pk[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        float v0 = f[2 * k] + (a.bias ? __ldg(a.bias + c0 + 2 * k) : 0.0f);
-                        float v1 = f[2 * k + 1] + (a.bias ? __ldg(a.bias + c0 + 2 * k + 1) : 0.0f);
+                        float v0 = f[2 * k] + bias_sh[c0 + 2 * k];
+                        float v1 = f[2 * k + 1] + bias_sh[c0 + 2 * k + 1];
                         if (a.relu) {
                             v0 = fmaxf(v0, 0.0f);
                             v1 = fmaxf(v1, 0.0f);
@@ -506,7 +519,7 @@ __global__ void __launch_bounds__(kHaloThreads, 1)
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (fail_sh && tid == 0) atomicExch(a.err, 1);
-    if (warp == 2) {
+    if (warp == kHaloMmaWarp) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
     }
@@ -608,6 +621,21 @@ bool map_act(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int c
     return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, cw == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// NHWC activations with c channels for the halo kernel: dims (c, w, h, n), box (8 channels, 10, 18, 1) without
+// swizzle, which lands in shared memory as one plane (pixel q of the 10 x 18 halo at byte 16 q)
+bool map_halo(CUtensorMap* m, const void* x, int nimg, int h, int w, int c)
+{
+    EncodeTiledFn f = encode_fn();
+    if (!f) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
+    const cuuint32_t box[4] = {8, 10, 18, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // weights [cout][k]: dims (k, cout), box (cw, bn)
@@ -718,8 +746,14 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
             return EDP_ERR_CUDA;
         configured[dev] = smem;
     }
-    CUtensorMap mw;
+    CUtensorMap mw, mx1, mx2;
     if (!map_wt(&mw, c.wt, 9 * (c.c1 + c.c2), c.cout, 32, BN)) return EDP_ERR_CUDA;
+    if (!map_halo(&mx1, c.x1, c.nimg, c.h, c.w, c.c1)) return EDP_ERR_CUDA;
+    if (c.c2 > 0) {
+        if (!map_halo(&mx2, c.x2, c.nimg, c.h, c.w, c.c2)) return EDP_ERR_CUDA;
+    } else {
+        mx2 = mx1;
+    }
     HaloArgs a;
     a.x1 = c.x1;
     a.x2 = c.x2;
@@ -740,12 +774,12 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
         return EDP_ERR_CUDA;
-    // CTAs per SM: shared memory (1 KiB per CTA reserved by the driver) and 256 tensor-memory columns per CTA
+    // CTAs per SM: shared memory (1 KiB per CTA reserved by the driver) and the 512 tensor-memory columns of an SM
     int per_sm = smem_sm / (smem + 1024);
-    if (per_sm > 2) per_sm = 2;
+    if (per_sm > 512 / kHaloTmemCols<BN>) per_sm = 512 / kHaloTmemCols<BN>;
     if (per_sm < 1) per_sm = 1;
     const int64_t grid = a.n_tiles < (int64_t)sms * per_sm ? a.n_tiles : (int64_t)sms * per_sm;
-    conv3x3_fwd_halo_kernel<BN><<<(unsigned)grid, kHaloThreads, smem, s>>>(mw, a);
+    conv3x3_fwd_halo_kernel<BN><<<(unsigned)grid, kHaloFwdThreads, smem, s>>>(mw, mx1, mx2, a);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
@@ -919,12 +953,12 @@ template <int M>
 __global__ void __launch_bounds__(kHaloThreads, 1) conv3x3_wgrad_tc_kernel(WgradTcArgs a)
 {
     constexpr int NP = M / 8;                                   // dz planes
-    constexpr int STAGE = NP * kDzPlane + kHaloStage;
+    constexpr int STAGE = NP * kDzPlane + kWgHaloStage;
     constexpr uint32_t TMEM_COLS = 512;                         // 9 taps x 32 columns
     constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((32u >> 3) << 17) |
                                ((uint32_t)(M >> 4) << 24);
     constexpr uint64_t DESC_A = ((uint64_t)(kDzPlane >> 4) << 32) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)1 << 46);
-    constexpr uint64_t DESC_B = ((uint64_t)(kHaloPlane >> 4) << 32) | ((uint64_t)(160 >> 4) << 16) | ((uint64_t)1 << 46);
+    constexpr uint64_t DESC_B = ((uint64_t)(kWgPlane >> 4) << 32) | ((uint64_t)(160 >> 4) << 16) | ((uint64_t)1 << 46);
     extern __shared__ unsigned char dsm[];
     __shared__ __align__(8) uint64_t full[kWgStages], empty[kWgStages], done_bar;
     __shared__ uint32_t tmem_base_sh;
@@ -990,7 +1024,7 @@ __global__ void __launch_bounds__(kHaloThreads, 1) conv3x3_wgrad_tc_kernel(Wgrad
                 const int gx = tx * 8 - 1 + px % 10, gy = ty * 16 - 1 + px / 10;
                 const bool ok = gx >= 0 && gx < a.w && gy >= 0 && gy < a.h;
                 const bf16* g = ok ? xs + (((int64_t)img * a.h + gy) * a.w + gx) * xcs + xco + 8 * pl : xs;
-                cp_async16(hs + (uint32_t)(pl * kHaloPlane + px * 16), g, ok);
+                cp_async16(hs + (uint32_t)(pl * kWgPlane + px * 16), g, ok);
             }
             asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&full[s])) : "memory");
         }
@@ -1071,7 +1105,7 @@ int g_wgrad_mode = 0;
 template <int M>
 int launch_wgrad_tc(const WgradArgs& w, int* err, cudaStream_t s)
 {
-    constexpr int SMEM = 128 + kWgStages * ((M / 8) * kDzPlane + kHaloStage);
+    constexpr int SMEM = 128 + kWgStages * ((M / 8) * kDzPlane + kWgHaloStage);
     static bool configured[64] = {false};
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;

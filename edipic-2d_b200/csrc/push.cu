@@ -172,7 +172,7 @@ __device__ __forceinline__ long long fix_round(double x)
 // One particle. Returns false when it was absorbed (the caller stores cell = -1).
 // ION: ion species (acc_E, RCX) instead of electrons (E, MCC selection); PER: periodic x; ROT: Boris rotation.
 // The collision decision word of one particle: word 0 of its Philox2x32 draw keyed by (id, step) for MCC selection
-// (electrons) or charge exchange (ions). Independent of the push, so a thread draws for all its particles at once.
+// (electrons) or charge exchange (ions).
 template <bool ION>
 __device__ __forceinline__ uint32_t push_draw(const PushArgs& a, uint32_t id)
 {
@@ -184,7 +184,7 @@ __device__ __forceinline__ uint32_t push_draw(const PushArgs& a, uint32_t id)
 template <bool ION, bool PER, bool ROT>
 __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool windowed, int wx0, int wy0, DepAcc& acc,
                                          int& cell, float& ox, float& oy, float& vx, float& vy, float& vz, uint32_t id,
-                                         uint32_t draw, bool& selected)
+                                         bool& selected)
 {
     const edp_kparams& kp = a.kp;
     int i = cell & 0xFFFF, j = cell >> 16;
@@ -299,9 +299,11 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     // (the 2^32 scaling is exact, so folding it into one factor rounds the same way)
     const double dx = (double)nx, dy = (double)ny, mxd = __dsub_rn(1.0, dx);
     const double A = __dmul_rn(__dsub_rn(1.0, dy), EDP_FIX_ONE), B = __dmul_rn(dy, EDP_FIX_ONE);
-    const long long q00 = fix_round(__dmul_rn(mxd, A));
-    const long long q10 = fix_round(__dmul_rn(dx, A));
-    const long long q01 = fix_round(__dmul_rn(mxd, B));
+    // both roundings give the same integers on this range; which one keeps the kernel out of spills at 64 registers
+    // differs by species (measured: the magic add for electrons, the conversion for ions)
+    const long long q00 = ION ? __double2ll_rn(__dmul_rn(mxd, A)) : fix_round(__dmul_rn(mxd, A));
+    const long long q10 = ION ? __double2ll_rn(__dmul_rn(dx, A)) : fix_round(__dmul_rn(dx, A));
+    const long long q01 = ION ? __double2ll_rn(__dmul_rn(mxd, B)) : fix_round(__dmul_rn(mxd, B));
     const long long q11 = 4294967296LL - q00 - q10 - q01;
     const int dlx = win_dx<PER>(ni - wx0, kp), dly = nj - wy0;
     if (windowed && (unsigned)dlx < EDP_WIN_CELLS && (unsigned)dly < EDP_WIN_CELLS) {
@@ -329,11 +331,12 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
         atomicAdd(&a.rho[r1 + i1], (unsigned long long)q11);
     }
     // ---- collisions in the epilogue, with the variates of the separate passes
-    if (!ION && a.do_coll) selected = (unsigned long long)draw < a.mcc->pmax_x;   // as edp_mcc_select
+    // the decision draw after the push, for the particles still present (as edp_mcc_select / edp_rcx_ion)
+    if (!ION && a.do_coll) selected = (unsigned long long)push_draw<false>(a, id) < a.mcc->pmax_x;
     if (ION && a.do_coll) {
         double dvx = vx, dvy = vy, dvz = vz;
-        if (edp_rcx_ion_drawn(a.rcx, draw, id, a.step, (uint32_t)(a.species - 1), kp.seed_lo, kp.seed_hi, dvx, dvy,
-                              dvz)) {
+        if (edp_rcx_ion_drawn(a.rcx, push_draw<true>(a, id), id, a.step, (uint32_t)(a.species - 1), kp.seed_lo,
+                              kp.seed_hi, dvx, dvy, dvz)) {
             vx = (float)dvx;
             vy = (float)dvy;
             vz = (float)dvz;
@@ -378,7 +381,7 @@ __device__ __forceinline__ void push_group_body(const PushArgs& a, Smem& s, int 
         sel[e] = false;
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                     a.do_coll ? push_draw<ION>(a, id[e]) : 0u, sel[e])) {
+                                     sel[e])) {
             c[e] = -1;
             sel[e] = false;
             atomicAdd(&s.cnt[17], 1ull);
@@ -536,7 +539,7 @@ __device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, i
         sel[e] = false;
         if (c[e] < 0) continue;
         if (!push_one<ION, PER, ROT>(a, s, WIN, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                     a.do_coll ? push_draw<ION>(a, id[e]) : 0u, sel[e])) {
+                                     sel[e])) {
             c[e] = -1;
             sel[e] = false;
             atomicAdd(&s.cnt[17], 1ull);
@@ -875,7 +878,6 @@ __global__ void __launch_bounds__(EDP_PUSH_THREADS, IPT == 4 ? 3 : 4) push_strea
                 if (c[e] < 0) continue;
                 bool sel = false;
                 if (!push_one<ION, PER, ROT>(a, s, true, wx0, wy0, acc, c[e], ox[e], oy[e], vx[e], vy[e], vz[e], id[e],
-                                             a.do_coll ? push_draw<ION>(a, id[e]) : 0u,
                                              sel)) {
                     c[e] = -1;
                     atomicAdd(&s.cnt[17], 1ull);
