@@ -287,6 +287,7 @@ constexpr int kHaloStages = 4;
 constexpr int kHaloBoxBytes = 180 * 16;               // one plane of the halo: 10 x 18 pixels x 8 channels
 constexpr int kHaloPlane = 2944;                      // plane stride: 184 pixel slots, 128-byte aligned (TMA)
 constexpr int kHaloStage = 4 * kHaloPlane;            // one 32-channel chunk
+constexpr int kHaloStagePad = 12288;                  // the halo rounded up to 1 KiB: streamed weights follow it
 constexpr int kWgPlane = 2912;                        // weight gradient (cp.async): 182 slots, bank-spread writes
 constexpr int kWgHaloStage = 4 * kWgPlane;
 constexpr int kHaloMaxWeights = 112 * 1024;           // largest resident weight set (9 x c_in x c_out x 2 bytes)
@@ -319,7 +320,7 @@ __device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity,
     return false;
 }
 
-template <int BN>
+template <int BN, bool STREAM>
 __global__ void __launch_bounds__(kHaloFwdThreads, 1)
     conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap mx1,
                             const __grid_constant__ CUtensorMap mx2, HaloArgs a)
@@ -335,6 +336,8 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
     constexpr uint64_t DESC_B = ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61) |
                                 ((uint64_t)1 << 16);
     constexpr int B_CHUNK = BN * 64;   // bytes of one (tap, chunk) weight box
+    // STREAM: the weights do not stay; each stage holds a chunk's halo and the chunk's nine (32, c_out) weight boxes
+    constexpr int SST = STREAM ? kHaloStagePad + 9 * B_CHUNK : kHaloStage;
     extern __shared__ unsigned char dsm[];
     __shared__ __align__(8) uint64_t full[kHaloStages], empty[kHaloStages], acc_full[2], acc_empty[2], wbar, done_bar;
     __shared__ uint32_t tmem_base_sh;
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cin = a.c1 + a.c2, n_chunks = cin / 32;
     const uint32_t wbase = (smem_u32(dsm) + 1023u) & ~1023u;
-    const uint32_t hbase = wbase + (uint32_t)(9 * n_chunks * B_CHUNK);
+    const uint32_t hbase = STREAM ? wbase : wbase + (uint32_t)(9 * n_chunks * B_CHUNK);
 
     for (int i = tid; i < BN; i += blockDim.x) bias_sh[i] = a.bias ? a.bias[i] : 0.0f;
     if (warp == kHaloMmaWarp) {
@@ -391,9 +394,14 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
                     const int c0 = cc * 32;
                     const CUtensorMap* m = c0 < a.c1 ? &mx1 : &mx2;
                     const int co = c0 < a.c1 ? c0 : c0 - a.c1;
-                    const uint32_t st = hbase + (uint32_t)(s * kHaloStage), fb = smem_u32(&full[s]);
+                    const uint32_t st = hbase + (uint32_t)(s * SST), fb = smem_u32(&full[s]);
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
-                                 "r"(4 * kHaloBoxBytes) : "memory");
+                                 "r"(4 * kHaloBoxBytes + (STREAM ? 9 * B_CHUNK : 0)) : "memory");
+                    if constexpr (STREAM)
+                        for (int tap = 0; tap < 9; ++tap)
+                            asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                                         ::"r"(st + (uint32_t)(kHaloStagePad + tap * B_CHUNK)), "l"(&mw),
+                                           "r"(tap * cin + c0), "r"(0), "r"(fb) : "memory");
                     for (int pl = 0; pl < 4; ++pl)
                         asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
                                      ::"r"(st + (uint32_t)(pl * kHaloPlane)), "l"(m), "r"(co + 8 * pl), "r"(gx0), "r"(gy0),
@@ -409,13 +417,16 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
     } else if (warp == kHaloMmaWarp) {
         // ---------------- weights once, then the MMAs (lane 0)
         if (lane == 0) {
-            const uint32_t wb = smem_u32(&wbar);
-            const uint32_t bytes = (uint32_t)(9 * n_chunks * B_CHUNK);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(wb), "r"(bytes) : "memory");
-            for (int k = 0; k < 9 * n_chunks; ++k)
-                asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
-                             ::"r"(wbase + (uint32_t)(k * B_CHUNK)), "l"(&mw), "r"(k * 32), "r"(0), "r"(wb) : "memory");
-            bool ok = mbar_wait_or_fail(wb, 0u, &fail_sh);
+            bool ok = true;
+            if constexpr (!STREAM) {
+                const uint32_t wb = smem_u32(&wbar);
+                const uint32_t bytes = (uint32_t)(9 * n_chunks * B_CHUNK);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(wb), "r"(bytes) : "memory");
+                for (int k = 0; k < 9 * n_chunks; ++k)
+                    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                                 ::"r"(wbase + (uint32_t)(k * B_CHUNK)), "l"(&mw), "r"(k * 32), "r"(0), "r"(wb) : "memory");
+                ok = mbar_wait_or_fail(wb, 0u, &fail_sh);
+            }
             int64_t it = 0, tl = 0;
             for (int64_t t = blockIdx.x; ok && t < a.n_tiles && !fail_sh; t += stride, ++tl) {
                 const int buf = (int)(tl & 1);
@@ -430,11 +441,12 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                    const uint32_t As = hbase + (uint32_t)(s * kHaloStage);
+                    const uint32_t As = hbase + (uint32_t)(s * SST);
                     for (int ks = 0; ks < 2; ++ks) {
                         for (int tap = 0; tap < 9; ++tap) {
                             const uint32_t a0 = As + (uint32_t)(((tap / 3) * 10 + tap % 3) * 16);
-                            const uint32_t b0 = wbase + (uint32_t)((tap * n_chunks + cc) * B_CHUNK);
+                            const uint32_t b0 = STREAM ? As + (uint32_t)(kHaloStagePad + tap * B_CHUNK)
+                                                       : wbase + (uint32_t)((tap * n_chunks + cc) * B_CHUNK);
                             const uint64_t da = DESC_A | (uint64_t)(((a0 + (uint32_t)(2 * ks * kHaloPlane)) >> 4) & 0x3FFFu);
                             const uint64_t db = DESC_B | (uint64_t)(((b0 + 32u * ks) >> 4) & 0x3FFFu);
                             const uint32_t accum = (cc > 0 || ks > 0 || tap >= NACC) ? 1u : 0u;
@@ -729,20 +741,22 @@ int launch_tma_cout(const ConvArgs& a, int* err, cudaStream_t s)
 }
 
 // the persistent halo kernel for c_out = BN: all 9 x c_in x BN weights resident, as many CTAs per SM as shared memory
-// and the two accumulators per CTA in tensor memory (512 columns per SM) allow, one per SM at least
-template <int BN>
+// and the two accumulators per CTA in tensor memory (512 columns per SM) allow, one per SM at least. STREAM: the
+// weights come with each chunk's halo instead of staying.
+template <int BN, bool STREAM>
 int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
 {
     const int n_chunks = (c.c1 + c.c2) / 32;
-    const int smem = 1024 + 9 * n_chunks * BN * 64 + kHaloStages * kHaloStage;
+    const int smem = STREAM ? 1024 + kHaloStages * (kHaloStagePad + 9 * BN * 64)
+                            : 1024 + 9 * n_chunks * BN * 64 + kHaloStages * kHaloStage;
     static int configured[64] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
     if (configured[dev] < smem) {
-        if (cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-                cudaSuccess ||
-            cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
-                cudaSuccess)
+        if (cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN, STREAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) != cudaSuccess ||
+            cudaFuncSetAttribute(conv3x3_fwd_halo_kernel<BN, STREAM>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 100) != cudaSuccess)
             return EDP_ERR_CUDA;
         configured[dev] = smem;
     }
@@ -779,19 +793,26 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
     if (per_sm > 512 / kHaloTmemCols<BN>) per_sm = 512 / kHaloTmemCols<BN>;
     if (per_sm < 1) per_sm = 1;
     const int64_t grid = a.n_tiles < (int64_t)sms * per_sm ? a.n_tiles : (int64_t)sms * per_sm;
-    conv3x3_fwd_halo_kernel<BN><<<(unsigned)grid, kHaloFwdThreads, smem, s>>>(mw, mx1, mx2, a);
+    conv3x3_fwd_halo_kernel<BN, STREAM><<<(unsigned)grid, kHaloFwdThreads, smem, s>>>(mw, mx1, mx2, a);
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
 }
 
-// 0: the halo kernel where it applies (c_out 32, 64 or 128, the weights fit in shared memory, at least two tiles
-// per SM), else the tile kernel; 1: always the tile kernel; 2: always the halo kernel (refused where it does not apply)
+// 0: the halo kernel where it applies (c_out 32, 64 or 128 with the weights resident in shared memory, or 32 and 64
+// with them streamed, at least two tiles per SM), else the tile kernel; 1: always the tile kernel; 2: always the halo
+// kernel (refused where it does not apply)
 int g_conv_mode = 0;
+
+bool halo_resident(const ConvArgs& c) { return 9LL * (c.c1 + c.c2) * c.cout * 2 <= kHaloMaxWeights; }
+
+bool halo_possible(const ConvArgs& c)
+{
+    return c.cout == 32 || c.cout == 64 || (c.cout == 128 && halo_resident(c));
+}
 
 bool halo_applies(const ConvArgs& c)
 {
     const int64_t tiles = (int64_t)((c.w + 7) / 8) * ((c.h + 15) / 16) * c.nimg;
-    return (c.cout == 32 || c.cout == 64 || c.cout == 128) && 9LL * (c.c1 + c.c2) * c.cout * 2 <= kHaloMaxWeights &&
-           tiles >= 2 * 148;
+    return halo_possible(c) && tiles >= 2 * 148;
 }
 
 // wt_t[c][8 - tap][n] = wt[n][tap][c]: the weights of the data gradient
@@ -1390,11 +1411,12 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
     if (!err) return EDP_ERR_CUDA;
     const bool halo = g_conv_mode == 2 || (g_conv_mode == 0 && halo_applies(a));
     if (halo) {
-        if (9LL * (c1 + c2) * cout * 2 > kHaloMaxWeights) return EDP_ERR_ARG;
+        if (!halo_possible(a)) return EDP_ERR_ARG;
+        const bool res = halo_resident(a);
         switch (cout) {
-        case 32: return launch_halo<32>(a, err, s);
-        case 64: return launch_halo<64>(a, err, s);
-        case 128: return launch_halo<128>(a, err, s);
+        case 32: return res ? launch_halo<32, false>(a, err, s) : launch_halo<32, true>(a, err, s);
+        case 64: return res ? launch_halo<64, false>(a, err, s) : launch_halo<64, true>(a, err, s);
+        case 128: return launch_halo<128, false>(a, err, s);
         default: return EDP_ERR_ARG;
         }
     }

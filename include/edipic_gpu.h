@@ -440,9 +440,9 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
 int edp_nn_flip_transpose(const void* wt, int32_t cout, int32_t cin, void* out, void* stream);
 /* nonzero in *out when a bounded wait of the tensor-core convolution gave up since the last call (then cleared) */
 int edp_nn_error(int32_t* out);
-/* the forward kernel edp_nn_conv3x3_fwd uses (process-wide): 0 automatic (the persistent halo kernel for c_out of
- * 32, 64 or 128 when the layer's weights fit in shared memory, 9 c_in c_out 2 <= 112 KiB, and it has at least 296
- * patches of 8 x 16 pixels; else the tile kernel), 1 the tile kernel, 2 the halo kernel (EDP_ERR_ARG where it does
+/* the forward kernel edp_nn_conv3x3_fwd uses (process-wide): 0 automatic (the persistent halo kernel for layers of at
+ * least 296 patches of 8 x 16 pixels with c_out 32 or 64, or 128 when the weights fit in shared memory,
+ * 9 c_in c_out 2 <= 112 KiB, else the tile kernel), 1 the tile kernel, 2 the halo kernel (EDP_ERR_ARG where it does
  * not apply). No counterpart in the reference. */
 int edp_nn_conv_select(int32_t mode);
 int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,

@@ -79,13 +79,15 @@ def test_conv_kernels_match_oracle(c1, c2, cout, n, h, w):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (64, 0, 64), (32, 0, 128)])
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (64, 0, 64), (32, 0, 128),
+                                        (128, 64, 64), (256, 0, 32)])
 @pytest.mark.parametrize("n,h,w", [(1, 23, 13), (2, 40, 36), (3, 150, 97)])
 def test_halo_conv_matches_oracle(c1, c2, cout, n, h, w):
     """The persistent halo kernel (edp_nn_conv_select(2): 8 x 16-pixel patches, one 10 x 18 halo per 32-channel
-    chunk for all nine taps, resident weights, two tensor-memory accumulators) against the oracle, on images that do
-    not fill their last patch, concatenated inputs, and more patches than CTAs (each CTA takes several); then the
-    automatic choice gives the same output as the tile kernel within the BF16 rounding of both."""
+    chunk for all nine taps, weights resident or, above 112 KiB, streamed with each chunk, two tensor-memory
+    accumulators) against the oracle, on images that do not fill their last patch, concatenated inputs, and more
+    patches than CTAs (each CTA takes several); then the tile kernel gives the same output within the BF16 rounding
+    of both."""
     lib = library()
     rng = np.random.default_rng(7 * c1 + c2 + cout + h)
     x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
