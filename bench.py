@@ -222,7 +222,9 @@ def fp64_cycle_leg(args, stream_of):
 def network_leg():
     """The learned warm start's convolutions on the tensor cores: each of the 14 layers of the encoder-decoder timed
     alone at the inference shape (one image of the 513 x 513-node grid padded to 576 x 576) and at the training shape
-    (4 images), and the whole forward pass. FLOPs = 2 x pixels x 9 x c_in x c_out per layer."""
+    (4 images), and the whole forward pass. FLOPs = 2 x pixels x 9 x c_in x c_out per layer. A layer's device time
+    (`us`, the FLOP rate) is 20 calls replayed from a CUDA graph; `call_us` is the same calls made one by one from
+    Python, with the host's call and launch overhead."""
     # (the image is the 513 x 513-node grid padded to a multiple of 64)
     import torch
     from edipic_b200 import library, warmstart
@@ -239,9 +241,9 @@ def network_leg():
     scale = [1, 1, p, p, p ** 2, p ** 2, p ** 3, p ** 3, p ** 2, p ** 2, p, p, 1, 1]
     net = warmstart.WarmStartNet(seed=0)
     out = {"shape": f"{H}x{W}", "peak_tflops": peak, "peak_kind": peak_kind}
-    st = torch.cuda.current_stream()
+    st = torch.cuda.Stream()
     for nb in (1, 4):
-        tot_t, tot_f, per = 0.0, 0.0, []
+        tot_t, tot_f, tot_c, per = 0.0, 0.0, 0.0, []
         for l, (ci, co) in enumerate(warmstart.LAYERS):
             h, w = H // scale[l], W // scale[l]
             x = torch.randn(nb, h, w, ci, device="cuda").to(torch.bfloat16)
@@ -250,33 +252,53 @@ def network_leg():
             wb, bb = net.theta_bf[wo:bo], net.theta[bo:bo + co].detach()
             args = (nb, h, w, C.c_void_p(x.data_ptr()), ci, None, 0, C.c_void_p(wb.data_ptr()),
                     C.c_void_p(bb.data_ptr()), co, 1, C.c_void_p(y.data_ptr()), C.c_void_p(st.cuda_stream))
+            torch.cuda.synchronize()
             for _ in range(3):
                 lib.edp_nn_conv3x3_fwd(*args)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             reps = 20
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            # per call, with the host's call overhead (ctypes, launch)
             e0.record(st)
             for _ in range(reps):
                 lib.edp_nn_conv3x3_fwd(*args)
             e1.record(st)
             e1.synchronize()
+            t_call = e0.elapsed_time(e1) / 1e3 / reps
+            # device time: the same calls replayed from a CUDA graph captured on the same stream
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=st):
+                for _ in range(reps):
+                    lib.edp_nn_conv3x3_fwd(*args)
+            g.replay()
+            torch.cuda.synchronize()
+            e0.record(st)
+            with torch.cuda.stream(st):
+                g.replay()
+            e1.record(st)
+            e1.synchronize()
             t = e0.elapsed_time(e1) / 1e3 / reps
+            del g
             f = 2.0 * nb * h * w * 9 * ci * co
             tot_t += t
+            tot_c += t_call
             tot_f += f
-            per.append({"layer": l, "cin": ci, "cout": co, "hw": [h, w], "us": 1e6 * t, "tflops": f / t / 1e12})
+            per.append({"layer": l, "cin": ci, "cout": co, "hw": [h, w], "us": 1e6 * t, "call_us": 1e6 * t_call,
+                        "tflops": f / t / 1e12})
         x = torch.randn(nb, H, W, 32, device="cuda").to(torch.bfloat16)
+        cs = torch.cuda.current_stream()   # the training wrappers launch on torch's current stream
         with torch.no_grad():
             for _ in range(3):
                 net.forward(x)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
+            e0.record(cs)
             for _ in range(10):
                 net.forward(x)
-            e1.record(st)
+            e1.record(cs)
             e1.synchronize()
         fwd = e0.elapsed_time(e1) / 10
         out[f"batch{nb}"] = {"conv_ms": 1e3 * tot_t, "conv_gflop": tot_f / 1e9, "conv_tflops": tot_f / tot_t / 1e12,
-                             "frac": tot_f / tot_t / 1e12 / peak, "forward_ms": fwd, "layers": per}
+                             "frac": tot_f / tot_t / 1e12 / peak, "conv_ms_per_call": 1e3 * tot_c,
+                             "forward_ms": fwd, "layers": per}
     return out
 
 

@@ -621,9 +621,53 @@ EncodeTiledFn encode_fn()
     return fn;
 }
 
-// NHWC activations with c channels: dims (c, w, h, n), box (cw, 16, 8, 1)
-bool map_act(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int cw)
+// Tensor maps already encoded, by what they encode (kind, address, sizes): a layer called again with the same
+// buffers, as every solve's inference and every training step does, copies its maps instead of encoding them. A map
+// holds no reference to the memory, so a buffer freed and another placed at the same address with the same sizes
+// needs exactly the same map.
+struct MapKey {
+    int kind;
+    const void* p;
+    int a, b, c, d, e;
+    bool operator==(const MapKey& o) const
+    {
+        return kind == o.kind && p == o.p && a == o.a && b == o.b && c == o.c && d == o.d && e == o.e;
+    }
+};
+
+bool map_cached(const MapKey& k, CUtensorMap* m, bool (*make)(const MapKey&, CUtensorMap*))
 {
+    constexpr int kEntries = 256;
+    static std::mutex mu;
+    static MapKey keys[kEntries];
+    static CUtensorMap maps[kEntries];
+    static int used = 0, next = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    MapKey key = k;
+    key.e = key.e * 64 + dev;   // maps are per device
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (int i = 0; i < used; ++i)
+            if (keys[i] == key) {
+                *m = maps[i];
+                return true;
+            }
+    }
+    if (!make(k, m)) return false;
+    std::lock_guard<std::mutex> lock(mu);
+    keys[next] = key;
+    maps[next] = *m;
+    next = (next + 1) % kEntries;
+    if (used < kEntries) ++used;
+    return true;
+}
+
+// NHWC activations with c channels: dims (c, w, h, n), box (cw, 16, 8, 1)
+bool make_act(const MapKey& k, CUtensorMap* m)
+{
+    const void* x = k.p;
+    const int nimg = k.a, h = k.b, w = k.c, c = k.d, cw = k.e;
     EncodeTiledFn f = encode_fn();
     if (!f) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
@@ -635,10 +679,17 @@ bool map_act(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int c
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool map_act(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int cw)
+{
+    return map_cached(MapKey{0, x, nimg, h, w, c, cw}, m, make_act);
+}
+
 // NHWC activations with c channels for the halo kernel: dims (c, w, h, n), box (8 channels, 10, 18, 1) without
 // swizzle, which lands in shared memory as one plane (pixel q of the 10 x 18 halo at byte 16 q)
-bool map_halo(CUtensorMap* m, const void* x, int nimg, int h, int w, int c)
+bool make_halo(const MapKey& k, CUtensorMap* m)
 {
+    const void* x = k.p;
+    const int nimg = k.a, h = k.b, w = k.c, c = k.d;
     EncodeTiledFn f = encode_fn();
     if (!f) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
@@ -650,9 +701,16 @@ bool map_halo(CUtensorMap* m, const void* x, int nimg, int h, int w, int c)
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// weights [cout][k]: dims (k, cout), box (cw, bn)
-bool map_wt(CUtensorMap* m, const void* wt, int k, int cout, int cw, int bn)
+bool map_halo(CUtensorMap* m, const void* x, int nimg, int h, int w, int c)
 {
+    return map_cached(MapKey{1, x, nimg, h, w, c, 0}, m, make_halo);
+}
+
+// weights [cout][k]: dims (k, cout), box (cw, bn)
+bool make_wt(const MapKey& key, CUtensorMap* m)
+{
+    const void* wt = key.p;
+    const int k = key.a, cout = key.b, cw = key.c, bn = key.d;
     EncodeTiledFn f = encode_fn();
     if (!f) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)cout};
@@ -662,6 +720,11 @@ bool map_wt(CUtensorMap* m, const void* wt, int k, int cout, int cw, int bn)
     return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(wt), dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, cw == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool map_wt(CUtensorMap* m, const void* wt, int k, int cout, int cw, int bn)
+{
+    return map_cached(MapKey{2, wt, k, cout, cw, bn, 0}, m, make_wt);
 }
 
 template <int BN, int CW>
