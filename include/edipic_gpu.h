@@ -186,9 +186,9 @@ int edp_get_stream(edp_ctx* ctx, void** stream_out);
  * do not depend on when sorts happen; this only moves the cost. Synchronises. */
 int edp_sort_particles(edp_ctx* ctx);
 /* No counterpart in the reference. Kernel of the mixed-precision push over the sorted particles: 0 one CTA per
- * sorted chunk, the threads load their particles (default); 1 persistent CTAs whose particle columns are streamed
- * into shared memory by bulk copies, 4 particles per thread, 2 stages in flight; 2 the same with 2 particles per
- * thread and 3 stages; 3 as 0 with 2 particles per thread (more resident warps); 4 as 0 with each thread's next 4
+ * sorted chunk, the threads load their particles; 1 persistent CTAs whose particle columns are streamed into shared
+ * memory by bulk copies, 4 particles per thread, 2 stages in flight; 2 the same with 2 particles per thread and 3
+ * stages; 3 as 0 with 2 particles per thread (more resident warps); 4 (default) as 0 with each thread's next 4
  * particles copied into shared memory by cp.async while it pushes the current ones. All give the same results;
  * only the speed differs. */
 int edp_set_push_kernel(edp_ctx* ctx, int32_t kind);
