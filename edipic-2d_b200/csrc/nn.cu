@@ -706,6 +706,28 @@ bool map_halo(CUtensorMap* m, const void* x, int nimg, int h, int w, int c)
     return map_cached(MapKey{1, x, nimg, h, w, c, 0}, m, make_halo);
 }
 
+// NHWC tensor with c channels for the weight gradient's patches: box (cb channels, 8 x, 16 y, 1), an 8 x 16 patch
+// as 128 pixel rows of cb channels (pixel q = 8 y + x), in the 64-byte (cb = 32) or 128-byte (cb = 64) swizzle
+bool make_patch(const MapKey& k, CUtensorMap* m)
+{
+    const void* x = k.p;
+    const int nimg = k.a, h = k.b, w = k.c, c = k.d, cb = k.e;
+    EncodeTiledFn f = encode_fn();
+    if (!f) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * w, (cuuint64_t)c * 2 * w * h};
+    const cuuint32_t box[4] = {(cuuint32_t)cb, 8, 16, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, cb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool map_patch(CUtensorMap* m, const void* x, int nimg, int h, int w, int c, int cb)
+{
+    return map_cached(MapKey{3, x, nimg, h, w, c, cb}, m, make_patch);
+}
+
 // weights [cout][k]: dims (k, cout), box (cw, bn)
 bool make_wt(const MapKey& key, CUtensorMap* m)
 {
@@ -1181,7 +1203,230 @@ __global__ void __launch_bounds__(kHaloThreads, 1) conv3x3_wgrad_tc_kernel(Wgrad
     }
 }
 
-// 0 (default) and 2: the weight gradient on tcgen05; 1: the mma.sync kernel
+// ------------------------------------------------------------------------------------------ weight gradient, taps in M
+// The weight gradient with the taps stacked along M: dw[n][tap][c] = sum_q dz[q - off(tap)][n] x[q][c] is, per
+// group of 4 taps, one GEMM with M = (tap, c) rows (4 taps x a 32-channel chunk of x = 128), N = n (a chunk of NB
+// output channels), K = the pixels q of an 8 x 16 patch. Its A operand is four copies of the x patch shifted by the
+// four taps' offsets, B the dz patch, both MN-major: each copy is one TMA box of (32 channels, 8 x, 16 y) of the NHWC
+// tensor, zero-filled off the image, landing as 128 pixel rows of 64 bytes in the 64-byte swizzle (one swizzle atom
+// of 32 channels across, 8-pixel groups 512 bytes apart = SBO, the taps one copy apart = LBO); dz comes the same way,
+// or as 64-channel boxes in the 128-byte swizzle. Taps 0-3 and 4-7 are two M = 128 MMAs per K step, tap 8 an
+// M = 64 MMA (its copy followed by a zero copy), so a patch takes 24 MMAs where the taps in N would take 72 of
+// M = 64 with half of each padding when c_out = 32. The three accumulators (3 x NB columns) stay
+// in tensor memory for the CTA's whole pixel range; at the end each lane adds its row (one tap and x channel) to dw
+// for every n (red.global.add.f32, 32 consecutive channels per warp and n). Roles: warp 0 lane 0 copies (TMA),
+// warp 1 lane 0 issues the MMAs, warps 2-5 read the accumulators back. Every wait is bounded.
+constexpr int kTapThreads = 192;
+constexpr int kTapStages = 2;
+constexpr int kTapCopy = 128 * 64;                     // one shifted copy: 128 pixels x 32 channels (64-byte swizzle)
+constexpr int kTapXBytes = 10 * kTapCopy;              // 9 taps, then a zero copy after tap 8
+
+template <int NB>
+__global__ void __launch_bounds__(kTapThreads, 1) conv3x3_wgrad_tap_kernel(const __grid_constant__ CUtensorMap mx1,
+                                                                        const __grid_constant__ CUtensorMap mx2,
+                                                                        const __grid_constant__ CUtensorMap mdz,
+                                                                        WgradTcArgs a)
+{
+    constexpr int STAGE = kTapXBytes + NB * 256;   // + the dz patch: 128 pixels x NB channels
+    constexpr uint32_t TMEM_COLS = 3 * NB <= 128 ? 128 : 3 * NB <= 256 ? 256 : 512;
+    // A and B both MN-major (bits 15, 16), M = 128 or 64, N = NB
+    constexpr uint32_t IDESC128 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                  ((uint32_t)(NB >> 3) << 17) | ((128u >> 4) << 24);
+    constexpr uint32_t IDESC64 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                 ((uint32_t)(NB >> 3) << 17) | ((64u >> 4) << 24);
+    // MN-major, swizzled: the 32 channels of a tap copy are one 64-byte swizzle atom per pixel row, 8-pixel groups
+    // 512 bytes apart (SBO), the taps one copy apart (LBO); dz: 32 channels in the same 64-byte layout, or 64-channel
+    // groups of 128-byte rows (8-pixel groups 1024 bytes apart, groups 128 pixels x 128 bytes apart)
+    constexpr uint64_t DESC_A = ((uint64_t)(512 >> 4) << 32) | ((uint64_t)(kTapCopy >> 4) << 16) | ((uint64_t)1 << 46) |
+                                ((uint64_t)4 << 61);
+    constexpr int B_ROW = NB == 32 ? 64 : 128;      // bytes per pixel row of the dz patch
+    constexpr uint64_t DESC_B = ((uint64_t)((8 * B_ROW) >> 4) << 32) | ((uint64_t)((128 * B_ROW) >> 4) << 16) |
+                                ((uint64_t)1 << 46) | ((uint64_t)(NB == 32 ? 4 : 2) << 61);
+    extern __shared__ unsigned char dsm[];
+    __shared__ __align__(8) uint64_t full[kTapStages], empty[kTapStages], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = a.c1 + a.c2;
+    const int c0 = blockIdx.y * 32;    // x channels of this CTA
+    const int n0 = blockIdx.z * NB;    // output channels of this CTA
+    const uint32_t base = (smem_u32(dsm) + 1023u) & ~1023u;
+    unsigned char* gbase = dsm + (base - smem_u32(dsm));
+
+    // the copy after tap 8's stays zero: the M = 64 MMA of tap 8 reads it as its padding rows
+    for (int st = 0; st < kTapStages; ++st)
+        for (int b = 9 * kTapCopy + tid * 16; b < 10 * kTapCopy; b += kTapThreads * 16)
+            *reinterpret_cast<uint4*>(gbase + st * STAGE + b) = make_uint4(0u, 0u, 0u, 0u);
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int st = 0; st < kTapStages; ++st) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[st])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[st])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&done_bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // the zero planes, for the MMAs' async reads
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    const int64_t stride = gridDim.x;
+
+    if (warp == 0) {
+        // ---------------- copies (lane 0): per patch the 36 planes of the nine shifted x copies and the dz planes
+        if (lane == 0) {
+            const CUtensorMap* mx = c0 < a.c1 ? &mx1 : &mx2;
+            const int xco = c0 < a.c1 ? c0 : c0 - a.c1;
+            constexpr uint32_t BYTES = 9 * kTapCopy + NB * 256;
+            int64_t it = 0;
+            for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride, ++it) {
+                const int s = (int)(it % kTapStages);
+                if (it >= kTapStages &&
+                    !mbar_wait_or_fail(smem_u32(&empty[s]), (uint32_t)(((it / kTapStages) - 1) & 1), &fail_sh))
+                    break;
+                const int tx = (int)(t % a.tiles_x), ty = (int)((t / a.tiles_x) % a.tiles_y);
+                const int img = (int)(t / ((int64_t)a.tiles_x * a.tiles_y));
+                const int px0 = tx * 8, py0 = ty * 16;
+                const uint32_t st = base + (uint32_t)(s * STAGE), fb = smem_u32(&full[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(BYTES) : "memory");
+                for (int tap = 0; tap < 9; ++tap)
+                    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                                 ::"r"(st + (uint32_t)(tap * kTapCopy)), "l"(mx), "r"(xco), "r"(px0 + tap % 3 - 1),
+                                   "r"(py0 + tap / 3 - 1), "r"(img), "r"(fb) : "memory");
+                for (int j = 0; j < NB * 2 / B_ROW; ++j)
+                    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+                                 ::"r"(st + (uint32_t)(kTapXBytes + j * 128 * B_ROW)), "l"(&mdz),
+                                   "r"(n0 + j * (B_ROW / 2)), "r"(px0), "r"(py0), "r"(img), "r"(fb) : "memory");
+            }
+            // copies still in flight after a failure land before the CTA leaves
+            for (int64_t q = it > kTapStages ? it - kTapStages : 0; q < it; ++q)
+                mbar_wait(smem_u32(&full[q % kTapStages]), (uint32_t)((q / kTapStages) & 1));
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMAs (lane 0): per K step of 16 pixels, taps 0-3, taps 4-7 (M = 128), tap 8 (M = 64)
+        if (lane == 0) {
+            int64_t it = 0;
+            for (int64_t t = blockIdx.x; t < a.n_tiles && !fail_sh; t += stride, ++it) {
+                const int s = (int)(it % kTapStages);
+                if (!mbar_wait_or_fail(smem_u32(&full[s]), (uint32_t)((it / kTapStages) & 1), &fail_sh)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t xs = base + (uint32_t)(s * STAGE), zs = xs + (uint32_t)kTapXBytes;
+                for (int ks = 0; ks < 8; ++ks) {
+                    // a K step is 16 pixel rows: two 8-row groups
+                    const uint64_t db = DESC_B | (uint64_t)(((zs + (uint32_t)(16 * B_ROW * ks)) >> 4) & 0x3FFFu);
+                    const uint32_t accum = (it > 0 || ks > 0) ? 1u : 0u;
+                    for (int g = 0; g < 3; ++g) {
+                        const uint64_t da =
+                            DESC_A | (uint64_t)(((xs + (uint32_t)(g * 4 * kTapCopy + 1024 * ks)) >> 4) & 0x3FFFu);
+                        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                                     ::"r"(tmem + (uint32_t)(g * NB)), "l"(da), "l"(db),
+                                       "r"(g < 2 ? IDESC128 : IDESC64), "r"(accum));
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                             ::"r"(smem_u32(&empty[s])) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         ::"r"(smem_u32(&done_bar)) : "memory");
+            mbar_wait_or_fail(smem_u32(&done_bar), 0u, &fail_sh);
+        }
+        __syncwarp();
+    }
+    __syncthreads();   // the copies and the MMAs are done (or gave up)
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp >= 2 && blockIdx.x < a.n_tiles && !fail_sh) {
+        // ---------------- the accumulators into dw: warp quarter q = warp % 4 reads lanes 32 q .. 32 q + 31
+        const int q = warp & 3;
+        for (int g = 0; g < 3; ++g) {
+            // M = 128 groups: row 32 q + lane = tap 4 g + q, x channel lane; the M = 64 group (tap 8): rows 0-15 in
+            // lanes 0-15, rows 16-31 in lanes 32-47, x channel 16 q + lane
+            if (g == 2 && q > 1) break;
+            const int tap = g < 2 ? 4 * g + q : 8;
+            const int c = g < 2 ? lane : 16 * q + lane;
+            const bool valid = g < 2 || lane < 16;
+            float* d = a.dw + ((int64_t)n0 * 9 + tap) * cin + c0 + c;
+            for (int h = 0; h < NB / 16; ++h) {
+                uint32_t v[16];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+                             " [%16];\n"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                               "=r"(v[14]), "=r"(v[15])
+                             : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * NB + 16 * h)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (valid)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        atomicAdd(d + (int64_t)(16 * h + j) * 9 * cin, __uint_as_float(v[j]));
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (fail_sh && tid == 0) atomicExch(a.err, 1);
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// one CTA per SM (two stages of the nine shifted x copies and the dz patch take most of its shared memory), the
+// patches split over the CTAs of each (x chunk, output chunk) pair
+template <int NB>
+int launch_wgrad_tap(const WgradArgs& w, int* err, cudaStream_t s)
+{
+    constexpr int SMEM = 1024 + kTapStages * (kTapXBytes + NB * 256);
+    static bool configured[64] = {false};
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EDP_ERR_CUDA;
+    if (!configured[dev]) {
+        if (cudaFuncSetAttribute(conv3x3_wgrad_tap_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) !=
+            cudaSuccess)
+            return EDP_ERR_CUDA;
+        configured[dev] = true;
+    }
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return EDP_ERR_CUDA;
+    CUtensorMap mx1, mx2, mdz;
+    if (!map_patch(&mx1, w.x, w.nimg, w.h, w.w, w.c1, 32)) return EDP_ERR_CUDA;
+    if (w.c2 > 0) {
+        if (!map_patch(&mx2, w.x2, w.nimg, w.h, w.w, w.c2, 32)) return EDP_ERR_CUDA;
+    } else {
+        mx2 = mx1;
+    }
+    if (!map_patch(&mdz, w.dz, w.nimg, w.h, w.w, w.cout, NB == 32 ? 32 : 64)) return EDP_ERR_CUDA;
+    WgradTcArgs a;
+    a.x1 = w.x;
+    a.x2 = w.x2;
+    a.c1 = w.c1;
+    a.c2 = w.c2;
+    a.dz = w.dz;
+    a.cout = w.cout;
+    a.nimg = w.nimg;
+    a.h = w.h;
+    a.w = w.w;
+    a.tiles_x = (w.w + 7) / 8;
+    a.tiles_y = (w.h + 15) / 16;
+    a.n_tiles = (int64_t)a.tiles_x * a.tiles_y * w.nimg;
+    a.dw = w.dw;
+    a.err = err;
+    const int n_c = (w.c1 + w.c2) / 32, n_n = w.cout / NB;
+    int64_t split = (sms + (int64_t)n_c * n_n - 1) / ((int64_t)n_c * n_n);
+    if (split > a.n_tiles) split = a.n_tiles;
+    if (split < 1) split = 1;
+    conv3x3_wgrad_tap_kernel<NB><<<dim3((unsigned)split, (unsigned)n_c, (unsigned)n_n), kTapThreads, SMEM, s>>>(
+        mx1, mx2, mdz, a);
+    return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
+}
+
+// 0 (default): the weight gradient on tcgen05 with the taps in M; 2: on tcgen05 with the taps in N; 1: mma.sync
 int g_wgrad_mode = 0;
 
 // one CTA per SM (its 9 x 32 accumulator columns take 512 of tensor memory), the patches split over the CTAs of each
@@ -1488,7 +1733,8 @@ int edp_nn_conv3x3_fwd(int32_t nimg, int32_t h, int32_t w, const void* x1, int32
     return launch_tma_cout<32>(a, err, s);
 }
 
-/* which weight-gradient kernel edp_nn_conv3x3_wgrad uses: 0 (default) or 2 tcgen05, 1 mma.sync */
+/* which weight-gradient kernel edp_nn_conv3x3_wgrad uses: 0 (default) tcgen05 with the taps in M, 2 tcgen05 with
+ * the taps in N, 1 mma.sync */
 int edp_nn_wgrad_select(int32_t mode)
 {
     if (mode < 0 || mode > 2) return EDP_ERR_ARG;
@@ -1547,7 +1793,16 @@ int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int
     if (g_wgrad_mode != 1) {
         int* err = tc_error_word();
         if (!err) return EDP_ERR_CUDA;
-        const int rc = cout % 128 == 0 ? launch_wgrad_tc<128>(a, err, s) : launch_wgrad_tc<64>(a, err, s);
+        int rc;
+        if (g_wgrad_mode == 2) {
+            rc = cout % 128 == 0 ? launch_wgrad_tc<128>(a, err, s) : launch_wgrad_tc<64>(a, err, s);
+        } else {
+            // output channels per CTA: the largest of 128, 64, 32 that divides c_out
+            const int nb = cout % 128 == 0 ? 128 : cout % 64 == 0 ? 64 : 32;
+            rc = nb == 128 ? launch_wgrad_tap<128>(a, err, s)
+                 : nb == 64 ? launch_wgrad_tap<64>(a, err, s)
+                            : launch_wgrad_tap<32>(a, err, s);
+        }
         if (rc != EDP_OK) return rc;
         if (db) {
             const int lanes = 1024 / cout;

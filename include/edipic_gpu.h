@@ -447,8 +447,8 @@ int edp_nn_error(int32_t* out);
 int edp_nn_conv_select(int32_t mode);
 int edp_nn_conv3x3_wgrad(int32_t nimg, int32_t h, int32_t w, const void* x1, int32_t c1, const void* x2, int32_t c2,
                          const void* dz, int32_t cout, float* dw, float* db, void* stream);
-/* the weight-gradient kernel edp_nn_conv3x3_wgrad uses (process-wide): 0 or 2 tcgen05 (default), 1 mma.sync.
- * No counterpart in the reference. */
+/* the weight-gradient kernel edp_nn_conv3x3_wgrad uses (process-wide): 0 (default) tcgen05 with the taps stacked in
+ * M, 2 tcgen05 with the taps' accumulators side by side in N, 1 mma.sync. No counterpart in the reference. */
 int edp_nn_wgrad_select(int32_t mode);
 /* f x f average pooling (h, w: input size) and nearest f x upsampling (h, w: output size), f = 2 or 4 */
 int edp_nn_pool(int32_t nimg, int32_t h, int32_t w, int32_t c, int32_t f, const void* x, void* y, void* stream);

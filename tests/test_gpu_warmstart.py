@@ -124,12 +124,14 @@ def test_halo_conv_matches_oracle(c1, c2, cout, n, h, w):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (128, 64, 128), (64, 0, 96)])
+@pytest.mark.parametrize("c1,c2,cout", [(32, 0, 32), (64, 32, 32), (32, 0, 64), (128, 64, 128), (64, 0, 96),
+                                        (32, 0, 256)])
 @pytest.mark.parametrize("n,h,w", [(1, 9, 9), (3, 150, 97)])
 def test_wgrad_kernels_match_oracle(c1, c2, cout, n, h, w):
-    """The weight gradient on tcgen05 (edp_nn_wgrad_select(0): 8 x 16-pixel patches as the K dimension, the nine
-    taps' accumulators in tensor memory, M = 64 output channels with zero rows past c_out, or 128) and on mma.sync
-    (select 1) against the oracle, accumulated onto a nonzero dw, with more patches than CTAs."""
+    """The weight gradient on tcgen05 with the taps in M (edp_nn_wgrad_select(0): four shifted copies of the x patch
+    per M = 128 MMA, tap 8 in an M = 64 one, K = the pixels of 8 x 16 patches), on tcgen05 with the taps in N
+    (select 2: the nine taps' accumulators in tensor memory, M = output channels) and on mma.sync (select 1), against
+    the oracle, accumulated onto a nonzero dw, with more patches than CTAs."""
     lib = library()
     rng = np.random.default_rng(5 * c1 + c2 + cout + h)
     x1 = O.bf16(rng.normal(0, 1, (n, h, w, c1)))
@@ -141,7 +143,7 @@ def test_wgrad_kernels_match_oracle(c1, c2, cout, n, h, w):
     w0 = rng.normal(0, 1, (cout, 9, cin)).astype(np.float32)
     rw, rb = O.conv_wgrad(xin, dz)
     try:
-        for mode in (0, 1):
+        for mode in (0, 1, 2):
             assert lib.edp_nn_wgrad_select(mode) == 0
             dw = _f32(w0)
             db = torch.zeros(cout, device="cuda", dtype=torch.float32)
