@@ -395,12 +395,42 @@ def time_layer(cin, cout, h, w, nimg, reps=10):
     return t * 1e6, 2.0 * nimg * h * w * 9 * cin * cout / t / 1e12
 
 
+def time_wgrad(cin, cout, h, w, nimg, reps=10):
+    """CUDA-event time (us) and TFLOP/s of one weight gradient (with the bias gradient) of the network's kind."""
+    torch = _torch()
+    lib = library()
+    st = torch.cuda.current_stream()
+    x = torch.randn(nimg, h, w, cin, device="cuda").to(torch.bfloat16)
+    dz = torch.randn(nimg, h, w, cout, device="cuda").to(torch.bfloat16)
+    dw = torch.zeros(cout, 9, cin, device="cuda")
+    db = torch.zeros(cout, device="cuda")
+    args = (nimg, h, w, _ptr(x), cin, None, 0, _ptr(dz), cout, _ptr(dw), _ptr(db), C.c_void_p(st.cuda_stream))
+    for _ in range(3):
+        _check(lib.edp_nn_conv3x3_wgrad(*args), "conv3x3_wgrad")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        lib.edp_nn_conv3x3_wgrad(*args)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / reps * 1e-3
+    return t * 1e6, 2.0 * nimg * h * w * 9 * cin * cout / t / 1e12
+
+
 if __name__ == "__main__":
-    # python -m edipic_b200.warmstart CIN COUT H W IMAGES [KERNEL]: times one convolution layer; KERNEL selects the
-    # forward kernel as edp_nn_conv_select does (0 automatic, 1 tile, 2 persistent halo)
+    # python -m edipic_b200.warmstart CIN COUT H W IMAGES [KERNEL]: times one forward convolution layer; KERNEL selects
+    # the forward kernel as edp_nn_conv_select does (0 automatic, 1 tile, 2 persistent halo).
+    # python -m edipic_b200.warmstart wgrad CIN COUT H W IMAGES [KERNEL]: the weight gradient instead; KERNEL as
+    # edp_nn_wgrad_select (0 tcgen05 with the taps in M, 1 mma.sync, 2 tcgen05 with the taps in N)
     import sys
-    a = [int(v) for v in sys.argv[1:6]]
-    if len(sys.argv) > 6:
-        _check(library().edp_nn_conv_select(int(sys.argv[6])), "edp_nn_conv_select")
-    us, tf = time_layer(*a)
-    print(f"{a[0]}->{a[1]} {a[4]}x{a[2]}x{a[3]}: {us:.1f} us, {tf:.1f} TFLOP/s")
+    argv = sys.argv[1:]
+    wgrad = bool(argv) and argv[0] == "wgrad"
+    if wgrad:
+        argv = argv[1:]
+    a = [int(v) for v in argv[0:5]]
+    if len(argv) > 5:
+        sel = library().edp_nn_wgrad_select if wgrad else library().edp_nn_conv_select
+        _check(sel(int(argv[5])), "kernel select")
+    us, tf = (time_wgrad if wgrad else time_layer)(*a)
+    kind = "wgrad" if wgrad else "fwd"
+    print(f"{kind} {a[0]}->{a[1]} {a[4]}x{a[2]}x{a[3]}: {us:.1f} us, {tf:.1f} TFLOP/s")
