@@ -22,12 +22,22 @@ __global__ void hist_kernel(const int32_t* __restrict__ cell, const unsigned lon
 {
     const int64_t n = (int64_t)*n_slots;
     const int lane = threadIdx.x & 31;
-    for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x; k0 < n; k0 += (int64_t)gridDim.x * blockDim.x) {
-        int64_t k = k0 + threadIdx.x;
-        int c = k < n ? cell[k] : -1;
-        uint32_t key = c >= 0 ? tile_key(c, k, ntx) : 0xFFFFFFFFu;
-        unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-        if (key != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&count[key], (uint32_t)__popc(peers));
+    // four blocks of slots per round, their loads issued together
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k0 = (int64_t)blockIdx.x * blockDim.x; k0 < n; k0 += 4 * step) {
+        int c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t k = k0 + u * step + threadIdx.x;
+            c[u] = k < n ? __ldcs(cell + k) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t k = k0 + u * step + threadIdx.x;
+            const uint32_t key = c[u] >= 0 ? tile_key(c[u], k, ntx) : 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+            if (key != 0xFFFFFFFFu && lane == __ffs(peers) - 1) atomicAdd(&count[key], (uint32_t)__popc(peers));
+        }
     }
 }
 
