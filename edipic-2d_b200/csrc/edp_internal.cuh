@@ -80,6 +80,14 @@ __device__ __forceinline__ uint32_t edp_tile_key(int cell, int64_t k, int ntx)
     return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)((k >> 5) & 255);
 }
 
+// the lanes of the (full) warp holding the same key as this lane; a run of 32 sorted slots mostly shares one key,
+// which a shuffle and a vote settle without the slower match
+__device__ __forceinline__ unsigned edp_warp_peers(uint32_t key)
+{
+    const uint32_t k0 = __shfl_sync(0xFFFFFFFFu, key, 0);
+    return __all_sync(0xFFFFFFFFu, key == k0) ? 0xFFFFFFFFu : __match_any_sync(0xFFFFFFFFu, key);
+}
+
 struct edp_species_fp64 {
     double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;  // x < -1e29: dead
     uint32_t* id = nullptr;

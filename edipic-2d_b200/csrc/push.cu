@@ -510,27 +510,13 @@ __device__ __forceinline__ void push_chunk_prefetch(const PushArgs& a, Smem& s, 
 // its cell before the push and its source slot) is a coalesced 128-byte run per column. A particle absorbed now
 // leaves a dead slot, compacted by the next sort. Called warp-uniformly (every lane, every block).
 template <bool ION, bool PER, bool ROT, bool WIN>
-__device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t b,
-                                                   int64_t lo, int64_t hi)
+__device__ __forceinline__ void scatter_body(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t b, int* c,
+                                             float* ox, float* oy, float* vx, float* vy, float* vz,
+                                             const uint32_t* id, const int* tag)
 {
     const int lane = threadIdx.x & 31;
-    int c[4], cpre[4], tag[4];
-    float ox[4], oy[4], vx[4], vy[4], vz[4];
-    uint32_t id[4];
+    int cpre[4];
     bool sel[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const int64_t k = b + 32 * e + lane;
-        const bool ok = k >= lo && k < hi;
-        c[e] = ok ? __ldcs(a.P.cell + k) : -1;
-        ox[e] = ok ? __ldcs(a.P.ox + k) : 0.f;
-        oy[e] = ok ? __ldcs(a.P.oy + k) : 0.f;
-        vx[e] = ok ? __ldcs(a.P.vx + k) : 0.f;
-        vy[e] = ok ? __ldcs(a.P.vy + k) : 0.f;
-        vz[e] = ok ? __ldcs(a.P.vz + k) : 0.f;
-        id[e] = ok ? __ldcs(a.P.id + k) : 0u;
-        tag[e] = ok ? __ldcs(a.P.tag + k) : 0;
-    }
     DepAcc acc;
     acc.b = -1;
 #pragma unroll
@@ -547,16 +533,23 @@ __device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, i
     }
     dep_flush(s, acc);
     __syncwarp();
+    // the four cursor atomics are issued before any of their results is used, so their round trips overlap
+    uint32_t key[4];
+    unsigned peers[4];
+    unsigned long long b0[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const uint32_t key = cpre[e] >= 0 ? edp_tile_key(cpre[e], b + 32 * e + lane, a.ntx) : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-        const int leader = __ffs(peers) - 1;
-        unsigned long long b0 = 0;
-        if (key != 0xFFFFFFFFu && lane == leader) b0 = atomicAdd(&a.cursor[key], (unsigned long long)__popc(peers));
-        b0 = __shfl_sync(0xFFFFFFFFu, b0, leader);
-        if (key == 0xFFFFFFFFu) continue;
-        const unsigned long long pos = b0 + __popc(peers & ((1u << lane) - 1u));
+        key[e] = cpre[e] >= 0 ? edp_tile_key(cpre[e], b + 32 * e + lane, a.ntx) : 0xFFFFFFFFu;
+        peers[e] = edp_warp_peers(key[e]);
+        b0[e] = 0;
+        if (key[e] != 0xFFFFFFFFu && lane == __ffs(peers[e]) - 1)
+            b0[e] = atomicAdd(&a.cursor[key[e]], (unsigned long long)__popc(peers[e]));
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const unsigned long long base = __shfl_sync(0xFFFFFFFFu, b0[e], __ffs(peers[e]) - 1);
+        if (key[e] == 0xFFFFFFFFu) continue;
+        const unsigned long long pos = base + __popc(peers[e] & ((1u << lane) - 1u));
         if ((int64_t)pos >= a.cap) {
             atomicOr(&a.dc->error_flags, EDP_EFLAG_CAPACITY);
             continue;
@@ -572,6 +565,30 @@ __device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, i
         __stcs(a.D.tag + pos, tag[e]);
         if (sel[e]) select_slot(a, s, (uint32_t)pos);
     }
+}
+
+template <bool ION, bool PER, bool ROT, bool WIN>
+__device__ __forceinline__ void push_block_scatter(const PushArgs& a, Smem& s, int wx0, int wy0, int64_t b,
+                                                   int64_t lo, int64_t hi)
+{
+    const int lane = threadIdx.x & 31;
+    int c[4], tag[4];
+    float ox[4], oy[4], vx[4], vy[4], vz[4];
+    uint32_t id[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int64_t k = b + 32 * e + lane;
+        const bool ok = k >= lo && k < hi;
+        c[e] = ok ? __ldcs(a.P.cell + k) : -1;
+        ox[e] = ok ? __ldcs(a.P.ox + k) : 0.f;
+        oy[e] = ok ? __ldcs(a.P.oy + k) : 0.f;
+        vx[e] = ok ? __ldcs(a.P.vx + k) : 0.f;
+        vy[e] = ok ? __ldcs(a.P.vy + k) : 0.f;
+        vz[e] = ok ? __ldcs(a.P.vz + k) : 0.f;
+        id[e] = ok ? __ldcs(a.P.id + k) : 0u;
+        tag[e] = ok ? __ldcs(a.P.tag + k) : 0;
+    }
+    scatter_body<ION, PER, ROT, WIN>(a, s, wx0, wy0, b, c, ox, oy, vx, vy, vz, id, tag);
 }
 
 // IPT particles per thread: 4 (128-bit accesses, 4 CTAs of 256 per SM) or 2 (64-bit, 5 CTAs per SM). SCAT: the
@@ -1510,8 +1527,17 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
             b.mcc = c->mcc_dev;
             b.born = c->born_dev;
             b.dc = c->dc;
+            // one resident wave: the selected list is strided over exactly the CTAs that fit at once, so no CTA
+            // waits for a second wave on a few SMs
+            static int coll_sm = 0, coll_per_sm = 0;
+            if (!coll_sm) {
+                EDP_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&coll_per_sm, collide_selected_kernel,
+                                                                          256, 0));
+                EDP_CUDA(c, cudaDeviceGetAttribute(&coll_sm, cudaDevAttrMultiProcessorCount, c->device));
+                coll_per_sm = std::max(coll_per_sm, 1);
+            }
             ++c->launches;
-            collide_selected_kernel<<<148 * 4, 256, 0, c->stream>>>(b);
+            collide_selected_kernel<<<(unsigned)(coll_sm * coll_per_sm), 256, 0, c->stream>>>(b);
         }
     } else {
         PushArgs64 a;

@@ -123,7 +123,7 @@ __global__ void scatter_kernel(edp_species_mixed src, edp_species_mixed dst, con
         int64_t k = k0 + threadIdx.x;
         int c = k < n ? src.cell[k] : -1;
         uint32_t key = c >= 0 ? tile_key(c, k, ntx) : 0xFFFFFFFFu;
-        unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+        unsigned peers = edp_warp_peers(key);
         int leader = __ffs(peers) - 1;
         unsigned long long base = 0;
         if (key != 0xFFFFFFFFu && lane == leader) base = atomicAdd(&cursor[key], (unsigned long long)__popc(peers));

@@ -81,10 +81,13 @@ def compare(mixed, fp64):
     return out
 
 
-def compare_paired(mixed, fp64):
+def compare_paired(mixed, fp64, rel_tol=0.01):
     """Paired analysis of runs with the same seeds (mixed[s] and fp64[s] from the same initial plasma): per component
     the per-seed differences d_s, z = mean(d) / (sd(d) / sqrt(seeds)); and the bias the test could detect, 3 sd(d) /
-    sqrt(seeds) relative to the component's mean, as its median over the components (the largest, the smallest)."""
+    sqrt(seeds) relative to the component's mean, as its median over the components (the largest, the smallest).
+    Because the pairing removes the seed's own noise, z sees relative biases of 1e-4 and below, which are no physics
+    difference; the equivalence score excess_z = max(0, |mean(d)| - rel_tol |m|) / se is the distance, in standard
+    errors, by which a component's bias exceeds the tolerance rel_tol of its mean m (0 while it stays inside)."""
     out = {}
     for k, floor in QUANTITIES:
         a = np.asarray([r[k] for r in mixed], dtype=np.float64)
@@ -95,8 +98,11 @@ def compare_paired(mixed, fp64):
         keep = (np.abs(m) > floor) & (se > 0)
         z = d.mean(0)[keep] / se[keep]
         detect = 3.0 * se[keep] / np.abs(m[keep])
+        excess = np.maximum(np.abs(d.mean(0)[keep]) - rel_tol * np.abs(m[keep]), 0.0) / se[keep]
         out[k] = dict(n=int(z.size), max_abs_z=float(np.abs(z).max()) if z.size else 0.0,
                       mean_z2=float((z ** 2).mean()) if z.size else 0.0,
+                      max_excess_z=float(excess.max()) if z.size else 0.0,
+                      max_rel_bias=float((np.abs(d.mean(0)[keep]) / np.abs(m[keep])).max()) if z.size else 0.0,
                       detectable_bias_median=float(np.median(detect)) if z.size else 0.0,
                       detectable_bias_max=float(detect.max()) if z.size else 0.0,
                       detectable_bias_min=float(detect.min()) if z.size else 0.0)

@@ -1,13 +1,16 @@
 """Long-run statistics of the mixed-precision cycle against the plain FP64 device cycle on the RF-driven periodic
 configuration (cfg4 physics, reduced to 64 x 64 cells, 64 particles per cell and 400 steps), over 8 seeds: the EEDF
 (device energy histogram), the electron and ion density profiles, the electron f(v_x) and the ion flux to each wall
-agree within their statistical errors. Both precisions start from the same seed, so the per-seed differences are
-tested (paired z-scores); the test also states the smallest relative bias it could detect."""
+agree within the statistical error across the seeds (Welch z-scores). Both precisions start from the same seed, so
+the per-seed differences are also tested (paired): their mean is so well resolved (relative biases of 1e-4 show)
+that the paired test is an equivalence test, asking that no component's bias exceed 1 % of its value by more than
+6 standard errors (t-distribution with 7 degrees of freedom), and it states the smallest relative bias it could
+detect."""
 import numpy as np
 import pytest
 
 from edipic_b200 import ELECTRONS, PREC_FP64, PREC_MIXED, Simulation, decks
-from edipic_b200.longrun import compare_paired, run
+from edipic_b200.longrun import compare, compare_paired, run
 
 
 @pytest.mark.gpu
@@ -15,17 +18,19 @@ def test_mixed_matches_fp64_statistically(tmp_path):
     kw = dict(steps=400, cells=(64, 64), ppc=64, burn_in=200, sample_every=20, workdir=str(tmp_path))
     mixed = [run(PREC_MIXED, 1000 + s, **kw) for s in range(8)]
     fp64 = [run(PREC_FP64, 1000 + s, **kw) for s in range(8)]
-    z = compare_paired(mixed, fp64)
-    for k, v in z.items():
+    welch = compare(mixed, fp64)
+    paired = compare_paired(mixed, fp64, rel_tol=0.01)
+    for k, v in paired.items():
         if k == "ion_flux" and v["n"] == 0:
             # few ions reach the walls in 200 steps: the two precisions may count exactly the same in every seed
             assert all(a["ion_flux"] == b["ion_flux"] for a, b in zip(mixed, fp64))
             continue
         assert v["n"] > 0, k
-        assert v["max_abs_z"] < 6.0, (k, v)
-        assert v["mean_z2"] < 2.5, (k, v)
+        assert v["max_excess_z"] < 6.0, (k, v)
+        w = welch[k]
+        assert w["max_abs_z"] < 5.0 and w["mean_z2"] < 2.0, (k, w)
     # the pairing makes the comparison sensitive: biases of a few percent of the EEDF or the density would show
-    assert z["eedf"]["detectable_bias_median"] < 0.05 and z["ne"]["detectable_bias_median"] < 0.05, z
+    assert paired["eedf"]["detectable_bias_median"] < 0.05 and paired["ne"]["detectable_bias_median"] < 0.05, paired
     assert min(r["ion_flux"][0] + r["ion_flux"][1] for r in mixed) > 0
 
 
