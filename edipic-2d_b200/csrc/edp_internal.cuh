@@ -311,27 +311,32 @@ __host__ __device__ inline void edp_philox(uint32_t c0, uint32_t c1, uint32_t c2
     out[3] = c3;
 }
 
-// Philox2x32-10 (Salmon et al. SC'11): 64-bit counter {c0, c1}, 32-bit key, multiplier 0xD256D193,
-// Weyl increment 0x9E3779B9
-__host__ __device__ inline void edp_philox2x32(uint32_t c0, uint32_t c1, uint32_t k, uint32_t out[2])
+// The per-particle collision decision draws: SplitMix64 (Steele, Lea and Flood, "Fast splittable pseudorandom
+// number generators", OOPSLA 2014), the generator whose state after n steps is s0 + n * gamma and whose output is the
+// mix64 finaliser of that state, evaluated at position n = (step << 32) | id of the stream seeded by
+// s0 = mix64(seed ^ tag). One draw per particle and step, keyed by (id, step) and independent of the slot order, like
+// the Philox variates; it costs two 64-bit multiplies where Philox2x32-10 takes ten 32-bit rounds, and the push makes
+// one for every particle. Word 0 of a draw is its high half, word 1 its low half.
+#define EDP_SPLITMIX_GAMMA 0x9E3779B97F4A7C15ull
+__host__ __device__ inline uint64_t edp_mix64(uint64_t z)
 {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-#ifdef __CUDA_ARCH__
-        uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
-#else
-        uint64_t p = (uint64_t)0xD256D193u * c0;
-        uint32_t hi = (uint32_t)(p >> 32), lo = (uint32_t)p;
-#endif
-        c0 = hi ^ k ^ c1;
-        c1 = lo;
-        k += 0x9E3779B9u;
-    }
-    out[0] = c0;
-    out[1] = c1;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// the state of the decision stream `tag` at position (step << 32) with id 0 (one per launch)
+__host__ __device__ inline uint64_t edp_draw_base(uint32_t seed_lo, uint32_t seed_hi, uint32_t tag, uint32_t step)
+{
+    const uint64_t s0 = edp_mix64((((uint64_t)seed_hi << 32) | seed_lo) ^ tag);
+    return s0 + ((uint64_t)step << 32) * EDP_SPLITMIX_GAMMA;
+}
+// the draw of particle `id` at the position that `base` names
+__host__ __device__ inline uint64_t edp_draw(uint64_t base, uint32_t id)
+{
+    return edp_mix64(base + (uint64_t)id * EDP_SPLITMIX_GAMMA);
 }
 
-// counter words of the Philox2x32 decision draws (xor-ed into the low seed word)
+// stream tags of the decision draws
 #define EDP_SEL_MCC 0x4D430000u
 #define EDP_SEL_RCX(s) (0x52430000u | (uint32_t)(s))
 
@@ -451,17 +456,14 @@ struct edp_mcc_out {
     int ion_species;
 };
 
-// Selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS as a per-electron Bernoulli(P_max) test. The per-particle
-// decision draws come from Philox2x32-10 (key = id, counter = {step, seed_lo ^ EDP_SEL_MCC}): word 0 is the
-// selection variate, word 1 the kind variate r. Returns r when selected.
+// Selection of PERFORM_ELECTRON_NEUTRAL_COLLISIONS as a per-electron Bernoulli(P_max) test. The decision draw of the
+// electron (stream EDP_SEL_MCC): word 0 is the selection variate, word 1 the kind variate r. Returns r when selected.
 __device__ __forceinline__ bool edp_mcc_select(const edp_mcc_dev* m, uint32_t id, uint32_t step, uint32_t seed_lo,
                                                uint32_t seed_hi, double& r)
 {
-    (void)seed_hi;
-    uint32_t w[2];
-    edp_philox2x32(step, seed_lo ^ EDP_SEL_MCC, id, w);
-    if ((unsigned long long)w[0] >= m->pmax_x) return false;
-    r = edp_u01(w[1]);
+    const uint64_t z = edp_draw(edp_draw_base(seed_lo, seed_hi, EDP_SEL_MCC, step), id);
+    if ((unsigned long long)(uint32_t)(z >> 32) >= m->pmax_x) return false;
+    r = edp_u01((uint32_t)z);
     return true;
 }
 
@@ -555,17 +557,16 @@ __device__ inline edp_mcc_out edp_mcc_electron(const edp_mcc_dev* m, uint32_t id
 
 // PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:90-121) for one ion; true on exchange.
 // The test r <= sqrt(P^2 + P_th^2), P = n dt N_sub |v| V_scale sigma(E), is evaluated as r^2 <= P^2 + P_th^2.
-// the same with the decision word w0 (word 0 of Philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id)) drawn by the
-// caller, so that a thread can draw for several ions at once
+// the same with the decision word w0 (word 0 of the ion's decision draw in stream EDP_SEL_RCX(species)) drawn by the
+// caller
 __device__ __forceinline__ bool edp_rcx_ion_drawn(const edp_rcx_dev& r, uint32_t w0, uint32_t id, uint32_t step,
                                                   uint32_t species, uint32_t seed_lo, uint32_t seed_hi, double& vx,
                                                   double& vy, double& vz);
 __device__ __forceinline__ bool edp_rcx_ion(const edp_rcx_dev& r, uint32_t id, uint32_t step, uint32_t species,
                                             uint32_t seed_lo, uint32_t seed_hi, double& vx, double& vy, double& vz)
 {
-    uint32_t w[2];
-    edp_philox2x32(step, seed_lo ^ EDP_SEL_RCX(species), id, w);
-    return edp_rcx_ion_drawn(r, w[0], id, step, species, seed_lo, seed_hi, vx, vy, vz);
+    const uint64_t z = edp_draw(edp_draw_base(seed_lo, seed_hi, EDP_SEL_RCX(species), step), id);
+    return edp_rcx_ion_drawn(r, (uint32_t)(z >> 32), id, step, species, seed_lo, seed_hi, vx, vy, vz);
 }
 __device__ __forceinline__ bool edp_rcx_ion_drawn(const edp_rcx_dev& r, uint32_t w0, uint32_t id, uint32_t step,
                                                   uint32_t species, uint32_t seed_lo, uint32_t seed_hi, double& vx,

@@ -28,6 +28,7 @@ struct PushArgs {
     float qh, ez_term, xmul;
     int use_rot, species, do_coll;
     uint32_t step;
+    uint64_t draw_base;            // edp_draw_base of this species' decision stream at this step
     const edp_mcc_dev* mcc;
     edp_rcx_dev rcx;
     edp_dev_counters* dc;
@@ -171,14 +172,11 @@ __device__ __forceinline__ long long fix_round(double x)
 
 // One particle. Returns false when it was absorbed (the caller stores cell = -1).
 // ION: ion species (acc_E, RCX) instead of electrons (E, MCC selection); PER: periodic x; ROT: Boris rotation.
-// The collision decision word of one particle: word 0 of its Philox2x32 draw keyed by (id, step) for MCC selection
-// (electrons) or charge exchange (ions).
-template <bool ION>
+// The collision decision word of one particle: word 0 of its decision draw keyed by (id, step), in the stream of MCC
+// selection (electrons) or charge exchange (ions) whose base the host computed for this launch.
 __device__ __forceinline__ uint32_t push_draw(const PushArgs& a, uint32_t id)
 {
-    uint32_t w[2];
-    edp_philox2x32(a.step, a.kp.seed_lo ^ (ION ? EDP_SEL_RCX((uint32_t)(a.species - 1)) : EDP_SEL_MCC), id, w);
-    return w[0];
+    return (uint32_t)(edp_draw(a.draw_base, id) >> 32);
 }
 
 template <bool ION, bool PER, bool ROT>
@@ -332,10 +330,10 @@ __device__ __forceinline__ bool push_one(const PushArgs& a, Smem& s, bool window
     }
     // ---- collisions in the epilogue, with the variates of the separate passes
     // the decision draw after the push, for the particles still present (as edp_mcc_select / edp_rcx_ion)
-    if (!ION && a.do_coll) selected = (unsigned long long)push_draw<false>(a, id) < a.mcc->pmax_x;
+    if (!ION && a.do_coll) selected = (unsigned long long)push_draw(a, id) < a.mcc->pmax_x;
     if (ION && a.do_coll) {
         double dvx = vx, dvy = vy, dvz = vz;
-        if (edp_rcx_ion_drawn(a.rcx, push_draw<true>(a, id), id, a.step, (uint32_t)(a.species - 1), kp.seed_lo,
+        if (edp_rcx_ion_drawn(a.rcx, push_draw(a, id), id, a.step, (uint32_t)(a.species - 1), kp.seed_lo,
                               kp.seed_hi, dvx, dvy, dvz)) {
             vx = (float)dvx;
             vy = (float)dvy;
@@ -1471,6 +1469,8 @@ int edp_launch_push(edp_ctx* c, int sp, bool ion_step, bool fuse)
         a.species = sp;
         a.do_coll = do_mcc || do_rcx;
         a.step = (uint32_t)c->t_cntr;
+        a.draw_base = edp_draw_base(c->kp.seed_lo, c->kp.seed_hi, is_ion ? EDP_SEL_RCX((uint32_t)s) : EDP_SEL_MCC,
+                                    a.step);
         a.mcc = c->mcc_dev;
         if (do_rcx) a.rcx = edp_make_rcx_dev(c, s);
         a.dc = c->dc;

@@ -57,10 +57,13 @@ inline void remove_particle(oracle_parts_t* p, int64_t k)
 
 inline double uniform(uint32_t x) { return ((double)x + 0.5) * 0x1p-32; }
 
-void philox_decision(uint32_t id, uint64_t seed, uint32_t step, uint32_t tag, uint32_t out[2])
+// the collision decision draw of particle `id` at `step` in stream `tag`: SplitMix64 seeded with mix64(seed ^ tag) at
+// position (step << 32) | id; word 0 is the high half
+void decision_draw(uint32_t id, uint64_t seed, uint32_t step, uint32_t tag, uint32_t out[2])
 {
-    uint32_t ctr[2] = {step, (uint32_t)seed ^ tag};
-    oracle_philox2x32_10(ctr, id, out);
+    const uint64_t z = oracle_splitmix64_at(oracle_mix64(seed ^ tag), ((uint64_t)step << 32) | id);
+    out[0] = (uint32_t)(z >> 32);
+    out[1] = (uint32_t)z;
 }
 
 void philox_block(uint32_t id, uint64_t seed, uint32_t step, uint32_t stream, uint32_t block, uint32_t out[4])
@@ -1213,7 +1216,7 @@ static void mcc_range(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, 
     const double pmax = tab->max_colliding_fraction;
     for (int64_t k = lo; k < hi; ++k) {
         uint32_t w[2];
-        philox_decision(e->id[k], c->seed, c->step, 0x4D430000u, w);
+        decision_draw(e->id[k], c->seed, c->step, 0x4D430000u, w);
         if (!(uniform(w[0]) < pmax)) continue;
         double r = uniform(w[1]);
         double vx = e->vx[k], vy = e->vy[k], vz = e->vz[k];
@@ -1304,7 +1307,7 @@ int64_t oracle_rcx_philox(const oracle_rcx_t* r, const oracle_mcc_ctx_t* c, uint
         double kf = (r->prob_factor * ((r->sigma_1eV * l) * l)) * r->v_scale_ms;
         double p2 = (kf * kf) * vsq + pt2;
         uint32_t w[2];
-        philox_decision(ions->id[k], c->seed, c->step, 0x52430000u | species, w);
+        decision_draw(ions->id[k], c->seed, c->step, 0x52430000u | species, w);
         double u = uniform(w[0]);
         if (u * u <= p2) {
             uint32_t b[4];

@@ -18,7 +18,9 @@ void   oracle_well_set_state(oracle_well_t* s, const uint32_t* words, int index)
 void   oracle_well_seed(oracle_well_t* s, int32_t seed);
 double oracle_well_next(oracle_well_t* s);
 void   oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
-void   oracle_philox2x32_10(const uint32_t ctr[2], uint32_t key, uint32_t out[2]);
+uint64_t oracle_mix64(uint64_t z);
+uint64_t oracle_splitmix64_at(uint64_t s0, uint64_t n);
+void   oracle_splitmix64_stream(uint64_t s0, int64_t count, uint64_t* out);
 
 /* ---------------------------------------------------------------- geometry
  * Node (i,j) of the reference's cluster arrays, one cluster covering the whole domain.

@@ -109,19 +109,28 @@ void oracle_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], ui
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* Philox2x32-10 of the same paper: 64-bit counter, 32-bit key, multiplier 0xD256D193, Weyl increment
- * 0x9E3779B9. The device cycle uses it for the per-particle decision draws. */
-void oracle_philox2x32_10(const uint32_t ctr_in[2], uint32_t key, uint32_t out[2])
+/* SplitMix64 (Steele, Lea and Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014): the state
+ * after n steps is s0 + n * 0x9E3779B97F4A7C15 (mod 2^64) and each output is the mix64 finaliser of the state. The
+ * device cycle evaluates it at one position per particle and step for the collision decision draws. */
+uint64_t oracle_mix64(uint64_t z)
 {
-    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], k = key;
-    for (int r = 0; r < 10; ++r) {
-        uint32_t hi, lo;
-        mulhilo(0xD256D193u, c0, &hi, &lo);
-        uint32_t n0 = hi ^ k ^ c1;
-        c1 = lo;
-        c0 = n0;
-        k += 0x9E3779B9u;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* output n (n = 1, 2, ...) of the sequential generator seeded with s0: mix64(s0 + n gamma) */
+uint64_t oracle_splitmix64_at(uint64_t s0, uint64_t n)
+{
+    return oracle_mix64(s0 + n * 0x9E3779B97F4A7C15ull);
+}
+
+/* the first `count` outputs of the sequential generator seeded with s0, stepped one state at a time */
+void oracle_splitmix64_stream(uint64_t s0, int64_t count, uint64_t* out)
+{
+    uint64_t s = s0;
+    for (int64_t k = 0; k < count; ++k) {
+        s += 0x9E3779B97F4A7C15ull;
+        out[k] = oracle_mix64(s);
     }
-    out[0] = c0;
-    out[1] = c1;
 }

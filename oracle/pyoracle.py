@@ -98,7 +98,9 @@ def lib():
             "oracle_well_seed": ([C.POINTER(Well), C.c_int32], None),
             "oracle_well_next": ([C.POINTER(Well)], C.c_double),
             "oracle_philox4x32_10": ([_U32, _U32, _U32], None),
-            "oracle_philox2x32_10": ([_U32, C.c_uint32, _U32], None),
+            "oracle_mix64": ([C.c_uint64], C.c_uint64),
+            "oracle_splitmix64_at": ([C.c_uint64, C.c_uint64], C.c_uint64),
+            "oracle_splitmix64_stream": ([C.c_uint64, C.c_int64, C.POINTER(C.c_uint64)], None),
             "oracle_nx_nodes": ([C.POINTER(Geom)], C.c_int32),
             "oracle_push": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64], None),
             "oracle_push_hits": ([C.POINTER(Geom), C.POINTER(Species), _D, _D, C.POINTER(Parts), _I64, _D,
@@ -174,10 +176,22 @@ def philox(ctr, key):
     return tuple(out)
 
 
-def philox2x32(ctr, key):
-    out = (C.c_uint32 * 2)()
-    lib().oracle_philox2x32_10((C.c_uint32 * 2)(*ctr), key, out)
-    return tuple(out)
+def splitmix64_stream(seed, count):
+    """The first `count` outputs of SplitMix64 seeded with `seed`, stepped one state at a time."""
+    out = (C.c_uint64 * count)()
+    lib().oracle_splitmix64_stream(seed, count, out)
+    return list(out)
+
+
+def splitmix64_at(seed, n):
+    """Output n (n >= 1) of SplitMix64 seeded with `seed`, evaluated directly at its position."""
+    return lib().oracle_splitmix64_at(seed, n)
+
+
+def decision_draw(seed, tag, step, pid):
+    """The collision decision draw (word 0, word 1) of particle `pid` at `step` in stream `tag`."""
+    z = splitmix64_at(lib().oracle_mix64(seed ^ tag), (step << 32) | pid)
+    return (z >> 32, z & 0xFFFFFFFF)
 
 
 def maxwell_tables():

@@ -47,10 +47,30 @@ def test_philox_known_answers(ctr, key, expect):
     assert pyoracle.philox(ctr, key) == expect
 
 
-@pytest.mark.parametrize("ctr,key,expect", [
-    ((0, 0), 0, (0xff1dae59, 0x6cd10df2)),
-    ((0xffffffff, 0xffffffff), 0xffffffff, (0x2c3f628b, 0xab4fd7ad)),
-    ((0x243f6a88, 0x85a308d3), 0x13198a2e, (0xdd7ce038, 0xf62a4c12)),
+# SplitMix64's published reference outputs (the sequential generator of Steele, Lea and Flood as distributed with the
+# xoshiro generators): seed 0 and seed 1234567
+@pytest.mark.parametrize("seed,expect", [
+    (0, [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F]),
+    (1234567, [6457827717110365317, 3203168211198807973, 9817491932198370423, 4593380528125082431,
+               16408922859458223821]),
 ])
-def test_philox2x32_known_answers(ctr, key, expect):
-    assert pyoracle.philox2x32(ctr, key) == expect
+def test_splitmix64_known_answers(seed, expect):
+    assert pyoracle.splitmix64_stream(seed, len(expect)) == expect
+    # the direct evaluation at a position, as the decision draws use it, is the same sequence
+    assert [pyoracle.splitmix64_at(seed, n + 1) for n in range(len(expect))] == expect
+
+
+def test_decision_draw_positions():
+    """A decision draw is output (step << 32 | id) of the stream seeded with mix64(seed ^ tag): stepping that stream
+    one state at a time reaches the same words, and distinct (id, step) give distinct draws."""
+    seed, tag = 0x0123456789ABCDEF, 0x4D430000
+    s0 = pyoracle.lib().oracle_mix64(seed ^ tag)
+    seq = pyoracle.splitmix64_stream(s0, 40)
+    for pid in range(1, 41):
+        z = seq[pid - 1]
+        assert pyoracle.decision_draw(seed, tag, 0, pid) == (z >> 32, z & 0xFFFFFFFF)
+    draws = {pyoracle.decision_draw(seed, tag, st, pid) for st in range(50) for pid in range(200)}
+    assert len(draws) == 50 * 200
+    # word 0 is uniform enough for a Bernoulli(P_max) selection at P_max = 1/64: counts over 2^16 draws
+    hits = sum(pyoracle.decision_draw(seed, tag, st, pid)[0] < (1 << 26) for st in range(64) for pid in range(1024))
+    assert abs(hits - 1024) < 5 * 32
