@@ -12,8 +12,8 @@ case function, 627 T_cntr, 628/629 the load-balance counters, 630 Save_probes_e_
 632 current_snap, 633 particle_master, 634 max_N_electrons, 635 N_electrons, 636 total_cathode_N_e_to_inject, then
 max_N_ions(s), N_ions(s) per species and last len_surf_charge. Values are in the machine's byte order.
 
-The device keeps no WELL19937a stream (its variates are Philox keyed by particle id and step), so a checkpoint written
-here carries either the RNG states of the checkpoint the run was loaded from, or per-rank states seeded as
+The device keeps no WELL19937a stream (its variates are counter-based, keyed by particle id and step), so a checkpoint
+written here carries either the RNG states of the checkpoint the run was loaded from, or per-rank states seeded as
 well_random_seed (pic2d_RandomNumberInterface.f90:39-57) does. The surface charges of dielectric inner objects are
 rank 0's REAL(8) block, each object's outline in the order of its boundary nodes (pic2d_Checkpoints.f90:806-812);
 dielectric walls and object potentials (external circuits) are outside the device path and rejected on loading.

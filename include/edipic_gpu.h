@@ -94,7 +94,7 @@ typedef struct edp_params {
     int32_t inner_ileft[EDP_MAX_INNER], inner_jbottom[EDP_MAX_INNER];
     int32_t inner_iright[EDP_MAX_INNER], inner_jtop[EDP_MAX_INNER];
     double inner_phi[EDP_MAX_INNER];
-    uint64_t seed;                  /* Philox key for all device random streams */
+    uint64_t seed;                  /* seed of all device random streams (SplitMix64 decisions, Philox variates) */
     int32_t precision;              /* edp_precision */
     int32_t solver;                 /* edp_solver */
     int32_t sort_every;             /* cell sort period in steps (mixed precision), 0 = never */
