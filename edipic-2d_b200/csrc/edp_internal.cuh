@@ -80,6 +80,35 @@ __device__ __forceinline__ uint32_t edp_tile_key(int cell, int64_t k, int ntx)
     return ((uint32_t)((j >> 4) * ntx + (i >> 4)) << 8) | (uint32_t)((k >> 5) & 255);
 }
 
+// Programmatic dependent launch for chains of short dependent kernels (the CG and multigrid kernels of a solve, the
+// convolutions of a network pass): a kernel launched by edp_launch_dependent may become resident while the kernel
+// before it in the stream is still running. Its first statement is edp_dependent_start(): it waits until that kernel
+// has completed and its writes are visible (griddepcontrol.wait, which returns at once for a kernel launched without
+// the attribute), then lets the kernel after it be launched (griddepcontrol.launch_dependents; that launch happens
+// once every CTA of this grid has said so or exited, so a waiting dependent never holds resources that a CTA of this
+// grid still needs).
+__device__ __forceinline__ void edp_dependent_start()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+inline cudaError_t edp_launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                        Args&&... args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
+
 // the lanes of the (full) warp holding the same key as this lane; a run of 32 sorted slots mostly shares one key,
 // which a shuffle and a vote settle without the slower match
 __device__ __forceinline__ unsigned edp_warp_peers(uint32_t key)

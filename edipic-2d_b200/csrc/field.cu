@@ -358,6 +358,7 @@ __global__ void cg_residual(edp_kparams kp, const int8_t* kind, const double* x,
 __global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, double* Ap, double* pAp, const double* ex,
                         const double* ey)
 {
+    edp_dependent_start();
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     double acc = 0.0;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
@@ -376,6 +377,7 @@ __global__ void cg_spmv(edp_kparams kp, const int8_t* kind, const double* p, dou
 __global__ void cg_update(edp_kparams kp, const int8_t* kind, const double* rr, const double* pAp, const double* p,
                           const double* Ap, double* x, double* r, double* rr_new)
 {
+    edp_dependent_start();
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     const double alpha = *rr / *pAp;
     double acc = 0.0;
@@ -393,6 +395,7 @@ __global__ void cg_update(edp_kparams kp, const int8_t* kind, const double* rr, 
 // sum of a.b over the unknown nodes
 __global__ void pcg_dot(edp_kparams kp, const int8_t* kind, const double* a, const double* b, double* out)
 {
+    edp_dependent_start();
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     double acc = 0.0;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
@@ -405,6 +408,7 @@ __global__ void pcg_dot(edp_kparams kp, const int8_t* kind, const double* a, con
 __global__ void pcg_direction(edp_kparams kp, const int8_t* kind, const double* rz, const double* rz_old,
                               const double* z, double* p)
 {
+    edp_dependent_start();
     int64_t n = (int64_t)kp.nxg * kp.nyg;
     const double beta = rz_old ? *rz / *rz_old : 0.0;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
@@ -587,21 +591,28 @@ static int cg_block(edp_ctx* c, const CgGeom& g, bool mg, int k0, int n, int che
         if (mg) {
             TRY(edp_mg_apply(c, c->cg_r, c->cg_z));
             ++c->launches;
-            pcg_dot<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_r, c->cg_z, rz);
+            EDP_CUDA(c, edp_launch_dependent(pcg_dot, dim3(gr), dim3(256), 0, c->stream, kp, (const int8_t*)c->cg_kind,
+                                              (const double*)c->cg_r, (const double*)c->cg_z, rz));
             const double* rz_prev = k == 0 ? nullptr : (j ? A + 4 * (j - 1) : P + 4 * (check - 1));
             ++c->launches;
-            pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rz_prev, c->cg_z, c->cg_p);
+            EDP_CUDA(c, edp_launch_dependent(pcg_direction, dim3(gr), dim3(256), 0, c->stream, kp, (const int8_t*)c->cg_kind,
+                                              (const double*)rz, rz_prev, (const double*)c->cg_z, c->cg_p));
         } else {
             rz = rr_before(k);
             if (k) {
                 ++c->launches;
-                pcg_direction<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, rr_before(k - 1), c->cg_r, c->cg_p);
+                EDP_CUDA(c, edp_launch_dependent(pcg_direction, dim3(gr), dim3(256), 0, c->stream, kp,
+                                                  (const int8_t*)c->cg_kind, (const double*)rz,
+                                                  (const double*)rr_before(k - 1), (const double*)c->cg_r, c->cg_p));
             }
         }
         ++c->launches;
-        cg_spmv<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, c->cg_p, c->cg_Ap, pAp, g.epsx, g.epsy);
+        EDP_CUDA(c, edp_launch_dependent(cg_spmv, dim3(gr), dim3(256), 0, c->stream, kp, (const int8_t*)c->cg_kind,
+                                          (const double*)c->cg_p, c->cg_Ap, pAp, g.epsx, g.epsy));
         ++c->launches;
-        cg_update<<<gr, 256, 0, c->stream>>>(kp, c->cg_kind, rz, pAp, c->cg_p, c->cg_Ap, c->phi, c->cg_r, A + 4 * j + 2);
+        EDP_CUDA(c, edp_launch_dependent(cg_update, dim3(gr), dim3(256), 0, c->stream, kp, (const int8_t*)c->cg_kind,
+                                          (const double*)rz, (const double*)pAp, (const double*)c->cg_p,
+                                          (const double*)c->cg_Ap, c->phi, c->cg_r, A + 4 * j + 2));
     }
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;

@@ -117,6 +117,7 @@ constexpr int kSw = kTx + 2 * kHalo, kSh = kTy + 2 * kHalo;
 __global__ void __launch_bounds__(256) mg_smooth_kernel(Lev L, int first_color, int zero_start, const double* uc,
                                                         int nxc)
 {
+    edp_dependent_start();
     __shared__ double su[kSh][kSw];
     __shared__ double sf[kSh][kSw];
     __shared__ int8_t sm[kSh][kSw];
@@ -165,6 +166,7 @@ __global__ void __launch_bounds__(256) mg_smooth_kernel(Lev L, int first_color, 
 
 __global__ void mg_restrict_kernel(Lev F, double* fc, const int8_t* maskc, int nxc, int nyc)
 {
+    edp_dependent_start();
     restrict_to(F, fc, maskc, nxc, nyc, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
                 (int64_t)gridDim.x * blockDim.x);
 }
@@ -184,6 +186,7 @@ struct CoarseArgs {
 // The bottom of the V-cycle in one CTA: every level lives in shared memory, phases are separated by barriers.
 __global__ void __launch_bounds__(kCoarseThreads, 1) mg_coarse_kernel(CoarseArgs a)
 {
+    edp_dependent_start();
     extern __shared__ __align__(16) unsigned char sm[];
     Lev L[EDP_MG_MAX_LEVELS];
     size_t off = 0;
@@ -427,10 +430,12 @@ int edp_mg_apply(edp_ctx* c, const double* r, double* z)
     for (int l = 0; l < lc; ++l) {
         Lev L = lev_of(c, l, u_of(l), f_of(l));
         ++c->launches;   // pre-smoothing from a zero correction: red, black, red, black
-        mg_smooth_kernel<<<tiles(L), 256, 0, c->stream>>>(L, 0, 1, nullptr, 0);
+        EDP_CUDA(c, edp_launch_dependent(mg_smooth_kernel, tiles(L), dim3(256), 0, c->stream, L, 0, 1,
+                                          (const double*)nullptr, 0));
         ++c->launches;
-        mg_restrict_kernel<<<grid_of_nodes(c->mg[l + 1].nx, c->mg[l + 1].ny), 256, 0, c->stream>>>(
-            L, c->mg[l + 1].f, c->mg[l + 1].mask, c->mg[l + 1].nx, c->mg[l + 1].ny);
+        EDP_CUDA(c, edp_launch_dependent(mg_restrict_kernel, dim3(grid_of_nodes(c->mg[l + 1].nx, c->mg[l + 1].ny)),
+                                          dim3(256), 0, c->stream, L, c->mg[l + 1].f,
+                                          (const int8_t*)c->mg[l + 1].mask, c->mg[l + 1].nx, c->mg[l + 1].ny));
     }
     CoarseArgs a;
     memset(&a, 0, sizeof(a));
@@ -447,11 +452,12 @@ int edp_mg_apply(edp_ctx* c, const double* r, double* z)
     a.cidx = c->mg_cidx;
     a.cn = c->mg_cn;
     ++c->launches;
-    mg_coarse_kernel<<<1, kCoarseThreads, c->mg_smem, c->stream>>>(a);
+    EDP_CUDA(c, edp_launch_dependent(mg_coarse_kernel, dim3(1), dim3(kCoarseThreads), c->mg_smem, c->stream, a));
     for (int l = lc - 1; l >= 0; --l) {
         Lev L = lev_of(c, l, u_of(l), f_of(l));
         ++c->launches;   // prolongation, then post-smoothing: black, red, black, red
-        mg_smooth_kernel<<<tiles(L), 256, 0, c->stream>>>(L, 1, 0, c->mg[l + 1].u, c->mg[l + 1].nx);
+        EDP_CUDA(c, edp_launch_dependent(mg_smooth_kernel, tiles(L), dim3(256), 0, c->stream, L, 1, 0,
+                                          (const double*)c->mg[l + 1].u, c->mg[l + 1].nx));
     }
     EDP_CUDA(c, cudaGetLastError());
     return EDP_OK;

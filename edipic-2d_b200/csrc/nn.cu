@@ -17,7 +17,6 @@
 #include <cuda_bf16.h>
 
 #include <mutex>
-#include <utility>
 #include <vector>
 
 namespace {
@@ -27,18 +26,6 @@ typedef __nv_bfloat16 bf16;
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
     return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Programmatic dependent launch between the convolutions of a forward pass: a kernel launched with
-// launch_dependent() may become resident while the kernel before it in the stream is still running. Its first
-// statement waits until that kernel has completed and its writes are visible (griddepcontrol.wait, which returns at
-// once for a kernel launched without the attribute), and it then lets the kernel after it be launched
-// (griddepcontrol.launch_dependents; the launch happens once every CTA of this grid has said so or exited, so a
-// waiting dependent never holds resources that a CTA of this grid still needs).
-__device__ __forceinline__ void dependent_start()
-{
-    asm volatile("griddepcontrol.wait;\n" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid)
@@ -131,7 +118,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     conv3x3_fwd_tma_kernel(const __grid_constant__ CUtensorMap mx1, const __grid_constant__ CUtensorMap mx2,
                            const __grid_constant__ CUtensorMap mw, TmaArgs ta)
 {
-    dependent_start();
+    edp_dependent_start();
     constexpr int STAGES = 4;
     constexpr int A_BYTES = 128 * CW * 2, B_BYTES = BN * CW * 2, STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
@@ -339,7 +326,7 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
     conv3x3_fwd_halo_kernel(const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap mx1,
                             const __grid_constant__ CUtensorMap mx2, HaloArgs a)
 {
-    dependent_start();
+    edp_dependent_start();
     // NACC partial accumulators per tile (tap % NACC), summed in the epilogue: consecutive MMAs of the short (small N)
     // chains go to independent accumulators; two tiles' sets of them (double buffering)
     constexpr int NACC = kHaloAcc<BN>;
@@ -557,7 +544,7 @@ __global__ void __launch_bounds__(kHaloFwdThreads, 1)
 __global__ void conv_finish_kernel(const float* __restrict__ ws, int ks, int64_t n4, int cout,
                                    const float* __restrict__ bias, int relu, bf16* __restrict__ y)
 {
-    dependent_start();
+    edp_dependent_start();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
         float4 v = reinterpret_cast<const float4*>(ws)[i];
         for (int z = 1; z < ks; ++z) {
@@ -765,24 +752,6 @@ bool map_wt(CUtensorMap* m, const void* wt, int k, int cout, int cw, int bn)
     return map_cached(MapKey{2, wt, k, cout, cw, bn, 0}, m, make_wt);
 }
 
-// launch with the programmatic-stream-serialisation attribute (the kernel starts with dependent_start())
-template <typename... KArgs, typename... Args>
-cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                             Args&&... args)
-{
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
-
 template <int BN, int CW>
 int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
 {
@@ -834,13 +803,13 @@ int launch_tma(const ConvArgs& c, int* err, cudaStream_t s)
         if (!ta.ws) return EDP_ERR_CUDA;
     }
     dim3 grid((unsigned)(ta.tiles_x * ta.tiles_y * c.nimg), c.cout / BN, (unsigned)ks);
-    if (launch_dependent(conv3x3_fwd_tma_kernel<BN, CW>, grid, dim3(kTcThreads), SMEM, s, m1, m2, mw, ta) != cudaSuccess)
+    if (edp_launch_dependent(conv3x3_fwd_tma_kernel<BN, CW>, grid, dim3(kTcThreads), SMEM, s, m1, m2, mw, ta) != cudaSuccess)
         return EDP_ERR_CUDA;
     if (ks > 1) {
         const int64_t n4 = P * c.cout / 4;
         int64_t g = (n4 + 255) / 256;
         if (g > 148 * 8) g = 148 * 8;
-        if (launch_dependent(conv_finish_kernel, dim3((unsigned)g), dim3(256), 0, s, (const float*)ta.ws, ks, n4, c.cout,
+        if (edp_launch_dependent(conv_finish_kernel, dim3((unsigned)g), dim3(256), 0, s, (const float*)ta.ws, ks, n4, c.cout,
                              c.bias, c.relu, c.y) != cudaSuccess)
             return EDP_ERR_CUDA;
     }
@@ -915,7 +884,7 @@ int launch_halo(const ConvArgs& c, int* err, cudaStream_t s)
     if (per_sm > 512 / kHaloTmemCols<BN>) per_sm = 512 / kHaloTmemCols<BN>;
     if (per_sm < 1) per_sm = 1;
     const int64_t grid = a.n_tiles < (int64_t)sms * per_sm ? a.n_tiles : (int64_t)sms * per_sm;
-    if (launch_dependent(conv3x3_fwd_halo_kernel<BN, STREAM>, dim3((unsigned)grid), dim3(kHaloFwdThreads), smem, s, mw,
+    if (edp_launch_dependent(conv3x3_fwd_halo_kernel<BN, STREAM>, dim3((unsigned)grid), dim3(kHaloFwdThreads), smem, s, mw,
                          mx1, mx2, a) != cudaSuccess)
         return EDP_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? EDP_OK : EDP_ERR_CUDA;
