@@ -206,8 +206,9 @@ int32_t oracle_en_scatter(int32_t kind, double energy_eV, double threshold_eV, d
                           double ion_velocity_factor, const double* maxwell_v, const double* u,
                           double* v, double* new_e, double* new_i);
 
-/* Per-particle null-collision MCC driven by Philox4x32-10, the variate layout shared with the GPU kernels:
- *   decision draws: Philox2x32-10, key = id, counter = {step, seed_lo ^ 0x4D430000}: {select, kind r};
+/* Per-particle null-collision MCC with the variate layout shared with the GPU kernels:
+ *   decision draws: SplitMix64 seeded with mix64(seed ^ 0x4D430000) at position (step << 32) | id: {select = high
+ *   half, kind r = low half};
  *   scattering variates: Philox4x32-10, key = {id, seed_lo}, counter = {step, 0, block 1/2, seed_hi};
  *   u = (x + 0.5) * 2^-32.
  * Ionisation products are appended to *born_e / *born_i (capacity checked). counters[k] counts kind k+1. */
@@ -222,9 +223,9 @@ typedef struct {
 void oracle_mcc_philox(const oracle_mcc_table_t* tab, const oracle_mcc_ctx_t* c, oracle_parts_t* e,
                        oracle_parts_t* born_e, oracle_parts_t* born_i, int64_t cap_born, int64_t* counters);
 
-/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126): hit variate from Philox2x32-10
- * (key = id, counter = {step, seed_lo ^ (0x52430000 | species)}), Maxwellian from Philox4x32-10 block 1 of stream
- * 1 + (species << 8). Returns the number of exchanges. */
+/* PERFORM_RESONANT_CHARGE_EXCHANGE (pic2d_inCollisionsSpecificProc.f90:48-126): hit variate = high half of the
+ * SplitMix64 decision draw of stream 0x52430000 | species (seeded with mix64(seed ^ tag), position (step << 32) | id),
+ * Maxwellian from Philox4x32-10 block 1 of stream 1 + (species << 8). Returns the number of exchanges. */
 typedef struct {
     double prob_factor;        /* ngas * dt * N_subcycles */
     double v_scale_ms;
