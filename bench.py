@@ -164,12 +164,13 @@ def cpu_baseline(args, seconds=12.0):
     """The oracle's cycle (the FP64 restatement of the reference routines) on the host cores: the line's
     workload per particle (its configuration's physics and particles per cell, the grid sampled to 256 x 128 cells)
     on all host threads and on one thread, plus the reference's own CPU-runnable case (cfg0: 128 x 128 cells,
-    64 + 64 per cell, FFT_X) on all threads. Each leg steps for about `seconds`."""
+    64 + 64 per cell, FFT_X) on all threads and on one thread. Each leg steps for about `seconds`."""
     threads = os.cpu_count() or 1
     sx, sy = min(args.cells_x, 256), min(args.cells_y, 128)
     v_all, st_all, el_all, n_all = _oracle_cycle_rate(args.config, sx, sy, args.ppc, threads, seconds)
     v_one, st_one, el_one, _ = _oracle_cycle_rate(args.config, sx, sy, args.ppc, 1, seconds)
     v_c0, st_c0, el_c0, n_c0 = _oracle_cycle_rate("cfg0", 128, 128, 64, threads, seconds)
+    v_c01, st_c01, el_c01, _ = _oracle_cycle_rate("cfg0", 128, 128, 64, 1, seconds)
     return {"value": v_all, "unit": "particle-steps/s", "cores": threads, "kind": "port",
             "cpu_model": host_cpu_model(),
             "sample": f"{args.config} physics on {sx}x{sy} cells x {args.ppc}+{args.ppc} per cell ({n_all} "
@@ -177,7 +178,8 @@ def cpu_baseline(args, seconds=12.0):
                       f"FFT_X (the reference's Fortran/MPI/PETSc cannot be built in this image)",
             "one_thread": {"value": v_one, "steps": st_one, "seconds": el_one},
             "cfg0_all_threads": {"value": v_c0, "steps": st_c0, "seconds": el_c0,
-                                 "sample": f"cfg0: 128x128 cells x 64+64 per cell ({n_c0} particles), FFT_X"}}
+                                 "sample": f"cfg0: 128x128 cells x 64+64 per cell ({n_c0} particles), FFT_X"},
+            "cfg0_one_thread": {"value": v_c01, "steps": st_c01, "seconds": el_c01}}
 
 
 def line_config(args, world=1, per_gpu_particles=None):
