@@ -344,8 +344,9 @@ __host__ __device__ inline void edp_philox(uint32_t c0, uint32_t c1, uint32_t c2
 // number generators", OOPSLA 2014), the generator whose state after n steps is s0 + n * gamma and whose output is the
 // mix64 finaliser of that state, evaluated at position n = (step << 32) | id of the stream seeded by
 // s0 = mix64(seed ^ tag). One draw per particle and step, keyed by (id, step) and independent of the slot order, like
-// the Philox variates; it costs two 64-bit multiplies where Philox2x32-10 takes ten 32-bit rounds, and the push makes
-// one for every particle. Word 0 of a draw is its high half, word 1 its low half.
+// the Philox variates; with the stream's position of id 0 computed once per launch (edp_draw_base) a draw costs one
+// 32 x 64-bit and two 64-bit multiplies where Philox2x32-10 takes ten dependent 32-bit rounds, and the push makes one
+// for every particle. Word 0 of a draw is its high half, word 1 its low half.
 #define EDP_SPLITMIX_GAMMA 0x9E3779B97F4A7C15ull
 __host__ __device__ inline uint64_t edp_mix64(uint64_t z)
 {
